@@ -1,0 +1,222 @@
+"""firefly_b200 — B200 (sm_100a) wavefront path tracer behind a C ABI.
+
+Python mirror of the reference's host-side interface (JakeKurtz/Firefly,
+CUDA-RayTracer/):
+
+* :class:`dScene` — the device scene (dScene.h:13-65): built from triangle
+  arrays, materials, lights and a camera; ``update()`` replaces the camera
+  (dScene::update, dScene.cpp:55-58).  The BVH is built on the device.
+* :class:`PathTracer` — the tracer (PathTracer.h:11-62): ``PathTracer(w, h)``,
+  ``draw(scene)`` and ``clear_buffer()``, with a headless film instead of the
+  GL surface.
+* :meth:`dScene.trace` — closest-hit / any-hit ray queries (wf_extend /
+  wf_shadow, kernel.cu:488-543).
+
+Everything runs in libfirefly_b200.so; this module only marshals arguments.
+Errors are raised as :class:`FireflyError` carrying the ABI status code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi as A
+from ._abi import (FF_MAT_COAT, FF_MAT_CONDUCTOR, FF_MAT_DIELECTRIC, FF_MAT_DIFFUSE, FF_MAT_MIX,
+                   FF_MODE_CORRECTED, FF_MODE_PARITY, FF_TRACE_ANY, FF_TRACE_CLOSEST)
+
+__all__ = ["Context", "dScene", "PathTracer", "FireflyError", "lib", "FF_MAT_MIX", "FF_MAT_DIFFUSE",
+           "FF_MAT_CONDUCTOR", "FF_MAT_DIELECTRIC", "FF_MAT_COAT", "FF_MODE_PARITY", "FF_MODE_CORRECTED",
+           "FF_TRACE_ANY", "FF_TRACE_CLOSEST", "HIT_DTYPE", "RAY_DTYPE"]
+
+RAY_DTYPE = np.dtype([("o", np.float32, 3), ("tmin", np.float32), ("d", np.float32, 3), ("tmax", np.float32)])
+HIT_DTYPE = np.dtype([("t", np.float32), ("u", np.float32), ("v", np.float32), ("prim", np.int32)])
+
+
+class FireflyError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{A.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def lib() -> C.CDLL:
+    return A.load()
+
+
+def _check(status: int, ctx_ptr=None):
+    if status != A.FF_OK:
+        msg = lib().ff_last_error_message(ctx_ptr)
+        raise FireflyError(status, (msg or b"").decode(errors="replace"))
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """One CUDA device and one stream (ff_context)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        opts = A.ff_device_opts(device=device, stream=stream, flags=0)
+        h = C.c_void_p()
+        _check(lib().ff_context_create(C.byref(opts), C.byref(h)))
+        self.handle = h
+        self.device = device
+
+    @property
+    def stream(self) -> int:
+        return lib().ff_context_stream(self.handle)
+
+    def sync(self):
+        _check(lib().ff_context_sync(self.handle), self.handle)
+
+    def close(self):
+        if self.handle:
+            lib().ff_context_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class dScene:
+    """Device scene (ff_scene).  Arrays are copied at construction."""
+
+    def __init__(self, ctx: Context, scene):
+        self.ctx = ctx
+        s = scene
+        self._keep = []
+        P = np.ascontiguousarray(s.positions, np.float32)
+        I = np.ascontiguousarray(s.indices, np.uint32)
+        N = None if s.normals is None else np.ascontiguousarray(s.normals, np.float32)
+        T = None if s.texcoords is None else np.ascontiguousarray(s.texcoords, np.float32)
+        M = None if s.material_ids is None else np.ascontiguousarray(s.material_ids, np.uint32)
+        E = None if s.env_rgb is None else np.ascontiguousarray(s.env_rgb, np.float32)
+        mats = (A.ff_material * max(1, len(s.materials)))(*s.materials)
+        lights = (A.ff_area_light * max(1, len(s.area_lights)))(*s.area_lights)
+        d = A.ff_scene_desc()
+        d.positions, d.num_vertices = _ptr(P), P.shape[0]
+        d.indices, d.num_triangles = _ptr(I), I.shape[0]
+        d.normals, d.texcoords, d.material_ids = _ptr(N), _ptr(T), _ptr(M)
+        d.materials = C.cast(mats, C.c_void_p)
+        d.num_materials = len(s.materials)
+        d.textures, d.num_textures = None, 0
+        d.env_rgb = _ptr(E)
+        d.env_width = 0 if E is None else E.shape[1]
+        d.env_height = 0 if E is None else E.shape[0]
+        for k in range(3):
+            d.env_color[k] = float(s.env_color[k])
+        d.area_lights = C.cast(lights, C.c_void_p)
+        d.num_area_lights = len(s.area_lights)
+        if s.camera is not None:
+            d.camera = s.camera
+        h = C.c_void_p()
+        _check(lib().ff_scene_create(ctx.handle, C.byref(d), C.byref(h)), ctx.handle)
+        self.handle = h
+        self.source = scene
+
+    def update(self, camera: A.ff_camera):
+        """dScene::update: replace the camera."""
+        _check(lib().ff_scene_update_camera(self.handle, C.byref(camera)), self.ctx.handle)
+
+    def stats(self) -> dict:
+        st = A.ff_scene_stats()
+        _check(lib().ff_scene_get_stats(self.handle, C.byref(st)), self.ctx.handle)
+        return {k: (list(getattr(st, k)) if k.startswith("scene_") else getattr(st, k)) for k, _ in st._fields_}
+
+    def trace(self, rays: np.ndarray, any_hit: bool = False, out: np.ndarray | None = None) -> np.ndarray:
+        """Host rays (n x 8 float32 or RAY_DTYPE) -> host hits (HIT_DTYPE).
+
+        Synchronous: copies the rays in, traces, copies the hits out.  Pass
+        pinned buffers (rays and ``out``) for full copy bandwidth."""
+        if rays.dtype == RAY_DTYPE:
+            rays = rays.view(np.float32)
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        if out is None:
+            out = np.empty(r.shape[0], HIT_DTYPE)
+        elif out.dtype != HIT_DTYPE or out.shape != (r.shape[0],) or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous HIT_DTYPE array with one entry per ray")
+        flags = A.FF_TRACE_ANY if any_hit else A.FF_TRACE_CLOSEST
+        _check(lib().ff_trace(self.ctx.handle, self.handle, _ptr(r), r.shape[0], _ptr(out), flags),
+               self.ctx.handle)
+        return out
+
+    def trace_device(self, rays_ptr: int, n: int, hits_ptr: int, any_hit: bool = False):
+        """Device pointers (e.g. torch tensors' data_ptr()), asynchronous on the context stream."""
+        flags = (A.FF_TRACE_ANY if any_hit else A.FF_TRACE_CLOSEST) | A.FF_MEM_DEVICE
+        _check(lib().ff_trace(self.ctx.handle, self.handle, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr), flags),
+               self.ctx.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().ff_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PathTracer:
+    """The wavefront tracer with its film (PathTracer(w, h), draw, clear_buffer)."""
+
+    def __init__(self, ctx: Context, w: int, h: int):
+        self.ctx = ctx
+        self.width, self.height = w, h
+        f = C.c_void_p()
+        _check(lib().ff_film_create(ctx.handle, w, h, C.byref(f)), ctx.handle)
+        self.film = f
+        self.last_stats = None
+
+    def draw(self, scene: dScene, spp: int = 1, max_depth: int = 3, rr_depth: int = 3, seed: int = 0,
+             mode: int = A.FF_MODE_PARITY, light: int = -1, max_paths: int = 0, sample_offset: int = 0,
+             shadow_offset: float = 0.001) -> dict:
+        s = A.ff_render_settings(spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed, mode=mode,
+                                 light=light, max_paths=max_paths, sample_offset=sample_offset, flags=0,
+                                 shadow_offset=shadow_offset)
+        st = A.ff_render_stats()
+        _check(lib().ff_render(self.ctx.handle, scene.handle, C.byref(s), self.film, C.byref(st)), self.ctx.handle)
+        self.last_stats = {k: getattr(st, k) for k, _ in st._fields_}
+        return self.last_stats
+
+    def clear_buffer(self):
+        _check(lib().ff_film_clear(self.film), self.ctx.handle)
+
+    def read(self):
+        """(rgba float32 [h, w, 4], n_samples uint32 [h, w])"""
+        rgba = np.empty((self.height, self.width, 4), np.float32)
+        n = np.empty((self.height, self.width), np.uint32)
+        _check(lib().ff_film_read(self.film, _ptr(rgba), _ptr(n), A.FF_MEM_HOST), self.ctx.handle)
+        return rgba, n
+
+    def image(self):
+        """Mean radiance per pixel (accum / n), float32 [h, w, 3]."""
+        rgba, n = self.read()
+        return rgba[..., :3] / np.maximum(n, 1)[..., None]
+
+    def tonemap(self, exposure: float = 1.0) -> np.ndarray:
+        out = np.empty((self.height, self.width, 4), np.uint8)
+        _check(lib().ff_film_tonemap(self.film, exposure, _ptr(out), A.FF_MEM_HOST), self.ctx.handle)
+        return out
+
+    def close(self):
+        if getattr(self, "film", None):
+            lib().ff_film_destroy(self.film)
+            self.film = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

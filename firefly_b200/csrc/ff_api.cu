@@ -1,0 +1,263 @@
+// ff_api.cu — the extern "C" entry points declared in include/firefly_b200.h.
+//
+// Every entry point catches FFError and CUDA failures and returns an
+// ff_status; nothing here exits or aborts the process (the reference calls
+// exit(99) from checkCudaErrors, CUDA-RayTracer/CudaHelpers.cpp:3-11).
+#include <cstring>
+#include <new>
+
+#include "ff_internal.h"
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <class F>
+ff_status guarded(ff_context* ctx, F&& f)
+{
+    try {
+        f();
+        return FF_OK;
+    } catch (const FFError& e) {
+        if (ctx) ctx->last_error = e.msg;
+        else g_create_error = e.msg;
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        if (ctx) ctx->last_error = "host allocation failed";
+        return FF_ERR_OOM;
+    } catch (...) {
+        if (ctx) ctx->last_error = "unknown internal error";
+        return FF_ERR_INTERNAL;
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) FF_CUDA_CHECK(cudaSetDevice(dev));
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+void upload(DevBuf& b, const void* host, size_t bytes, cudaStream_t st)
+{
+    b.alloc(bytes);
+    if (bytes) FF_CUDA_CHECK(cudaMemcpyAsync(b.ptr, host, bytes, cudaMemcpyHostToDevice, st));
+}
+
+}  // namespace
+
+size_t ff_scene::device_bytes() const
+{
+    size_t total = nodes.bytes + tris.bytes + shade.bytes + materials.bytes + tex_table.bytes + area_lights.bytes +
+                   env.rgb.bytes + env.marginal.bytes + env.conditional.bytes + env.pdf.bytes + env.denom.bytes;
+    for (auto* t : textures) total += t->bytes;
+    return total;
+}
+
+// Defined in ff_envmap.cu and ff_scene.cu.
+void ff_build_env_tables(ff_context* ctx, ff_scene* s);
+void ff_build_shading(ff_context* ctx, ff_scene* s, const ff_scene_desc* d, const float3* d_pos,
+                      const uint3* d_idx);
+
+extern "C" {
+
+ff_status ff_context_create(const ff_device_opts* opts, ff_context** out)
+{
+    if (!out) return FF_ERR_INVALID_ARG;
+    *out = nullptr;
+    ff_context* ctx = new (std::nothrow) ff_context();
+    if (!ctx) return FF_ERR_OOM;
+    ff_status st = guarded(nullptr, [&] {
+        int ndev = 0;
+        FF_CUDA_CHECK(cudaGetDeviceCount(&ndev));
+        int dev = opts ? opts->device : 0;
+        FF_REQUIRE(dev >= 0 && dev < ndev, "device ordinal out of range");
+        ctx->device = dev;
+        DeviceGuard g(dev);
+        FF_CUDA_CHECK(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, dev));
+        if (opts && opts->stream) {
+            ctx->stream = reinterpret_cast<cudaStream_t>(opts->stream);
+            ctx->own_stream = false;
+        } else {
+            FF_CUDA_CHECK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+            ctx->own_stream = true;
+        }
+        ctx->counters.alloc(256);
+        FF_CUDA_CHECK(cudaMemsetAsync(ctx->counters.ptr, 0, 256, ctx->stream));
+        FF_CUDA_CHECK(cudaEventCreate(&ctx->ev0));
+        FF_CUDA_CHECK(cudaEventCreate(&ctx->ev1));
+    });
+    if (st != FF_OK) {
+        delete ctx;
+        return st;
+    }
+    *out = ctx;
+    return FF_OK;
+}
+
+ff_status ff_context_destroy(ff_context* ctx)
+{
+    if (!ctx) return FF_ERR_INVALID_ARG;
+    {
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(ctx->device);
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+        ctx->counters.release();
+        ctx->io_rays.release();
+        ctx->io_hits.release();
+        if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+        if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+        if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    delete ctx;
+    return FF_OK;
+}
+
+const char* ff_last_error_message(const ff_context* ctx)
+{
+    if (!ctx) return g_create_error.c_str();
+    return ctx->last_error.c_str();
+}
+
+ff_status ff_context_sync(ff_context* ctx)
+{
+    if (!ctx) return FF_ERR_INVALID_ARG;
+    return guarded(ctx, [&] {
+        DeviceGuard g(ctx->device);
+        FF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+void* ff_context_stream(const ff_context* ctx) { return ctx ? reinterpret_cast<void*>(ctx->stream) : nullptr; }
+
+ff_status ff_scene_create(ff_context* ctx, const ff_scene_desc* d, ff_scene** out)
+{
+    if (!ctx || !d || !out) return FF_ERR_INVALID_ARG;
+    *out = nullptr;
+    ff_scene* s = new (std::nothrow) ff_scene();
+    if (!s) return FF_ERR_OOM;
+    s->ctx = ctx;
+    ff_status st = guarded(ctx, [&] {
+        DeviceGuard g(ctx->device);
+        FF_REQUIRE(d->num_triangles == 0 || (d->positions && d->indices), "positions and indices are required");
+        FF_REQUIRE(d->num_triangles == 0 || d->num_vertices > 0, "num_vertices must be > 0");
+        FF_REQUIRE(d->num_triangles < (1u << 30), "too many triangles");
+        for (uint64_t i = 0; i < 3ull * d->num_triangles; ++i)
+            FF_REQUIRE(d->indices[i] < d->num_vertices, "triangle index out of range");
+        if (d->material_ids) {
+            for (uint32_t i = 0; i < d->num_triangles; ++i)
+                FF_REQUIRE(d->material_ids[i] < (d->num_materials ? d->num_materials : 1u),
+                           "material id out of range");
+        }
+        for (uint32_t m = 0; m < d->num_materials; ++m) {
+            const ff_material& mt = d->materials[m];
+            FF_REQUIRE(mt.kind >= FF_MAT_MIX && mt.kind <= FF_MAT_COAT, "unknown material kind");
+            FF_REQUIRE(mt.base_color_tex < (int32_t)d->num_textures, "texture index out of range");
+            FF_REQUIRE(mt.roughness_tex < (int32_t)d->num_textures, "texture index out of range");
+        }
+        FF_REQUIRE(!d->env_rgb || (d->env_width > 0 && d->env_height > 0), "environment map has zero size");
+        FF_REQUIRE(d->num_area_lights == 0 || d->area_lights, "area_lights is NULL");
+        cudaStream_t stream = ctx->stream;
+        DevBuf pos, idx;
+        upload(pos, d->positions, sizeof(float) * 3ull * d->num_vertices, stream);
+        upload(idx, d->indices, sizeof(uint32_t) * 3ull * d->num_triangles, stream);
+        ff_build_bvh(ctx, s, pos.as<float3>(), idx.as<uint3>(), d->num_triangles);
+        FF_REQUIRE(s->depth <= (uint32_t)kMaxStackDepth, "BVH deeper than the traversal stack");
+        ff_build_shading(ctx, s, d, pos.as<float3>(), idx.as<uint3>());
+        s->camera = d->camera;
+        FF_CUDA_CHECK(cudaStreamSynchronize(stream));
+    });
+    if (st != FF_OK) {
+        delete s;
+        return st;
+    }
+    *out = s;
+    return FF_OK;
+}
+
+ff_status ff_scene_destroy(ff_scene* s)
+{
+    if (!s) return FF_ERR_INVALID_ARG;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    delete s;
+    if (prev >= 0) cudaSetDevice(prev);
+    return FF_OK;
+}
+
+ff_status ff_scene_update_camera(ff_scene* s, const ff_camera* cam)
+{
+    if (!s || !cam) return FF_ERR_INVALID_ARG;
+    s->camera = *cam;
+    return FF_OK;
+}
+
+ff_status ff_scene_get_stats(const ff_scene* s, ff_scene_stats* out)
+{
+    if (!s || !out) return FF_ERR_INVALID_ARG;
+    std::memset(out, 0, sizeof(*out));
+    out->num_triangles = s->num_tris;
+    out->num_nodes = s->num_nodes;
+    out->num_leaf_refs = s->num_tris;
+    out->bvh_depth = s->depth;
+    out->device_bytes = s->device_bytes();
+    out->build_ms = s->build_ms;
+    out->scene_lo[0] = s->lo.x;
+    out->scene_lo[1] = s->lo.y;
+    out->scene_lo[2] = s->lo.z;
+    out->scene_hi[0] = s->hi.x;
+    out->scene_hi[1] = s->hi.y;
+    out->scene_hi[2] = s->hi.z;
+    return FF_OK;
+}
+
+ff_status ff_trace(ff_context* ctx, const ff_scene* s, const ff_ray* rays, uint64_t n, ff_hit* hits,
+                   uint32_t flags)
+{
+    if (!ctx || !s) return FF_ERR_INVALID_ARG;
+    if (n == 0) return FF_OK;
+    if (!rays || !hits) return FF_ERR_INVALID_ARG;
+    if (s->ctx != ctx) {
+        ctx->last_error = "scene belongs to another context";
+        return FF_ERR_INVALID_ARG;
+    }
+    return guarded(ctx, [&] {
+        DeviceGuard g(ctx->device);
+        const bool any = (flags & FF_TRACE_ANY) != 0;
+        if (flags & FF_MEM_DEVICE) {
+            FF_REQUIRE((reinterpret_cast<uintptr_t>(rays) & 15) == 0 && (reinterpret_cast<uintptr_t>(hits) & 15) == 0,
+                       "device rays and hits must be 16-byte aligned");
+            ff_launch_trace(ctx, s, rays, n, hits, any);
+        } else {
+            ctx->io_rays.alloc(sizeof(ff_ray) * n);
+            ctx->io_hits.alloc(sizeof(ff_hit) * n);
+            FF_CUDA_CHECK(cudaMemcpyAsync(ctx->io_rays.ptr, rays, sizeof(ff_ray) * n, cudaMemcpyHostToDevice,
+                                          ctx->stream));
+            ff_launch_trace(ctx, s, ctx->io_rays.as<ff_ray>(), n, ctx->io_hits.as<ff_hit>(), any);
+            FF_CUDA_CHECK(cudaMemcpyAsync(hits, ctx->io_hits.ptr, sizeof(ff_hit) * n, cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+            unsigned int err = 0;
+            FF_CUDA_CHECK(cudaMemcpyAsync(&err, ctx->counters.as<char>() + 8, sizeof(err), cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+            FF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+            if (err) {
+                FF_CUDA_CHECK(cudaMemsetAsync(ctx->counters.as<char>() + 8, 0, sizeof(err), ctx->stream));
+                throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
+            }
+        }
+    });
+}
+
+}  // extern "C"

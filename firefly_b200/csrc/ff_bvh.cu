@@ -1,0 +1,604 @@
+// ff_bvh.cu — device build of the 8-wide BVH with quantised child boxes.
+//
+// Replaces the reference's host SAH build (CUDA-RayTracer/BVH.cpp:52-331,
+// configured at dScene.cpp:372) and its serial device gather
+// (d_reorder_primitives, kernel.cu:184-191).  Pipeline, all on the device:
+//   1. per-triangle records, bounds and centroids           (k_prep)
+//   2. scene centroid bounds                                  (k_centroid_bounds)
+//   3. 63-bit Morton keys, radix sort                         (k_morton + cub)
+//   4. binary radix tree over the sorted keys (Karras 2012)   (k_radix_tree)
+//   5. bottom-up bounds with arrival counters                 (k_bounds_up)
+//   6. top-down collapse into 8-wide nodes, octant-ordered
+//      slots, 8-bit conservative quantisation, leaves of up
+//      to 3 consecutive triangles                             (k_collapse, one launch per level)
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <climits>
+
+#include "ff_internal.h"
+
+namespace {
+
+constexpr int kLeafMax = 3;
+
+struct BinNode {
+    int32_t left, right;   // >= 0: internal node index; < 0: ~leaf (sorted position)
+    uint32_t first, last;  // sorted primitive range
+    float3 lo, hi;
+};
+
+FF_D uint64_t expand21(uint32_t v)
+{
+    uint64_t x = v & 0x1fffffu;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+
+FF_D int ordered_key(float f)
+{
+    int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+FF_HD float from_ordered_key(int k)
+{
+#ifdef __CUDA_ARCH__
+    return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff);
+#else
+    int i = k >= 0 ? k : k ^ 0x7fffffff;
+    float f;
+    memcpy(&f, &i, 4);
+    return f;
+#endif
+}
+
+__global__ void k_prep(const float3* __restrict__ pos, const uint3* __restrict__ idx, uint32_t n,
+                       FFTri* __restrict__ rec, float3* __restrict__ blo, float3* __restrict__ bhi,
+                       float3* __restrict__ cen, int* __restrict__ cbounds, int* __restrict__ bad)
+{
+    // slots 0..5: centroid bounds (min xyz, max xyz); 6..11: triangle bounds
+    __shared__ int s_b[12];
+    if (threadIdx.x < 12) s_b[threadIdx.x] = ((threadIdx.x % 6) < 3) ? INT_MAX : INT_MIN;
+    __syncthreads();
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        uint3 t = idx[i];
+        float3 v0 = pos[t.x], v1 = pos[t.y], v2 = pos[t.z];
+        bool finite = isfinite(v0.x) && isfinite(v0.y) && isfinite(v0.z) && isfinite(v1.x) &&
+                      isfinite(v1.y) && isfinite(v1.z) && isfinite(v2.x) && isfinite(v2.y) &&
+                      isfinite(v2.z);
+        if (!finite) atomicExch(bad, 1);
+        FFTri r;
+        r.a = make_float4(v0.x, v0.y, v0.z, __int_as_float((int)i));
+        float3 e1 = rn_sub(v1, v0), e2 = rn_sub(v2, v0);
+        r.b = make_float4(e1.x, e1.y, e1.z, 0.f);
+        r.c = make_float4(e2.x, e2.y, e2.z, 0.f);
+        rec[i] = r;
+        float3 lo = fmin3(fmin3(v0, v1), v2), hi = fmax3(fmax3(v0, v1), v2);
+        blo[i] = lo;
+        bhi[i] = hi;
+        float3 c = make_float3(0.5f * lo.x + 0.5f * hi.x, 0.5f * lo.y + 0.5f * hi.y, 0.5f * lo.z + 0.5f * hi.z);
+        cen[i] = c;
+        atomicMin(&s_b[0], ordered_key(c.x));
+        atomicMin(&s_b[1], ordered_key(c.y));
+        atomicMin(&s_b[2], ordered_key(c.z));
+        atomicMax(&s_b[3], ordered_key(c.x));
+        atomicMax(&s_b[4], ordered_key(c.y));
+        atomicMax(&s_b[5], ordered_key(c.z));
+        atomicMin(&s_b[6], ordered_key(lo.x));
+        atomicMin(&s_b[7], ordered_key(lo.y));
+        atomicMin(&s_b[8], ordered_key(lo.z));
+        atomicMax(&s_b[9], ordered_key(hi.x));
+        atomicMax(&s_b[10], ordered_key(hi.y));
+        atomicMax(&s_b[11], ordered_key(hi.z));
+    }
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        if ((threadIdx.x % 6) < 3) atomicMin(&cbounds[threadIdx.x], s_b[threadIdx.x]);
+        else atomicMax(&cbounds[threadIdx.x], s_b[threadIdx.x]);
+    }
+}
+
+__global__ void k_morton(const float3* __restrict__ cen, uint32_t n, const int* __restrict__ cb,
+                         uint64_t* __restrict__ keys, uint32_t* __restrict__ vals)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 lo = make_float3(from_ordered_key(cb[0]), from_ordered_key(cb[1]), from_ordered_key(cb[2]));
+    float3 hi = make_float3(from_ordered_key(cb[3]), from_ordered_key(cb[4]), from_ordered_key(cb[5]));
+    float3 c = cen[i];
+    float3 ext = hi - lo;
+    const float scale = 2097151.0f;  // 2^21 - 1
+    float fx = ext.x > 0.f ? (c.x - lo.x) / ext.x : 0.f;
+    float fy = ext.y > 0.f ? (c.y - lo.y) / ext.y : 0.f;
+    float fz = ext.z > 0.f ? (c.z - lo.z) / ext.z : 0.f;
+    uint32_t qx = (uint32_t)fminf(fmaxf(fx * scale, 0.f), scale);
+    uint32_t qy = (uint32_t)fminf(fmaxf(fy * scale, 0.f), scale);
+    uint32_t qz = (uint32_t)fminf(fmaxf(fz * scale, 0.f), scale);
+    keys[i] = (expand21(qx) << 2) | (expand21(qy) << 1) | expand21(qz);
+    vals[i] = i;
+}
+
+// Common-prefix length of sorted keys i and j, with the position breaking ties
+// between equal keys (Karras 2012, "Maximizing parallelism in the
+// construction of BVHs, octrees, and k-d trees").
+FF_D int delta(const uint64_t* __restrict__ keys, int n, int i, int j)
+{
+    if (j < 0 || j >= n) return -1;
+    uint64_t a = keys[i], b = keys[j];
+    if (a == b) return 64 + __clz((uint32_t)(i ^ j));
+    return __clzll(a ^ b);
+}
+
+__global__ void k_radix_tree(const uint64_t* __restrict__ keys, int n, BinNode* __restrict__ nodes,
+                             int32_t* __restrict__ parent_int, int32_t* __restrict__ parent_leaf)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta(keys, n, i, j);
+    int s = 0;
+    for (int div = 2;; div <<= 1) {
+        int t = (l + div - 1) / div;
+        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t <= 1) break;
+    }
+    int gamma = i + s * d + min(d, 0);
+    int lo = min(i, j), hi = max(i, j);
+    BinNode nd;
+    nd.first = lo;
+    nd.last = hi;
+    if (lo == gamma) {
+        nd.left = ~gamma;
+        parent_leaf[gamma] = i;
+    } else {
+        nd.left = gamma;
+        parent_int[gamma] = i;
+    }
+    if (hi == gamma + 1) {
+        nd.right = ~(gamma + 1);
+        parent_leaf[gamma + 1] = i;
+    } else {
+        nd.right = gamma + 1;
+        parent_int[gamma + 1] = i;
+    }
+    nd.lo = make_float3(0, 0, 0);
+    nd.hi = make_float3(0, 0, 0);
+    nodes[i] = nd;
+    if (i == 0) parent_int[0] = -1;
+}
+
+__device__ __forceinline__ float3 ldcg3(const float3* p)
+{
+    const float* f = reinterpret_cast<const float*>(p);
+    return make_float3(__ldcg(f), __ldcg(f + 1), __ldcg(f + 2));
+}
+
+__global__ void k_bounds_up(int n, const uint32_t* __restrict__ order, const float3* __restrict__ blo,
+                            const float3* __restrict__ bhi, BinNode* nodes,
+                            const int32_t* __restrict__ parent_int, const int32_t* __restrict__ parent_leaf,
+                            uint32_t* __restrict__ arrivals)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int p = parent_leaf[k];
+    // a radix tree over n keys has depth < n; the bound only guards against
+    // a malformed tree looping forever
+    for (int guard = 0; p >= 0 && guard < n; ++guard) {
+        __threadfence();
+        if (atomicAdd(&arrivals[p], 1u) == 0) return;  // first child to arrive stops here
+        __threadfence();
+        BinNode* nd = &nodes[p];
+        int l = nd->left, r = nd->right;
+        float3 llo, lhi, rlo, rhi;
+        if (l < 0) {
+            uint32_t t = order[~l];
+            llo = blo[t];
+            lhi = bhi[t];
+        } else {
+            llo = ldcg3(&nodes[l].lo);
+            lhi = ldcg3(&nodes[l].hi);
+        }
+        if (r < 0) {
+            uint32_t t = order[~r];
+            rlo = blo[t];
+            rhi = bhi[t];
+        } else {
+            rlo = ldcg3(&nodes[r].lo);
+            rhi = ldcg3(&nodes[r].hi);
+        }
+        float3 lo = fmin3(llo, rlo), hi = fmax3(lhi, rhi);
+        __stcg(&nd->lo.x, lo.x);
+        __stcg(&nd->lo.y, lo.y);
+        __stcg(&nd->lo.z, lo.z);
+        __stcg(&nd->hi.x, hi.x);
+        __stcg(&nd->hi.y, hi.y);
+        __stcg(&nd->hi.z, hi.z);
+        p = parent_int[p];
+    }
+}
+
+struct CollapseItem {
+    int32_t ref;       // binary node ref (>= 0 internal, < 0 ~leaf)
+    uint32_t wide;     // index of the wide node to fill
+};
+
+struct ChildInfo {
+    int32_t ref;
+    uint32_t first, last;
+    float3 lo, hi;
+};
+
+// 2^k for k in [-126, 126], built from the exponent bits.
+FF_D float pow2i(int k) { return __int_as_float((k + 127) << 23); }
+
+FF_D float half_area(float3 lo, float3 hi)
+{
+    float3 d = hi - lo;
+    return d.x * d.y + d.y * d.z + d.z * d.x;
+}
+
+// Quantisation exponent for one axis: the smallest e with (hi - lo) / 2^e <= 253,
+// raised so that one grid step is at least 2^-20 of the coordinate magnitude.
+FF_D int quant_exp(float lo, float hi)
+{
+    float ext = __fsub_ru(hi, lo);
+    int e = -126;
+    if (ext > 0.f) {
+        int ex;
+        frexpf(ext / 253.0f, &ex);  // ext/253 = m * 2^ex, m in [0.5, 1)
+        e = ex;                     // 2^ex > ext/253
+    }
+    float mag = fmaxf(fabsf(lo), fabsf(hi));
+    if (mag > 0.f) {
+        int em;
+        frexpf(mag, &em);
+        e = max(e, em - 20);
+    }
+    e = max(e, -126);
+    e = min(e, 126);
+    // guard against rounding in the division above
+    while (e < 126 && __fmul_ru(ext, pow2i(-e)) > 253.0f) ++e;
+    return e;
+}
+
+__global__ void k_collapse(const CollapseItem* __restrict__ in, uint32_t n_in, CollapseItem* __restrict__ out,
+                           uint32_t* __restrict__ counters /* 0: out size, 1: node count, 2: tri count, 3: error */,
+                           uint32_t node_cap, uint32_t tri_cap,
+                           const BinNode* __restrict__ bin, const uint32_t* __restrict__ order,
+                           const float3* __restrict__ blo, const float3* __restrict__ bhi,
+                           const FFTri* __restrict__ rec, FFNode8* __restrict__ wnodes, FFTri* __restrict__ wtris)
+{
+    uint32_t it = blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= n_in) return;
+    CollapseItem item = in[it];
+
+    ChildInfo ch[8];
+    int nc = 0;
+    auto info = [&](int32_t ref) {
+        ChildInfo c;
+        c.ref = ref;
+        if (ref < 0) {
+            uint32_t k = ~ref;
+            uint32_t t = order[k];
+            c.first = c.last = k;
+            c.lo = blo[t];
+            c.hi = bhi[t];
+        } else {
+            const BinNode& b = bin[ref];
+            c.first = b.first;
+            c.last = b.last;
+            c.lo = b.lo;
+            c.hi = b.hi;
+        }
+        return c;
+    };
+    if (item.ref < 0) {
+        ch[nc++] = info(item.ref);
+    } else {
+        const BinNode& b = bin[item.ref];
+        ch[nc++] = info(b.left);
+        ch[nc++] = info(b.right);
+    }
+    // Open the largest internal child until 8 slots are used.
+    while (nc < 8) {
+        int best = -1;
+        float best_a = -1.f;
+        for (int c = 0; c < nc; ++c) {
+            if (ch[c].ref >= 0) {
+                float a = half_area(ch[c].lo, ch[c].hi);
+                if (a > best_a) {
+                    best_a = a;
+                    best = c;
+                }
+            }
+        }
+        if (best < 0) break;
+        const BinNode& b = bin[ch[best].ref];
+        ChildInfo r = info(b.right);
+        ch[best] = info(b.left);
+        ch[nc++] = r;
+    }
+
+    float3 nlo = ch[0].lo, nhi = ch[0].hi;
+    for (int c = 1; c < nc; ++c) {
+        nlo = fmin3(nlo, ch[c].lo);
+        nhi = fmax3(nhi, ch[c].hi);
+    }
+    float3 ncen = 0.5f * (nlo + nhi);
+
+    // Octant-ordered slot assignment: slot s gets the child whose centre lies
+    // furthest against the direction signs of octant s (bit a set = negative
+    // along axis a), so rays of octant s meet it first.
+    int slot_of[8];
+    int child_in[8];
+    for (int s = 0; s < 8; ++s) child_in[s] = -1;
+    for (int c = 0; c < nc; ++c) slot_of[c] = -1;
+    for (int k = 0; k < nc; ++k) {
+        float best = 3.4e38f;
+        int bc = -1, bs = -1;
+        for (int c = 0; c < nc; ++c) {
+            if (slot_of[c] >= 0) continue;
+            float3 dc = 0.5f * (ch[c].lo + ch[c].hi) - ncen;
+            for (int s = 0; s < 8; ++s) {
+                if (child_in[s] >= 0) continue;
+                float cost = ((s & 1) ? -dc.x : dc.x) + ((s & 2) ? -dc.y : dc.y) + ((s & 4) ? -dc.z : dc.z);
+                if (cost < best) {
+                    best = cost;
+                    bc = c;
+                    bs = s;
+                }
+            }
+        }
+        slot_of[bc] = bs;
+        child_in[bs] = bc;
+    }
+
+    // Classify children and allocate.
+    uint32_t n_internal = 0, n_tris = 0;
+    for (int c = 0; c < nc; ++c) {
+        uint32_t cnt = ch[c].last - ch[c].first + 1;
+        if (ch[c].ref >= 0 && cnt > kLeafMax) ++n_internal;
+        else n_tris += cnt;
+    }
+    uint32_t child_base = n_internal ? atomicAdd(&counters[1], n_internal) : 0;
+    uint32_t tri_base = n_tris ? atomicAdd(&counters[2], n_tris) : 0;
+    uint32_t out_base = n_internal ? atomicAdd(&counters[0], n_internal) : 0;
+    // Capacity guards: a correct build never trips them; if one does, the
+    // error flag is set and nothing is written out of bounds.
+    if (child_base + n_internal > node_cap || tri_base + n_tris > tri_cap || out_base + n_internal > node_cap ||
+        item.wide >= node_cap || n_tris > 24) {
+        atomicExch(&counters[3], 1u);
+        return;
+    }
+
+    FFNode8 node;
+    node.px = nlo.x;
+    node.py = nlo.y;
+    node.pz = nlo.z;
+    int ex = quant_exp(nlo.x, nhi.x), ey = quant_exp(nlo.y, nhi.y), ez = quant_exp(nlo.z, nhi.z);
+    node.ex = (uint8_t)(ex + 127);
+    node.ey = (uint8_t)(ey + 127);
+    node.ez = (uint8_t)(ez + 127);
+    float isx = pow2i(-ex), isy = pow2i(-ey), isz = pow2i(-ez);
+    node.child_base = child_base;
+    node.tri_base = tri_base;
+    uint8_t imask = 0;
+    uint32_t next_child = 0, next_tri = 0;
+    for (int s = 0; s < 8; ++s) {
+        int c = child_in[s];
+        if (c < 0) {
+            node.meta[s] = 0;
+            node.qlox[s] = node.qloy[s] = node.qloz[s] = 0;
+            node.qhix[s] = node.qhiy[s] = node.qhiz[s] = 0;
+            continue;
+        }
+        const ChildInfo& ci = ch[c];
+        auto qlo = [](float v, float p, float is) {
+            float q = floorf(__fsub_rd(v, p) * is) - 1.f;
+            return (uint8_t)fminf(fmaxf(q, 0.f), 255.f);
+        };
+        auto qhi = [](float v, float p, float is) {
+            float q = ceilf(__fsub_ru(v, p) * is) + 1.f;
+            return (uint8_t)fminf(fmaxf(q, 0.f), 255.f);
+        };
+        node.qlox[s] = qlo(ci.lo.x, nlo.x, isx);
+        node.qloy[s] = qlo(ci.lo.y, nlo.y, isy);
+        node.qloz[s] = qlo(ci.lo.z, nlo.z, isz);
+        node.qhix[s] = qhi(ci.hi.x, nlo.x, isx);
+        node.qhiy[s] = qhi(ci.hi.y, nlo.y, isy);
+        node.qhiz[s] = qhi(ci.hi.z, nlo.z, isz);
+        uint32_t cnt = ci.last - ci.first + 1;
+        if (ci.ref >= 0 && cnt > kLeafMax) {
+            imask |= (uint8_t)(1u << s);
+            node.meta[s] = (uint8_t)(0x20u | (24u + s));
+            uint32_t wi = child_base + next_child;
+            out[out_base + next_child] = CollapseItem{ci.ref, wi};
+            ++next_child;
+        } else {
+            uint32_t unary = (1u << cnt) - 1u;
+            node.meta[s] = (uint8_t)((unary << 5) | next_tri);
+            for (uint32_t k = ci.first; k <= ci.last; ++k) wtris[tri_base + next_tri++] = rec[order[k]];
+        }
+    }
+    node.imask = imask;
+    wnodes[item.wide] = node;
+}
+
+// Structural check of the finished BVH: every child index and triangle range
+// in bounds, every triangle referenced exactly once.  err[0] counts failures.
+__global__ void k_validate(const FFNode8* __restrict__ nodes, uint32_t num_nodes, const FFTri* __restrict__ tris,
+                           uint32_t num_tris, uint32_t* __restrict__ tri_refs, uint32_t* __restrict__ err)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= num_nodes) return;
+    const FFNode8 nd = nodes[i];
+    uint32_t n_int = __popc((uint32_t)nd.imask);
+    if (n_int && (nd.child_base == 0 || nd.child_base + n_int > num_nodes)) atomicAdd(err, 1u);
+    for (int s = 0; s < 8; ++s) {
+        uint32_t m = nd.meta[s];
+        bool internal = (nd.imask >> s) & 1u;
+        if (m == 0) {
+            if (internal) atomicAdd(err, 1u);
+            continue;
+        }
+        if (internal) continue;
+        uint32_t unary = m >> 5, off = m & 31u;
+        uint32_t cnt = __popc(unary);
+        if (unary != (1u << cnt) - 1u || off + cnt > 24u || nd.tri_base + off + cnt > num_tris) {
+            atomicAdd(err, 1u);
+            continue;
+        }
+        for (uint32_t k = 0; k < cnt; ++k) {
+            uint32_t orig = (uint32_t)__float_as_int(tris[nd.tri_base + off + k].a.w);
+            if (orig < num_tris) atomicAdd(&tri_refs[orig], 1u);
+            else atomicAdd(err, 1u);
+        }
+    }
+}
+
+__global__ void k_validate_refs(const uint32_t* __restrict__ tri_refs, uint32_t n, uint32_t* __restrict__ err)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && tri_refs[i] != 1u) atomicAdd(err, 1u);
+}
+
+__global__ void k_init_counters(uint32_t* c, int* cb)
+{
+    c[0] = 0;
+    c[1] = 1;  // root occupies node 0
+    c[2] = 0;
+    c[3] = 0;
+    for (int i = 0; i < 3; ++i) cb[i] = INT_MAX;
+    for (int i = 3; i < 6; ++i) cb[i] = INT_MIN;
+    for (int i = 6; i < 9; ++i) cb[i] = INT_MAX;
+    for (int i = 9; i < 12; ++i) cb[i] = INT_MIN;
+    cb[12] = 0;  // non-finite vertex flag
+}
+
+}  // namespace
+
+void ff_build_bvh(ff_context* ctx, ff_scene* s, const float3* d_pos, const uint3* d_idx, uint32_t n)
+{
+    cudaStream_t st = ctx->stream;
+    s->num_tris = n;
+    if (n == 0) {
+        s->num_nodes = 0;
+        s->depth = 0;
+        return;
+    }
+    cudaEvent_t e0, e1;
+    FF_CUDA_CHECK(cudaEventCreate(&e0));
+    FF_CUDA_CHECK(cudaEventCreate(&e1));
+    FF_CUDA_CHECK(cudaEventRecord(e0, st));
+
+    DevBuf rec, blo, bhi, cen, keys, keys2, vals, vals2, bin, pint, pleaf, arrivals, qa, qb, misc, temp;
+    rec.alloc(sizeof(FFTri) * n);
+    blo.alloc(sizeof(float3) * n);
+    bhi.alloc(sizeof(float3) * n);
+    cen.alloc(sizeof(float3) * n);
+    keys.alloc(sizeof(uint64_t) * n);
+    keys2.alloc(sizeof(uint64_t) * n);
+    vals.alloc(sizeof(uint32_t) * n);
+    vals2.alloc(sizeof(uint32_t) * n);
+    misc.alloc(64 * sizeof(uint32_t));
+    uint32_t* counters = misc.as<uint32_t>();
+    int* cb = reinterpret_cast<int*>(counters + 16);
+
+    const int B = 256;
+    const uint32_t G = (n + B - 1) / B;
+    k_init_counters<<<1, 1, 0, st>>>(counters, cb);
+    k_prep<<<G, B, 0, st>>>(d_pos, d_idx, n, rec.as<FFTri>(), blo.as<float3>(), bhi.as<float3>(),
+                            cen.as<float3>(), cb, cb + 12);
+    k_morton<<<G, B, 0, st>>>(cen.as<float3>(), n, cb, keys.as<uint64_t>(), vals.as<uint32_t>());
+    size_t temp_bytes = 0;
+    FF_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys.as<uint64_t>(), keys2.as<uint64_t>(),
+                                                  vals.as<uint32_t>(), vals2.as<uint32_t>(), (int)n, 0, 63, st));
+    temp.alloc(std::max<size_t>(temp_bytes, 16));
+    FF_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(temp.ptr, temp_bytes, keys.as<uint64_t>(), keys2.as<uint64_t>(),
+                                                  vals.as<uint32_t>(), vals2.as<uint32_t>(), (int)n, 0, 63, st));
+    const uint64_t* skeys = keys2.as<uint64_t>();
+    const uint32_t* order = vals2.as<uint32_t>();
+
+    uint32_t n_int = n > 1 ? n - 1 : 1;
+    bin.alloc(sizeof(BinNode) * n_int);
+    pint.alloc(sizeof(int32_t) * n_int);
+    pleaf.alloc(sizeof(int32_t) * n);
+    arrivals.alloc(sizeof(uint32_t) * n_int);
+    FF_CUDA_CHECK(cudaMemsetAsync(arrivals.ptr, 0, sizeof(uint32_t) * n_int, st));
+    if (n > 1) {
+        k_radix_tree<<<(n - 1 + B - 1) / B, B, 0, st>>>(skeys, (int)n, bin.as<BinNode>(), pint.as<int32_t>(),
+                                                       pleaf.as<int32_t>());
+        k_bounds_up<<<G, B, 0, st>>>((int)n, order, blo.as<float3>(), bhi.as<float3>(), bin.as<BinNode>(),
+                                     pint.as<int32_t>(), pleaf.as<int32_t>(), arrivals.as<uint32_t>());
+    }
+
+    // Wide nodes: at most one per binary internal node with more than
+    // kLeafMax primitives, plus the root.
+    uint32_t max_wide = n / 2 + 2;
+    s->nodes.alloc(sizeof(FFNode8) * max_wide);
+    s->tris.alloc(sizeof(FFTri) * n);
+    qa.alloc(sizeof(CollapseItem) * max_wide);
+    qb.alloc(sizeof(CollapseItem) * max_wide);
+
+    CollapseItem root{n > 1 ? 0 : ~0, 0u};
+    FF_CUDA_CHECK(cudaMemcpyAsync(qa.ptr, &root, sizeof(root), cudaMemcpyHostToDevice, st));
+    uint32_t n_in = 1;
+    uint32_t depth = 0;
+    CollapseItem* qin = qa.as<CollapseItem>();
+    CollapseItem* qout = qb.as<CollapseItem>();
+    uint32_t host_counters[4];
+    while (n_in > 0) {
+        FF_CUDA_CHECK(cudaMemsetAsync(counters, 0, sizeof(uint32_t), st));
+        k_collapse<<<(n_in + 127) / 128, 128, 0, st>>>(qin, n_in, qout, counters, max_wide, n, bin.as<BinNode>(), order,
+                                                      blo.as<float3>(), bhi.as<float3>(), rec.as<FFTri>(),
+                                                      s->nodes.as<FFNode8>(), s->tris.as<FFTri>());
+        FF_CUDA_CHECK(cudaMemcpyAsync(host_counters, counters, sizeof(host_counters), cudaMemcpyDeviceToHost, st));
+        FF_CUDA_CHECK(cudaStreamSynchronize(st));
+        ++depth;
+        n_in = host_counters[0];
+        std::swap(qin, qout);
+        if (host_counters[3]) throw FFError{FF_ERR_INTERNAL, "BVH collapse exceeded its capacity"};
+        if (depth > 200) throw FFError{FF_ERR_INTERNAL, "BVH collapse did not terminate"};
+    }
+    int hb[13];
+    FF_CUDA_CHECK(cudaMemcpyAsync(hb, cb, sizeof(hb), cudaMemcpyDeviceToHost, st));
+    FF_CUDA_CHECK(cudaEventRecord(e1, st));
+    FF_CUDA_CHECK(cudaStreamSynchronize(st));
+    FF_CUDA_CHECK(cudaGetLastError());
+    if (hb[12]) throw FFError{FF_ERR_INVALID_ARG, "scene has non-finite vertex positions"};
+    if (host_counters[2] != n) throw FFError{FF_ERR_INTERNAL, "BVH collapse lost triangles"};
+    s->num_nodes = host_counters[1];
+    {
+        DevBuf refs;
+        refs.alloc(sizeof(uint32_t) * (n + 1));
+        uint32_t* d_err = refs.as<uint32_t>() + n;
+        FF_CUDA_CHECK(cudaMemsetAsync(refs.ptr, 0, sizeof(uint32_t) * (n + 1), st));
+        k_validate<<<(s->num_nodes + 127) / 128, 128, 0, st>>>(s->nodes.as<FFNode8>(), s->num_nodes,
+                                                              s->tris.as<FFTri>(), n, refs.as<uint32_t>(), d_err);
+        k_validate_refs<<<G, B, 0, st>>>(refs.as<uint32_t>(), n, d_err);
+        uint32_t h_err = 0;
+        FF_CUDA_CHECK(cudaMemcpyAsync(&h_err, d_err, sizeof(h_err), cudaMemcpyDeviceToHost, st));
+        FF_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (h_err) throw FFError{FF_ERR_INTERNAL, "BVH validation failed"};
+    }
+    s->depth = depth;
+    s->lo = make_float3(from_ordered_key(hb[6]), from_ordered_key(hb[7]), from_ordered_key(hb[8]));
+    s->hi = make_float3(from_ordered_key(hb[9]), from_ordered_key(hb[10]), from_ordered_key(hb[11]));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    s->build_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}

@@ -1,0 +1,135 @@
+// ff_internal.h — host-side objects behind the opaque handles of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "ff_common.cuh"
+#include "firefly_b200.h"
+
+// Deepest 8-wide BVH the traversal stack can serve (checked at scene build).
+constexpr int kMaxStackDepth = 64;
+
+// Raised inside the implementation and turned into an ff_status at the ABI.
+struct FFError {
+    ff_status status;
+    std::string msg;
+};
+
+#define FF_CUDA_CHECK(expr)                                                              \
+    do {                                                                                 \
+        cudaError_t _e = (expr);                                                         \
+        if (_e != cudaSuccess) {                                                         \
+            throw FFError{_e == cudaErrorMemoryAllocation ? FF_ERR_OOM : FF_ERR_CUDA,    \
+                          std::string(#expr) + ": " + cudaGetErrorString(_e)};           \
+        }                                                                                \
+    } while (0)
+
+#define FF_REQUIRE(cond, msg)                                  \
+    do {                                                       \
+        if (!(cond)) throw FFError{FF_ERR_INVALID_ARG, (msg)}; \
+    } while (0)
+
+// Owning device allocation.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    void alloc(size_t n)
+    {
+        if (n <= bytes && ptr) return;
+        release();
+        if (n == 0) return;
+        FF_CUDA_CHECK(cudaMalloc(&ptr, n));
+        bytes = n;
+    }
+    template <class T>
+    T* as() const { return reinterpret_cast<T*>(ptr); }
+};
+
+struct ff_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int num_sms = 148;
+    std::string last_error;
+    DevBuf counters;      // small scratch of uint32 counters for persistent kernels
+    DevBuf io_rays, io_hits;  // staging for host-pointer ff_trace calls
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+// Per-original-triangle shading attributes (read once per hit).
+struct FFShadeTri {
+    float3 n0, n1, n2;   // vertex normals
+    float2 uv0, uv1, uv2;
+    float3 face_n;
+    uint32_t material;
+};
+
+struct FFEnvLight {
+    int width = 0, height = 0;
+    float3 color = {1.f, 1.f, 1.f};
+    DevBuf rgb;           // float3 texels (width*height)
+    DevBuf marginal;      // double[height]
+    DevBuf conditional;   // double[height*width]
+    DevBuf pdf;           // float[height*width]
+    DevBuf denom;         // double
+};
+
+struct ff_scene {
+    ff_context* ctx = nullptr;
+    uint32_t num_tris = 0;
+    uint32_t num_nodes = 0;
+    uint32_t depth = 0;
+    float build_ms = 0.f;
+    float3 lo{0, 0, 0}, hi{0, 0, 0};
+    DevBuf nodes;         // FFNode8[num_nodes]
+    DevBuf tris;          // FFTri[num_tris] in leaf order
+    DevBuf shade;         // FFShadeTri[num_tris] by original index
+    DevBuf materials;     // ff_material[num_materials]
+    uint32_t num_materials = 0;
+    std::vector<DevBuf*> textures;
+    DevBuf tex_table;     // device table of texture descriptors
+    DevBuf area_lights;   // ff_area_light[]
+    uint32_t num_area_lights = 0;
+    FFEnvLight env;
+    ff_camera camera{};
+    ~ff_scene()
+    {
+        for (auto* t : textures) delete t;
+    }
+    FFBvhView view() const
+    {
+        return FFBvhView{nodes.as<FFNode8>(), tris.as<FFTri>(), num_nodes, num_tris};
+    }
+    size_t device_bytes() const;
+};
+
+struct ff_film {
+    ff_context* ctx = nullptr;
+    uint32_t width = 0, height = 0;
+    DevBuf accum;         // float4 per pixel: radiance sum (xyz)
+    DevBuf comp;          // float4 per pixel: Kahan compensation
+    DevBuf count;         // uint32 per pixel
+};
+
+// ff_bvh.cu: device BVH build from host or device triangle data already on
+// the device (positions float3[V], indices uint3[T]).
+void ff_build_bvh(ff_context* ctx, ff_scene* s, const float3* d_pos, const uint3* d_idx,
+                  uint32_t num_tris);
+
+// ff_trace.cu
+void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n,
+                     ff_hit* d_hits, bool any_hit);

@@ -1,0 +1,105 @@
+// ff_scene.cu — per-triangle shading attributes, materials, lights and
+// textures uploaded at scene creation.
+//
+// Replaces the reference's mesh flattening into 200-byte dTriangle records
+// (d_process_mesh + dTriangle::init, CUDA-RayTracer/kernel.cu:162-182,
+// dTriangle.cu:22-32) and the managed-memory material / light tables
+// (dScene.cpp:172-298).  Traversal reads only the 48-byte FFTri records;
+// the attributes below are read once per hit, by original triangle index.
+#include "ff_internal.h"
+
+namespace {
+
+__global__ void k_build_shading(const float3* __restrict__ pos, const uint3* __restrict__ idx,
+                                const float3* __restrict__ nrm, const float2* __restrict__ uv,
+                                const uint32_t* __restrict__ mat, uint32_t n, FFShadeTri* __restrict__ out)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint3 t = idx[i];
+    float3 v0 = pos[t.x], v1 = pos[t.y], v2 = pos[t.z];
+    // dTriangle::init: face_normal = normalize(cross(v1 - v0, v2 - v0))
+    float3 c = rn_cross(rn_sub(v1, v0), rn_sub(v2, v0));
+    float l2 = rn_dot(c, c);
+    float inv = 1.0f / sqrtf(l2);
+    float3 fn = make_float3(c.x * inv, c.y * inv, c.z * inv);
+    FFShadeTri s;
+    s.face_n = fn;
+    if (nrm) {
+        s.n0 = nrm[t.x];
+        s.n1 = nrm[t.y];
+        s.n2 = nrm[t.z];
+    } else {
+        s.n0 = s.n1 = s.n2 = fn;
+    }
+    if (uv) {
+        s.uv0 = uv[t.x];
+        s.uv1 = uv[t.y];
+        s.uv2 = uv[t.z];
+    } else {
+        s.uv0 = s.uv1 = s.uv2 = make_float2(0.f, 0.f);
+    }
+    s.material = mat ? mat[i] : 0u;
+    out[i] = s;
+}
+
+}  // namespace
+
+void ff_build_env_tables(ff_context* ctx, ff_scene* s);
+
+void ff_build_shading(ff_context* ctx, ff_scene* s, const ff_scene_desc* d, const float3* d_pos, const uint3* d_idx)
+{
+    cudaStream_t st = ctx->stream;
+    const uint32_t n = d->num_triangles;
+    DevBuf nrm, uv, mat;
+    if (d->normals && d->num_vertices) {
+        nrm.alloc(sizeof(float3) * d->num_vertices);
+        FF_CUDA_CHECK(cudaMemcpyAsync(nrm.ptr, d->normals, sizeof(float3) * d->num_vertices, cudaMemcpyHostToDevice, st));
+    }
+    if (d->texcoords && d->num_vertices) {
+        uv.alloc(sizeof(float2) * d->num_vertices);
+        FF_CUDA_CHECK(cudaMemcpyAsync(uv.ptr, d->texcoords, sizeof(float2) * d->num_vertices, cudaMemcpyHostToDevice, st));
+    }
+    if (d->material_ids && n) {
+        mat.alloc(sizeof(uint32_t) * n);
+        FF_CUDA_CHECK(cudaMemcpyAsync(mat.ptr, d->material_ids, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st));
+    }
+    if (n) {
+        s->shade.alloc(sizeof(FFShadeTri) * n);
+        k_build_shading<<<(n + 255) / 256, 256, 0, st>>>(d_pos, d_idx, nrm.as<float3>(), uv.as<float2>(),
+                                                         mat.as<uint32_t>(), n, s->shade.as<FFShadeTri>());
+        FF_CUDA_CHECK(cudaGetLastError());
+    }
+    // Materials: a default grey FF_MAT_MIX when none are given.
+    std::vector<ff_material> mats(d->materials, d->materials + d->num_materials);
+    if (mats.empty()) {
+        ff_material m{};
+        m.base_color[0] = m.base_color[1] = m.base_color[2] = 0.5f;
+        m.fresnel[0] = m.fresnel[1] = m.fresnel[2] = 0.04f;
+        m.roughness = 1.f;
+        m.ior = 1.5f;
+        m.kind = FF_MAT_MIX;
+        m.base_color_tex = m.roughness_tex = -1;
+        mats.push_back(m);
+    }
+    s->num_materials = (uint32_t)mats.size();
+    s->materials.alloc(sizeof(ff_material) * mats.size());
+    FF_CUDA_CHECK(cudaMemcpyAsync(s->materials.ptr, mats.data(), sizeof(ff_material) * mats.size(),
+                                  cudaMemcpyHostToDevice, st));
+    s->num_area_lights = d->num_area_lights;
+    if (d->num_area_lights) {
+        s->area_lights.alloc(sizeof(ff_area_light) * d->num_area_lights);
+        FF_CUDA_CHECK(cudaMemcpyAsync(s->area_lights.ptr, d->area_lights, sizeof(ff_area_light) * d->num_area_lights,
+                                      cudaMemcpyHostToDevice, st));
+    }
+    s->env.color = make_float3(d->env_color[0], d->env_color[1], d->env_color[2]);
+    if (d->env_rgb) {
+        s->env.width = (int)d->env_width;
+        s->env.height = (int)d->env_height;
+        s->env.rgb.alloc(sizeof(float3) * d->env_width * d->env_height);
+        FF_CUDA_CHECK(cudaMemcpyAsync(s->env.rgb.ptr, d->env_rgb, sizeof(float3) * d->env_width * d->env_height,
+                                      cudaMemcpyHostToDevice, st));
+        ff_build_env_tables(ctx, s);
+    }
+    FF_CUDA_CHECK(cudaStreamSynchronize(st));
+}

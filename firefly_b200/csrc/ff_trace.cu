@@ -1,0 +1,118 @@
+// ff_trace.cu — persistent closest-hit / any-hit trace kernel behind ff_trace.
+//
+// Replaces wf_extend / wf_shadow (CUDA-RayTracer/kernel.cu:488-543), which
+// launch one thread per queued ray over a binary BVH with a 64-entry local
+// stack.  Here every warp is persistent: idle lanes take new rays from a
+// global counter with one warp-aggregated atomic, so lanes whose rays finish
+// early are refilled instead of idling until the slowest ray of the warp ends
+// (Aila & Laine 2009, "Understanding the efficiency of ray traversal on GPUs").
+#include "ff_internal.h"
+#include "ff_trace.cuh"
+
+static_assert(kMaxStack == kMaxStackDepth, "stack size must match the build-time depth check");
+
+namespace {
+
+constexpr int kTraceBlock = 128;
+// Refill when at least this many lanes of the warp are idle.
+constexpr int kRefillIdle = 8;
+
+template <bool ANY>
+__global__ void __launch_bounds__(kTraceBlock, 4)
+    k_trace(FFBvhView bvh, const ff_ray* __restrict__ rays, ff_hit* __restrict__ hits, uint64_t n,
+            unsigned long long* __restrict__ counter, unsigned int* __restrict__ err)
+{
+    // A ray visits every node at most once; more steps than nodes means a
+    // malformed BVH.  The ray is then ended and counted in err[0] instead of
+    // looping.
+    const uint32_t max_steps = bvh.num_nodes + 2u;
+    __shared__ uint2 s_stack[kShortStack * kTraceBlock];
+    FFStack st;
+    st.sm = s_stack + threadIdx.x;
+    st.stride = kTraceBlock;
+    st.sp = 0;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+
+    FFRayState r;
+    uint2 cur = make_uint2(0u, 0u);
+    uint64_t ray_id = 0;
+    uint32_t steps = 0;
+    bool active = false;
+    bool exhausted = false;
+
+    while (true) {
+        // Refill idle lanes with new rays.
+        const uint32_t want = __ballot_sync(0xffffffffu, !active && !exhausted);
+        if (want) {
+            const uint32_t leader = __ffs(want) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(want));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!active && !exhausted) {
+                ray_id = base + __popc(want & lt_mask);
+                if (ray_id < n) {
+                    const float4 r0 = __ldg(reinterpret_cast<const float4*>(rays + ray_id));
+                    const float4 r1 = __ldg(reinterpret_cast<const float4*>(rays + ray_id) + 1);
+                    ff_ray_setup(r, make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), r0.w, r1.w, ANY);
+                    cur = ff_root_group(r);
+                    st.reset();
+                    steps = 0;
+                    active = bvh.num_nodes > 0;
+                    if (!active) {
+                        hits[ray_id] = ff_hit{r.tmax, 0.f, 0.f, -1};
+                    }
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) {
+            if (__all_sync(0xffffffffu, exhausted)) break;
+            continue;
+        }
+        // Traverse until enough lanes are idle to make a refill worthwhile.
+        while (true) {
+            if (active) {
+                const bool done = ff_traverse_step<ANY>(bvh, r, cur, st);
+                if (st.overflow || ++steps > max_steps) atomicAdd(err, 1u);
+                if (done || steps > max_steps) {
+                    const int32_t prim = r.prim == 0xffffffffu ? -1 : (int32_t)r.prim;
+                    const float4 out = make_float4(r.tmax, r.u, r.v, __int_as_float(prim));
+                    *reinterpret_cast<float4*>(hits + ray_id) = out;
+                    active = false;
+                }
+            }
+            const uint32_t idle = __ballot_sync(0xffffffffu, !active && !exhausted);
+            const uint32_t busy = __ballot_sync(0xffffffffu, active);
+            if (busy == 0u || __popc(idle) >= kRefillIdle) break;
+        }
+    }
+}
+
+}  // namespace
+
+void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n, ff_hit* d_hits,
+                     bool any_hit)
+{
+    if (n == 0) return;
+    unsigned long long* counter = ctx->counters.as<unsigned long long>();
+    // counters: [0..7] ray counter, [8..11] traversal error count (sticky
+    // until read by ff_trace_errors / the host-pointer path)
+    unsigned int* err = reinterpret_cast<unsigned int*>(ctx->counters.as<char>() + 8);
+    FF_CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), ctx->stream));
+    int blocks_per_sm = 0;
+    if (any_hit)
+        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true>, kTraceBlock, 0));
+    else
+        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false>, kTraceBlock, 0));
+    blocks_per_sm = blocks_per_sm < 1 ? 1 : blocks_per_sm;
+    uint64_t grid = (uint64_t)ctx->num_sms * blocks_per_sm;
+    const uint64_t need = (n + kTraceBlock - 1) / kTraceBlock;
+    if (grid > need) grid = need;
+    if (any_hit)
+        k_trace<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err);
+    else
+        k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err);
+    FF_CUDA_CHECK(cudaGetLastError());
+}

@@ -1,0 +1,271 @@
+/*
+ * firefly_b200.h — C ABI of the B200 (sm_100a) wavefront path tracer.
+ *
+ * The reference (JakeKurtz/Firefly, directory CUDA-RayTracer/) reaches its
+ * device code through C++ free functions defined in kernel.cu and called from
+ * the dScene and PathTracer classes.  This header is the replacement seam: plain
+ * C types, plain pointers and sizes, status codes instead of exit()/abort().
+ * Each entry point names the reference interface it replaces.
+ *
+ * Threading: a context is bound to one CUDA device and one stream.  Calls on
+ * one context must be externally serialised; separate contexts (one per GPU)
+ * may be used from separate threads.
+ *
+ * Memory: every handle owns the device memory it allocates and frees it in
+ * its *_destroy call.  Input arrays are copied during the create call.  Output
+ * buffers are caller-provided; FF_MEM_DEVICE in a flags word says the pointer
+ * is device memory of the context's device, otherwise it is host memory.
+ */
+#ifndef FIREFLY_B200_H
+#define FIREFLY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FF_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define FF_API __attribute__((visibility("default")))
+#else
+#define FF_API
+#endif
+
+/* Status codes.  The reference terminates the process on any CUDA error
+ * (CudaHelpers.cpp:3-11 checkCudaErrors -> exit(99); massert.cpp:3-12 ->
+ * abort()); every call here returns one of these instead. */
+typedef enum ff_status {
+    FF_OK = 0,
+    FF_ERR_INVALID_ARG = 1,
+    FF_ERR_OOM = 2,
+    FF_ERR_CUDA = 3,
+    FF_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+    FF_ERR_UNSUPPORTED = 5,
+    FF_ERR_INTERNAL = 6
+} ff_status;
+
+typedef struct ff_context ff_context;
+typedef struct ff_scene ff_scene;
+typedef struct ff_film ff_film;
+
+/* Pointer-location flags for buffers passed across the ABI. */
+#define FF_MEM_HOST   0u
+#define FF_MEM_DEVICE 1u
+
+/* ---------------------------------------------------------------- context */
+
+typedef struct ff_device_opts {
+    int32_t device;       /* CUDA ordinal */
+    void* stream;         /* cudaStream_t to run on; NULL = a stream owned by the context */
+    uint32_t flags;       /* reserved, 0 */
+} ff_device_opts;
+
+/* Replaces PathTracer::init_interop's stream/event creation
+ * (PathTracer.cpp:81-96) without the GL interop. */
+FF_API ff_status ff_context_create(const ff_device_opts* opts, ff_context** out);
+FF_API ff_status ff_context_destroy(ff_context* ctx);
+/* Message of the last failed call on this context (never NULL). */
+FF_API const char* ff_last_error_message(const ff_context* ctx);
+/* Synchronise the context's stream. */
+FF_API ff_status ff_context_sync(ff_context* ctx);
+/* The stream the context launches on (a cudaStream_t). */
+FF_API void* ff_context_stream(const ff_context* ctx);
+
+/* ------------------------------------------------------------------ scene */
+
+/* Material kinds.  FF_MAT_MIX is the reference's only wired material: the
+ * 50/50 diffuse + GGX mixture of BRDF_L/BRDF_f/BRDF_pdf (dMaterial.cu:363-469).
+ * FF_MAT_DIFFUSE and FF_MAT_CONDUCTOR are its single-lobe stages
+ * (wf_mat_diffuse / wf_mat_cook, kernel.cu:546-614).  FF_MAT_DIELECTRIC and
+ * FF_MAT_COAT have no counterpart in the reference (it defines refract() at
+ * dMaterial.cu:97-113 but never uses it). */
+typedef enum ff_material_kind {
+    FF_MAT_MIX = 0,
+    FF_MAT_DIFFUSE = 1,
+    FF_MAT_CONDUCTOR = 2,
+    FF_MAT_DIELECTRIC = 3,
+    FF_MAT_COAT = 4
+} ff_material_kind;
+
+/* Flattened dMaterial (dMaterial.cuh:9-31): glTF metallic-roughness factors.
+ * Textures are referenced by index into ff_scene_desc.textures, -1 = none. */
+typedef struct ff_material {
+    float base_color[3];      /* baseColorFactor */
+    float emissive[3];        /* emissiveColorFactor */
+    float fresnel[3];         /* f0 of the dielectric part, default 0.04 */
+    float roughness;          /* roughnessFactor */
+    float metallic;           /* metallicFactor */
+    float radiance;           /* emission scale, emissive_L = radiance * emissive */
+    float ior;                /* FF_MAT_DIELECTRIC / FF_MAT_COAT only */
+    int32_t kind;             /* ff_material_kind */
+    int32_t base_color_tex;   /* -1 = none */
+    int32_t roughness_tex;    /* -1 = none */
+    int32_t pad;
+} ff_material;
+
+/* RGB float texture, row-major, texel (x, y) at data[3*(y*width + x)]. */
+typedef struct ff_texture_desc {
+    const float* rgb;
+    uint32_t width, height;
+} ff_texture_desc;
+
+/* Rectangular area light, the reference's _Rectangle (Rectangle.cuh:24-123)
+ * wrapped by dAreaLight (dAreaLight.cu:18-68): p0 + s*a + t*b, s,t in [0,1]. */
+typedef struct ff_area_light {
+    float p0[3], a[3], b[3], normal[3];
+    float emissive[3];        /* emissiveColorFactor of the light's material */
+    float radiance;           /* radiance of the light's material */
+} ff_area_light;
+
+/* dCamera (dCamera.cuh:9-22) with the inverse view-projection given directly
+ * (the reference computes glm::inverse(P*V) on the host, dScene.cpp:381-391).
+ * inv_view_proj is the reference's Matrix4x4 m[4][4] flattened row-major,
+ * used as m * float4 (dMatrix.cuh:61-69). */
+typedef struct ff_camera {
+    float inv_view_proj[16];
+    float lens_radius;        /* thin lens, 0 = pinhole */
+    float focal_distance;     /* dCamera::f */
+    float exposure;           /* dCamera::exposure_time */
+    float pixel_jitter;       /* origin jitter scale, reference 0.005 (dCamera.cu:22) */
+} ff_camera;
+
+typedef struct ff_scene_desc {
+    const float* positions;       /* float3 per vertex */
+    uint32_t num_vertices;
+    const uint32_t* indices;      /* uint3 per triangle */
+    uint32_t num_triangles;
+    const float* normals;         /* float3 per vertex, NULL = face normals */
+    const float* texcoords;       /* float2 per vertex, NULL = zeros */
+    const uint32_t* material_ids; /* per triangle, NULL = all 0 */
+    const ff_material* materials;
+    uint32_t num_materials;
+    const ff_texture_desc* textures;
+    uint32_t num_textures;
+    /* Environment light (dEnvironmentLight): an equirectangular RGB32F map
+     * (env_rgb != NULL) or a constant colour. */
+    const float* env_rgb;
+    uint32_t env_width, env_height;
+    float env_color[3];
+    const ff_area_light* area_lights;
+    uint32_t num_area_lights;
+    ff_camera camera;
+    uint32_t flags;               /* reserved, 0 */
+} ff_scene_desc;
+
+typedef struct ff_scene_stats {
+    uint32_t num_triangles;
+    uint32_t num_nodes;           /* 8-wide BVH nodes */
+    uint32_t num_leaf_refs;       /* triangle references stored in leaves */
+    uint32_t bvh_depth;
+    uint64_t device_bytes;        /* device memory held by the scene */
+    float build_ms;               /* device BVH build time */
+    float scene_lo[3], scene_hi[3];
+} ff_scene_stats;
+
+/* Replaces dScene::dScene(Scene*) and dScene::load_scene (dScene.cpp:19-23,
+ * 60-80): materials, mesh flattening (process_mesh, kernel.cu:714-723),
+ * camera, lights (add_environment_light kernel.cu:742-771, add_area_lights
+ * kernel.cu:733-739) and the BVH (BVHAccel, dScene.cpp:364-379, plus
+ * reorder_primitives kernel.cu:701-712).  The BVH is built on the device. */
+FF_API ff_status ff_scene_create(ff_context* ctx, const ff_scene_desc* desc, ff_scene** out);
+FF_API ff_status ff_scene_destroy(ff_scene* scene);
+/* Replaces dScene::update / update_camera (dScene.cpp:55-58, 381-391). */
+FF_API ff_status ff_scene_update_camera(ff_scene* scene, const ff_camera* camera);
+FF_API ff_status ff_scene_get_stats(const ff_scene* scene, ff_scene_stats* out);
+
+/* -------------------------------------------------------------- ray query */
+
+/* A ray as the trace entry point consumes it (32 bytes).  The reference's
+ * dRay (dRay.cuh:5-11) has no interval; tmin = 0, tmax = +inf reproduce it. */
+typedef struct ff_ray {
+    float ox, oy, oz, tmin;
+    float dx, dy, dz, tmax;
+} ff_ray;
+
+/* Closest-hit result (16 bytes).  prim is the caller's ORIGINAL triangle
+ * index (the reference reports the post-reorder index, dTriangle.cu:172;
+ * orderedPrims maps it back, BVH.cpp:95-96), -1 on a miss.  u weights the
+ * second vertex and v the third, as in dTriangle::hit (dTriangle.cu:94-97). */
+typedef struct ff_hit {
+    float t, u, v;
+    int32_t prim;
+} ff_hit;
+
+#define FF_TRACE_CLOSEST 0u   /* intersect(), dTriangle.cu:140-213 */
+#define FF_TRACE_ANY     2u   /* intersect_shadows(), dTriangle.cu:215-259 */
+/* Location of rays/hits: FF_MEM_DEVICE (bit 0) or host. */
+
+/* Replaces wf_extend / wf_shadow (kernel.cu:488-543): trace n rays against
+ * the scene.  Closest-hit follows dTriangle::intersect (culling Moller-Trumbore,
+ * FP64 reciprocal of det) and returns the hit with the smallest t, ties to the
+ * lowest original triangle index, counting hits with tmin <= t < min(tmax,1e32).
+ * Any-hit follows dTriangle::shadow_hit (two-sided) and sets prim to the index
+ * of some occluder with tmin <= t < tmax, or -1.  flags = FF_TRACE_* |
+ * FF_MEM_DEVICE when rays and hits are device pointers.  With host pointers
+ * the call copies in and out and returns after the hits are on the host. */
+FF_API ff_status ff_trace(ff_context* ctx, const ff_scene* scene, const ff_ray* rays,
+                   uint64_t n, ff_hit* hits, uint32_t flags);
+
+/* ------------------------------------------------------------------- film */
+
+/* Headless film replacing the GL surface of Interop (Interop.cpp:78-86) and
+ * the accumulatebuffer / n_samples pair (PathTracer.cpp:22-23). */
+FF_API ff_status ff_film_create(ff_context* ctx, uint32_t width, uint32_t height, ff_film** out);
+FF_API ff_status ff_film_destroy(ff_film* film);
+/* Replaces PathTracer::clear_buffer (PathTracer.cpp:150-170). */
+FF_API ff_status ff_film_clear(ff_film* film);
+/* Accumulated radiance (RGBA float, A = 0) and per-pixel sample counts.
+ * Either pointer may be NULL.  flags: FF_MEM_DEVICE or host. */
+FF_API ff_status ff_film_read(ff_film* film, float* rgba, uint32_t* n_samples, uint32_t flags);
+/* Display image the way wf_logic writes its surface (kernel.cu:447-454):
+ * accum/n * exposure, x/(1+x), then 8-bit.  rgba8 is width*height*4 bytes. */
+FF_API ff_status ff_film_tonemap(ff_film* film, float exposure, uint8_t* rgba8, uint32_t flags);
+
+/* ----------------------------------------------------------------- render */
+
+#define FF_MODE_PARITY    0u  /* reproduce the reference's behaviours, see DESIGN */
+#define FF_MODE_CORRECTED 1u  /* unbiased RR, offset extension rays, fixed MIS gating */
+
+typedef struct ff_render_settings {
+    uint32_t spp;               /* samples per pixel added by this call */
+    uint32_t max_depth;         /* MAX_PATH_LENGTH, reference 3 (PathTracer.h:21) */
+    uint32_t rr_depth;          /* RR when path length > rr_depth, reference 3 (kernel.cu:372) */
+    uint32_t seed;
+    uint32_t mode;              /* FF_MODE_* */
+    int32_t light;              /* -1 = environment, k >= 0 = area light k; reference wires 1 = env (kernel.cu:397) */
+    uint32_t max_paths;         /* path pool size, 0 = automatic */
+    uint32_t sample_offset;     /* index of the first sample (progressive rendering) */
+    uint32_t flags;             /* FF_RENDER_* */
+    float shadow_offset;        /* SHADOW_OFFSET, reference 0.001 (kernel.cu:20) */
+} ff_render_settings;
+
+typedef struct ff_render_stats {
+    uint64_t extension_rays;    /* closest-hit queries traced */
+    uint64_t shadow_rays;       /* any-hit queries traced */
+    uint64_t samples;           /* completed paths */
+    uint32_t frames;            /* wavefront iterations */
+    float ms_total;
+    float ms_trace_extension, ms_trace_shadow, ms_logic, ms_shade;
+} ff_render_stats;
+
+/* Replaces PathTracer::draw + wavefront_pathtrace (PathTracer.cpp:59-79,
+ * kernel.cu:658-676): run the wavefront until every pixel of the film has
+ * received settings->spp more samples.  stats may be NULL. */
+FF_API ff_status ff_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* settings,
+                    ff_film* film, ff_render_stats* stats);
+
+/* Environment-map importance tables (kernel.cu:65-149): the marginal CDF
+ * (height doubles), the conditional CDFs (height*width doubles, row-major) and
+ * the pdf texture (height*width floats, already scaled by w*h/(2*pi^2)), as
+ * the device scans produced them.  Any pointer may be NULL.  Host memory. */
+FF_API ff_status ff_scene_read_env_tables(const ff_scene* scene, double* marginal, double* conditional,
+                                   float* pdf, double* pdf_denom);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FIREFLY_B200_H */

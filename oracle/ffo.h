@@ -1,0 +1,58 @@
+/*
+ * ffo.h — the CPU oracle: a plain-C restatement of the reference's hot-path
+ * arithmetic (JakeKurtz/Firefly, CUDA-RayTracer/).  TEST INFRASTRUCTURE ONLY.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+ * load this code, and only as the checker or the timed CPU baseline.  The
+ * product (firefly_b200/) never calls it.
+ *
+ * Parity pins: tests/golden/ holds vectors produced by the reference's own
+ * routines compiled for the host (oracle/_ref, recipe in oracle/Makefile);
+ * tests/test_oracle_golden.py checks every function here against them.
+ *
+ * Build with -ffp-contract=off: every float expression is evaluated in the
+ * reference's operand order with one rounding per operation, as the
+ * reference's host build does (x86-64 SSE, no FMA).
+ */
+#ifndef FFO_H
+#define FFO_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- ray/triangle (dTriangle.cu:34-138) ---- */
+/* dTriangle::intersect with TEST_CULL (dTriangle.cu:34-61): returns 1 on a
+ * front-face hit and writes t, u, v; leaves them untouched on early exits. */
+int ffo_intersect_cull(const float* v0, const float* v1, const float* v2,
+                       const float* o, const float* d, float* t, float* u, float* v);
+/* dTriangle::shadow_hit (dTriangle.cu:110-138): two-sided, u/v in double. */
+int ffo_shadow_hit(const float* v0, const float* v1, const float* v2,
+                   const float* o, const float* d, float* t);
+
+/* Brute-force ray queries over a triangle soup (tris: n_tris x 9 floats,
+ * v0 v1 v2).  rays: n x 8 floats (o, tmin, d, tmax) as ff_ray.  hits: n x 4
+ * words (t, u, v as float bits, prim as int32).  any != 0 selects the any-hit
+ * query.  Work is split over nthreads POSIX threads. */
+void ffo_trace_brute(const float* tris, int64_t n_tris, const float* rays, int64_t n,
+                     void* hits, int any, int nthreads);
+
+/* ---- sampler (dRandom.cu:10-27) ---- */
+uint32_t ffo_wang_hash(uint32_t s);
+/* The seeded replacement of the reference's clock-seeded random():
+ * wang_hash(key ^ wang_hash(dim)) * 2^-32 rounded to float (may be 1.0f,
+ * as the reference's conversion may). */
+float ffo_rand(uint32_t key, uint32_t dim);
+/* Per-(pixel, sample) stream key. */
+uint32_t ffo_path_key(uint32_t seed, uint32_t pixel, uint32_t sample);
+
+/* ---- CPU render (restated wavefront stages) ---- */
+typedef struct ffo_scene ffo_scene;
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,49 @@
+"""The C-ABI library loads and exports every symbol include/*.h declares (CPU only)."""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols() -> set[str]:
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        txt = h.read_text()
+        names |= set(re.findall(r"^FF_API\s+[\w\s\*]+?\b(ff_\w+)\s*\(", txt, flags=re.M))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    for must in ["ff_context_create", "ff_scene_create", "ff_trace", "ff_render", "ff_film_read"]:
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(ff_lib):
+    from firefly_b200 import _abi
+    names = declared_symbols()
+    missing = [n for n in sorted(names) if not hasattr(ff_lib, n)]
+    assert not missing, f"not exported: {missing}"
+    # the ctypes table covers the same set
+    assert names == set(_abi.SIGNATURES), names ^ set(_abi.SIGNATURES)
+
+
+def test_context_create_without_device_reports_status(ff_lib):
+    from tests.conftest import has_gpu
+    if has_gpu():
+        return
+    h = ctypes.c_void_p()
+    st = ff_lib.ff_context_create(None, ctypes.byref(h))
+    assert st != 0 and not h.value
+    assert isinstance(ff_lib.ff_last_error_message(None), bytes)
+
+
+def test_null_arguments_are_rejected(ff_lib):
+    assert ff_lib.ff_context_create(None, None) == 1
+    assert ff_lib.ff_context_destroy(None) == 1
+    assert ff_lib.ff_scene_destroy(None) == 1
+    assert ff_lib.ff_film_destroy(None) == 1
+    assert ff_lib.ff_trace(None, None, None, 0, None, 0) == 1
