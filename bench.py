@@ -204,8 +204,11 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     import firefly_b200 as ff
 
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated stream shared by the library and the timing events
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     ctx = ff.Context(local, stream=stream.cuda_stream)
+    assert ctx.stream == stream.cuda_stream
     scn, batches = build_workload(args.rays, seed_offset=17 * rank)
     ds = ff.dScene(ctx, scn)
     n = batches[0][1].shape[0]

@@ -18,6 +18,7 @@ Errors are raised as :class:`FireflyError` carrying the ABI status code.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -62,6 +63,7 @@ class Context:
         _check(lib().ff_context_create(C.byref(opts), C.byref(h)))
         self.handle = h
         self.device = device
+        self._children = weakref.WeakSet()   # scenes and tracers, closed before the context
 
     @property
     def stream(self) -> int:
@@ -71,7 +73,9 @@ class Context:
         _check(lib().ff_context_sync(self.handle), self.handle)
 
     def close(self):
-        if self.handle:
+        if getattr(self, "handle", None):
+            for child in list(self._children):
+                child.close()
             lib().ff_context_destroy(self.handle)
             self.handle = None
 
@@ -123,6 +127,7 @@ class dScene:
         _check(lib().ff_scene_create(ctx.handle, C.byref(d), C.byref(h)), ctx.handle)
         self.handle = h
         self.source = scene
+        ctx._children.add(self)
 
     def update(self, camera: A.ff_camera):
         """dScene::update: replace the camera."""
@@ -158,7 +163,8 @@ class dScene:
 
     def close(self):
         if getattr(self, "handle", None):
-            lib().ff_scene_destroy(self.handle)
+            if getattr(self.ctx, "handle", None):
+                lib().ff_scene_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
@@ -178,6 +184,7 @@ class PathTracer:
         _check(lib().ff_film_create(ctx.handle, w, h, C.byref(f)), ctx.handle)
         self.film = f
         self.last_stats = None
+        ctx._children.add(self)
 
     def draw(self, scene: dScene, spp: int = 1, max_depth: int = 3, rr_depth: int = 3, seed: int = 0,
              mode: int = A.FF_MODE_PARITY, light: int = -1, max_paths: int = 0, sample_offset: int = 0,
@@ -212,7 +219,8 @@ class PathTracer:
 
     def close(self):
         if getattr(self, "film", None):
-            lib().ff_film_destroy(self.film)
+            if getattr(self.ctx, "handle", None):
+                lib().ff_film_destroy(self.film)
             self.film = None
 
     def __del__(self):
