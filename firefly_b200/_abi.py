@@ -20,6 +20,7 @@ FF_ERR_INTERNAL = 6
 STATUS_NAMES = {0: "FF_OK", 1: "FF_ERR_INVALID_ARG", 2: "FF_ERR_OOM", 3: "FF_ERR_CUDA",
                 4: "FF_ERR_TIMEOUT", 5: "FF_ERR_UNSUPPORTED", 6: "FF_ERR_INTERNAL"}
 
+FF_NOALLOC_MAX_RAYS = 65536
 FF_MEM_HOST = 0
 FF_MEM_DEVICE = 1
 FF_TRACE_CLOSEST = 0
@@ -103,6 +104,7 @@ SIGNATURES = {
     "ff_scene_update_camera": (C.c_int, [P, C.POINTER(ff_camera)]),
     "ff_scene_get_stats": (C.c_int, [P, C.POINTER(ff_scene_stats)]),
     "ff_trace": (C.c_int, [P, P, P, C.c_uint64, P, C.c_uint32]),
+    "ff_trace_host_noalloc": (C.c_int, [P, P, P, C.c_uint64, P, C.c_uint32]),
     "ff_film_create": (C.c_int, [P, C.c_uint32, C.c_uint32, PP]),
     "ff_film_destroy": (C.c_int, [P]),
     "ff_film_clear": (C.c_int, [P]),

@@ -133,3 +133,8 @@ void ff_build_bvh(ff_context* ctx, ff_scene* s, const float3* d_pos, const uint3
 // ff_trace.cu
 void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n,
                      ff_hit* d_hits, bool any_hit);
+
+// ff_trace.cu: the trace launch with caller-supplied counters (used by the
+// no-allocation entry point).
+void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n,
+                             ff_hit* d_hits, bool any_hit, unsigned long long* counter, unsigned int* err);

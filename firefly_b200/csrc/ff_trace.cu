@@ -116,3 +116,25 @@ void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, u
         k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err);
     FF_CUDA_CHECK(cudaGetLastError());
 }
+
+// Same launch as ff_launch_trace, with the work counter and the error counter
+// supplied by the caller instead of taken from the context's allocation.
+void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n, ff_hit* d_hits,
+                             bool any_hit, unsigned long long* counter, unsigned int* err)
+{
+    if (n == 0) return;
+    int blocks_per_sm = 0;
+    if (any_hit)
+        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true>, kTraceBlock, 0));
+    else
+        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false>, kTraceBlock, 0));
+    blocks_per_sm = blocks_per_sm < 1 ? 1 : blocks_per_sm;
+    uint64_t grid = (uint64_t)ctx->num_sms * blocks_per_sm;
+    const uint64_t need = (n + kTraceBlock - 1) / kTraceBlock;
+    if (grid > need) grid = need;
+    if (any_hit)
+        k_trace<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err);
+    else
+        k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err);
+    FF_CUDA_CHECK(cudaGetLastError());
+}

@@ -209,6 +209,24 @@ typedef struct ff_hit {
 FF_API ff_status ff_trace(ff_context* ctx, const ff_scene* scene, const ff_ray* rays,
                    uint64_t n, ff_hit* hits, uint32_t flags);
 
+/* Host-pointer ray query that allocates no device memory.  No counterpart in
+ * the reference.  For callers that cannot allocate device memory: an
+ * application whose device memory is owned by its own pool allocator under a
+ * fixed budget, or an interactive loop that cannot take the implicit device
+ * synchronisation of cudaMalloc / cudaFree (ff_trace's host path grows its
+ * staging buffers with cudaMalloc).  Same query and results as ff_trace with
+ * host pointers (flags: FF_TRACE_CLOSEST or FF_TRACE_ANY, FF_MEM_DEVICE is
+ * rejected), for at most FF_NOALLOC_MAX_RAYS rays per call; larger n returns
+ * FF_ERR_INVALID_ARG.  Its scratch is one fixed array of about 3 MiB in the
+ * library's device image, held by every GPU that loads the library until the
+ * process exits.  The first call on a device looks up that array's device
+ * address; make that first call before any stream capture.  All calls on a
+ * device share the array: calls whose GPU work overlaps race and must be
+ * serialised by the caller. */
+#define FF_NOALLOC_MAX_RAYS 65536u
+FF_API ff_status ff_trace_host_noalloc(ff_context* ctx, const ff_scene* scene, const ff_ray* rays,
+                                       uint64_t n, ff_hit* hits, uint32_t flags);
+
 /* ------------------------------------------------------------------- film */
 
 /* Headless film replacing the GL surface of Interop (Interop.cpp:78-86) and

@@ -1,0 +1,67 @@
+"""ff_trace_host_noalloc: the host-pointer ray query that allocates no device
+memory, for callers that cannot allocate (an application whose device memory
+is owned by its own pool allocator, or a loop that cannot take the implicit
+synchronisation of cudaMalloc / cudaFree).
+
+The entry point is called through the C ABI and its hits must equal those of
+ff_trace (the existing entry point) bit for bit, the tolerance of every trace
+test here, on two calls in a row: the scratch array it stages through keeps
+the previous call's contents, so the second call checks that nothing stale
+leaks into it.  The file is named to be collected last.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(lib, ctx, ds, rays, any_hit):
+    import firefly_b200 as ff
+    from firefly_b200 import _abi as A
+    r = np.ascontiguousarray(rays, np.float32)
+    out = np.empty(len(r), ff.HIT_DTYPE)
+    flags = A.FF_TRACE_ANY if any_hit else A.FF_TRACE_CLOSEST
+    st = lib.ff_trace_host_noalloc(ctx.handle, ds.handle, r.ctypes.data_as(C.c_void_p), len(r),
+                                   out.ctypes.data_as(C.c_void_p), flags)
+    return st, out
+
+
+def test_noalloc_matches_ff_trace_on_two_calls():
+    import firefly_b200 as ff
+    from firefly_b200 import _abi as A
+    from firefly_b200 import scenes
+
+    lib = ff.lib()
+    ctx = ff.Context(0)
+    try:
+        scn = scenes.small_room(seed=0)
+        ds = ff.dScene(ctx, scn)
+        # call 1: the maximum size, closest-hit
+        rays1 = scenes.incoherent_rays(scn, A.FF_NOALLOC_MAX_RAYS, seed=101)
+        st, got1 = _noalloc(lib, ctx, ds, rays1, any_hit=False)
+        assert st == A.FF_OK, lib.ff_last_error_message(ctx.handle)
+        ref1 = ds.trace(rays1)
+        assert np.array_equal(got1.view(np.uint32), ref1.view(np.uint32))
+        # call 2: fewer rays, any-hit, into the same scratch
+        rays2 = scenes.with_random_tmax(scenes.incoherent_rays(scn, 40_000, seed=102), scn, seed=103)
+        st, got2 = _noalloc(lib, ctx, ds, rays2, any_hit=True)
+        assert st == A.FF_OK, lib.ff_last_error_message(ctx.handle)
+        ref2 = ds.trace(rays2, any_hit=True)
+        assert np.array_equal(got2.view(np.uint32), ref2.view(np.uint32))
+        assert 0 < (got2["prim"] >= 0).sum() < len(rays2)
+        # beyond the maximum: rejected with a message naming the limit
+        big = np.zeros((A.FF_NOALLOC_MAX_RAYS + 1, 8), np.float32)
+        st, _ = _noalloc(lib, ctx, ds, big, any_hit=False)
+        assert st == A.FF_ERR_INVALID_ARG
+        assert b"FF_NOALLOC_MAX_RAYS" in lib.ff_last_error_message(ctx.handle)
+        # device pointers are rejected (this entry point stages host memory)
+        st = lib.ff_trace_host_noalloc(ctx.handle, ds.handle, rays1.ctypes.data_as(C.c_void_p), 1,
+                                       got1.ctypes.data_as(C.c_void_p), A.FF_MEM_DEVICE)
+        assert st == A.FF_ERR_INVALID_ARG
+        ds.close()
+    finally:
+        ctx.close()
