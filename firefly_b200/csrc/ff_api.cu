@@ -261,3 +261,18 @@ ff_status ff_trace(ff_context* ctx, const ff_scene* s, const ff_ray* rays, uint6
 }
 
 }  // extern "C"
+
+extern "C" ff_status ff_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* settings, ff_film* film,
+                               ff_render_stats* stats)
+{
+    if (!ctx || !scene || !settings || !film) return FF_ERR_INVALID_ARG;
+    if (scene->ctx != ctx || film->ctx != ctx) {
+        ctx->last_error = "scene or film belongs to another context";
+        return FF_ERR_INVALID_ARG;
+    }
+    return guarded(ctx, [&] {
+        DeviceGuard g(ctx->device);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        ff_wavefront_render(ctx, scene, settings, film, stats);
+    });
+}

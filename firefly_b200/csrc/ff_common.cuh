@@ -29,6 +29,7 @@ FF_HD float3 f3(float s) { return make_float3(s, s, s); }
 FF_HD float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
 FF_HD float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
 FF_HD float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+FF_HD float3 operator-(float s, float3 a) { return make_float3(s - a.x, s - a.y, s - a.z); }
 FF_HD float3 operator*(float3 a, float3 b) { return make_float3(a.x * b.x, a.y * b.y, a.z * b.z); }
 FF_HD float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
 FF_HD float3 operator*(float s, float3 a) { return make_float3(s * a.x, s * a.y, s * a.z); }

@@ -117,13 +117,22 @@ struct ff_scene {
     size_t device_bytes() const;
 };
 
+struct FFWavefrontWS;
+void ff_wavefront_ws_free(FFWavefrontWS* ws);
+
 struct ff_film {
     ff_context* ctx = nullptr;
     uint32_t width = 0, height = 0;
     DevBuf accum;         // float4 per pixel: radiance sum (xyz)
     DevBuf comp;          // float4 per pixel: Kahan compensation
     DevBuf count;         // uint32 per pixel
+    FFWavefrontWS* ws = nullptr;  // path pool and queues of ff_render, kept between calls
+    ~ff_film() { ff_wavefront_ws_free(ws); }
 };
+
+// ff_wavefront.cu
+void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, ff_film* film,
+                         ff_render_stats* stats);
 
 // ff_bvh.cu: device BVH build from host or device triangle data already on
 // the device (positions float3[V], indices uint3[T]).
@@ -138,3 +147,8 @@ void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, u
 // no-allocation entry point).
 void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n,
                              ff_hit* d_hits, bool any_hit, unsigned long long* counter, unsigned int* err);
+
+// ff_trace.cu: trace a device queue whose length is in device memory.
+void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
+                           uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter,
+                           unsigned int* err);

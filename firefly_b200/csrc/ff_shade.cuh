@@ -1,0 +1,425 @@
+// ff_shade.cuh — materials, lights, camera and sampler of the wavefront path
+// tracer, following the reference's arithmetic operation by operation
+// (parity mode).  Compiled without FMA contraction (-fmad=false): every float
+// expression rounds once per operation in the reference's operand order, and
+// every place the reference widens to double (its FP64 GGX terms, MIS
+// weights, CDFs) widens here too.
+//
+// Sources (CUDA-RayTracer/): dMaterial.cu:90-469, dEnvironmentLight.cu:41-103,
+// dAreaLight.cu:18-68, Rectangle.cuh:24-123, dCamera.cu:10-36,
+// dRandom.cu:49-126, dMath.cuh:1300-1507, Helpers.cu:16-31.
+#pragma once
+
+#include "ff_common.cuh"
+
+// ------------------------------------------------------------- dimensions
+// Parity sampler: draw d of bounce b of a path sample uses ff_rand(key,
+// 32*b + d).  The reference draws from a clock-seeded stream in call order;
+// fixing one dimension per call site keeps every draw reproducible even when
+// a conditional call site is skipped (the area light's visibility and pdf
+// redraws happen only on some branches).  Pairs drawn through
+// make_float2(random(), random()) give x the second draw of the pair, the
+// order the reference's host build evaluates the arguments in.
+enum FFDim : uint32_t {
+    DIM_CAM_JITTER = 0,    // 0, 1  UniformSampleSquare in gen_ray
+    DIM_CAM_LENS = 2,      // 2, 3  ConcentricSampleDisk in gen_ray
+    DIM_LIGHT = 4,         // 4, 5  light get_direction
+    DIM_NEE_PDF = 6,       // 6, 7  area light get_pdf redraw in BRDF_L's NEE term
+    DIM_SPEC = 8,          // 8, 9  spec_sample e0, e1
+    DIM_DIFF = 10,         // 10,11 diff_sample e0, e1
+    DIM_SPEC_VIS = 12,     // 12,13 area light visible() redraw, spec MIS ray
+    DIM_SPEC_PDF = 14,     // 14,15 area light get_pdf redraw, spec MIS
+    DIM_DIFF_VIS = 16,     // 16,17 area light visible() redraw, diff MIS ray
+    DIM_DIFF_PDF = 18,     // 18,19 area light get_pdf redraw, diff MIS
+    DIM_LOBE = 20,         // 20    random() < 0.5 lobe choice
+    DIM_NEE_VIS = 21,      // 21,22 area light visible() redraw of the NEE ray (wf_shadow)
+    DIM_RR = 23,           // 23    Russian roulette
+    DIM_EXTRA = 24         // 24..31 materials without a reference counterpart
+};
+
+FF_D uint32_t dim_of(uint32_t bounce, uint32_t d) { return 32u * bounce + d; }
+
+// UniformSampleSquare / make_float2(random(), random()): x = second draw.
+FF_D float2 rand2(uint32_t key, uint32_t bounce, uint32_t d0)
+{
+    float first = ff_rand(key, dim_of(bounce, d0));
+    float second = ff_rand(key, dim_of(bounce, d0 + 1));
+    return make_float2(second, first);
+}
+
+// ----------------------------------------------------------- vector helpers
+// (dMath.cuh) normalize = v * rsqrtf(dot(v, v)); the reference's host build
+// defines rsqrtf as 1.0f / sqrtf (dMath.cuh:70-73).
+FF_D float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+FF_D float3 cross3(float3 a, float3 b)
+{
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+FF_D float3 normalize3(float3 v)
+{
+    float inv = 1.0f / sqrtf(dot3(v, v));
+    return v * inv;
+}
+FF_D float length3(float3 v) { return sqrtf(dot3(v, v)); }
+// reflect(i, n) = i - 2.0f * n * dot(n, i)  (dMath.cuh:1402)
+FF_D float3 reflect3(float3 i, float3 n) { return i - (2.0f * n) * dot3(n, i); }
+// clamp(f, a, b) = fmaxf(a, fminf(f, b)) with the host's a < b ? a : b forms
+FF_D float hmin(float a, float b) { return a < b ? a : b; }
+FF_D float hmax(float a, float b) { return a > b ? a : b; }
+FF_D float clampf(float f, float a, float b) { return hmax(a, hmin(f, b)); }
+FF_D float3 lerp3(float3 a, float3 b, float w) { return a * (1.f - w) + b * w; }
+// luminance returns (0.299 r + 0.587 g + 0.114 b) evaluated in double, as float (dMath.cuh:1503-1507)
+FF_D float luminance(float3 c) { return (float)(0.299 * (double)c.x + 0.587 * (double)c.y + 0.114 * (double)c.z); }
+// x^2 and x^5 of the reference's pow(x, 2) / pow(x, 5) (double pow of a widened float)
+FF_D double sq_d(double x) { return x * x; }
+FF_D double pow5_d(double x)
+{
+    double x2 = x * x;
+    return x2 * x2 * x;
+}
+
+// get_orthogonal_vec (dMath.cuh:1450-1463)
+FF_D float3 orthogonal_axis(float3 in)
+{
+    if (fabsf(in.x) < 0.57735026919f) return make_float3(1, 0, 0);
+    if (fabsf(in.y) < 0.57735026919f) return make_float3(0, 1, 0);
+    return make_float3(0, 0, 1);
+}
+
+// sample_spherical_map / sample_spherical_direction (dMath.cuh:1483-1500)
+FF_D float2 spherical_map(float3 d)
+{
+    float2 uv = make_float2(atan2f(d.z, d.x), asinf(d.y));
+    uv.x = uv.x * FF_1_2PI;
+    uv.y = uv.y * FF_1_PI;
+    uv.x = uv.x + 0.5f;
+    uv.y = uv.y + 0.5f;
+    return uv;
+}
+FF_D float3 spherical_direction(float2 uv)
+{
+    float theta = FF_2PI * uv.x;
+    float phi = FF_PI * uv.y;
+    float x = cosf(theta) * sinf(phi);
+    float y = cosf(phi);
+    float z = sinf(theta) * sinf(phi);
+    return make_float3(-x, -y, -z);
+}
+
+// ConcentricSampleDisk(u) (dRandom.cu:83-102)
+FF_D float2 concentric_disk(float2 u)
+{
+    float2 o = make_float2(2.f * u.x - 1.f, 2.f * u.y - 1.f);
+    if (o.x == 0 && o.y == 0) return make_float2(0, 0);
+    float theta, r;
+    if (fabsf(o.x) > fabsf(o.y)) {
+        r = o.x;
+        theta = FF_PI_4 * (o.y / o.x);
+    } else {
+        r = o.y;
+        theta = FF_PI_2 - FF_PI_4 * (o.x / o.y);
+    }
+    return make_float2(r * cosf(theta), r * sinf(theta));
+}
+
+// -------------------------------------------------------------- materials
+struct FFIsect {
+    float3 position;
+    float3 normal;
+    uint32_t material;
+    uint32_t prim;
+};
+
+// diff_get_pdf = 1.f / (2.f * M_PI) in float, returned as double (dMaterial.cu:160-163)
+FF_D double diff_get_pdf() { return (double)(1.f / (2.f * FF_PI)); }
+
+// fresnel(f0, h, wo) = f0 + (1 - f0) * pow(1 - fmaxf(0, dot(h, wo)), 5) (dMaterial.cu:90-92)
+FF_D float3 fresnel3(float3 f0, float3 h, float3 wo)
+{
+    float x = 1.f - hmax(0.f, dot3(h, wo));
+    float p = (float)pow5_d((double)x);
+    return f0 + (1.f - f0) * p;
+}
+
+// ggxtr_ndf (dMaterial.cu:120-125)
+FF_D double ggx_ndf(float3 n, float3 h, float r)
+{
+    double a2 = r * r * r * r;
+    double nh2 = sq_d((double)hmax(0.f, dot3(n, h)));
+    return a2 / ((double)FF_PI * sq_d(nh2 * (a2 - 1.0) + 1.0));
+}
+
+// geo_atten (dMaterial.cu:126-137); k = powf(r + 1, 2) / 8 in float
+FF_D double geo_atten(float3 wi, float3 wo, float3 n, float r)
+{
+    float rp = r + 1.f;
+    double k = (double)((rp * rp) / 8.f);
+    double nl = hmax(dot3(n, wi), 0.f);
+    double nv = hmax(dot3(n, wo), 0.f);
+    double g1 = nl / (nl * (1.0 - k) + k);
+    double g2 = nv / (nv * (1.0 - k) + k);
+    return g1 * g2;
+}
+
+// power_heuristic(1, f, 1, g) (dMaterial.cu:114-119)
+FF_D double power_heuristic(double f, double g) { return (f * f) / (f * f + g * g); }
+
+FF_D float3 f0_of(const ff_material& m, float3 albedo)
+{
+    return lerp3(make_float3(m.fresnel[0], m.fresnel[1], m.fresnel[2]), albedo, m.metallic);
+}
+
+// diff_f (dMaterial.cu:164-178)
+FF_D float3 diff_f(const ff_material& mat, float3 n, float3 wi, float3 wo)
+{
+    (void)n;
+    float m = mat.metallic;
+    float3 a = make_float3(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
+    float3 f0 = f0_of(mat, a);
+    float3 wh = normalize3(wo + wi);
+    float3 F = fresnel3(f0, wh, wi);
+    float3 kd = make_float3(1.f, 1.f, 1.f) - F;
+    kd = kd * (float)(1.0 - (double)m);
+    return (kd * a) * FF_1_PI;
+}
+
+// spec_get_pdf (dMaterial.cu:255-265), returned as float
+FF_D float spec_get_pdf(float3 n, float3 wi, float3 wo, float r)
+{
+    float3 wh = normalize3(wo + wi);
+    double wh_dot_n = hmax(dot3(wh, n), 0.f);
+    double wo_dot_wh = hmax(dot3(wo, wh), 0.f);
+    double D = ggx_ndf(n, wh, r);
+    return (float)((D * wh_dot_n) / (double)hmax((float)(4.0 * wo_dot_wh), 0.001f));
+}
+
+// spec_f (dMaterial.cu:266-288)
+FF_D float3 spec_f(const ff_material& mat, float3 n, float3 wi, float3 wo)
+{
+    float r = mat.roughness;
+    float3 a = make_float3(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
+    float3 f0 = f0_of(mat, a);
+    float3 wh = normalize3(wo + wi);
+    double n_dot_wi = hmax(dot3(n, wi), 0.f);
+    double n_dot_wo = hmax(dot3(n, wo), 0.f);
+    double D = ggx_ndf(n, wh, r);
+    double G = geo_atten(wi, wo, n, r);
+    float3 F = fresnel3(f0, wh, wi);
+    float3 num = (float)(D * G) * F;
+    return num / hmax((float)(4.0 * n_dot_wo * n_dot_wi), 0.001f);
+}
+
+// Orthonormal frame of the sampling routines: T = normalize(cross(N, axis)), B = normalize(cross(N, T)).
+FF_D void frame(float3 N, float3& T, float3& B)
+{
+    T = normalize3(cross3(N, orthogonal_axis(N)));
+    B = normalize3(cross3(N, T));
+}
+
+// diff_sample (dMaterial.cu:139-159): uniform hemisphere around N
+FF_D float3 diff_sample(float3 N, float e0, float e1)
+{
+    float sin_theta = sqrtf(1.f - e0 * e0);
+    float phi = 2.f * FF_PI * e1;
+    float x = sin_theta * cosf(phi);
+    float z = sin_theta * sinf(phi);
+    float3 T, B;
+    frame(N, T, B);
+    return normalize3(T * x + N * e0 + B * z);
+}
+
+// spec_sample (dMaterial.cu:229-254): GGX half vector, theta and phi in double
+FF_D float3 spec_sample(float3 N, float3 wo, float r, float e0, float e1)
+{
+    double theta = (double)atanf(r * r * sqrtf(e0 / (1.f - e0)));
+    double phi = (double)(2 * FF_PI * e1);
+    float3 h = make_float3((float)(sin(theta) * cos(phi)), (float)cos(theta), (float)(sin(theta) * sin(phi)));
+    float3 T, B;
+    frame(N, T, B);
+    float3 s = T * h.x + N * h.y + B * h.z;
+    return -reflect3(wo, normalize3(s));
+}
+
+// BRDF_f = spec_f + diff_f; BRDF_pdf = 0.5 (spec_pdf + diff_pdf) (dMaterial.cu:459-469)
+FF_D float3 brdf_f(const ff_material& m, float3 n, float3 wi, float3 wo)
+{
+    return spec_f(m, n, wi, wo) + diff_f(m, n, wi, wo);
+}
+FF_D float brdf_pdf(const ff_material& m, float3 n, float3 wi, float3 wo)
+{
+    float sp = spec_get_pdf(n, wi, wo, m.roughness);
+    float dp = (float)diff_get_pdf();
+    return (float)(0.5 * (double)(sp + dp));
+}
+
+// ----------------------------------------------------------------- lights
+// Environment light with importance tables (dEnvironmentLight.cu).
+struct FFEnvView {
+    const float3* rgb;       // width*height texels, row y = v * height
+    const double* marginal;  // marginal_y[height]
+    const double* cond;      // conds_y[height][width] row-major
+    const float* pdf;        // pdf texels, already scaled by w*h/(2 pi^2)
+    int width, height;
+    float3 color;            // constant colour when rgb == nullptr
+    float radius;            // 10000 (dEnvironmentLight.cu:14)
+};
+
+// tex2DLod<float4> with normalised coordinates, wrap addressing and linear
+// filtering: x_B = x*W - 0.5, i = floor(x_B), alpha = frac(x_B) with 8
+// fractional bits, as the CUDA Programming Guide specifies texture filtering.
+FF_D float3 tex_bilinear(const float3* texels, int w, int h, float u, float v)
+{
+    float xb = u * (float)w - 0.5f;
+    float yb = v * (float)h - 0.5f;
+    float fx = floorf(xb), fy = floorf(yb);
+    float ax = xb - fx, ay = yb - fy;
+    ax = floorf(ax * 256.f + 0.5f) / 256.f;
+    ay = floorf(ay * 256.f + 0.5f) / 256.f;
+    int ix = (int)fx, iy = (int)fy;
+    int x0 = ix % w;
+    x0 = x0 < 0 ? x0 + w : x0;
+    int x1 = (x0 + 1 == w) ? 0 : x0 + 1;
+    int y0 = iy % h;
+    y0 = y0 < 0 ? y0 + h : y0;
+    int y1 = (y0 + 1 == h) ? 0 : y0 + 1;
+    float3 t00 = texels[y0 * w + x0], t10 = texels[y0 * w + x1];
+    float3 t01 = texels[y1 * w + x0], t11 = texels[y1 * w + x1];
+    float w00 = (1.f - ax) * (1.f - ay), w10 = ax * (1.f - ay), w01 = (1.f - ax) * ay, w11 = ax * ay;
+    return make_float3(w00 * t00.x + w10 * t10.x + w01 * t01.x + w11 * t11.x,
+                       w00 * t00.y + w10 * t10.y + w01 * t01.y + w11 * t11.y,
+                       w00 * t00.z + w10 * t10.z + w01 * t01.z + w11 * t11.z);
+}
+
+// upper_bound (Helpers.cu:16-31), including its list[left <= val] index.
+FF_D int upper_bound_ref(const double* list, int size, float val)
+{
+    int left = 0, right = size;
+    while (left < right) {
+        int middle = (right - left) / 2 + left;
+        if ((double)val >= list[middle]) left = middle + 1;
+        else right = middle;
+    }
+    if (left < size && list[(left <= val) ? 1 : 0] != 0.0) left++;
+    return left;
+}
+
+FF_D float3 env_L(const FFEnvView& e, float3 wi)
+{
+    if (!e.rgb) return e.color;
+    float2 uv = spherical_map(wi);
+    return tex_bilinear(e.rgb, e.width, e.height, uv.x, uv.y);
+}
+
+// get_direction (dEnvironmentLight.cu:41-58); ex = first draw, ey = second.
+FF_D void env_sample(const FFEnvView& e, float3 pos, float ex, float ey, float3& wi, float3& sp)
+{
+    int y = (int)((float)upper_bound_ref(e.marginal, e.height, ey) - 1.f);
+    y = y < 0 ? 0 : (y >= e.height ? e.height - 1 : y);
+    int x = (int)((float)upper_bound_ref(e.cond + (size_t)y * e.width, e.width, ex) - 1.f);
+    x = x < 0 ? 0 : (x >= e.width ? e.width - 1 : x);
+    float u = (float)x / (float)e.width;
+    float v = (float)y / (float)e.height;
+    float3 dir = spherical_direction(make_float2(u, v));
+    sp = make_float3(0.f, 0.f, 0.f) + dir * e.radius;
+    wi = normalize3(sp - pos);
+}
+
+// get_pdf(isect, wi) (dEnvironmentLight.cu:83-103): pdf texel over sin(acos(wi.z))
+FF_D float env_pdf(const FFEnvView& e, float3 wi)
+{
+    float2 uv = spherical_map(wi);
+    int x = (int)(uv.x * (float)(e.width - 1));
+    int y = (int)(uv.y * (float)(e.height - 1));
+    float p = (x >= 0 && y >= 0 && x < e.width && y < e.height) ? e.pdf[(size_t)y * e.width + x] : 0.f;
+    return p / sinf(acosf(clampf(wi.z, -1.f, 1.f)));
+}
+
+// Rectangle area light (Rectangle.cuh, dAreaLight.cu)
+struct FFRect {
+    float3 p0, a, b, n;
+    float a_len2, b_len2, inv_area;
+    float3 Le;  // radiance * emissiveColorFactor
+};
+
+FF_D FFRect make_rect(const ff_area_light& L)
+{
+    FFRect r;
+    r.p0 = make_float3(L.p0[0], L.p0[1], L.p0[2]);
+    r.a = make_float3(L.a[0], L.a[1], L.a[2]);
+    r.b = make_float3(L.b[0], L.b[1], L.b[2]);
+    r.n = make_float3(L.normal[0], L.normal[1], L.normal[2]);
+    float la = length3(r.a), lb = length3(r.b);
+    r.a_len2 = la * la;
+    r.b_len2 = lb * lb;
+    r.inv_area = 1.f / (la * lb);
+    r.Le = L.radiance * make_float3(L.emissive[0], L.emissive[1], L.emissive[2]);
+    return r;
+}
+
+// _Rectangle::sample with u = UniformSampleSquare()
+FF_D float3 rect_sample(const FFRect& r, float2 u) { return r.p0 + u.x * r.a + u.y * r.b; }
+
+// _Rectangle::hit(ray) (Rectangle.cuh:74-97)
+FF_D bool rect_hit(const FFRect& r, float3 o, float3 d)
+{
+    float t = dot3(r.p0 - o, r.n) / dot3(d, r.n);
+    float3 p = o + t * d;
+    float3 p0p = p - r.p0;
+    if (t <= FF_K_EPSILON) return false;
+    float pa = dot3(p0p, r.a);
+    if (pa < 0.0f || pa > r.a_len2) return false;
+    float pb = dot3(p0p, r.b);
+    if (pb < 0.0f || pb > r.b_len2) return false;
+    return true;
+}
+
+// dAreaLight::L (dAreaLight.cu:26-34)
+FF_D float3 rect_L(const FFRect& r, float3 wi)
+{
+    float nd = dot3(-r.n, wi);
+    return nd > 0.0f ? r.Le : make_float3(0.f, 0.f, 0.f);
+}
+
+// dAreaLight::get_pdf(isect, wi) (dAreaLight.cu:47-57): a freshly drawn point
+FF_D float rect_pdf(const FFRect& r, float3 pos, float2 u)
+{
+    float3 sp = rect_sample(r, u);
+    float3 w = normalize3(sp - pos);
+    float nd = fabsf(dot3(r.n, -w));
+    float dist = length3(sp - pos);
+    float d2 = dist * dist;
+    return (d2 / nd) * r.inv_area;
+}
+
+// --------------------------------------------------------------- camera
+// dCamera::gen_ray (dCamera.cu:10-36); the NDC is computed in double because
+// the reference adds the double literal 0.5 to the pixel coordinate.
+FF_D float4 mat_mul4(const float* m, float4 v)
+{
+    // Matrix4x4 * float4 (dMatrix.cuh:61-69): out.c = sum_i m[i][c] * v_i
+    return make_float4(m[0] * v.x + m[4] * v.y + m[8] * v.z + m[12] * v.w,
+                       m[1] * v.x + m[5] * v.y + m[9] * v.z + m[13] * v.w,
+                       m[2] * v.x + m[6] * v.y + m[10] * v.z + m[14] * v.w,
+                       m[3] * v.x + m[7] * v.y + m[11] * v.z + m[15] * v.w);
+}
+
+FF_D void gen_camera_ray(const ff_camera& cam, int hres, int vres, int px, int py, float2 jitter, float2 lens,
+                         float3& o, float3& d)
+{
+    float ndx = (float)(2.f * (((double)px + 0.5) / hres) - 1.f);
+    float ndy = (float)(1.f - 2.f * (((double)py + 0.5) / vres));
+    float4 pn = mat_mul4(cam.inv_view_proj, make_float4(ndx, ndy, -1.f, 1.f));
+    float4 pf = mat_mul4(cam.inv_view_proj, make_float4(ndx, ndy, 1.f, 1.f));
+    float3 p_near = make_float3(pn.x / pn.w, pn.y / pn.w, pn.z / pn.w);
+    float3 p_far = make_float3(pf.x / pf.w, pf.y / pf.w, pf.z / pf.w);
+    float2 sp = make_float2(jitter.x * cam.pixel_jitter, jitter.y * cam.pixel_jitter);
+    o = p_near + make_float3(sp.x, sp.y, 0.f);
+    d = normalize3(p_far - p_near);
+    if (cam.lens_radius > 0.f) {
+        float3 focal = o + d * cam.focal_distance;
+        float2 pl = concentric_disk(lens);
+        pl = make_float2(pl.x * cam.lens_radius, pl.y * cam.lens_radius);
+        o = o + make_float3(pl.x, pl.y, 0.f);
+        d = normalize3(focal - o);
+    }
+}

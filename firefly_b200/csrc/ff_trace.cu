@@ -20,8 +20,12 @@ constexpr int kRefillIdle = 8;
 template <bool ANY>
 __global__ void __launch_bounds__(kTraceBlock, 4)
     k_trace(FFBvhView bvh, const ff_ray* __restrict__ rays, ff_hit* __restrict__ hits, uint64_t n,
-            unsigned long long* __restrict__ counter, unsigned int* __restrict__ err)
+            unsigned long long* __restrict__ counter, unsigned int* __restrict__ err,
+            const uint32_t* __restrict__ n_dev)
 {
+    // Queue-driven launches (the wavefront) read the ray count written by the
+    // producing stage; n is then the queue capacity.
+    if (n_dev) n = min(n, (uint64_t)*n_dev);
     // A ray visits every node at most once; more steps than nodes means a
     // malformed BVH.  The ray is then ended and counted in err[0] instead of
     // looping.
@@ -111,9 +115,9 @@ void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, u
     const uint64_t need = (n + kTraceBlock - 1) / kTraceBlock;
     if (grid > need) grid = need;
     if (any_hit)
-        k_trace<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err);
+        k_trace<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err, nullptr);
     else
-        k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err);
+        k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err, nullptr);
     FF_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -133,8 +137,34 @@ void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d
     const uint64_t need = (n + kTraceBlock - 1) / kTraceBlock;
     if (grid > need) grid = need;
     if (any_hit)
-        k_trace<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err);
+        k_trace<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err, nullptr);
     else
-        k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err);
+        k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err, nullptr);
+    FF_CUDA_CHECK(cudaGetLastError());
+}
+
+// Trace a device-resident queue whose length the previous stage wrote to
+// n_dev (at most cap rays), on the context's stream.  counter must be zeroed
+// by the caller before the launch.
+void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
+                           uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter, unsigned int* err)
+{
+    if (cap == 0) return;
+    static int bps[2] = {0, 0};
+    int& blocks_per_sm = bps[any_hit ? 1 : 0];
+    if (blocks_per_sm == 0) {
+        if (any_hit)
+            FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true>, kTraceBlock, 0));
+        else
+            FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false>, kTraceBlock, 0));
+        blocks_per_sm = blocks_per_sm < 1 ? 1 : blocks_per_sm;
+    }
+    uint64_t grid = (uint64_t)ctx->num_sms * blocks_per_sm;
+    const uint64_t need = (cap + kTraceBlock - 1) / kTraceBlock;
+    if (grid > need) grid = need;
+    if (any_hit)
+        k_trace<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev);
+    else
+        k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev);
     FF_CUDA_CHECK(cudaGetLastError());
 }

@@ -1,22 +1,796 @@
-// ff_wavefront.cu — wavefront stages (filled in next).
+// ff_wavefront.cu — the wavefront path tracer behind ff_render.
+//
+// Replaces wavefront_pathtrace and its stages (CUDA-RayTracer/kernel.cu:
+// wf_logic :298-455, wf_generate :458-485, wf_extend :488-523, wf_shadow
+// :526-543, wf_mat_diffuse :546-577, wf_mat_cook :580-614, wf_mat_mix
+// :617-651, driver :658-676) and the PathTracer frame loop
+// (PathTracer.cpp:59-79).
+//
+// One frame advances every path in flight by one bounce, as in the
+// reference:
+//   k_logic    consume the previous extension hit and shadow answers; add
+//              the NEE contribution, update the throughput, Russian roulette;
+//              terminated paths start their next sample with a camera ray
+//              (wf_generate fused in); continuing paths sample the light and
+//              are compacted into one queue per material kind with warp
+//              ballots.
+//   k_shade<K> per material kind: BRDF_L / BRDF_f / BRDF_pdf of the
+//              reference's mix material (or the single-lobe and added kinds),
+//              the continuation ray, and up to three shadow rays: the NEE ray
+//              of wf_shadow and the two BSDF-sampled visibility rays that
+//              BRDF_L traces inline in the reference.
+//   k_trace    closest-hit over the extension queue, any-hit over the shadow
+//              queue (persistent kernel of ff_trace.cu, queue length read on
+//              the device).
+// The path pool has m slots per pixel; slot j always renders pixel j % (w*h)
+// and samples j / (w*h) + k*m, and keeps a compensated (Kahan) FP32 sum of its
+// radiance.  The film adds the m slot sums per pixel in a fixed order, so
+// results do not depend on scheduling.  Frames repeat until no slot has work.
+#include <algorithm>
+#include <vector>
+
 #include "ff_internal.h"
+#include "ff_shade.cuh"
 
-extern "C" {
+namespace {
 
-ff_status ff_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* settings, ff_film* film,
-                    ff_render_stats* stats)
+constexpr int kKinds = 5;
+constexpr uint32_t PH_START = 0, PH_FLIGHT = 1, PH_DONE = 2;
+constexpr int32_t SQ_NONE = -1, SQ_BLOCKED = -2;
+
+// Counter words of one frame (zeroed at the start of each frame).
+enum { C_EXT = 0, C_SH = 1, C_MAT = 2, C_ACTIVE = 2 + kKinds, C_WORDS = 8 + kKinds };
+
+struct WF {
+    // launch constants
+    uint32_t P, WH, W, H, m;
+    uint32_t seed, max_depth, rr_depth, mode;
+    int32_t light;
+    float shadow_offset;
+    // slot state
+    uint32_t* samples_left;
+    uint32_t* next_sample;
+    uint32_t* key;
+    uint32_t* length;
+    uint32_t* phase;
+    float4* beta;
+    float4* ray_o;
+    float4* ray_d;
+    int32_t* ext_q;
+    int4* sh_q;
+    float4* c_nee;
+    float4* c_spec;
+    float4* c_diff;
+    float4* ext_fp;   // f.xyz, pdf
+    float* ext_cos;
+    float4* hit_pos;  // xyz, w = material index bits
+    float4* hit_nrm;
+    float4* light_wi;
+    float4* light_sp;
+    float4* acc;
+    float4* acc_c;
+    uint32_t* cnt;
+    // queues
+    ff_ray* ext_rays;
+    ff_hit* ext_hits;
+    ff_ray* sh_rays;
+    ff_hit* sh_hits;
+    uint32_t* mat_queue;   // kKinds * P
+    uint32_t* ctr;         // C_WORDS
+    unsigned long long* totals;  // [0] extension rays, [1] shadow rays, [2] samples
+    // scene
+    const FFShadeTri* shade;
+    const ff_material* mats;
+    const ff_area_light* area;
+    uint32_t n_area;
+    FFEnvView env;
+    ff_camera cam;
+};
+
+__device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
+__device__ __forceinline__ float4 f4(float3 v, float w = 0.f) { return make_float4(v.x, v.y, v.z, w); }
+
+// Warp-aggregated append (the reference's atomicAggInc, kernel.cu:24-36, on
+// *_sync intrinsics): one atomic per warp and per queue.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want, unsigned long long* total)
 {
-    (void)scene; (void)settings; (void)film; (void)stats;
-    if (!ctx) return FF_ERR_INVALID_ARG;
-    ctx->last_error = "ff_render is not available in this build";
-    return FF_ERR_UNSUPPORTED;
+    const uint32_t mask = __ballot_sync(__activemask(), want);
+    if (!want) return 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) {
+        base = atomicAdd(counter, (uint32_t)__popc(mask));
+        if (total) atomicAdd(total, (unsigned long long)__popc(mask));
+    }
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
 }
 
-ff_status ff_scene_read_env_tables(const ff_scene* scene, double* marginal, double* conditional, float* pdf,
-                                   double* pdf_denom)
+__device__ __forceinline__ void kahan_add(float4& sum, float4& c, float3 x)
 {
-    (void)scene; (void)marginal; (void)conditional; (void)pdf; (void)pdf_denom;
-    return FF_ERR_UNSUPPORTED;
+    float3 y = make_float3(x.x - c.x, x.y - c.y, x.z - c.z);
+    float3 t = make_float3(sum.x + y.x, sum.y + y.y, sum.z + y.z);
+    c = make_float4((t.x - sum.x) - y.x, (t.y - sum.y) - y.y, (t.z - sum.z) - y.z, 0.f);
+    sum = make_float4(t.x, t.y, t.z, 0.f);
 }
 
+__device__ __forceinline__ uint32_t slot_pixel(const WF& w, uint32_t s) { return s % w.WH; }
+
+// wf_generate + dCamera::gen_ray for slot s, sample `sample`.
+__device__ void start_sample(const WF& w, uint32_t s, uint32_t sample, bool& push, ff_ray& ray)
+{
+    const uint32_t pix = slot_pixel(w, s);
+    const uint32_t key = ff_path_key(w.seed, pix, sample);
+    w.key[s] = key;
+    w.length[s] = 0;
+    w.beta[s] = make_float4(1.f, 1.f, 1.f, 0.f);
+    const int x = (int)(pix % w.W), y = (int)(pix / w.W);
+    float3 o, d;
+    gen_camera_ray(w.cam, (int)w.W, (int)w.H, x, y, rand2(key, 0, DIM_CAM_JITTER), rand2(key, 0, DIM_CAM_LENS), o, d);
+    w.ray_o[s] = f4(o);
+    w.ray_d[s] = f4(d);
+    ray = ff_ray{o.x, o.y, o.z, 0.f, d.x, d.y, d.z, __int_as_float(0x7f800000)};
+    push = true;
+}
+
+__global__ void __launch_bounds__(256) k_logic(WF w)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    bool push_ext = false;
+    ff_ray ray{};
+    int kind = -1;
+    bool active = false;
+    if (s < w.P) {
+        uint32_t ph = w.phase[s];
+        if (ph == PH_START) {
+            const uint32_t smp = w.next_sample[s];
+            w.next_sample[s] = smp + w.m;
+            start_sample(w, s, smp, push_ext, ray);
+            w.phase[s] = PH_FLIGHT;
+            active = true;
+        } else if (ph == PH_FLIGHT) {
+            active = true;
+            const uint32_t key = w.key[s];
+            const ff_hit hit = w.ext_hits[w.ext_q[s]];
+            const uint32_t L = w.length[s] + 1;  // wf_extend's length++
+            const bool found = hit.prim >= 0;
+            const float3 ro = xyz(w.ray_o[s]), rd = xyz(w.ray_d[s]);
+            float3 beta = xyz(w.beta[s]);
+            float4 acc = w.acc[s], accc = w.acc_c[s];
+            bool terminate = (L > w.max_depth) || !found;
+            // kernel.cu:332-338: environment radiance on a camera-ray miss
+            if (!found && L == 1) kahan_add(acc, accc, beta * env_L(w.env, rd));
+            if (L > 1) {
+                // kernel.cu:357-359: light_brdf * beta when the NEE ray was unoccluded
+                const int4 q = w.sh_q[s];
+                const bool vis = q.x >= 0 && w.sh_hits[q.x].prim < 0;
+                const bool vis_s = q.y >= 0 && w.sh_hits[q.y].prim < 0;
+                const bool vis_d = q.z >= 0 && w.sh_hits[q.z].prim < 0;
+                if (w.mode == FF_MODE_CORRECTED) {
+                    // every term gated by its own visibility ray
+                    float3 lb = make_float3(0.f, 0.f, 0.f);
+                    if (vis) lb = lb + xyz(w.c_nee[s]);
+                    if (vis_s) lb = lb + xyz(w.c_spec[s]);
+                    if (vis_d) lb = lb + xyz(w.c_diff[s]);
+                    if (vis || vis_s || vis_d) kahan_add(acc, accc, lb * beta);
+                } else if (vis) {
+                    // parity: the whole light_brdf, MIS terms included, rides on the NEE ray
+                    float3 lb = xyz(w.c_nee[s]);
+                    if (vis_s) lb = lb + xyz(w.c_spec[s]);
+                    if (vis_d) lb = lb + xyz(w.c_diff[s]);
+                    kahan_add(acc, accc, lb * beta);
+                }
+                const float4 fp = w.ext_fp[s];
+                const float3 f = xyz(fp);
+                const float pdf = fp.w;
+                const float cosine = w.ext_cos[s];
+                if (f == make_float3(0.f, 0.f, 0.f) || pdf == 0.f) {
+                    terminate = true;
+                } else {
+                    beta *= (f * cosine) / pdf;
+                    if (L > w.rr_depth) {
+                        const float q_rr = hmax(0.05f, 1.f - beta.y);
+                        if (ff_rand(key, dim_of(L, DIM_RR)) < q_rr) terminate = true;
+                        else if (w.mode == FF_MODE_CORRECTED) beta = beta / (1.f - q_rr);
+                    }
+                }
+            }
+            w.acc[s] = acc;
+            w.acc_c[s] = accc;
+            if (terminate) {
+                w.cnt[s] += 1u;
+                const uint32_t left = w.samples_left[s] - 1u;
+                w.samples_left[s] = left;
+                if (left > 0) {
+                    const uint32_t smp = w.next_sample[s];
+                    w.next_sample[s] = smp + w.m;
+                    start_sample(w, s, smp, push_ext, ray);
+                } else {
+                    w.phase[s] = PH_DONE;
+                    active = false;
+                }
+            } else {
+                // Continue: hit attributes (dTriangle::hit, dTriangle.cu:94-105).
+                const FFShadeTri& t = w.shade[hit.prim];
+                const float u = hit.u, v = hit.v;
+                const float3 n = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
+                const float3 pos = ro + hit.t * rd;
+                // Light sample (kernel.cu:435, light get_direction).
+                float3 wi, sp;
+                if (w.light < 0) {
+                    env_sample(w.env, pos, ff_rand(key, dim_of(L, DIM_LIGHT)), ff_rand(key, dim_of(L, DIM_LIGHT + 1)),
+                               wi, sp);
+                } else {
+                    const FFRect r = make_rect(w.area[w.light]);
+                    sp = rect_sample(r, rand2(key, L, DIM_LIGHT));
+                    wi = normalize3(sp - pos);
+                }
+                w.length[s] = L;
+                w.beta[s] = f4(beta);
+                w.hit_pos[s] = f4(pos, __uint_as_float(t.material));
+                w.hit_nrm[s] = f4(n);
+                w.light_wi[s] = f4(wi);
+                w.light_sp[s] = f4(sp);
+                kind = w.mats[t.material].kind;
+            }
+        }
+    }
+    // compaction into the extension queue and the material queues
+    const uint32_t qe = warp_append(&w.ctr[C_EXT], push_ext, &w.totals[0]);
+    if (push_ext) {
+        w.ext_rays[qe] = ray;
+        w.ext_q[s] = (int32_t)qe;
+    }
+#pragma unroll
+    for (int k = 0; k < kKinds; ++k) {
+        const uint32_t qm = warp_append(&w.ctr[C_MAT + k], kind == k, nullptr);
+        if (kind == k) w.mat_queue[(size_t)k * w.P + qm] = s;
+    }
+    const uint32_t am = __ballot_sync(0xffffffffu, active);
+    if ((threadIdx.x & 31u) == 0 && am) atomicAdd(&w.ctr[C_ACTIVE], (uint32_t)__popc(am));
+}
+
+struct ShadeOut {
+    float3 c_nee, c_spec, c_diff;
+    bool ray_nee, ray_spec, ray_diff;   // shadow rays to trace
+    ff_ray r_nee, r_spec, r_diff;
+    float3 ext_o, ext_d, ext_f;
+    float ext_pdf, ext_cos;
+};
+
+__device__ __forceinline__ ff_ray make_ray(float3 o, float3 d, float tmax)
+{
+    return ff_ray{o.x, o.y, o.z, 0.f, d.x, d.y, d.z, tmax};
+}
+
+// Light radiance toward wi, pdf of wi, and the visibility ray of light.visible()
+// (env: any occluder; area: the rectangle must be hit, and the occluder must
+// lie before the projection of a fresh sample point).
+struct LightCtx {
+    const WF* w;
+    bool is_env;
+    FFRect rect;
+};
+
+__device__ __forceinline__ float3 light_L(const LightCtx& lc, float3 wi)
+{
+    return lc.is_env ? env_L(lc.w->env, wi) : rect_L(lc.rect, wi);
+}
+__device__ __forceinline__ float light_pdf(const LightCtx& lc, float3 pos, float3 wi, uint32_t key, uint32_t L,
+                                           uint32_t dim)
+{
+    return lc.is_env ? env_pdf(lc.w->env, wi) : rect_pdf(lc.rect, pos, rand2(key, L, dim));
+}
+// Visibility ray of light.visible(ray): returns false when the reference
+// answers "not visible" without tracing (area light missed).
+__device__ __forceinline__ bool light_vis_ray(const LightCtx& lc, float3 o, float3 d, uint32_t key, uint32_t L,
+                                              uint32_t dim, ff_ray& out)
+{
+    if (lc.is_env) {
+        out = make_ray(o, d, FF_K_HUGE);
+        return true;
+    }
+    if (!rect_hit(lc.rect, o, d)) return false;
+    const float ts = dot3(rect_sample(lc.rect, rand2(key, L, dim)) - o, d);
+    out = make_ray(o, d, ts);
+    return true;
+}
+
+// wf_mat_mix + BRDF_L / BRDF_f / BRDF_pdf (kernel.cu:617-651, dMaterial.cu:363-469)
+__device__ void shade_mix(const WF& w, const LightCtx& lc, const ff_material& mat, float3 pos, float3 n, float3 wo,
+                          float3 wi, float3 sp, uint32_t key, uint32_t L, ShadeOut& o)
+{
+    (void)sp;
+    const bool corrected = w.mode == FF_MODE_CORRECTED;
+    const float r = mat.roughness;
+    float3 Lsum = make_float3(0.f, 0.f, 0.f);
+    const float3 Li = light_L(lc, wi);
+    const float n_dot_wi = dot3(n, wi);
+    if (n_dot_wi > 0.f) {
+        const double diff_pdf = diff_get_pdf();
+        const double spec_pdf = spec_get_pdf(n, wi, wo, r);
+        const double lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+        if (lpdf > 0.f && Li != make_float3(0.f, 0.f, 0.f)) {
+            const double diff_w = power_heuristic(lpdf, diff_pdf);
+            const double spec_w = power_heuristic(lpdf, spec_pdf);
+            float3 f = spec_f(mat, n, wi, wo) * n_dot_wi;
+            if (f != make_float3(0.f, 0.f, 0.f)) Lsum = Lsum + ((f * (float)spec_w) * Li) / (float)lpdf;
+            f = diff_f(mat, n, wi, wo) * n_dot_wi;
+            if (f != make_float3(0.f, 0.f, 0.f)) Lsum = Lsum + ((f * (float)diff_w) * Li) / (float)lpdf;
+        }
+    }
+    o.c_nee = Lsum;
+    const float3 wi_spec = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
+    const float3 wi_diff = diff_sample(n, ff_rand(key, dim_of(L, DIM_DIFF)), ff_rand(key, dim_of(L, DIM_DIFF + 1)));
+    // BSDF-sampled MIS terms; their visibility is traced as shadow rays
+    o.ray_spec = o.ray_diff = false;
+    {
+        const float3 org = pos + wi_spec * 0.001f;
+        const float nd = dot3(n, wi_spec);
+        ff_ray vr;
+        if (nd > 0.f && light_vis_ray(lc, org, wi_spec, key, L, DIM_SPEC_VIS, vr)) {
+            const double spdf = spec_get_pdf(n, wi_spec, wo, r);
+            const double lpdf = light_pdf(lc, pos, wi_spec, key, L, DIM_SPEC_PDF);
+            const double wgt = power_heuristic(spdf, lpdf);
+            const float3 f = spec_f(mat, n, wi_spec, wo) * nd;
+            const float3 Li2 = light_L(lc, wi_spec);
+            if (f != make_float3(0.f, 0.f, 0.f) && spdf > 0.f && Li2 != make_float3(0.f, 0.f, 0.f)) {
+                o.c_spec = ((f * Li2) * (float)wgt) / (float)spdf;
+                o.ray_spec = true;
+                o.r_spec = vr;
+            }
+        }
+    }
+    {
+        // dMaterial.cu:431: the reference offsets this ray along wi_spec (parity)
+        const float3 org = corrected ? pos + wi_diff * 0.001f : pos + wi_spec * 0.001f;
+        const float nd = dot3(n, wi_diff);
+        ff_ray vr;
+        if (nd > 0.f && light_vis_ray(lc, org, wi_diff, key, L, DIM_DIFF_VIS, vr)) {
+            const double dpdf = diff_get_pdf();
+            const double lpdf = light_pdf(lc, pos, wi_diff, key, L, DIM_DIFF_PDF);
+            const double wgt = power_heuristic(dpdf, lpdf);
+            const float3 f = diff_f(mat, n, wi_diff, wo) * nd;
+            const float3 Li2 = light_L(lc, wi_diff);
+            if (f != make_float3(0.f, 0.f, 0.f) && dpdf > 0.f && Li2 != make_float3(0.f, 0.f, 0.f)) {
+                o.c_diff = ((f * Li2) * (float)wgt) / (float)dpdf;
+                o.ray_diff = true;
+                o.r_diff = vr;
+            }
+        }
+    }
+    const float3 dir = ff_rand(key, dim_of(L, DIM_LOBE)) < 0.5f ? wi_diff : wi_spec;
+    o.ext_d = dir;
+    o.ext_f = brdf_f(mat, n, dir, wo);
+    o.ext_pdf = brdf_pdf(mat, n, dir, wo);
+    o.ext_cos = hmax(0.f, dot3(n, dir));
+}
+
+// wf_mat_diffuse (kernel.cu:546-577): diff_L returns 0 in the reference (dMaterial.cu:179-227).
+__device__ void shade_diffuse(const WF& w, const LightCtx& lc, const ff_material& mat, float3 pos, float3 n,
+                              float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
+{
+    o.c_nee = make_float3(0.f, 0.f, 0.f);
+    if (w.mode == FF_MODE_CORRECTED) {
+        const float nd = dot3(n, wi);
+        const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+        const float3 Li = light_L(lc, wi);
+        if (nd > 0.f && lpdf > 0.f) o.c_nee = ((diff_f(mat, n, wi, wo) * nd) * Li) / lpdf;
+    }
+    o.ray_spec = o.ray_diff = false;
+    const float3 dir = diff_sample(n, ff_rand(key, dim_of(L, DIM_DIFF)), ff_rand(key, dim_of(L, DIM_DIFF + 1)));
+    o.ext_d = dir;
+    o.ext_f = diff_f(mat, n, dir, wo);
+    o.ext_pdf = (float)diff_get_pdf();
+    o.ext_cos = hmax(0.f, dot3(n, dir));
+}
+
+// wf_mat_cook (kernel.cu:580-614): spec_L returns 0 in the reference (dMaterial.cu:314-361).
+__device__ void shade_conductor(const WF& w, const LightCtx& lc, const ff_material& mat, float3 pos, float3 n,
+                                float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
+{
+    o.c_nee = make_float3(0.f, 0.f, 0.f);
+    if (w.mode == FF_MODE_CORRECTED) {
+        const float nd = dot3(n, wi);
+        const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+        const float3 Li = light_L(lc, wi);
+        if (nd > 0.f && lpdf > 0.f) o.c_nee = ((spec_f(mat, n, wi, wo) * nd) * Li) / lpdf;
+    }
+    o.ray_spec = o.ray_diff = false;
+    const float r = mat.roughness;
+    const float3 dir = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
+    o.ext_d = dir;
+    o.ext_f = spec_f(mat, n, dir, wo);
+    o.ext_pdf = spec_get_pdf(n, dir, wo, r);
+    o.ext_cos = hmax(0.f, dot3(n, dir));
+}
+
+// Thin GGX dielectric (no reference counterpart): with probability equal to
+// the Schlick reflectance at the surface's IOR the path reflects off a GGX
+// lobe, otherwise it is transmitted through the sheet unchanged.  The
+// transmission is a delta lobe (no NEE through it); the GGX reflection gets
+// light-sampled NEE.
+__device__ void shade_dielectric(const WF& w, const LightCtx& lc, const ff_material& mat, float3 pos, float3 n,
+                                 float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
+{
+    (void)w;
+    const float eta = mat.ior > 0.f ? mat.ior : 1.5f;
+    const float r0 = ((eta - 1.f) / (eta + 1.f)) * ((eta - 1.f) / (eta + 1.f));
+    const float cos_o = fabsf(dot3(n, wo));
+    const float x = 1.f - cos_o;
+    const float Fr = r0 + (1.f - r0) * x * x * x * x * x;
+    ff_material m = mat;
+    m.fresnel[0] = m.fresnel[1] = m.fresnel[2] = r0;
+    m.base_color[0] = m.base_color[1] = m.base_color[2] = 1.f;
+    m.metallic = 0.f;
+    o.ray_spec = o.ray_diff = false;
+    o.c_nee = make_float3(0.f, 0.f, 0.f);
+    const float nd = dot3(n, wi);
+    const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+    if (nd > 0.f && lpdf > 0.f) o.c_nee = ((spec_f(m, n, wi, wo) * nd) * light_L(lc, wi)) / lpdf;
+    if (ff_rand(key, dim_of(L, DIM_EXTRA)) < Fr) {
+        const float3 dir = spec_sample(n, wo, m.roughness, ff_rand(key, dim_of(L, DIM_SPEC)),
+                                       ff_rand(key, dim_of(L, DIM_SPEC + 1)));
+        o.ext_d = dir;
+        o.ext_f = spec_f(m, n, dir, wo) / Fr;
+        o.ext_pdf = spec_get_pdf(n, dir, wo, m.roughness);
+        o.ext_cos = hmax(0.f, dot3(n, dir));
+    } else {
+        const float3 tint = make_float3(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
+        o.ext_d = -wo;
+        o.ext_f = tint;
+        o.ext_pdf = 1.f;
+        o.ext_cos = 1.f;
+    }
+}
+
+// Diffuse base under a GGX clear coat (no reference counterpart): the coat
+// reflects with Schlick Fresnel at the coat IOR, the base is Lambertian
+// weighted by (1 - F).  Continuation picks the coat lobe or the base with
+// equal probability; the pdf is the 50/50 mixture, as BRDF_pdf's.
+__device__ float3 coat_f(const ff_material& mat, float3 n, float3 wi, float3 wo, float r0)
+{
+    ff_material c = mat;
+    c.fresnel[0] = c.fresnel[1] = c.fresnel[2] = r0;
+    c.base_color[0] = c.base_color[1] = c.base_color[2] = 1.f;
+    c.metallic = 0.f;
+    const float3 spec = spec_f(c, n, wi, wo);
+    const float3 h = normalize3(wo + wi);
+    const float x = 1.f - hmax(0.f, dot3(h, wi));
+    const float F = r0 + (1.f - r0) * x * x * x * x * x;
+    const float3 a = make_float3(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
+    return spec + a * ((1.f - F) * FF_1_PI);
+}
+
+__device__ void shade_coat(const WF& w, const LightCtx& lc, const ff_material& mat, float3 pos, float3 n, float3 wo,
+                           float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
+{
+    (void)w;
+    const float eta = mat.ior > 0.f ? mat.ior : 1.5f;
+    const float r0 = ((eta - 1.f) / (eta + 1.f)) * ((eta - 1.f) / (eta + 1.f));
+    o.ray_spec = o.ray_diff = false;
+    o.c_nee = make_float3(0.f, 0.f, 0.f);
+    const float nd = dot3(n, wi);
+    const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+    if (nd > 0.f && lpdf > 0.f) o.c_nee = ((coat_f(mat, n, wi, wo, r0) * nd) * light_L(lc, wi)) / lpdf;
+    const float r = mat.roughness;
+    float3 dir;
+    if (ff_rand(key, dim_of(L, DIM_LOBE)) < 0.5f) {
+        dir = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
+    } else {
+        // cosine-weighted hemisphere (concentric disk lifted to the hemisphere)
+        const float2 dsk = concentric_disk(make_float2(ff_rand(key, dim_of(L, DIM_DIFF)),
+                                                       ff_rand(key, dim_of(L, DIM_DIFF + 1))));
+        const float z = sqrtf(hmax(0.f, 1.f - dsk.x * dsk.x - dsk.y * dsk.y));
+        float3 T, B;
+        frame(n, T, B);
+        dir = normalize3(T * dsk.x + B * dsk.y + n * z);
+    }
+    const float c = hmax(0.f, dot3(n, dir));
+    o.ext_d = dir;
+    o.ext_f = coat_f(mat, n, dir, wo, r0);
+    o.ext_pdf = 0.5f * spec_get_pdf(n, dir, wo, r) + 0.5f * c * FF_1_PI;
+    o.ext_cos = c;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(128) k_shade(WF w)
+{
+    const uint32_t n = w.ctr[C_MAT + KIND];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // every lane runs the same number of iterations so the queue appends can use full-warp ballots
+    const uint32_t iters = (n + stride - 1) / stride;
+    const uint32_t base = blockIdx.x * blockDim.x + threadIdx.x;
+    LightCtx lc;
+    lc.w = &w;
+    lc.is_env = w.light < 0;
+    if (!lc.is_env) lc.rect = make_rect(w.area[w.light]);
+    for (uint32_t it = 0; it < iters; ++it) {
+        const uint32_t qi = base + it * stride;
+        const bool valid = qi < n;
+        ShadeOut o;
+        o.ray_nee = o.ray_spec = o.ray_diff = false;
+        uint32_t s = 0;
+        if (valid) {
+            s = w.mat_queue[(size_t)KIND * w.P + qi];
+            const float4 hp = w.hit_pos[s];
+            const float3 pos = xyz(hp);
+            const ff_material mat = w.mats[__float_as_uint(hp.w)];
+            const float3 n = xyz(w.hit_nrm[s]);
+            const float3 wo = -xyz(w.ray_d[s]);
+            const float3 wi = xyz(w.light_wi[s]);
+            const float3 sp = xyz(w.light_sp[s]);
+            const uint32_t key = w.key[s];
+            const uint32_t L = w.length[s];
+            o.c_spec = o.c_diff = make_float3(0.f, 0.f, 0.f);
+            if (KIND == FF_MAT_MIX) shade_mix(w, lc, mat, pos, n, wo, wi, sp, key, L, o);
+            else if (KIND == FF_MAT_DIFFUSE) shade_diffuse(w, lc, mat, pos, n, wo, wi, key, L, o);
+            else if (KIND == FF_MAT_CONDUCTOR) shade_conductor(w, lc, mat, pos, n, wo, wi, key, L, o);
+            else if (KIND == FF_MAT_DIELECTRIC) shade_dielectric(w, lc, mat, pos, n, wo, wi, key, L, o);
+            else shade_coat(w, lc, mat, pos, n, wo, wi, key, L, o);
+            // NEE shadow ray of wf_shadow: light_ray = position + normal * SHADOW_OFFSET (kernel.cu:437)
+            const float3 lo = pos + n * w.shadow_offset;
+            o.ray_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, o.r_nee);
+            // continuation ray: the reference starts it at the hit point (kernel.cu:643)
+            o.ext_o = pos;
+            if (w.mode == FF_MODE_CORRECTED) {
+                const float side = dot3(o.ext_d, n) >= 0.f ? 1.f : -1.f;
+                o.ext_o = pos + n * (side * w.shadow_offset);
+            }
+            w.c_nee[s] = f4(o.c_nee);
+            w.c_spec[s] = f4(o.c_spec);
+            w.c_diff[s] = f4(o.c_diff);
+            w.ext_fp[s] = f4(o.ext_f, o.ext_pdf);
+            w.ext_cos[s] = o.ext_cos;
+            w.ray_o[s] = f4(o.ext_o);
+            w.ray_d[s] = f4(o.ext_d);
+        }
+        const uint32_t qe = warp_append(&w.ctr[C_EXT], valid, &w.totals[0]);
+        if (valid) {
+            w.ext_rays[qe] = make_ray(o.ext_o, o.ext_d, __int_as_float(0x7f800000));
+            w.ext_q[s] = (int32_t)qe;
+        }
+        const uint32_t q0 = warp_append(&w.ctr[C_SH], o.ray_nee, &w.totals[1]);
+        const uint32_t q1 = warp_append(&w.ctr[C_SH], o.ray_spec, &w.totals[1]);
+        const uint32_t q2 = warp_append(&w.ctr[C_SH], o.ray_diff, &w.totals[1]);
+        if (o.ray_nee) w.sh_rays[q0] = o.r_nee;
+        if (o.ray_spec) w.sh_rays[q1] = o.r_spec;
+        if (o.ray_diff) w.sh_rays[q2] = o.r_diff;
+        if (valid)
+            w.sh_q[s] = make_int4(o.ray_nee ? (int)q0 : SQ_BLOCKED, o.ray_spec ? (int)q1 : SQ_NONE,
+                                  o.ray_diff ? (int)q2 : SQ_NONE, 0);
+    }
+}
+
+__global__ void k_init(WF w, uint32_t spp, uint32_t sample_offset)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= w.P) return;
+    const uint32_t lane = s / w.WH;  // which of the m slots of its pixel
+    const uint32_t left = lane < spp ? (spp - lane + w.m - 1) / w.m : 0u;
+    w.samples_left[s] = left;
+    w.next_sample[s] = sample_offset + lane;
+    w.phase[s] = left ? PH_START : PH_DONE;
+    w.acc[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    w.acc_c[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    w.cnt[s] = 0;
+    w.sh_q[s] = make_int4(SQ_NONE, SQ_NONE, SQ_NONE, 0);
+}
+
+// Film += the m slot sums of each pixel, in slot order (compensated).
+__global__ void k_resolve(WF w, float4* __restrict__ film_acc, float4* __restrict__ film_c, uint32_t* __restrict__ film_n)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= w.WH) return;
+    float4 sum = film_acc[p], c = film_c[p];
+    uint32_t n = film_n[p];
+    for (uint32_t k = 0; k < w.m; ++k) {
+        const uint32_t s = p + k * w.WH;
+        const float4 a = w.acc[s], ac = w.acc_c[s];
+        kahan_add(sum, c, make_float3(a.x - ac.x, a.y - ac.y, a.z - ac.z));
+        n += w.cnt[s];
+    }
+    film_acc[p] = sum;
+    film_c[p] = c;
+    film_n[p] = n;
+}
+
+__global__ void k_reset_counters(uint32_t* ctr, unsigned long long* trace_counters)
+{
+    if (threadIdx.x < C_WORDS) ctr[threadIdx.x] = 0;
+    if (threadIdx.x < 2) trace_counters[threadIdx.x] = 0ull;
+}
+
+}  // namespace
+
+// Per-film workspace: slot arrays and queues, reused while the pool size is unchanged.
+struct FFWavefrontWS {
+    uint32_t P = 0;
+    DevBuf buf;
+    WF w{};
+    unsigned int* err = nullptr;
+    unsigned long long* trace_ctr = nullptr;  // [0] closest, [1] any
+    uint32_t* h_active = nullptr;             // pinned host word for the frame-loop check
+    ~FFWavefrontWS()
+    {
+        if (h_active) cudaFreeHost(h_active);
+    }
+};
+
+void ff_wavefront_ws_free(FFWavefrontWS* ws) { delete ws; }
+
+namespace {
+
+template <class T>
+T* carve(char*& p, size_t n)
+{
+    T* r = reinterpret_cast<T*>(p);
+    size_t bytes = (sizeof(T) * n + 255) & ~size_t(255);
+    p += bytes;
+    return r;
+}
+
+size_t ws_bytes(uint32_t P)
+{
+    size_t b = 0;
+    auto add = [&](size_t s, size_t n) { b += (s * n + 255) & ~size_t(255); };
+    add(4, P) /*samples_left*/; add(4, P); add(4, P); add(4, P); add(4, P);
+    add(16, P) /*beta*/; add(16, P); add(16, P); add(4, P); add(16, P);
+    add(16, P); add(16, P); add(16, P); add(16, P); add(4, P);
+    add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(4, P);
+    add(sizeof(ff_ray), P); add(sizeof(ff_hit), P); add(sizeof(ff_ray), 3ull * P); add(sizeof(ff_hit), 3ull * P);
+    add(4, (size_t)kKinds * P); add(4, 64); add(8, 8); add(4, 4); add(8, 4);
+    return b;
+}
+
+void ws_setup(FFWavefrontWS* ws, uint32_t P)
+{
+    if (ws->P == P && ws->buf.ptr) return;
+    ws->buf.release();
+    ws->buf.alloc(ws_bytes(P));
+    char* p = ws->buf.as<char>();
+    WF& w = ws->w;
+    w.P = P;
+    w.samples_left = carve<uint32_t>(p, P);
+    w.next_sample = carve<uint32_t>(p, P);
+    w.key = carve<uint32_t>(p, P);
+    w.length = carve<uint32_t>(p, P);
+    w.phase = carve<uint32_t>(p, P);
+    w.beta = carve<float4>(p, P);
+    w.ray_o = carve<float4>(p, P);
+    w.ray_d = carve<float4>(p, P);
+    w.ext_q = carve<int32_t>(p, P);
+    w.sh_q = carve<int4>(p, P);
+    w.c_nee = carve<float4>(p, P);
+    w.c_spec = carve<float4>(p, P);
+    w.c_diff = carve<float4>(p, P);
+    w.ext_fp = carve<float4>(p, P);
+    w.ext_cos = carve<float>(p, P);
+    w.hit_pos = carve<float4>(p, P);
+    w.hit_nrm = carve<float4>(p, P);
+    w.light_wi = carve<float4>(p, P);
+    w.light_sp = carve<float4>(p, P);
+    w.acc = carve<float4>(p, P);
+    w.acc_c = carve<float4>(p, P);
+    w.cnt = carve<uint32_t>(p, P);
+    w.ext_rays = carve<ff_ray>(p, P);
+    w.ext_hits = carve<ff_hit>(p, P);
+    w.sh_rays = carve<ff_ray>(p, 3ull * P);
+    w.sh_hits = carve<ff_hit>(p, 3ull * P);
+    w.mat_queue = carve<uint32_t>(p, (size_t)kKinds * P);
+    w.ctr = carve<uint32_t>(p, 64);
+    w.totals = carve<unsigned long long>(p, 8);
+    ws->err = carve<unsigned int>(p, 4);
+    ws->trace_ctr = carve<unsigned long long>(p, 4);
+    ws->P = P;
+}
+
+}  // namespace
+
+void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, ff_film* film,
+                         ff_render_stats* stats)
+{
+    FF_REQUIRE(st->spp > 0, "spp must be > 0");
+    FF_REQUIRE(st->max_depth >= 1 && st->max_depth <= 64, "max_depth must be in [1, 64]");
+    FF_REQUIRE(st->mode == FF_MODE_PARITY || st->mode == FF_MODE_CORRECTED, "unknown mode");
+    if (st->light < 0) {
+        FF_REQUIRE(scene->env.width > 0, "light -1 (environment) needs an environment map");
+    } else {
+        FF_REQUIRE((uint32_t)st->light < scene->num_area_lights, "light index out of range");
+    }
+    cudaStream_t stream = ctx->stream;
+    const uint32_t WH = film->width * film->height;
+    const uint64_t target = st->max_paths ? st->max_paths : (1u << 21);
+    uint32_t m = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(st->spp, target / WH));
+    while ((uint64_t)m * WH > (1ull << 31)) --m;
+    const uint32_t P = m * WH;
+    if (!film->ws) film->ws = new FFWavefrontWS();
+    FFWavefrontWS* ws = film->ws;
+    ws_setup(ws, P);
+    WF& w = ws->w;
+    w.WH = WH;
+    w.W = film->width;
+    w.H = film->height;
+    w.m = m;
+    w.seed = st->seed;
+    w.max_depth = st->max_depth;
+    w.rr_depth = st->rr_depth;
+    w.mode = st->mode;
+    w.light = st->light;
+    w.shadow_offset = st->shadow_offset > 0.f ? st->shadow_offset : 0.001f;
+    w.shade = scene->shade.as<FFShadeTri>();
+    w.mats = scene->materials.as<ff_material>();
+    w.area = scene->area_lights.as<ff_area_light>();
+    w.n_area = scene->num_area_lights;
+    w.env.rgb = scene->env.rgb.as<float3>();
+    w.env.marginal = scene->env.marginal.as<double>();
+    w.env.cond = scene->env.conditional.as<double>();
+    w.env.pdf = scene->env.pdf.as<float>();
+    w.env.width = scene->env.width;
+    w.env.height = scene->env.height;
+    w.env.color = scene->env.color;
+    w.env.radius = 10000.f;
+    w.cam = scene->camera;
+    const FFBvhView bvh = scene->view();
+
+    // which material kinds occur
+    std::vector<ff_material> mats(scene->num_materials);
+    FF_CUDA_CHECK(cudaMemcpyAsync(mats.data(), scene->materials.ptr, sizeof(ff_material) * mats.size(),
+                                  cudaMemcpyDeviceToHost, stream));
+    FF_CUDA_CHECK(cudaMemsetAsync(w.totals, 0, 8 * sizeof(unsigned long long), stream));
+    FF_CUDA_CHECK(cudaMemsetAsync(ws->err, 0, sizeof(unsigned int), stream));
+    FF_CUDA_CHECK(cudaStreamSynchronize(stream));
+    bool kind_used[kKinds] = {false, false, false, false, false};
+    for (auto& mt : mats) kind_used[mt.kind] = true;
+
+    FF_CUDA_CHECK(cudaEventRecord(ctx->ev0, stream));
+    k_init<<<(P + 255) / 256, 256, 0, stream>>>(w, st->spp, st->sample_offset);
+    FF_CUDA_CHECK(cudaGetLastError());
+    int shade_blocks = ctx->num_sms * 8;
+    uint32_t frames = 0;
+    uint32_t active = 1;
+    if (!ws->h_active) FF_CUDA_CHECK(cudaMallocHost(&ws->h_active, sizeof(uint32_t)));
+    uint32_t* h_active = ws->h_active;
+    const uint32_t max_frames = (st->spp + 1) * (st->max_depth + 2) + 8;
+    while (active && frames < max_frames) {
+        // a batch of frames between host checks
+        for (int b = 0; b < 4; ++b) {
+            k_reset_counters<<<1, 32, 0, stream>>>(w.ctr, ws->trace_ctr);
+            k_logic<<<(P + 255) / 256, 256, 0, stream>>>(w);
+            if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX><<<shade_blocks, 128, 0, stream>>>(w);
+            if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE><<<shade_blocks, 128, 0, stream>>>(w);
+            if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR><<<shade_blocks, 128, 0, stream>>>(w);
+            if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC><<<shade_blocks, 128, 0, stream>>>(w);
+            if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT><<<shade_blocks, 128, 0, stream>>>(w);
+            FF_CUDA_CHECK(cudaGetLastError());
+            ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err);
+            ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, w.sh_hits, true, ws->trace_ctr + 1,
+                                  ws->err);
+            ++frames;
+        }
+        FF_CUDA_CHECK(cudaMemcpyAsync(h_active, w.ctr + C_ACTIVE, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        FF_CUDA_CHECK(cudaStreamSynchronize(stream));
+        active = *h_active;
+    }
+    if (active) throw FFError{FF_ERR_INTERNAL, "wavefront did not finish within its frame bound"};
+    k_resolve<<<(WH + 255) / 256, 256, 0, stream>>>(w, film->accum.as<float4>(), film->comp.as<float4>(),
+                                                   film->count.as<uint32_t>());
+    FF_CUDA_CHECK(cudaGetLastError());
+    FF_CUDA_CHECK(cudaEventRecord(ctx->ev1, stream));
+    unsigned long long totals[3] = {0, 0, 0};
+    unsigned int err = 0;
+    FF_CUDA_CHECK(cudaMemcpyAsync(totals, w.totals, sizeof(totals), cudaMemcpyDeviceToHost, stream));
+    FF_CUDA_CHECK(cudaMemcpyAsync(&err, ws->err, sizeof(err), cudaMemcpyDeviceToHost, stream));
+    FF_CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (err) throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        stats->extension_rays = totals[0];
+        stats->shadow_rays = totals[1];
+        stats->samples = (uint64_t)st->spp * WH;
+        stats->frames = frames;
+        stats->ms_total = ms;
+    }
 }

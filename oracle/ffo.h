@@ -48,8 +48,50 @@ float ffo_rand(uint32_t key, uint32_t dim);
 /* Per-(pixel, sample) stream key. */
 uint32_t ffo_path_key(uint32_t seed, uint32_t pixel, uint32_t sample);
 
-/* ---- CPU render (restated wavefront stages) ---- */
-typedef struct ffo_scene ffo_scene;
+/* ---- CPU render (restated wavefront stages, ffo_render.c) ---- */
+typedef struct {
+    float base_color[3];
+    float fresnel[3];
+    float roughness;
+    float metallic;
+    int32_t kind;          /* 0 mix (wf_mat_mix), 1 diffuse (wf_mat_diffuse), 2 conductor (wf_mat_cook) */
+} ffo_material;
+
+typedef struct {
+    float p0[3], a[3], b[3], normal[3];
+    float emissive[3];
+    float radiance;
+} ffo_area_light;
+
+typedef struct {
+    const float* tris;          /* num_tris x 9: v0 v1 v2 */
+    const float* normals;       /* num_tris x 9: vertex normals n0 n1 n2 */
+    const uint32_t* material_ids;
+    int32_t num_tris;
+    const ffo_material* materials;
+    int32_t num_materials;
+    const ffo_area_light* area_lights;
+    int32_t num_area_lights;
+    const float* env_rgb;       /* env_h x env_w x 3, or NULL (constant env_color) */
+    int32_t env_w, env_h;
+    float env_color[3];
+    float cam_inv[16];          /* Matrix4x4 m[i][j] at 4*i + j */
+    float cam_lens_radius, cam_focal, cam_jitter;
+    int32_t width, height, spp, sample_offset, max_depth, rr_depth;
+    uint32_t seed;
+    int32_t mode;               /* 0 parity, 1 corrected */
+    int32_t light;              /* -1 environment, k area light k */
+    float shadow_offset;
+    int32_t threads;
+} ffo_render_desc;
+
+/* Renders every pixel's spp samples; out_rgb (width*height*3 doubles) gets
+ * the per-pixel radiance sums.  stats[0..1] = extension and shadow rays.
+ * Returns 0, or 1 for an invalid light selection. */
+int ffo_render(const ffo_render_desc* d, double* out_rgb, uint64_t* stats);
+
+/* Environment tables of kernel.cu:65-149 (marginal[h], cond[h*w], pdf[h*w]). */
+void ffo_env_build(const float* rgb, int w, int h, double* marginal, double* cond, float* pdf, double* denom);
 
 #ifdef __cplusplus
 }

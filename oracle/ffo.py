@@ -81,3 +81,93 @@ def shadow_hit(v0, v1, v2, o, d):
     t = C.c_float(0)
     ok = lib.ffo_shadow_hit(*[_p(a) for a in arrs], C.byref(t))
     return ok, t.value
+
+
+# ------------------------------------------------------------------ render
+class ffo_material(C.Structure):
+    _fields_ = [("base_color", C.c_float * 3), ("fresnel", C.c_float * 3), ("roughness", C.c_float),
+                ("metallic", C.c_float), ("kind", C.c_int32)]
+
+
+class ffo_area_light(C.Structure):
+    _fields_ = [("p0", C.c_float * 3), ("a", C.c_float * 3), ("b", C.c_float * 3), ("normal", C.c_float * 3),
+                ("emissive", C.c_float * 3), ("radiance", C.c_float)]
+
+
+class ffo_render_desc(C.Structure):
+    _fields_ = [("tris", C.c_void_p), ("normals", C.c_void_p), ("material_ids", C.c_void_p),
+                ("num_tris", C.c_int32), ("materials", C.c_void_p), ("num_materials", C.c_int32),
+                ("area_lights", C.c_void_p), ("num_area_lights", C.c_int32),
+                ("env_rgb", C.c_void_p), ("env_w", C.c_int32), ("env_h", C.c_int32), ("env_color", C.c_float * 3),
+                ("cam_inv", C.c_float * 16), ("cam_lens_radius", C.c_float), ("cam_focal", C.c_float),
+                ("cam_jitter", C.c_float), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
+                ("sample_offset", C.c_int32), ("max_depth", C.c_int32), ("rr_depth", C.c_int32),
+                ("seed", C.c_uint32), ("mode", C.c_int32), ("light", C.c_int32), ("shadow_offset", C.c_float),
+                ("threads", C.c_int32)]
+
+
+def render(scene, width, height, spp, max_depth=3, rr_depth=3, seed=0, mode=0, light=-1, sample_offset=0,
+           shadow_offset=0.001, threads=None):
+    """Oracle render: per-pixel radiance SUMS (height x width x 3, float64) and
+    (extension rays, shadow rays)."""
+    lib = load()
+    lib.ffo_render.restype = C.c_int
+    lib.ffo_render.argtypes = [C.POINTER(ffo_render_desc), C.c_void_p, C.c_void_p]
+    tris = scene.triangle_soup()
+    if scene.normals is None:
+        raise ValueError("oracle render needs per-vertex normals")
+    nrm = np.ascontiguousarray(scene.normals[scene.indices].reshape(-1, 9), np.float32)
+    mids = None if scene.material_ids is None else np.ascontiguousarray(scene.material_ids, np.uint32)
+    mats = (ffo_material * max(1, len(scene.materials)))()
+    for i, m in enumerate(scene.materials):
+        for k in range(3):
+            mats[i].base_color[k] = m.base_color[k]
+            mats[i].fresnel[k] = m.fresnel[k]
+        mats[i].roughness, mats[i].metallic, mats[i].kind = m.roughness, m.metallic, m.kind
+    lights = (ffo_area_light * max(1, len(scene.area_lights)))()
+    for i, L in enumerate(scene.area_lights):
+        for f in ("p0", "a", "b", "normal", "emissive"):
+            for k in range(3):
+                getattr(lights[i], f)[k] = getattr(L, f)[k]
+        lights[i].radiance = L.radiance
+    env = None if scene.env_rgb is None else np.ascontiguousarray(scene.env_rgb, np.float32)
+    d = ffo_render_desc()
+    d.tris, d.normals = tris.ctypes.data, nrm.ctypes.data
+    d.material_ids = None if mids is None else mids.ctypes.data
+    d.num_tris = len(tris)
+    d.materials, d.num_materials = C.cast(mats, C.c_void_p), len(scene.materials)
+    d.area_lights, d.num_area_lights = C.cast(lights, C.c_void_p), len(scene.area_lights)
+    d.env_rgb = None if env is None else env.ctypes.data
+    d.env_w = 0 if env is None else env.shape[1]
+    d.env_h = 0 if env is None else env.shape[0]
+    for k in range(3):
+        d.env_color[k] = scene.env_color[k]
+    cam = scene.camera
+    for k in range(16):
+        d.cam_inv[k] = cam.inv_view_proj[k]
+    d.cam_lens_radius, d.cam_focal, d.cam_jitter = cam.lens_radius, cam.focal_distance, cam.pixel_jitter
+    d.width, d.height, d.spp, d.sample_offset = width, height, spp, sample_offset
+    d.max_depth, d.rr_depth, d.seed, d.mode, d.light = max_depth, rr_depth, seed, mode, light
+    d.shadow_offset = shadow_offset
+    d.threads = threads or os.cpu_count() or 1
+    out = np.zeros((height, width, 3), np.float64)
+    stats = np.zeros(2, np.uint64)
+    rc = lib.ffo_render(C.byref(d), out.ctypes.data, stats.ctypes.data)
+    if rc != 0:
+        raise ValueError("oracle render: invalid light selection")
+    return out, (int(stats[0]), int(stats[1]))
+
+
+def env_build(rgb: np.ndarray):
+    """Environment tables of the reference (marginal, conditional, pdf, denom)."""
+    lib = load()
+    lib.ffo_env_build.restype = None
+    lib.ffo_env_build.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    marginal = np.zeros(h, np.float64)
+    cond = np.zeros((h, w), np.float64)
+    pdf = np.zeros((h, w), np.float32)
+    denom = np.zeros(1, np.float64)
+    lib.ffo_env_build(rgb.ctypes.data, w, h, marginal.ctypes.data, cond.ctypes.data, pdf.ctypes.data, denom.ctypes.data)
+    return marginal, cond, pdf, float(denom[0])

@@ -1,0 +1,699 @@
+/*
+ * ffo_render.c — CPU restatement of the reference's wavefront path tracer,
+ * one path sample at a time.  TEST INFRASTRUCTURE ONLY (see ffo.h).
+ * Compile with -ffp-contract=off.
+ *
+ * Follows CUDA-RayTracer/:
+ *   wf_logic      kernel.cu:298-455   wf_generate  kernel.cu:458-485
+ *   wf_extend     kernel.cu:488-523   wf_shadow    kernel.cu:526-543
+ *   wf_mat_mix    kernel.cu:617-651   BRDF_L / BRDF_f / BRDF_pdf dMaterial.cu:363-469
+ *   wf_mat_diffuse kernel.cu:546-577  wf_mat_cook  kernel.cu:580-614
+ *   lobes         dMaterial.cu:90-313 lights dEnvironmentLight.cu:41-103, dAreaLight.cu:18-68,
+ *                                      Rectangle.cuh:74-123
+ *   camera        dCamera.cu:10-36    sampler warps dRandom.cu:49-126
+ *   env tables    kernel.cu:65-149    upper_bound Helpers.cu:16-31
+ * with the reference's clock-seeded random() replaced by the seeded
+ * per-(pixel, sample) stream ffo_rand(key, 32 * bounce + site): one fixed
+ * dimension per call site (sites listed in ffo.h), x of a make_float2
+ * (random(), random()) pair taking the second draw of the pair.
+ * Intersections are brute force over all triangles (ffo_trace.c).
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ffo.h"
+
+#define K_EPS 1e-6f
+#define K_HUGE 1e32f
+#define PI_F 3.14159265358979323846f
+#define TWO_PI_F 6.28318530717958647692f
+#define PI_2_F 1.57079632679489661923f
+#define PI_4_F 0.785398163397448309615f
+#define INV_PI_F 0.318309886183790671537f
+#define INV_2PI_F 0.159154943091895335768f
+
+typedef struct { float x, y, z; } v3;
+
+static inline v3 V(float x, float y, float z) { v3 r = {x, y, z}; return r; }
+static inline v3 add(v3 a, v3 b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 sub(v3 a, v3 b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 neg(v3 a) { return V(-a.x, -a.y, -a.z); }
+static inline v3 mul(v3 a, v3 b) { return V(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline v3 muls(v3 a, float s) { return V(a.x * s, a.y * s, a.z * s); }
+static inline v3 smul(float s, v3 a) { return V(s * a.x, s * a.y, s * a.z); }
+static inline v3 divs(v3 a, float s) { return V(a.x / s, a.y / s, a.z / s); }
+static inline v3 ssub(float s, v3 a) { return V(s - a.x, s - a.y, s - a.z); }
+static inline int iszero(v3 a) { return a.x == 0.f && a.y == 0.f && a.z == 0.f; }
+static inline float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline v3 cross(v3 a, v3 b) { return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+/* normalize: v * rsqrtf(dot(v,v)), host rsqrtf = 1.0f / sqrtf (dMath.cuh:70-73, 1300-1304) */
+static inline v3 normalize(v3 v) { float inv = 1.0f / sqrtf(dot(v, v)); return muls(v, inv); }
+static inline float length(v3 v) { return sqrtf(dot(v, v)); }
+/* reflect (dMath.cuh:1402) */
+static inline v3 reflect(v3 i, v3 n) { return sub(i, muls(smul(2.0f, n), dot(n, i))); }
+/* host fminf/fmaxf of dMath.cuh:40-48 */
+static inline float hmin(float a, float b) { return a < b ? a : b; }
+static inline float hmax(float a, float b) { return a > b ? a : b; }
+static inline float clampf_(float f, float a, float b) { return hmax(a, hmin(f, b)); }
+static inline v3 lerp3(v3 a, v3 b, float w) { return add(muls(a, 1.f - w), muls(b, w)); }
+static inline double sq(double x) { return x * x; }
+static inline double pow5(double x) { double x2 = x * x; return x2 * x2 * x; }
+static inline v3 ld3(const float* p) { return V(p[0], p[1], p[2]); }
+
+/* ----------------------------------------------------------- sampler */
+enum {
+    DIM_CAM_JITTER = 0, DIM_CAM_LENS = 2, DIM_LIGHT = 4, DIM_NEE_PDF = 6, DIM_SPEC = 8, DIM_DIFF = 10,
+    DIM_SPEC_VIS = 12, DIM_SPEC_PDF = 14, DIM_DIFF_VIS = 16, DIM_DIFF_PDF = 18, DIM_LOBE = 20,
+    DIM_NEE_VIS = 21, DIM_RR = 23, DIM_EXTRA = 24
+};
+static inline float R(uint32_t key, uint32_t b, uint32_t d) { return ffo_rand(key, 32u * b + d); }
+typedef struct { float x, y; } v2;
+static inline v2 R2(uint32_t key, uint32_t b, uint32_t d)
+{
+    float first = R(key, b, d), second = R(key, b, d + 1);
+    v2 r = {second, first};
+    return r;
+}
+
+static v3 orthogonal_axis(v3 in)
+{
+    if (fabsf(in.x) < 0.57735026919f) return V(1, 0, 0);
+    if (fabsf(in.y) < 0.57735026919f) return V(0, 1, 0);
+    return V(0, 0, 1);
+}
+static void frame(v3 N, v3* T, v3* B)
+{
+    *T = normalize(cross(N, orthogonal_axis(N)));
+    *B = normalize(cross(N, *T));
+}
+static v2 spherical_map(v3 d)
+{
+    v2 uv = {atan2f(d.z, d.x), asinf(d.y)};
+    uv.x = uv.x * INV_2PI_F;
+    uv.y = uv.y * INV_PI_F;
+    uv.x = uv.x + 0.5f;
+    uv.y = uv.y + 0.5f;
+    return uv;
+}
+static v3 spherical_direction(v2 uv)
+{
+    float theta = TWO_PI_F * uv.x, phi = PI_F * uv.y;
+    float x = cosf(theta) * sinf(phi), y = cosf(phi), z = sinf(theta) * sinf(phi);
+    return V(-x, -y, -z);
+}
+static v2 concentric_disk(v2 u)
+{
+    v2 o = {2.f * u.x - 1.f, 2.f * u.y - 1.f};
+    v2 zero = {0, 0};
+    if (o.x == 0 && o.y == 0) return zero;
+    float theta, r;
+    if (fabsf(o.x) > fabsf(o.y)) { r = o.x; theta = PI_4_F * (o.y / o.x); }
+    else { r = o.y; theta = PI_2_F - PI_4_F * (o.x / o.y); }
+    v2 out = {r * cosf(theta), r * sinf(theta)};
+    return out;
+}
+
+/* ---------------------------------------------------------- materials */
+static double diff_get_pdf(void) { return (double)(1.f / (2.f * PI_F)); }
+static v3 fresnel3(v3 f0, v3 h, v3 wo)
+{
+    float x = 1.f - hmax(0.f, dot(h, wo));
+    float p = (float)pow5((double)x);
+    return add(f0, muls(ssub(1.f, f0), p));
+}
+static double ggx_ndf(v3 n, v3 h, float r)
+{
+    double a2 = r * r * r * r;
+    double nh2 = sq((double)hmax(0.f, dot(n, h)));
+    return a2 / ((double)PI_F * sq(nh2 * (a2 - 1.0) + 1.0));
+}
+static double geo_atten(v3 wi, v3 wo, v3 n, float r)
+{
+    float rp = r + 1.f;
+    double k = (double)((rp * rp) / 8.f);
+    double nl = hmax(dot(n, wi), 0.f), nv = hmax(dot(n, wo), 0.f);
+    double g1 = nl / (nl * (1.0 - k) + k), g2 = nv / (nv * (1.0 - k) + k);
+    return g1 * g2;
+}
+static double power_heuristic(double f, double g) { return (f * f) / (f * f + g * g); }
+static v3 f0_of(const ffo_material* m, v3 a) { return lerp3(ld3(m->fresnel), a, m->metallic); }
+static v3 diff_f(const ffo_material* mat, v3 wi, v3 wo)
+{
+    float m = mat->metallic;
+    v3 a = ld3(mat->base_color);
+    v3 f0 = f0_of(mat, a);
+    v3 wh = normalize(add(wo, wi));
+    v3 F = fresnel3(f0, wh, wi);
+    v3 kd = sub(V(1.f, 1.f, 1.f), F);
+    kd = muls(kd, (float)(1.0 - (double)m));
+    return muls(mul(kd, a), INV_PI_F);
+}
+static float spec_get_pdf(v3 n, v3 wi, v3 wo, float r)
+{
+    v3 wh = normalize(add(wo, wi));
+    double whn = hmax(dot(wh, n), 0.f), wowh = hmax(dot(wo, wh), 0.f);
+    double D = ggx_ndf(n, wh, r);
+    return (float)((D * whn) / (double)hmax((float)(4.0 * wowh), 0.001f));
+}
+static v3 spec_f(const ffo_material* mat, v3 n, v3 wi, v3 wo)
+{
+    float r = mat->roughness;
+    v3 a = ld3(mat->base_color);
+    v3 f0 = f0_of(mat, a);
+    v3 wh = normalize(add(wo, wi));
+    double ndwi = hmax(dot(n, wi), 0.f), ndwo = hmax(dot(n, wo), 0.f);
+    double D = ggx_ndf(n, wh, r), G = geo_atten(wi, wo, n, r);
+    v3 F = fresnel3(f0, wh, wi);
+    v3 num = smul((float)(D * G), F);
+    return divs(num, hmax((float)(4.0 * ndwo * ndwi), 0.001f));
+}
+static v3 diff_sample(v3 N, float e0, float e1)
+{
+    float st = sqrtf(1.f - e0 * e0), phi = 2.f * PI_F * e1;
+    float x = st * cosf(phi), z = st * sinf(phi);
+    v3 T, B;
+    frame(N, &T, &B);
+    return normalize(add(add(muls(T, x), muls(N, e0)), muls(B, z)));
+}
+static v3 spec_sample(v3 N, v3 wo, float r, float e0, float e1)
+{
+    double theta = (double)atanf(r * r * sqrtf(e0 / (1.f - e0)));
+    double phi = (double)(2 * PI_F * e1);
+    v3 h = V((float)(sin(theta) * cos(phi)), (float)cos(theta), (float)(sin(theta) * sin(phi)));
+    v3 T, B;
+    frame(N, &T, &B);
+    v3 s = add(add(muls(T, h.x), muls(N, h.y)), muls(B, h.z));
+    return neg(reflect(wo, normalize(s)));
+}
+static v3 brdf_f(const ffo_material* m, v3 n, v3 wi, v3 wo) { return add(spec_f(m, n, wi, wo), diff_f(m, wi, wo)); }
+static float brdf_pdf(const ffo_material* m, v3 n, v3 wi, v3 wo)
+{
+    float sp = spec_get_pdf(n, wi, wo, m->roughness);
+    float dp = (float)diff_get_pdf();
+    return (float)(0.5 * (double)(sp + dp));
+}
+
+/* ------------------------------------------------------------- lights */
+/* luminance (dMath.cuh:1503-1507): double arithmetic, float result */
+static float luminance(v3 c) { return (float)(0.299 * (double)c.x + 0.587 * (double)c.y + 0.114 * (double)c.z); }
+
+/* tex2DLod, linear filter, wrap, normalised coords, 8 fractional weight bits */
+static v3 tex_bilinear(const float* rgb, int w, int h, float u, float v)
+{
+    float xb = u * (float)w - 0.5f, yb = v * (float)h - 0.5f;
+    float fx = floorf(xb), fy = floorf(yb);
+    float ax = xb - fx, ay = yb - fy;
+    ax = floorf(ax * 256.f + 0.5f) / 256.f;
+    ay = floorf(ay * 256.f + 0.5f) / 256.f;
+    int ix = (int)fx, iy = (int)fy;
+    int x0 = ix % w; x0 = x0 < 0 ? x0 + w : x0;
+    int x1 = (x0 + 1 == w) ? 0 : x0 + 1;
+    int y0 = iy % h; y0 = y0 < 0 ? y0 + h : y0;
+    int y1 = (y0 + 1 == h) ? 0 : y0 + 1;
+    const float *t00 = rgb + 3 * (y0 * w + x0), *t10 = rgb + 3 * (y0 * w + x1);
+    const float *t01 = rgb + 3 * (y1 * w + x0), *t11 = rgb + 3 * (y1 * w + x1);
+    float w00 = (1.f - ax) * (1.f - ay), w10 = ax * (1.f - ay), w01 = (1.f - ax) * ay, w11 = ax * ay;
+    return V(w00 * t00[0] + w10 * t10[0] + w01 * t01[0] + w11 * t11[0],
+             w00 * t00[1] + w10 * t10[1] + w01 * t01[1] + w11 * t11[1],
+             w00 * t00[2] + w10 * t10[2] + w01 * t01[2] + w11 * t11[2]);
+}
+
+static int upper_bound_ref(const double* list, int size, float val)
+{
+    int left = 0, right = size;
+    while (left < right) {
+        int middle = (right - left) / 2 + left;
+        if ((double)val >= list[middle]) left = middle + 1;
+        else right = middle;
+    }
+    if (left < size && list[(left <= val) ? 1 : 0] != 0.0) left++;
+    return left;
+}
+
+/* The serial table build of kernel.cu:65-149 over the emulated texture. */
+void ffo_env_build(const float* rgb, int w, int h, double* marginal, double* cond, float* pdf, double* denom_out)
+{
+    double denom = 0.0;
+    for (int j = 0; j < h; j++) {
+        float v = (float)j / (float)h;
+        double st = (double)sinf(PI_F * v);
+        for (int i = 0; i < w; i++) {
+            float u = (float)i / (float)w;
+            double lum = luminance(tex_bilinear(rgb, w, h, u, v));
+            denom += lum * st;
+        }
+    }
+    double* mp = (double*)malloc(sizeof(double) * (size_t)h);
+    for (int j = 0; j < h; j++) {
+        float v = (float)j / (float)h;
+        double st = (double)sinf(PI_F * v) / denom;
+        mp[j] = 0.f;
+        for (int i = 0; i < w; i++) {
+            float u = (float)i / (float)w;
+            double lum = luminance(tex_bilinear(rgb, w, h, u, v));
+            mp[j] += lum * st;
+        }
+        marginal[j] = j ? mp[j] + marginal[j - 1] : mp[j];
+    }
+    for (int y = 0; y < h; y++) {
+        float v = (float)y / (float)h;
+        double st = (double)sinf(PI_F * v);
+        double val = st / (denom * mp[y]);
+        double* row = cond + (size_t)y * w;
+        for (int x = 0; x < w; x++) {
+            float u = (float)x / (float)w;
+            double lum = luminance(tex_bilinear(rgb, w, h, u, v));
+            row[x] = lum * val;
+            if (x) row[x] += row[x - 1];
+        }
+    }
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            float u = (float)x / (float)w, v = (float)y / (float)h;
+            double st = (double)sinf(PI_F * v);
+            double lum = luminance(tex_bilinear(rgb, w, h, u, v));
+            float p = (float)((lum * st) / denom);
+            p *= (float)(w * h) / (2.f * PI_F * PI_F);
+            pdf[(size_t)y * w + x] = p;
+        }
+    if (denom_out) *denom_out = denom;
+    free(mp);
+}
+
+typedef struct { v3 p0, a, b, n; float a_len2, b_len2, inv_area; v3 Le; } rect_t;
+
+static rect_t make_rect(const ffo_area_light* L)
+{
+    rect_t r;
+    r.p0 = ld3(L->p0); r.a = ld3(L->a); r.b = ld3(L->b); r.n = ld3(L->normal);
+    float la = length(r.a), lb = length(r.b);
+    r.a_len2 = la * la;
+    r.b_len2 = lb * lb;
+    r.inv_area = 1.f / (la * lb);
+    r.Le = smul(L->radiance, ld3(L->emissive));
+    return r;
+}
+static v3 rect_sample(const rect_t* r, v2 u) { return add(add(r->p0, smul(u.x, r->a)), smul(u.y, r->b)); }
+static int rect_hit(const rect_t* r, v3 o, v3 d)
+{
+    float t = dot(sub(r->p0, o), r->n) / dot(d, r->n);
+    v3 p = add(o, smul(t, d));
+    v3 p0p = sub(p, r->p0);
+    if (t <= K_EPS) return 0;
+    float pa = dot(p0p, r->a);
+    if (pa < 0.0f || pa > r->a_len2) return 0;
+    float pb = dot(p0p, r->b);
+    if (pb < 0.0f || pb > r->b_len2) return 0;
+    return 1;
+}
+static v3 rect_L(const rect_t* r, v3 wi) { return dot(neg(r->n), wi) > 0.0f ? r->Le : V(0, 0, 0); }
+static float rect_pdf(const rect_t* r, v3 pos, v2 u)
+{
+    v3 sp = rect_sample(r, u);
+    v3 w = normalize(sub(sp, pos));
+    float nd = fabsf(dot(r->n, neg(w)));
+    float dist = length(sub(sp, pos));
+    float d2 = dist * dist;
+    return (d2 / nd) * r->inv_area;
+}
+
+typedef struct {
+    const ffo_render_desc* d;
+    int is_env;
+    rect_t rect;
+    const double* marginal;
+    const double* cond;
+    const float* pdf;
+} light_ctx;
+
+static v3 env_L(const ffo_render_desc* d, v3 wi)
+{
+    if (!d->env_rgb) return ld3(d->env_color);
+    v2 uv = spherical_map(wi);
+    return tex_bilinear(d->env_rgb, d->env_w, d->env_h, uv.x, uv.y);
+}
+static float env_pdf(const light_ctx* lc, v3 wi)
+{
+    const ffo_render_desc* d = lc->d;
+    v2 uv = spherical_map(wi);
+    int x = (int)(uv.x * (float)(d->env_w - 1)), y = (int)(uv.y * (float)(d->env_h - 1));
+    float p = (x >= 0 && y >= 0 && x < d->env_w && y < d->env_h) ? lc->pdf[(size_t)y * d->env_w + x] : 0.f;
+    return p / sinf(acosf(clampf_(wi.z, -1.f, 1.f)));
+}
+static void env_sample(const light_ctx* lc, v3 pos, float ex, float ey, v3* wi, v3* sp)
+{
+    const ffo_render_desc* d = lc->d;
+    int y = (int)((float)upper_bound_ref(lc->marginal, d->env_h, ey) - 1.f);
+    y = y < 0 ? 0 : (y >= d->env_h ? d->env_h - 1 : y);
+    int x = (int)((float)upper_bound_ref(lc->cond + (size_t)y * d->env_w, d->env_w, ex) - 1.f);
+    x = x < 0 ? 0 : (x >= d->env_w ? d->env_w - 1 : x);
+    v2 uv = {(float)x / (float)d->env_w, (float)y / (float)d->env_h};
+    v3 dir = spherical_direction(uv);
+    *sp = add(V(0.f, 0.f, 0.f), muls(dir, 10000.f));
+    *wi = normalize(sub(*sp, pos));
+}
+static v3 light_L(const light_ctx* lc, v3 wi) { return lc->is_env ? env_L(lc->d, wi) : rect_L(&lc->rect, wi); }
+static float light_pdf(const light_ctx* lc, v3 pos, v3 wi, uint32_t key, uint32_t L, uint32_t dim)
+{
+    return lc->is_env ? env_pdf(lc, wi) : rect_pdf(&lc->rect, pos, R2(key, L, dim));
+}
+
+typedef struct { v3 o, d; float tmax; } ray_t;
+
+static int light_vis_ray(const light_ctx* lc, v3 o, v3 d, uint32_t key, uint32_t L, uint32_t dim, ray_t* out)
+{
+    if (lc->is_env) { out->o = o; out->d = d; out->tmax = K_HUGE; return 1; }
+    if (!rect_hit(&lc->rect, o, d)) return 0;
+    float ts = dot(sub(rect_sample(&lc->rect, R2(key, L, dim)), o), d);
+    out->o = o; out->d = d; out->tmax = ts;
+    return 1;
+}
+
+/* ------------------------------------------------------------- tracing */
+static int closest(const ffo_render_desc* d, v3 o, v3 dir, float* t_out, float* u_out, float* v_out)
+{
+    float best = K_HUGE, bu = 0, bv = 0;
+    int prim = -1;
+    const float oo[3] = {o.x, o.y, o.z}, dd[3] = {dir.x, dir.y, dir.z};
+    for (int i = 0; i < d->num_tris; ++i) {
+        const float* tri = d->tris + 9 * (size_t)i;
+        float t, u, v;
+        if (ffo_intersect_cull(tri, tri + 3, tri + 6, oo, dd, &t, &u, &v) && !(t < 0) && t < best) {
+            best = t; bu = u; bv = v; prim = i;
+        }
+    }
+    *t_out = best; *u_out = bu; *v_out = bv;
+    return prim;
+}
+static int occluded(const ffo_render_desc* d, const ray_t* r)
+{
+    const float oo[3] = {r->o.x, r->o.y, r->o.z}, dd[3] = {r->d.x, r->d.y, r->d.z};
+    for (int i = 0; i < d->num_tris; ++i) {
+        const float* tri = d->tris + 9 * (size_t)i;
+        float t;
+        if (ffo_shadow_hit(tri, tri + 3, tri + 6, oo, dd, &t) && t >= 0.f && t < r->tmax) return 1;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------- shading */
+typedef struct {
+    v3 c_nee, c_spec, c_diff;
+    int has_nee, has_spec, has_diff;
+    ray_t r_nee, r_spec, r_diff;
+    v3 ext_o, ext_d, ext_f;
+    float ext_pdf, ext_cos;
+} shade_t;
+
+static void shade_mix(const light_ctx* lc, int corrected, const ffo_material* mat, v3 pos, v3 n, v3 wo, v3 wi,
+                      uint32_t key, uint32_t L, shade_t* o)
+{
+    float r = mat->roughness;
+    v3 Lsum = V(0, 0, 0);
+    v3 Li = light_L(lc, wi);
+    float ndwi = dot(n, wi);
+    if (ndwi > 0.f) {
+        double dp = diff_get_pdf();
+        double sp = spec_get_pdf(n, wi, wo, r);
+        double lp = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+        if (lp > 0.f && !iszero(Li)) {
+            double dw = power_heuristic(lp, dp), sw = power_heuristic(lp, sp);
+            v3 f = muls(spec_f(mat, n, wi, wo), ndwi);
+            if (!iszero(f)) Lsum = add(Lsum, divs(mul(muls(f, (float)sw), Li), (float)lp));
+            f = muls(diff_f(mat, wi, wo), ndwi);
+            if (!iszero(f)) Lsum = add(Lsum, divs(mul(muls(f, (float)dw), Li), (float)lp));
+        }
+    }
+    o->c_nee = Lsum;
+    v3 wi_spec = spec_sample(n, wo, r, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1));
+    v3 wi_diff = diff_sample(n, R(key, L, DIM_DIFF), R(key, L, DIM_DIFF + 1));
+    o->has_spec = o->has_diff = 0;
+    {
+        v3 org = add(pos, muls(wi_spec, 0.001f));
+        float nd = dot(n, wi_spec);
+        ray_t vr;
+        if (nd > 0.f && light_vis_ray(lc, org, wi_spec, key, L, DIM_SPEC_VIS, &vr)) {
+            double sp = spec_get_pdf(n, wi_spec, wo, r);
+            double lp = light_pdf(lc, pos, wi_spec, key, L, DIM_SPEC_PDF);
+            double w = power_heuristic(sp, lp);
+            v3 f = muls(spec_f(mat, n, wi_spec, wo), nd);
+            v3 Li2 = light_L(lc, wi_spec);
+            if (!iszero(f) && sp > 0.f && !iszero(Li2)) {
+                o->c_spec = divs(muls(mul(f, Li2), (float)w), (float)sp);
+                o->has_spec = 1;
+                o->r_spec = vr;
+            }
+        }
+    }
+    {
+        v3 org = corrected ? add(pos, muls(wi_diff, 0.001f)) : add(pos, muls(wi_spec, 0.001f));
+        float nd = dot(n, wi_diff);
+        ray_t vr;
+        if (nd > 0.f && light_vis_ray(lc, org, wi_diff, key, L, DIM_DIFF_VIS, &vr)) {
+            double dp = diff_get_pdf();
+            double lp = light_pdf(lc, pos, wi_diff, key, L, DIM_DIFF_PDF);
+            double w = power_heuristic(dp, lp);
+            v3 f = muls(diff_f(mat, wi_diff, wo), nd);
+            v3 Li2 = light_L(lc, wi_diff);
+            if (!iszero(f) && dp > 0.f && !iszero(Li2)) {
+                o->c_diff = divs(muls(mul(f, Li2), (float)w), (float)dp);
+                o->has_diff = 1;
+                o->r_diff = vr;
+            }
+        }
+    }
+    v3 dir = R(key, L, DIM_LOBE) < 0.5f ? wi_diff : wi_spec;
+    o->ext_d = dir;
+    o->ext_f = brdf_f(mat, n, dir, wo);
+    o->ext_pdf = brdf_pdf(mat, n, dir, wo);
+    o->ext_cos = hmax(0.f, dot(n, dir));
+}
+
+static void shade_diffuse(const light_ctx* lc, int corrected, const ffo_material* mat, v3 pos, v3 n, v3 wo, v3 wi,
+                          uint32_t key, uint32_t L, shade_t* o)
+{
+    o->c_nee = V(0, 0, 0);
+    if (corrected) {
+        float nd = dot(n, wi);
+        float lp = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+        v3 Li = light_L(lc, wi);
+        if (nd > 0.f && lp > 0.f) o->c_nee = divs(mul(muls(diff_f(mat, wi, wo), nd), Li), lp);
+    }
+    o->has_spec = o->has_diff = 0;
+    v3 dir = diff_sample(n, R(key, L, DIM_DIFF), R(key, L, DIM_DIFF + 1));
+    o->ext_d = dir;
+    o->ext_f = diff_f(mat, dir, wo);
+    o->ext_pdf = (float)diff_get_pdf();
+    o->ext_cos = hmax(0.f, dot(n, dir));
+}
+
+static void shade_conductor(const light_ctx* lc, int corrected, const ffo_material* mat, v3 pos, v3 n, v3 wo, v3 wi,
+                            uint32_t key, uint32_t L, shade_t* o)
+{
+    o->c_nee = V(0, 0, 0);
+    if (corrected) {
+        float nd = dot(n, wi);
+        float lp = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+        v3 Li = light_L(lc, wi);
+        if (nd > 0.f && lp > 0.f) o->c_nee = divs(mul(muls(spec_f(mat, n, wi, wo), nd), Li), lp);
+    }
+    o->has_spec = o->has_diff = 0;
+    float r = mat->roughness;
+    v3 dir = spec_sample(n, wo, r, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1));
+    o->ext_d = dir;
+    o->ext_f = spec_f(mat, n, dir, wo);
+    o->ext_pdf = spec_get_pdf(n, dir, wo, r);
+    o->ext_cos = hmax(0.f, dot(n, dir));
+}
+
+/* gen_ray (dCamera.cu:10-36); NDC in double because of the 0.5 double literal */
+static void camera_ray(const ffo_render_desc* d, int px, int py, v2 jit, v2 lens, v3* o, v3* dir)
+{
+    const float* m = d->cam_inv;
+    float ndx = (float)(2.f * (((double)px + 0.5) / d->width) - 1.f);
+    float ndy = (float)(1.f - 2.f * (((double)py + 0.5) / d->height));
+    float pn[4], pf[4];
+    for (int c = 0; c < 4; ++c) {
+        pn[c] = m[c] * ndx + m[4 + c] * ndy + m[8 + c] * -1.f + m[12 + c] * 1.f;
+        pf[c] = m[c] * ndx + m[4 + c] * ndy + m[8 + c] * 1.f + m[12 + c] * 1.f;
+    }
+    v3 p_near = V(pn[0] / pn[3], pn[1] / pn[3], pn[2] / pn[3]);
+    v3 p_far = V(pf[0] / pf[3], pf[1] / pf[3], pf[2] / pf[3]);
+    v2 sp = {jit.x * d->cam_jitter, jit.y * d->cam_jitter};
+    *o = add(p_near, V(sp.x, sp.y, 0.f));
+    *dir = normalize(sub(p_far, p_near));
+    if (d->cam_lens_radius > 0.f) {
+        v3 focal = add(*o, muls(*dir, d->cam_focal));
+        v2 pl = concentric_disk(lens);
+        pl.x = pl.x * d->cam_lens_radius;
+        pl.y = pl.y * d->cam_lens_radius;
+        *o = add(*o, V(pl.x, pl.y, 0.f));
+        *dir = normalize(sub(focal, *o));
+    }
+}
+
+/* One path sample; returns its radiance (sum of the contributions). */
+static void path_sample(const ffo_render_desc* d, const light_ctx* lc, int px, int py, uint32_t sample, double out[3],
+                        uint64_t* n_ext, uint64_t* n_sh)
+{
+    const int corrected = d->mode == 1;
+    uint32_t pixel = (uint32_t)(py * d->width + px);
+    uint32_t key = ffo_path_key(d->seed, pixel, sample);
+    v3 o, dir;
+    camera_ray(d, px, py, R2(key, 0, DIM_CAM_JITTER), R2(key, 0, DIM_CAM_LENS), &o, &dir);
+    v3 beta = V(1, 1, 1);
+    uint32_t L = 0;
+    shade_t sh;
+    memset(&sh, 0, sizeof(sh));
+    int vis_nee = 0, vis_spec = 0, vis_diff = 0;
+    out[0] = out[1] = out[2] = 0.0;
+    for (;;) {
+        float t, u, v;
+        int prim = closest(d, o, dir, &t, &u, &v);
+        (*n_ext)++;
+        L += 1;
+        int found = prim >= 0;
+        int terminate = (L > (uint32_t)d->max_depth) || !found;
+        if (!found && L == 1) {
+            v3 c = mul(beta, env_L(d, dir));
+            out[0] += c.x; out[1] += c.y; out[2] += c.z;
+        }
+        if (L > 1) {
+            if (corrected) {
+                if (vis_nee || vis_spec || vis_diff) {
+                    v3 lb = V(0, 0, 0);
+                    if (vis_nee) lb = add(lb, sh.c_nee);
+                    if (vis_spec) lb = add(lb, sh.c_spec);
+                    if (vis_diff) lb = add(lb, sh.c_diff);
+                    v3 c = mul(lb, beta);
+                    out[0] += c.x; out[1] += c.y; out[2] += c.z;
+                }
+            } else if (vis_nee) {
+                v3 lb = sh.c_nee;
+                if (sh.has_spec && vis_spec) lb = add(lb, sh.c_spec);
+                if (sh.has_diff && vis_diff) lb = add(lb, sh.c_diff);
+                v3 c = mul(lb, beta);
+                out[0] += c.x; out[1] += c.y; out[2] += c.z;
+            }
+            if (iszero(sh.ext_f) || sh.ext_pdf == 0.f) {
+                terminate = 1;
+            } else {
+                beta = mul(beta, divs(muls(sh.ext_f, sh.ext_cos), sh.ext_pdf));
+                if (L > (uint32_t)d->rr_depth) {
+                    float q = hmax(0.05f, 1.f - beta.y);
+                    if (R(key, L, DIM_RR) < q) terminate = 1;
+                    else if (corrected) beta = divs(beta, 1.f - q);
+                }
+            }
+        }
+        if (terminate) break;
+        /* hit attributes (dTriangle::hit) */
+        const float* nn = d->normals + 9 * (size_t)prim;
+        v3 n0 = ld3(nn), n1 = ld3(nn + 3), n2 = ld3(nn + 6);
+        v3 n = normalize(add(add(smul(u, n1), smul(v, n2)), smul((1.f - u) - v, n0)));
+        v3 pos = add(o, smul(t, dir));
+        v3 wi, sp;
+        if (lc->is_env) {
+            env_sample(lc, pos, R(key, L, DIM_LIGHT), R(key, L, DIM_LIGHT + 1), &wi, &sp);
+        } else {
+            sp = rect_sample(&lc->rect, R2(key, L, DIM_LIGHT));
+            wi = normalize(sub(sp, pos));
+        }
+        const ffo_material* mat = &d->materials[d->material_ids ? d->material_ids[prim] : 0];
+        v3 wo = neg(dir);
+        memset(&sh, 0, sizeof(sh));
+        if (mat->kind == 0) shade_mix(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
+        else if (mat->kind == 1) shade_diffuse(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
+        else shade_conductor(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
+        v3 lo = add(pos, muls(n, d->shadow_offset));
+        sh.has_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, &sh.r_nee);
+        vis_nee = sh.has_nee && !occluded(d, &sh.r_nee);
+        vis_spec = sh.has_spec && !occluded(d, &sh.r_spec);
+        vis_diff = sh.has_diff && !occluded(d, &sh.r_diff);
+        *n_sh += (uint64_t)(sh.has_nee + sh.has_spec + sh.has_diff);
+        o = pos;
+        if (corrected) {
+            float side = dot(sh.ext_d, n) >= 0.f ? 1.f : -1.f;
+            o = add(pos, muls(n, side * d->shadow_offset));
+        }
+        dir = sh.ext_d;
+    }
+}
+
+typedef struct {
+    const ffo_render_desc* d;
+    const light_ctx* lc;
+    double* out;
+    int row0, row1;
+    uint64_t n_ext, n_sh;
+} rjob_t;
+
+static void* render_rows(void* arg)
+{
+    rjob_t* j = (rjob_t*)arg;
+    const ffo_render_desc* d = j->d;
+    for (int y = j->row0; y < j->row1; ++y)
+        for (int x = 0; x < d->width; ++x) {
+            double* px = j->out + 3 * ((size_t)y * d->width + x);
+            for (int s = 0; s < d->spp; ++s) {
+                double c[3];
+                path_sample(d, j->lc, x, y, (uint32_t)(d->sample_offset + s), c, &j->n_ext, &j->n_sh);
+                px[0] += c[0]; px[1] += c[1]; px[2] += c[2];
+            }
+        }
+    return NULL;
+}
+
+int ffo_render(const ffo_render_desc* d, double* out_rgb, uint64_t* stats)
+{
+    light_ctx lc;
+    memset(&lc, 0, sizeof(lc));
+    lc.d = d;
+    lc.is_env = d->light < 0;
+    double *marginal = NULL, *cond = NULL;
+    float* pdf = NULL;
+    if (lc.is_env) {
+        if (!d->env_rgb) return 1;
+        marginal = (double*)malloc(sizeof(double) * d->env_h);
+        cond = (double*)malloc(sizeof(double) * (size_t)d->env_w * d->env_h);
+        pdf = (float*)malloc(sizeof(float) * (size_t)d->env_w * d->env_h);
+        ffo_env_build(d->env_rgb, d->env_w, d->env_h, marginal, cond, pdf, NULL);
+        lc.marginal = marginal;
+        lc.cond = cond;
+        lc.pdf = pdf;
+    } else {
+        if (d->light >= d->num_area_lights) return 1;
+        lc.rect = make_rect(&d->area_lights[d->light]);
+    }
+    memset(out_rgb, 0, sizeof(double) * 3 * (size_t)d->width * d->height);
+    int nt = d->threads > 0 ? d->threads : 1;
+    if (nt > 256) nt = 256;
+    pthread_t th[256];
+    rjob_t jobs[256];
+    int rows = d->height;
+    for (int k = 0; k < nt; ++k) {
+        jobs[k].d = d;
+        jobs[k].lc = &lc;
+        jobs[k].out = out_rgb;
+        jobs[k].row0 = rows * k / nt;
+        jobs[k].row1 = rows * (k + 1) / nt;
+        jobs[k].n_ext = jobs[k].n_sh = 0;
+        if (pthread_create(&th[k], NULL, render_rows, &jobs[k]) != 0) {
+            render_rows(&jobs[k]);
+            th[k] = 0;
+        }
+    }
+    uint64_t ne = 0, ns = 0;
+    for (int k = 0; k < nt; ++k) {
+        if (th[k]) pthread_join(th[k], NULL);
+        ne += jobs[k].n_ext;
+        ns += jobs[k].n_sh;
+    }
+    if (stats) { stats[0] = ne; stats[1] = ns; }
+    free(marginal);
+    free(cond);
+    free(pdf);
+    return 0;
+}

@@ -1,0 +1,125 @@
+"""Image parity of ff_render against the oracle's restatement of the
+reference's wavefront stages, with the same per-pixel sampler seeds.
+
+Tolerance (north star): mean relative error <= 1e-4, measured as
+    mre = sum |gpu - oracle| / sum |oracle|
+over all pixels and channels of the per-pixel mean radiance.  Both sides
+follow the reference's arithmetic operation by operation; what remains are
+last-bit differences of the device and host sinf/cosf/atan2f/asinf/acosf/atanf
+and FP64 sin/cos, which occasionally send a path across a triangle edge.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from firefly_b200 import scenes
+from tests.conftest import cpu_threads
+
+pytestmark = pytest.mark.gpu
+
+MRE_TOL = 1e-4
+
+
+def _gpu_render(ctx, scn, w, h, spp, **kw):
+    import firefly_b200 as ff
+    ds = ff.dScene(ctx, scn)
+    pt = ff.PathTracer(ctx, w, h)
+    stats = pt.draw(ds, spp=spp, **kw)
+    rgba, n = pt.read()
+    pt.close()
+    ds.close()
+    return rgba[..., :3].astype(np.float64), n, stats
+
+
+def _mre(a, b):
+    return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-30))
+
+
+def _parity(ctx, oracle, scn, w, h, spp, light=0, max_depth=5, rr_depth=3, seed=0, mode=0, **kw):
+    got, n, stats = _gpu_render(ctx, scn, w, h, spp, light=light, max_depth=max_depth, rr_depth=rr_depth,
+                                seed=seed, mode=mode, **kw)
+    ref, (ref_ext, ref_sh) = oracle.render(scn, w, h, spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed,
+                                           mode=mode, light=light, threads=cpu_threads())
+    assert np.all(n == spp)
+    mre = _mre(got / spp, ref / spp)
+    assert mre <= MRE_TOL, f"mean relative error {mre:.3e} > {MRE_TOL}"
+    # the same paths were traced
+    assert abs(stats["extension_rays"] - ref_ext) <= max(2, 1e-3 * ref_ext), (stats["extension_rays"], ref_ext)
+    assert abs(stats["shadow_rays"] - ref_sh) <= max(2, 1e-3 * ref_sh), (stats["shadow_rays"], ref_sh)
+    return got, ref, stats, mre
+
+
+def test_small_room_parity_64(ctx, oracle):
+    scn = scenes.small_room(seed=0, width=64, height=64)
+    got, ref, stats, mre = _parity(ctx, oracle, scn, 64, 64, 4)
+    assert (ref.sum(-1) > 0).mean() > 0.8   # the light reaches most pixels
+
+
+def test_small_room_parity_full_config(ctx, oracle):
+    """The plain-tracer workload itself: 256 x 256, 16 spp, depth 5, RR from depth 3, seed 0."""
+    scn = scenes.small_room(seed=0)
+    _parity(ctx, oracle, scn, 256, 256, 16)
+
+
+def test_parity_with_lens_and_depth3(ctx, oracle):
+    scn = scenes.small_room(seed=1, width=48, height=40, lens_radius=0.05)
+    _parity(ctx, oracle, scn, 48, 40, 3, max_depth=3, rr_depth=2, seed=7)
+
+
+def test_parity_single_lobe_materials(ctx, oracle):
+    import firefly_b200 as ff
+    for kind in (ff.FF_MAT_DIFFUSE, ff.FF_MAT_CONDUCTOR):
+        scn = scenes.small_room(seed=2, width=40, height=40, kind=kind)
+        for m in scn.materials:
+            m.roughness = 0.4
+        # parity: the reference's diff_L / spec_L return 0, so only corrected mode carries light
+        _parity(ctx, oracle, scn, 40, 40, 2, mode=ff.FF_MODE_CORRECTED)
+
+
+def test_corrected_mode_parity(ctx, oracle):
+    import firefly_b200 as ff
+    scn = scenes.small_room(seed=3, width=48, height=48)
+    _parity(ctx, oracle, scn, 48, 48, 4, mode=ff.FF_MODE_CORRECTED)
+
+
+def test_progressive_and_pool_size_invariance(ctx):
+    import firefly_b200 as ff
+    scn = scenes.small_room(seed=0, width=64, height=48)
+    ds = ff.dScene(ctx, scn)
+    pt = ff.PathTracer(ctx, 64, 48)
+    pt.draw(ds, spp=8, max_depth=5, seed=5)
+    one, n1 = pt.read()
+    pt.clear_buffer()
+    z, nz = pt.read()
+    assert np.all(nz == 0) and np.all(z == 0)
+    # two progressive calls, small pool (one slot per pixel)
+    pt.draw(ds, spp=3, max_depth=5, seed=5, sample_offset=0, max_paths=64 * 48)
+    pt.draw(ds, spp=5, max_depth=5, seed=5, sample_offset=3, max_paths=64 * 48)
+    two, n2 = pt.read()
+    assert np.array_equal(n1, n2)
+    assert np.allclose(one, two, rtol=1e-5, atol=1e-6)
+    # determinism
+    pt.clear_buffer()
+    pt.draw(ds, spp=8, max_depth=5, seed=5)
+    again, _ = pt.read()
+    assert np.array_equal(one, again)
+    img8 = pt.tonemap(1.0)
+    assert img8.shape == (48, 64, 4) and img8[..., 3].min() == 255
+    pt.close()
+    ds.close()
+
+
+def test_render_argument_errors(ctx):
+    import firefly_b200 as ff
+    scn = scenes.small_room(seed=0, width=16, height=16)
+    ds = ff.dScene(ctx, scn)
+    pt = ff.PathTracer(ctx, 16, 16)
+    with pytest.raises(ff.FireflyError):
+        pt.draw(ds, spp=1, light=-1)     # no environment map in this scene
+    with pytest.raises(ff.FireflyError):
+        pt.draw(ds, spp=1, light=3)      # no such area light
+    with pytest.raises(ff.FireflyError):
+        pt.draw(ds, spp=0, light=0)
+    pt.close()
+    ds.close()
