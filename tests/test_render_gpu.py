@@ -43,6 +43,9 @@ def _parity(ctx, oracle, scn, w, h, spp, light=0, max_depth=5, rr_depth=3, seed=
                                            mode=mode, light=light, threads=cpu_threads())
     assert np.all(n == spp)
     mre = _mre(got / spp, ref / spp)
+    print(f"[parity] {w}x{h} spp={spp} depth={max_depth} mode={mode}: mre={mre:.3e} "
+          f"ext={stats['extension_rays']}/{ref_ext} shadow={stats['shadow_rays']}/{ref_sh} "
+          f"gpu_ms={stats['ms_total']:.2f} frames={stats['frames']}")
     assert mre <= MRE_TOL, f"mean relative error {mre:.3e} > {MRE_TOL}"
     # the same paths were traced
     assert abs(stats["extension_rays"] - ref_ext) <= max(2, 1e-3 * ref_ext), (stats["extension_rays"], ref_ext)
@@ -88,20 +91,20 @@ def test_progressive_and_pool_size_invariance(ctx):
     scn = scenes.small_room(seed=0, width=64, height=48)
     ds = ff.dScene(ctx, scn)
     pt = ff.PathTracer(ctx, 64, 48)
-    pt.draw(ds, spp=8, max_depth=5, seed=5)
+    pt.draw(ds, spp=8, max_depth=5, seed=5, light=0)
     one, n1 = pt.read()
     pt.clear_buffer()
     z, nz = pt.read()
     assert np.all(nz == 0) and np.all(z == 0)
     # two progressive calls, small pool (one slot per pixel)
-    pt.draw(ds, spp=3, max_depth=5, seed=5, sample_offset=0, max_paths=64 * 48)
-    pt.draw(ds, spp=5, max_depth=5, seed=5, sample_offset=3, max_paths=64 * 48)
+    pt.draw(ds, spp=3, max_depth=5, seed=5, sample_offset=0, max_paths=64 * 48, light=0)
+    pt.draw(ds, spp=5, max_depth=5, seed=5, sample_offset=3, max_paths=64 * 48, light=0)
     two, n2 = pt.read()
     assert np.array_equal(n1, n2)
     assert np.allclose(one, two, rtol=1e-5, atol=1e-6)
     # determinism
     pt.clear_buffer()
-    pt.draw(ds, spp=8, max_depth=5, seed=5)
+    pt.draw(ds, spp=8, max_depth=5, seed=5, light=0)
     again, _ = pt.read()
     assert np.array_equal(one, again)
     img8 = pt.tonemap(1.0)
