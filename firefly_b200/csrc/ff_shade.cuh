@@ -324,6 +324,38 @@ FF_D void env_sample(const FFEnvView& e, float3 pos, float ex, float ey, float3&
     wi = normalize3(sp - pos);
 }
 
+// Corrected-mode environment sampling (no reference counterpart): the texel
+// picked from the same CDFs is sampled uniformly and mapped with the inverse
+// of spherical_map, so the sampled direction looks up the texel it came
+// from; the pdf uses that mapping's Jacobian, cos(latitude) = sqrt(1 - y^2).
+// The reference maps the texel corner through sample_spherical_direction
+// (a different parametrisation) and divides by sin(acos(wi.z)).
+FF_D void env_sample_corrected(const FFEnvView& e, float3 pos, float ex, float ey, float jx, float jy, float3& wi,
+                               float3& sp)
+{
+    int y = (int)((float)upper_bound_ref(e.marginal, e.height, ey) - 1.f);
+    y = y < 0 ? 0 : (y >= e.height ? e.height - 1 : y);
+    int x = (int)((float)upper_bound_ref(e.cond + (size_t)y * e.width, e.width, ex) - 1.f);
+    x = x < 0 ? 0 : (x >= e.width ? e.width - 1 : x);
+    const float u = ((float)x + jx) / (float)e.width;
+    const float v = ((float)y + jy) / (float)e.height;
+    const float phi = (u - 0.5f) * FF_2PI;
+    const float lat = (v - 0.5f) * FF_PI;
+    const float cl = cosf(lat);
+    wi = make_float3(cl * cosf(phi), sinf(lat), cl * sinf(phi));
+    sp = pos + wi * e.radius;
+}
+FF_D float env_pdf_corrected(const FFEnvView& e, float3 wi)
+{
+    float2 uv = spherical_map(wi);
+    int x = (int)(uv.x * (float)e.width);
+    int y = (int)(uv.y * (float)e.height);
+    x = x < 0 ? 0 : (x >= e.width ? e.width - 1 : x);
+    y = y < 0 ? 0 : (y >= e.height ? e.height - 1 : y);
+    const float cl = sqrtf(hmax(0.f, 1.f - wi.y * wi.y));
+    return cl > 0.f ? e.pdf[(size_t)y * e.width + x] / cl : 0.f;
+}
+
 // get_pdf(isect, wi) (dEnvironmentLight.cu:83-103): pdf texel over sin(acos(wi.z))
 FF_D float env_pdf(const FFEnvView& e, float3 wi)
 {

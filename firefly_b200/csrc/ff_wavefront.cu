@@ -219,8 +219,12 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 // Light sample (kernel.cu:435, light get_direction).
                 float3 wi, sp;
                 if (w.light < 0) {
-                    env_sample(w.env, pos, ff_rand(key, dim_of(L, DIM_LIGHT)), ff_rand(key, dim_of(L, DIM_LIGHT + 1)),
-                               wi, sp);
+                    const float ex = ff_rand(key, dim_of(L, DIM_LIGHT)), ey = ff_rand(key, dim_of(L, DIM_LIGHT + 1));
+                    if (w.mode == FF_MODE_CORRECTED)
+                        env_sample_corrected(w.env, pos, ex, ey, ff_rand(key, dim_of(L, DIM_EXTRA + 1)),
+                                             ff_rand(key, dim_of(L, DIM_EXTRA + 2)), wi, sp);
+                    else
+                        env_sample(w.env, pos, ex, ey, wi, sp);
                 } else {
                     const FFRect r = make_rect(w.area[w.light]);
                     sp = rect_sample(r, rand2(key, L, DIM_LIGHT));
@@ -270,6 +274,7 @@ __device__ __forceinline__ ff_ray make_ray(float3 o, float3 d, float tmax)
 struct LightCtx {
     const WF* w;
     bool is_env;
+    bool corrected;
     FFRect rect;
 };
 
@@ -280,7 +285,8 @@ __device__ __forceinline__ float3 light_L(const LightCtx& lc, float3 wi)
 __device__ __forceinline__ float light_pdf(const LightCtx& lc, float3 pos, float3 wi, uint32_t key, uint32_t L,
                                            uint32_t dim)
 {
-    return lc.is_env ? env_pdf(lc.w->env, wi) : rect_pdf(lc.rect, pos, rand2(key, L, dim));
+    if (lc.is_env) return lc.corrected ? env_pdf_corrected(lc.w->env, wi) : env_pdf(lc.w->env, wi);
+    return rect_pdf(lc.rect, pos, rand2(key, L, dim));
 }
 // Visibility ray of light.visible(ray): returns false when the reference
 // answers "not visible" without tracing (area light missed).
@@ -505,6 +511,7 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
     LightCtx lc;
     lc.w = &w;
     lc.is_env = w.light < 0;
+    lc.corrected = w.mode == FF_MODE_CORRECTED;
     if (!lc.is_env) lc.rect = make_rect(w.area[w.light]);
     for (uint32_t it = 0; it < iters; ++it) {
         const uint32_t qi = base + it * stride;

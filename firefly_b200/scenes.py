@@ -277,3 +277,205 @@ def with_random_tmax(rays: np.ndarray, scene: Scene, seed: int = 2) -> np.ndarra
     out = rays.copy()
     out[:, 7] = (rng.uniform(0.1, 10.0, size=len(rays)) * diag).astype(np.float32)
     return out
+
+
+# ------------------------------------------------------- environment maps
+def sky_env(width: int = 2048, height: int = 1024, seed: int = 0, sun_dir=(0.35, 0.8, 0.25),
+            sun_radiance: float = 5e4, sun_diameter_deg: float = 0.5) -> np.ndarray:
+    """Synthetic equirectangular sky, (height, width, 3) float32, row y at v = y/height.
+
+    A vertical gradient (zenith blue to a bright horizon, darker ground) times
+    log-normal(0, 0.5) per-texel noise, plus a sun disc of the given angular
+    diameter and radiance.  Texel directions follow the reference's
+    spherical mapping: u = atan2(z, x)/2pi + 0.5, v = asin(y)/pi + 0.5."""
+    rng = np.random.default_rng(seed)
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    U, Vv = np.meshgrid(u, v)
+    phi = (U - 0.5) * 2 * math.pi
+    lat = (Vv - 0.5) * math.pi
+    dy = np.sin(lat)
+    dx = np.cos(lat) * np.cos(phi)
+    dz = np.cos(lat) * np.sin(phi)
+    t = np.clip(dy, -1, 1)
+    zenith = np.array([0.25, 0.45, 0.95])
+    horizon = np.array([0.9, 0.9, 1.0])
+    ground = np.array([0.25, 0.22, 0.2])
+    up = np.clip(t, 0, 1)[..., None]
+    sky = np.where(t[..., None] >= 0, horizon * (1 - up) + zenith * up, ground * (0.5 + 0.5 * (1 + t[..., None])))
+    noise = rng.lognormal(0.0, 0.5, size=(height, width, 1))
+    img = sky * noise
+    s = np.asarray(sun_dir, np.float64)
+    s /= np.linalg.norm(s)
+    cosang = dx * s[0] + dy * s[1] + dz * s[2]
+    half = math.radians(sun_diameter_deg) / 2
+    # at least the texel nearest the sun direction lights up, so the sun survives any resolution
+    disc = cosang >= math.cos(half)
+    su = math.atan2(s[2], s[0]) / (2 * math.pi) + 0.5
+    sv = math.asin(s[1]) / math.pi + 0.5
+    disc[min(height - 1, int(sv * height)), min(width - 1, int(su * width))] = True
+    img[disc] = sun_radiance
+    return img.astype(np.float32)
+
+
+def sphere_under_sky(seed: int = 0, width: int = 64, height: int = 64, env_w: int = 128, env_h: int = 64,
+                     kind=A.FF_MAT_MIX) -> Scene:
+    """Open scene for the environment light: a ground quad and a UV sphere
+    under a synthetic sky."""
+    rng = np.random.default_rng(seed)
+    gP = np.array([[-20, 0, -20], [-20, 0, 20], [20, 0, 20], [20, 0, -20]], np.float32)
+    gI = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+    gN = np.tile(np.array([0, 1, 0], np.float32), (4, 1))
+    radius = float(rng.uniform(1.0, 1.5))
+    sP, sI, sN = uv_sphere((0.0, radius, 0.0), radius, seg_u=32, seg_v=16)
+    P = np.concatenate([gP, sP])
+    N = np.concatenate([gN, sN])
+    I = np.concatenate([gI, sI + len(gP)]).astype(np.uint32)
+    mat_ids = np.concatenate([np.zeros(len(gI), np.uint32), np.ones(len(sI), np.uint32)])
+    albedo = rng.uniform(0.2, 0.8, size=(2, 3))
+    mats = [material(albedo[0], kind=kind, roughness=0.8), material(albedo[1], kind=kind, roughness=0.5)]
+    cam = make_camera(eye=(0.0, 2.5, 6.0), center=(0.0, radius, 0.0), fovy=50.0, aspect=width / height,
+                      near=0.05, far=100.0)
+    env = sky_env(env_w, env_h, seed=seed, sun_radiance=200.0, sun_diameter_deg=4.0)
+    return Scene(positions=P.astype(np.float32), indices=I, normals=N.astype(np.float32), material_ids=mat_ids,
+                 materials=mats, env_rgb=env, camera=cam, width=width, height=height)
+
+
+# ----------------------------------------------------- at-scale workload
+def icosphere(subdiv: int):
+    """Unit icosphere: 20 * 4^subdiv triangles, outward winding."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    V = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    V /= np.linalg.norm(V, axis=1, keepdims=True)
+    F = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    for _ in range(subdiv):
+        e = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]])
+        e.sort(axis=1)
+        key = e[:, 0] * len(V) + e[:, 1]
+        uniq, inv = np.unique(key, return_inverse=True)
+        a, b = uniq // len(V), uniq % len(V)
+        mid = V[a] + V[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = len(V)
+        V = np.concatenate([V, mid])
+        nf = len(F)
+        m01, m12, m20 = inv[:nf] + base, inv[nf:2 * nf] + base, inv[2 * nf:] + base
+        F = np.concatenate([np.stack([F[:, 0], m01, m20], 1), np.stack([F[:, 1], m12, m01], 1),
+                            np.stack([F[:, 2], m20, m12], 1), np.stack([m01, m12, m20], 1)])
+    return V, F
+
+
+def value_noise3(p: np.ndarray, seed: int, octaves: int = 4) -> np.ndarray:
+    """Fractal value noise in [-1, 1]: lattice values hashed from integer
+    coordinates, smoothstep-interpolated, octaves at doubling frequency and
+    halving amplitude."""
+    rng = np.random.default_rng(seed)
+    table = rng.uniform(-1.0, 1.0, size=256)
+    perm = rng.permutation(256)
+
+    def lattice(ix, iy, iz):
+        h = perm[(perm[(perm[ix & 255] + iy) & 255] + iz) & 255]
+        return table[h]
+
+    total = np.zeros(len(p))
+    amp, freq, norm = 1.0, 1.0, 0.0
+    for _ in range(octaves):
+        q = p * freq
+        i = np.floor(q).astype(np.int64)
+        f = q - i
+        s = f * f * (3 - 2 * f)
+        acc = np.zeros(len(p))
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    w = ((s[:, 0] if dx else 1 - s[:, 0]) * (s[:, 1] if dy else 1 - s[:, 1]) *
+                         (s[:, 2] if dz else 1 - s[:, 2]))
+                    acc += w * lattice(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz)
+        total += amp * acc
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return total / norm
+
+
+def displaced_icosphere(subdiv: int = 8, seed: int = 0, width: int = 1920, height: int = 1080,
+                        env_w: int = 2048, env_h: int = 1024) -> Scene:
+    """The at-scale workload: an icosphere subdivided `subdiv` times (8 ->
+    1,310,720 triangles) displaced radially by 4-octave value noise of
+    amplitude 0.1 x radius, inside a 12-triangle room (floor, four walls and
+    half a ceiling, open to the sky over the other half), triangles grouped by
+    a seeded 3D noise into 4 material classes (diffuse, GGX conductor with
+    roughness U[0.05, 0.6], thin GGX dielectric of IOR 1.5, diffuse under a
+    GGX coat), a 2048 x 1024 sky with a 0.5 degree sun of radiance 5e4."""
+    rng = np.random.default_rng(seed)
+    V, F = icosphere(subdiv)
+    radius, center = 2.0, np.array([0.0, 2.4, 0.0])
+    disp = value_noise3(V * 2.0 + 10.0, seed + 1, octaves=4)
+    Pv = center + V * (radius * (1.0 + 0.1 * disp))[:, None]
+    # vertex normals of the displaced surface (area-weighted face normals)
+    tri = Pv[F]
+    fn = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    Nv = np.zeros_like(Pv)
+    for k in range(3):
+        np.add.at(Nv, F[:, k], fn)
+    Nv /= np.linalg.norm(Nv, axis=1, keepdims=True)
+    # room: 12 triangles (floor, four walls, half a ceiling), normals inward
+    lo, hi = np.array([-8.0, 0.0, -8.0]), np.array([8.0, 9.0, 8.0])
+    room_tris, room_P = [], []
+
+    def quad(a, b, c, d):
+        base = len(room_P)
+        room_P.extend([a, b, c, d])
+        room_tris.extend([[base, base + 1, base + 2], [base, base + 2, base + 3]])
+
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    quad([x0, y0, z0], [x0, y0, z1], [x1, y0, z1], [x1, y0, z0])          # floor, normal +y
+    quad([x0, y0, z0], [x0, y1, z0], [x0, y1, z1], [x0, y0, z1])          # x = x0, normal +x
+    quad([x1, y0, z0], [x1, y0, z1], [x1, y1, z1], [x1, y1, z0])          # x = x1, normal -x
+    quad([x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0])          # z = z0, normal +z
+    quad([x0, y0, z1], [x0, y1, z1], [x1, y1, z1], [x1, y0, z1])          # z = z1, normal -z
+    quad([x0, y1, 0.0], [x1, y1, 0.0], [x1, y1, z1], [x0, y1, z1])        # ceiling over z > 0, normal -y
+    rP = np.asarray(room_P, np.float64)
+    rI = np.asarray(room_tris, np.int64)
+    rt = rP[rI]
+    rn = np.cross(rt[:, 1] - rt[:, 0], rt[:, 2] - rt[:, 0])
+    rn /= np.linalg.norm(rn, axis=1, keepdims=True)
+    inward = ((lo + hi) / 2 - rt.mean(1)) * rn
+    assert np.all(inward.sum(1) > 0), "room triangles must face inward"
+    rN = np.zeros_like(rP)
+    for t_, (i0, i1, i2) in enumerate(rI):
+        rN[[i0, i1, i2]] = rn[t_]
+    P = np.concatenate([rP, Pv]).astype(np.float32)
+    N = np.concatenate([rN, Nv]).astype(np.float32)
+    I = np.concatenate([rI, F + len(rP)]).astype(np.uint32)
+    # materials: 0 = room (the reference's mix material); classes 1..4 x 8 variants
+    mats = [material((0.7, 0.7, 0.68), kind=A.FF_MAT_MIX, roughness=0.9)]
+    kinds = [A.FF_MAT_DIFFUSE, A.FF_MAT_CONDUCTOR, A.FF_MAT_DIELECTRIC, A.FF_MAT_COAT]
+    variants = 8
+    for kd in kinds:
+        for _ in range(variants):
+            alb = rng.uniform(0.2, 0.9, 3)
+            if kd == A.FF_MAT_DIFFUSE:
+                mats.append(material(alb, kind=kd, roughness=1.0))
+            elif kd == A.FF_MAT_CONDUCTOR:
+                mats.append(material(alb, kind=kd, roughness=float(rng.uniform(0.05, 0.6)), metallic=1.0))
+            elif kd == A.FF_MAT_DIELECTRIC:
+                mats.append(material((0.95, 0.97, 1.0), kind=kd, roughness=float(rng.uniform(0.05, 0.3)), ior=1.5))
+            else:
+                mats.append(material(alb, kind=kd, roughness=float(rng.uniform(0.05, 0.3)), ior=1.5))
+    cen = Pv[F].mean(axis=1)
+    cls_noise = value_noise3(cen * 1.5 + 3.0, seed + 2, octaves=2)
+    q = np.quantile(cls_noise, [0.25, 0.5, 0.75])
+    cls = np.searchsorted(q, cls_noise)
+    var = (np.arange(len(F)) * 2654435761 % 2**32 >> 16) % variants
+    sphere_mat = 1 + cls * variants + var
+    mat_ids = np.concatenate([np.zeros(len(rI), np.uint32), sphere_mat.astype(np.uint32)])
+    cam = make_camera(eye=(0.0, 3.2, 7.4), center=(0.0, 2.2, 0.0), fovy=50.0, aspect=width / height,
+                      near=0.05, far=100.0)
+    env = sky_env(env_w, env_h, seed=seed)
+    return Scene(positions=P, indices=I, normals=N, material_ids=mat_ids, materials=mats, env_rgb=env,
+                 camera=cam, width=width, height=height)

@@ -322,6 +322,7 @@ static float rect_pdf(const rect_t* r, v3 pos, v2 u)
 typedef struct {
     const ffo_render_desc* d;
     int is_env;
+    int corrected;
     rect_t rect;
     const double* marginal;
     const double* cond;
@@ -354,10 +355,35 @@ static void env_sample(const light_ctx* lc, v3 pos, float ex, float ey, v3* wi, 
     *sp = add(V(0.f, 0.f, 0.f), muls(dir, 10000.f));
     *wi = normalize(sub(*sp, pos));
 }
+/* corrected mode: uniform point in the chosen texel, inverse of spherical_map, cos(latitude) Jacobian */
+static void env_sample_corrected(const light_ctx* lc, v3 pos, float ex, float ey, float jx, float jy, v3* wi, v3* sp)
+{
+    const ffo_render_desc* d = lc->d;
+    int y = (int)((float)upper_bound_ref(lc->marginal, d->env_h, ey) - 1.f);
+    y = y < 0 ? 0 : (y >= d->env_h ? d->env_h - 1 : y);
+    int x = (int)((float)upper_bound_ref(lc->cond + (size_t)y * d->env_w, d->env_w, ex) - 1.f);
+    x = x < 0 ? 0 : (x >= d->env_w ? d->env_w - 1 : x);
+    float u = ((float)x + jx) / (float)d->env_w, v = ((float)y + jy) / (float)d->env_h;
+    float phi = (u - 0.5f) * TWO_PI_F, lat = (v - 0.5f) * PI_F;
+    float cl = cosf(lat);
+    *wi = V(cl * cosf(phi), sinf(lat), cl * sinf(phi));
+    *sp = add(pos, muls(*wi, 10000.f));
+}
+static float env_pdf_corrected(const light_ctx* lc, v3 wi)
+{
+    const ffo_render_desc* d = lc->d;
+    v2 uv = spherical_map(wi);
+    int x = (int)(uv.x * (float)d->env_w), y = (int)(uv.y * (float)d->env_h);
+    x = x < 0 ? 0 : (x >= d->env_w ? d->env_w - 1 : x);
+    y = y < 0 ? 0 : (y >= d->env_h ? d->env_h - 1 : y);
+    float cl = sqrtf(hmax(0.f, 1.f - wi.y * wi.y));
+    return cl > 0.f ? lc->pdf[(size_t)y * d->env_w + x] / cl : 0.f;
+}
 static v3 light_L(const light_ctx* lc, v3 wi) { return lc->is_env ? env_L(lc->d, wi) : rect_L(&lc->rect, wi); }
 static float light_pdf(const light_ctx* lc, v3 pos, v3 wi, uint32_t key, uint32_t L, uint32_t dim)
 {
-    return lc->is_env ? env_pdf(lc, wi) : rect_pdf(&lc->rect, pos, R2(key, L, dim));
+    if (lc->is_env) return lc->corrected ? env_pdf_corrected(lc, wi) : env_pdf(lc, wi);
+    return rect_pdf(&lc->rect, pos, R2(key, L, dim));
 }
 
 typedef struct { v3 o, d; float tmax; } ray_t;
@@ -596,7 +622,11 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc, int px, i
         v3 pos = add(o, smul(t, dir));
         v3 wi, sp;
         if (lc->is_env) {
-            env_sample(lc, pos, R(key, L, DIM_LIGHT), R(key, L, DIM_LIGHT + 1), &wi, &sp);
+            if (corrected)
+                env_sample_corrected(lc, pos, R(key, L, DIM_LIGHT), R(key, L, DIM_LIGHT + 1), R(key, L, DIM_EXTRA + 1),
+                                     R(key, L, DIM_EXTRA + 2), &wi, &sp);
+            else
+                env_sample(lc, pos, R(key, L, DIM_LIGHT), R(key, L, DIM_LIGHT + 1), &wi, &sp);
         } else {
             sp = rect_sample(&lc->rect, R2(key, L, DIM_LIGHT));
             wi = normalize(sub(sp, pos));
@@ -652,6 +682,7 @@ int ffo_render(const ffo_render_desc* d, double* out_rgb, uint64_t* stats)
     memset(&lc, 0, sizeof(lc));
     lc.d = d;
     lc.is_env = d->light < 0;
+    lc.corrected = d->mode == 1;
     double *marginal = NULL, *cond = NULL;
     float* pdf = NULL;
     if (lc.is_env) {
