@@ -26,9 +26,12 @@ constexpr int kEnvBlock = 256;
 
 __device__ __forceinline__ double row_sin(int j, int h)
 {
-    // sin(M_PI * v) with M_PI a float constant: sinf of a float, widened
+    // sin(M_PI * v) with M_PI a float constant: the float sine of a float
+    // argument, widened.  The reference's host build gets a correctly rounded
+    // sinf from libm; the double sine rounded to float reproduces it (the
+    // device's single-precision sinf may differ in the last bit).
     const float v = (float)j / (float)h;
-    return (double)sinf(FF_PI * v);
+    return (double)(float)sin((double)(FF_PI * v));
 }
 
 __global__ void __launch_bounds__(kEnvBlock) k_env_rows(const float3* __restrict__ rgb, int w, int h,

@@ -728,3 +728,105 @@ int ffo_render(const ffo_render_desc* d, double* out_rgb, uint64_t* stats)
     free(pdf);
     return 0;
 }
+
+/* ---------------------------------------------------------------------
+ * Probe entry points: the restated routines one by one, for the golden
+ * vectors of tests/golden/ (made from the reference's own routines).
+ * mat8 = base[3], fresnel[3], roughness, metallic; vectors are float[3].
+ * ------------------------------------------------------------------- */
+static ffo_material mat_of(const float* m8)
+{
+    ffo_material m;
+    for (int k = 0; k < 3; ++k) { m.base_color[k] = m8[k]; m.fresnel[k] = m8[3 + k]; }
+    m.roughness = m8[6];
+    m.metallic = m8[7];
+    m.kind = 0;
+    return m;
+}
+static void st3(float* o, v3 v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; }
+
+/* out: diff_f[3], spec_f[3], spec_pdf, BRDF_pdf, BRDF_f[3], fresnel[3], D, G, diff_pdf (17) */
+void ffo_probe_material(const float* m8, const float* n3, const float* wi3, const float* wo3, float* out)
+{
+    ffo_material m = mat_of(m8);
+    v3 n = ld3(n3), wi = ld3(wi3), wo = ld3(wo3);
+    st3(out, diff_f(&m, wi, wo));
+    st3(out + 3, spec_f(&m, n, wi, wo));
+    out[6] = spec_get_pdf(n, wi, wo, m.roughness);
+    out[7] = brdf_pdf(&m, n, wi, wo);
+    st3(out + 8, brdf_f(&m, n, wi, wo));
+    v3 wh = normalize(add(wo, wi));
+    st3(out + 11, fresnel3(ld3(m.fresnel), wh, wi));
+    out[14] = (float)ggx_ndf(n, wh, m.roughness);
+    out[15] = (float)geo_atten(wi, wo, n, m.roughness);
+    out[16] = (float)diff_get_pdf();
+}
+void ffo_probe_diff_sample(const float* n3, float e0, float e1, float* out3) { st3(out3, diff_sample(ld3(n3), e0, e1)); }
+void ffo_probe_spec_sample(const float* n3, const float* wo3, float r, float e0, float e1, float* out3)
+{
+    st3(out3, spec_sample(ld3(n3), ld3(wo3), r, e0, e1));
+}
+void ffo_probe_concentric_disk(float u0, float u1, float* out2)
+{
+    v2 u = {u0, u1};
+    v2 r = concentric_disk(u);
+    out2[0] = r.x;
+    out2[1] = r.y;
+}
+int ffo_probe_upper_bound(const double* list, int size, float val) { return upper_bound_ref(list, size, val); }
+void ffo_probe_tex(const float* rgb, int w, int h, float u, float v, float* out3) { st3(out3, tex_bilinear(rgb, w, h, u, v)); }
+/* camera: inv16, lens, focal, jitter scale, W, H, px, py, jitter draws (x, y), lens draws (x, y) -> o[3], d[3] */
+void ffo_probe_camera(const float* inv16, float lens, float focal, float jitter, int W, int H, int px, int py,
+                      const float* jit2, const float* lens2, float* out6)
+{
+    ffo_render_desc d;
+    memset(&d, 0, sizeof(d));
+    for (int k = 0; k < 16; ++k) d.cam_inv[k] = inv16[k];
+    d.cam_lens_radius = lens;
+    d.cam_focal = focal;
+    d.cam_jitter = jitter;
+    d.width = W;
+    d.height = H;
+    v2 j = {jit2[0], jit2[1]}, l = {lens2[0], lens2[1]};
+    v3 o, dir;
+    camera_ray(&d, px, py, j, l, &o, &dir);
+    st3(out6, o);
+    st3(out6 + 3, dir);
+}
+/* environment: sample (ex, ey) from tables, L and pdf of a direction */
+void ffo_probe_env(const float* rgb, int w, int h, const double* marginal, const double* cond, const float* pdf,
+                   const float* pos3, float ex, float ey, const float* q3, float* out)
+{
+    ffo_render_desc d;
+    memset(&d, 0, sizeof(d));
+    d.env_rgb = rgb;
+    d.env_w = w;
+    d.env_h = h;
+    light_ctx lc;
+    memset(&lc, 0, sizeof(lc));
+    lc.d = &d;
+    lc.is_env = 1;
+    lc.marginal = marginal;
+    lc.cond = cond;
+    lc.pdf = pdf;
+    v3 wi, sp;
+    env_sample(&lc, ld3(pos3), ex, ey, &wi, &sp);
+    st3(out, wi);
+    st3(out + 3, sp);
+    st3(out + 6, env_L(&d, ld3(q3)));
+    out[9] = env_pdf(&lc, ld3(q3));
+}
+/* area light: sample point from draws (x, y), L(wi), pdf with redraw (x, y), rect hit */
+void ffo_probe_area(const ffo_area_light* L, const float* pos3, const float* u2, const float* wi3, const float* u2pdf,
+                    const float* ray8, float* out)
+{
+    rect_t r = make_rect(L);
+    v2 u = {u2[0], u2[1]}, up = {u2pdf[0], u2pdf[1]};
+    v3 sp = rect_sample(&r, u);
+    st3(out, sp);
+    st3(out + 3, normalize(sub(sp, ld3(pos3))));
+    st3(out + 6, rect_L(&r, ld3(wi3)));
+    out[9] = rect_pdf(&r, ld3(pos3), up);
+    v3 o = V(ray8[0], ray8[1], ray8[2]), dd = V(ray8[4], ray8[5], ray8[6]);
+    out[10] = (float)rect_hit(&r, o, dd);
+}
