@@ -34,13 +34,19 @@ def test_env_tables_match_oracle(ctx, oracle, w, h):
     ds = ff.dScene(ctx, scn)
     gm, gc, gp, gd = _tables(ds, w, h)
     rm, rc, rp, rd = oracle.env_build(scn.env_rgb)
-    # FP64 sums reassociated into block reductions and scans: agreement to ~1e-13 relative
-    assert abs(gd - rd) <= 1e-12 * abs(rd)
-    assert np.allclose(gm, rm, rtol=1e-11, atol=0)
+    # The FP64 sums are reassociated into block reductions and scans, and the
+    # float sine of a row (sin(M_PI * v), a float in the reference) can land
+    # one float ulp away from the host libm's sinf (row 6 of 64 does: glibc
+    # returns 0.2902847, the device's correctly rounded double sine gives
+    # 0.29028466).  That row's marginal pdf then differs by up to one float
+    # ulp (6e-8 relative) and the denominator by ~1e-10; the conditional CDFs
+    # are normalised per row and agree to 1e-15.
+    assert abs(gd - rd) <= 1e-8 * abs(rd)
+    assert np.allclose(gm, rm, rtol=1.2e-7, atol=0)
     ok = np.isfinite(rc)
     assert np.array_equal(ok, np.isfinite(gc))        # rows of zero probability are NaN in both
-    assert np.allclose(gc[ok], rc[ok], rtol=1e-11, atol=1e-300)
-    assert np.allclose(gp, rp, rtol=2e-7, atol=0)       # the float pdf may differ in its last bit
+    assert np.allclose(gc[ok], rc[ok], rtol=1e-12, atol=1e-300)
+    assert np.allclose(gp, rp, rtol=1e-6, atol=0)       # the float pdf may differ in its last bits
     assert abs(gm[-1] - 1.0) < 1e-9                      # a normalised marginal CDF
     ds.close()
 
@@ -56,8 +62,16 @@ def test_env_render_parity(ctx, oracle):
         ref, (re, rs) = oracle.render(scn, 64, 64, 4, max_depth=4, rr_depth=3, seed=11, mode=mode, light=-1,
                                       threads=cpu_threads())
         got = rgba[..., :3].astype(np.float64)
-        mre = float(np.abs(got - ref).sum() / np.abs(ref).sum())
-        print(f"[parity] env mode={mode}: mre={mre:.3e} ext={st['extension_rays']}/{re} shadow={st['shadow_rays']}/{rs}")
+        # parity mode keeps the reference's non-finite pixels (its env pdf divides
+        # by sin(acos(wi.z)), which is 0 at the poles of the z axis): they must
+        # occur at the same pixels on both sides
+        bad_g, bad_r = ~np.isfinite(got), ~np.isfinite(ref)
+        fin = ~(bad_g | bad_r)
+        mre = float(np.abs(got[fin] - ref[fin]).sum() / np.abs(ref[fin]).sum())
+        print(f"[parity] env mode={mode}: mre={mre:.3e} nonfinite gpu={int(bad_g.sum())} oracle={int(bad_r.sum())} "
+              f"ext={st['extension_rays']}/{re} shadow={st['shadow_rays']}/{rs}")
+        assert np.array_equal(bad_g, bad_r)
+        assert bad_g.mean() < 0.01
         assert mre <= 1e-4
         assert np.all(n == 4)
         pt.close()
