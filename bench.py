@@ -1,19 +1,25 @@
-"""Benchmark: BVH trace throughput (Mrays/s) on the trace micro-benchmark workload.
+"""Benchmark of the wavefront path tracer: Mrays/s (BVH trace).
 
-Workload (one step): the 4,120-triangle small room (24-triangle box + 64x32
-UV sphere), four batches of rays traced through the public ff_trace entry
-point: 16,777,216 coherent pinhole camera rays (4096 x 4096 pixel centres)
-and 16,777,216 incoherent rays (origins uniform in the scene box, directions
-uniform on the sphere), each once closest-hit and once any-hit with tmax ~
-U[0.1, 10] x scene diagonal.  67,108,864 ray queries per step per GPU.
+Default workload (`--workload render`), one step = one full render:
+  an icosphere subdivided 8 times (1,310,720 triangles) displaced by 4-octave
+  value noise inside a 12-triangle room, 33 materials of 5 kinds (the
+  reference's mix material on the room; diffuse, GGX conductor, thin GGX
+  dielectric and coated diffuse on the sphere, grouped by 3D noise), a
+  2048 x 1024 sky with a 0.5 degree sun of radiance 5e4 as the light;
+  1920 x 1080 at 64 samples per pixel, maximum depth 8, Russian roulette after
+  depth 3, corrected mode.  Rays = extension (closest-hit) + shadow (any-hit)
+  queries the wavefront traced.  Every step renders 64 new samples per pixel.
+`value` is whole-job rays per second with the scene resident in HBM (weak
+scaling: every rank renders its own frame).  `e2e` times the same render
+through the public entry points with the camera uploaded from and the image
+read back to pinned host memory every step.
 
-`value` is whole-job ray queries per second with rays resident in HBM
-(weak scaling: every rank traces its own full ray set).  `e2e` is the same
-metric through ff_trace with pinned host buffers: the host-to-device copy of
-the rays and the device-to-host copy of the hits are inside the timed region.
+`--workload trace`: the trace micro-benchmark (4,120-triangle room, 16M
+coherent + 16M incoherent rays, closest-hit and any-hit through ff_trace).
+The render line reports it in config.trace_micro when --with-trace is given.
 
 Usage:
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload render|trace]
 Under torchrun every rank runs one GPU; rank 0 prints one JSON line.
 """
 from __future__ import annotations
@@ -34,9 +40,12 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "Mrays/s (BVH trace)"
-WORKLOAD = "trace micro: small room 4120 tris, 16M coherent + 16M incoherent rays, closest + any-hit"
+RENDER_WORKLOAD = ("wavefront path tracer at scale: displaced icosphere 1,310,720 tris in a 12-tri room, 5 material "
+                   "kinds, 2048x1024 sky + sun, 1920x1080, 64 spp, depth 8")
+TRACE_WORKLOAD = "trace micro: small room 4120 tris, 16M coherent + 16M incoherent rays, closest + any-hit"
 RAYS_PER_SET = 4096 * 4096
 RAY_BYTES, HIT_BYTES = 32, 16
+RENDER = dict(width=1920, height=1080, spp=64, max_depth=8, rr_depth=3)
 
 
 def dist_env():
@@ -57,19 +66,6 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def build_workload(n_per_set: int, seed_offset: int):
-    from firefly_b200 import scenes
-    scn = scenes.small_room(seed=0)
-    side = int(round(math.sqrt(n_per_set)))
-    coh = scenes.camera_rays(scn, side, side)
-    inc = scenes.incoherent_rays(scn, side * side, seed=1 + seed_offset)
-    coh_any = scenes.with_random_tmax(coh, scn, seed=2 + seed_offset)
-    inc_any = scenes.with_random_tmax(inc, scn, seed=3 + seed_offset)
-    batches = [("coherent_closest", coh, False), ("incoherent_closest", inc, False),
-               ("coherent_any", coh_any, True), ("incoherent_any", inc_any, True)]
-    return scn, batches
-
-
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -80,7 +76,7 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = Path(os.environ.get("FF_CLOCK_LOG", f"/tmp/ff_clocks_{os.getpid()}.csv"))
+        self.path = Path(f"/tmp/ff_clocks_{os.getpid()}.csv")
 
     def start(self):
         try:
@@ -118,24 +114,60 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ------------------------------------------------------------------ workloads
+def render_scene():
+    from firefly_b200 import scenes
+    return scenes.displaced_icosphere(subdiv=8, width=RENDER["width"], height=RENDER["height"])
+
+
+def trace_batches(n_per_set: int, seed_offset: int):
+    from firefly_b200 import scenes
+    scn = scenes.small_room(seed=0)
+    side = int(round(math.sqrt(n_per_set)))
+    coh = scenes.camera_rays(scn, side, side)
+    inc = scenes.incoherent_rays(scn, side * side, seed=1 + seed_offset)
+    coh_any = scenes.with_random_tmax(coh, scn, seed=2 + seed_offset)
+    inc_any = scenes.with_random_tmax(inc, scn, seed=3 + seed_offset)
+    return scn, [("coherent_closest", coh, False), ("incoherent_closest", inc, False),
+                 ("coherent_any", coh_any, True), ("incoherent_any", inc_any, True)]
+
+
 # ------------------------------------------------------------- CPU baselines
+def cpu_render_rate(scn, target_s: float, threads: int):
+    """The reference's own path tracer compiled for the host (oracle/_ref:
+    its gen_ray, SAH BVH, intersect(), lights and BRDF_L/BRDF_f/BRDF_pdf with
+    their inline visibility rays) on every k-th pixel of the frame at the
+    workload's spp and depth.  Returns (Mrays/s, kind, sample text, seconds)."""
+    from oracle import ffref
+    if not ffref.available():
+        return None
+    W, H = RENDER["width"], RENDER["height"]
+    # calibrate on a sparse sample, then size the timed sample to target_s
+    stride = 4099
+    _, st, ms = ffref.render(scn, W, H, RENDER["spp"], RENDER["max_depth"], RENDER["rr_depth"], light=-1,
+                             threads=threads, pixel_stride=stride)
+    per_pixel_s = ms[0] / 1e3 / max(1, st[2] // RENDER["spp"])
+    n_pix = max(64, int(target_s / max(per_pixel_s, 1e-9)))
+    stride = max(1, (W * H) // n_pix)
+    _, st, ms = ffref.render(scn, W, H, RENDER["spp"], RENDER["max_depth"], RENDER["rr_depth"], light=-1,
+                             threads=threads, pixel_stride=stride)
+    rays = st[0] + st[1]
+    desc = (f"every {stride}th pixel of the 1920x1080 frame ({st[2] // RENDER['spp']} pixels x {RENDER['spp']} spp, "
+            f"{rays} rays, {ms[0] / 1e3:.1f} s) with the reference's host-compiled path tracer on {threads} threads; "
+            f"its SAH BVH build took {ms[1] / 1e3:.1f} s (not timed)")
+    return rays / (ms[0] / 1e3) / 1e6, "reference", desc, ms[0] / 1e3
+
+
 def cpu_trace_rate(batches, target_s: float, threads: int):
-    """Time the reference's own BVH + intersect()/intersect_shadows(), compiled
-    for the host (oracle/_ref), over a strided sample of every batch.  Falls
-    back to the oracle's brute-force restatement when the reference build is
-    absent.  Returns (Mrays/s, kind, sample description)."""
+    """The reference's BVH + intersect()/intersect_shadows() compiled for the
+    host on a strided sample of every trace batch."""
     import ctypes as C
-    from oracle import ffo
+    from oracle import ffo, ffref
     from firefly_b200 import scenes
     scn = scenes.small_room(seed=0)
     tris = scn.triangle_soup()
-    ref_path = ffo.REF_LIB
-    if ref_path.exists():
-        lib = C.CDLL(str(ref_path))
-        P = C.c_void_p
-        lib.ffref_bvh_build.restype = P
-        lib.ffref_bvh_build.argtypes = [P, C.c_int, C.POINTER(C.c_double)]
-        lib.ffref_bvh_trace.argtypes = [P, P, C.c_long, P, C.c_int, C.c_int]
+    if ffref.available():
+        lib = ffref.load()
         ms = C.c_double()
         h = lib.ffref_bvh_build(tris.ctypes.data, len(tris), C.byref(ms))
 
@@ -147,7 +179,7 @@ def cpu_trace_rate(batches, target_s: float, threads: int):
         def run(rays, any_hit):
             ffo.trace_brute(tris, rays, any_hit=any_hit, threads=threads)
         kind = "port"
-    # calibrate on a small sample, then size the timed sample to target_s
+
     def sample(n):
         return [(np.ascontiguousarray(r[:: max(1, len(r) // n)][:n]), a) for _, r, a in batches]
     probe = sample(4096)
@@ -171,19 +203,31 @@ def run_reference(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    _, batches = build_workload(RAYS_PER_SET, 0)
     rates = []
     kind = desc = None
-    for i in range(args.warmup + args.steps):
-        rate, kind, desc, _ = cpu_trace_rate(batches, target_s=args.ref_step_s, threads=threads)
-        if i >= args.warmup:
-            rates.append(rate)
+    if args.workload == "render":
+        scn = render_scene()
+        for i in range(args.warmup + args.steps):
+            r = cpu_render_rate(scn, target_s=args.ref_step_s, threads=threads)
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libffref.so was not built"}))
+                return 0
+            rate, kind, desc, _ = r
+            if i >= args.warmup:
+                rates.append(rate)
+        workload, cfg = RENDER_WORKLOAD, dict(RENDER)
+    else:
+        _, batches = trace_batches(RAYS_PER_SET, 0)
+        for i in range(args.warmup + args.steps):
+            rate, kind, desc, _ = cpu_trace_rate(batches, target_s=args.ref_step_s, threads=threads)
+            if i >= args.warmup:
+                rates.append(rate)
+        workload, cfg = TRACE_WORKLOAD, {"rays_per_step": 4 * RAYS_PER_SET}
     value = statistics.median(rates)
     line = {"metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": WORKLOAD, "rays_per_step": 4 * RAYS_PER_SET},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": workload, **cfg},
             "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": kind,
                              "sample": desc},
             "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -192,7 +236,7 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ our arm
-def run_ours(args):
+def setup_dist():
     import torch
     ws, rank, local = dist_env()
     dist = None
@@ -201,18 +245,24 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    import firefly_b200 as ff
+    return ws, rank, local, dist
 
-    # a dedicated stream shared by the library and the timing events
-    stream = torch.cuda.Stream(dev)
-    torch.cuda.set_stream(stream)
-    ctx = ff.Context(local, stream=stream.cuda_stream)
-    assert ctx.stream == stream.cuda_stream
-    scn, batches = build_workload(args.rays, seed_offset=17 * rank)
+
+def max_over_ranks(dist, dev, x: float) -> float:
+    import torch
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def trace_micro(ctx, ds_dev, args, rank, dev, stream, barrier, steps):
+    """Trace micro-benchmark on this rank; returns (rays per step, per-batch ms, total ms, batches, scene)."""
+    import torch
+    import firefly_b200 as ff
+    scn, batches = trace_batches(args.rays, seed_offset=17 * rank)
     ds = ff.dScene(ctx, scn)
     n = batches[0][1].shape[0]
-
     d_rays = [torch.from_numpy(r).to(dev) for _, r, _ in batches]
     d_hits = [torch.empty((len(r), 4), dtype=torch.int32, device=dev) for _, r, _ in batches]
     torch.cuda.synchronize(dev)
@@ -224,91 +274,80 @@ def run_ours(args):
             ds.trace_device(d_rays[k].data_ptr(), len(r), d_hits[k].data_ptr(), any_hit=any_hit)
             if evs is not None:
                 evs[k][1].record(stream)
+    for _ in range(3):
+        step()
+    barrier()
+    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in batches] for _ in range(steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for s in range(steps):
+        step(evs[s])
+    t1.record(stream)
+    barrier()
+    per = [statistics.mean(evs[s][k][0].elapsed_time(evs[s][k][1]) for s in range(steps)) for k in range(len(batches))]
+    total = t0.elapsed_time(t1)
+    return n * len(batches), per, total, batches, scn, ds, d_rays, d_hits
+
+
+def run_trace(args, ws, rank, local, dist):
+    import torch
+    import firefly_b200 as ff
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx = ff.Context(local, stream=stream.cuda_stream)
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize(dev)
-
-    for _ in range(args.warmup):
-        step()
-    barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    launch_evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in batches] for _ in range(args.steps)]
-    t0.record(stream)
-    for s in range(args.steps):
-        step(launch_evs[s])
-    t1.record(stream)
-    barrier()
+    rays_per_step, per, total_ms, batches, scn, ds, d_rays, d_hits = trace_micro(ctx, None, args, rank, dev, stream,
+                                                                                barrier, args.steps)
     clk = clocks.stop()
-    ms = t0.elapsed_time(t1)
-    per_batch_ms = [statistics.mean(launch_evs[s][k][0].elapsed_time(launch_evs[s][k][1]) for s in range(args.steps))
-                    for k in range(len(batches))]
-    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    rays_per_step = n * len(batches)
+    ms_max = max_over_ranks(dist, dev, total_ms)
     value = ws * rays_per_step * args.steps / (ms_max / 1e3) / 1e6
-
-    # end-to-end through the public entry point with pinned host buffers
+    n = batches[0][1].shape[0]
+    # end to end through ff_trace with pinned host buffers
     h_rays = [torch.from_numpy(r).pin_memory() for _, r, _ in batches]
     h_hits = [torch.empty((len(r), 4), dtype=torch.int32).pin_memory() for _, r, _ in batches]
-    h_views = [(hr.numpy(), hh.numpy().view(np.uint8).view(ff.HIT_DTYPE).reshape(-1)) for hr, hh in zip(h_rays, h_hits)]
+    views = [(hr.numpy(), hh.numpy().view(np.uint8).view(ff.HIT_DTYPE).reshape(-1)) for hr, hh in zip(h_rays, h_hits)]
 
     def e2e_step():
         for k, (_, r, any_hit) in enumerate(batches):
-            ds.trace(h_views[k][0], any_hit=any_hit, out=h_views[k][1])
-
-    for _ in range(max(1, min(args.warmup, 2))):
-        e2e_step()
+            ds.trace(views[k][0], any_hit=any_hit, out=views[k][1])
+    e2e_step()
     barrier()
     e2e_steps = max(1, min(args.steps, 5))
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(e2e_steps):
         e2e_step()
     e1.record(stream)
     barrier()
-    e_ms = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
-    if dist is not None:
-        dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
-    e2e_value = ws * rays_per_step * e2e_steps / (float(e_ms.item()) / 1e3) / 1e6
-
-    # correctness spot check of the timed outputs against the host path
-    check = batches[1][1][:50_000]
-    ok = np.array_equal(ds.trace(check)["prim"], h_views[1][1][:50_000]["prim"])
-
+    e_ms = max_over_ranks(dist, dev, e0.elapsed_time(e1))
+    e2e_value = ws * rays_per_step * e2e_steps / (e_ms / 1e3) / 1e6
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        # roofline of the dominant kernel (closest-hit trace of incoherent rays):
-        # algorithmic bytes = 32 B ray in + 16 B hit out per ray
-        k_dom = int(np.argmax(per_batch_ms))
-        achieved = n * (RAY_BYTES + HIT_BYTES) / (per_batch_ms[k_dom] / 1e3) / 1e9
+        k_dom = int(np.argmax(per))
+        achieved = n * (RAY_BYTES + HIT_BYTES) / (per[k_dom] / 1e3) / 1e9
         cpu = None
         if not args.no_cpu:
             rate, kind, desc, _ = cpu_trace_rate(batches, target_s=args.cpu_s, threads=os.cpu_count() or 1)
-            cpu = {"value": round(rate, 3), "unit": "Mrays/s", "cores": os.cpu_count() or 1, "kind": kind,
-                   "sample": desc}
+            cpu = {"value": round(rate, 3), "unit": "Mrays/s", "cores": os.cpu_count() or 1, "kind": kind, "sample": desc}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "rays_per_step": rays_per_step, "triangles": scn.num_triangles,
-                       "bvh_nodes": ds.stats()["num_nodes"], "bvh_depth": ds.stats()["bvh_depth"],
+            "config": {"workload": TRACE_WORKLOAD, "rays_per_step": rays_per_step, "triangles": scn.num_triangles,
                        "l2": "inputs larger than L2 (512 MiB of rays per batch)", "parallelism": f"replicas{ws}",
-                       "per_batch_mrays": {b[0]: round(n / (t / 1e3) / 1e6, 1) for b, t in zip(batches, per_batch_ms)},
-                       "hits_match_host_path": bool(ok)},
+                       "per_batch_mrays": {b[0]: round(n / (t / 1e3) / 1e6, 1) for b, t in zip(batches, per)}},
             "roofline": {"bound": "hbm", "kernel": f"k_trace ({batches[k_dom][0]})", "achieved": round(achieved, 2),
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": None,
                          "peak_source": peak_kind, "bytes_per_ray": RAY_BYTES + HIT_BYTES},
             "cpu_baseline": cpu,
-            "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
-                    "h2d_bytes_per_step": int(rays_per_step * RAY_BYTES),
+            "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": int(rays_per_step * RAY_BYTES),
                     "d2h_bytes_per_step": int(rays_per_step * HIT_BYTES)},
             "gpu_launches": len(batches) * args.steps,
             "clocks": clk,
@@ -316,28 +355,162 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     ds.close()
     ctx.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    return 0
+
+
+def run_render(args, ws, rank, local, dist):
+    import torch
+    import firefly_b200 as ff
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx = ff.Context(local, stream=stream.cuda_stream)
+    assert ctx.stream == stream.cuda_stream
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    scn = render_scene()
+    ds = ff.dScene(ctx, scn)
+    W, H = RENDER["width"], RENDER["height"]
+    pt = ff.PathTracer(ctx, W, H)
+    kw = dict(spp=RENDER["spp"], max_depth=RENDER["max_depth"], rr_depth=RENDER["rr_depth"], light=-1,
+              mode=ff.FF_MODE_CORRECTED, seed=1000 * rank)
+    step_no = [0]
+
+    def step(profile=False):
+        pt.clear_buffer()
+        st = pt.draw(ds, sample_offset=RENDER["spp"] * step_no[0], profile=profile, **kw)
+        step_no[0] += 1
+        return st
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    t0.record(stream)
+    for _ in range(args.steps):
+        stats.append(step())
+    t1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms_max = max_over_ranks(dist, dev, t0.elapsed_time(t1))
+    rays = sum(s["extension_rays"] + s["shadow_rays"] for s in stats)
+    rays_max = max_over_ranks(dist, dev, float(rays))
+    value = ws * rays_max / (ms_max / 1e3) / 1e6
+    samples = sum(s["samples"] for s in stats)
+    # one profiled step (outside the timed region): per-stage device time
+    prof = step(profile=True)
+    # end to end through the public entry points: camera in, image out, pinned host memory
+    img = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    cnt = torch.empty((H, W), dtype=torch.int32).pin_memory()
+    cam = scn.camera
+    import ctypes as C
+    lib = ff.lib()
+
+    def e2e_step():
+        ds.update(cam)
+        pt.clear_buffer()
+        st = pt.draw(ds, sample_offset=RENDER["spp"] * step_no[0], **kw)
+        step_no[0] += 1
+        rc = lib.ff_film_read(pt.film, C.c_void_p(img.data_ptr()), C.c_void_p(cnt.data_ptr()), 0)
+        assert rc == 0
+        return st
+    e2e_step()
+    barrier()
+    e2e_steps = max(1, min(args.steps, 3))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    est = []
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        est.append(e2e_step())
+    e1.record(stream)
+    barrier()
+    e_ms = max_over_ranks(dist, dev, e0.elapsed_time(e1))
+    e_rays = sum(s["extension_rays"] + s["shadow_rays"] for s in est)
+    e2e_value = ws * e_rays / (e_ms / 1e3) / 1e6
+    image = img.numpy()[..., :3] / np.maximum(cnt.numpy(), 1)[..., None]
+    finite = bool(np.isfinite(image).all())
+
+    trace = None
+    if args.with_trace:
+        rps, per, total, batches, tscn, tds, _, _ = trace_micro(ctx, None, args, rank, dev, stream, barrier, 3)
+        trace = {"workload": TRACE_WORKLOAD, "mrays": round(rps * 3 / (total / 1e3) / 1e6, 1),
+                 "per_batch_mrays": {b[0]: round(len(b[1]) / (t / 1e3) / 1e6, 1) for b, t in zip(batches, per)}}
+        tds.close()
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        # dominant kernel: the shadow-ray trace (k_trace<any>) or the extension trace
+        stage = {"k_trace<any> (shadow queue)": (prof["ms_trace_shadow"], prof["shadow_rays"]),
+                 "k_trace<closest> (extension queue)": (prof["ms_trace_extension"], prof["extension_rays"])}
+        dom = max(stage, key=lambda k: stage[k][0])
+        dms, drays = stage[dom]
+        achieved = drays * (RAY_BYTES + HIT_BYTES) / (dms / 1e3) / 1e9
+        cpu = None
+        if not args.no_cpu:
+            r = cpu_render_rate(scn, target_s=args.cpu_s, threads=os.cpu_count() or 1)
+            if r is not None:
+                cpu = {"value": round(r[0], 3), "unit": "Mrays/s", "cores": os.cpu_count() or 1, "kind": r[1],
+                       "sample": r[2]}
+        pstat = {k: round(prof[k], 2) for k in ("ms_total", "ms_logic", "ms_shade", "ms_trace_extension", "ms_trace_shadow")}
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": RENDER_WORKLOAD, **RENDER, "triangles": scn.num_triangles,
+                       "bvh_nodes": ds.stats()["num_nodes"], "bvh_build_ms": round(ds.stats()["build_ms"], 2),
+                       "mode": "corrected", "light": "environment (importance-sampled sky + sun)",
+                       "rays_per_step": int(rays / args.steps), "msamples_per_s": round(ws * samples / (ms_max / 1e3) / 1e6, 2),
+                       "frames_per_step": stats[-1]["frames"], "stage_ms_profiled_step": pstat,
+                       "l2": "each step traces ~1.3G rays over a 0.27 GB scene; per-step state and queues ~0.5 GB",
+                       "parallelism": f"replicas{ws}", "image_finite": finite, "trace_micro": trace},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 5), "traffic": None, "peak_source": peak_kind,
+                         "bytes_per_ray": RAY_BYTES + HIT_BYTES},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 80,
+                    "d2h_bytes_per_step": int(W * H * (16 + 4))},
+            "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    pt.close()
+    ds.close()
+    ctx.close()
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--rays", type=int, default=RAYS_PER_SET, help="rays per batch (4 batches per step)")
-    ap.add_argument("--cpu-s", type=float, default=12.0, help="target seconds of CPU baseline work")
-    ap.add_argument("--ref-step-s", type=float, default=4.0, help="reference arm: seconds of CPU work per step")
+    ap.add_argument("--workload", choices=["render", "trace"], default="render")
+    ap.add_argument("--rays", type=int, default=RAYS_PER_SET, help="trace workload: rays per batch")
+    ap.add_argument("--cpu-s", type=float, default=15.0, help="target seconds of CPU-baseline work")
+    ap.add_argument("--ref-step-s", type=float, default=6.0, help="reference arm: seconds of CPU work per step")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--with-trace", action="store_true", help="also run the trace micro-benchmark (render line)")
+    ap.add_argument("--spp", type=int, default=RENDER["spp"], help="render workload: samples per pixel per step")
     args = ap.parse_args(argv)
+    RENDER["spp"] = args.spp
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
-    return run_ours(args)
+    ws, rank, local, dist = setup_dist()
+    if args.workload == "render":
+        run_render(args, ws, rank, local, dist)
+    else:
+        run_trace(args, ws, rank, local, dist)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
 
 
 if __name__ == "__main__":

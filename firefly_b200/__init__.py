@@ -188,10 +188,11 @@ class PathTracer:
 
     def draw(self, scene: dScene, spp: int = 1, max_depth: int = 3, rr_depth: int = 3, seed: int = 0,
              mode: int = A.FF_MODE_PARITY, light: int = -1, max_paths: int = 0, sample_offset: int = 0,
-             shadow_offset: float = 0.001) -> dict:
+             shadow_offset: float = 0.001, profile: bool = False) -> dict:
+        """PathTracer::draw: render `spp` more samples per pixel into the film."""
         s = A.ff_render_settings(spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed, mode=mode,
-                                 light=light, max_paths=max_paths, sample_offset=sample_offset, flags=0,
-                                 shadow_offset=shadow_offset)
+                                 light=light, max_paths=max_paths, sample_offset=sample_offset,
+                                 flags=A.FF_RENDER_PROFILE if profile else 0, shadow_offset=shadow_offset)
         st = A.ff_render_stats()
         _check(lib().ff_render(self.ctx.handle, scene.handle, C.byref(s), self.film, C.byref(st)), self.ctx.handle)
         self.last_stats = {k: getattr(st, k) for k, _ in st._fields_}

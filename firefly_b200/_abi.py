@@ -25,6 +25,7 @@ FF_MEM_HOST = 0
 FF_MEM_DEVICE = 1
 FF_TRACE_CLOSEST = 0
 FF_TRACE_ANY = 2
+FF_RENDER_PROFILE = 1
 FF_MODE_PARITY = 0
 FF_MODE_CORRECTED = 1
 
@@ -87,7 +88,8 @@ class ff_render_settings(C.Structure):
 class ff_render_stats(C.Structure):
     _fields_ = [("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("samples", C.c_uint64),
                 ("frames", C.c_uint32), ("ms_total", C.c_float), ("ms_trace_extension", C.c_float),
-                ("ms_trace_shadow", C.c_float), ("ms_logic", C.c_float), ("ms_shade", C.c_float)]
+                ("ms_trace_shadow", C.c_float), ("ms_logic", C.c_float), ("ms_shade", C.c_float),
+                ("kernel_launches", C.c_uint32)]
 
 
 # Every symbol include/firefly_b200.h declares, with its ctypes signature.

@@ -303,9 +303,13 @@ FF_D int upper_bound_ref(const double* list, int size, float val)
     return left;
 }
 
-FF_D float3 env_L(const FFEnvView& e, float3 wi)
+// dEnvironmentLight::L (dEnvironmentLight.cu:60-72).  A normalised direction
+// can carry a component one ulp above 1, where asinf returns NaN; the
+// reference keeps that NaN (parity), corrected mode clamps it.
+FF_D float3 env_L(const FFEnvView& e, float3 wi, bool corrected = false)
 {
     if (!e.rgb) return e.color;
+    if (corrected) wi.y = clampf(wi.y, -1.f, 1.f);
     float2 uv = spherical_map(wi);
     return tex_bilinear(e.rgb, e.width, e.height, uv.x, uv.y);
 }

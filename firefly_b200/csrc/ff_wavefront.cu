@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             float4 acc = w.acc[s], accc = w.acc_c[s];
             bool terminate = (L > w.max_depth) || !found;
             // kernel.cu:332-338: environment radiance on a camera-ray miss
-            if (!found && L == 1) kahan_add(acc, accc, beta * env_L(w.env, rd));
+            if (!found && L == 1) kahan_add(acc, accc, beta * env_L(w.env, rd, w.mode == FF_MODE_CORRECTED));
             if (L > 1) {
                 // kernel.cu:357-359: light_brdf * beta when the NEE ray was unoccluded
                 const int4 q = w.sh_q[s];
@@ -192,7 +192,11 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                     if (L > w.rr_depth) {
                         const float q_rr = hmax(0.05f, 1.f - beta.y);
                         if (ff_rand(key, dim_of(L, DIM_RR)) < q_rr) terminate = true;
-                        else if (w.mode == FF_MODE_CORRECTED) beta = beta / (1.f - q_rr);
+                        else if (w.mode == FF_MODE_CORRECTED) {
+                            // a draw of exactly 1.0 survives q = 1: no finite compensation exists
+                            if (q_rr >= 1.f) terminate = true;
+                            else beta = beta / (1.f - q_rr);
+                        }
                     }
                 }
             }
@@ -280,7 +284,7 @@ struct LightCtx {
 
 __device__ __forceinline__ float3 light_L(const LightCtx& lc, float3 wi)
 {
-    return lc.is_env ? env_L(lc.w->env, wi) : rect_L(lc.rect, wi);
+    return lc.is_env ? env_L(lc.w->env, wi, lc.corrected) : rect_L(lc.rect, wi);
 }
 __device__ __forceinline__ float light_pdf(const LightCtx& lc, float3 pos, float3 wi, uint32_t key, uint32_t L,
                                            uint32_t dim)
@@ -755,6 +759,18 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     k_init<<<(P + 255) / 256, 256, 0, stream>>>(w, st->spp, st->sample_offset);
     FF_CUDA_CHECK(cudaGetLastError());
     int shade_blocks = ctx->num_sms * 8;
+    int n_kinds = 0;
+    for (int k = 0; k < kKinds; ++k) n_kinds += kind_used[k] ? 1 : 0;
+    // Optional per-stage timing: events around the stages of every frame.
+    const bool profile = stats && (st->flags & FF_RENDER_PROFILE);
+    std::vector<cudaEvent_t> evs;
+    auto mark = [&](void) {
+        if (!profile) return;
+        cudaEvent_t e;
+        FF_CUDA_CHECK(cudaEventCreate(&e));
+        FF_CUDA_CHECK(cudaEventRecord(e, stream));
+        evs.push_back(e);
+    };
     uint32_t frames = 0;
     uint32_t active = 1;
     if (!ws->h_active) FF_CUDA_CHECK(cudaMallocHost(&ws->h_active, sizeof(uint32_t)));
@@ -764,16 +780,21 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
         // a batch of frames between host checks
         for (int b = 0; b < 4; ++b) {
             k_reset_counters<<<1, 32, 0, stream>>>(w.ctr, ws->trace_ctr);
+            mark();
             k_logic<<<(P + 255) / 256, 256, 0, stream>>>(w);
+            mark();
             if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX><<<shade_blocks, 128, 0, stream>>>(w);
             if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE><<<shade_blocks, 128, 0, stream>>>(w);
             if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR><<<shade_blocks, 128, 0, stream>>>(w);
             if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC><<<shade_blocks, 128, 0, stream>>>(w);
             if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT><<<shade_blocks, 128, 0, stream>>>(w);
             FF_CUDA_CHECK(cudaGetLastError());
+            mark();
             ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err);
+            mark();
             ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, w.sh_hits, true, ws->trace_ctr + 1,
                                   ws->err);
+            mark();
             ++frames;
         }
         FF_CUDA_CHECK(cudaMemcpyAsync(h_active, w.ctr + C_ACTIVE, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
@@ -794,6 +815,23 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     if (stats) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        if (profile) {
+            // 5 marks per frame: logic | shade | trace ext | trace shadow
+            float t[4] = {0.f, 0.f, 0.f, 0.f};
+            for (size_t f = 0; f + 4 < evs.size() + 1 && f + 4 <= evs.size(); f += 5) {
+                for (int k = 0; k < 4; ++k) {
+                    float x = 0.f;
+                    cudaEventElapsedTime(&x, evs[f + k], evs[f + k + 1]);
+                    t[k] += x;
+                }
+            }
+            stats->ms_logic = t[0];
+            stats->ms_shade = t[1];
+            stats->ms_trace_extension = t[2];
+            stats->ms_trace_shadow = t[3];
+        }
+        for (auto e : evs) cudaEventDestroy(e);
+        stats->kernel_launches = frames * (3u + (uint32_t)n_kinds) + 2u;
         stats->extension_rays = totals[0];
         stats->shadow_rays = totals[1];
         stats->samples = (uint64_t)st->spp * WH;

@@ -244,6 +244,8 @@ FF_API ff_status ff_film_tonemap(ff_film* film, float exposure, uint8_t* rgba8, 
 
 /* ----------------------------------------------------------------- render */
 
+#define FF_RENDER_PROFILE 1u  /* ff_render_settings.flags: time every stage with CUDA events */
+
 #define FF_MODE_PARITY    0u  /* reproduce the reference's behaviours, see DESIGN */
 #define FF_MODE_CORRECTED 1u  /* unbiased RR, offset extension rays, fixed MIS gating */
 
@@ -266,7 +268,9 @@ typedef struct ff_render_stats {
     uint64_t samples;           /* completed paths */
     uint32_t frames;            /* wavefront iterations */
     float ms_total;
+    /* per-stage device time, filled with FF_RENDER_PROFILE */
     float ms_trace_extension, ms_trace_shadow, ms_logic, ms_shade;
+    uint32_t kernel_launches;   /* kernels this call launched */
 } ff_render_stats;
 
 /* Replaces PathTracer::draw + wavefront_pathtrace (PathTracer.cpp:59-79,

@@ -37,11 +37,31 @@ static thread_local const uint32_t* g_seq = nullptr;
 static thread_local int g_seq_n = 0;
 static thread_local int g_seq_i = 0;
 
+// Without a sequence (the timed renders), clock() advances a per-thread
+// counter so every random() call draws a new value, as a running clock does.
+static thread_local uint32_t g_free_clock = 0;
+
 long ffref_clock(void)
 {
     if (g_seq && g_seq_i < g_seq_n) return (long)g_seq[g_seq_i++];
     ++g_seq_i;
+    if (!g_seq) return (long)(g_free_clock += 7919u);
     return 0;
+}
+
+// Every visibility query of the reference goes through intersect_shadows
+// (dTriangle.cu:215-259), called from the lights' visible().  The library is
+// linked with --wrap for that symbol so the renders can count the rays.
+static thread_local uint64_t g_shadow_calls = 0;
+extern "C" bool __real__Z17intersect_shadowsPK13LinearBVHNodePK9dTriangleRK4dRayRf(const LinearBVHNode*,
+                                                                                  const dTriangle*, const dRay&,
+                                                                                  float&);
+extern "C" bool __wrap__Z17intersect_shadowsPK13LinearBVHNodePK9dTriangleRK4dRayRf(const LinearBVHNode* n,
+                                                                                  const dTriangle* t, const dRay& r,
+                                                                                  float& tmin)
+{
+    ++g_shadow_calls;
+    return __real__Z17intersect_shadowsPK13LinearBVHNodePK9dTriangleRK4dRayRf(n, t, r, tmin);
 }
 
 // ---------------------------------------------------- texture emulation
@@ -103,6 +123,10 @@ void ffref_surf_read_float(unsigned long long obj, int x_bytes, int y, float* ou
 }
 
 extern "C" {
+void ffref_env_free(void* h);
+void ffref_area_free(void* h);
+void* ffref_env_create(const float* rgb, int w, int h);
+void* ffref_area_create(const float* rect12, float radiance, const float* emissive3);
 
 // ------------------------------------------------------------------ misc
 void ffref_set_clock(const uint32_t* seq, int n)
@@ -571,6 +595,170 @@ int ffref_area_hit(void* h, const float* ray8)
     RefArea* a = (RefArea*)h;
     dRay r(make_float3(ray8[0], ray8[1], ray8[2]), make_float3(ray8[4], ray8[5], ray8[6]));
     return a->rect->hit(r) ? 1 : 0;
+}
+
+// ------------------------------------------------------------------ render
+// The reference's path tracer on the host: dCamera::gen_ray, intersect()
+// over its SAH BVH, the lights' get_direction / L / visible, and BRDF_L /
+// BRDF_f / BRDF_pdf of the mix material (with their inline visibility
+// traversals), driven by a restatement of the per-path logic of wf_logic /
+// wf_generate / wf_mat_mix / wf_extend / wf_shadow (kernel.cu:298-651): one
+// path per pixel sample, one bounce per iteration.  random() draws from the
+// free-running per-thread clock.  Pixels rendered: every `pixel_stride`-th
+// pixel (all of them for 1).  out_rgb (w*h*3 floats, may be NULL) receives
+// the radiance sums; stats[0..2] = extension rays, visibility rays, samples.
+struct RenderDesc {
+    const float* tris;           // T x 9
+    const float* normals;        // T x 9 vertex normals
+    const uint32_t* material_ids;
+    int num_tris;
+    const float* mats;           // M x 8: base[3], fresnel[3], roughness, metallic
+    int num_mats;
+    const float* env_rgb;        // env_h x env_w x 3 or NULL
+    int env_w, env_h;
+    const float* rect;           // 12 floats + radiance + emissive[3], or NULL
+    const float* cam_inv;        // 16
+    float lens_radius, focal;
+    int width, height, spp, max_depth, rr_depth, light_env, threads, pixel_stride;
+};
+
+void ffref_render(const RenderDesc* d, float* out_rgb, uint64_t* stats, double* ms)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    double bms = 0;
+    RefBVH* bvh = (RefBVH*)ffref_bvh_build(d->tris, d->num_tris, &bms);
+    std::vector<dMaterial> mats(d->num_mats);
+    for (int m = 0; m < d->num_mats; ++m) {
+        const float* p = d->mats + 8 * m;
+        mats[m].baseColorFactor = make_float3(p[0], p[1], p[2]);
+        mats[m].fresnel = make_float3(p[3], p[4], p[5]);
+        mats[m].roughnessFactor = p[6];
+        mats[m].metallicFactor = p[7];
+    }
+    // vertex normals and materials into the reordered triangles
+    for (int i = 0; i < d->num_tris; ++i) {
+        int orig = bvh->ordered[i];
+        const float* n = d->normals + 9 * (size_t)orig;
+        bvh->tris[i].v0.normal = make_float3(n[0], n[1], n[2]);
+        bvh->tris[i].v1.normal = make_float3(n[3], n[4], n[5]);
+        bvh->tris[i].v2.normal = make_float3(n[6], n[7], n[8]);
+        bvh->tris[i].material = &mats[d->material_ids ? d->material_ids[orig] : 0];
+    }
+    RefEnv* env = nullptr;
+    RefArea* area = nullptr;
+    dLight* lights[2] = {nullptr, nullptr};
+    int light_id = 0;
+    if (d->light_env) {
+        env = (RefEnv*)ffref_env_create(d->env_rgb, d->env_w, d->env_h);
+        lights[0] = env->light;
+    } else {
+        area = (RefArea*)ffref_area_create(d->rect, d->rect[12], d->rect + 13);
+        lights[0] = area->light;
+    }
+    dFilm film;
+    film.hres = d->width;
+    film.vres = d->height;
+    const int stride = d->pixel_stride > 0 ? d->pixel_stride : 1;
+    const long npix = ((long)d->width * d->height + stride - 1) / stride;
+    std::atomic<long> next{0};
+    std::atomic<uint64_t> n_ext{0}, n_sh{0}, n_samp{0};
+    auto work = [&](int tid) {
+        g_free_clock = 0x9e3779b9u * (uint32_t)(tid + 1);
+        dCamera cam;
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) cam.inv_view_proj_mat.m[i][j] = d->cam_inv[4 * i + j];
+        cam.lens_radius = d->lens_radius;
+        cam.f = d->focal;
+        uint64_t ext = 0, samples = 0;
+        g_shadow_calls = 0;
+        for (;;) {
+            long k = next.fetch_add(64);
+            if (k >= npix) break;
+            long kend = std::min(npix, k + 64);
+            for (long q = k; q < kend; ++q) {
+                long pix = q * stride;
+                int x = (int)(pix % d->width), y = (int)(pix / d->width);
+                float3 acc = make_float3(0.f);
+                for (int s = 0; s < d->spp; ++s) {
+                    // wf_generate
+                    dRay ray = cam.gen_ray(&film, make_float2((float)x, (float)y));
+                    float3 beta = make_float3(1.f);
+                    uint32_t L = 0;
+                    float3 light_brdf = make_float3(0.f), ext_brdf = make_float3(0.f);
+                    float ext_pdf = 0.f, ext_cos = 0.f;
+                    bool light_visible = false;
+                    for (;;) {
+                        // wf_extend
+                        Isect is;
+                        intersect(bvh->nodes, bvh->tris.data(), ray, is);
+                        ++ext;
+                        ++L;
+                        // wf_logic
+                        bool terminate = (L > (uint32_t)d->max_depth) || !is.wasFound;
+                        if (!is.wasFound && L == 1 && env) {
+                            float3 sp;
+                            acc += beta * env->light->L(is, ray.d, sp);
+                        }
+                        if (L > 1) {
+                            if (light_visible) acc += light_brdf * beta;
+                            if (ext_brdf == make_float3(0, 0, 0) || ext_pdf == 0.f) {
+                                terminate = true;
+                            } else {
+                                beta *= ext_brdf * ext_cos / ext_pdf;
+                                if (L > (uint32_t)d->rr_depth) {
+                                    float q_rr = fmaxf((float).05, 1 - beta.y);
+                                    if (random() < q_rr) terminate = true;
+                                }
+                            }
+                        }
+                        if (terminate) break;
+                        float3 lightdir, sample_point;
+                        lights[light_id]->get_direction(is, lightdir, sample_point);
+                        dRay shadow_ray(is.position + is.normal * 0.001f, lightdir);
+                        // wf_mat_mix
+                        const float3 wo = -ray.d;
+                        float3 ext_dir;
+                        light_brdf = BRDF_L(lights, bvh->nodes, bvh->tris.data(), is, shadow_ray.d, wo, light_id,
+                                            sample_point, ext_dir);
+                        ext_brdf = BRDF_f(is, ext_dir, wo);
+                        ext_pdf = BRDF_pdf(is, ext_dir, wo);
+                        ext_cos = fmaxf(0.0, dot(get_normal(is), ext_dir));
+                        ray = dRay(is.position, ext_dir);
+                        // wf_shadow
+                        light_visible = lights[light_id]->visible(bvh->nodes, bvh->tris.data(), shadow_ray);
+                    }
+                    ++samples;
+                }
+                if (out_rgb) {
+                    out_rgb[3 * pix] = acc.x;
+                    out_rgb[3 * pix + 1] = acc.y;
+                    out_rgb[3 * pix + 2] = acc.z;
+                }
+            }
+        }
+        n_ext += ext;
+        n_sh += g_shadow_calls;
+        n_samp += samples;
+    };
+    auto t1 = std::chrono::steady_clock::now();
+    int nt = d->threads > 0 ? d->threads : 1;
+    std::vector<std::thread> th;
+    for (int k = 1; k < nt; ++k) th.emplace_back(work, k);
+    work(0);
+    for (auto& x : th) x.join();
+    auto t2 = std::chrono::steady_clock::now();
+    if (stats) {
+        stats[0] = n_ext;
+        stats[1] = n_sh;
+        stats[2] = n_samp;
+    }
+    if (ms) {
+        ms[0] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        ms[1] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+    if (env) ffref_env_free(env);
+    if (area) ffref_area_free(area);
+    ffref_bvh_free(bvh);
 }
 
 void ffref_area_free(void* h)

@@ -332,6 +332,7 @@ typedef struct {
 static v3 env_L(const ffo_render_desc* d, v3 wi)
 {
     if (!d->env_rgb) return ld3(d->env_color);
+    if (d->mode == 1) wi.y = clampf_(wi.y, -1.f, 1.f);   /* corrected mode: no asinf(>1) NaN */
     v2 uv = spherical_map(wi);
     return tex_bilinear(d->env_rgb, d->env_w, d->env_h, uv.x, uv.y);
 }
@@ -610,7 +611,10 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc, int px, i
                 if (L > (uint32_t)d->rr_depth) {
                     float q = hmax(0.05f, 1.f - beta.y);
                     if (R(key, L, DIM_RR) < q) terminate = 1;
-                    else if (corrected) beta = divs(beta, 1.f - q);
+                    else if (corrected) {
+                        if (q >= 1.f) terminate = 1;
+                        else beta = divs(beta, 1.f - q);
+                    }
                 }
             }
         }
