@@ -6,9 +6,11 @@ library is missing or a CUDA device is absent, calls fail with an error.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libfirefly_b200.so"
+# FIREFLY_B200_LIB overrides the library location (e.g. an alternative build).
+LIB_PATH = Path(os.environ.get("FIREFLY_B200_LIB", Path(__file__).resolve().parent / "lib" / "libfirefly_b200.so"))
 
 FF_OK = 0
 FF_ERR_INVALID_ARG = 1

@@ -80,6 +80,7 @@ ff_status ff_film_create(ff_context* ctx, uint32_t w, uint32_t h, ff_film** out)
         f->accum.alloc(sizeof(float4) * n);
         f->comp.alloc(sizeof(float4) * n);
         f->count.alloc(sizeof(uint32_t) * n);
+        f->staging.alloc(sizeof(float4) * n);
         FF_CUDA_CHECK(cudaMemsetAsync(f->accum.ptr, 0, sizeof(float4) * n, ctx->stream));
         FF_CUDA_CHECK(cudaMemsetAsync(f->comp.ptr, 0, sizeof(float4) * n, ctx->stream));
         FF_CUDA_CHECK(cudaMemsetAsync(f->count.ptr, 0, sizeof(uint32_t) * n, ctx->stream));
@@ -122,12 +123,7 @@ ff_status ff_film_read(ff_film* f, float* rgba, uint32_t* n_samples, uint32_t fl
         cudaStream_t st = f->ctx->stream;
         const bool dev = (flags & FF_MEM_DEVICE) != 0;
         if (rgba) {
-            DevBuf tmp;
-            float4* dst = reinterpret_cast<float4*>(rgba);
-            if (!dev) {
-                tmp.alloc(sizeof(float4) * n);
-                dst = tmp.as<float4>();
-            }
+            float4* dst = dev ? reinterpret_cast<float4*>(rgba) : f->staging.as<float4>();
             k_resolve<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(f->accum.as<float4>(), f->comp.as<float4>(),
                                                                    (uint32_t)n, dst);
             FF_CUDA_CHECK(cudaGetLastError());
@@ -151,12 +147,7 @@ ff_status ff_film_tonemap(ff_film* f, float exposure, uint8_t* rgba8, uint32_t f
         const size_t n = (size_t)f->width * f->height;
         cudaStream_t st = f->ctx->stream;
         const bool dev = (flags & FF_MEM_DEVICE) != 0;
-        DevBuf tmp;
-        uchar4* dst = reinterpret_cast<uchar4*>(rgba8);
-        if (!dev) {
-            tmp.alloc(sizeof(uchar4) * n);
-            dst = tmp.as<uchar4>();
-        }
+        uchar4* dst = dev ? reinterpret_cast<uchar4*>(rgba8) : f->staging.as<uchar4>();
         k_tonemap<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(f->accum.as<float4>(), f->comp.as<float4>(),
                                                                f->count.as<uint32_t>(), (uint32_t)n, exposure, dst);
         FF_CUDA_CHECK(cudaGetLastError());

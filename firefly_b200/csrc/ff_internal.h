@@ -126,6 +126,7 @@ struct ff_film {
     DevBuf accum;         // float4 per pixel: radiance sum (xyz)
     DevBuf comp;          // float4 per pixel: Kahan compensation
     DevBuf count;         // uint32 per pixel
+    DevBuf staging;       // float4 per pixel: resolved image / tonemapped bytes on their way to the host
     FFWavefrontWS* ws = nullptr;  // path pool and queues of ff_render, kept between calls
     ~ff_film() { ff_wavefront_ws_free(ws); }
 };

@@ -18,7 +18,7 @@ constexpr int kTraceBlock = 128;
 constexpr int kRefillIdle = 8;
 
 template <bool ANY>
-__global__ void __launch_bounds__(kTraceBlock, 4)
+__global__ void __launch_bounds__(kTraceBlock, 8)
     k_trace(FFBvhView bvh, const ff_ray* __restrict__ rays, ff_hit* __restrict__ hits, uint64_t n,
             unsigned long long* __restrict__ counter, unsigned int* __restrict__ err,
             const uint32_t* __restrict__ n_dev)

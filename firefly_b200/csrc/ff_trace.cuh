@@ -37,6 +37,15 @@ FF_D uint32_t byte_of(uint32_t lo4, uint32_t hi4, int s)
     return ((s < 4 ? lo4 : hi4) >> (8 * (s & 3))) & 0xffu;
 }
 
+// Byte s of (lo4, hi4) as a float, without an integer-to-float conversion:
+// one byte permute builds the float 2^23 + byte (exponent byte 0x4B, the byte
+// in the low mantissa bits), one subtraction removes 2^23.  Exact for 0..255.
+FF_D float byte_as_float(uint32_t lo4, uint32_t hi4, int s)
+{
+    const uint32_t bits = __byte_perm(s < 4 ? lo4 : hi4, 0x4B000000u, 0x7440u | (uint32_t)(s & 3));
+    return __uint_as_float(bits) - 8388608.0f;
+}
+
 // Intersect the ray with the 8 child boxes of node idx.  Returns the new node
 // group (x = child_base, y = hit bits 24..31 in traversal order | imask) and
 // the triangle group (x = tri_base, y = 24-bit mask of triangles to test).
@@ -67,12 +76,12 @@ FF_D void ff_intersect_node(const FFNode8* __restrict__ nodes, uint32_t idx, con
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
         const uint32_t meta = byte_of(n1.z, n1.w, s);
-        const float tnx = fmaf((float)byte_of(nx0, nx1, s), ax, bx);
-        const float tny = fmaf((float)byte_of(ny0, ny1, s), ay, by);
-        const float tnz = fmaf((float)byte_of(nz0, nz1, s), az, bz);
-        const float tfx = fmaf((float)byte_of(fx0, fx1, s), ax, bx);
-        const float tfy = fmaf((float)byte_of(fy0, fy1, s), ay, by);
-        const float tfz = fmaf((float)byte_of(fz0, fz1, s), az, bz);
+        const float tnx = fmaf(byte_as_float(nx0, nx1, s), ax, bx);
+        const float tny = fmaf(byte_as_float(ny0, ny1, s), ay, by);
+        const float tnz = fmaf(byte_as_float(nz0, nz1, s), az, bz);
+        const float tfx = fmaf(byte_as_float(fx0, fx1, s), ax, bx);
+        const float tfy = fmaf(byte_as_float(fy0, fy1, s), ay, by);
+        const float tfz = fmaf(byte_as_float(fz0, fz1, s), az, bz);
         float tn = fmaxf(fmaxf(tnx, tny), tnz);
         float tf = fminf(fminf(tfx, tfy), tfz);
         tn = tn - fabsf(tn) * FF_BOX_WIDEN;
