@@ -113,7 +113,14 @@ class dScene:
         d.normals, d.texcoords, d.material_ids = _ptr(N), _ptr(T), _ptr(M)
         d.materials = C.cast(mats, C.c_void_p)
         d.num_materials = len(s.materials)
-        d.textures, d.num_textures = None, 0
+        texs = [np.ascontiguousarray(t, np.float32) for t in getattr(s, "textures", [])]
+        self._keep.append(texs)
+        tdesc = (A.ff_texture_desc * max(1, len(texs)))()
+        for i, t in enumerate(texs):
+            tdesc[i].rgb, tdesc[i].width, tdesc[i].height = t.ctypes.data, t.shape[1], t.shape[0]
+        self._keep.append(tdesc)
+        d.textures = C.cast(tdesc, C.c_void_p) if texs else None
+        d.num_textures = len(texs)
         d.env_rgb = _ptr(E)
         d.env_width = 0 if E is None else E.shape[1]
         d.env_height = 0 if E is None else E.shape[0]
@@ -132,6 +139,42 @@ class dScene:
     def update(self, camera: A.ff_camera):
         """dScene::update: replace the camera."""
         _check(lib().ff_scene_update_camera(self.handle, C.byref(camera)), self.ctx.handle)
+
+    def set_texture(self, index: int, rgb: np.ndarray):
+        """Replace the texels of texture `index` (same size)."""
+        t = np.ascontiguousarray(rgb, np.float32)
+        _check(lib().ff_scene_set_texture(self.handle, index, _ptr(t), A.FF_MEM_HOST), self.ctx.handle)
+
+    def set_environment(self, rgb: np.ndarray, keep_tables: bool = False):
+        """Replace the environment map's texels (same size); rebuilds the
+        importance tables unless keep_tables."""
+        e = np.ascontiguousarray(rgb, np.float32)
+        flags = A.FF_ENV_KEEP_TABLES if keep_tables else 0
+        _check(lib().ff_scene_set_environment(self.handle, _ptr(e), flags), self.ctx.handle)
+
+    def render_adjoint(self, width: int, height: int, d_image: np.ndarray, texture: int = 0, grad_texture=None,
+                       grad_env=None, spp: int = 1, max_depth: int = 3, rr_depth: int = 3, seed: int = 0,
+                       light: int = -1, sample_offset: int = 0, shadow_offset: float = 0.001,
+                       store_all: bool = False) -> dict:
+        """Path-replay adjoint of PathTracer.draw(mode=FF_MODE_CORRECTED) with
+        the same settings: adds dL/d(texture texels) to grad_texture and
+        dL/d(env texels) to grad_env (float32 host arrays), given d_image =
+        dL/dI of the mean-radiance image (height, width, 3)."""
+        dimg = np.ascontiguousarray(d_image, np.float32)
+        s = A.ff_render_settings(spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed,
+                                 mode=A.FF_MODE_CORRECTED, light=light, max_paths=0, sample_offset=sample_offset,
+                                 flags=0, shadow_offset=shadow_offset)
+        d = A.ff_adjoint_desc(width=width, height=height, d_image=dimg.ctypes.data, texture=texture,
+                              grad_texture=None if grad_texture is None else grad_texture.ctypes.data,
+                              grad_env=None if grad_env is None else grad_env.ctypes.data,
+                              flags=A.FF_ADJOINT_STORE_ALL if store_all else 0)
+        for g in (grad_texture, grad_env):
+            if g is not None and (g.dtype != np.float32 or not g.flags.c_contiguous):
+                raise ValueError("gradient buffers must be contiguous float32")
+        st = A.ff_render_stats()
+        _check(lib().ff_render_adjoint(self.ctx.handle, self.handle, C.byref(s), C.byref(d), C.byref(st)),
+               self.ctx.handle)
+        return {k: getattr(st, k) for k, _ in st._fields_}
 
     def stats(self) -> dict:
         st = A.ff_scene_stats()

@@ -28,6 +28,8 @@ FF_MEM_DEVICE = 1
 FF_TRACE_CLOSEST = 0
 FF_TRACE_ANY = 2
 FF_RENDER_PROFILE = 1
+FF_ADJOINT_STORE_ALL = 4
+FF_ENV_KEEP_TABLES = 8
 FF_MODE_PARITY = 0
 FF_MODE_CORRECTED = 1
 
@@ -94,6 +96,11 @@ class ff_render_stats(C.Structure):
                 ("kernel_launches", C.c_uint32)]
 
 
+class ff_adjoint_desc(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("d_image", C.c_void_p), ("texture", C.c_int32),
+                ("grad_texture", C.c_void_p), ("grad_env", C.c_void_p), ("flags", C.c_uint32)]
+
+
 # Every symbol include/firefly_b200.h declares, with its ctypes signature.
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
@@ -116,6 +123,10 @@ SIGNATURES = {
     "ff_film_tonemap": (C.c_int, [P, C.c_float, P, C.c_uint32]),
     "ff_render": (C.c_int, [P, P, C.POINTER(ff_render_settings), P, C.POINTER(ff_render_stats)]),
     "ff_scene_read_env_tables": (C.c_int, [P, P, P, P, P]),
+    "ff_render_adjoint": (C.c_int, [P, P, C.POINTER(ff_render_settings), C.POINTER(ff_adjoint_desc),
+                                    C.POINTER(ff_render_stats)]),
+    "ff_scene_set_texture": (C.c_int, [P, C.c_uint32, P, C.c_uint32]),
+    "ff_scene_set_environment": (C.c_int, [P, P, C.c_uint32]),
 }
 
 _lib = None

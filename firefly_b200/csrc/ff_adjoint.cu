@@ -1,0 +1,422 @@
+// ff_adjoint.cu — path-replay adjoint of the path tracer (no reference
+// counterpart: the reference renders only).
+//
+// For a loss L(I) of the mean-radiance image I, given dL/dI per pixel, the
+// adjoint accumulates dL/d(texel) of one albedo texture and of the
+// environment map.  One thread per pixel sample, the path computed exactly as
+// ff_render computes it in corrected mode (same sampler dimensions, same
+// shading code, ff_paths.cuh):
+//   pass 1  trace the path and sum its radiance L_s;
+//   pass 2  replay it from the same seed (path replay backpropagation:
+//           nothing is stored per vertex) and, at every vertex k whose albedo
+//           a_k comes from the texture, add dL/dI * L_{>=k} / a_k to the
+//           texels of its bilinear footprint, L_{>=k} = L_s - (radiance added
+//           before vertex k); at every NEE and camera-miss lookup of the
+//           environment, add dL/dI * (contribution / radiance looked up) to
+//           the env texels of the lookup's footprint.
+// The store-all variant keeps the vertices of pass 1 in local memory and
+// needs no replay; it is the reference the replay is checked against.
+// Sampling is detached: the importance tables and the Russian-roulette
+// probability are not differentiated.  Gradients reach albedo textures of
+// FF_MAT_DIFFUSE surfaces (their BRDF is linear in the albedo) and the
+// environment through camera misses and the NEE term.
+// Scatter: texel gradients go to global memory with atomicAdd after a
+// warp-level pre-reduction of lanes that hit the same texel (__match_any_sync).
+#include "ff_internal.h"
+#include "ff_paths.cuh"
+#include "ff_trace.cuh"
+
+namespace {
+
+using namespace ffp;
+
+constexpr int kAdjBlock = 128;
+constexpr int kMaxVerts = 16;
+
+struct ADJ {
+    FFBvhView bvh;
+    const FFShadeTri* shade;
+    const ff_material* mats;
+    const FFTexView* tex;
+    const ff_area_light* area;
+    FFEnvView env;
+    ff_camera cam;
+    uint32_t W, H, spp, sample_offset, seed, max_depth, rr_depth;
+    int32_t light;
+    float shadow_offset;
+    const float* d_image;   // W*H*3
+    int32_t texture;        // texture receiving gradients, -1 none
+    float* grad_tex;        // texels*3
+    float* grad_env;        // env texels*3 or nullptr
+    unsigned long long* rays;
+    unsigned int* err;
+};
+
+// Warp-cooperative scatter of a float3 into grad[3*idx .. 3*idx+2]: lanes
+// holding the same index are summed first, one lane per distinct index issues
+// the atomics.
+__device__ void scatter_add(float* grad, uint32_t idx, float3 v)
+{
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, idx);
+    float3 sum = make_float3(0.f, 0.f, 0.f);
+    for (uint32_t m = peers; m; m &= m - 1) {
+        const int src = __ffs(m) - 1;
+        sum.x += __shfl_sync(peers, v.x, src);
+        sum.y += __shfl_sync(peers, v.y, src);
+        sum.z += __shfl_sync(peers, v.z, src);
+    }
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) {
+        atomicAdd(grad + 3 * (size_t)idx + 0, sum.x);
+        atomicAdd(grad + 3 * (size_t)idx + 1, sum.y);
+        atomicAdd(grad + 3 * (size_t)idx + 2, sum.z);
+    }
+}
+
+// Bilinear footprint of tex_bilinear: texel indices and weights.
+struct Footprint {
+    uint32_t idx[4];
+    float w[4];
+};
+__device__ Footprint footprint(int w, int h, float u, float v)
+{
+    float xb = u * (float)w - 0.5f;
+    float yb = v * (float)h - 0.5f;
+    float fx = floorf(xb), fy = floorf(yb);
+    float ax = xb - fx, ay = yb - fy;
+    ax = floorf(ax * 256.f + 0.5f) / 256.f;
+    ay = floorf(ay * 256.f + 0.5f) / 256.f;
+    int ix = (int)fx, iy = (int)fy;
+    int x0 = ix % w;
+    x0 = x0 < 0 ? x0 + w : x0;
+    int x1 = (x0 + 1 == w) ? 0 : x0 + 1;
+    int y0 = iy % h;
+    y0 = y0 < 0 ? y0 + h : y0;
+    int y1 = (y0 + 1 == h) ? 0 : y0 + 1;
+    Footprint f;
+    f.idx[0] = y0 * w + x0;
+    f.idx[1] = y0 * w + x1;
+    f.idx[2] = y1 * w + x0;
+    f.idx[3] = y1 * w + x1;
+    f.w[0] = (1.f - ax) * (1.f - ay);
+    f.w[1] = ax * (1.f - ay);
+    f.w[2] = (1.f - ax) * ay;
+    f.w[3] = ax * ay;
+    return f;
+}
+
+__device__ void scatter_footprint(float* grad, const Footprint& f, float3 g)
+{
+    for (int i = 0; i < 4; ++i) scatter_add(grad, f.idx[i], g * f.w[i]);
+}
+
+__device__ bool closest_hit(const ADJ& a, float3 o, float3 d, FFStack& st, ff_hit& h)
+{
+    FFRayState r;
+    ff_ray_setup(r, o, d, 0.f, __int_as_float(0x7f800000), false);
+    if (a.bvh.num_nodes) {
+        uint2 cur = ff_root_group(r);
+        st.reset();
+        uint32_t steps = 0;
+        while (!ff_traverse_step<false>(a.bvh, r, cur, st)) {
+            if (++steps > a.bvh.num_nodes + 2 || st.overflow) {
+                atomicAdd(a.err, 1u);
+                break;
+            }
+        }
+    }
+    h = ff_hit{r.tmax, r.u, r.v, r.prim == 0xffffffffu ? -1 : (int32_t)r.prim};
+    return h.prim >= 0;
+}
+
+__device__ bool occluded(const ADJ& a, const ff_ray& ray, FFStack& st)
+{
+    if (!a.bvh.num_nodes) return false;
+    FFRayState r;
+    ff_ray_setup(r, make_float3(ray.ox, ray.oy, ray.oz), make_float3(ray.dx, ray.dy, ray.dz), ray.tmin, ray.tmax, true);
+    uint2 cur = ff_root_group(r);
+    st.reset();
+    uint32_t steps = 0;
+    while (!ff_traverse_step<true>(a.bvh, r, cur, st)) {
+        if (++steps > a.bvh.num_nodes + 2 || st.overflow) {
+            atomicAdd(a.err, 1u);
+            break;
+        }
+    }
+    return r.prim != 0xffffffffu;
+}
+
+struct VertexRec {
+    float3 a;           // albedo at the vertex (texture-fed diffuse only)
+    float3 L_before;    // radiance added before the vertex's terms
+    float u, v;         // texcoords
+};
+
+// One path sample.  MODE 0: primal (returns L_s).  MODE 1: replay with
+// gradients (L_total = L_s of pass 1).  MODE 2: primal that records the
+// vertices into rec (store-all).
+template <int MODE>
+__device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack& st, float3 L_total, float3 dI,
+                           VertexRec* rec, int* n_rec, uint64_t& rays)
+{
+    const uint32_t key = ff_path_key(a.seed, pix, sample);
+    float3 o, d;
+    gen_camera_ray(a.cam, (int)a.W, (int)a.H, (int)(pix % a.W), (int)(pix / a.W), rand2(key, 0, DIM_CAM_JITTER),
+                   rand2(key, 0, DIM_CAM_LENS), o, d);
+    LightCtx lc;
+    lc.env = a.env;
+    lc.is_env = a.light < 0;
+    lc.corrected = true;
+    if (!lc.is_env) lc.rect = make_rect(a.area[a.light]);
+    float3 beta = make_float3(1.f, 1.f, 1.f);
+    float3 Lacc = make_float3(0.f, 0.f, 0.f);
+    ShadeOut sh;
+    bool vis = false, vis_s = false, vis_d = false;
+    float3 nee_env_coef = make_float3(0.f, 0.f, 0.f), nee_dir = make_float3(0.f, 0.f, 0.f);
+    uint32_t L = 0;
+    for (;;) {
+        ff_hit hit;
+        const bool found = closest_hit(a, o, d, st, hit);
+        ++rays;
+        L += 1;
+        bool terminate = (L > a.max_depth) || !found;
+        if (!found && L == 1) {
+            const float3 Le = env_L(a.env, d, true);
+            const float3 c = beta * Le;
+            if (MODE != 0 && a.grad_env && a.env.rgb) {
+                float3 dd = d;
+                dd.y = clampf(dd.y, -1.f, 1.f);
+                const float2 uv = spherical_map(dd);
+                scatter_footprint(a.grad_env, footprint(a.env.width, a.env.height, uv.x, uv.y), dI * beta);
+            }
+            Lacc = Lacc + c;
+        }
+        if (L > 1) {
+            float3 lb = make_float3(0.f, 0.f, 0.f);
+            if (vis) lb = lb + sh.c_nee;
+            if (vis_s) lb = lb + sh.c_spec;
+            if (vis_d) lb = lb + sh.c_diff;
+            if (vis || vis_s || vis_d) {
+                if (MODE != 0 && vis && a.grad_env && lc.is_env && a.env.rgb) {
+                    // NEE term c_nee = coef * Le(wl): d/dLe = beta * coef
+                    const float2 uv = spherical_map(nee_dir);
+                    scatter_footprint(a.grad_env, footprint(a.env.width, a.env.height, uv.x, uv.y),
+                                      dI * beta * nee_env_coef);
+                }
+                Lacc = Lacc + lb * beta;
+            }
+            if (sh.ext_f == make_float3(0.f, 0.f, 0.f) || sh.ext_pdf == 0.f) {
+                terminate = true;
+            } else {
+                beta *= (sh.ext_f * sh.ext_cos) / sh.ext_pdf;
+                if (L > a.rr_depth) {
+                    const float q = hmax(0.05f, 1.f - beta.y);
+                    if (ff_rand(key, dim_of(L, DIM_RR)) < q) terminate = true;
+                    else if (q >= 1.f) terminate = true;
+                    else beta = beta / (1.f - q);
+                }
+            }
+        }
+        if (terminate) break;
+        // hit attributes
+        const FFShadeTri& t = a.shade[hit.prim];
+        const float u = hit.u, v = hit.v;
+        const float3 n = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
+        const float3 pos = o + hit.t * d;
+        const float wuv = (1.f - u) - v;
+        const float2 tuv = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x, u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
+        float3 wi, sp;
+        if (lc.is_env) {
+            env_sample_corrected(a.env, pos, ff_rand(key, dim_of(L, DIM_LIGHT)), ff_rand(key, dim_of(L, DIM_LIGHT + 1)),
+                                 ff_rand(key, dim_of(L, DIM_EXTRA + 1)), ff_rand(key, dim_of(L, DIM_EXTRA + 2)), wi, sp);
+        } else {
+            sp = rect_sample(lc.rect, rand2(key, L, DIM_LIGHT));
+            wi = normalize3(sp - pos);
+        }
+        const ff_material& mm = a.mats[t.material];
+        const FFSurf surf = resolve_surface(mm, a.tex, tuv);
+        const float3 wo = -d;
+        sh.c_spec = sh.c_diff = make_float3(0.f, 0.f, 0.f);
+        switch (surf.kind) {
+            case FF_MAT_MIX: shade_mix(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, sp, key, L, sh); break;
+            case FF_MAT_DIFFUSE: shade_diffuse(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+            case FF_MAT_CONDUCTOR: shade_conductor(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+            case FF_MAT_DIELECTRIC: shade_dielectric(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+            default: shade_coat(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+        }
+        const float3 lo = pos + n * a.shadow_offset;
+        sh.ray_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, sh.r_nee);
+        vis = sh.ray_nee && !occluded(a, sh.r_nee, st);
+        vis_s = sh.ray_spec && !occluded(a, sh.r_spec, st);
+        vis_d = sh.ray_diff && !occluded(a, sh.r_diff, st);
+        rays += (sh.ray_nee ? 1 : 0) + (sh.ray_spec ? 1 : 0) + (sh.ray_diff ? 1 : 0);
+        // d(c_nee)/d(Le) for the environment gradient: c_nee is linear in Le(wi)
+        nee_dir = wi;
+        nee_dir.y = clampf(nee_dir.y, -1.f, 1.f);
+        {
+            const float3 Li = light_L(lc, wi);
+            nee_env_coef = make_float3(Li.x != 0.f ? sh.c_nee.x / Li.x : 0.f, Li.y != 0.f ? sh.c_nee.y / Li.y : 0.f,
+                                       Li.z != 0.f ? sh.c_nee.z / Li.z : 0.f);
+        }
+        const bool tex_grad = surf.kind == FF_MAT_DIFFUSE && mm.base_color_tex >= 0 && mm.base_color_tex == a.texture;
+        if (MODE == 1 && tex_grad) {
+            // L_{>=k} / a_k: everything from this vertex on carries one factor a_k
+            const float3 Lge = L_total - Lacc;
+            const float3 g = make_float3(surf.albedo.x > 0.f ? Lge.x / surf.albedo.x : 0.f,
+                                         surf.albedo.y > 0.f ? Lge.y / surf.albedo.y : 0.f,
+                                         surf.albedo.z > 0.f ? Lge.z / surf.albedo.z : 0.f);
+            const FFTexView tv = a.tex[a.texture];
+            scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, tuv.x, tuv.y), dI * g);
+        }
+        if (MODE == 2 && tex_grad && *n_rec < kMaxVerts) {
+            VertexRec& r = rec[(*n_rec)++];
+            r.a = surf.albedo;
+            r.L_before = Lacc;
+            r.u = tuv.x;
+            r.v = tuv.y;
+        }
+        const float side = dot3(sh.ext_d, n) >= 0.f ? 1.f : -1.f;
+        o = pos + n * (side * a.shadow_offset);
+        d = sh.ext_d;
+    }
+    return Lacc;
+}
+
+template <bool STORE_ALL>
+__global__ void __launch_bounds__(kAdjBlock) k_adjoint(ADJ a)
+{
+    __shared__ uint2 s_stack[kShortStack * kAdjBlock];
+    FFStack st;
+    st.sm = s_stack + threadIdx.x;
+    st.stride = kAdjBlock;
+    st.sp = 0;
+    st.overflow = false;
+    const uint64_t n = (uint64_t)a.W * a.H * a.spp;
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t rays = 0;
+    if (i < n) {
+        const uint32_t pix = (uint32_t)(i % ((uint64_t)a.W * a.H));
+        const uint32_t sample = a.sample_offset + (uint32_t)(i / ((uint64_t)a.W * a.H));
+        const float inv_spp = 1.f / (float)a.spp;
+        const float3 dI = make_float3(a.d_image[3 * (size_t)pix] * inv_spp, a.d_image[3 * (size_t)pix + 1] * inv_spp,
+                                      a.d_image[3 * (size_t)pix + 2] * inv_spp);
+        if (!STORE_ALL) {
+            const float3 Ls = run_path<0>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, nullptr, nullptr, rays);
+            run_path<1>(a, pix, sample, st, Ls, dI, nullptr, nullptr, rays);
+        } else {
+            VertexRec rec[kMaxVerts];
+            int n_rec = 0;
+            const float3 Ls = run_path<2>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, rec, &n_rec, rays);
+            for (int k = 0; k < n_rec; ++k) {
+                const VertexRec& r = rec[k];
+                const float3 Lge = Ls - r.L_before;
+                const float3 g = make_float3(r.a.x > 0.f ? Lge.x / r.a.x : 0.f, r.a.y > 0.f ? Lge.y / r.a.y : 0.f,
+                                             r.a.z > 0.f ? Lge.z / r.a.z : 0.f);
+                const FFTexView tv = a.tex[a.texture];
+                scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, r.u, r.v), dI * g);
+            }
+        }
+    }
+    // per-warp ray count
+    for (int off = 16; off; off >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, off);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(a.rays, (unsigned long long)rays);
+}
+
+}  // namespace
+
+void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, const ff_adjoint_desc* ad,
+                       ff_render_stats* stats)
+{
+    FF_REQUIRE(ad->width > 0 && ad->height > 0 && ad->d_image, "adjoint image required");
+    FF_REQUIRE(st->spp > 0 && st->max_depth >= 1 && st->max_depth < (uint32_t)kMaxVerts, "spp > 0, 1 <= max_depth < 16");
+    FF_REQUIRE(ad->texture < (int32_t)scene->textures.size(), "texture index out of range");
+    FF_REQUIRE(ad->texture < 0 || ad->grad_texture, "grad_texture required for a texture gradient");
+    if (st->light < 0) FF_REQUIRE(scene->env.width > 0, "light -1 (environment) needs an environment map");
+    else FF_REQUIRE((uint32_t)st->light < scene->num_area_lights, "light index out of range");
+    cudaStream_t stream = ctx->stream;
+    const bool dev = (ad->flags & FF_MEM_DEVICE) != 0;
+    const size_t npix = (size_t)ad->width * ad->height;
+    const size_t ntex = ad->texture >= 0 ? (size_t)3 * [&] {
+        FFTexView v;
+        FF_CUDA_CHECK(cudaMemcpy(&v, scene->tex_table.as<FFTexView>() + ad->texture, sizeof(v), cudaMemcpyDeviceToHost));
+        return (size_t)v.width * v.height;
+    }() : 0;
+    const size_t nenv = (size_t)3 * scene->env.width * scene->env.height;
+    DevBuf dimg, gtex, genv, ctr;
+    const float* d_image = ad->d_image;
+    float* g_tex = ad->grad_texture;
+    float* g_env = ad->grad_env;
+    if (!dev) {
+        dimg.alloc(sizeof(float) * 3 * npix);
+        FF_CUDA_CHECK(cudaMemcpyAsync(dimg.ptr, ad->d_image, sizeof(float) * 3 * npix, cudaMemcpyHostToDevice, stream));
+        d_image = dimg.as<float>();
+        if (ntex) {
+            gtex.alloc(sizeof(float) * ntex);
+            FF_CUDA_CHECK(cudaMemcpyAsync(gtex.ptr, ad->grad_texture, sizeof(float) * ntex, cudaMemcpyHostToDevice, stream));
+            g_tex = gtex.as<float>();
+        }
+        if (ad->grad_env && nenv) {
+            genv.alloc(sizeof(float) * nenv);
+            FF_CUDA_CHECK(cudaMemcpyAsync(genv.ptr, ad->grad_env, sizeof(float) * nenv, cudaMemcpyHostToDevice, stream));
+            g_env = genv.as<float>();
+        }
+    }
+    ctr.alloc(64);
+    FF_CUDA_CHECK(cudaMemsetAsync(ctr.ptr, 0, 64, stream));
+    ADJ a;
+    a.bvh = scene->view();
+    a.shade = scene->shade.as<FFShadeTri>();
+    a.mats = scene->materials.as<ff_material>();
+    a.tex = scene->tex_table.as<FFTexView>();
+    a.area = scene->area_lights.as<ff_area_light>();
+    a.env.rgb = scene->env.rgb.as<float3>();
+    a.env.marginal = scene->env.marginal.as<double>();
+    a.env.cond = scene->env.conditional.as<double>();
+    a.env.pdf = scene->env.pdf.as<float>();
+    a.env.width = scene->env.width;
+    a.env.height = scene->env.height;
+    a.env.color = scene->env.color;
+    a.env.radius = 10000.f;
+    a.cam = scene->camera;
+    a.W = ad->width;
+    a.H = ad->height;
+    a.spp = st->spp;
+    a.sample_offset = st->sample_offset;
+    a.seed = st->seed;
+    a.max_depth = st->max_depth;
+    a.rr_depth = st->rr_depth;
+    a.light = st->light;
+    a.shadow_offset = st->shadow_offset > 0.f ? st->shadow_offset : 0.001f;
+    a.d_image = d_image;
+    a.texture = ad->texture;
+    a.grad_tex = g_tex;
+    a.grad_env = (ad->grad_env && nenv) ? g_env : nullptr;
+    a.rays = ctr.as<unsigned long long>();
+    a.err = reinterpret_cast<unsigned int*>(ctr.as<char>() + 8);
+    const uint64_t n = (uint64_t)npix * st->spp;
+    const uint64_t blocks = (n + kAdjBlock - 1) / kAdjBlock;
+    FF_REQUIRE(blocks < (1ull << 31), "adjoint launch too large");
+    FF_CUDA_CHECK(cudaEventRecord(ctx->ev0, stream));
+    if (ad->flags & FF_ADJOINT_STORE_ALL) k_adjoint<true><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    else k_adjoint<false><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    FF_CUDA_CHECK(cudaGetLastError());
+    FF_CUDA_CHECK(cudaEventRecord(ctx->ev1, stream));
+    if (!dev) {
+        if (ntex)
+            FF_CUDA_CHECK(cudaMemcpyAsync(ad->grad_texture, g_tex, sizeof(float) * ntex, cudaMemcpyDeviceToHost, stream));
+        if (ad->grad_env && nenv)
+            FF_CUDA_CHECK(cudaMemcpyAsync(ad->grad_env, g_env, sizeof(float) * nenv, cudaMemcpyDeviceToHost, stream));
+    }
+    unsigned long long h_ctr[2] = {0, 0};
+    FF_CUDA_CHECK(cudaMemcpyAsync(h_ctr, ctr.ptr, sizeof(h_ctr), cudaMemcpyDeviceToHost, stream));
+    FF_CUDA_CHECK(cudaStreamSynchronize(stream));
+    if ((unsigned int)h_ctr[1]) throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        stats->extension_rays = h_ctr[0];
+        stats->samples = n;
+        stats->ms_total = ms;
+        stats->kernel_launches = 1;
+    }
+}

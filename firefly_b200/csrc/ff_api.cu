@@ -276,3 +276,49 @@ extern "C" ff_status ff_render(ff_context* ctx, ff_scene* scene, const ff_render
         ff_wavefront_render(ctx, scene, settings, film, stats);
     });
 }
+
+extern "C" ff_status ff_render_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_settings* settings,
+                                       const ff_adjoint_desc* desc, ff_render_stats* stats)
+{
+    if (!ctx || !scene || !settings || !desc) return FF_ERR_INVALID_ARG;
+    if (scene->ctx != ctx) {
+        ctx->last_error = "scene belongs to another context";
+        return FF_ERR_INVALID_ARG;
+    }
+    return guarded(ctx, [&] {
+        DeviceGuard g(ctx->device);
+        FF_REQUIRE(settings->mode == FF_MODE_CORRECTED, "the adjoint follows FF_MODE_CORRECTED paths");
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        ff_adjoint_render(ctx, scene, settings, desc, stats);
+    });
+}
+
+extern "C" ff_status ff_scene_set_texture(ff_scene* s, uint32_t index, const float* rgb, uint32_t flags)
+{
+    if (!s || !rgb) return FF_ERR_INVALID_ARG;
+    ff_context* ctx = s->ctx;
+    return guarded(ctx, [&] {
+        DeviceGuard g(ctx->device);
+        FF_REQUIRE(index < s->textures.size(), "texture index out of range");
+        DevBuf* b = s->textures[index];
+        FF_CUDA_CHECK(cudaMemcpyAsync(b->ptr, rgb, b->bytes,
+                                      (flags & FF_MEM_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        FF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+extern "C" ff_status ff_scene_set_environment(ff_scene* s, const float* rgb, uint32_t flags)
+{
+    if (!s || !rgb) return FF_ERR_INVALID_ARG;
+    ff_context* ctx = s->ctx;
+    return guarded(ctx, [&] {
+        DeviceGuard g(ctx->device);
+        FF_REQUIRE(s->env.width > 0, "scene has no environment map");
+        FF_CUDA_CHECK(cudaMemcpyAsync(s->env.rgb.ptr, rgb, sizeof(float3) * s->env.width * s->env.height,
+                                      (flags & FF_MEM_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        if (!(flags & FF_ENV_KEEP_TABLES)) ff_build_env_tables(ctx, s);
+        FF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}

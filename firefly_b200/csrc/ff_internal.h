@@ -153,3 +153,8 @@ void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d
 void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
                            uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter,
                            unsigned int* err);
+
+// ff_adjoint.cu
+void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, const ff_adjoint_desc* ad,
+                       ff_render_stats* stats);
+void ff_build_env_tables(ff_context* ctx, ff_scene* s);

@@ -7,6 +7,7 @@
 // (dScene.cpp:172-298).  Traversal reads only the 48-byte FFTri records;
 // the attributes below are read once per hit, by original triangle index.
 #include "ff_internal.h"
+#include "ff_shade.cuh"
 
 namespace {
 
@@ -86,6 +87,23 @@ void ff_build_shading(ff_context* ctx, ff_scene* s, const ff_scene_desc* d, cons
     s->materials.alloc(sizeof(ff_material) * mats.size());
     FF_CUDA_CHECK(cudaMemcpyAsync(s->materials.ptr, mats.data(), sizeof(ff_material) * mats.size(),
                                   cudaMemcpyHostToDevice, st));
+    // textures: one RGB float array each, plus a device table of views
+    if (d->num_textures) {
+        std::vector<FFTexView> views(d->num_textures);
+        for (uint32_t i = 0; i < d->num_textures; ++i) {
+            const ff_texture_desc& td = d->textures[i];
+            FF_REQUIRE(td.rgb && td.width > 0 && td.height > 0, "texture without texels");
+            DevBuf* b = new DevBuf();
+            s->textures.push_back(b);
+            b->alloc(sizeof(float3) * td.width * td.height);
+            FF_CUDA_CHECK(cudaMemcpyAsync(b->ptr, td.rgb, sizeof(float3) * td.width * td.height, cudaMemcpyHostToDevice, st));
+            views[i] = FFTexView{b->as<float3>(), (int)td.width, (int)td.height};
+        }
+        s->tex_table.alloc(sizeof(FFTexView) * views.size());
+        FF_CUDA_CHECK(cudaMemcpyAsync(s->tex_table.ptr, views.data(), sizeof(FFTexView) * views.size(),
+                                      cudaMemcpyHostToDevice, st));
+        FF_CUDA_CHECK(cudaStreamSynchronize(st));
+    }
     s->num_area_lights = d->num_area_lights;
     if (d->num_area_lights) {
         s->area_lights.alloc(sizeof(ff_area_light) * d->num_area_lights);

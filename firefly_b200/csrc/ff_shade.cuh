@@ -130,6 +130,23 @@ struct FFIsect {
     uint32_t prim;
 };
 
+// A material resolved at a hit point: the reference's get_albedo /
+// get_roughness / get_metallic (dMaterial.cu:10-60) read a texture when one
+// is bound, else the factor.
+struct FFSurf {
+    float3 albedo;
+    float3 fresnel;    // dielectric f0
+    float roughness;
+    float metallic;
+    float ior;
+    int kind;
+};
+
+struct FFTexView {
+    const float3* rgb;
+    int width, height;
+};
+
 // diff_get_pdf = 1.f / (2.f * M_PI) in float, returned as double (dMaterial.cu:160-163)
 FF_D double diff_get_pdf() { return (double)(1.f / (2.f * FF_PI)); }
 
@@ -164,17 +181,14 @@ FF_D double geo_atten(float3 wi, float3 wo, float3 n, float r)
 // power_heuristic(1, f, 1, g) (dMaterial.cu:114-119)
 FF_D double power_heuristic(double f, double g) { return (f * f) / (f * f + g * g); }
 
-FF_D float3 f0_of(const ff_material& m, float3 albedo)
-{
-    return lerp3(make_float3(m.fresnel[0], m.fresnel[1], m.fresnel[2]), albedo, m.metallic);
-}
+FF_D float3 f0_of(const FFSurf& m, float3 albedo) { return lerp3(m.fresnel, albedo, m.metallic); }
 
 // diff_f (dMaterial.cu:164-178)
-FF_D float3 diff_f(const ff_material& mat, float3 n, float3 wi, float3 wo)
+FF_D float3 diff_f(const FFSurf& mat, float3 n, float3 wi, float3 wo)
 {
     (void)n;
     float m = mat.metallic;
-    float3 a = make_float3(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
+    float3 a = mat.albedo;
     float3 f0 = f0_of(mat, a);
     float3 wh = normalize3(wo + wi);
     float3 F = fresnel3(f0, wh, wi);
@@ -194,10 +208,10 @@ FF_D float spec_get_pdf(float3 n, float3 wi, float3 wo, float r)
 }
 
 // spec_f (dMaterial.cu:266-288)
-FF_D float3 spec_f(const ff_material& mat, float3 n, float3 wi, float3 wo)
+FF_D float3 spec_f(const FFSurf& mat, float3 n, float3 wi, float3 wo)
 {
     float r = mat.roughness;
-    float3 a = make_float3(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
+    float3 a = mat.albedo;
     float3 f0 = f0_of(mat, a);
     float3 wh = normalize3(wo + wi);
     double n_dot_wi = hmax(dot3(n, wi), 0.f);
@@ -241,11 +255,11 @@ FF_D float3 spec_sample(float3 N, float3 wo, float r, float e0, float e1)
 }
 
 // BRDF_f = spec_f + diff_f; BRDF_pdf = 0.5 (spec_pdf + diff_pdf) (dMaterial.cu:459-469)
-FF_D float3 brdf_f(const ff_material& m, float3 n, float3 wi, float3 wo)
+FF_D float3 brdf_f(const FFSurf& m, float3 n, float3 wi, float3 wo)
 {
     return spec_f(m, n, wi, wo) + diff_f(m, n, wi, wo);
 }
-FF_D float brdf_pdf(const ff_material& m, float3 n, float3 wi, float3 wo)
+FF_D float brdf_pdf(const FFSurf& m, float3 n, float3 wi, float3 wo)
 {
     float sp = spec_get_pdf(n, wi, wo, m.roughness);
     float dp = (float)diff_get_pdf();
@@ -254,6 +268,27 @@ FF_D float brdf_pdf(const ff_material& m, float3 n, float3 wi, float3 wo)
 
 // ----------------------------------------------------------------- lights
 // Environment light with importance tables (dEnvironmentLight.cu).
+FF_D float3 tex_bilinear(const float3* texels, int w, int h, float u, float v);
+
+FF_D FFSurf resolve_surface(const ff_material& m, const FFTexView* tex, float2 uv)
+{
+    FFSurf s;
+    s.albedo = make_float3(m.base_color[0], m.base_color[1], m.base_color[2]);
+    if (m.base_color_tex >= 0) {
+        const FFTexView t = tex[m.base_color_tex];
+        s.albedo = tex_bilinear(t.rgb, t.width, t.height, uv.x, uv.y);
+    }
+    s.roughness = m.roughness;
+    if (m.roughness_tex >= 0) {
+        const FFTexView t = tex[m.roughness_tex];
+        s.roughness = hmax(tex_bilinear(t.rgb, t.width, t.height, uv.x, uv.y).x, 0.01f);
+    }
+    s.fresnel = make_float3(m.fresnel[0], m.fresnel[1], m.fresnel[2]);
+    s.metallic = m.metallic;
+    s.ior = m.ior;
+    s.kind = m.kind;
+    return s;
+}
 struct FFEnvView {
     const float3* rgb;       // width*height texels, row y = v * height
     const double* marginal;  // marginal_y[height]

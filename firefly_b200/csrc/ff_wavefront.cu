@@ -30,10 +30,11 @@
 #include <vector>
 
 #include "ff_internal.h"
-#include "ff_shade.cuh"
+#include "ff_paths.cuh"
 
 namespace {
 
+using namespace ffp;
 constexpr int kKinds = 5;
 constexpr uint32_t PH_START = 0, PH_FLIGHT = 1, PH_DONE = 2;
 constexpr int32_t SQ_NONE = -1, SQ_BLOCKED = -2;
@@ -83,6 +84,8 @@ struct WF {
     const ff_material* mats;
     const ff_area_light* area;
     uint32_t n_area;
+    const FFTexView* tex;
+    float2* hit_uv;
     FFEnvView env;
     ff_camera cam;
 };
@@ -220,6 +223,10 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 const float u = hit.u, v = hit.v;
                 const float3 n = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
                 const float3 pos = ro + hit.t * rd;
+                // texcoord = u * uv1 + v * uv2 + (1 - u - v) * uv0 (dTriangle.cu:97)
+                const float wuv = (1.f - u) - v;
+                w.hit_uv[s] = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x,
+                                          u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
                 // Light sample (kernel.cu:435, light get_direction).
                 float3 wi, sp;
                 if (w.light < 0) {
@@ -259,251 +266,6 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
     if ((threadIdx.x & 31u) == 0 && am) atomicAdd(&w.ctr[C_ACTIVE], (uint32_t)__popc(am));
 }
 
-struct ShadeOut {
-    float3 c_nee, c_spec, c_diff;
-    bool ray_nee, ray_spec, ray_diff;   // shadow rays to trace
-    ff_ray r_nee, r_spec, r_diff;
-    float3 ext_o, ext_d, ext_f;
-    float ext_pdf, ext_cos;
-};
-
-__device__ __forceinline__ ff_ray make_ray(float3 o, float3 d, float tmax)
-{
-    return ff_ray{o.x, o.y, o.z, 0.f, d.x, d.y, d.z, tmax};
-}
-
-// Light radiance toward wi, pdf of wi, and the visibility ray of light.visible()
-// (env: any occluder; area: the rectangle must be hit, and the occluder must
-// lie before the projection of a fresh sample point).
-struct LightCtx {
-    const WF* w;
-    bool is_env;
-    bool corrected;
-    FFRect rect;
-};
-
-__device__ __forceinline__ float3 light_L(const LightCtx& lc, float3 wi)
-{
-    return lc.is_env ? env_L(lc.w->env, wi, lc.corrected) : rect_L(lc.rect, wi);
-}
-__device__ __forceinline__ float light_pdf(const LightCtx& lc, float3 pos, float3 wi, uint32_t key, uint32_t L,
-                                           uint32_t dim)
-{
-    if (lc.is_env) return lc.corrected ? env_pdf_corrected(lc.w->env, wi) : env_pdf(lc.w->env, wi);
-    return rect_pdf(lc.rect, pos, rand2(key, L, dim));
-}
-// Visibility ray of light.visible(ray): returns false when the reference
-// answers "not visible" without tracing (area light missed).
-__device__ __forceinline__ bool light_vis_ray(const LightCtx& lc, float3 o, float3 d, uint32_t key, uint32_t L,
-                                              uint32_t dim, ff_ray& out)
-{
-    if (lc.is_env) {
-        out = make_ray(o, d, FF_K_HUGE);
-        return true;
-    }
-    if (!rect_hit(lc.rect, o, d)) return false;
-    const float ts = dot3(rect_sample(lc.rect, rand2(key, L, dim)) - o, d);
-    out = make_ray(o, d, ts);
-    return true;
-}
-
-// wf_mat_mix + BRDF_L / BRDF_f / BRDF_pdf (kernel.cu:617-651, dMaterial.cu:363-469)
-__device__ void shade_mix(const WF& w, const LightCtx& lc, const ff_material& mat, float3 pos, float3 n, float3 wo,
-                          float3 wi, float3 sp, uint32_t key, uint32_t L, ShadeOut& o)
-{
-    (void)sp;
-    const bool corrected = w.mode == FF_MODE_CORRECTED;
-    const float r = mat.roughness;
-    float3 Lsum = make_float3(0.f, 0.f, 0.f);
-    const float3 Li = light_L(lc, wi);
-    const float n_dot_wi = dot3(n, wi);
-    if (n_dot_wi > 0.f) {
-        const double diff_pdf = diff_get_pdf();
-        const double spec_pdf = spec_get_pdf(n, wi, wo, r);
-        const double lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
-        if (lpdf > 0.f && Li != make_float3(0.f, 0.f, 0.f)) {
-            const double diff_w = power_heuristic(lpdf, diff_pdf);
-            const double spec_w = power_heuristic(lpdf, spec_pdf);
-            float3 f = spec_f(mat, n, wi, wo) * n_dot_wi;
-            if (f != make_float3(0.f, 0.f, 0.f)) Lsum = Lsum + ((f * (float)spec_w) * Li) / (float)lpdf;
-            f = diff_f(mat, n, wi, wo) * n_dot_wi;
-            if (f != make_float3(0.f, 0.f, 0.f)) Lsum = Lsum + ((f * (float)diff_w) * Li) / (float)lpdf;
-        }
-    }
-    o.c_nee = Lsum;
-    const float3 wi_spec = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
-    const float3 wi_diff = diff_sample(n, ff_rand(key, dim_of(L, DIM_DIFF)), ff_rand(key, dim_of(L, DIM_DIFF + 1)));
-    // BSDF-sampled MIS terms; their visibility is traced as shadow rays
-    o.ray_spec = o.ray_diff = false;
-    {
-        const float3 org = pos + wi_spec * 0.001f;
-        const float nd = dot3(n, wi_spec);
-        ff_ray vr;
-        if (nd > 0.f && light_vis_ray(lc, org, wi_spec, key, L, DIM_SPEC_VIS, vr)) {
-            const double spdf = spec_get_pdf(n, wi_spec, wo, r);
-            const double lpdf = light_pdf(lc, pos, wi_spec, key, L, DIM_SPEC_PDF);
-            const double wgt = power_heuristic(spdf, lpdf);
-            const float3 f = spec_f(mat, n, wi_spec, wo) * nd;
-            const float3 Li2 = light_L(lc, wi_spec);
-            if (f != make_float3(0.f, 0.f, 0.f) && spdf > 0.f && Li2 != make_float3(0.f, 0.f, 0.f)) {
-                o.c_spec = ((f * Li2) * (float)wgt) / (float)spdf;
-                o.ray_spec = true;
-                o.r_spec = vr;
-            }
-        }
-    }
-    {
-        // dMaterial.cu:431: the reference offsets this ray along wi_spec (parity)
-        const float3 org = corrected ? pos + wi_diff * 0.001f : pos + wi_spec * 0.001f;
-        const float nd = dot3(n, wi_diff);
-        ff_ray vr;
-        if (nd > 0.f && light_vis_ray(lc, org, wi_diff, key, L, DIM_DIFF_VIS, vr)) {
-            const double dpdf = diff_get_pdf();
-            const double lpdf = light_pdf(lc, pos, wi_diff, key, L, DIM_DIFF_PDF);
-            const double wgt = power_heuristic(dpdf, lpdf);
-            const float3 f = diff_f(mat, n, wi_diff, wo) * nd;
-            const float3 Li2 = light_L(lc, wi_diff);
-            if (f != make_float3(0.f, 0.f, 0.f) && dpdf > 0.f && Li2 != make_float3(0.f, 0.f, 0.f)) {
-                o.c_diff = ((f * Li2) * (float)wgt) / (float)dpdf;
-                o.ray_diff = true;
-                o.r_diff = vr;
-            }
-        }
-    }
-    const float3 dir = ff_rand(key, dim_of(L, DIM_LOBE)) < 0.5f ? wi_diff : wi_spec;
-    o.ext_d = dir;
-    o.ext_f = brdf_f(mat, n, dir, wo);
-    o.ext_pdf = brdf_pdf(mat, n, dir, wo);
-    o.ext_cos = hmax(0.f, dot3(n, dir));
-}
-
-// wf_mat_diffuse (kernel.cu:546-577): diff_L returns 0 in the reference (dMaterial.cu:179-227).
-__device__ void shade_diffuse(const WF& w, const LightCtx& lc, const ff_material& mat, float3 pos, float3 n,
-                              float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
-{
-    o.c_nee = make_float3(0.f, 0.f, 0.f);
-    if (w.mode == FF_MODE_CORRECTED) {
-        const float nd = dot3(n, wi);
-        const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
-        const float3 Li = light_L(lc, wi);
-        if (nd > 0.f && lpdf > 0.f) o.c_nee = ((diff_f(mat, n, wi, wo) * nd) * Li) / lpdf;
-    }
-    o.ray_spec = o.ray_diff = false;
-    const float3 dir = diff_sample(n, ff_rand(key, dim_of(L, DIM_DIFF)), ff_rand(key, dim_of(L, DIM_DIFF + 1)));
-    o.ext_d = dir;
-    o.ext_f = diff_f(mat, n, dir, wo);
-    o.ext_pdf = (float)diff_get_pdf();
-    o.ext_cos = hmax(0.f, dot3(n, dir));
-}
-
-// wf_mat_cook (kernel.cu:580-614): spec_L returns 0 in the reference (dMaterial.cu:314-361).
-__device__ void shade_conductor(const WF& w, const LightCtx& lc, const ff_material& mat, float3 pos, float3 n,
-                                float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
-{
-    o.c_nee = make_float3(0.f, 0.f, 0.f);
-    if (w.mode == FF_MODE_CORRECTED) {
-        const float nd = dot3(n, wi);
-        const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
-        const float3 Li = light_L(lc, wi);
-        if (nd > 0.f && lpdf > 0.f) o.c_nee = ((spec_f(mat, n, wi, wo) * nd) * Li) / lpdf;
-    }
-    o.ray_spec = o.ray_diff = false;
-    const float r = mat.roughness;
-    const float3 dir = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
-    o.ext_d = dir;
-    o.ext_f = spec_f(mat, n, dir, wo);
-    o.ext_pdf = spec_get_pdf(n, dir, wo, r);
-    o.ext_cos = hmax(0.f, dot3(n, dir));
-}
-
-// Thin GGX dielectric (no reference counterpart): with probability equal to
-// the Schlick reflectance at the surface's IOR the path reflects off a GGX
-// lobe, otherwise it is transmitted through the sheet unchanged.  The
-// transmission is a delta lobe (no NEE through it); the GGX reflection gets
-// light-sampled NEE.
-__device__ void shade_dielectric(const WF& w, const LightCtx& lc, const ff_material& mat, float3 pos, float3 n,
-                                 float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
-{
-    (void)w;
-    const float eta = mat.ior > 0.f ? mat.ior : 1.5f;
-    const float r0 = ((eta - 1.f) / (eta + 1.f)) * ((eta - 1.f) / (eta + 1.f));
-    const float cos_o = fabsf(dot3(n, wo));
-    const float x = 1.f - cos_o;
-    const float Fr = r0 + (1.f - r0) * x * x * x * x * x;
-    ff_material m = mat;
-    m.fresnel[0] = m.fresnel[1] = m.fresnel[2] = r0;
-    m.base_color[0] = m.base_color[1] = m.base_color[2] = 1.f;
-    m.metallic = 0.f;
-    o.ray_spec = o.ray_diff = false;
-    o.c_nee = make_float3(0.f, 0.f, 0.f);
-    const float nd = dot3(n, wi);
-    const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
-    if (nd > 0.f && lpdf > 0.f) o.c_nee = ((spec_f(m, n, wi, wo) * nd) * light_L(lc, wi)) / lpdf;
-    if (ff_rand(key, dim_of(L, DIM_EXTRA)) < Fr) {
-        const float3 dir = spec_sample(n, wo, m.roughness, ff_rand(key, dim_of(L, DIM_SPEC)),
-                                       ff_rand(key, dim_of(L, DIM_SPEC + 1)));
-        o.ext_d = dir;
-        o.ext_f = spec_f(m, n, dir, wo) / Fr;
-        o.ext_pdf = spec_get_pdf(n, dir, wo, m.roughness);
-        o.ext_cos = hmax(0.f, dot3(n, dir));
-    } else {
-        const float3 tint = make_float3(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
-        o.ext_d = -wo;
-        o.ext_f = tint;
-        o.ext_pdf = 1.f;
-        o.ext_cos = 1.f;
-    }
-}
-
-// Diffuse base under a GGX clear coat (no reference counterpart): the coat
-// reflects with Schlick Fresnel at the coat IOR, the base is Lambertian
-// weighted by (1 - F).  Continuation picks the coat lobe or the base with
-// equal probability; the pdf is the 50/50 mixture, as BRDF_pdf's.
-__device__ float3 coat_f(const ff_material& mat, float3 n, float3 wi, float3 wo, float r0)
-{
-    ff_material c = mat;
-    c.fresnel[0] = c.fresnel[1] = c.fresnel[2] = r0;
-    c.base_color[0] = c.base_color[1] = c.base_color[2] = 1.f;
-    c.metallic = 0.f;
-    const float3 spec = spec_f(c, n, wi, wo);
-    const float3 h = normalize3(wo + wi);
-    const float x = 1.f - hmax(0.f, dot3(h, wi));
-    const float F = r0 + (1.f - r0) * x * x * x * x * x;
-    const float3 a = make_float3(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
-    return spec + a * ((1.f - F) * FF_1_PI);
-}
-
-__device__ void shade_coat(const WF& w, const LightCtx& lc, const ff_material& mat, float3 pos, float3 n, float3 wo,
-                           float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
-{
-    (void)w;
-    const float eta = mat.ior > 0.f ? mat.ior : 1.5f;
-    const float r0 = ((eta - 1.f) / (eta + 1.f)) * ((eta - 1.f) / (eta + 1.f));
-    o.ray_spec = o.ray_diff = false;
-    o.c_nee = make_float3(0.f, 0.f, 0.f);
-    const float nd = dot3(n, wi);
-    const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
-    if (nd > 0.f && lpdf > 0.f) o.c_nee = ((coat_f(mat, n, wi, wo, r0) * nd) * light_L(lc, wi)) / lpdf;
-    const float r = mat.roughness;
-    float3 dir;
-    if (ff_rand(key, dim_of(L, DIM_LOBE)) < 0.5f) {
-        dir = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
-    } else {
-        // cosine-weighted hemisphere (concentric disk lifted to the hemisphere)
-        const float2 dsk = concentric_disk(make_float2(ff_rand(key, dim_of(L, DIM_DIFF)),
-                                                       ff_rand(key, dim_of(L, DIM_DIFF + 1))));
-        const float z = sqrtf(hmax(0.f, 1.f - dsk.x * dsk.x - dsk.y * dsk.y));
-        float3 T, B;
-        frame(n, T, B);
-        dir = normalize3(T * dsk.x + B * dsk.y + n * z);
-    }
-    const float c = hmax(0.f, dot3(n, dir));
-    o.ext_d = dir;
-    o.ext_f = coat_f(mat, n, dir, wo, r0);
-    o.ext_pdf = 0.5f * spec_get_pdf(n, dir, wo, r) + 0.5f * c * FF_1_PI;
-    o.ext_cos = c;
-}
-
 template <int KIND>
 __global__ void __launch_bounds__(128) k_shade(WF w)
 {
@@ -513,7 +275,7 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
     const uint32_t iters = (n + stride - 1) / stride;
     const uint32_t base = blockIdx.x * blockDim.x + threadIdx.x;
     LightCtx lc;
-    lc.w = &w;
+    lc.env = w.env;
     lc.is_env = w.light < 0;
     lc.corrected = w.mode == FF_MODE_CORRECTED;
     if (!lc.is_env) lc.rect = make_rect(w.area[w.light]);
@@ -527,7 +289,7 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
             s = w.mat_queue[(size_t)KIND * w.P + qi];
             const float4 hp = w.hit_pos[s];
             const float3 pos = xyz(hp);
-            const ff_material mat = w.mats[__float_as_uint(hp.w)];
+            const FFSurf mat = resolve_surface(w.mats[__float_as_uint(hp.w)], w.tex, w.hit_uv[s]);
             const float3 n = xyz(w.hit_nrm[s]);
             const float3 wo = -xyz(w.ray_d[s]);
             const float3 wi = xyz(w.light_wi[s]);
@@ -535,11 +297,11 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
             const uint32_t key = w.key[s];
             const uint32_t L = w.length[s];
             o.c_spec = o.c_diff = make_float3(0.f, 0.f, 0.f);
-            if (KIND == FF_MAT_MIX) shade_mix(w, lc, mat, pos, n, wo, wi, sp, key, L, o);
-            else if (KIND == FF_MAT_DIFFUSE) shade_diffuse(w, lc, mat, pos, n, wo, wi, key, L, o);
-            else if (KIND == FF_MAT_CONDUCTOR) shade_conductor(w, lc, mat, pos, n, wo, wi, key, L, o);
-            else if (KIND == FF_MAT_DIELECTRIC) shade_dielectric(w, lc, mat, pos, n, wo, wi, key, L, o);
-            else shade_coat(w, lc, mat, pos, n, wo, wi, key, L, o);
+            if (KIND == FF_MAT_MIX) shade_mix(w.mode, lc, mat, pos, n, wo, wi, sp, key, L, o);
+            else if (KIND == FF_MAT_DIFFUSE) shade_diffuse(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
+            else if (KIND == FF_MAT_CONDUCTOR) shade_conductor(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
+            else if (KIND == FF_MAT_DIELECTRIC) shade_dielectric(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
+            else shade_coat(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
             // NEE shadow ray of wf_shadow: light_ray = position + normal * SHADOW_OFFSET (kernel.cu:437)
             const float3 lo = pos + n * w.shadow_offset;
             o.ray_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, o.r_nee);
@@ -649,7 +411,7 @@ size_t ws_bytes(uint32_t P)
     add(4, P) /*samples_left*/; add(4, P); add(4, P); add(4, P); add(4, P);
     add(16, P) /*beta*/; add(16, P); add(16, P); add(4, P); add(16, P);
     add(16, P); add(16, P); add(16, P); add(16, P); add(4, P);
-    add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(4, P);
+    add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(4, P); add(8, P);
     add(sizeof(ff_ray), P); add(sizeof(ff_hit), P); add(sizeof(ff_ray), 3ull * P); add(sizeof(ff_hit), 3ull * P);
     add(4, (size_t)kKinds * P); add(4, 64); add(8, 8); add(4, 4); add(8, 4);
     return b;
@@ -685,6 +447,7 @@ void ws_setup(FFWavefrontWS* ws, uint32_t P)
     w.acc = carve<float4>(p, P);
     w.acc_c = carve<float4>(p, P);
     w.cnt = carve<uint32_t>(p, P);
+    w.hit_uv = carve<float2>(p, P);
     w.ext_rays = carve<ff_ray>(p, P);
     w.ext_hits = carve<ff_hit>(p, P);
     w.sh_rays = carve<ff_ray>(p, 3ull * P);
@@ -734,6 +497,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     w.mats = scene->materials.as<ff_material>();
     w.area = scene->area_lights.as<ff_area_light>();
     w.n_area = scene->num_area_lights;
+    w.tex = scene->tex_table.as<FFTexView>();
     w.env.rgb = scene->env.rgb.as<float3>();
     w.env.marginal = scene->env.marginal.as<double>();
     w.env.cond = scene->env.conditional.as<double>();

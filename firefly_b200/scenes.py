@@ -160,6 +160,7 @@ class Scene:
     area_lights: list = field(default_factory=list)
     env_rgb: np.ndarray | None = None
     env_color: tuple = (0.0, 0.0, 0.0)
+    textures: list = field(default_factory=list)   # (h, w, 3) float32 arrays, indexed by ff_material.*_tex
     camera: A.ff_camera | None = None
     width: int = 256
     height: int = 256
@@ -177,7 +178,7 @@ class Scene:
 
 
 def material(base_color, kind=A.FF_MAT_MIX, roughness=1.0, metallic=0.0, ior=1.5, fresnel=0.04,
-             emissive=(0, 0, 0), radiance=0.0) -> A.ff_material:
+             emissive=(0, 0, 0), radiance=0.0, base_color_tex=-1, roughness_tex=-1) -> A.ff_material:
     m = A.ff_material()
     for k in range(3):
         m.base_color[k] = float(base_color[k])
@@ -188,8 +189,8 @@ def material(base_color, kind=A.FF_MAT_MIX, roughness=1.0, metallic=0.0, ior=1.5
     m.radiance = radiance
     m.ior = ior
     m.kind = kind
-    m.base_color_tex = -1
-    m.roughness_tex = -1
+    m.base_color_tex = base_color_tex
+    m.roughness_tex = roughness_tex
     return m
 
 
@@ -479,3 +480,83 @@ def displaced_icosphere(subdiv: int = 8, seed: int = 0, width: int = 1920, heigh
     env = sky_env(env_w, env_h, seed=seed)
     return Scene(positions=P, indices=I, normals=N, material_ids=mat_ids, materials=mats, env_rgb=env,
                  camera=cam, width=width, height=height)
+
+
+def perlin2(res: int, seed: int, octaves: int = 5, base: int = 4) -> np.ndarray:
+    """Seeded 2D gradient (Perlin) noise fBm on a res x res grid, in [-1, 1] roughly."""
+    rng = np.random.default_rng(seed)
+    out = np.zeros((res, res))
+    amp, total = 1.0, 0.0
+    for o in range(octaves):
+        cells = base * 2 ** o
+        ang = rng.uniform(0, 2 * math.pi, size=(cells + 1, cells + 1))
+        gx, gy = np.cos(ang), np.sin(ang)
+        t = (np.arange(res) + 0.5) / res * cells
+        i0 = np.floor(t).astype(int)
+        f = t - i0
+        fy, fx = np.meshgrid(f, f, indexing="ij")
+        iy, ix = np.meshgrid(i0, i0, indexing="ij")
+
+        def dotg(dy, dx):
+            return gx[iy + dy, ix + dx] * (fx - dx) + gy[iy + dy, ix + dx] * (fy - dy)
+        sx = fx * fx * fx * (fx * (fx * 6 - 15) + 10)
+        sy = fy * fy * fy * (fy * (fy * 6 - 15) + 10)
+        n0 = dotg(0, 0) * (1 - sx) + dotg(0, 1) * sx
+        n1 = dotg(1, 0) * (1 - sx) + dotg(1, 1) * sx
+        out += amp * (n0 * (1 - sy) + n1 * sy)
+        total += amp
+        amp *= 0.5
+    return out / total * 1.5
+
+
+def albedo_texture(res: int = 512, seed: int = 0) -> np.ndarray:
+    """Seeded Perlin RGB albedo in [0.1, 0.9], (res, res, 3) float32."""
+    ch = [np.clip(0.5 + 0.4 * perlin2(res, seed * 3 + c), 0.1, 0.9) for c in range(3)]
+    return np.stack(ch, -1).astype(np.float32)
+
+
+def textured_room(seed: int = 0, width: int = 512, height: int = 512, albedo=None, env=None, tex_res: int = 512,
+                  env_w: int = 256, env_h: int = 128, kind=A.FF_MAT_DIFFUSE) -> Scene:
+    """The small room opened to the sky (no ceiling) for inverse rendering:
+    floor, walls and sphere carry one albedo texture (texture 0); the
+    environment map lights the room.  `albedo` (res, res, 3) and `env`
+    (env_h, env_w, 3) default to the hidden parameters: a seeded Perlin
+    albedo in [0.1, 0.9] and a synthetic sky."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.array([-5, 0, -5], np.float32), np.array([5, 10, 5], np.float32)
+    rP, rI = box_room(lo, hi)
+    keep = [0, 1, 4, 5, 6, 7, 8, 9, 10, 11]          # quads of box_room without the ceiling (2, 3)
+    tri_keep = np.concatenate([[2 * q, 2 * q + 1] for q in keep])
+    rI = rI[tri_keep]
+    # per-face uv: project on the two axes spanning each quad
+    rUV = np.zeros((len(rP), 2), np.float32)
+    for q in keep:
+        vs = np.unique(rI[2 * keep.index(q):2 * keep.index(q) + 2].ravel())
+        p = rP[vs]
+        span = p.max(0) - p.min(0)
+        axes = np.argsort(-span)[:2]
+        rUV[vs] = (p[:, axes] - lo[axes]) / (hi[axes] - lo[axes])
+    tri = rP[rI].astype(np.float64)
+    rn = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    rn /= np.linalg.norm(rn, axis=1, keepdims=True)
+    rN = np.zeros_like(rP)
+    for t, (i0, i1, i2) in enumerate(rI):
+        rN[[i0, i1, i2]] = rn[t]
+    radius = float(rng.uniform(1.0, 2.0))
+    center = np.array([rng.uniform(-2.5, 2.5), rng.uniform(radius + 0.5, 5.0), rng.uniform(-2.5, 2.5)])
+    sP, sI, sN = uv_sphere(center, radius)
+    d = (sP - center) / radius
+    sUV = np.stack([np.arctan2(d[:, 2], d[:, 0]) / (2 * math.pi) + 0.5, np.arccos(np.clip(d[:, 1], -1, 1)) / math.pi],
+                   -1).astype(np.float32)
+    P = np.concatenate([rP, sP]).astype(np.float32)
+    N = np.concatenate([rN, sN]).astype(np.float32)
+    UV = np.concatenate([rUV, sUV]).astype(np.float32)
+    I = np.concatenate([rI, sI + len(rP)]).astype(np.uint32)
+    mat_ids = np.zeros(len(I), np.uint32)
+    mats = [material((0.5, 0.5, 0.5), kind=kind, roughness=1.0, base_color_tex=0)]
+    tex = albedo_texture(tex_res, seed) if albedo is None else np.asarray(albedo, np.float32)
+    sky = sky_env(env_w, env_h, seed=seed, sun_radiance=300.0, sun_diameter_deg=6.0) if env is None else env
+    cam = make_camera(eye=(0.0, 8.0, 4.9), center=(center[0], center[1], center[2]), fovy=70.0, aspect=width / height,
+                      near=0.05, far=60.0)
+    return Scene(positions=P, indices=I, normals=N, texcoords=UV, material_ids=mat_ids, materials=mats,
+                 env_rgb=np.asarray(sky, np.float32), textures=[tex], camera=cam, width=width, height=height)

@@ -279,6 +279,46 @@ typedef struct ff_render_stats {
 FF_API ff_status ff_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* settings,
                     ff_film* film, ff_render_stats* stats);
 
+/* -------------------------------------------------------------- adjoint */
+
+#define FF_ADJOINT_STORE_ALL 4u   /* ff_adjoint_desc.flags: store-all-vertices reference variant */
+#define FF_ENV_KEEP_TABLES   8u   /* ff_scene_set_environment: keep the importance tables */
+
+/* Gradient request of ff_render_adjoint.  d_image is dL/dI for the mean
+ * radiance image I (width*height*3 floats).  Gradients are ADDED to
+ * grad_texture (texels*3 floats of texture `texture`) and grad_env
+ * (env texels*3 floats).  flags: FF_MEM_DEVICE when every pointer is device
+ * memory, FF_ADJOINT_STORE_ALL for the store-all reference variant. */
+typedef struct ff_adjoint_desc {
+    uint32_t width, height;
+    const float* d_image;
+    int32_t texture;          /* texture receiving gradients, -1 = none */
+    float* grad_texture;
+    float* grad_env;          /* NULL = no environment gradient */
+    uint32_t flags;
+} ff_adjoint_desc;
+
+/* Path-replay adjoint of ff_render (no counterpart in the reference, which
+ * renders only): the same paths as ff_render in FF_MODE_CORRECTED for the same
+ * settings (seed, spp, sample_offset, depths, light), replayed from their
+ * seeds; gradients of the albedo texture of FF_MAT_DIFFUSE surfaces and of the
+ * environment map (camera misses and NEE), with detached sampling.
+ * settings->mode must be FF_MODE_CORRECTED.  stats: rays traced, samples,
+ * device time. */
+FF_API ff_status ff_render_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_settings* settings,
+                                   const ff_adjoint_desc* desc, ff_render_stats* stats);
+
+/* Replace the texels of texture `index` (same size; width*height*3 floats).
+ * flags: FF_MEM_DEVICE for a device pointer.  No counterpart in the reference,
+ * whose textures are immutable CUDA texture objects (dTexture.cu:21-111). */
+FF_API ff_status ff_scene_set_texture(ff_scene* scene, uint32_t index, const float* rgb, uint32_t flags);
+
+/* Replace the environment map's texels (same size) and rebuild its
+ * importance tables, unless flags has FF_ENV_KEEP_TABLES.  flags may also hold
+ * FF_MEM_DEVICE.  No counterpart in the reference (add_environment_light,
+ * kernel.cu:742-771, runs once at scene load). */
+FF_API ff_status ff_scene_set_environment(ff_scene* scene, const float* rgb, uint32_t flags);
+
 /* Environment-map importance tables (kernel.cu:65-149): the marginal CDF
  * (height doubles), the conditional CDFs (height*width doubles, row-major) and
  * the pdf texture (height*width floats, already scaled by w*h/(2*pi^2)), as

@@ -55,7 +55,14 @@ typedef struct {
     float roughness;
     float metallic;
     int32_t kind;          /* 0 mix (wf_mat_mix), 1 diffuse (wf_mat_diffuse), 2 conductor (wf_mat_cook) */
+    int32_t base_color_tex;  /* -1 = none */
+    int32_t roughness_tex;   /* -1 = none */
 } ffo_material;
+
+typedef struct {
+    const float* rgb;      /* height x width x 3 */
+    int32_t width, height;
+} ffo_texture;
 
 typedef struct {
     float p0[3], a[3], b[3], normal[3];
@@ -68,6 +75,9 @@ typedef struct {
     const float* normals;       /* num_tris x 9: vertex normals n0 n1 n2 */
     const uint32_t* material_ids;
     int32_t num_tris;
+    const float* texcoords;     /* num_tris x 6: uv0 uv1 uv2, or NULL */
+    const ffo_texture* textures;
+    int32_t num_textures;
     const ffo_material* materials;
     int32_t num_materials;
     const ffo_area_light* area_lights;

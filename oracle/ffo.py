@@ -86,7 +86,12 @@ def shadow_hit(v0, v1, v2, o, d):
 # ------------------------------------------------------------------ render
 class ffo_material(C.Structure):
     _fields_ = [("base_color", C.c_float * 3), ("fresnel", C.c_float * 3), ("roughness", C.c_float),
-                ("metallic", C.c_float), ("kind", C.c_int32)]
+                ("metallic", C.c_float), ("kind", C.c_int32), ("base_color_tex", C.c_int32),
+                ("roughness_tex", C.c_int32)]
+
+
+class ffo_texture(C.Structure):
+    _fields_ = [("rgb", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32)]
 
 
 class ffo_area_light(C.Structure):
@@ -96,7 +101,8 @@ class ffo_area_light(C.Structure):
 
 class ffo_render_desc(C.Structure):
     _fields_ = [("tris", C.c_void_p), ("normals", C.c_void_p), ("material_ids", C.c_void_p),
-                ("num_tris", C.c_int32), ("materials", C.c_void_p), ("num_materials", C.c_int32),
+                ("num_tris", C.c_int32), ("texcoords", C.c_void_p), ("textures", C.c_void_p),
+                ("num_textures", C.c_int32), ("materials", C.c_void_p), ("num_materials", C.c_int32),
                 ("area_lights", C.c_void_p), ("num_area_lights", C.c_int32),
                 ("env_rgb", C.c_void_p), ("env_w", C.c_int32), ("env_h", C.c_int32), ("env_color", C.c_float * 3),
                 ("cam_inv", C.c_float * 16), ("cam_lens_radius", C.c_float), ("cam_focal", C.c_float),
@@ -124,6 +130,14 @@ def render(scene, width, height, spp, max_depth=3, rr_depth=3, seed=0, mode=0, l
             mats[i].base_color[k] = m.base_color[k]
             mats[i].fresnel[k] = m.fresnel[k]
         mats[i].roughness, mats[i].metallic, mats[i].kind = m.roughness, m.metallic, m.kind
+        mats[i].base_color_tex, mats[i].roughness_tex = m.base_color_tex, m.roughness_tex
+    texs = [np.ascontiguousarray(t, np.float32) for t in getattr(scene, "textures", [])]
+    tdesc = (ffo_texture * max(1, len(texs)))()
+    for i, t in enumerate(texs):
+        tdesc[i].rgb, tdesc[i].width, tdesc[i].height = t.ctypes.data, t.shape[1], t.shape[0]
+    tc = None
+    if scene.texcoords is not None:
+        tc = np.ascontiguousarray(scene.texcoords[scene.indices].reshape(-1, 6), np.float32)
     lights = (ffo_area_light * max(1, len(scene.area_lights)))()
     for i, L in enumerate(scene.area_lights):
         for f in ("p0", "a", "b", "normal", "emissive"):
@@ -135,6 +149,8 @@ def render(scene, width, height, spp, max_depth=3, rr_depth=3, seed=0, mode=0, l
     d.tris, d.normals = tris.ctypes.data, nrm.ctypes.data
     d.material_ids = None if mids is None else mids.ctypes.data
     d.num_tris = len(tris)
+    d.texcoords = None if tc is None else tc.ctypes.data
+    d.textures, d.num_textures = C.cast(tdesc, C.c_void_p), len(texs)
     d.materials, d.num_materials = C.cast(mats, C.c_void_p), len(scene.materials)
     d.area_lights, d.num_area_lights = C.cast(lights, C.c_void_p), len(scene.area_lights)
     d.env_rgb = None if env is None else env.ctypes.data

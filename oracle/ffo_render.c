@@ -138,11 +138,13 @@ static double geo_atten(v3 wi, v3 wo, v3 n, float r)
     return g1 * g2;
 }
 static double power_heuristic(double f, double g) { return (f * f) / (f * f + g * g); }
-static v3 f0_of(const ffo_material* m, v3 a) { return lerp3(ld3(m->fresnel), a, m->metallic); }
-static v3 diff_f(const ffo_material* mat, v3 wi, v3 wo)
+/* a material resolved at a hit point (get_albedo / get_roughness, dMaterial.cu:10-43) */
+typedef struct { v3 albedo; v3 fresnel; float roughness, metallic; int kind; } surf_t;
+static v3 f0_of(const surf_t* m, v3 a) { return lerp3(m->fresnel, a, m->metallic); }
+static v3 diff_f(const surf_t* mat, v3 wi, v3 wo)
 {
     float m = mat->metallic;
-    v3 a = ld3(mat->base_color);
+    v3 a = mat->albedo;
     v3 f0 = f0_of(mat, a);
     v3 wh = normalize(add(wo, wi));
     v3 F = fresnel3(f0, wh, wi);
@@ -157,10 +159,10 @@ static float spec_get_pdf(v3 n, v3 wi, v3 wo, float r)
     double D = ggx_ndf(n, wh, r);
     return (float)((D * whn) / (double)hmax((float)(4.0 * wowh), 0.001f));
 }
-static v3 spec_f(const ffo_material* mat, v3 n, v3 wi, v3 wo)
+static v3 spec_f(const surf_t* mat, v3 n, v3 wi, v3 wo)
 {
     float r = mat->roughness;
-    v3 a = ld3(mat->base_color);
+    v3 a = mat->albedo;
     v3 f0 = f0_of(mat, a);
     v3 wh = normalize(add(wo, wi));
     double ndwi = hmax(dot(n, wi), 0.f), ndwo = hmax(dot(n, wo), 0.f);
@@ -187,8 +189,8 @@ static v3 spec_sample(v3 N, v3 wo, float r, float e0, float e1)
     v3 s = add(add(muls(T, h.x), muls(N, h.y)), muls(B, h.z));
     return neg(reflect(wo, normalize(s)));
 }
-static v3 brdf_f(const ffo_material* m, v3 n, v3 wi, v3 wo) { return add(spec_f(m, n, wi, wo), diff_f(m, wi, wo)); }
-static float brdf_pdf(const ffo_material* m, v3 n, v3 wi, v3 wo)
+static v3 brdf_f(const surf_t* m, v3 n, v3 wi, v3 wo) { return add(spec_f(m, n, wi, wo), diff_f(m, wi, wo)); }
+static float brdf_pdf(const surf_t* m, v3 n, v3 wi, v3 wo)
 {
     float sp = spec_get_pdf(n, wi, wo, m->roughness);
     float dp = (float)diff_get_pdf();
@@ -434,7 +436,7 @@ typedef struct {
     float ext_pdf, ext_cos;
 } shade_t;
 
-static void shade_mix(const light_ctx* lc, int corrected, const ffo_material* mat, v3 pos, v3 n, v3 wo, v3 wi,
+static void shade_mix(const light_ctx* lc, int corrected, const surf_t* mat, v3 pos, v3 n, v3 wo, v3 wi,
                       uint32_t key, uint32_t L, shade_t* o)
 {
     float r = mat->roughness;
@@ -498,7 +500,7 @@ static void shade_mix(const light_ctx* lc, int corrected, const ffo_material* ma
     o->ext_cos = hmax(0.f, dot(n, dir));
 }
 
-static void shade_diffuse(const light_ctx* lc, int corrected, const ffo_material* mat, v3 pos, v3 n, v3 wo, v3 wi,
+static void shade_diffuse(const light_ctx* lc, int corrected, const surf_t* mat, v3 pos, v3 n, v3 wo, v3 wi,
                           uint32_t key, uint32_t L, shade_t* o)
 {
     o->c_nee = V(0, 0, 0);
@@ -516,7 +518,7 @@ static void shade_diffuse(const light_ctx* lc, int corrected, const ffo_material
     o->ext_cos = hmax(0.f, dot(n, dir));
 }
 
-static void shade_conductor(const light_ctx* lc, int corrected, const ffo_material* mat, v3 pos, v3 n, v3 wo, v3 wi,
+static void shade_conductor(const light_ctx* lc, int corrected, const surf_t* mat, v3 pos, v3 n, v3 wo, v3 wi,
                             uint32_t key, uint32_t L, shade_t* o)
 {
     o->c_nee = V(0, 0, 0);
@@ -635,7 +637,29 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc, int px, i
             sp = rect_sample(&lc->rect, R2(key, L, DIM_LIGHT));
             wi = normalize(sub(sp, pos));
         }
-        const ffo_material* mat = &d->materials[d->material_ids ? d->material_ids[prim] : 0];
+        const ffo_material* mm = &d->materials[d->material_ids ? d->material_ids[prim] : 0];
+        surf_t sf;
+        sf.albedo = ld3(mm->base_color);
+        sf.fresnel = ld3(mm->fresnel);
+        sf.roughness = mm->roughness;
+        sf.metallic = mm->metallic;
+        sf.kind = mm->kind;
+        if (d->texcoords && (mm->base_color_tex >= 0 || mm->roughness_tex >= 0)) {
+            /* texcoord = u * uv1 + v * uv2 + (1 - u - v) * uv0 (dTriangle.cu:97) */
+            const float* tc = d->texcoords + 6 * (size_t)prim;
+            float wuv = (1.f - u) - v;
+            float tu = u * tc[2] + v * tc[4] + wuv * tc[0];
+            float tv = u * tc[3] + v * tc[5] + wuv * tc[1];
+            if (mm->base_color_tex >= 0) {
+                const ffo_texture* tx = &d->textures[mm->base_color_tex];
+                sf.albedo = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv);
+            }
+            if (mm->roughness_tex >= 0) {
+                const ffo_texture* tx = &d->textures[mm->roughness_tex];
+                sf.roughness = hmax(tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv).x, 0.01f);
+            }
+        }
+        const surf_t* mat = &sf;
         v3 wo = neg(dir);
         memset(&sh, 0, sizeof(sh));
         if (mat->kind == 0) shade_mix(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
@@ -738,10 +762,11 @@ int ffo_render(const ffo_render_desc* d, double* out_rgb, uint64_t* stats)
  * vectors of tests/golden/ (made from the reference's own routines).
  * mat8 = base[3], fresnel[3], roughness, metallic; vectors are float[3].
  * ------------------------------------------------------------------- */
-static ffo_material mat_of(const float* m8)
+static surf_t mat_of(const float* m8)
 {
-    ffo_material m;
-    for (int k = 0; k < 3; ++k) { m.base_color[k] = m8[k]; m.fresnel[k] = m8[3 + k]; }
+    surf_t m;
+    m.albedo = V(m8[0], m8[1], m8[2]);
+    m.fresnel = V(m8[3], m8[4], m8[5]);
     m.roughness = m8[6];
     m.metallic = m8[7];
     m.kind = 0;
@@ -752,7 +777,7 @@ static void st3(float* o, v3 v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; }
 /* out: diff_f[3], spec_f[3], spec_pdf, BRDF_pdf, BRDF_f[3], fresnel[3], D, G, diff_pdf (17) */
 void ffo_probe_material(const float* m8, const float* n3, const float* wi3, const float* wo3, float* out)
 {
-    ffo_material m = mat_of(m8);
+    surf_t m = mat_of(m8);
     v3 n = ld3(n3), wi = ld3(wi3), wo = ld3(wo3);
     st3(out, diff_f(&m, wi, wo));
     st3(out + 3, spec_f(&m, n, wi, wo));
@@ -760,7 +785,7 @@ void ffo_probe_material(const float* m8, const float* n3, const float* wi3, cons
     out[7] = brdf_pdf(&m, n, wi, wo);
     st3(out + 8, brdf_f(&m, n, wi, wo));
     v3 wh = normalize(add(wo, wi));
-    st3(out + 11, fresnel3(ld3(m.fresnel), wh, wi));
+    st3(out + 11, fresnel3(m.fresnel, wh, wi));
     out[14] = (float)ggx_ndf(n, wh, m.roughness);
     out[15] = (float)geo_atten(wi, wo, n, m.roughness);
     out[16] = (float)diff_get_pdf();

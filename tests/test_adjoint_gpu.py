@@ -1,0 +1,138 @@
+"""Path-replay adjoint: against the store-all-vertices adjoint, against FP64
+central finite differences with common random numbers (same seeds, so every
+path not touching the perturbed texel is bit-identical between the two
+renders), and through torch.autograd."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from firefly_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+W = H = 48
+SET = dict(spp=8, max_depth=3, rr_depth=3, seed=3, light=-1)   # rr_depth = max_depth: no roulette
+
+
+@pytest.fixture(scope="module")
+def setup(ctx):
+    import firefly_b200 as ff
+    target = scenes.textured_room(seed=0, width=W, height=H, tex_res=32, env_w=32, env_h=16)
+    start = scenes.textured_room(seed=0, width=W, height=H, tex_res=32, env_w=32, env_h=16,
+                                 albedo=np.full((32, 32, 3), 0.5, np.float32))
+    ds = ff.dScene(ctx, start)
+    pt = ff.PathTracer(ctx, W, H)
+    # reference image from the hidden parameters
+    ds.set_texture(0, target.textures[0])
+    pt.draw(ds, mode=ff.FF_MODE_CORRECTED, **SET)
+    ref = pt.image().astype(np.float64)
+    ds.set_texture(0, start.textures[0])
+    yield ds, pt, start, target, ref
+    pt.close()
+    ds.close()
+
+
+def loss_and_grad_image(pt, ds, ref, **kw):
+    import firefly_b200 as ff
+    pt.clear_buffer()
+    pt.draw(ds, mode=ff.FF_MODE_CORRECTED, **{**SET, **kw})
+    img = pt.image().astype(np.float64)
+    diff = img - ref
+    return 0.5 * float((diff * diff).sum()) / diff.size, (diff / diff.size).astype(np.float32)
+
+
+def test_replay_matches_store_all(setup):
+    ds, pt, start, target, ref = setup
+    _, dimg = loss_and_grad_image(pt, ds, ref)
+    g1, e1 = np.zeros_like(start.textures[0]), np.zeros_like(start.env_rgb)
+    g2, e2 = np.zeros_like(start.textures[0]), np.zeros_like(start.env_rgb)
+    st = ds.render_adjoint(W, H, dimg, grad_texture=g1, grad_env=e1, **SET)
+    ds.render_adjoint(W, H, dimg, grad_texture=g2, grad_env=e2, store_all=True, **SET)
+    assert st["samples"] == W * H * SET["spp"] and st["extension_rays"] > 0
+    assert np.abs(g1).max() > 0 and np.abs(e1).max() > 0
+    assert np.allclose(g1, g2, rtol=1e-4, atol=1e-7 * np.abs(g1).max())
+    assert np.allclose(e1, e2, rtol=1e-4, atol=1e-7 * np.abs(e1).max())
+
+
+def test_albedo_gradient_vs_central_differences(setup):
+    ds, pt, start, target, ref = setup
+    _, dimg = loss_and_grad_image(pt, ds, ref)
+    g = np.zeros_like(start.textures[0])
+    ds.render_adjoint(W, H, dimg, grad_texture=g, **SET)
+    rng = np.random.default_rng(1)
+    flat = np.abs(g).reshape(-1)
+    # 64 texel channels among those the camera's paths reach
+    cand = np.nonzero(flat > 1e-3 * flat.max())[0]
+    picks = rng.choice(cand, size=min(64, len(cand)), replace=False)
+    eps = 1e-3
+    tex = start.textures[0].copy()
+    fd = []
+    for k in picks:
+        t = tex.copy().reshape(-1)
+        t[k] += eps
+        ds.set_texture(0, t.reshape(tex.shape))
+        lp, _ = loss_and_grad_image(pt, ds, ref)
+        t[k] -= 2 * eps
+        ds.set_texture(0, t.reshape(tex.shape))
+        lm, _ = loss_and_grad_image(pt, ds, ref)
+        fd.append((lp - lm) / (2 * eps))
+    ds.set_texture(0, tex)
+    fd = np.array(fd)
+    ad = g.reshape(-1)[picks].astype(np.float64)
+    rel = np.abs(ad - fd) / np.maximum(np.abs(fd), 1e-12)
+    print(f"[adjoint] albedo FD: median rel err {np.median(rel):.2e}, max {rel.max():.2e}, n={len(picks)}")
+    assert np.median(rel) < 1e-2
+    assert np.mean(rel < 5e-2) > 0.9
+    assert np.corrcoef(ad, fd)[0, 1] > 0.999
+
+
+def test_env_gradient_vs_central_differences(setup):
+    ds, pt, start, target, ref = setup
+    _, dimg = loss_and_grad_image(pt, ds, ref)
+    e = np.zeros_like(start.env_rgb)
+    ds.render_adjoint(W, H, dimg, grad_env=e, texture=-1, **SET)
+    flat = np.abs(e).reshape(-1)
+    picks = np.argsort(-flat)[:24]
+    env = start.env_rgb.copy()
+    fd = []
+    for k in picks:
+        eps = 1e-3 * max(1.0, abs(env.reshape(-1)[k]))
+        x = env.copy().reshape(-1)
+        x[k] += eps
+        ds.set_environment(x.reshape(env.shape), keep_tables=True)
+        lp, _ = loss_and_grad_image(pt, ds, ref)
+        x[k] -= 2 * eps
+        ds.set_environment(x.reshape(env.shape), keep_tables=True)
+        lm, _ = loss_and_grad_image(pt, ds, ref)
+        fd.append((lp - lm) / (2 * eps))
+    ds.set_environment(env, keep_tables=True)
+    fd = np.array(fd)
+    ad = e.reshape(-1)[picks].astype(np.float64)
+    rel = np.abs(ad - fd) / np.maximum(np.abs(fd), 1e-12)
+    print(f"[adjoint] env FD: median rel err {np.median(rel):.2e}, max {rel.max():.2e}, n={len(picks)}")
+    assert np.median(rel) < 1e-2
+    assert np.corrcoef(ad, fd)[0, 1] > 0.999
+
+
+def test_autograd_descent_reduces_loss(setup):
+    from tests.ff_autograd import RenderFn
+    ds, pt, start, target, ref = setup
+    albedo = torch.from_numpy(start.textures[0].copy()).requires_grad_(True)
+    env = torch.from_numpy(start.env_rgb.copy()).requires_grad_(True)
+    opt = torch.optim.Adam([albedo], lr=2e-2)
+    reft = torch.from_numpy(ref.astype(np.float32))
+    losses = []
+    for it in range(15):
+        opt.zero_grad()
+        img = RenderFn.apply(albedo, env, ds, pt, {**SET, "seed": 100 + it, "keep_tables": True})
+        loss = 0.5 * ((img - reft) ** 2).mean()
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            albedo.clamp_(0.01, 1.0)
+        losses.append(float(loss))
+    print(f"[adjoint] autograd loss {losses[0]:.4e} -> {losses[-1]:.4e}")
+    assert losses[-1] < 0.7 * losses[0]
+    ds.set_texture(0, start.textures[0])
