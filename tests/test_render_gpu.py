@@ -126,3 +126,19 @@ def test_render_argument_errors(ctx):
         pt.draw(ds, spp=0, light=0)
     pt.close()
     ds.close()
+
+
+def test_textured_env_scene_parity(ctx, oracle):
+    """Albedo texture (bilinear, wrap, 8-bit weights as the reference's texture
+    units filter) on room and sphere, lit by the environment map."""
+    import firefly_b200 as ff
+    scn = scenes.textured_room(seed=4, width=48, height=48, tex_res=64, env_w=64, env_h=32)
+    for mode in (ff.FF_MODE_PARITY, ff.FF_MODE_CORRECTED):
+        got, n, stats = _gpu_render(ctx, scn, 48, 48, 4, light=-1, max_depth=4, rr_depth=3, seed=9, mode=mode)
+        ref, _ = oracle.render(scn, 48, 48, 4, max_depth=4, rr_depth=3, seed=9, mode=mode, light=-1,
+                               threads=cpu_threads())
+        fin = np.isfinite(got) & np.isfinite(ref)
+        assert np.array_equal(np.isfinite(got), np.isfinite(ref))
+        mre = _mre(got[fin], ref[fin])
+        print(f"[parity] textured env mode={mode}: mre={mre:.3e}")
+        assert mre <= MRE_TOL
