@@ -496,13 +496,75 @@ def run_render(args, ws, rank, local, dist):
     ctx.close()
 
 
+INVERSE_WORKLOAD = ("inverse rendering on the room opened to the sky at 512x512: hidden 512x512 Perlin albedo in "
+                    "[0.1, 0.9] + 256x128 sky; target at 256 spp; start 0.5 albedo + flat env; 16-spp path-replay "
+                    "adjoint, Adam lr 1e-2, 200 steps")
+
+
+def inverse_experiment(ctx, steps=200, res=512, dev=None):
+    """C4 workload; returns a dict of results (timings, losses, parameter errors)."""
+    import torch
+    import firefly_b200 as ff
+    from firefly_b200 import inverse, scenes
+    hidden = scenes.textured_room(seed=0, width=res, height=res, tex_res=512, env_w=256, env_h=128)
+    flat_env = np.full_like(hidden.env_rgb, float(hidden.env_rgb[hidden.env_rgb < 100].mean()))
+    start = scenes.textured_room(seed=0, width=res, height=res, albedo=np.full((512, 512, 3), 0.5, np.float32),
+                                 env=flat_env)
+    ds = ff.dScene(ctx, hidden)
+    pt = ff.PathTracer(ctx, res, res)
+    t0 = time.perf_counter()
+    pt.draw(ds, spp=256, max_depth=3, rr_depth=3, seed=12345, light=-1, mode=ff.FF_MODE_CORRECTED)
+    target = torch.from_numpy(pt.image().astype(np.float32)).to(dev)
+    t_target = time.perf_counter() - t0
+    albedo = torch.from_numpy(start.textures[0].copy()).to(dev)
+    env = torch.from_numpy(start.env_rgb.copy()).to(dev)
+    tex_err0 = float(np.sqrt(((start.textures[0] - hidden.textures[0]) ** 2).mean()))
+    t0 = time.perf_counter()
+    res_opt = inverse.optimize(ds, pt, target, albedo, env, steps=steps, spp=16, lr=1e-2, max_depth=3, rr_depth=3)
+    wall = time.perf_counter() - t0
+    tex_err1 = float(np.sqrt(((albedo.cpu().numpy() - hidden.textures[0]) ** 2).mean()))
+    e_h = hidden.env_rgb
+    sky = e_h < 100
+    env_err = lambda e: float(np.abs(e[sky] - e_h[sky]).mean() / np.abs(e_h[sky]).mean())
+    out = {"workload": INVERSE_WORKLOAD, "steps": steps, "wall_s": round(wall, 2),
+           "adjoint_spp_per_s": round(res_opt["adjoint_spp_per_s"], 1),
+           "adjoint_ms_per_step": round(res_opt["ms_adjoint"] / steps, 3),
+           "primal_ms_per_step": round(res_opt["ms_primal"] / steps, 3), "target_render_s": round(t_target, 2),
+           "loss_first": res_opt["losses"][0], "loss_last": res_opt["losses"][-1],
+           "albedo_rmse_start": round(tex_err0, 4), "albedo_rmse_end": round(tex_err1, 4),
+           "env_rel_err_start": round(env_err(flat_env), 4), "env_rel_err_end": round(env_err(env.cpu().numpy()), 4)}
+    pt.close()
+    ds.close()
+    return out
+
+
+def run_inverse(args, ws, rank, local, dist):
+    import torch
+    import firefly_b200 as ff
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx = ff.Context(local, stream=stream.cuda_stream)
+    clocks = ClockSampler(local)
+    clocks.start()
+    r = inverse_experiment(ctx, steps=args.steps if args.steps > 5 else 200, dev=dev)
+    clk = clocks.stop()
+    if rank == 0:
+        line = {"metric": "adjoint spp/s", "value": r["adjoint_spp_per_s"], "unit": "samples/s", "n_gpus": ws,
+                "steps": r["steps"], "warmup": 0, "ms_per_step": r["adjoint_ms_per_step"] + r["primal_ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": r, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["render", "trace"], default="render")
+    ap.add_argument("--workload", choices=["render", "trace", "inverse"], default="render")
     ap.add_argument("--rays", type=int, default=RAYS_PER_SET, help="trace workload: rays per batch")
     ap.add_argument("--cpu-s", type=float, default=15.0, help="target seconds of CPU-baseline work")
     ap.add_argument("--ref-step-s", type=float, default=6.0, help="reference arm: seconds of CPU work per step")
@@ -518,6 +580,8 @@ def main(argv=None):
     ws, rank, local, dist = setup_dist()
     if args.workload == "render":
         run_render(args, ws, rank, local, dist)
+    elif args.workload == "inverse":
+        run_inverse(args, ws, rank, local, dist)
     else:
         run_trace(args, ws, rank, local, dist)
     if dist is not None:

@@ -101,6 +101,11 @@ class ff_adjoint_desc(C.Structure):
                 ("grad_texture", C.c_void_p), ("grad_env", C.c_void_p), ("flags", C.c_uint32)]
 
 
+class ff_adam_params(C.Structure):
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float), ("lo", C.c_float),
+                ("hi", C.c_float), ("step", C.c_uint32)]
+
+
 # Every symbol include/firefly_b200.h declares, with its ctypes signature.
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
@@ -127,6 +132,7 @@ SIGNATURES = {
                                     C.POINTER(ff_render_stats)]),
     "ff_scene_set_texture": (C.c_int, [P, C.c_uint32, P, C.c_uint32]),
     "ff_scene_set_environment": (C.c_int, [P, P, C.c_uint32]),
+    "ff_optimizer_adam_step": (C.c_int, [P, P, P, P, P, C.c_uint64, C.POINTER(ff_adam_params)]),
 }
 
 _lib = None

@@ -420,3 +420,46 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
         stats->kernel_launches = 1;
     }
 }
+
+namespace {
+
+// One Adam step (Kingma & Ba 2015) with bias correction, then a clamp of the
+// parameter to [lo, hi]: m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2,
+// p -= lr * (m / (1-b1^t)) / (sqrt(v / (1-b2^t)) + eps).
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       uint64_t n, float lr, float b1, float b2, float eps, float c1, float c2, float lo, float hi)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float step = lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    p[i] = fminf(fmaxf(p[i] - step, lo), hi);
+}
+
+}  // namespace
+
+extern "C" ff_status ff_optimizer_adam_step(ff_context* ctx, float* param, const float* grad, float* m, float* v,
+                                            uint64_t n, const ff_adam_params* hp)
+{
+    if (!ctx || !param || !grad || !m || !v || !hp) return FF_ERR_INVALID_ARG;
+    if (n == 0) return FF_OK;
+    try {
+        FF_CUDA_CHECK(cudaSetDevice(ctx->device));
+        FF_REQUIRE(hp->step >= 1, "Adam step counts from 1");
+        const float c1 = 1.f - powf(hp->beta1, (float)hp->step);
+        const float c2 = 1.f - powf(hp->beta2, (float)hp->step);
+        const uint64_t blocks = (n + 255) / 256;
+        FF_REQUIRE(blocks < (1ull << 31), "parameter vector too large");
+        k_adam<<<(unsigned)blocks, 256, 0, ctx->stream>>>(param, grad, m, v, n, hp->lr, hp->beta1, hp->beta2, hp->eps,
+                                                         c1, c2, hp->lo, hp->hi);
+        FF_CUDA_CHECK(cudaGetLastError());
+        return FF_OK;
+    } catch (const FFError& e) {
+        ctx->last_error = e.msg;
+        return e.status;
+    }
+}

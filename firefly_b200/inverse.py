@@ -1,0 +1,79 @@
+"""Inverse rendering with the path-replay adjoint: recover an albedo texture
+and an environment map from a target image.
+
+Every iteration renders the current parameters (ff_render, corrected mode),
+forms dL/dI of L = 0.5 * mean((I - target)^2), runs ff_render_adjoint with the
+same seed and settings, and applies one Adam step per parameter
+(ff_optimizer_adam_step); the environment's importance tables are rebuilt
+from the updated map.  Parameters, gradients, moments and images stay on the
+device (torch tensors are used only as device buffers).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+from . import _abi as A
+from . import lib
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, lr: float = 1e-2,
+             max_depth: int = 3, rr_depth: int = 3, seed: int = 0, light: int = -1, texture: int = 0,
+             callback=None) -> dict:
+    """target: device float32 [h, w, 3]; albedo [th, tw, 3] and env [eh, ew, 3]:
+    device float32 tensors updated in place.  Returns timings and the loss
+    history."""
+    import torch
+    L = lib()
+    ctx = ds.ctx
+    dev = albedo.device
+    h, w = target.shape[:2]
+    g_tex, g_env = torch.zeros_like(albedo), torch.zeros_like(env)
+    m_tex, v_tex, m_env, v_env = (torch.zeros_like(x) for x in (albedo, albedo, env, env))
+    rgba = torch.empty((h, w, 4), dtype=torch.float32, device=dev)
+    cnt = torch.empty((h, w), dtype=torch.int32, device=dev)
+    losses, t_primal, t_adjoint, adj_samples = [], 0.0, 0.0, 0
+    for it in range(steps):
+        torch.cuda.synchronize(dev)
+        rc = L.ff_scene_set_texture(ds.handle, texture, _p(albedo), A.FF_MEM_DEVICE)
+        rc |= L.ff_scene_set_environment(ds.handle, _p(env), A.FF_MEM_DEVICE)
+        if rc:
+            raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
+        tracer.clear_buffer()
+        st = tracer.draw(ds, spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed + it, light=light,
+                         mode=A.FF_MODE_CORRECTED)
+        t_primal += st["ms_total"]
+        rc = L.ff_film_read(tracer.film, _p(rgba), _p(cnt), A.FF_MEM_DEVICE)
+        if rc:
+            raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
+        img = rgba[..., :3] / cnt.clamp(min=1)[..., None].float()
+        diff = img - target
+        losses.append(float(0.5 * (diff * diff).mean()))
+        d_image = (diff / diff.numel()).contiguous()
+        g_tex.zero_()
+        g_env.zero_()
+        s = A.ff_render_settings(spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed + it,
+                                 mode=A.FF_MODE_CORRECTED, light=light, max_paths=0, sample_offset=0, flags=0,
+                                 shadow_offset=0.001)
+        d = A.ff_adjoint_desc(width=w, height=h, d_image=d_image.data_ptr(), texture=texture,
+                              grad_texture=g_tex.data_ptr(), grad_env=g_env.data_ptr(), flags=A.FF_MEM_DEVICE)
+        ast = A.ff_render_stats()
+        rc = L.ff_render_adjoint(ctx.handle, ds.handle, C.byref(s), C.byref(d), C.byref(ast))
+        if rc:
+            raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
+        t_adjoint += ast.ms_total
+        adj_samples += ast.samples
+        for prm, g, m, v, hi in ((albedo, g_tex, m_tex, v_tex, 1.0), (env, g_env, m_env, v_env, 1e6)):
+            hp = A.ff_adam_params(lr=lr, beta1=0.9, beta2=0.999, eps=1e-8, lo=1e-3, hi=hi, step=it + 1)
+            rc = L.ff_optimizer_adam_step(ctx.handle, _p(prm), _p(g), _p(m), _p(v), prm.numel(), C.byref(hp))
+            if rc:
+                raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
+        if callback:
+            callback(it, losses[-1])
+    torch.cuda.synchronize(dev)
+    return {"losses": losses, "ms_primal": t_primal, "ms_adjoint": t_adjoint, "adjoint_samples": adj_samples,
+            "adjoint_spp_per_s": adj_samples / (t_adjoint / 1e3) if t_adjoint > 0 else 0.0}

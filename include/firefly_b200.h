@@ -319,6 +319,19 @@ FF_API ff_status ff_scene_set_texture(ff_scene* scene, uint32_t index, const flo
  * kernel.cu:742-771, runs once at scene load). */
 FF_API ff_status ff_scene_set_environment(ff_scene* scene, const float* rgb, uint32_t flags);
 
+/* Adam hyper-parameters and step number (from 1); the parameter is clamped
+ * to [lo, hi] after the update. */
+typedef struct ff_adam_params {
+    float lr, beta1, beta2, eps, lo, hi;
+    uint32_t step;
+} ff_adam_params;
+
+/* One Adam update of n device floats on the context's stream (asynchronous),
+ * for inverse rendering with ff_render_adjoint.  No counterpart in the
+ * reference.  param, grad, m, v are device pointers. */
+FF_API ff_status ff_optimizer_adam_step(ff_context* ctx, float* param, const float* grad, float* m, float* v,
+                                        uint64_t n, const ff_adam_params* hp);
+
 /* Environment-map importance tables (kernel.cu:65-149): the marginal CDF
  * (height doubles), the conditional CDFs (height*width doubles, row-major) and
  * the pdf texture (height*width floats, already scaled by w*h/(2*pi^2)), as
