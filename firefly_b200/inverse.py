@@ -23,10 +23,12 @@ def _p(t):
 
 def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, lr: float = 1e-2,
              max_depth: int = 3, rr_depth: int = 3, seed: int = 0, light: int = -1, texture: int = 0,
-             callback=None) -> dict:
+             lr_env: float | None = None, callback=None) -> dict:
     """target: device float32 [h, w, 3]; albedo [th, tw, 3] and env [eh, ew, 3]:
-    device float32 tensors updated in place.  Returns timings and the loss
+    device float32 tensors updated in place (env only when its learning rate,
+    lr_env, defaulting to lr, is non-zero).  Returns timings and the loss
     history."""
+    lr_env = lr if lr_env is None else lr_env
     import torch
     L = lib()
     ctx = ds.ctx
@@ -67,8 +69,10 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
             raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
         t_adjoint += ast.ms_total
         adj_samples += ast.samples
-        for prm, g, m, v, hi in ((albedo, g_tex, m_tex, v_tex, 1.0), (env, g_env, m_env, v_env, 1e6)):
-            hp = A.ff_adam_params(lr=lr, beta1=0.9, beta2=0.999, eps=1e-8, lo=1e-3, hi=hi, step=it + 1)
+        for prm, g, m, v, hi, rate in ((albedo, g_tex, m_tex, v_tex, 1.0, lr), (env, g_env, m_env, v_env, 1e6, lr_env)):
+            if rate == 0:
+                continue
+            hp = A.ff_adam_params(lr=rate, beta1=0.9, beta2=0.999, eps=1e-8, lo=1e-3, hi=hi, step=it + 1)
             rc = L.ff_optimizer_adam_step(ctx.handle, _p(prm), _p(g), _p(m), _p(v), prm.numel(), C.byref(hp))
             if rc:
                 raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
