@@ -2,8 +2,11 @@
 and an environment map from a target image.
 
 Every iteration renders the current parameters (ff_render, corrected mode),
-forms dL/dI of L = 0.5 * mean((I - target)^2), runs ff_render_adjoint with the
-same seed and settings, and applies one Adam step per parameter
+forms dL/dI of L = 0.5 * mean((I - target)^2), runs ff_render_adjoint with
+the same settings but an independent seed, and applies one Adam step per
+parameter.  The two passes must not share samples: with the same samples
+E[dL/dI * dI/dtheta] picks up the covariance of the estimate and the descent
+minimises the image's variance (darkening it) instead of its error
 (ff_optimizer_adam_step); the environment's importance tables are rebuilt
 from the updated map.  Parameters, gradients, moments and images stay on the
 device (torch tensors are used only as device buffers).
@@ -58,7 +61,7 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
         d_image = (diff / diff.numel()).contiguous()
         g_tex.zero_()
         g_env.zero_()
-        s = A.ff_render_settings(spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed + it,
+        s = A.ff_render_settings(spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed + it + 0x40000000,
                                  mode=A.FF_MODE_CORRECTED, light=light, max_paths=0, sample_offset=0, flags=0,
                                  shadow_offset=0.001)
         d = A.ff_adjoint_desc(width=w, height=h, d_image=d_image.data_ptr(), texture=texture,
