@@ -501,7 +501,7 @@ INVERSE_WORKLOAD = ("inverse rendering on the room opened to the sky at 512x512:
                     "adjoint, Adam lr 1e-2, 200 steps")
 
 
-def inverse_experiment(ctx, steps=200, res=512, dev=None):
+def inverse_experiment(ctx, steps=200, res=512, dev=None, known_lighting=False):
     """C4 workload; returns a dict of results (timings, losses, parameter errors)."""
     import torch
     import firefly_b200 as ff
@@ -517,16 +517,27 @@ def inverse_experiment(ctx, steps=200, res=512, dev=None):
     target = torch.from_numpy(pt.image().astype(np.float32)).to(dev)
     t_target = time.perf_counter() - t0
     albedo = torch.from_numpy(start.textures[0].copy()).to(dev)
-    env = torch.from_numpy(start.env_rgb.copy()).to(dev)
+    env = torch.from_numpy((hidden.env_rgb if known_lighting else start.env_rgb).copy()).to(dev)
     tex_err0 = float(np.sqrt(((start.textures[0] - hidden.textures[0]) ** 2).mean()))
     t0 = time.perf_counter()
-    res_opt = inverse.optimize(ds, pt, target, albedo, env, steps=steps, spp=16, lr=1e-2, max_depth=3, rr_depth=3)
+    res_opt = inverse.optimize(ds, pt, target, albedo, env, steps=steps, spp=16, lr=1e-2, max_depth=3, rr_depth=3,
+                               lr_env=0.0 if known_lighting else None)
     wall = time.perf_counter() - t0
     tex_err1 = float(np.sqrt(((albedo.cpu().numpy() - hidden.textures[0]) ** 2).mean()))
     e_h = hidden.env_rgb
     sky = e_h < 100
     env_err = lambda e: float(np.abs(e[sky] - e_h[sky]).mean() / np.abs(e_h[sky]).mean())
-    out = {"workload": INVERSE_WORKLOAD, "steps": steps, "wall_s": round(wall, 2),
+    # held-out image error (fresh seed, 64 spp) before and after
+    def heldout(tex, e):
+        ds.set_texture(0, tex)
+        ds.set_environment(e)
+        pt.clear_buffer()
+        pt.draw(ds, spp=64, max_depth=3, rr_depth=3, seed=777, light=-1, mode=ff.FF_MODE_CORRECTED)
+        return float(((pt.image() - target.cpu().numpy()) ** 2).mean())
+    h0 = heldout(start.textures[0], hidden.env_rgb if known_lighting else start.env_rgb)
+    h1 = heldout(albedo.cpu().numpy(), env.cpu().numpy())
+    out = {"workload": INVERSE_WORKLOAD + (" (known lighting: albedo only)" if known_lighting else ""),
+           "steps": steps, "wall_s": round(wall, 2), "heldout_mse_start": h0, "heldout_mse_end": h1,
            "adjoint_spp_per_s": round(res_opt["adjoint_spp_per_s"], 1),
            "adjoint_ms_per_step": round(res_opt["ms_adjoint"] / steps, 3),
            "primal_ms_per_step": round(res_opt["ms_primal"] / steps, 3), "target_render_s": round(t_target, 2),
@@ -548,6 +559,8 @@ def run_inverse(args, ws, rank, local, dist):
     clocks = ClockSampler(local)
     clocks.start()
     r = inverse_experiment(ctx, steps=args.steps if args.steps > 5 else 200, dev=dev)
+    r["known_lighting_run"] = inverse_experiment(ctx, steps=args.steps if args.steps > 5 else 200, dev=dev,
+                                                 known_lighting=True)
     clk = clocks.stop()
     if rank == 0:
         line = {"metric": "adjoint spp/s", "value": r["adjoint_spp_per_s"], "unit": "samples/s", "n_gpus": ws,

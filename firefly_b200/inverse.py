@@ -42,6 +42,9 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
     rgba = torch.empty((h, w, 4), dtype=torch.float32, device=dev)
     cnt = torch.empty((h, w), dtype=torch.int32, device=dev)
     losses, t_primal, t_adjoint, adj_samples = [], 0.0, 0.0, 0
+    # The library runs on the context's stream, torch on its current stream:
+    # every hand-over between the two waits for the producer (torch side:
+    # torch.cuda.synchronize; library side: ctx.sync).
     for it in range(steps):
         torch.cuda.synchronize(dev)
         rc = L.ff_scene_set_texture(ds.handle, texture, _p(albedo), A.FF_MEM_DEVICE)
@@ -55,12 +58,14 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
         rc = L.ff_film_read(tracer.film, _p(rgba), _p(cnt), A.FF_MEM_DEVICE)
         if rc:
             raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
+        ctx.sync()
         img = rgba[..., :3] / cnt.clamp(min=1)[..., None].float()
         diff = img - target
         losses.append(float(0.5 * (diff * diff).mean()))
         d_image = (diff / diff.numel()).contiguous()
         g_tex.zero_()
         g_env.zero_()
+        torch.cuda.synchronize(dev)
         s = A.ff_render_settings(spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed + it + 0x40000000,
                                  mode=A.FF_MODE_CORRECTED, light=light, max_paths=0, sample_offset=0, flags=0,
                                  shadow_offset=0.001)
@@ -79,6 +84,7 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
             rc = L.ff_optimizer_adam_step(ctx.handle, _p(prm), _p(g), _p(m), _p(v), prm.numel(), C.byref(hp))
             if rc:
                 raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
+        ctx.sync()
         if callback:
             callback(it, losses[-1])
     torch.cuda.synchronize(dev)
