@@ -26,11 +26,15 @@ def _p(t):
 
 def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, lr: float = 1e-2,
              max_depth: int = 3, rr_depth: int = 3, seed: int = 0, light: int = -1, texture: int = 0,
-             lr_env: float | None = None, callback=None) -> dict:
+             lr_env: float | None = None, lr_decay: float = 1.0, callback=None) -> dict:
     """target: device float32 [h, w, 3]; albedo [th, tw, 3] and env [eh, ew, 3]:
     device float32 tensors updated in place (env only when its learning rate,
-    lr_env, defaulting to lr, is non-zero).  Returns timings and the loss
-    history."""
+    lr_env, defaulting to lr, is non-zero).  Both rates fall geometrically by
+    the factor lr_decay over the run (1: constant): Adam's steps have the
+    size of the rate whatever the gradient's signal-to-noise ratio, so with a
+    constant rate the texels that few samples see keep drifting by about the
+    rate per step once their mean gradient is lost in the Monte Carlo noise.
+    Returns timings and the loss history."""
     lr_env = lr if lr_env is None else lr_env
     import torch
     L = lib()
@@ -77,10 +81,11 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
             raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
         t_adjoint += ast.ms_total
         adj_samples += ast.samples
+        fall = lr_decay ** (it / max(1, steps - 1))
         for prm, g, m, v, hi, rate in ((albedo, g_tex, m_tex, v_tex, 1.0, lr), (env, g_env, m_env, v_env, 1e6, lr_env)):
             if rate == 0:
                 continue
-            hp = A.ff_adam_params(lr=rate, beta1=0.9, beta2=0.999, eps=1e-8, lo=1e-3, hi=hi, step=it + 1)
+            hp = A.ff_adam_params(lr=rate * fall, beta1=0.9, beta2=0.999, eps=1e-8, lo=1e-3, hi=hi, step=it + 1)
             rc = L.ff_optimizer_adam_step(ctx.handle, _p(prm), _p(g), _p(m), _p(v), prm.numel(), C.byref(hp))
             if rc:
                 raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())

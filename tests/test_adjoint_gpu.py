@@ -140,24 +140,28 @@ def test_autograd_descent_reduces_loss(setup):
 
 def test_inverse_driver_on_device(ctx):
     """firefly_b200.inverse.optimize: device-resident parameters, native Adam
-    steps; the loss falls and the albedo moves toward the hidden one."""
+    steps; under known lighting the albedo moves to the hidden one and the
+    held-out image error falls to the floor that the noise sets.  (The
+    training loss is no measure here: it holds the 8-spp image's variance,
+    which grows with the albedo.)"""
     import firefly_b200 as ff
     from firefly_b200 import inverse
     # a soft sky (no hard sun): low variance, so 40 noisy steps can show the fit
     sky = scenes.sky_env(32, 16, seed=0, sun_radiance=8.0, sun_diameter_deg=20.0)
     hidden = scenes.textured_room(seed=0, width=40, height=40, tex_res=32, env=sky)
     start = scenes.textured_room(seed=0, width=40, height=40, env=sky,
-                                 albedo=np.full((32, 32, 3), 0.5, np.float32))
+                                 albedo=np.full((32, 32, 3), 0.2, np.float32))
     ds = ff.dScene(ctx, hidden)
     pt = ff.PathTracer(ctx, 40, 40)
     pt.draw(ds, spp=64, max_depth=3, seed=77, light=-1, mode=ff.FF_MODE_CORRECTED)
     target = torch.from_numpy(pt.image().astype(np.float32)).cuda()
     albedo = torch.from_numpy(start.textures[0].copy()).cuda()
     env = torch.from_numpy(hidden.env_rgb.copy()).cuda()      # known lighting: recover the albedo alone
-    r = inverse.optimize(ds, pt, target, albedo, env, steps=40, spp=8, lr=2e-2, lr_env=0.0)
-    print(f"[adjoint] driver loss {r['losses'][0]:.4e} -> {r['losses'][-1]:.4e}, {r['adjoint_spp_per_s']:.3e} spp/s")
-    assert np.mean(r["losses"][-5:]) < np.mean(r["losses"][:5])
+    r = inverse.optimize(ds, pt, target, albedo, env, steps=40, spp=8, lr=2e-2, lr_env=0.0, lr_decay=0.1)
+    assert len(r["losses"]) == 40 and np.all(np.isfinite(r["losses"]))
     assert r["adjoint_spp_per_s"] > 0
+    rmse = lambda a: float(np.sqrt(((a - hidden.textures[0]) ** 2).mean()))
+    r0, r1 = rmse(start.textures[0]), rmse(albedo.cpu().numpy())
 
     def heldout(tex):
         # fresh seed, more samples: the image error, not the noisy training loss
@@ -165,8 +169,10 @@ def test_inverse_driver_on_device(ctx):
         pt.clear_buffer()
         pt.draw(ds, spp=64, max_depth=3, seed=991, light=-1, mode=ff.FF_MODE_CORRECTED)
         return float(((pt.image() - target.cpu().numpy()) ** 2).mean())
-    e0, e1 = heldout(start.textures[0]), heldout(albedo.cpu().numpy())
-    print(f"[adjoint] held-out image error {e0:.4e} -> {e1:.4e}")
-    assert e1 < 0.5 * e0
+    e0, e1, ef = heldout(start.textures[0]), heldout(albedo.cpu().numpy()), heldout(hidden.textures[0])
+    print(f"[adjoint] driver albedo rmse {r0:.4f} -> {r1:.4f}; held-out image error {e0:.4e} -> {e1:.4e} "
+          f"(hidden albedo {ef:.4e}); {r['adjoint_spp_per_s']:.3e} spp/s")
+    assert r1 < 0.5 * r0
+    assert e1 - ef < 0.25 * (e0 - ef)
     pt.close()
     ds.close()
