@@ -446,6 +446,21 @@ def run_render(args, ws, rank, local, dist):
     e2e_value = ws * e_rays / (e_ms / 1e3) / 1e6
     image = img.numpy()[..., :3] / np.maximum(cnt.numpy(), 1)[..., None]
     finite = bool(np.isfinite(image).all())
+    conv = None
+    if rank == 0 and not args.no_relmse:
+        # relMSE of the step's image against a float64-accumulated 16k-spp render
+        # of the centre tile (1/16 of the pixels) under its own seed
+        from firefly_b200 import convergence
+        tile = convergence.centre_tile(W, H)
+        ref, info = convergence.reference_image(ctx, ds, cam, W, H, tile=tile, max_depth=kw["max_depth"],
+                                                rr_depth=kw["rr_depth"], light=-1, mode=ff.FF_MODE_CORRECTED)
+        x0, y0, tw, th = tile
+        crop = image[y0:y0 + th, x0:x0 + tw]
+        conv = {"relmse": round(convergence.relmse(crop, ref), 6),
+                "relmse_trimmed_1e-4": round(convergence.relmse_trimmed(crop, ref), 6),
+                "median_pixel_rel_sq_err": round(float(np.median(convergence.pixel_terms(crop, ref))), 6),
+                "spp": int(cnt.numpy()[y0, x0]), "reference_spp": info["spp"], "tile": info["tile"],
+                "reference_s": round(info["seconds"], 1), "accumulation": "float64"}
 
     trace = None
     if args.with_trace:
@@ -480,7 +495,7 @@ def run_render(args, ws, rank, local, dist):
                        "l2": "each step traces ~1.3G rays over a 0.27 GB scene; per-step state and queues ~0.5 GB",
                        "parallelism": (f"sample-parallel x{ws}: disjoint sample ranges of one frame, one film "
                                        f"all-reduce (41 MB) per step" if ws > 1 else "1 GPU"),
-                       "image_finite": finite, "trace_micro": trace},
+                       "image_finite": finite, "relmse_vs_16k_spp": conv, "trace_micro": trace},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 5), "traffic": None, "peak_source": peak_kind,
                          "bytes_per_ray": RAY_BYTES + HIT_BYTES},
@@ -587,6 +602,7 @@ def main(argv=None):
     ap.add_argument("--cpu-s", type=float, default=15.0, help="target seconds of CPU-baseline work")
     ap.add_argument("--ref-step-s", type=float, default=6.0, help="reference arm: seconds of CPU work per step")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-relmse", action="store_true", help="skip the 16k-spp reference tile and its relMSE")
     ap.add_argument("--with-trace", action="store_true", help="also run the trace micro-benchmark (render line)")
     ap.add_argument("--spp", type=int, default=RENDER["spp"], help="render workload: samples per pixel per step")
     args = ap.parse_args(argv)
