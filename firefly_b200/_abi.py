@@ -30,6 +30,9 @@ FF_TRACE_ANY = 2
 FF_RENDER_PROFILE = 1
 FF_ADJOINT_STORE_ALL = 4
 FF_ENV_KEEP_TABLES = 8
+FF_CACHE_GRADIENTS_ONLY = 16
+FF_CACHE_LEVELS = 16
+FF_CACHE_MLP_PARAMS = 5 * 64 * 64
 FF_MODE_PARITY = 0
 FF_MODE_CORRECTED = 1
 
@@ -106,6 +109,21 @@ class ff_adam_params(C.Structure):
                 ("hi", C.c_float), ("step", C.c_uint32)]
 
 
+class ff_cache_params(C.Structure):
+    _fields_ = [("log2_table_size", C.c_uint32), ("base_resolution", C.c_uint32), ("max_resolution", C.c_uint32),
+                ("seed", C.c_uint32), ("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
+                ("eps", C.c_float), ("rough_threshold", C.c_float), ("train_paths", C.c_uint32),
+                ("train_batch", C.c_uint32), ("flags", C.c_uint32)]
+
+
+# ff_cache_record as a numpy structured dtype (64 bytes)
+import numpy as _np  # noqa: E402
+CACHE_RECORD_DTYPE = _np.dtype([("pos", _np.float32, 3), ("roughness", _np.float32), ("wo", _np.float32, 3),
+                                ("value_r", _np.float32), ("normal", _np.float32, 3), ("value_g", _np.float32),
+                                ("pixel", _np.uint32), ("value_b", _np.float32), ("pad", _np.float32, 2)])
+assert CACHE_RECORD_DTYPE.itemsize == 64
+
+
 # Every symbol include/firefly_b200.h declares, with its ctypes signature.
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
@@ -133,6 +151,14 @@ SIGNATURES = {
     "ff_scene_set_texture": (C.c_int, [P, C.c_uint32, P, C.c_uint32]),
     "ff_scene_set_environment": (C.c_int, [P, P, C.c_uint32]),
     "ff_optimizer_adam_step": (C.c_int, [P, P, P, P, P, C.c_uint64, C.POINTER(ff_adam_params)]),
+    "ff_cache_create": (C.c_int, [P, P, C.POINTER(ff_cache_params), PP]),
+    "ff_cache_destroy": (C.c_int, [P]),
+    "ff_cache_reset": (C.c_int, [P]),
+    "ff_cache_query": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32]),
+    "ff_cache_train": (C.c_int, [P, P, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
+    "ff_cache_read_params": (C.c_int, [P, P, P, P, P]),
+    "ff_cache_write_params": (C.c_int, [P, P, P]),
+    "ff_render_cached": (C.c_int, [P, P, P, C.POINTER(ff_render_settings), P, C.POINTER(ff_render_stats)]),
 }
 
 _lib = None

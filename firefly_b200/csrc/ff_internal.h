@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "ff_cache.cuh"
 #include "ff_common.cuh"
 #include "firefly_b200.h"
 
@@ -158,3 +159,30 @@ void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* 
 void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, const ff_adjoint_desc* ad,
                        ff_render_stats* stats);
 void ff_build_env_tables(ff_context* ctx, ff_scene* s);
+
+// ff_cache.cu: learned radiance cache.
+struct ff_cache {
+    ff_context* ctx = nullptr;
+    ff_cache_params prm{};
+    float3 lo{0, 0, 0}, hi{0, 0, 0};  // scene box
+    ffc::Grid grid{};
+    DevBuf table, table_h, grid_grad, grid_m, grid_v;   // float2 / half2 per grid entry
+    DevBuf mlp, mlp_img, mlp_grad, mlp_m, mlp_v;        // FP32 weights, their bf16 images, Adam state
+    DevBuf loss;          // float: sum of training losses since the last reset of the counter
+    DevBuf err;           // uint32: tensor-core waits that gave up
+    uint32_t step = 0;    // Adam steps taken
+    // ff_render_cached workspace
+    DevBuf queries, train_recs, frame, counters;
+    uint32_t ws_pixels = 0, ws_train = 0;
+    DevBuf io_recs, io_out;   // staging for host-pointer calls
+};
+void ff_cache_setup_grid(ff_cache* c);
+void ff_cache_init_params(ff_cache* c);
+void ff_cache_refresh_copies(ff_cache* c);
+uint32_t ff_cache_num_params();
+void ff_cache_launch_infer(ff_cache* c, const void* recs, uint32_t n_max, const uint32_t* n_dev, float* out_rgb,
+                           float4* frame);
+void ff_cache_launch_train(ff_cache* c, const void* recs, uint32_t n, bool gradients_only);
+void ff_cache_launch_train_slice(ff_cache* c, const void* recs, uint32_t offset, uint32_t n_max, const uint32_t* n_dev);
+void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* cache, const ff_render_settings* st, ff_film* film,
+                      ff_render_stats* stats);

@@ -253,3 +253,42 @@ FF_D uint2 ff_root_group(const FFRayState& r)
 {
     return make_uint2(0u, (1u << 31) | (1u << (7u ^ r.oct_inv)));
 }
+
+// One whole traversal per thread (megakernel paths): closest hit of the ray
+// (o, d, [0, inf)) or any hit of `ray`; a traversal that exceeds its step
+// bound or overflows the stack counts in *err and reports what it found.
+FF_D bool ff_closest_hit(const FFBvhView& bvh, float3 o, float3 d, FFStack& st, unsigned int* err, ff_hit& h)
+{
+    FFRayState r;
+    ff_ray_setup(r, o, d, 0.f, __int_as_float(0x7f800000), false);
+    if (bvh.num_nodes) {
+        uint2 cur = ff_root_group(r);
+        st.reset();
+        uint32_t steps = 0;
+        while (!ff_traverse_step<false>(bvh, r, cur, st)) {
+            if (++steps > bvh.num_nodes + 2 || st.overflow) {
+                atomicAdd(err, 1u);
+                break;
+            }
+        }
+    }
+    h = ff_hit{r.tmax, r.u, r.v, r.prim == 0xffffffffu ? -1 : (int32_t)r.prim};
+    return h.prim >= 0;
+}
+
+FF_D bool ff_occluded(const FFBvhView& bvh, const ff_ray& ray, FFStack& st, unsigned int* err)
+{
+    if (!bvh.num_nodes) return false;
+    FFRayState r;
+    ff_ray_setup(r, make_float3(ray.ox, ray.oy, ray.oz), make_float3(ray.dx, ray.dy, ray.dz), ray.tmin, ray.tmax, true);
+    uint2 cur = ff_root_group(r);
+    st.reset();
+    uint32_t steps = 0;
+    while (!ff_traverse_step<true>(bvh, r, cur, st)) {
+        if (++steps > bvh.num_nodes + 2 || st.overflow) {
+            atomicAdd(err, 1u);
+            break;
+        }
+    }
+    return r.prim != 0xffffffffu;
+}

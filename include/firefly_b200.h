@@ -339,6 +339,79 @@ FF_API ff_status ff_optimizer_adam_step(ff_context* ctx, float* param, const flo
 FF_API ff_status ff_scene_read_env_tables(const ff_scene* scene, double* marginal, double* conditional,
                                    float* pdf, double* pdf_denom);
 
+/* ------------------------------------------------------------------------
+ * Learned radiance cache (no counterpart in the reference).  A multiresolution
+ * hash grid (FF_CACHE_LEVELS levels x 2 features, 2^log2_table_size entries per
+ * level, resolutions from base_resolution to max_resolution cells across the
+ * scene box) and an MLP of 4 hidden ReLU layers of 64 units with 3 outputs,
+ * bf16 weights and FP32 accumulation on the tensor cores.  Inputs: the hash
+ * features of the position, degree-4 spherical harmonics of the outgoing
+ * direction, the normal, the roughness and a constant 1.  Trained with Adam on
+ * the relative L2 loss sum_c (y_c - t_c)^2 / (y_c^2 + 0.01), mean over records.
+ * ------------------------------------------------------------------------ */
+typedef struct ff_cache ff_cache;
+
+#define FF_CACHE_LEVELS 16
+#define FF_CACHE_MLP_PARAMS (5 * 64 * 64)  /* W0..W3 [64][64], W4 [64][64] with rows 3..63 zero; W[out][in] */
+
+typedef struct ff_cache_params {
+    uint32_t log2_table_size;   /* entries per level = 2^log2_table_size (19) */
+    uint32_t base_resolution;   /* cells across the box at level 0 (16) */
+    uint32_t max_resolution;    /* cells across the box at the last level (2048) */
+    uint32_t seed;              /* parameter initialisation */
+    float lr, beta1, beta2, eps;    /* Adam */
+    float rough_threshold;      /* ff_render_cached: roughness at or above which a vertex is rough */
+    uint32_t train_paths;       /* ff_render_cached: training paths per frame (65536) */
+    uint32_t train_batch;       /* ff_render_cached: records per optimiser step (16384) */
+    uint32_t flags;             /* reserved, 0 */
+} ff_cache_params;
+
+/* One cache record: a path vertex and a value (training: the target radiance
+ * leaving the vertex toward wo; render queries: the path throughput). */
+typedef struct ff_cache_record {
+    float pos[3];               /* world space */
+    float roughness;
+    float wo[3];                /* unit direction toward the previous vertex */
+    float value_r;
+    float normal[3];
+    float value_g;
+    uint32_t pixel;             /* render queries: film pixel */
+    float value_b;
+    float pad[2];
+} ff_cache_record;              /* 64 bytes */
+
+#define FF_CACHE_GRADIENTS_ONLY 16u  /* ff_cache_train: accumulate gradients, take no optimiser step */
+
+/* The cache's box is the scene's bounding box. */
+FF_API ff_status ff_cache_create(ff_context* ctx, const ff_scene* scene, const ff_cache_params* params,
+                                 ff_cache** out);
+FF_API ff_status ff_cache_destroy(ff_cache* cache);
+/* Re-initialise every parameter and the optimiser state. */
+FF_API ff_status ff_cache_reset(ff_cache* cache);
+/* rgb[3*i..] = the MLP's output for record i.  flags: FF_MEM_DEVICE when both
+ * pointers are device memory. */
+FF_API ff_status ff_cache_query(ff_cache* cache, const ff_cache_record* records, uint32_t n, float* rgb,
+                                uint32_t flags);
+/* One optimiser step on the n records (their value = target radiance), or
+ * only the gradients with FF_CACHE_GRADIENTS_ONLY.  loss (host, may be NULL)
+ * receives the batch's mean relative L2 loss. */
+FF_API ff_status ff_cache_train(ff_cache* cache, const ff_cache_record* records, uint32_t n, uint32_t flags,
+                                float* loss);
+/* FP32 parameters and gradient accumulators (host memory, any may be NULL):
+ * mlp and grad_mlp FF_CACHE_MLP_PARAMS floats, grid and grad_grid
+ * FF_CACHE_LEVELS * 2^log2_table_size * 2 floats. */
+FF_API ff_status ff_cache_read_params(ff_cache* cache, float* mlp, float* grid, float* grad_mlp, float* grad_grid);
+FF_API ff_status ff_cache_write_params(ff_cache* cache, const float* mlp, const float* grid);
+/* Render settings->spp frames of one path per pixel each into the film:
+ * paths run as in ff_render (corrected mode) up to the first rough vertex
+ * after the camera hit, where they end with throughput x the cache's radiance;
+ * settings->max_depth bounds specular chains.  Every frame also traces
+ * params.train_paths full-length training paths from random pixels, whose
+ * radiance from their first rough vertex on trains the cache (one or more
+ * optimiser steps of train_batch records) after the frame's queries. */
+FF_API ff_status ff_render_cached(ff_context* ctx, ff_scene* scene, ff_cache* cache,
+                                  const ff_render_settings* settings, ff_film* film, ff_render_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,228 @@
+"""Learned radiance cache on the tensor cores against a float32 PyTorch
+restatement of the same network: the hash-grid encoding, spherical
+harmonics, the bf16-rounded forward (operands rounded to bf16 where the
+kernel rounds them, products accumulated in float32), the relative-L2
+gradients of the weights and of the grid, online fitting, and the cached
+render."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from firefly_b200 import convergence, scenes
+
+pytestmark = pytest.mark.gpu
+
+LOG2_T = 14          # small tables keep the float32 restatement quick
+BASE, MAXRES = 16, 512
+
+
+def bf16(x):
+    return x.to(torch.bfloat16).to(torch.float32)
+
+
+class Ref:
+    """The cache's network in torch (CPU, float32)."""
+
+    def __init__(self, stats, log2_T=LOG2_T, base=BASE, maxres=MAXRES):
+        lo = np.asarray(stats["scene_lo"], np.float32)
+        hi = np.asarray(stats["scene_hi"], np.float32)
+        e = (hi - lo) * np.float32(0.01) + np.float32(1e-4)
+        self.lo = lo - e
+        hi2 = hi + e
+        self.inv_ext = np.float32(1.0) / np.maximum(hi2 - self.lo, np.float32(1e-6))
+        self.T = 1 << log2_T
+        b = math.exp((math.log(maxres) - math.log(base)) / 15)
+        self.cells = [int(math.floor(base * b ** l + 1e-9)) for l in range(16)]
+        self.dense = [(c + 1) if (c + 1) ** 3 <= self.T else 0 for c in self.cells]
+
+    def corners(self, pos):
+        p = np.clip((pos.astype(np.float32) - self.lo) * self.inv_ext, 0, 1).astype(np.float32)
+        idx, w = [], []
+        for l, (c, side) in enumerate(zip(self.cells, self.dense)):
+            f = p * np.float32(c)
+            i = np.clip(np.floor(f).astype(np.int64), 0, c - 1)
+            t = np.clip(f - i.astype(np.float32), 0, 1)
+            li, lw = [], []
+            for k in range(8):
+                off = np.array([k & 1, (k >> 1) & 1, k >> 2])
+                x = (i + off).astype(np.uint64)
+                if side:
+                    h = x[:, 0] + side * (x[:, 1] + side * x[:, 2])
+                else:
+                    h = (x[:, 0] ^ ((x[:, 1] * 2654435761) & 0xFFFFFFFF) ^ ((x[:, 2] * 805459861) & 0xFFFFFFFF))
+                li.append((h & (self.T - 1)).astype(np.int64) + l * self.T)
+                ww = np.where(off == 1, t, 1 - t).prod(-1)
+                lw.append(ww.astype(np.float32))
+            idx.append(np.stack(li, -1))
+            w.append(np.stack(lw, -1))
+        return np.stack(idx, 1), np.stack(w, 1)          # (n, 16, 8)
+
+    @staticmethod
+    def sh(d):
+        x, y, z = d[:, 0], d[:, 1], d[:, 2]
+        pi = math.pi
+        c = [0.5 / math.sqrt(pi), math.sqrt(3 / (4 * pi)), math.sqrt(15 / pi) / 2, math.sqrt(5 / pi) / 4,
+             math.sqrt(15 / pi) / 4, math.sqrt(35 / (2 * pi)) / 4, math.sqrt(105 / pi) / 2,
+             math.sqrt(21 / (2 * pi)) / 4, math.sqrt(7 / pi) / 4, math.sqrt(105 / pi) / 4]
+        xx, yy, zz = x * x, y * y, z * z
+        return torch.stack([torch.full_like(x, c[0]), -c[1] * y, c[1] * z, -c[1] * x, c[2] * x * y, -c[2] * y * z,
+                            c[3] * (3 * zz - 1), -c[2] * x * z, c[4] * (xx - yy), -c[5] * y * (3 * xx - yy),
+                            c[6] * x * y * z, -c[7] * y * (5 * zz - 1), c[8] * z * (5 * zz - 3),
+                            -c[7] * x * (5 * zz - 1), c[9] * z * (xx - yy), -c[5] * x * (xx - 3 * yy)], -1)
+
+    def forward(self, recs, mlp, grid_h):
+        """mlp (5, 64, 64) and grid_h (16*T, 2) torch tensors (grid_h = the
+        float16 values the encoder reads); returns y (n, 3) float32."""
+        idx, w = self.corners(recs["pos"])
+        idx = torch.from_numpy(idx)
+        w = torch.from_numpy(w)
+        feats = (grid_h[idx] * w[..., None]).sum(2).reshape(len(recs), 32)
+        d = torch.from_numpy(recs["wo"].astype(np.float32))
+        n = torch.from_numpy(recs["normal"].astype(np.float32))
+        r = torch.from_numpy(recs["roughness"].astype(np.float32))[:, None]
+        x = torch.cat([feats, self.sh(d), n, r, torch.ones_like(r), torch.zeros(len(recs), 11)], -1)
+        a = bf16(x)
+        for l in range(4):
+            a = bf16(torch.relu(a @ bf16(mlp[l]).T))
+        return a @ bf16(mlp[4][:3]).T
+
+
+def random_records(stats, n, seed):
+    rng = np.random.default_rng(seed)
+    lo, hi = np.asarray(stats["scene_lo"]), np.asarray(stats["scene_hi"])
+    pos = rng.uniform(lo, hi, size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    nn = rng.normal(size=(n, 3))
+    nn /= np.linalg.norm(nn, axis=1, keepdims=True)
+    from firefly_b200.cache import records
+    return records(pos, d, nn, rng.uniform(0, 1, n), value=rng.uniform(0, 2, (n, 3)))
+
+
+@pytest.fixture(scope="module")
+def setup(ctx):
+    import firefly_b200 as ff
+    from firefly_b200.cache import RadianceCache
+    scn = scenes.small_room(seed=0, width=64, height=64)
+    ds = ff.dScene(ctx, scn)
+    cache = RadianceCache(ds, log2_table_size=LOG2_T, base_resolution=BASE, max_resolution=MAXRES, lr=1e-2)
+    ref = Ref(ds.stats())
+    rng = np.random.default_rng(5)
+    mlp = rng.uniform(-1, 1, (5, 64, 64)).astype(np.float32) * np.float32(math.sqrt(6 / 128))
+    mlp[4, 3:] = 0
+    grid = rng.uniform(-1, 1, (16, 1 << LOG2_T, 2)).astype(np.float32)
+    cache.write_params(mlp=mlp, grid=grid)
+    yield ff, ds, cache, ref, mlp, grid
+    cache.close()
+    ds.close()
+
+
+def test_query_matches_reference(setup):
+    ff, ds, cache, ref, mlp, grid = setup
+    recs = random_records(ds.stats(), 1000, 1)       # 8 tiles, a ragged last one
+    y = cache.query(recs)
+    grid_h = torch.from_numpy(grid.reshape(-1, 2).astype(np.float16).astype(np.float32))
+    y_ref = ref.forward(recs, torch.from_numpy(mlp), grid_h).numpy()
+    err = np.abs(y - y_ref)
+    scale = np.abs(y_ref).max()
+    print(f"[cache] query: max |err| {err.max():.3e}, mean {err.mean():.3e}, |y| max {scale:.3f}")
+    assert np.all(np.isfinite(y))
+    assert err.max() <= 2e-2 * scale
+    assert err.mean() <= 2e-3 * scale
+    # edge cases: one record, an exact multiple of the tile
+    assert np.allclose(cache.query(recs[:1]), y[:1], atol=1e-6)
+    assert np.allclose(cache.query(recs[:256]), y[:256], atol=1e-6)
+
+
+def test_gradients_match_reference(setup):
+    ff, ds, cache, ref, mlp, grid = setup
+    recs = random_records(ds.stats(), 700, 2)
+    cache.train(recs, gradients_only=True)
+    p = cache.read_params()
+    # torch: the same forward with straight-through bf16 casts, relative L2 with a constant denominator
+    W = torch.from_numpy(mlp).clone().requires_grad_(True)
+    G = torch.from_numpy(grid.reshape(-1, 2).astype(np.float16).astype(np.float32)).requires_grad_(True)
+    y = ref.forward(recs, W, G)
+    t = torch.from_numpy(np.stack([recs["value_r"], recs["value_g"], recs["value_b"]], -1))
+    loss = ((y - t) ** 2 / (y.detach() ** 2 + 0.01)).sum() / len(recs)
+    loss.backward()
+    gw, gw_ref = p["grad_mlp"], W.grad.numpy()
+    for l in range(5):
+        rows = 3 if l == 4 else 64
+        a, b = gw[l, :rows], gw_ref[l, :rows]
+        rel = np.abs(a - b).max() / np.abs(b).max()
+        print(f"[cache] dW{l}: max rel err {rel:.3e} (|dW| max {np.abs(b).max():.3e})")
+        assert rel < 5e-2
+    assert np.all(gw[4, 3:] == 0)
+    gg, gg_ref = p["grad_grid"].reshape(-1, 2), G.grad.numpy()
+    touched = np.abs(gg_ref).sum(-1) > 0
+    rel = np.abs(gg[touched] - gg_ref[touched]).max() / np.abs(gg_ref).max()
+    print(f"[cache] grid grad: {touched.sum()} entries, max rel err {rel:.3e}")
+    assert rel < 5e-2
+    assert np.all(gg[~touched] == 0)
+
+
+def test_online_fit_reduces_loss(ctx):
+    import firefly_b200 as ff
+    from firefly_b200.cache import RadianceCache
+    scn = scenes.small_room(seed=0, width=64, height=64)
+    ds = ff.dScene(ctx, scn)
+    cache = RadianceCache(ds, log2_table_size=16, lr=1e-2)
+    st = ds.stats()
+    rng = np.random.default_rng(3)
+    lo, hi = np.asarray(st["scene_lo"]), np.asarray(st["scene_hi"])
+    from firefly_b200.cache import records
+
+    def batch(n):
+        pos = rng.uniform(lo, hi, size=(n, 3))
+        d = rng.normal(size=(n, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        u = (pos - lo) / (hi - lo)
+        target = np.stack([1 + 0.5 * np.sin(6 * u[:, 0]), 1.5 + 0.5 * np.cos(5 * u[:, 1]) * d[:, 1],
+                           0.5 + u[:, 2] ** 2], -1)
+        return records(pos, d, d, 0.5, value=target)
+
+    losses = [cache.train(batch(16384)) for _ in range(300)]
+    test = batch(4096)
+    y = cache.query(test)
+    t = np.stack([test["value_r"], test["value_g"], test["value_b"]], -1)
+    rel = float(np.mean(np.abs(y - t) / t))
+    print(f"[cache] fit: loss {np.mean(losses[:5]):.3e} -> {np.mean(losses[-5:]):.3e}, held-out mean rel err {rel:.3f}")
+    assert np.mean(losses[-5:]) < 0.05 * np.mean(losses[:5])
+    assert rel < 0.1
+    cache.close()
+    ds.close()
+
+
+def test_cached_render_converges(ctx):
+    """Cached frames of the small room against a float64 16k-spp reference of
+    the plain tracer (same scene, depth 5): finite, unbiased to within the
+    cache's error, and less noisy than plain paths at equal frame count."""
+    import firefly_b200 as ff
+    from firefly_b200.cache import RadianceCache
+    W = H = 128
+    scn = scenes.small_room(seed=0, width=W, height=H)
+    ds = ff.dScene(ctx, scn)
+    kw = dict(max_depth=5, rr_depth=3, light=0)
+    ref, _ = convergence.reference_image(ctx, ds, scn.camera, W, H, spp=4096, mode=ff.FF_MODE_CORRECTED, **kw)
+    cache = RadianceCache(ds, train_paths=8192, train_batch=8192)
+    pt = ff.PathTracer(ctx, W, H)
+    cache.render(ds, pt, frames=64, seed=1, **kw)          # warm-up: train
+    pt.clear_buffer()
+    st = cache.render(ds, pt, frames=64, seed=2, sample_offset=64, **kw)
+    img = pt.image()
+    e_cache = convergence.relmse(img, ref)
+    pt.clear_buffer()
+    pt.draw(ds, spp=64, seed=3, mode=ff.FF_MODE_CORRECTED, **kw)
+    e_plain = convergence.relmse(pt.image(), ref)
+    bias = float(np.abs(img.mean() - ref.mean()) / ref.mean())
+    print(f"[cache] render 64 frames: relMSE cache {e_cache:.4f} vs plain 64 spp {e_plain:.4f}; mean bias {bias:.4f}; "
+          f"{st['ms_total']:.1f} ms, rays {st['extension_rays']}+{st['shadow_rays']}")
+    assert np.all(np.isfinite(img)) and img.min() >= 0
+    assert bias < 0.05
+    assert e_cache < 0.05
+    pt.close()
+    cache.close()
+    ds.close()
