@@ -55,15 +55,16 @@ def dist_env():
     return ws, rank, local
 
 
-def measured_peaks():
+def measured_peaks(key: str = "hbm_gbs"):
+    """(peak, "measured" | "fallback"): HBM copy GB/s or dense bf16 TFLOP/s."""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         try:
             d = json.loads(p.read_text())
-            return float(d["hbm_gbs"]), "measured"
+            return float(d[key]), "measured"
         except Exception:
             pass
-    return 6650.0, "fallback"
+    return (6650.0 if key == "hbm_gbs" else 1590.0), "fallback"
 
 
 class ClockSampler:
@@ -591,13 +592,148 @@ def run_inverse(args, ws, rank, local, dist):
     ctx.close()
 
 
+CACHE_WORKLOAD = ("small room (24-tri box + 64x32 UV sphere, area light radiance 15) at 1920x1080, depth 5, "
+                  "RR from 3, corrected mode: time until the progressively accumulated image reaches relMSE 0.01 "
+                  "on the centre tile (480x270) against a float64-accumulated 16k-spp render; learned radiance cache "
+                  "(hash grid 16 levels x 2 x 2^19, MLP 4 x 64 ReLU bf16 on tcgen05, 65,536 training paths per "
+                  "frame, Adam in steps of 16,384) against the plain wavefront tracer")
+CACHE_TARGET = 0.01
+
+
+def checkpoints(limit):
+    """Sample counts at which the accumulated image is judged (about +25% each)."""
+    out, k = [], 1
+    while k <= limit:
+        out.append(k)
+        k = max(k + 1, int(round(k * 1.25)))
+    return out
+
+
+def run_cache(args, ws, rank, local, dist):
+    import ctypes as C
+    import torch
+    import firefly_b200 as ff
+    from firefly_b200 import _abi as A
+    from firefly_b200 import convergence, scenes
+    from firefly_b200.cache import RadianceCache
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx = ff.Context(local, stream=stream.cuda_stream)
+    W, H = 1920, 1080
+    scn = scenes.small_room(seed=0, width=W, height=H)
+    ds = ff.dScene(ctx, scn)
+    kw = dict(max_depth=5, rr_depth=3, light=0)
+    tile = convergence.centre_tile(W, H)
+    ref, info = convergence.reference_image(ctx, ds, scn.camera, W, H, tile=tile, mode=ff.FF_MODE_CORRECTED, **kw)
+    x0, y0, tw, th = tile
+    pt = ff.PathTracer(ctx, W, H)
+    cps = checkpoints(args.cache_max_frames)
+
+    def judge():
+        img = pt.image()
+        return convergence.relmse(img[y0:y0 + th, x0:x0 + tw], ref)
+
+    def progressive(render_more):
+        """(ms to reach the target or None, trajectory [(frames, ms, relMSE)])"""
+        pt.clear_buffer()
+        ms, done, traj, hit = 0.0, 0, [], None
+        for c in cps:
+            ms += render_more(c - done, done)
+            done = c
+            e = judge()
+            traj.append((c, round(ms, 2), round(e, 5)))
+            if e <= CACHE_TARGET:
+                hit = ms
+                break
+        return hit, traj
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    # the plain tracer: one draw call per increment
+    plain_ms, plain_traj = progressive(
+        lambda k, done: pt.draw(ds, spp=k, seed=11, sample_offset=done, mode=ff.FF_MODE_CORRECTED, **kw)["ms_total"])
+    # the cache from scratch: warm-up frames (trained, then discarded) count in the time
+    cache = RadianceCache(ds)
+    pt.clear_buffer()
+    warm = cache.render(ds, pt, frames=args.cache_warmup, seed=12, **kw)
+    warm_ms = warm["ms_total"]
+    cache_ms, cache_traj = progressive(
+        lambda k, done: cache.render(ds, pt, frames=k, seed=13, sample_offset=args.cache_warmup + done,
+                                     **kw)["ms_total"])
+    cache_total = None if cache_ms is None else warm_ms + cache_ms
+    # one profiled frame: stage times, queries and records
+    s = A.ff_render_settings(spp=4, max_depth=5, rr_depth=3, seed=14, mode=ff.FF_MODE_CORRECTED, light=0,
+                             max_paths=0, sample_offset=200000, flags=A.FF_RENDER_PROFILE, shadow_offset=0.001)
+    st = A.ff_render_stats()
+    rc = ff.lib().ff_render_cached(ctx.handle, ds.handle, cache.handle, C.byref(s), pt.film, C.byref(st))
+    assert rc == 0
+    prof = {k: getattr(st, k) for k, _ in st._fields_}
+    # end to end: camera in, warm-up, frames, image to pinned host memory
+    img_h = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    cnt_h = torch.empty((H, W), dtype=torch.int32).pin_memory()
+    frames_needed = cache_traj[-1][0]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cache.reset()
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    ds.update(scn.camera)
+    pt.clear_buffer()
+    cache.render(ds, pt, frames=args.cache_warmup, seed=12, **kw)
+    pt.clear_buffer()
+    cache.render(ds, pt, frames=frames_needed, seed=13, sample_offset=args.cache_warmup, **kw)
+    rc = ff.lib().ff_film_read(pt.film, C.c_void_p(img_h.data_ptr()), C.c_void_p(cnt_h.data_ptr()), 0)
+    assert rc == 0
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ms = max_over_ranks(dist, dev, cache_total if cache_total is not None else float("nan"))
+    if rank == 0:
+        peak, peak_kind = measured_peaks("bf16_tflops")
+        q_flops = prof["cache_queries"] * 2.0 * (4 * 64 * 64 + 16 * 64)
+        q_tflops = q_flops / (prof["ms_cache_query"] / 1e3) / 1e12 if prof["ms_cache_query"] > 0 else None
+        line = {"metric": "time-to-relMSE 0.01 (learned radiance cache)", "value": None if ms != ms else round(ms, 2),
+                "unit": "ms", "n_gpus": ws, "steps": len(cache_traj), "warmup": args.cache_warmup,
+                "ms_per_step": None, "higher_is_better": False, "scaling": "replicas", "vs_baseline": None,
+                "dtype": "bf16 MLP / f32 paths", "data": "synthetic",
+                "config": {"workload": CACHE_WORKLOAD, "target_relmse": CACHE_TARGET,
+                           "plain_tracer_ms": None if plain_ms is None else round(plain_ms, 2),
+                           "speedup_vs_plain": (None if (plain_ms is None or cache_total is None)
+                                                else round(plain_ms / cache_total, 3)),
+                           "cache_warmup_frames": args.cache_warmup, "cache_warmup_ms": round(warm_ms, 2),
+                           "trajectory_plain": plain_traj, "trajectory_cache": cache_traj,
+                           "reference": info, "tile": list(tile),
+                           "profiled_4_frames": {k: (round(v, 3) if isinstance(v, float) else v)
+                                                 for k, v in prof.items()},
+                           "parallelism": "1 GPU" if ws == 1 else f"{ws} independent replicas (time = max over ranks)"},
+                "roofline": {"bound": "tensor", "kernel": "k_cache_infer (+ k_frame_to_film)",
+                             "achieved": None if q_tflops is None else round(q_tflops, 3), "peak": peak,
+                             "unit": "TFLOP/s", "frac": None if q_tflops is None else round(q_tflops / peak, 5),
+                             "traffic": None, "peak_source": peak_kind,
+                             "flops_per_query": 2 * (4 * 64 * 64 + 16 * 64)},
+                "cpu_baseline": None,
+                "cpu_baseline_note": "not timed for the cache: the plain tracer on the same GPU is the comparator",
+                "e2e": {"value": round(e2e_ms, 2), "unit": "ms", "h2d_bytes_per_step": 80,
+                        "d2h_bytes_per_step": W * H * 20},
+                "gpu_launches": int(warm["kernel_launches"]) + sum(1 for _ in cache_traj),
+                "clocks": clk}
+        print(json.dumps(line), flush=True)
+    cache.close()
+    pt.close()
+    ds.close()
+    ctx.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["render", "trace", "inverse"], default="render")
+    ap.add_argument("--workload", choices=["render", "trace", "inverse", "cache"], default="render")
+    ap.add_argument("--cache-warmup", type=int, default=16, help="cache workload: training frames before accumulating")
+    ap.add_argument("--cache-max-frames", type=int, default=1024, help="cache workload: give up after this many")
     ap.add_argument("--rays", type=int, default=RAYS_PER_SET, help="trace workload: rays per batch")
     ap.add_argument("--cpu-s", type=float, default=15.0, help="target seconds of CPU-baseline work")
     ap.add_argument("--ref-step-s", type=float, default=6.0, help="reference arm: seconds of CPU work per step")
@@ -616,6 +752,8 @@ def main(argv=None):
         run_render(args, ws, rank, local, dist)
     elif args.workload == "inverse":
         run_inverse(args, ws, rank, local, dist)
+    elif args.workload == "cache":
+        run_cache(args, ws, rank, local, dist)
     else:
         run_trace(args, ws, rank, local, dist)
     if dist is not None:

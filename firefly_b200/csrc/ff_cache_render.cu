@@ -243,9 +243,14 @@ __device__ __forceinline__ void kahan(float& sum, float& comp, float x)
 }
 
 __global__ void k_frame_to_film(const float4* __restrict__ frame, uint32_t n, float4* __restrict__ acc,
-                                float4* __restrict__ comp, uint32_t* __restrict__ cnt)
+                                float4* __restrict__ comp, uint32_t* __restrict__ cnt, const uint32_t* __restrict__ rec_cnt,
+                                unsigned long long* __restrict__ rec_total)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        rec_total[0] += rec_cnt[0];
+        rec_total[1] += rec_cnt[1];
+    }
     if (i >= n) return;
     const float4 f = frame[i];
     float4 s = acc[i], c = comp[i];
@@ -283,6 +288,7 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
     uint32_t* cnt = c->counters.as<uint32_t>();            // [0] queries, [1] training records
     unsigned long long* rays = reinterpret_cast<unsigned long long*>(c->counters.as<char>() + 16);
     unsigned int* err = reinterpret_cast<unsigned int*>(c->counters.as<char>() + 32);
+    unsigned long long* totals = reinterpret_cast<unsigned long long*>(c->counters.as<char>() + 48);
     CR a;
     a.bvh = scene->view();
     a.shade = scene->shade.as<FFShadeTri>();
@@ -315,25 +321,47 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
     a.rays = rays;
     a.err = err;
     const uint32_t blocks = (npix + n_train + kBlock - 1) / kBlock;
+    const bool profile = (st->flags & FF_RENDER_PROFILE) != 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    if (profile)
+        for (auto& e : ev) FF_CUDA_CHECK(cudaEventCreate(&e));
+    float ms_paths = 0.f, ms_train = 0.f, ms_query = 0.f;
     uint64_t launches = 0;
     FF_CUDA_CHECK(cudaEventRecord(ctx->ev0, stream));
     for (uint32_t f = 0; f < st->spp; ++f) {
         a.frame = st->sample_offset + f;
         FF_CUDA_CHECK(cudaMemsetAsync(cnt, 0, 8, stream));
+        if (profile) FF_CUDA_CHECK(cudaEventRecord(ev[0], stream));
         k_cached_paths<<<blocks, kBlock, 0, stream>>>(a);
         launches += 1;
+        if (profile) FF_CUDA_CHECK(cudaEventRecord(ev[1], stream));
         for (uint32_t off = 0; off < n_train; off += batch) {
             ff_cache_launch_train_slice(c, a.train, off, std::min(batch, n_train - off), cnt + 1);
             launches += 3;
         }
+        if (profile) FF_CUDA_CHECK(cudaEventRecord(ev[2], stream));
         ff_cache_launch_infer(c, a.queries, npix, cnt, nullptr, a.frame_rgb);
         k_frame_to_film<<<(npix + 255) / 256, 256, 0, stream>>>(a.frame_rgb, npix, film->accum.as<float4>(),
-                                                                 film->comp.as<float4>(), film->count.as<uint32_t>());
+                                                                 film->comp.as<float4>(), film->count.as<uint32_t>(),
+                                                                 cnt, totals);
         launches += 2;
         FF_CUDA_CHECK(cudaGetLastError());
+        if (profile) {
+            FF_CUDA_CHECK(cudaEventRecord(ev[3], stream));
+            FF_CUDA_CHECK(cudaEventSynchronize(ev[3]));
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[0], ev[1]);
+            ms_paths += t;
+            cudaEventElapsedTime(&t, ev[1], ev[2]);
+            ms_train += t;
+            cudaEventElapsedTime(&t, ev[2], ev[3]);
+            ms_query += t;
+        }
     }
+    if (profile)
+        for (auto& e : ev) cudaEventDestroy(e);
     FF_CUDA_CHECK(cudaEventRecord(ctx->ev1, stream));
-    unsigned long long h[4] = {0, 0, 0, 0};
+    unsigned long long h[6] = {0, 0, 0, 0, 0, 0};
     FF_CUDA_CHECK(cudaMemcpyAsync(h, c->counters.as<char>() + 16, sizeof(h), cudaMemcpyDeviceToHost, stream));
     FF_CUDA_CHECK(cudaStreamSynchronize(stream));
     if ((unsigned int)h[2]) throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
@@ -346,5 +374,10 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
         stats->frames = st->spp;
         stats->ms_total = ms;
         stats->kernel_launches = launches;
+        stats->ms_cache_paths = ms_paths;
+        stats->ms_cache_train = ms_train;
+        stats->ms_cache_query = ms_query;
+        stats->cache_queries = h[4];
+        stats->cache_records = h[5];
     }
 }

@@ -271,6 +271,10 @@ typedef struct ff_render_stats {
     /* per-stage device time, filled with FF_RENDER_PROFILE */
     float ms_trace_extension, ms_trace_shadow, ms_logic, ms_shade;
     uint32_t kernel_launches;   /* kernels this call launched */
+    /* ff_render_cached: device time of its stages (FF_RENDER_PROFILE) and the
+     * cache queries answered and training records produced */
+    float ms_cache_paths, ms_cache_train, ms_cache_query;
+    uint64_t cache_queries, cache_records;
 } ff_render_stats;
 
 /* Replaces PathTracer::draw + wavefront_pathtrace (PathTracer.cpp:59-79,
