@@ -624,6 +624,20 @@ def run_cache(args, ws, rank, local, dist):
     scn = scenes.small_room(seed=0, width=W, height=H)
     ds = ff.dScene(ctx, scn)
     kw = dict(max_depth=5, rr_depth=3, light=0)
+    if args.cache_frames_only:
+        # a short run for profilers: cached frames only, no reference, no plain tracer
+        cache = RadianceCache(ds)
+        pt = ff.PathTracer(ctx, W, H)
+        st = cache.render(ds, pt, frames=args.cache_frames_only, seed=12, **kw)
+        if rank == 0:
+            print(json.dumps({"workload": "cached frames only (profiling)", "frames": args.cache_frames_only,
+                              "ms_total": st["ms_total"], "queries": st["cache_queries"],
+                              "records": st["cache_records"]}), flush=True)
+        cache.close()
+        pt.close()
+        ds.close()
+        ctx.close()
+        return
     tile = convergence.centre_tile(W, H)
     ref, info = convergence.reference_image(ctx, ds, scn.camera, W, H, tile=tile, mode=ff.FF_MODE_CORRECTED, **kw)
     x0, y0, tw, th = tile
@@ -734,6 +748,8 @@ def main(argv=None):
     ap.add_argument("--workload", choices=["render", "trace", "inverse", "cache"], default="render")
     ap.add_argument("--cache-warmup", type=int, default=16, help="cache workload: training frames before accumulating")
     ap.add_argument("--cache-max-frames", type=int, default=1024, help="cache workload: give up after this many")
+    ap.add_argument("--cache-frames-only", type=int, default=0,
+                    help="cache workload: only render this many cached frames (for profilers)")
     ap.add_argument("--rays", type=int, default=RAYS_PER_SET, help="trace workload: rays per batch")
     ap.add_argument("--cpu-s", type=float, default=15.0, help="target seconds of CPU-baseline work")
     ap.add_argument("--ref-step-s", type=float, default=6.0, help="reference arm: seconds of CPU work per step")
