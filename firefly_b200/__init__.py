@@ -23,10 +23,10 @@ import weakref
 import numpy as np
 
 from . import _abi as A
-from ._abi import (FF_MAT_COAT, FF_MAT_CONDUCTOR, FF_MAT_DIELECTRIC, FF_MAT_DIFFUSE, FF_MAT_MIX,
+from ._abi import (FF_LIGHT_ALL, FF_MAT_COAT, FF_MAT_CONDUCTOR, FF_MAT_DIELECTRIC, FF_MAT_DIFFUSE, FF_MAT_MIX,
                    FF_MODE_CORRECTED, FF_MODE_PARITY, FF_TRACE_ANY, FF_TRACE_CLOSEST)
 
-__all__ = ["Context", "dScene", "PathTracer", "FireflyError", "lib", "FF_MAT_MIX", "FF_MAT_DIFFUSE",
+__all__ = ["Context", "dScene", "PathTracer", "FireflyError", "lib", "FF_LIGHT_ALL", "FF_MAT_MIX", "FF_MAT_DIFFUSE",
            "FF_MAT_CONDUCTOR", "FF_MAT_DIELECTRIC", "FF_MAT_COAT", "FF_MODE_PARITY", "FF_MODE_CORRECTED",
            "FF_TRACE_ANY", "FF_TRACE_CLOSEST", "HIT_DTYPE", "RAY_DTYPE"]
 
@@ -128,6 +128,10 @@ class dScene:
             d.env_color[k] = float(s.env_color[k])
         d.area_lights = C.cast(lights, C.c_void_p)
         d.num_area_lights = len(s.area_lights)
+        dls = list(getattr(s, "directional_lights", []) or [])
+        dirs = (A.ff_directional_light * max(1, len(dls)))(*dls)
+        d.directional_lights = C.cast(dirs, C.c_void_p)
+        d.num_directional_lights = len(dls)
         if s.camera is not None:
             d.camera = s.camera
         h = C.c_void_p()

@@ -28,6 +28,7 @@ FF_MEM_DEVICE = 1
 FF_TRACE_CLOSEST = 0
 FF_TRACE_ANY = 2
 FF_RENDER_PROFILE = 1
+FF_LIGHT_ALL = -2
 FF_ADJOINT_STORE_ALL = 4
 FF_ENV_KEEP_TABLES = 8
 FF_CACHE_GRADIENTS_ONLY = 16
@@ -63,6 +64,11 @@ class ff_area_light(C.Structure):
                 ("emissive", C.c_float * 3), ("radiance", C.c_float)]
 
 
+class ff_directional_light(C.Structure):
+    _fields_ = [("direction", C.c_float * 3), ("emissive", C.c_float * 3), ("radiance", C.c_float),
+                ("pad", C.c_float)]
+
+
 class ff_camera(C.Structure):
     _fields_ = [("inv_view_proj", C.c_float * 16), ("lens_radius", C.c_float), ("focal_distance", C.c_float),
                 ("exposure", C.c_float), ("pixel_jitter", C.c_float)]
@@ -77,7 +83,8 @@ class ff_scene_desc(C.Structure):
                 ("env_rgb", C.c_void_p), ("env_width", C.c_uint32), ("env_height", C.c_uint32),
                 ("env_color", C.c_float * 3),
                 ("area_lights", C.c_void_p), ("num_area_lights", C.c_uint32),
-                ("camera", ff_camera), ("flags", C.c_uint32)]
+                ("camera", ff_camera), ("flags", C.c_uint32),
+                ("directional_lights", C.c_void_p), ("num_directional_lights", C.c_uint32)]
 
 
 class ff_scene_stats(C.Structure):

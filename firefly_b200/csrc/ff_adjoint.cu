@@ -40,6 +40,7 @@ struct ADJ {
     const FFTexView* tex;
     const ff_area_light* area;
     FFEnvView env;
+    FFLightSet lights;
     ff_camera cam;
     uint32_t W, H, spp, sample_offset, seed, max_depth, rr_depth;
     int32_t light;
@@ -163,11 +164,7 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
     float3 o, d;
     gen_camera_ray(a.cam, (int)a.W, (int)a.H, (int)(pix % a.W), (int)(pix / a.W), rand2(key, 0, DIM_CAM_JITTER),
                    rand2(key, 0, DIM_CAM_LENS), o, d);
-    LightCtx lc;
-    lc.env = a.env;
-    lc.is_env = a.light < 0;
-    lc.corrected = true;
-    if (!lc.is_env) lc.rect = make_rect(a.area[a.light]);
+    const LightCtx lc = select_light(a.lights, key, 0u);   // a fixed light (FF_LIGHT_ALL is rejected)
     float3 beta = make_float3(1.f, 1.f, 1.f);
     float3 Lacc = make_float3(0.f, 0.f, 0.f);
     ShadeOut sh;
@@ -226,13 +223,7 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
         const float wuv = (1.f - u) - v;
         const float2 tuv = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x, u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
         float3 wi, sp;
-        if (lc.is_env) {
-            env_sample_corrected(a.env, pos, ff_rand(key, dim_of(L, DIM_LIGHT)), ff_rand(key, dim_of(L, DIM_LIGHT + 1)),
-                                 ff_rand(key, dim_of(L, DIM_EXTRA + 1)), ff_rand(key, dim_of(L, DIM_EXTRA + 2)), wi, sp);
-        } else {
-            sp = rect_sample(lc.rect, rand2(key, L, DIM_LIGHT));
-            wi = normalize3(sp - pos);
-        }
+        sample_light(lc, pos, key, L, wi, sp);
         const ff_material& mm = a.mats[t.material];
         const FFSurf surf = resolve_surface(mm, a.tex, tuv);
         const float3 wo = -d;
@@ -331,8 +322,8 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
     FF_REQUIRE(st->spp > 0 && st->max_depth >= 1 && st->max_depth < (uint32_t)kMaxVerts, "spp > 0, 1 <= max_depth < 16");
     FF_REQUIRE(ad->texture < (int32_t)scene->textures.size(), "texture index out of range");
     FF_REQUIRE(ad->texture < 0 || ad->grad_texture, "grad_texture required for a texture gradient");
-    if (st->light < 0) FF_REQUIRE(scene->env.width > 0, "light -1 (environment) needs an environment map");
-    else FF_REQUIRE((uint32_t)st->light < scene->num_area_lights, "light index out of range");
+    FF_REQUIRE(st->light != FF_LIGHT_ALL, "the adjoint needs one light (FF_LIGHT_ALL is not supported)");
+    ff_check_light(scene, st->light, FF_MODE_CORRECTED);
     cudaStream_t stream = ctx->stream;
     const bool dev = (ad->flags & FF_MEM_DEVICE) != 0;
     const size_t npix = (size_t)ad->width * ad->height;
@@ -369,14 +360,8 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
     a.mats = scene->materials.as<ff_material>();
     a.tex = scene->tex_table.as<FFTexView>();
     a.area = scene->area_lights.as<ff_area_light>();
-    a.env.rgb = scene->env.rgb.as<float3>();
-    a.env.marginal = scene->env.marginal.as<double>();
-    a.env.cond = scene->env.conditional.as<double>();
-    a.env.pdf = scene->env.pdf.as<float>();
-    a.env.width = scene->env.width;
-    a.env.height = scene->env.height;
-    a.env.color = scene->env.color;
-    a.env.radius = 10000.f;
+    a.env = ff_env_view(scene);
+    a.lights = ff_light_set(scene, st->light, FF_MODE_CORRECTED);
     a.cam = scene->camera;
     a.W = ad->width;
     a.H = ad->height;

@@ -56,7 +56,7 @@ void upload(DevBuf& b, const void* host, size_t bytes, cudaStream_t st)
 
 size_t ff_scene::device_bytes() const
 {
-    size_t total = nodes.bytes + tris.bytes + shade.bytes + materials.bytes + tex_table.bytes + area_lights.bytes +
+    size_t total = nodes.bytes + tris.bytes + shade.bytes + materials.bytes + tex_table.bytes + area_lights.bytes + dir_lights.bytes +
                    env.rgb.bytes + env.marginal.bytes + env.conditional.bytes + env.pdf.bytes + env.denom.bytes;
     for (auto* t : textures) total += t->bytes;
     return total;
@@ -167,6 +167,7 @@ ff_status ff_scene_create(ff_context* ctx, const ff_scene_desc* d, ff_scene** ou
         }
         FF_REQUIRE(!d->env_rgb || (d->env_width > 0 && d->env_height > 0), "environment map has zero size");
         FF_REQUIRE(d->num_area_lights == 0 || d->area_lights, "area_lights is NULL");
+        FF_REQUIRE(d->num_directional_lights == 0 || d->directional_lights, "directional_lights is NULL");
         cudaStream_t stream = ctx->stream;
         DevBuf pos, idx;
         upload(pos, d->positions, sizeof(float) * 3ull * d->num_vertices, stream);

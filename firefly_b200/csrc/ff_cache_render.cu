@@ -38,6 +38,7 @@ struct CR {
     const FFTexView* tex;
     const ff_area_light* area;
     FFEnvView env;
+    FFLightSet lights;
     ff_camera cam;
     uint32_t W, H, frame, seed, max_depth, rr_depth, n_train;
     int32_t light;
@@ -120,11 +121,8 @@ __global__ void __launch_bounds__(kBlock) k_cached_paths(CR a)
         float3 o, d;
         gen_camera_ray(a.cam, (int)a.W, (int)a.H, (int)(pix % a.W), (int)(pix / a.W), rand2(key, 0, DIM_CAM_JITTER),
                        rand2(key, 0, DIM_CAM_LENS), o, d);
-        LightCtx lc;
-        lc.env = a.env;
-        lc.is_env = a.light < 0;
-        lc.corrected = true;
-        if (!lc.is_env) lc.rect = make_rect(a.area[a.light]);
+        const bool per_vertex = a.lights.light == FF_LIGHT_ALL;
+        LightCtx lc = select_light(a.lights, key, 0u);
         float3 beta = make_float3(1.f, 1.f, 1.f);
         float3 beta_rel = make_float3(1.f, 1.f, 1.f);   // throughput since the training vertex
         float3 Lacc = make_float3(0.f, 0.f, 0.f), Ltail = make_float3(0.f, 0.f, 0.f);
@@ -187,13 +185,8 @@ __global__ void __launch_bounds__(kBlock) k_cached_paths(CR a)
                 beta_rel = make_float3(1.f, 1.f, 1.f);
             }
             float3 wi, sp;
-            if (lc.is_env) {
-                env_sample_corrected(a.env, pos, ff_rand(key, dim_of(L, DIM_LIGHT)), ff_rand(key, dim_of(L, DIM_LIGHT + 1)),
-                                     ff_rand(key, dim_of(L, DIM_EXTRA + 1)), ff_rand(key, dim_of(L, DIM_EXTRA + 2)), wi, sp);
-            } else {
-                sp = rect_sample(lc.rect, rand2(key, L, DIM_LIGHT));
-                wi = normalize3(sp - pos);
-            }
+            if (per_vertex) lc = select_light(a.lights, key, L);
+            sample_light(lc, pos, key, L, wi, sp);
             sh.c_spec = sh.c_diff = make_float3(0.f, 0.f, 0.f);
             switch (surf.kind) {
                 case FF_MAT_MIX: shade_mix(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, sp, key, L, sh); break;
@@ -268,8 +261,7 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
                       ff_render_stats* stats)
 {
     FF_REQUIRE(st->spp > 0 && st->max_depth >= 1 && st->max_depth <= 64, "spp > 0, 1 <= max_depth <= 64");
-    if (st->light < 0) FF_REQUIRE(scene->env.width > 0, "light -1 (environment) needs an environment map");
-    else FF_REQUIRE((uint32_t)st->light < scene->num_area_lights, "light index out of range");
+    ff_check_light(scene, st->light, FF_MODE_CORRECTED);
     const uint32_t W = film->width, H = film->height, npix = W * H;
     const uint32_t n_train = c->prm.train_paths;
     const uint32_t batch = c->prm.train_batch ? c->prm.train_batch : (n_train ? n_train : 1u);
@@ -295,14 +287,8 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
     a.mats = scene->materials.as<ff_material>();
     a.tex = scene->tex_table.as<FFTexView>();
     a.area = scene->area_lights.as<ff_area_light>();
-    a.env.rgb = scene->env.rgb.as<float3>();
-    a.env.marginal = scene->env.marginal.as<double>();
-    a.env.cond = scene->env.conditional.as<double>();
-    a.env.pdf = scene->env.pdf.as<float>();
-    a.env.width = scene->env.width;
-    a.env.height = scene->env.height;
-    a.env.color = scene->env.color;
-    a.env.radius = 10000.f;
+    a.env = ff_env_view(scene);
+    a.lights = ff_light_set(scene, st->light, FF_MODE_CORRECTED);
     a.cam = scene->camera;
     a.W = W;
     a.H = H;

@@ -105,6 +105,8 @@ struct ff_scene {
     DevBuf tex_table;     // device table of texture descriptors
     DevBuf area_lights;   // ff_area_light[]
     uint32_t num_area_lights = 0;
+    DevBuf dir_lights;    // ff_directional_light[], directions normalised
+    uint32_t num_dir_lights = 0;
     FFEnvLight env;
     ff_camera camera{};
     ~ff_scene()
@@ -159,6 +161,15 @@ void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* 
 void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, const ff_adjoint_desc* ad,
                        ff_render_stats* stats);
 void ff_build_env_tables(ff_context* ctx, ff_scene* s);
+
+// ff_scene.cu: device views of the scene's lights for the path kernels.
+namespace ffp {
+struct FFLightSet;
+}
+struct FFEnvView;
+FFEnvView ff_env_view(const ff_scene* s);
+void ff_check_light(const ff_scene* s, int32_t light, uint32_t mode);   // FF_REQUIRE on bad indices
+ffp::FFLightSet ff_light_set(const ff_scene* s, int32_t light, uint32_t mode);
 
 // ff_cache.cu: learned radiance cache.
 struct ff_cache {

@@ -25,23 +25,90 @@ __device__ __forceinline__ ff_ray make_ray(float3 o, float3 d, float tmax)
 }
 
 // Light radiance toward wi, pdf of wi, and the visibility ray of light.visible()
-// (env: any occluder; area: the rectangle must be hit, and the occluder must
-// lie before the projection of a fresh sample point).
+// (env and directional: any occluder; area: the rectangle must be hit, and
+// the occluder must lie before the projection of a fresh sample point).
+// `scale` is the number of lights when one is chosen per vertex (FF_LIGHT_ALL):
+// the chosen light's contributions count for all of them.
 struct LightCtx {
     FFEnvView env;
     bool is_env;
+    bool is_dir;        // dDirectionalLight: delta light
     bool corrected;
     FFRect rect;
+    float3 dir, dir_Le;
+    float scale;
 };
+
+// The lights of a render: -1 env, 0..A-1 area, A..A+D-1 directional,
+// FF_LIGHT_ALL one of all (env first when present) per vertex.
+struct FFLightSet {
+    FFEnvView env;
+    bool has_env;
+    const ff_area_light* area;
+    uint32_t n_area;
+    const ff_directional_light* dirs;
+    uint32_t n_dir;
+    int32_t light;
+    bool corrected;
+};
+
+__device__ __forceinline__ LightCtx select_light(const FFLightSet& s, uint32_t key, uint32_t L)
+{
+    LightCtx lc;
+    lc.env = s.env;
+    lc.corrected = s.corrected;
+    lc.is_env = lc.is_dir = false;
+    lc.scale = 1.f;
+    int32_t id = s.light;
+    if (id == FF_LIGHT_ALL) {
+        const uint32_t n = (s.has_env ? 1u : 0u) + s.n_area + s.n_dir;
+        const uint32_t k = min((uint32_t)(ff_rand(key, dim_of(L, DIM_LIGHT_SEL)) * (float)n), n - 1u);
+        lc.scale = (float)n;
+        id = s.has_env ? (int32_t)k - 1 : (int32_t)k;
+    }
+    if (id < 0) {
+        lc.is_env = true;
+    } else if ((uint32_t)id < s.n_area) {
+        lc.rect = make_rect(s.area[id]);
+    } else {
+        const ff_directional_light& d = s.dirs[(uint32_t)id - s.n_area];
+        lc.is_dir = true;
+        lc.dir = make_float3(d.direction[0], d.direction[1], d.direction[2]);
+        lc.dir_Le = d.radiance * make_float3(d.emissive[0], d.emissive[1], d.emissive[2]);
+    }
+    return lc;
+}
+
+// light.get_direction (kernel.cu:435): the NEE direction and sample point.
+__device__ __forceinline__ void sample_light(const LightCtx& lc, float3 pos, uint32_t key, uint32_t L, float3& wi,
+                                             float3& sp)
+{
+    if (lc.is_env) {
+        const float ex = ff_rand(key, dim_of(L, DIM_LIGHT)), ey = ff_rand(key, dim_of(L, DIM_LIGHT + 1));
+        if (lc.corrected)
+            env_sample_corrected(lc.env, pos, ex, ey, ff_rand(key, dim_of(L, DIM_EXTRA + 1)),
+                                 ff_rand(key, dim_of(L, DIM_EXTRA + 2)), wi, sp);
+        else
+            env_sample(lc.env, pos, ex, ey, wi, sp);
+    } else if (lc.is_dir) {
+        wi = lc.dir;                         // dDirectionalLight::get_direction
+        sp = pos;
+    } else {
+        sp = rect_sample(lc.rect, rand2(key, L, DIM_LIGHT));
+        wi = normalize3(sp - pos);
+    }
+}
 
 __device__ __forceinline__ float3 light_L(const LightCtx& lc, float3 wi)
 {
-    return lc.is_env ? env_L(lc.env, wi, lc.corrected) : rect_L(lc.rect, wi);
+    const float3 Le = lc.is_env ? env_L(lc.env, wi, lc.corrected) : (lc.is_dir ? lc.dir_Le : rect_L(lc.rect, wi));
+    return lc.scale == 1.f ? Le : Le * lc.scale;
 }
 __device__ __forceinline__ float light_pdf(const LightCtx& lc, float3 pos, float3 wi, uint32_t key, uint32_t L,
                                            uint32_t dim)
 {
     if (lc.is_env) return lc.corrected ? env_pdf_corrected(lc.env, wi) : env_pdf(lc.env, wi);
+    if (lc.is_dir) return 1.f;
     return rect_pdf(lc.rect, pos, rand2(key, L, dim));
 }
 // Visibility ray of light.visible(ray): returns false when the reference
@@ -49,7 +116,7 @@ __device__ __forceinline__ float light_pdf(const LightCtx& lc, float3 pos, float
 __device__ __forceinline__ bool light_vis_ray(const LightCtx& lc, float3 o, float3 d, uint32_t key, uint32_t L,
                                               uint32_t dim, ff_ray& out)
 {
-    if (lc.is_env) {
+    if (lc.is_env || lc.is_dir) {
         out = make_ray(o, d, FF_K_HUGE);
         return true;
     }
@@ -74,8 +141,9 @@ __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf
         const double spec_pdf = spec_get_pdf(n, wi, wo, r);
         const double lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
         if (lpdf > 0.f && Li != make_float3(0.f, 0.f, 0.f)) {
-            const double diff_w = power_heuristic(lpdf, diff_pdf);
-            const double spec_w = power_heuristic(lpdf, spec_pdf);
+            // dMaterial.cu:386-393: weights 1 for a delta light
+            const double diff_w = lc.is_dir ? 1.0 : power_heuristic(lpdf, diff_pdf);
+            const double spec_w = lc.is_dir ? 1.0 : power_heuristic(lpdf, spec_pdf);
             float3 f = spec_f(mat, n, wi, wo) * n_dot_wi;
             if (f != make_float3(0.f, 0.f, 0.f)) Lsum = Lsum + ((f * (float)spec_w) * Li) / (float)lpdf;
             f = diff_f(mat, n, wi, wo) * n_dot_wi;
@@ -85,9 +153,10 @@ __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf
     o.c_nee = Lsum;
     const float3 wi_spec = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
     const float3 wi_diff = diff_sample(n, ff_rand(key, dim_of(L, DIM_DIFF)), ff_rand(key, dim_of(L, DIM_DIFF + 1)));
-    // BSDF-sampled MIS terms; their visibility is traced as shadow rays
+    // BSDF-sampled MIS terms (none for a delta light, dMaterial.cu:410);
+    // their visibility is traced as shadow rays
     o.ray_spec = o.ray_diff = false;
-    {
+    if (!lc.is_dir) {
         const float3 org = pos + wi_spec * 0.001f;
         const float nd = dot3(n, wi_spec);
         ff_ray vr;
@@ -104,7 +173,7 @@ __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf
             }
         }
     }
-    {
+    if (!lc.is_dir) {
         // dMaterial.cu:431: the reference offsets this ray along wi_spec (parity)
         const float3 org = corrected ? pos + wi_diff * 0.001f : pos + wi_spec * 0.001f;
         const float nd = dot3(n, wi_diff);

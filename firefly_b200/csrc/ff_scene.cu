@@ -6,7 +6,9 @@
 // dTriangle.cu:22-32) and the managed-memory material / light tables
 // (dScene.cpp:172-298).  Traversal reads only the 48-byte FFTri records;
 // the attributes below are read once per hit, by original triangle index.
+#include <cmath>
 #include "ff_internal.h"
+#include "ff_paths.cuh"
 #include "ff_shade.cuh"
 
 namespace {
@@ -110,6 +112,23 @@ void ff_build_shading(ff_context* ctx, ff_scene* s, const ff_scene_desc* d, cons
         FF_CUDA_CHECK(cudaMemcpyAsync(s->area_lights.ptr, d->area_lights, sizeof(ff_area_light) * d->num_area_lights,
                                       cudaMemcpyHostToDevice, st));
     }
+    // dDirectionalLight(dir) normalises its direction (dDirectionalLight.cu:10-14)
+    s->num_dir_lights = d->num_directional_lights;
+    if (d->num_directional_lights) {
+        std::vector<ff_directional_light> dl(d->directional_lights, d->directional_lights + d->num_directional_lights);
+        for (auto& l : dl) {
+            const double x = l.direction[0], y = l.direction[1], z = l.direction[2];
+            const double len = std::sqrt(x * x + y * y + z * z);
+            FF_REQUIRE(len > 0.0 && std::isfinite(len), "directional light without a direction");
+            l.direction[0] = (float)(x / len);
+            l.direction[1] = (float)(y / len);
+            l.direction[2] = (float)(z / len);
+        }
+        s->dir_lights.alloc(sizeof(ff_directional_light) * dl.size());
+        FF_CUDA_CHECK(cudaMemcpyAsync(s->dir_lights.ptr, dl.data(), sizeof(ff_directional_light) * dl.size(),
+                                      cudaMemcpyHostToDevice, st));
+        FF_CUDA_CHECK(cudaStreamSynchronize(st));
+    }
     s->env.color = make_float3(d->env_color[0], d->env_color[1], d->env_color[2]);
     if (d->env_rgb) {
         s->env.width = (int)d->env_width;
@@ -120,4 +139,45 @@ void ff_build_shading(ff_context* ctx, ff_scene* s, const ff_scene_desc* d, cons
         ff_build_env_tables(ctx, s);
     }
     FF_CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
+FFEnvView ff_env_view(const ff_scene* s)
+{
+    FFEnvView e;
+    e.rgb = s->env.rgb.as<float3>();
+    e.marginal = s->env.marginal.as<double>();
+    e.cond = s->env.conditional.as<double>();
+    e.pdf = s->env.pdf.as<float>();
+    e.width = s->env.width;
+    e.height = s->env.height;
+    e.color = s->env.color;
+    e.radius = 10000.f;   // dEnvironmentLight.cu:14
+    return e;
+}
+
+void ff_check_light(const ff_scene* s, int32_t light, uint32_t mode)
+{
+    if (light == FF_LIGHT_ALL) {
+        FF_REQUIRE(mode == FF_MODE_CORRECTED, "FF_LIGHT_ALL (light selection) needs FF_MODE_CORRECTED");
+        FF_REQUIRE(s->env.width > 0 || s->num_area_lights + s->num_dir_lights > 0, "the scene has no light");
+    } else if (light < 0) {
+        FF_REQUIRE(light == -1, "light must be -1, FF_LIGHT_ALL or a light index");
+        FF_REQUIRE(s->env.width > 0, "light -1 (environment) needs an environment map");
+    } else {
+        FF_REQUIRE((uint32_t)light < s->num_area_lights + s->num_dir_lights, "light index out of range");
+    }
+}
+
+ffp::FFLightSet ff_light_set(const ff_scene* s, int32_t light, uint32_t mode)
+{
+    ffp::FFLightSet l;
+    l.env = ff_env_view(s);
+    l.has_env = s->env.width > 0;
+    l.area = s->area_lights.as<ff_area_light>();
+    l.n_area = s->num_area_lights;
+    l.dirs = s->dir_lights.as<ff_directional_light>();
+    l.n_dir = s->num_dir_lights;
+    l.light = light;
+    l.corrected = mode == FF_MODE_CORRECTED;
+    return l;
 }

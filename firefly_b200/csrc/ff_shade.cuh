@@ -34,7 +34,8 @@ enum FFDim : uint32_t {
     DIM_LOBE = 20,         // 20    random() < 0.5 lobe choice
     DIM_NEE_VIS = 21,      // 21,22 area light visible() redraw of the NEE ray (wf_shadow)
     DIM_RR = 23,           // 23    Russian roulette
-    DIM_EXTRA = 24         // 24..31 materials without a reference counterpart
+    DIM_EXTRA = 24,        // 24..26 materials without a reference counterpart, corrected env jitter
+    DIM_LIGHT_SEL = 27     // 27    light choice under FF_LIGHT_ALL
 };
 
 FF_D uint32_t dim_of(uint32_t bounce, uint32_t d) { return 32u * bounce + d; }

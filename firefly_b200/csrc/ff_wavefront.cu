@@ -87,6 +87,7 @@ struct WF {
     const FFTexView* tex;
     float2* hit_uv;
     FFEnvView env;
+    FFLightSet lights;
     ff_camera cam;
 };
 
@@ -229,18 +230,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                                           u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
                 // Light sample (kernel.cu:435, light get_direction).
                 float3 wi, sp;
-                if (w.light < 0) {
-                    const float ex = ff_rand(key, dim_of(L, DIM_LIGHT)), ey = ff_rand(key, dim_of(L, DIM_LIGHT + 1));
-                    if (w.mode == FF_MODE_CORRECTED)
-                        env_sample_corrected(w.env, pos, ex, ey, ff_rand(key, dim_of(L, DIM_EXTRA + 1)),
-                                             ff_rand(key, dim_of(L, DIM_EXTRA + 2)), wi, sp);
-                    else
-                        env_sample(w.env, pos, ex, ey, wi, sp);
-                } else {
-                    const FFRect r = make_rect(w.area[w.light]);
-                    sp = rect_sample(r, rand2(key, L, DIM_LIGHT));
-                    wi = normalize3(sp - pos);
-                }
+                sample_light(select_light(w.lights, key, L), pos, key, L, wi, sp);
                 w.length[s] = L;
                 w.beta[s] = f4(beta);
                 w.hit_pos[s] = f4(pos, __uint_as_float(t.material));
@@ -274,11 +264,8 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
     // every lane runs the same number of iterations so the queue appends can use full-warp ballots
     const uint32_t iters = (n + stride - 1) / stride;
     const uint32_t base = blockIdx.x * blockDim.x + threadIdx.x;
-    LightCtx lc;
-    lc.env = w.env;
-    lc.is_env = w.light < 0;
-    lc.corrected = w.mode == FF_MODE_CORRECTED;
-    if (!lc.is_env) lc.rect = make_rect(w.area[w.light]);
+    const bool per_vertex = w.lights.light == FF_LIGHT_ALL;
+    const LightCtx lc0 = select_light(w.lights, 0u, 0u);   // the fixed light (no draw unless per_vertex)
     for (uint32_t it = 0; it < iters; ++it) {
         const uint32_t qi = base + it * stride;
         const bool valid = qi < n;
@@ -296,6 +283,7 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
             const float3 sp = xyz(w.light_sp[s]);
             const uint32_t key = w.key[s];
             const uint32_t L = w.length[s];
+            const LightCtx lc = per_vertex ? select_light(w.lights, key, L) : lc0;
             o.c_spec = o.c_diff = make_float3(0.f, 0.f, 0.f);
             if (KIND == FF_MAT_MIX) shade_mix(w.mode, lc, mat, pos, n, wo, wi, sp, key, L, o);
             else if (KIND == FF_MAT_DIFFUSE) shade_diffuse(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
@@ -468,11 +456,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     FF_REQUIRE(st->spp > 0, "spp must be > 0");
     FF_REQUIRE(st->max_depth >= 1 && st->max_depth <= 64, "max_depth must be in [1, 64]");
     FF_REQUIRE(st->mode == FF_MODE_PARITY || st->mode == FF_MODE_CORRECTED, "unknown mode");
-    if (st->light < 0) {
-        FF_REQUIRE(scene->env.width > 0, "light -1 (environment) needs an environment map");
-    } else {
-        FF_REQUIRE((uint32_t)st->light < scene->num_area_lights, "light index out of range");
-    }
+    ff_check_light(scene, st->light, st->mode);
     cudaStream_t stream = ctx->stream;
     const uint32_t WH = film->width * film->height;
     const uint64_t target = st->max_paths ? st->max_paths : (1u << 21);
@@ -498,14 +482,8 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     w.area = scene->area_lights.as<ff_area_light>();
     w.n_area = scene->num_area_lights;
     w.tex = scene->tex_table.as<FFTexView>();
-    w.env.rgb = scene->env.rgb.as<float3>();
-    w.env.marginal = scene->env.marginal.as<double>();
-    w.env.cond = scene->env.conditional.as<double>();
-    w.env.pdf = scene->env.pdf.as<float>();
-    w.env.width = scene->env.width;
-    w.env.height = scene->env.height;
-    w.env.color = scene->env.color;
-    w.env.radius = 10000.f;
+    w.env = ff_env_view(scene);
+    w.lights = ff_light_set(scene, st->light, st->mode);
     w.cam = scene->camera;
     const FFBvhView bvh = scene->view();
 

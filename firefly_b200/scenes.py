@@ -158,6 +158,7 @@ class Scene:
     material_ids: np.ndarray | None = None
     materials: list = field(default_factory=list)
     area_lights: list = field(default_factory=list)
+    directional_lights: list = field(default_factory=list)   # light indices after the area lights
     env_rgb: np.ndarray | None = None
     env_color: tuple = (0.0, 0.0, 0.0)
     textures: list = field(default_factory=list)   # (h, w, 3) float32 arrays, indexed by ff_material.*_tex
@@ -175,6 +176,16 @@ class Scene:
 
     def bounds(self):
         return self.positions.min(0), self.positions.max(0)
+
+
+def directional_light(direction, emissive=(1.0, 1.0, 1.0), radiance=1.0) -> A.ff_directional_light:
+    """A directional light shining from `direction` (toward the light)."""
+    L = A.ff_directional_light()
+    for k in range(3):
+        L.direction[k] = float(direction[k])
+        L.emissive[k] = float(emissive[k])
+    L.radiance = float(radiance)
+    return L
 
 
 def material(base_color, kind=A.FF_MAT_MIX, roughness=1.0, metallic=0.0, ior=1.5, fresnel=0.04,

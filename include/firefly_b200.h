@@ -120,6 +120,18 @@ typedef struct ff_area_light {
     float radiance;           /* radiance of the light's material */
 } ff_area_light;
 
+/* Directional light, the reference's dDirectionalLight (dDirectionalLight.cu:
+ * 5-57): a delta light from `direction` (pointing from the scene toward the
+ * light; normalised on upload), radiance * emissive, pdf 1, visibility by an
+ * any-hit ray of unbounded length.  Added by add_directional_lights
+ * (kernel.cu:725-731). */
+typedef struct ff_directional_light {
+    float direction[3];
+    float emissive[3];
+    float radiance;
+    float pad;
+} ff_directional_light;
+
 /* dCamera (dCamera.cuh:9-22) with the inverse view-projection given directly
  * (the reference computes glm::inverse(P*V) on the host, dScene.cpp:381-391).
  * inv_view_proj is the reference's Matrix4x4 m[4][4] flattened row-major,
@@ -153,6 +165,8 @@ typedef struct ff_scene_desc {
     uint32_t num_area_lights;
     ff_camera camera;
     uint32_t flags;               /* reserved, 0 */
+    const ff_directional_light* directional_lights;
+    uint32_t num_directional_lights;
 } ff_scene_desc;
 
 typedef struct ff_scene_stats {
@@ -244,6 +258,7 @@ FF_API ff_status ff_film_tonemap(ff_film* film, float exposure, uint8_t* rgba8, 
 
 /* ----------------------------------------------------------------- render */
 
+#define FF_LIGHT_ALL (-2)      /* ff_render_settings.light: uniform light selection per vertex */
 #define FF_RENDER_PROFILE 1u  /* ff_render_settings.flags: time every stage with CUDA events */
 
 #define FF_MODE_PARITY    0u  /* reproduce the reference's behaviours, see DESIGN */
@@ -255,7 +270,9 @@ typedef struct ff_render_settings {
     uint32_t rr_depth;          /* RR when path length > rr_depth, reference 3 (kernel.cu:372) */
     uint32_t seed;
     uint32_t mode;              /* FF_MODE_* */
-    int32_t light;              /* -1 = environment, k >= 0 = area light k; reference wires 1 = env (kernel.cu:397) */
+    int32_t light;              /* -1 = environment, 0..A-1 = area light k, A..A+D-1 = directional light k-A,
+                                   FF_LIGHT_ALL = one light per vertex chosen uniformly among all of them
+                                   (corrected mode); the reference wires 1 = env (kernel.cu:397) */
     uint32_t max_paths;         /* path pool size, 0 = automatic */
     uint32_t sample_offset;     /* index of the first sample (progressive rendering) */
     uint32_t flags;             /* FF_RENDER_* */

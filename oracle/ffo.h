@@ -70,6 +70,15 @@ typedef struct {
     float radiance;
 } ffo_area_light;
 
+/* dDirectionalLight (dDirectionalLight.cu:5-57): direction toward the light
+ * (normalised by ffo_render in double), radiance * emissive, pdf 1, delta. */
+typedef struct ffo_dir_light {
+    float direction[3];
+    float emissive[3];
+    float radiance;
+    float pad;
+} ffo_dir_light;
+
 typedef struct {
     const float* tris;          /* num_tris x 9: v0 v1 v2 */
     const float* normals;       /* num_tris x 9: vertex normals n0 n1 n2 */
@@ -93,6 +102,10 @@ typedef struct {
     int32_t light;              /* -1 environment, k area light k */
     float shadow_offset;
     int32_t threads;
+    /* light: -1 env, 0..A-1 area, A..A+D-1 directional, -2 one light per
+     * vertex chosen uniformly among all (corrected mode) */
+    const ffo_dir_light* dir_lights;
+    int32_t num_dir_lights;
 } ffo_render_desc;
 
 /* Renders every pixel's spp samples; out_rgb (width*height*3 doubles) gets

@@ -109,7 +109,12 @@ class ffo_render_desc(C.Structure):
                 ("cam_jitter", C.c_float), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
                 ("sample_offset", C.c_int32), ("max_depth", C.c_int32), ("rr_depth", C.c_int32),
                 ("seed", C.c_uint32), ("mode", C.c_int32), ("light", C.c_int32), ("shadow_offset", C.c_float),
-                ("threads", C.c_int32)]
+                ("threads", C.c_int32), ("dir_lights", C.c_void_p), ("num_dir_lights", C.c_int32)]
+
+
+class ffo_dir_light(C.Structure):
+    _fields_ = [("direction", C.c_float * 3), ("emissive", C.c_float * 3), ("radiance", C.c_float),
+                ("pad", C.c_float)]
 
 
 def render(scene, width, height, spp, max_depth=3, rr_depth=3, seed=0, mode=0, light=-1, sample_offset=0,
@@ -153,6 +158,14 @@ def render(scene, width, height, spp, max_depth=3, rr_depth=3, seed=0, mode=0, l
     d.textures, d.num_textures = C.cast(tdesc, C.c_void_p), len(texs)
     d.materials, d.num_materials = C.cast(mats, C.c_void_p), len(scene.materials)
     d.area_lights, d.num_area_lights = C.cast(lights, C.c_void_p), len(scene.area_lights)
+    dls = list(getattr(scene, "directional_lights", []) or [])
+    dirs = (ffo_dir_light * max(1, len(dls)))()
+    for i, L in enumerate(dls):
+        for k in range(3):
+            dirs[i].direction[k] = L.direction[k]
+            dirs[i].emissive[k] = L.emissive[k]
+        dirs[i].radiance = L.radiance
+    d.dir_lights, d.num_dir_lights = C.cast(dirs, C.c_void_p), len(dls)
     d.env_rgb = None if env is None else env.ctypes.data
     d.env_w = 0 if env is None else env.shape[1]
     d.env_h = 0 if env is None else env.shape[0]

@@ -66,7 +66,7 @@ static inline v3 ld3(const float* p) { return V(p[0], p[1], p[2]); }
 enum {
     DIM_CAM_JITTER = 0, DIM_CAM_LENS = 2, DIM_LIGHT = 4, DIM_NEE_PDF = 6, DIM_SPEC = 8, DIM_DIFF = 10,
     DIM_SPEC_VIS = 12, DIM_SPEC_PDF = 14, DIM_DIFF_VIS = 16, DIM_DIFF_PDF = 18, DIM_LOBE = 20,
-    DIM_NEE_VIS = 21, DIM_RR = 23, DIM_EXTRA = 24
+    DIM_NEE_VIS = 21, DIM_RR = 23, DIM_EXTRA = 24, DIM_LIGHT_SEL = 27
 };
 static inline float R(uint32_t key, uint32_t b, uint32_t d) { return ffo_rand(key, 32u * b + d); }
 typedef struct { float x, y; } v2;
@@ -324,8 +324,11 @@ static float rect_pdf(const rect_t* r, v3 pos, v2 u)
 typedef struct {
     const ffo_render_desc* d;
     int is_env;
+    int is_dir;          /* delta light (dDirectionalLight) */
     int corrected;
     rect_t rect;
+    v3 dir, dir_Le;
+    float scale;         /* number of lights under per-vertex selection, else 1 */
     const double* marginal;
     const double* cond;
     const float* pdf;
@@ -382,10 +385,15 @@ static float env_pdf_corrected(const light_ctx* lc, v3 wi)
     float cl = sqrtf(hmax(0.f, 1.f - wi.y * wi.y));
     return cl > 0.f ? lc->pdf[(size_t)y * d->env_w + x] / cl : 0.f;
 }
-static v3 light_L(const light_ctx* lc, v3 wi) { return lc->is_env ? env_L(lc->d, wi) : rect_L(&lc->rect, wi); }
+static v3 light_L(const light_ctx* lc, v3 wi)
+{
+    v3 Le = lc->is_env ? env_L(lc->d, wi) : (lc->is_dir ? lc->dir_Le : rect_L(&lc->rect, wi));
+    return lc->scale == 1.f ? Le : muls(Le, lc->scale);
+}
 static float light_pdf(const light_ctx* lc, v3 pos, v3 wi, uint32_t key, uint32_t L, uint32_t dim)
 {
     if (lc->is_env) return lc->corrected ? env_pdf_corrected(lc, wi) : env_pdf(lc, wi);
+    if (lc->is_dir) return 1.f;
     return rect_pdf(&lc->rect, pos, R2(key, L, dim));
 }
 
@@ -393,7 +401,7 @@ typedef struct { v3 o, d; float tmax; } ray_t;
 
 static int light_vis_ray(const light_ctx* lc, v3 o, v3 d, uint32_t key, uint32_t L, uint32_t dim, ray_t* out)
 {
-    if (lc->is_env) { out->o = o; out->d = d; out->tmax = K_HUGE; return 1; }
+    if (lc->is_env || lc->is_dir) { out->o = o; out->d = d; out->tmax = K_HUGE; return 1; }
     if (!rect_hit(&lc->rect, o, d)) return 0;
     float ts = dot(sub(rect_sample(&lc->rect, R2(key, L, dim)), o), d);
     out->o = o; out->d = d; out->tmax = ts;
@@ -448,7 +456,8 @@ static void shade_mix(const light_ctx* lc, int corrected, const surf_t* mat, v3 
         double sp = spec_get_pdf(n, wi, wo, r);
         double lp = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
         if (lp > 0.f && !iszero(Li)) {
-            double dw = power_heuristic(lp, dp), sw = power_heuristic(lp, sp);
+            /* dMaterial.cu:386-393: weights 1 for a delta light */
+            double dw = lc->is_dir ? 1.0 : power_heuristic(lp, dp), sw = lc->is_dir ? 1.0 : power_heuristic(lp, sp);
             v3 f = muls(spec_f(mat, n, wi, wo), ndwi);
             if (!iszero(f)) Lsum = add(Lsum, divs(mul(muls(f, (float)sw), Li), (float)lp));
             f = muls(diff_f(mat, wi, wo), ndwi);
@@ -459,7 +468,7 @@ static void shade_mix(const light_ctx* lc, int corrected, const surf_t* mat, v3 
     v3 wi_spec = spec_sample(n, wo, r, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1));
     v3 wi_diff = diff_sample(n, R(key, L, DIM_DIFF), R(key, L, DIM_DIFF + 1));
     o->has_spec = o->has_diff = 0;
-    {
+    if (!lc->is_dir) {   /* no BSDF-sampled terms for a delta light (dMaterial.cu:410) */
         v3 org = add(pos, muls(wi_spec, 0.001f));
         float nd = dot(n, wi_spec);
         ray_t vr;
@@ -476,7 +485,7 @@ static void shade_mix(const light_ctx* lc, int corrected, const surf_t* mat, v3 
             }
         }
     }
-    {
+    if (!lc->is_dir) {
         v3 org = corrected ? add(pos, muls(wi_diff, 0.001f)) : add(pos, muls(wi_spec, 0.001f));
         float nd = dot(n, wi_diff);
         ray_t vr;
@@ -563,9 +572,40 @@ static void camera_ray(const ffo_render_desc* d, int px, int py, v2 jit, v2 lens
     }
 }
 
+/* The light of a vertex: the fixed one, or under light == -2 one of all
+ * lights (env first when present, then area, then directional) chosen from
+ * the draw DIM_LIGHT_SEL, its contributions scaled by the number of lights. */
+static light_ctx select_light(const light_ctx* base, uint32_t key, uint32_t L)
+{
+    const ffo_render_desc* d = base->d;
+    light_ctx lc = *base;
+    int id = d->light;
+    lc.scale = 1.f;
+    if (id == -2) {
+        uint32_t n = (d->env_rgb ? 1u : 0u) + (uint32_t)d->num_area_lights + (uint32_t)d->num_dir_lights;
+        uint32_t k = (uint32_t)(R(key, L, DIM_LIGHT_SEL) * (float)n);
+        if (k > n - 1) k = n - 1;
+        lc.scale = (float)n;
+        id = d->env_rgb ? (int)k - 1 : (int)k;
+    }
+    lc.is_env = id < 0;
+    lc.is_dir = 0;
+    if (id >= 0 && id < d->num_area_lights) {
+        lc.rect = make_rect(&d->area_lights[id]);
+    } else if (id >= d->num_area_lights) {
+        const ffo_dir_light* dl = &d->dir_lights[id - d->num_area_lights];
+        double x = dl->direction[0], y = dl->direction[1], z = dl->direction[2];
+        double len = sqrt(x * x + y * y + z * z);
+        lc.is_dir = 1;
+        lc.dir = V((float)(x / len), (float)(y / len), (float)(z / len));
+        lc.dir_Le = smul(dl->radiance, ld3(dl->emissive));
+    }
+    return lc;
+}
+
 /* One path sample; returns its radiance (sum of the contributions). */
-static void path_sample(const ffo_render_desc* d, const light_ctx* lc, int px, int py, uint32_t sample, double out[3],
-                        uint64_t* n_ext, uint64_t* n_sh)
+static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int px, int py, uint32_t sample,
+                        double out[3], uint64_t* n_ext, uint64_t* n_sh)
 {
     const int corrected = d->mode == 1;
     uint32_t pixel = (uint32_t)(py * d->width + px);
@@ -627,12 +667,17 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc, int px, i
         v3 n = normalize(add(add(smul(u, n1), smul(v, n2)), smul((1.f - u) - v, n0)));
         v3 pos = add(o, smul(t, dir));
         v3 wi, sp;
+        const light_ctx lcv = select_light(lc_base, key, L);
+        const light_ctx* lc = &lcv;
         if (lc->is_env) {
             if (corrected)
                 env_sample_corrected(lc, pos, R(key, L, DIM_LIGHT), R(key, L, DIM_LIGHT + 1), R(key, L, DIM_EXTRA + 1),
                                      R(key, L, DIM_EXTRA + 2), &wi, &sp);
             else
                 env_sample(lc, pos, R(key, L, DIM_LIGHT), R(key, L, DIM_LIGHT + 1), &wi, &sp);
+        } else if (lc->is_dir) {
+            wi = lc->dir;
+            sp = pos;
         } else {
             sp = rect_sample(&lc->rect, R2(key, L, DIM_LIGHT));
             wi = normalize(sub(sp, pos));
@@ -709,12 +754,16 @@ int ffo_render(const ffo_render_desc* d, double* out_rgb, uint64_t* stats)
     light_ctx lc;
     memset(&lc, 0, sizeof(lc));
     lc.d = d;
-    lc.is_env = d->light < 0;
+    lc.is_env = d->light == -1;
     lc.corrected = d->mode == 1;
+    lc.scale = 1.f;
     double *marginal = NULL, *cond = NULL;
     float* pdf = NULL;
-    if (lc.is_env) {
-        if (!d->env_rgb) return 1;
+    const int n_lights = (d->env_rgb ? 1 : 0) + d->num_area_lights + d->num_dir_lights;
+    if (d->light == -2 && (!lc.corrected || n_lights == 0)) return 1;
+    if (d->light < -2 || (d->light == -1 && !d->env_rgb)) return 1;
+    if (d->light >= d->num_area_lights + d->num_dir_lights) return 1;
+    if (d->env_rgb && (lc.is_env || d->light == -2)) {
         marginal = (double*)malloc(sizeof(double) * d->env_h);
         cond = (double*)malloc(sizeof(double) * (size_t)d->env_w * d->env_h);
         pdf = (float*)malloc(sizeof(float) * (size_t)d->env_w * d->env_h);
@@ -722,9 +771,6 @@ int ffo_render(const ffo_render_desc* d, double* out_rgb, uint64_t* stats)
         lc.marginal = marginal;
         lc.cond = cond;
         lc.pdf = pdf;
-    } else {
-        if (d->light >= d->num_area_lights) return 1;
-        lc.rect = make_rect(&d->area_lights[d->light]);
     }
     memset(out_rgb, 0, sizeof(double) * 3 * (size_t)d->width * d->height);
     int nt = d->threads > 0 ? d->threads : 1;

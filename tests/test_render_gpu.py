@@ -142,3 +142,36 @@ def test_textured_env_scene_parity(ctx, oracle):
         mre = _mre(got[fin], ref[fin])
         print(f"[parity] textured env mode={mode}: mre={mre:.3e}")
         assert mre <= MRE_TOL
+
+
+def test_directional_light_and_light_selection_parity(ctx, oracle):
+    """dDirectionalLight (delta: MIS weights 1, no BSDF-sampled visibility
+    rays) as light 0 of the room open to the sky, in both modes; and
+    FF_LIGHT_ALL (one of env + area + directional chosen per vertex, scaled
+    by the light count) in corrected mode."""
+    import firefly_b200 as ff
+    scn = scenes.textured_room(seed=5, width=40, height=40, tex_res=32, env_w=64, env_h=32, kind=ff.FF_MAT_MIX)
+    scn.directional_lights = [scenes.directional_light((0.3, 1.0, 0.2), (1.0, 0.95, 0.8), 2.5)]
+    scn.area_lights = [scenes.area_light((-1.0, 9.0, -1.0), (2.0, 0.0, 0.0), (0.0, 0.0, 2.0), (0.0, -1.0, 0.0),
+                                        radiance=8.0)]
+    for light, mode in ((1, ff.FF_MODE_PARITY), (1, ff.FF_MODE_CORRECTED), (ff.FF_LIGHT_ALL, ff.FF_MODE_CORRECTED)):
+        got, n, stats = _gpu_render(ctx, scn, 40, 40, 4, light=light, max_depth=4, rr_depth=3, seed=13, mode=mode)
+        ref, (re, rs) = oracle.render(scn, 40, 40, 4, max_depth=4, rr_depth=3, seed=13, mode=mode, light=light,
+                                      threads=cpu_threads())
+        fin = np.isfinite(got) & np.isfinite(ref)
+        assert np.array_equal(np.isfinite(got), np.isfinite(ref))
+        mre = _mre(got[fin], ref[fin])
+        print(f"[parity] light={light} mode={mode}: mre={mre:.3e} ext={stats['extension_rays']}/{re} "
+              f"shadow={stats['shadow_rays']}/{rs} mean={ref[fin].mean():.4f}")
+        assert ref[fin].mean() > 0
+        assert mre <= MRE_TOL
+        assert abs(stats["shadow_rays"] - rs) <= max(2, 1e-3 * rs)
+    import firefly_b200 as ff2
+    ds = ff2.dScene(ctx, scn)
+    pt = ff2.PathTracer(ctx, 8, 8)
+    with pytest.raises(ff2.FireflyError):
+        pt.draw(ds, spp=1, light=ff2.FF_LIGHT_ALL, mode=ff2.FF_MODE_PARITY)   # selection needs the corrected mode
+    with pytest.raises(ff2.FireflyError):
+        pt.draw(ds, spp=1, light=2)                                           # 1 area + 1 directional light
+    pt.close()
+    ds.close()
