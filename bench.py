@@ -290,6 +290,43 @@ def trace_micro(ctx, ds_dev, args, rank, dev, stream, barrier, steps):
     return n * len(batches), per, total, batches, scn, ds, d_rays, d_hits
 
 
+# DRAM bytes per ray of k_trace launches, from an ncu capture at 4,194,304
+# rays per launch (profiles/k_trace_trace_micro.md); traffic scales with rays.
+TRACE_DRAM_BYTES_PER_RAY = {"coherent_closest": (134.470144e6 + 42.339328e6) / 4194304,
+                            "incoherent_closest": (135.088384e6 + 40.223232e6) / 4194304,
+                            "coherent_any": (134.470144e6 + 42.339328e6) / 4194304,
+                            "incoherent_any": (135.088384e6 + 40.223232e6) / 4194304}
+
+
+def reference_cuda_trace(scn, batches, d_hits):
+    """The reference's own GPU traversal (intersect / intersect_shadows of
+    CUDA-RayTracer/dTriangle.cu, built unmodified for sm_100a) over its own
+    SAH BVH, on the same rays: Mrays/s per batch and agreement of its hits
+    with ours.  Outside the timed region; None when oracle/_ref lacks it."""
+    try:
+        from oracle import ffrefcuda
+    except Exception:
+        return None
+    if not ffrefcuda.available():
+        return {"unavailable": "oracle/_ref/libffrefcuda.so was not built (no reference checkout at build time)"}
+    bvh = ffrefcuda.RefGpuBVH(scn.triangle_soup())
+    out, agree = {}, {}
+    total_rays, total_ms = 0, 0.0
+    for k, (name, rays, any_hit) in enumerate(batches):
+        t, prim, ms = bvh.trace(rays, any_hit=any_hit, reps=2)
+        out[name] = round(len(rays) / (ms / 1e3) / 1e6, 1)
+        total_rays += len(rays)
+        total_ms += ms
+        ours = d_hits[k].cpu().numpy()[:, 3]
+        agree[name] = round(float(np.mean((ours >= 0) == (prim >= 0)) if any_hit else np.mean(ours == prim)), 6)
+    bvh.close()
+    return {"mrays": round(total_rays / (total_ms / 1e3) / 1e6, 1), "per_batch_mrays": out,
+            "hit_agreement_with_ours": agree, "bvh_nodes": bvh.num_nodes,
+            "build": "CUDA-RayTracer/dRay.cu + dTriangle.cu unmodified, nvcc 12.9 -O3 sm_100a (FMA contraction on, "
+                     "nvcc's default), 64-thread blocks as wavefront_pathtrace launches them, BVH2 from the "
+                     "reference's host SAH build, 200-byte dTriangle records, 80-byte Isect written per ray"}
+
+
 def run_trace(args, ws, rank, local, dist):
     import torch
     import firefly_b200 as ff
@@ -337,15 +374,20 @@ def run_trace(args, ws, rank, local, dist):
         if not args.no_cpu:
             rate, kind, desc, _ = cpu_trace_rate(batches, target_s=args.cpu_s, threads=os.cpu_count() or 1)
             cpu = {"value": round(rate, 3), "unit": "Mrays/s", "cores": os.cpu_count() or 1, "kind": kind, "sample": desc}
+        ref_cuda = reference_cuda_trace(scn, batches, d_hits) if not args.no_ref_cuda else None
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": TRACE_WORKLOAD, "rays_per_step": rays_per_step, "triangles": scn.num_triangles,
                        "l2": "inputs larger than L2 (512 MiB of rays per batch)", "parallelism": f"replicas{ws}",
-                       "per_batch_mrays": {b[0]: round(n / (t / 1e3) / 1e6, 1) for b, t in zip(batches, per)}},
+                       "per_batch_mrays": {b[0]: round(n / (t / 1e3) / 1e6, 1) for b, t in zip(batches, per)},
+                       "reference_cuda": ref_cuda},
             "roofline": {"bound": "hbm", "kernel": f"k_trace ({batches[k_dom][0]})", "achieved": round(achieved, 2),
-                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": None,
+                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5),
+                         "traffic": int(TRACE_DRAM_BYTES_PER_RAY[batches[k_dom][0]] * n),
+                         "traffic_source": "ncu dram__bytes_read+write of a 4,194,304-ray launch, scaled to the "
+                                           "launch's rays (profiles/k_trace_trace_micro.md)",
                          "peak_source": peak_kind, "bytes_per_ray": RAY_BYTES + HIT_BYTES},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": int(rays_per_step * RAY_BYTES),
@@ -755,6 +797,7 @@ def main(argv=None):
     ap.add_argument("--ref-step-s", type=float, default=6.0, help="reference arm: seconds of CPU work per step")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-relmse", action="store_true", help="skip the 16k-spp reference tile and its relMSE")
+    ap.add_argument("--no-ref-cuda", action="store_true", help="trace workload: skip the reference's GPU traversal")
     ap.add_argument("--with-trace", action="store_true", help="also run the trace micro-benchmark (render line)")
     ap.add_argument("--spp", type=int, default=RENDER["spp"], help="render workload: samples per pixel per step")
     args = ap.parse_args(argv)

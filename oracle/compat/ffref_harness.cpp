@@ -232,6 +232,25 @@ void* ffref_bvh_build(const float* tris9, int n, double* build_ms)
 
 int ffref_bvh_num_nodes(void* h) { return ((RefBVH*)h)->num_nodes; }
 
+// The host build's arrays, for uploading the same BVH to the reference's
+// own GPU traversal (oracle/_ref/libffrefcuda.so): nodes, reordered
+// triangles, the position -> original index map, and the struct sizes.
+void ffref_bvh_data(void* h, const void** nodes, const void** tris, const int** ordered, int* num_tris)
+{
+    RefBVH* b = (RefBVH*)h;
+    *nodes = b->nodes;
+    *tris = b->tris.data();
+    *ordered = b->ordered.data();
+    *num_tris = (int)b->tris.size();
+}
+
+void ffref_sizes(int* node_bytes, int* tri_bytes, int* isect_bytes)
+{
+    *node_bytes = (int)sizeof(LinearBVHNode);
+    *tri_bytes = (int)sizeof(dTriangle);
+    *isect_bytes = (int)sizeof(Isect);
+}
+
 void ffref_bvh_free(void* h) { delete (RefBVH*)h; }
 
 // intersect() / intersect_shadows() (dTriangle.cu:140-259) per ray over

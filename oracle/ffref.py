@@ -42,6 +42,12 @@ def load() -> C.CDLL:
         lib.ffref_bvh_trace.argtypes = [P, P, C.c_long, P, C.c_int, C.c_int]
         lib.ffref_bvh_free.restype = None
         lib.ffref_bvh_free.argtypes = [P]
+        lib.ffref_bvh_num_nodes.restype = C.c_int
+        lib.ffref_bvh_num_nodes.argtypes = [P]
+        lib.ffref_bvh_data.restype = None
+        lib.ffref_bvh_data.argtypes = [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(C.c_int)]
+        lib.ffref_sizes.restype = None
+        lib.ffref_sizes.argtypes = [C.POINTER(C.c_int)] * 3
         _lib = lib
     return _lib
 
