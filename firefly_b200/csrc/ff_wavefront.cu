@@ -256,7 +256,9 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
     if ((threadIdx.x & 31u) == 0 && am) atomicAdd(&w.ctr[C_ACTIVE], (uint32_t)__popc(am));
 }
 
-template <int KIND>
+// SEL: the light is chosen per vertex (FF_LIGHT_ALL); otherwise one light
+// context serves the whole launch (fewer live registers).
+template <int KIND, bool SEL>
 __global__ void __launch_bounds__(128) k_shade(WF w)
 {
     const uint32_t n = w.ctr[C_MAT + KIND];
@@ -264,8 +266,8 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
     // every lane runs the same number of iterations so the queue appends can use full-warp ballots
     const uint32_t iters = (n + stride - 1) / stride;
     const uint32_t base = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool per_vertex = w.lights.light == FF_LIGHT_ALL;
-    const LightCtx lc0 = select_light(w.lights, 0u, 0u);   // the fixed light (no draw unless per_vertex)
+    LightCtx lc;
+    if (!SEL) lc = select_light(w.lights, 0u, 0u);   // the fixed light
     for (uint32_t it = 0; it < iters; ++it) {
         const uint32_t qi = base + it * stride;
         const bool valid = qi < n;
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
             const float3 sp = xyz(w.light_sp[s]);
             const uint32_t key = w.key[s];
             const uint32_t L = w.length[s];
-            const LightCtx lc = per_vertex ? select_light(w.lights, key, L) : lc0;
+            if (SEL) lc = select_light(w.lights, key, L);
             o.c_spec = o.c_diff = make_float3(0.f, 0.f, 0.f);
             if (KIND == FF_MAT_MIX) shade_mix(w.mode, lc, mat, pos, n, wo, wi, sp, key, L, o);
             else if (KIND == FF_MAT_DIFFUSE) shade_diffuse(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
@@ -525,11 +527,19 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
             mark();
             k_logic<<<(P + 255) / 256, 256, 0, stream>>>(w);
             mark();
-            if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX><<<shade_blocks, 128, 0, stream>>>(w);
-            if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE><<<shade_blocks, 128, 0, stream>>>(w);
-            if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR><<<shade_blocks, 128, 0, stream>>>(w);
-            if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC><<<shade_blocks, 128, 0, stream>>>(w);
-            if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT><<<shade_blocks, 128, 0, stream>>>(w);
+            if (w.lights.light == FF_LIGHT_ALL) {
+                if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX, true><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE, true><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR, true><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC, true><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT, true><<<shade_blocks, 128, 0, stream>>>(w);
+            } else {
+                if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT, false><<<shade_blocks, 128, 0, stream>>>(w);
+            }
             FF_CUDA_CHECK(cudaGetLastError());
             mark();
             ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err);
