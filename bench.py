@@ -788,7 +788,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["render", "trace", "inverse", "cache"], default="render")
-    ap.add_argument("--cache-warmup", type=int, default=16, help="cache workload: training frames before accumulating")
+    ap.add_argument("--cache-warmup", type=int, default=2, help="cache workload: training frames before accumulating")
     ap.add_argument("--cache-max-frames", type=int, default=1024, help="cache workload: give up after this many")
     ap.add_argument("--cache-frames-only", type=int, default=0,
                     help="cache workload: only render this many cached frames (for profilers)")

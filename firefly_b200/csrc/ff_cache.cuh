@@ -42,6 +42,27 @@ struct alignas(16) Record {
 };
 static_assert(sizeof(Record) == 64, "record layout");
 
+__device__ __forceinline__ Record make_record(float3 pos, float rough, float3 wo, float3 n, float3 v, uint32_t pixel)
+{
+    Record r;
+    r.px = pos.x;
+    r.py = pos.y;
+    r.pz = pos.z;
+    r.rough = rough;
+    r.wx = wo.x;
+    r.wy = wo.y;
+    r.wz = wo.z;
+    r.v0 = v.x;
+    r.nx = n.x;
+    r.ny = n.y;
+    r.nz = n.z;
+    r.v1 = v.y;
+    r.pixel = pixel;
+    r.v2 = v.z;
+    r.pad0 = r.pad1 = 0.f;
+    return r;
+}
+
 __device__ __forceinline__ float3 normalised_pos(const Grid& g, float px, float py, float pz)
 {
     float3 p = make_float3((px - g.lo.x) * g.inv_ext.x, (py - g.lo.y) * g.inv_ext.y, (pz - g.lo.z) * g.inv_ext.z);

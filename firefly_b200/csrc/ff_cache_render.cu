@@ -1,22 +1,21 @@
 // ff_cache_render.cu — path tracing with the learned radiance cache.
 //
 // One frame = one path per pixel plus `train_paths` training paths:
-//   k_cached_paths  one thread per path (megakernel: the same vertex code,
-//                   ff_paths.cuh, and sampler dimensions as ff_render in
-//                   corrected mode).  A pixel path ends at its first rough
-//                   vertex after the camera hit and appends a query record
-//                   (vertex, throughput, pixel); what it gathered before that
-//                   vertex goes to the frame buffer.  A training path, from a
-//                   random pixel with its own samples, runs to the full depth
-//                   and appends one training record: its first rough vertex
-//                   after the camera hit and the radiance the rest of the path
-//                   brought back to it (throughput relative to that vertex).
-//   train           ff_cache_launch_train over the frame's training records,
-//                   in optimiser steps of train_batch records;
-//   infer           ff_cache_launch_infer over the queries: frame[pixel] +=
-//                   throughput * max(cache, 0);
-//   k_frame_to_film the frame joins the film (Kahan-compensated sum, count+1).
-// Record counts stay on the device; no host synchronisation inside a frame.
+//   k_training_paths  one thread per training path (megakernel: the same
+//                     vertex code, ff_paths.cuh, and sampler as ff_render in
+//                     corrected mode), from a random pixel with its own
+//                     samples, to the full depth; it appends one training
+//                     record: its first rough vertex after the camera hit and
+//                     the radiance the rest of the path brought back to it
+//                     (throughput relative to that vertex);
+//   train             ff_cache_launch_train over the frame's records, in
+//                     optimiser steps of train_batch records;
+//   pixel paths       the wavefront stages of ff_render (ff_wavefront.cu) in
+//                     cache mode: a path ends at its first rough vertex after
+//                     the camera hit with a query record; the cache's answers
+//                     (throughput x max(cache, 0)) join the path sums before
+//                     the film update.
+// Record counts stay on the device.
 #include <cstring>
 
 #include "ff_cache.cuh"
@@ -43,21 +42,11 @@ struct CR {
     uint32_t W, H, frame, seed, max_depth, rr_depth, n_train;
     int32_t light;
     float shadow_offset, rough_threshold;
-    float4* frame_rgb;
-    Record* queries;
-    uint32_t* n_queries;
     Record* train;
     uint32_t* n_train_out;
     unsigned long long* rays;     // [0] extension, [1] shadow
     unsigned int* err;
 };
-
-__device__ __forceinline__ bool is_rough(const FFSurf& s, float threshold)
-{
-    if (s.kind == FF_MAT_DIFFUSE) return true;
-    if (s.kind == FF_MAT_DIELECTRIC) return false;
-    return s.roughness >= threshold;
-}
 
 __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want)
 {
@@ -71,28 +60,9 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want)
     return base + __popc(mask & ((1u << lane) - 1u));
 }
 
-__device__ __forceinline__ Record make_record(float3 pos, float rough, float3 wo, float3 n, float3 v, uint32_t pixel)
-{
-    Record r;
-    r.px = pos.x;
-    r.py = pos.y;
-    r.pz = pos.z;
-    r.rough = rough;
-    r.wx = wo.x;
-    r.wy = wo.y;
-    r.wz = wo.z;
-    r.v0 = v.x;
-    r.nx = n.x;
-    r.ny = n.y;
-    r.nz = n.z;
-    r.v1 = v.y;
-    r.pixel = pixel;
-    r.v2 = v.z;
-    r.pad0 = r.pad1 = 0.f;
-    return r;
-}
+using ffc::make_record;
 
-__global__ void __launch_bounds__(kBlock) k_cached_paths(CR a)
+__global__ void __launch_bounds__(kBlock) k_training_paths(CR a)
 {
     __shared__ uint2 s_stack[kShortStack * kBlock];
     FFStack st;
@@ -101,23 +71,16 @@ __global__ void __launch_bounds__(kBlock) k_cached_paths(CR a)
     st.sp = 0;
     st.overflow = false;
     const uint32_t npix = a.W * a.H;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool training = i >= npix;
-    const bool active = i < npix + a.n_train;
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = j < a.n_train;
     uint64_t n_ext = 0, n_shadow = 0;
-    bool want_query = false, want_train = false;
+    bool want_train = false;
     Record rec;
     if (active) {
-        uint32_t pix, key;
-        if (!training) {
-            pix = i;
-            key = ff_path_key(a.seed, pix, a.frame);
-        } else {
-            const uint32_t j = i - npix;
-            const uint32_t h = ff_wang_hash(ff_wang_hash(a.seed ^ 0x6A09E667u) ^ ff_wang_hash(a.frame * 0x9E3779B9u + j));
-            pix = (uint32_t)(((uint64_t)h * npix) >> 32);
-            key = ff_path_key(a.seed ^ 0xBB67AE85u, pix, a.frame * a.n_train + j);
-        }
+        // a random pixel, samples independent of the frame's pixel paths
+        const uint32_t h = ff_wang_hash(ff_wang_hash(a.seed ^ 0x6A09E667u) ^ ff_wang_hash(a.frame * 0x9E3779B9u + j));
+        const uint32_t pix = (uint32_t)(((uint64_t)h * npix) >> 32);
+        const uint32_t key = ff_path_key(a.seed ^ 0xBB67AE85u, pix, a.frame * a.n_train + j);
         float3 o, d;
         gen_camera_ray(a.cam, (int)a.W, (int)a.H, (int)(pix % a.W), (int)(pix / a.W), rand2(key, 0, DIM_CAM_JITTER),
                        rand2(key, 0, DIM_CAM_LENS), o, d);
@@ -173,12 +136,6 @@ __global__ void __launch_bounds__(kBlock) k_cached_paths(CR a)
             const FFSurf surf = resolve_surface(mm, a.tex, tuv);
             const float3 wo = -d;
             if (L >= 2 && !tail && is_rough(surf, a.rough_threshold)) {
-                if (!training) {
-                    // the cache answers for everything from this vertex on
-                    rec = make_record(pos, surf.roughness, wo, n, beta, pix);
-                    want_query = true;
-                    break;
-                }
                 rec = make_record(pos, surf.roughness, wo, n, make_float3(0.f, 0.f, 0.f), pix);
                 tail = true;
                 want_train = true;
@@ -205,7 +162,6 @@ __global__ void __launch_bounds__(kBlock) k_cached_paths(CR a)
             o = pos + n * (side * a.shadow_offset);
             d = sh.ext_d;
         }
-        if (!training) a.frame_rgb[pix] = make_float4(Lacc.x, Lacc.y, Lacc.z, 0.f);
         if (want_train) {
             rec.v0 = Ltail.x;
             rec.v1 = Ltail.y;
@@ -213,8 +169,6 @@ __global__ void __launch_bounds__(kBlock) k_cached_paths(CR a)
             want_train = isfinite(Ltail.x) && isfinite(Ltail.y) && isfinite(Ltail.z);
         }
     }
-    const uint32_t qs = warp_append(a.n_queries, want_query);
-    if (want_query) a.queries[qs] = rec;
     const uint32_t ts = warp_append(a.n_train_out, want_train);
     if (want_train) a.train[ts] = rec;
     for (int off = 16; off; off >>= 1) {
@@ -227,32 +181,10 @@ __global__ void __launch_bounds__(kBlock) k_cached_paths(CR a)
     }
 }
 
-__device__ __forceinline__ void kahan(float& sum, float& comp, float x)
+__global__ void k_tally(const uint32_t* __restrict__ n, unsigned long long* __restrict__ total)
 {
-    const float y = x - comp;
-    const float t = sum + y;
-    comp = (t - sum) - y;
-    sum = t;
-}
-
-__global__ void k_frame_to_film(const float4* __restrict__ frame, uint32_t n, float4* __restrict__ acc,
-                                float4* __restrict__ comp, uint32_t* __restrict__ cnt, const uint32_t* __restrict__ rec_cnt,
-                                unsigned long long* __restrict__ rec_total)
-{
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
-        rec_total[0] += rec_cnt[0];
-        rec_total[1] += rec_cnt[1];
-    }
-    if (i >= n) return;
-    const float4 f = frame[i];
-    float4 s = acc[i], c = comp[i];
-    kahan(s.x, c.x, f.x);
-    kahan(s.y, c.y, f.y);
-    kahan(s.z, c.z, f.z);
-    acc[i] = s;
-    comp[i] = c;
-    cnt[i] += 1u;
+    total[0] += n[0];
+    total[1] += n[1];
 }
 
 }  // namespace
@@ -268,7 +200,6 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
     cudaStream_t stream = ctx->stream;
     if (c->ws_pixels < npix) {
         c->queries.alloc(sizeof(Record) * (size_t)npix);
-        c->frame.alloc(sizeof(float4) * (size_t)npix);
         c->ws_pixels = npix;
     }
     if (c->ws_train < n_train) {
@@ -299,70 +230,81 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
     a.light = st->light;
     a.shadow_offset = st->shadow_offset > 0.f ? st->shadow_offset : 0.001f;
     a.rough_threshold = c->prm.rough_threshold;
-    a.frame_rgb = c->frame.as<float4>();
-    a.queries = c->queries.as<Record>();
-    a.n_queries = cnt;
     a.train = c->train_recs.as<Record>();
     a.n_train_out = cnt + 1;
     a.rays = rays;
     a.err = err;
-    const uint32_t blocks = (npix + n_train + kBlock - 1) / kBlock;
+    // the pixel paths: one sample per pixel per frame through the wavefront
+    ff_render_settings ps = *st;
+    ps.spp = 1;
+    ps.mode = FF_MODE_CORRECTED;
+    ps.max_paths = npix;
+    ps.flags = 0;
+    FFCacheHook hook{c, c->queries.ptr, cnt, npix, c->prm.rough_threshold, nullptr, nullptr};
     const bool profile = (st->flags & FF_RENDER_PROFILE) != 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    if (profile)
-        for (auto& e : ev) FF_CUDA_CHECK(cudaEventCreate(&e));
-    float ms_paths = 0.f, ms_train = 0.f, ms_query = 0.f;
-    uint64_t launches = 0;
-    FF_CUDA_CHECK(cudaEventRecord(ctx->ev0, stream));
+    for (auto& e : ev) FF_CUDA_CHECK(cudaEventCreate(&e));
+    float ms_paths = 0.f, ms_train = 0.f;
+    uint64_t launches = 0, ext = 0, shadow = 0;
+    FF_CUDA_CHECK(cudaEventRecord(ev[0], stream));
+    cudaEvent_t evq[2] = {nullptr, nullptr};
+    if (profile) {
+        for (auto& e : evq) FF_CUDA_CHECK(cudaEventCreate(&e));
+        hook.ev_query0 = evq[0];
+        hook.ev_query1 = evq[1];
+    }
+    float ms_query = 0.f;
     for (uint32_t f = 0; f < st->spp; ++f) {
         a.frame = st->sample_offset + f;
-        FF_CUDA_CHECK(cudaMemsetAsync(cnt, 0, 8, stream));
-        if (profile) FF_CUDA_CHECK(cudaEventRecord(ev[0], stream));
-        k_cached_paths<<<blocks, kBlock, 0, stream>>>(a);
-        launches += 1;
+        FF_CUDA_CHECK(cudaMemsetAsync(cnt + 1, 0, 4, stream));
         if (profile) FF_CUDA_CHECK(cudaEventRecord(ev[1], stream));
+        if (n_train) {
+            k_training_paths<<<(n_train + kBlock - 1) / kBlock, kBlock, 0, stream>>>(a);
+            launches += 1;
+        }
         for (uint32_t off = 0; off < n_train; off += batch) {
             ff_cache_launch_train_slice(c, a.train, off, std::min(batch, n_train - off), cnt + 1);
             launches += 3;
         }
         if (profile) FF_CUDA_CHECK(cudaEventRecord(ev[2], stream));
-        ff_cache_launch_infer(c, a.queries, npix, cnt, nullptr, a.frame_rgb);
-        k_frame_to_film<<<(npix + 255) / 256, 256, 0, stream>>>(a.frame_rgb, npix, film->accum.as<float4>(),
-                                                                 film->comp.as<float4>(), film->count.as<uint32_t>(),
-                                                                 cnt, totals);
-        launches += 2;
+        ps.sample_offset = st->sample_offset + f;
+        ff_render_stats ws{};
+        ff_wavefront_render(ctx, scene, &ps, film, &ws, &hook);
+        k_tally<<<1, 1, 0, stream>>>(cnt, totals);
         FF_CUDA_CHECK(cudaGetLastError());
+        launches += ws.kernel_launches + 2;
+        ext += ws.extension_rays;
+        shadow += ws.shadow_rays;
         if (profile) {
-            FF_CUDA_CHECK(cudaEventRecord(ev[3], stream));
-            FF_CUDA_CHECK(cudaEventSynchronize(ev[3]));
             float t = 0.f;
-            cudaEventElapsedTime(&t, ev[0], ev[1]);
-            ms_paths += t;
+            FF_CUDA_CHECK(cudaEventSynchronize(ev[2]));
             cudaEventElapsedTime(&t, ev[1], ev[2]);
             ms_train += t;
-            cudaEventElapsedTime(&t, ev[2], ev[3]);
+            cudaEventElapsedTime(&t, evq[0], evq[1]);
             ms_query += t;
+            ms_paths += ws.ms_total - t;
         }
     }
-    if (profile)
-        for (auto& e : ev) cudaEventDestroy(e);
-    FF_CUDA_CHECK(cudaEventRecord(ctx->ev1, stream));
+    FF_CUDA_CHECK(cudaEventRecord(ev[3], stream));
     unsigned long long h[6] = {0, 0, 0, 0, 0, 0};
     FF_CUDA_CHECK(cudaMemcpyAsync(h, c->counters.as<char>() + 16, sizeof(h), cudaMemcpyDeviceToHost, stream));
     FF_CUDA_CHECK(cudaStreamSynchronize(stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[3]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (auto& e : evq)
+        if (e) cudaEventDestroy(e);
     if ((unsigned int)h[2]) throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
     if (stats) {
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-        stats->extension_rays = h[0];
-        stats->shadow_rays = h[1];
+        stats->extension_rays = h[0] + ext;
+        stats->shadow_rays = h[1] + shadow;
         stats->samples = (uint64_t)npix * st->spp;
         stats->frames = st->spp;
         stats->ms_total = ms;
-        stats->kernel_launches = launches;
-        stats->ms_cache_paths = ms_paths;
-        stats->ms_cache_train = ms_train;
-        stats->ms_cache_query = ms_query;
+        stats->kernel_launches = (uint32_t)launches;
+        stats->ms_cache_paths = ms_paths;   // pixel paths (wavefront stages)
+        stats->ms_cache_train = ms_train;   // training paths and optimiser steps
+        stats->ms_cache_query = ms_query;   // k_cache_infer over the frame's queries
         stats->cache_queries = h[4];
         stats->cache_records = h[5];
     }

@@ -134,9 +134,20 @@ struct ff_film {
     ~ff_film() { ff_wavefront_ws_free(ws); }
 };
 
-// ff_wavefront.cu
+// ff_wavefront.cu.  With a cache hook, paths end at their first rough vertex
+// after the camera hit with a query record (slot index as the pixel), and the
+// cache's answers join the slot sums before the film update.
+struct ff_cache;
+struct FFCacheHook {
+    ff_cache* cache;
+    void* queries;            // ffc::Record[capacity]
+    uint32_t* n_queries;      // device counter
+    uint32_t capacity;
+    float rough_threshold;
+    cudaEvent_t ev_query0, ev_query1;   // recorded around the inference when not null
+};
 void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, ff_film* film,
-                         ff_render_stats* stats);
+                         ff_render_stats* stats, const FFCacheHook* hook = nullptr);
 
 // ff_bvh.cu: device BVH build from host or device triangle data already on
 // the device (positions float3[V], indices uint3[T]).

@@ -126,6 +126,15 @@ __device__ __forceinline__ bool light_vis_ray(const LightCtx& lc, float3 o, floa
     return true;
 }
 
+// A vertex where the radiance cache may answer: diffuse, or glossy enough
+// (roughness at or above the threshold); a thin dielectric never.
+__device__ __forceinline__ bool is_rough(const FFSurf& s, float threshold)
+{
+    if (s.kind == FF_MAT_DIFFUSE) return true;
+    if (s.kind == FF_MAT_DIELECTRIC) return false;
+    return s.roughness >= threshold;
+}
+
 // wf_mat_mix + BRDF_L / BRDF_f / BRDF_pdf (kernel.cu:617-651, dMaterial.cu:363-469)
 __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf& mat, float3 pos, float3 n, float3 wo,
                           float3 wi, float3 sp, uint32_t key, uint32_t L, ShadeOut& o)

@@ -89,6 +89,12 @@ struct WF {
     FFEnvView env;
     FFLightSet lights;
     ff_camera cam;
+    // learned radiance cache (ff_render_cached): a path ends at its first
+    // rough vertex after the camera hit and leaves a query record there
+    uint32_t cache_mode;
+    float rough_threshold;
+    ffc::Record* queries;
+    uint32_t* n_queries;
 };
 
 __device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
@@ -206,6 +212,41 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             }
             w.acc[s] = acc;
             w.acc_c[s] = accc;
+            bool query = false;
+            ffc::Record rec;
+            if (!terminate) {
+                // Continue: hit attributes (dTriangle::hit, dTriangle.cu:94-105).
+                const FFShadeTri& t = w.shade[hit.prim];
+                const float u = hit.u, v = hit.v;
+                const float3 n = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
+                const float3 pos = ro + hit.t * rd;
+                // texcoord = u * uv1 + v * uv2 + (1 - u - v) * uv0 (dTriangle.cu:97)
+                const float wuv = (1.f - u) - v;
+                const float2 uv = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x,
+                                              u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
+                if (w.cache_mode && L >= 2) {
+                    const FFSurf surf = resolve_surface(w.mats[t.material], w.tex, uv);
+                    if (is_rough(surf, w.rough_threshold)) {
+                        // the cache answers for everything from this vertex on
+                        rec = ffc::make_record(pos, surf.roughness, -rd, n, beta, s);
+                        query = true;
+                        terminate = true;
+                    }
+                }
+                if (!query) {
+                    w.hit_uv[s] = uv;
+                    // Light sample (kernel.cu:435, light get_direction).
+                    float3 wi, sp;
+                    sample_light(select_light(w.lights, key, L), pos, key, L, wi, sp);
+                    w.length[s] = L;
+                    w.beta[s] = f4(beta);
+                    w.hit_pos[s] = f4(pos, __uint_as_float(t.material));
+                    w.hit_nrm[s] = f4(n);
+                    w.light_wi[s] = f4(wi);
+                    w.light_sp[s] = f4(sp);
+                    kind = w.mats[t.material].kind;
+                }
+            }
             if (terminate) {
                 w.cnt[s] += 1u;
                 const uint32_t left = w.samples_left[s] - 1u;
@@ -218,26 +259,10 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                     w.phase[s] = PH_DONE;
                     active = false;
                 }
-            } else {
-                // Continue: hit attributes (dTriangle::hit, dTriangle.cu:94-105).
-                const FFShadeTri& t = w.shade[hit.prim];
-                const float u = hit.u, v = hit.v;
-                const float3 n = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
-                const float3 pos = ro + hit.t * rd;
-                // texcoord = u * uv1 + v * uv2 + (1 - u - v) * uv0 (dTriangle.cu:97)
-                const float wuv = (1.f - u) - v;
-                w.hit_uv[s] = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x,
-                                          u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
-                // Light sample (kernel.cu:435, light get_direction).
-                float3 wi, sp;
-                sample_light(select_light(w.lights, key, L), pos, key, L, wi, sp);
-                w.length[s] = L;
-                w.beta[s] = f4(beta);
-                w.hit_pos[s] = f4(pos, __uint_as_float(t.material));
-                w.hit_nrm[s] = f4(n);
-                w.light_wi[s] = f4(wi);
-                w.light_sp[s] = f4(sp);
-                kind = w.mats[t.material].kind;
+            }
+            if (w.cache_mode) {
+                const uint32_t qi = warp_append(w.n_queries, query, nullptr);
+                if (query) w.queries[qi] = rec;
             }
         }
     }
@@ -453,7 +478,7 @@ void ws_setup(FFWavefrontWS* ws, uint32_t P)
 }  // namespace
 
 void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, ff_film* film,
-                         ff_render_stats* stats)
+                         ff_render_stats* stats, const FFCacheHook* hook)
 {
     FF_REQUIRE(st->spp > 0, "spp must be > 0");
     FF_REQUIRE(st->max_depth >= 1 && st->max_depth <= 64, "max_depth must be in [1, 64]");
@@ -487,6 +512,14 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     w.env = ff_env_view(scene);
     w.lights = ff_light_set(scene, st->light, st->mode);
     w.cam = scene->camera;
+    w.cache_mode = hook ? 1u : 0u;
+    w.rough_threshold = hook ? hook->rough_threshold : 0.f;
+    w.queries = hook ? static_cast<ffc::Record*>(hook->queries) : nullptr;
+    w.n_queries = hook ? hook->n_queries : nullptr;
+    if (hook) {
+        FF_REQUIRE(hook->capacity >= P, "cache query buffer smaller than the path pool");
+        FF_CUDA_CHECK(cudaMemsetAsync(hook->n_queries, 0, sizeof(uint32_t), stream));
+    }
     const FFBvhView bvh = scene->view();
 
     // which material kinds occur
@@ -554,6 +587,12 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
         active = *h_active;
     }
     if (active) throw FFError{FF_ERR_INTERNAL, "wavefront did not finish within its frame bound"};
+    // cache answers join their slots' sums before the film update
+    if (hook) {
+        if (hook->ev_query0) FF_CUDA_CHECK(cudaEventRecord(hook->ev_query0, stream));
+        ff_cache_launch_infer(hook->cache, hook->queries, P, hook->n_queries, nullptr, w.acc);
+        if (hook->ev_query1) FF_CUDA_CHECK(cudaEventRecord(hook->ev_query1, stream));
+    }
     k_resolve<<<(WH + 255) / 256, 256, 0, stream>>>(w, film->accum.as<float4>(), film->comp.as<float4>(),
                                                    film->count.as<uint32_t>());
     FF_CUDA_CHECK(cudaGetLastError());
