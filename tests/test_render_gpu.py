@@ -175,3 +175,20 @@ def test_directional_light_and_light_selection_parity(ctx, oracle):
         pt.draw(ds, spp=1, light=2)                                           # 1 area + 1 directional light
     pt.close()
     ds.close()
+
+
+def test_gltf_round_trip_renders_the_same(ctx, tmp_path):
+    """A scene written to .glb and imported again (triangles regrouped by
+    material, so the BVH differs) renders the same image with the same seeds."""
+    import firefly_b200 as ff
+    from firefly_b200 import gltf
+    scn = scenes.small_room(seed=1, width=48, height=48)
+    p = tmp_path / "room.glb"
+    gltf.save(p, scn)
+    imp = gltf.load(p, 48, 48)
+    imp.camera, imp.area_lights = scn.camera, scn.area_lights
+    a, _, _ = _gpu_render(ctx, scn, 48, 48, 4, light=0, max_depth=5, rr_depth=3, seed=3, mode=ff.FF_MODE_CORRECTED)
+    b, _, _ = _gpu_render(ctx, imp, 48, 48, 4, light=0, max_depth=5, rr_depth=3, seed=3, mode=ff.FF_MODE_CORRECTED)
+    mre = _mre(b, a)
+    print(f"[gltf] round-trip render mre={mre:.3e}")
+    assert mre < 1e-4
