@@ -260,6 +260,15 @@ class PathTracer:
         rgba, n = self.read()
         return rgba[..., :3] / np.maximum(n, 1)[..., None]
 
+    def save(self, path, exposure: float = 1.0):
+        """Tonemapped 8-bit PNG (ff_film_tonemap), or the float mean radiance
+        as PFM when the path ends in .pfm."""
+        from . import image
+        if str(path).lower().endswith(".pfm"):
+            image.write_pfm(path, self.image())
+        else:
+            image.write_png(path, self.tonemap(exposure))
+
     def tonemap(self, exposure: float = 1.0) -> np.ndarray:
         out = np.empty((self.height, self.width, 4), np.uint8)
         _check(lib().ff_film_tonemap(self.film, exposure, _ptr(out), A.FF_MEM_HOST), self.ctx.handle)
