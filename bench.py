@@ -602,6 +602,8 @@ def inverse_experiment(ctx, steps=200, res=512, dev=None, known_lighting=False):
            "steps": steps, "wall_s": round(wall, 2), "heldout_mse_start": h0, "heldout_mse_end": h1,
            "heldout_mse_hidden_params": hf,
            "adjoint_spp_per_s": round(res_opt["adjoint_spp_per_s"], 1),
+           "grad_atomics_per_step": int(res_opt["grad_atomics"] / steps),
+           "kernel_launches_per_step": round(res_opt["kernel_launches"] / steps, 1),
            "adjoint_ms_per_step": round(res_opt["ms_adjoint"] / steps, 3),
            "primal_ms_per_step": round(res_opt["ms_primal"] / steps, 3), "target_render_s": round(t_target, 2),
            "loss_first": res_opt["losses"][0], "loss_last": res_opt["losses"][-1],
@@ -625,13 +627,81 @@ def run_inverse(args, ws, rank, local, dist):
     r["known_lighting_run"] = inverse_experiment(ctx, steps=args.steps if args.steps > 5 else 200, dev=dev,
                                                  known_lighting=True)
     clk = clocks.stop()
+    e2e = inverse_e2e(ctx, dev, stream)
     if rank == 0:
+        peak, peak_kind = measured_peaks()
+        adj_ms = r["adjoint_ms_per_step"]
+        achieved = r["grad_atomics_per_step"] * 12 / (adj_ms / 1e3) / 1e9
+        cpu = None if args.no_cpu else inverse_cpu_baseline(target_s=args.cpu_s)
         line = {"metric": "adjoint spp/s", "value": r["adjoint_spp_per_s"], "unit": "samples/s", "n_gpus": ws,
                 "steps": r["steps"], "warmup": 0, "ms_per_step": r["adjoint_ms_per_step"] + r["primal_ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": r, "clocks": clk}
+                "data": "synthetic", "config": r,
+                "roofline": {"bound": "hbm", "kernel": "k_adjoint (path replay)", "achieved": round(achieved, 2),
+                             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": None,
+                             "peak_source": peak_kind,
+                             "note": "algorithmic bytes = 12 B of float atomics per texel touch after the warp "
+                                     "pre-reduction (counted by the kernel); the kernel also traces every path twice"},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": r["steps"], "clocks": clk}
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def inverse_e2e(ctx, dev, stream, iters=5, res=512):
+    """The adjoint through the public API with host buffers: d_image in,
+    texture and env gradients out, every call (ff_render_adjoint with host
+    pointers)."""
+    import torch
+    import firefly_b200 as ff
+    from firefly_b200 import scenes
+    sky = scenes.sky_env(256, 128, seed=0, sun_radiance=8.0, sun_diameter_deg=20.0)
+    scn = scenes.textured_room(seed=0, width=res, height=res, tex_res=512, env=sky)
+    ds = ff.dScene(ctx, scn)
+    rng = np.random.default_rng(0)
+    d_image = (rng.normal(size=(res, res, 3)) / (res * res * 3)).astype(np.float32)
+    g_tex = np.zeros((512, 512, 3), np.float32)
+    g_env = np.zeros_like(sky, dtype=np.float32)
+    ds.render_adjoint(res, res, d_image, grad_texture=g_tex, grad_env=g_env, spp=16, seed=1)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    samples = 0
+    e0.record(stream)
+    for k in range(iters):
+        st = ds.render_adjoint(res, res, d_image, grad_texture=g_tex, grad_env=g_env, spp=16, seed=2 + k)
+        samples += st["samples"]
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    ds.close()
+    return {"value": round(samples / (ms / 1e3), 1), "unit": "samples/s",
+            "h2d_bytes_per_step": int(d_image.nbytes + g_tex.nbytes + g_env.nbytes),
+            "d2h_bytes_per_step": int(g_tex.nbytes + g_env.nbytes)}
+
+
+def inverse_cpu_baseline(target_s=15.0):
+    """The oracle's path tracer (C restatement, all host threads) on the same
+    scene: primal samples per second over a pixel subset, the lower bound of a
+    CPU adjoint sample's cost (the replay traces every path twice)."""
+    try:
+        from oracle import ffo
+    except Exception:
+        return None
+    from firefly_b200 import scenes
+    sky = scenes.sky_env(256, 128, seed=0, sun_radiance=8.0, sun_diameter_deg=20.0)
+    res = 64
+    scn = scenes.textured_room(seed=0, width=res, height=res, tex_res=512, env=sky)
+    threads = os.cpu_count() or 1
+    spp, ms = 16, 0.0
+    t0 = time.perf_counter()
+    ffo.render(scn, res, res, spp, max_depth=3, rr_depth=3, seed=1, mode=1, light=-1, threads=threads)
+    dt = time.perf_counter() - t0
+    spp2 = max(16, int(spp * target_s / max(dt, 1e-3)))
+    t0 = time.perf_counter()
+    ffo.render(scn, res, res, spp2, max_depth=3, rr_depth=3, seed=2, mode=1, light=-1, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": round(res * res * spp2 / dt, 1), "unit": "samples/s", "cores": threads, "kind": "port",
+            "sample": f"the oracle's path tracer on the same scene at {res}x{res} x {spp2} spp ({dt:.1f} s), "
+                      "primal samples only"}
 
 
 CACHE_WORKLOAD = ("small room (24-tri box + 64x32 UV sphere, area light radiance 15) at 1920x1080, depth 5, "

@@ -56,7 +56,7 @@ struct ADJ {
 // Warp-cooperative scatter of a float3 into grad[3*idx .. 3*idx+2]: lanes
 // holding the same index are summed first, one lane per distinct index issues
 // the atomics.
-__device__ void scatter_add(float* grad, uint32_t idx, float3 v)
+__device__ uint32_t scatter_add(float* grad, uint32_t idx, float3 v)
 {
     const uint32_t active = __activemask();
     const uint32_t peers = __match_any_sync(active, idx);
@@ -71,7 +71,9 @@ __device__ void scatter_add(float* grad, uint32_t idx, float3 v)
         atomicAdd(grad + 3 * (size_t)idx + 0, sum.x);
         atomicAdd(grad + 3 * (size_t)idx + 1, sum.y);
         atomicAdd(grad + 3 * (size_t)idx + 2, sum.z);
+        return 1u;   // one texel touched (12 B of atomics)
     }
+    return 0u;
 }
 
 // Bilinear footprint of tex_bilinear: texel indices and weights.
@@ -106,9 +108,11 @@ __device__ Footprint footprint(int w, int h, float u, float v)
     return f;
 }
 
-__device__ void scatter_footprint(float* grad, const Footprint& f, float3 g)
+__device__ uint32_t scatter_footprint(float* grad, const Footprint& f, float3 g)
 {
-    for (int i = 0; i < 4; ++i) scatter_add(grad, f.idx[i], g * f.w[i]);
+    uint32_t n = 0;
+    for (int i = 0; i < 4; ++i) n += scatter_add(grad, f.idx[i], g * f.w[i]);
+    return n;
 }
 
 __device__ bool closest_hit(const ADJ& a, float3 o, float3 d, FFStack& st, ff_hit& h)
@@ -158,7 +162,7 @@ struct VertexRec {
 // vertices into rec (store-all).
 template <int MODE>
 __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack& st, float3 L_total, float3 dI,
-                           VertexRec* rec, int* n_rec, uint64_t& rays)
+                           VertexRec* rec, int* n_rec, uint64_t& rays, uint64_t& atom)
 {
     const uint32_t key = ff_path_key(a.seed, pix, sample);
     float3 o, d;
@@ -184,7 +188,7 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
                 float3 dd = d;
                 dd.y = clampf(dd.y, -1.f, 1.f);
                 const float2 uv = spherical_map(dd);
-                scatter_footprint(a.grad_env, footprint(a.env.width, a.env.height, uv.x, uv.y), dI * beta);
+                atom += scatter_footprint(a.grad_env, footprint(a.env.width, a.env.height, uv.x, uv.y), dI * beta);
             }
             Lacc = Lacc + c;
         }
@@ -197,7 +201,7 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
                 if (MODE != 0 && vis && a.grad_env && lc.is_env && a.env.rgb) {
                     // NEE term c_nee = coef * Le(wl): d/dLe = beta * coef
                     const float2 uv = spherical_map(nee_dir);
-                    scatter_footprint(a.grad_env, footprint(a.env.width, a.env.height, uv.x, uv.y),
+                    atom += scatter_footprint(a.grad_env, footprint(a.env.width, a.env.height, uv.x, uv.y),
                                       dI * beta * nee_env_coef);
                 }
                 Lacc = Lacc + lb * beta;
@@ -257,7 +261,7 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
                                          surf.albedo.y > 0.f ? Lge.y / surf.albedo.y : 0.f,
                                          surf.albedo.z > 0.f ? Lge.z / surf.albedo.z : 0.f);
             const FFTexView tv = a.tex[a.texture];
-            scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, tuv.x, tuv.y), dI * g);
+            atom += scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, tuv.x, tuv.y), dI * g);
         }
         if (MODE == 2 && tex_grad && *n_rec < kMaxVerts) {
             VertexRec& r = rec[(*n_rec)++];
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(ADJ a)
     st.overflow = false;
     const uint64_t n = (uint64_t)a.W * a.H * a.spp;
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t rays = 0;
+    uint64_t rays = 0, atom = 0;
     if (i < n) {
         const uint32_t pix = (uint32_t)(i % ((uint64_t)a.W * a.H));
         const uint32_t sample = a.sample_offset + (uint32_t)(i / ((uint64_t)a.W * a.H));
@@ -292,25 +296,31 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(ADJ a)
         const float3 dI = make_float3(a.d_image[3 * (size_t)pix] * inv_spp, a.d_image[3 * (size_t)pix + 1] * inv_spp,
                                       a.d_image[3 * (size_t)pix + 2] * inv_spp);
         if (!STORE_ALL) {
-            const float3 Ls = run_path<0>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, nullptr, nullptr, rays);
-            run_path<1>(a, pix, sample, st, Ls, dI, nullptr, nullptr, rays);
+            const float3 Ls = run_path<0>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, nullptr, nullptr, rays, atom);
+            run_path<1>(a, pix, sample, st, Ls, dI, nullptr, nullptr, rays, atom);
         } else {
             VertexRec rec[kMaxVerts];
             int n_rec = 0;
-            const float3 Ls = run_path<2>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, rec, &n_rec, rays);
+            const float3 Ls = run_path<2>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, rec, &n_rec, rays, atom);
             for (int k = 0; k < n_rec; ++k) {
                 const VertexRec& r = rec[k];
                 const float3 Lge = Ls - r.L_before;
                 const float3 g = make_float3(r.a.x > 0.f ? Lge.x / r.a.x : 0.f, r.a.y > 0.f ? Lge.y / r.a.y : 0.f,
                                              r.a.z > 0.f ? Lge.z / r.a.z : 0.f);
                 const FFTexView tv = a.tex[a.texture];
-                scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, r.u, r.v), dI * g);
+                atom += scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, r.u, r.v), dI * g);
             }
         }
     }
     // per-warp ray count
-    for (int off = 16; off; off >>= 1) rays += __shfl_down_sync(0xffffffffu, rays, off);
-    if ((threadIdx.x & 31u) == 0) atomicAdd(a.rays, (unsigned long long)rays);
+    for (int off = 16; off; off >>= 1) {
+        rays += __shfl_down_sync(0xffffffffu, rays, off);
+        atom += __shfl_down_sync(0xffffffffu, atom, off);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        atomicAdd(a.rays, (unsigned long long)rays);
+        atomicAdd(a.rays + 2, (unsigned long long)atom);
+    }
 }
 
 }  // namespace
@@ -392,7 +402,7 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
         if (ad->grad_env && nenv)
             FF_CUDA_CHECK(cudaMemcpyAsync(ad->grad_env, g_env, sizeof(float) * nenv, cudaMemcpyDeviceToHost, stream));
     }
-    unsigned long long h_ctr[2] = {0, 0};
+    unsigned long long h_ctr[3] = {0, 0, 0};
     FF_CUDA_CHECK(cudaMemcpyAsync(h_ctr, ctr.ptr, sizeof(h_ctr), cudaMemcpyDeviceToHost, stream));
     FF_CUDA_CHECK(cudaStreamSynchronize(stream));
     if ((unsigned int)h_ctr[1]) throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
@@ -400,6 +410,7 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
         stats->extension_rays = h_ctr[0];
+        stats->grad_atomics = h_ctr[2];
         stats->samples = n;
         stats->ms_total = ms;
         stats->kernel_launches = 1;

@@ -45,7 +45,7 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
     m_tex, v_tex, m_env, v_env = (torch.zeros_like(x) for x in (albedo, albedo, env, env))
     rgba = torch.empty((h, w, 4), dtype=torch.float32, device=dev)
     cnt = torch.empty((h, w), dtype=torch.int32, device=dev)
-    losses, t_primal, t_adjoint, adj_samples = [], 0.0, 0.0, 0
+    losses, t_primal, t_adjoint, adj_samples, atomics, launches = [], 0.0, 0.0, 0, 0, 0
     # The library runs on the context's stream, torch on its current stream:
     # every hand-over between the two waits for the producer (torch side:
     # torch.cuda.synchronize; library side: ctx.sync).
@@ -59,6 +59,7 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
         st = tracer.draw(ds, spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed + it, light=light,
                          mode=A.FF_MODE_CORRECTED)
         t_primal += st["ms_total"]
+        launches += st["kernel_launches"]
         rc = L.ff_film_read(tracer.film, _p(rgba), _p(cnt), A.FF_MEM_DEVICE)
         if rc:
             raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
@@ -81,6 +82,8 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
             raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
         t_adjoint += ast.ms_total
         adj_samples += ast.samples
+        atomics += ast.grad_atomics
+        launches += ast.kernel_launches + 2
         fall = lr_decay ** (it / max(1, steps - 1))
         for prm, g, m, v, hi, rate in ((albedo, g_tex, m_tex, v_tex, 1.0, lr), (env, g_env, m_env, v_env, 1e6, lr_env)):
             if rate == 0:
@@ -94,4 +97,5 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
             callback(it, losses[-1])
     torch.cuda.synchronize(dev)
     return {"losses": losses, "ms_primal": t_primal, "ms_adjoint": t_adjoint, "adjoint_samples": adj_samples,
+            "grad_atomics": atomics, "kernel_launches": launches,
             "adjoint_spp_per_s": adj_samples / (t_adjoint / 1e3) if t_adjoint > 0 else 0.0}

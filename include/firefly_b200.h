@@ -292,6 +292,9 @@ typedef struct ff_render_stats {
      * cache queries answered and training records produced */
     float ms_cache_paths, ms_cache_train, ms_cache_query;
     uint64_t cache_queries, cache_records;
+    /* ff_render_adjoint: texels touched by gradient atomics after the warp
+     * pre-reduction (3 float atomics = 12 B each) */
+    uint64_t grad_atomics;
 } ff_render_stats;
 
 /* Replaces PathTracer::draw + wavefront_pathtrace (PathTracer.cpp:59-79,
