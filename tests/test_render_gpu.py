@@ -192,3 +192,22 @@ def test_gltf_round_trip_renders_the_same(ctx, tmp_path):
     mre = _mre(b, a)
     print(f"[gltf] round-trip render mre={mre:.3e}")
     assert mre < 1e-4
+
+
+def test_render_edge_cases(ctx, oracle):
+    """One-pixel film, depth 1 (camera hits only), an empty scene lit by the
+    environment, and a film larger than the path pool (max_paths)."""
+    import firefly_b200 as ff
+    scn = scenes.small_room(seed=2, width=16, height=16)
+    _parity(ctx, oracle, scn, 1, 1, 8, max_depth=5)
+    _parity(ctx, oracle, scn, 16, 16, 2, max_depth=1)
+    sky = scenes.sphere_under_sky(seed=3, width=16, height=16, env_w=64, env_h=32)
+    empty = scenes.Scene(positions=np.zeros((0, 3), np.float32), indices=np.zeros((0, 3), np.uint32),
+                         normals=np.zeros((0, 3), np.float32), env_rgb=sky.env_rgb, camera=sky.camera)
+    got, n, _ = _gpu_render(ctx, empty, 16, 16, 2, light=-1, mode=ff.FF_MODE_CORRECTED)
+    assert np.all(n == 2) and np.all(np.isfinite(got)) and got.min() > 0      # every camera ray sees the sky
+    got_small_pool, n2, st = _gpu_render(ctx, scn, 16, 16, 3, light=0, max_depth=5, rr_depth=3, seed=4,
+                                         mode=ff.FF_MODE_CORRECTED, max_paths=100)
+    ref, _ = oracle.render(scn, 16, 16, 3, max_depth=5, rr_depth=3, seed=4, mode=1, light=0, threads=cpu_threads())
+    assert np.all(n2 == 3)
+    assert _mre(got_small_pool / 3, ref / 3) <= MRE_TOL
