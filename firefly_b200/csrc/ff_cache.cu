@@ -591,7 +591,7 @@ void ff_cache_launch_infer(ff_cache* c, const void* recs, uint32_t n_max, const 
 // batch is records [offset, offset + n_max) of a list whose length is on the
 // device, and the loss is normalised by the records actually present.
 static void launch_train(ff_cache* c, const Record* recs, uint32_t offset, uint32_t n_max, const uint32_t* n_dev,
-                         uint32_t n_norm, bool gradients_only)
+                         uint32_t n_norm, bool gradients_only, cudaStream_t st)
 {
     static bool attr = false;
     if (!attr) {
@@ -604,7 +604,7 @@ static void launch_train(ff_cache* c, const Record* recs, uint32_t offset, uint3
     a.inv_n = 1.f / (float)std::max<uint32_t>(n_norm, 1u);
     const uint32_t tiles = (n_max + kTile - 1) / kTile;
     const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)c->ctx->num_sms);
-    k_cache_train<<<grid, kThreads, kTrainSmem, c->ctx->stream>>>(a);
+    k_cache_train<<<grid, kThreads, kTrainSmem, st>>>(a);
     FF_CUDA_CHECK(cudaGetLastError());
     if (gradients_only) return;
     c->step += 1;
@@ -615,7 +615,6 @@ static void launch_train(ff_cache* c, const Record* recs, uint32_t offset, uint3
     hp.eps = c->prm.eps;
     hp.c1 = 1.f - (float)std::pow((double)hp.b1, (double)c->step);
     hp.c2 = 1.f - (float)std::pow((double)hp.b2, (double)c->step);
-    cudaStream_t st = c->ctx->stream;
     k_adam_mlp<<<grid_for(kParams, 256), 256, 0, st>>>(c->mlp.as<float>(), c->mlp_grad.as<float>(), c->mlp_m.as<float>(),
                                                       c->mlp_v.as<float>(), c->mlp_img.as<uint8_t>(), hp);
     const uint32_t ng = kLevels << c->prm.log2_table_size;
@@ -627,12 +626,13 @@ static void launch_train(ff_cache* c, const Record* recs, uint32_t offset, uint3
 
 void ff_cache_launch_train(ff_cache* c, const void* recs, uint32_t n, bool gradients_only)
 {
-    launch_train(c, static_cast<const Record*>(recs), 0, n, nullptr, n, gradients_only);
+    launch_train(c, static_cast<const Record*>(recs), 0, n, nullptr, n, gradients_only, c->ctx->stream);
 }
 
-void ff_cache_launch_train_slice(ff_cache* c, const void* recs, uint32_t offset, uint32_t n_max, const uint32_t* n_dev)
+void ff_cache_launch_train_slice(ff_cache* c, const void* recs, uint32_t offset, uint32_t n_max, const uint32_t* n_dev,
+                                 cudaStream_t st)
 {
-    launch_train(c, static_cast<const Record*>(recs), offset, n_max, n_dev, n_max, false);
+    launch_train(c, static_cast<const Record*>(recs), offset, n_max, n_dev, n_max, false, st);
 }
 
 void ff_cache_refresh_copies(ff_cache* c)

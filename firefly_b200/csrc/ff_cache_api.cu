@@ -103,6 +103,9 @@ ff_status ff_cache_create(ff_context* ctx, const ff_scene* scene, const ff_cache
         FF_CUDA_CHECK(cudaMemsetAsync(c->err.ptr, 0, sizeof(unsigned int), ctx->stream));
         ff_cache_setup_grid(c);
         ff_cache_init_params(c);
+        FF_CUDA_CHECK(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking));
+        FF_CUDA_CHECK(cudaEventCreateWithFlags(&c->ev_frame, cudaEventDisableTiming));
+        FF_CUDA_CHECK(cudaEventCreateWithFlags(&c->ev_trained, cudaEventDisableTiming));
         FF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
     });
     if (st != FF_OK) {

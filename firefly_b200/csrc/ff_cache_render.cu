@@ -240,7 +240,7 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
     ps.mode = FF_MODE_CORRECTED;
     ps.max_paths = npix;
     ps.flags = 0;
-    FFCacheHook hook{c, c->queries.ptr, cnt, npix, c->prm.rough_threshold, nullptr, nullptr};
+    FFCacheHook hook{c, c->queries.ptr, cnt, npix, c->prm.rough_threshold, nullptr, nullptr, nullptr};
     const bool profile = (st->flags & FF_RENDER_PROFILE) != 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     for (auto& e : ev) FF_CUDA_CHECK(cudaEventCreate(&e));
@@ -254,19 +254,28 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
         hook.ev_query1 = evq[1];
     }
     float ms_query = 0.f;
+    // Per frame, the training paths and the optimiser steps run on the
+    // cache's own stream beside the pixel paths; the inference waits for
+    // them, and the next frame's training waits for this frame's inference
+    // (it reads the weights the training updates).
+    cudaStream_t aux = c->aux;
+    hook.wait_before_query = c->ev_trained;
     for (uint32_t f = 0; f < st->spp; ++f) {
         a.frame = st->sample_offset + f;
-        FF_CUDA_CHECK(cudaMemsetAsync(cnt + 1, 0, 4, stream));
-        if (profile) FF_CUDA_CHECK(cudaEventRecord(ev[1], stream));
+        FF_CUDA_CHECK(cudaEventRecord(c->ev_frame, stream));
+        FF_CUDA_CHECK(cudaStreamWaitEvent(aux, c->ev_frame, 0));
+        FF_CUDA_CHECK(cudaMemsetAsync(cnt + 1, 0, 4, aux));
+        if (profile) FF_CUDA_CHECK(cudaEventRecord(ev[1], aux));
         if (n_train) {
-            k_training_paths<<<(n_train + kBlock - 1) / kBlock, kBlock, 0, stream>>>(a);
+            k_training_paths<<<(n_train + kBlock - 1) / kBlock, kBlock, 0, aux>>>(a);
             launches += 1;
         }
         for (uint32_t off = 0; off < n_train; off += batch) {
-            ff_cache_launch_train_slice(c, a.train, off, std::min(batch, n_train - off), cnt + 1);
+            ff_cache_launch_train_slice(c, a.train, off, std::min(batch, n_train - off), cnt + 1, aux);
             launches += 3;
         }
-        if (profile) FF_CUDA_CHECK(cudaEventRecord(ev[2], stream));
+        if (profile) FF_CUDA_CHECK(cudaEventRecord(ev[2], aux));
+        FF_CUDA_CHECK(cudaEventRecord(c->ev_trained, aux));
         ps.sample_offset = st->sample_offset + f;
         ff_render_stats ws{};
         ff_wavefront_render(ctx, scene, &ps, film, &ws, &hook);
@@ -285,7 +294,7 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
             ms_paths += ws.ms_total - t;
         }
     }
-    FF_CUDA_CHECK(cudaEventRecord(ev[3], stream));
+    FF_CUDA_CHECK(cudaEventRecord(ev[3], stream));   // the last inference waited for the last training
     unsigned long long h[6] = {0, 0, 0, 0, 0, 0};
     FF_CUDA_CHECK(cudaMemcpyAsync(h, c->counters.as<char>() + 16, sizeof(h), cudaMemcpyDeviceToHost, stream));
     FF_CUDA_CHECK(cudaStreamSynchronize(stream));

@@ -145,6 +145,7 @@ struct FFCacheHook {
     uint32_t capacity;
     float rough_threshold;
     cudaEvent_t ev_query0, ev_query1;   // recorded around the inference when not null
+    cudaEvent_t wait_before_query;      // the stream waits for it before the inference when not null
 };
 void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, ff_film* film,
                          ff_render_stats* stats, const FFCacheHook* hook = nullptr);
@@ -193,10 +194,22 @@ struct ff_cache {
     DevBuf loss;          // float: sum of training losses since the last reset of the counter
     DevBuf err;           // uint32: tensor-core waits that gave up
     uint32_t step = 0;    // Adam steps taken
-    // ff_render_cached workspace
+    // ff_render_cached workspace: training runs on `aux`, beside the pixel
+    // paths on the context's stream
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_frame = nullptr, ev_trained = nullptr;
     DevBuf queries, train_recs, frame, counters;
     uint32_t ws_pixels = 0, ws_train = 0;
     DevBuf io_recs, io_out;   // staging for host-pointer calls
+    ~ff_cache()
+    {
+        if (aux) {
+            cudaStreamSynchronize(aux);
+            cudaStreamDestroy(aux);
+        }
+        if (ev_frame) cudaEventDestroy(ev_frame);
+        if (ev_trained) cudaEventDestroy(ev_trained);
+    }
 };
 void ff_cache_setup_grid(ff_cache* c);
 void ff_cache_init_params(ff_cache* c);
@@ -205,6 +218,7 @@ uint32_t ff_cache_num_params();
 void ff_cache_launch_infer(ff_cache* c, const void* recs, uint32_t n_max, const uint32_t* n_dev, float* out_rgb,
                            float4* frame);
 void ff_cache_launch_train(ff_cache* c, const void* recs, uint32_t n, bool gradients_only);
-void ff_cache_launch_train_slice(ff_cache* c, const void* recs, uint32_t offset, uint32_t n_max, const uint32_t* n_dev);
+void ff_cache_launch_train_slice(ff_cache* c, const void* recs, uint32_t offset, uint32_t n_max, const uint32_t* n_dev,
+                                 cudaStream_t st);
 void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* cache, const ff_render_settings* st, ff_film* film,
                       ff_render_stats* stats);

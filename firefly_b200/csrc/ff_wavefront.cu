@@ -589,6 +589,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     if (active) throw FFError{FF_ERR_INTERNAL, "wavefront did not finish within its frame bound"};
     // cache answers join their slots' sums before the film update
     if (hook) {
+        if (hook->wait_before_query) FF_CUDA_CHECK(cudaStreamWaitEvent(stream, hook->wait_before_query, 0));
         if (hook->ev_query0) FF_CUDA_CHECK(cudaEventRecord(hook->ev_query0, stream));
         ff_cache_launch_infer(hook->cache, hook->queries, P, hook->n_queries, nullptr, w.acc);
         if (hook->ev_query1) FF_CUDA_CHECK(cudaEventRecord(hook->ev_query1, stream));
