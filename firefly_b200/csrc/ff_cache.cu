@@ -22,6 +22,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <atomic>
 #include <cmath>
 #include <new>
 
@@ -554,6 +555,17 @@ void ff_cache_init_params(ff_cache* c)
     c->step = 0;
 }
 
+// The dynamic shared memory above 48 KB is an attribute of the kernel on each
+// device: set once per (kernel, device).
+static void allow_smem(ff_cache* c, const void* fn, uint32_t bytes, int which)
+{
+    static std::atomic<uint64_t> done[2];
+    const uint64_t bit = 1ull << (c->ctx->device & 63);
+    if (done[which].load() & bit) return;
+    FF_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done[which].fetch_or(bit);
+}
+
 static CacheArgs make_args(ff_cache* c, const Record* recs, uint32_t n, const uint32_t* n_dev)
 {
     CacheArgs a{};
@@ -571,11 +583,7 @@ static CacheArgs make_args(ff_cache* c, const Record* recs, uint32_t n, const ui
 void ff_cache_launch_infer(ff_cache* c, const void* recs, uint32_t n_max, const uint32_t* n_dev, float* out_rgb,
                            float4* frame)
 {
-    static bool attr = false;
-    if (!attr) {
-        FF_CUDA_CHECK(cudaFuncSetAttribute(k_cache_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
-        attr = true;
-    }
+    allow_smem(c, reinterpret_cast<const void*>(k_cache_infer), kInferSmem, 0);
     if (n_max == 0) return;
     CacheArgs a = make_args(c, static_cast<const Record*>(recs), n_max, n_dev);
     a.out_rgb = out_rgb;
@@ -593,11 +601,7 @@ void ff_cache_launch_infer(ff_cache* c, const void* recs, uint32_t n_max, const 
 static void launch_train(ff_cache* c, const Record* recs, uint32_t offset, uint32_t n_max, const uint32_t* n_dev,
                          uint32_t n_norm, bool gradients_only, cudaStream_t st)
 {
-    static bool attr = false;
-    if (!attr) {
-        FF_CUDA_CHECK(cudaFuncSetAttribute(k_cache_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem));
-        attr = true;
-    }
+    allow_smem(c, reinterpret_cast<const void*>(k_cache_train), kTrainSmem, 1);
     if (n_max == 0) return;
     CacheArgs a = make_args(c, recs + offset, n_max, n_dev);
     a.offset = offset;
