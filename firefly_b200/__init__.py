@@ -159,11 +159,12 @@ class dScene:
     def render_adjoint(self, width: int, height: int, d_image: np.ndarray, texture: int = 0, grad_texture=None,
                        grad_env=None, spp: int = 1, max_depth: int = 3, rr_depth: int = 3, seed: int = 0,
                        light: int = -1, sample_offset: int = 0, shadow_offset: float = 0.001,
-                       store_all: bool = False) -> dict:
+                       store_all: bool = False, roughness_texture: int = -1, grad_roughness=None) -> dict:
         """Path-replay adjoint of PathTracer.draw(mode=FF_MODE_CORRECTED) with
-        the same settings: adds dL/d(texture texels) to grad_texture and
-        dL/d(env texels) to grad_env (float32 host arrays), given d_image =
-        dL/dI of the mean-radiance image (height, width, 3)."""
+        the same settings: adds dL/d(texture texels) to grad_texture,
+        dL/d(env texels) to grad_env and dL/d(roughness texels, channel 0) to
+        grad_roughness (float32 host arrays shaped like their textures), given
+        d_image = dL/dI of the mean-radiance image (height, width, 3)."""
         dimg = np.ascontiguousarray(d_image, np.float32)
         s = A.ff_render_settings(spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed,
                                  mode=A.FF_MODE_CORRECTED, light=light, max_paths=0, sample_offset=sample_offset,
@@ -171,8 +172,10 @@ class dScene:
         d = A.ff_adjoint_desc(width=width, height=height, d_image=dimg.ctypes.data, texture=texture,
                               grad_texture=None if grad_texture is None else grad_texture.ctypes.data,
                               grad_env=None if grad_env is None else grad_env.ctypes.data,
-                              flags=A.FF_ADJOINT_STORE_ALL if store_all else 0)
-        for g in (grad_texture, grad_env):
+                              flags=A.FF_ADJOINT_STORE_ALL if store_all else 0,
+                              roughness_texture=roughness_texture,
+                              grad_roughness=None if grad_roughness is None else grad_roughness.ctypes.data)
+        for g in (grad_texture, grad_env, grad_roughness):
             if g is not None and (g.dtype != np.float32 or not g.flags.c_contiguous):
                 raise ValueError("gradient buffers must be contiguous float32")
         st = A.ff_render_stats()

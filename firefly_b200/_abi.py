@@ -105,12 +105,13 @@ class ff_render_stats(C.Structure):
                 ("ms_trace_shadow", C.c_float), ("ms_logic", C.c_float), ("ms_shade", C.c_float),
                 ("kernel_launches", C.c_uint32), ("ms_cache_paths", C.c_float), ("ms_cache_train", C.c_float),
                 ("ms_cache_query", C.c_float), ("cache_queries", C.c_uint64), ("cache_records", C.c_uint64),
-                ("grad_atomics", C.c_uint64)]
+                ("grad_atomics", C.c_uint64), ("grad_atomics_roughness", C.c_uint64)]
 
 
 class ff_adjoint_desc(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("d_image", C.c_void_p), ("texture", C.c_int32),
-                ("grad_texture", C.c_void_p), ("grad_env", C.c_void_p), ("flags", C.c_uint32)]
+                ("grad_texture", C.c_void_p), ("grad_env", C.c_void_p), ("flags", C.c_uint32),
+                ("roughness_texture", C.c_int32), ("grad_roughness", C.c_void_p)]
 
 
 class ff_adam_params(C.Structure):

@@ -18,7 +18,11 @@
 // needs no replay; it is the reference the replay is checked against.
 // Sampling is detached: the importance tables and the Russian-roulette
 // probability are not differentiated.  Gradients reach albedo textures of
-// FF_MAT_DIFFUSE surfaces (their BRDF is linear in the albedo) and the
+// FF_MAT_DIFFUSE surfaces (their BRDF is linear in the albedo), roughness
+// textures of the GGX surfaces (mixed, conductor, thin dielectric, coat:
+// at vertex k, dI . [d(own terms)/dr + L_{>k} * dlog(ext_f)/dr] with
+// L_{>k} = L_s - (radiance up to and including vertex k's own terms), the
+// directions, pdfs and MIS weights held at their sampled values) and the
 // environment through camera misses and the NEE term.
 // Scatter: texel gradients go to global memory with atomicAdd after a
 // warp-level pre-reduction of lanes that hit the same texel (__match_any_sync).
@@ -49,6 +53,8 @@ struct ADJ {
     int32_t texture;        // texture receiving gradients, -1 none
     float* grad_tex;        // texels*3
     float* grad_env;        // env texels*3 or nullptr
+    int32_t rough_texture;  // roughness texture receiving gradients (channel x), -1 none
+    float* grad_rough;      // texels*3 of rough_texture (channel x written) or nullptr
     unsigned long long* rays;
     unsigned int* err;
 };
@@ -115,6 +121,60 @@ __device__ uint32_t scatter_footprint(float* grad, const Footprint& f, float3 g)
     return n;
 }
 
+// Scalar variant for the roughness channel: adds to grad[3*idx] only.
+__device__ uint32_t scatter_add1(float* grad, uint32_t idx, float v)
+{
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, idx);
+    float sum = 0.f;
+    for (uint32_t m = peers; m; m &= m - 1) sum += __shfl_sync(peers, v, __ffs(m) - 1);
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) {
+        atomicAdd(grad + 3 * (size_t)idx, sum);
+        return 1u;
+    }
+    return 0u;
+}
+__device__ uint32_t scatter_footprint1(float* grad, const Footprint& f, float g)
+{
+    uint32_t n = 0;
+    for (int i = 0; i < 4; ++i) n += scatter_add1(grad, f.idx[i], g * f.w[i]);
+    return n;
+}
+
+// Roughness derivative of one vertex's terms (detached sampling: directions,
+// pdfs, MIS weights and the roulette stay fixed; only the GGX values D and G
+// move with r).  `imm` is d/dr of the radiance the vertex adds itself
+// (NEE, and for the mixed material the BSDF-sampled light hit; both are
+// beta-weighted), `dext` is d/dr log(ext_f) per channel: everything the path
+// gathers after the vertex carries one factor ext_f.
+struct RoughDeriv {
+    float3 imm, dext;
+};
+__device__ RoughDeriv rough_deriv(const ShadeOut& sh, float3 n, float3 wo, float3 wi, float r, bool vis, bool vis_s,
+                                  float3 beta)
+{
+    // each derivative is evaluated only where its GGX value is non-zero: the
+    // thin dielectric's transmission continues along -wo, where the half
+    // vector of ggx_dlog_dr is undefined (0 * NaN would poison the sum)
+    const float3 zero = make_float3(0.f, 0.f, 0.f);
+    RoughDeriv d;
+    float3 imm = zero;
+    if (vis && sh.c_nee_ggx != zero) imm = imm + sh.c_nee_ggx * (float)ggx_dlog_dr(n, wi, wo, r);
+    if (vis_s && sh.c_spec != zero) {
+        const float3 ws = make_float3(sh.r_spec.dx, sh.r_spec.dy, sh.r_spec.dz);
+        imm = imm + sh.c_spec * (float)ggx_dlog_dr(n, ws, wo, r);
+    }
+    d.imm = imm * beta;
+    d.dext = zero;
+    if (sh.ext_pdf != 0.f && sh.ext_f_ggx != zero) {
+        const float s = (float)ggx_dlog_dr(n, sh.ext_d, wo, r);
+        const float3 df = sh.ext_f_ggx * s;
+        d.dext = make_float3(sh.ext_f.x != 0.f ? df.x / sh.ext_f.x : 0.f, sh.ext_f.y != 0.f ? df.y / sh.ext_f.y : 0.f,
+                             sh.ext_f.z != 0.f ? df.z / sh.ext_f.z : 0.f);
+    }
+    return d;
+}
+
 __device__ bool closest_hit(const ADJ& a, float3 o, float3 d, FFStack& st, ff_hit& h)
 {
     FFRayState r;
@@ -155,14 +215,20 @@ struct VertexRec {
     float3 a;           // albedo at the vertex (texture-fed diffuse only)
     float3 L_before;    // radiance added before the vertex's terms
     float u, v;         // texcoords
+    bool albedo;        // the vertex takes an albedo gradient
+    bool rough;         // the vertex takes a roughness gradient
+    float g_imm;        // dI . d(own terms)/dr
+    float3 dext;        // d/dr log(ext_f)
+    float3 L_after;     // radiance added up to and including the vertex's own terms
 };
 
 // One path sample.  MODE 0: primal (returns L_s).  MODE 1: replay with
 // gradients (L_total = L_s of pass 1).  MODE 2: primal that records the
-// vertices into rec (store-all).
-template <int MODE>
+// vertices into rec (store-all).  ROUGH: roughness gradients requested (a
+// separate instantiation keeps the albedo/environment kernel's registers).
+template <int MODE, bool ROUGH>
 __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack& st, float3 L_total, float3 dI,
-                           VertexRec* rec, int* n_rec, uint64_t& rays, uint64_t& atom)
+                           VertexRec* rec, int* n_rec, uint64_t& rays, uint64_t& atom, uint64_t& atom_r)
 {
     const uint32_t key = ff_path_key(a.seed, pix, sample);
     float3 o, d;
@@ -254,6 +320,26 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
                                        Li.z != 0.f ? sh.c_nee.z / Li.z : 0.f);
         }
         const bool tex_grad = surf.kind == FF_MAT_DIFFUSE && mm.base_color_tex >= 0 && mm.base_color_tex == a.texture;
+        // roughness gradient: GGX surfaces whose roughness comes from the
+        // texture (above the 0.01 floor of resolve_surface, where it is flat)
+        const bool rough_grad = ROUGH && MODE != 0 && surf.kind != FF_MAT_DIFFUSE && mm.roughness_tex >= 0 &&
+                                mm.roughness_tex == a.rough_texture && surf.roughness > 0.01f;
+        RoughDeriv rd;
+        float3 L_after = Lacc;
+        if (rough_grad) {
+            rd = rough_deriv(sh, n, wo, wi, surf.roughness, vis, vis_s, beta);
+            float3 own = make_float3(0.f, 0.f, 0.f);
+            if (vis) own = own + sh.c_nee;
+            if (vis_s) own = own + sh.c_spec;
+            if (vis_d) own = own + sh.c_diff;
+            L_after = Lacc + own * beta;
+        }
+        if (MODE == 1 && rough_grad) {
+            const float3 Lgt = L_total - L_after;
+            const float g = dot3(dI, rd.imm + Lgt * rd.dext);
+            const FFTexView tv = a.tex[a.rough_texture];
+            atom_r += scatter_footprint1(a.grad_rough, footprint(tv.width, tv.height, tuv.x, tuv.y), g);
+        }
         if (MODE == 1 && tex_grad) {
             // L_{>=k} / a_k: everything from this vertex on carries one factor a_k
             const float3 Lge = L_total - Lacc;
@@ -263,12 +349,19 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
             const FFTexView tv = a.tex[a.texture];
             atom += scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, tuv.x, tuv.y), dI * g);
         }
-        if (MODE == 2 && tex_grad && *n_rec < kMaxVerts) {
+        if (MODE == 2 && (tex_grad || rough_grad) && *n_rec < kMaxVerts) {
             VertexRec& r = rec[(*n_rec)++];
             r.a = surf.albedo;
             r.L_before = Lacc;
             r.u = tuv.x;
             r.v = tuv.y;
+            r.albedo = tex_grad;
+            r.rough = rough_grad;
+            if (rough_grad) {
+                r.g_imm = dot3(dI, rd.imm);
+                r.dext = rd.dext;
+                r.L_after = L_after;
+            }
         }
         const float side = dot3(sh.ext_d, n) >= 0.f ? 1.f : -1.f;
         o = pos + n * (side * a.shadow_offset);
@@ -277,7 +370,7 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
     return Lacc;
 }
 
-template <bool STORE_ALL>
+template <bool STORE_ALL, bool ROUGH>
 __global__ void __launch_bounds__(kAdjBlock) k_adjoint(ADJ a)
 {
     __shared__ uint2 s_stack[kShortStack * kAdjBlock];
@@ -288,7 +381,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(ADJ a)
     st.overflow = false;
     const uint64_t n = (uint64_t)a.W * a.H * a.spp;
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t rays = 0, atom = 0;
+    uint64_t rays = 0, atom = 0, atom_r = 0;
     if (i < n) {
         const uint32_t pix = (uint32_t)(i % ((uint64_t)a.W * a.H));
         const uint32_t sample = a.sample_offset + (uint32_t)(i / ((uint64_t)a.W * a.H));
@@ -296,14 +389,22 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(ADJ a)
         const float3 dI = make_float3(a.d_image[3 * (size_t)pix] * inv_spp, a.d_image[3 * (size_t)pix + 1] * inv_spp,
                                       a.d_image[3 * (size_t)pix + 2] * inv_spp);
         if (!STORE_ALL) {
-            const float3 Ls = run_path<0>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, nullptr, nullptr, rays, atom);
-            run_path<1>(a, pix, sample, st, Ls, dI, nullptr, nullptr, rays, atom);
+            const float3 Ls =
+                run_path<0, ROUGH>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, nullptr, nullptr, rays, atom, atom_r);
+            run_path<1, ROUGH>(a, pix, sample, st, Ls, dI, nullptr, nullptr, rays, atom, atom_r);
         } else {
             VertexRec rec[kMaxVerts];
             int n_rec = 0;
-            const float3 Ls = run_path<2>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, rec, &n_rec, rays, atom);
+            const float3 Ls =
+                run_path<2, ROUGH>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, rec, &n_rec, rays, atom, atom_r);
             for (int k = 0; k < n_rec; ++k) {
                 const VertexRec& r = rec[k];
+                if (ROUGH && r.rough) {
+                    const float g = r.g_imm + dot3(dI, (Ls - r.L_after) * r.dext);
+                    const FFTexView tv = a.tex[a.rough_texture];
+                    atom_r += scatter_footprint1(a.grad_rough, footprint(tv.width, tv.height, r.u, r.v), g);
+                }
+                if (!r.albedo) continue;
                 const float3 Lge = Ls - r.L_before;
                 const float3 g = make_float3(r.a.x > 0.f ? Lge.x / r.a.x : 0.f, r.a.y > 0.f ? Lge.y / r.a.y : 0.f,
                                              r.a.z > 0.f ? Lge.z / r.a.z : 0.f);
@@ -316,10 +417,12 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(ADJ a)
     for (int off = 16; off; off >>= 1) {
         rays += __shfl_down_sync(0xffffffffu, rays, off);
         atom += __shfl_down_sync(0xffffffffu, atom, off);
+        atom_r += __shfl_down_sync(0xffffffffu, atom_r, off);
     }
     if ((threadIdx.x & 31u) == 0) {
         atomicAdd(a.rays, (unsigned long long)rays);
         atomicAdd(a.rays + 2, (unsigned long long)atom);
+        if (atom_r) atomicAdd(a.rays + 3, (unsigned long long)atom_r);
     }
 }
 
@@ -337,16 +440,22 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
     cudaStream_t stream = ctx->stream;
     const bool dev = (ad->flags & FF_MEM_DEVICE) != 0;
     const size_t npix = (size_t)ad->width * ad->height;
-    const size_t ntex = ad->texture >= 0 ? (size_t)3 * [&] {
+    const bool rough = ad->grad_roughness != nullptr;
+    FF_REQUIRE(!rough || (ad->roughness_texture >= 0 && ad->roughness_texture < (int32_t)scene->textures.size()),
+               "roughness_texture out of range");
+    auto texels = [&](int32_t t) {
         FFTexView v;
-        FF_CUDA_CHECK(cudaMemcpy(&v, scene->tex_table.as<FFTexView>() + ad->texture, sizeof(v), cudaMemcpyDeviceToHost));
+        FF_CUDA_CHECK(cudaMemcpy(&v, scene->tex_table.as<FFTexView>() + t, sizeof(v), cudaMemcpyDeviceToHost));
         return (size_t)v.width * v.height;
-    }() : 0;
+    };
+    const size_t ntex = ad->texture >= 0 ? (size_t)3 * texels(ad->texture) : 0;
+    const size_t nrough = rough ? (size_t)3 * texels(ad->roughness_texture) : 0;
     const size_t nenv = (size_t)3 * scene->env.width * scene->env.height;
-    DevBuf dimg, gtex, genv, ctr;
+    DevBuf dimg, gtex, genv, grough, ctr;
     const float* d_image = ad->d_image;
     float* g_tex = ad->grad_texture;
     float* g_env = ad->grad_env;
+    float* g_rough = ad->grad_roughness;
     if (!dev) {
         dimg.alloc(sizeof(float) * 3 * npix);
         FF_CUDA_CHECK(cudaMemcpyAsync(dimg.ptr, ad->d_image, sizeof(float) * 3 * npix, cudaMemcpyHostToDevice, stream));
@@ -360,6 +469,12 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
             genv.alloc(sizeof(float) * nenv);
             FF_CUDA_CHECK(cudaMemcpyAsync(genv.ptr, ad->grad_env, sizeof(float) * nenv, cudaMemcpyHostToDevice, stream));
             g_env = genv.as<float>();
+        }
+        if (nrough) {
+            grough.alloc(sizeof(float) * nrough);
+            FF_CUDA_CHECK(cudaMemcpyAsync(grough.ptr, ad->grad_roughness, sizeof(float) * nrough,
+                                          cudaMemcpyHostToDevice, stream));
+            g_rough = grough.as<float>();
         }
     }
     ctr.alloc(64);
@@ -386,14 +501,19 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
     a.texture = ad->texture;
     a.grad_tex = g_tex;
     a.grad_env = (ad->grad_env && nenv) ? g_env : nullptr;
+    a.rough_texture = rough ? ad->roughness_texture : -1;
+    a.grad_rough = rough ? g_rough : nullptr;
     a.rays = ctr.as<unsigned long long>();
     a.err = reinterpret_cast<unsigned int*>(ctr.as<char>() + 8);
     const uint64_t n = (uint64_t)npix * st->spp;
     const uint64_t blocks = (n + kAdjBlock - 1) / kAdjBlock;
     FF_REQUIRE(blocks < (1ull << 31), "adjoint launch too large");
     FF_CUDA_CHECK(cudaEventRecord(ctx->ev0, stream));
-    if (ad->flags & FF_ADJOINT_STORE_ALL) k_adjoint<true><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
-    else k_adjoint<false><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    const bool store_all = (ad->flags & FF_ADJOINT_STORE_ALL) != 0;
+    if (store_all && rough) k_adjoint<true, true><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    else if (store_all) k_adjoint<true, false><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    else if (rough) k_adjoint<false, true><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    else k_adjoint<false, false><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
     FF_CUDA_CHECK(cudaGetLastError());
     FF_CUDA_CHECK(cudaEventRecord(ctx->ev1, stream));
     if (!dev) {
@@ -401,8 +521,11 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
             FF_CUDA_CHECK(cudaMemcpyAsync(ad->grad_texture, g_tex, sizeof(float) * ntex, cudaMemcpyDeviceToHost, stream));
         if (ad->grad_env && nenv)
             FF_CUDA_CHECK(cudaMemcpyAsync(ad->grad_env, g_env, sizeof(float) * nenv, cudaMemcpyDeviceToHost, stream));
+        if (nrough)
+            FF_CUDA_CHECK(cudaMemcpyAsync(ad->grad_roughness, g_rough, sizeof(float) * nrough, cudaMemcpyDeviceToHost,
+                                          stream));
     }
-    unsigned long long h_ctr[3] = {0, 0, 0};
+    unsigned long long h_ctr[4] = {0, 0, 0, 0};
     FF_CUDA_CHECK(cudaMemcpyAsync(h_ctr, ctr.ptr, sizeof(h_ctr), cudaMemcpyDeviceToHost, stream));
     FF_CUDA_CHECK(cudaStreamSynchronize(stream));
     if ((unsigned int)h_ctr[1]) throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
@@ -411,6 +534,7 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
         stats->extension_rays = h_ctr[0];
         stats->grad_atomics = h_ctr[2];
+        stats->grad_atomics_roughness = h_ctr[3];
         stats->samples = n;
         stats->ms_total = ms;
         stats->kernel_launches = 1;

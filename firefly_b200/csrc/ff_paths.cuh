@@ -13,6 +13,9 @@ namespace ffp {
 
 struct ShadeOut {
     float3 c_nee, c_spec, c_diff;
+    // GGX parts of c_nee and ext_f (the terms that depend on the roughness),
+    // read by the adjoint only; c_spec, when set, is GGX throughout
+    float3 c_nee_ggx, ext_f_ggx;
     bool ray_nee, ray_spec, ray_diff;   // shadow rays to trace
     ff_ray r_nee, r_spec, r_diff;
     float3 ext_o, ext_d, ext_f;
@@ -143,6 +146,7 @@ __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf
     const bool corrected = mode == FF_MODE_CORRECTED;
     const float r = mat.roughness;
     float3 Lsum = make_float3(0.f, 0.f, 0.f);
+    o.c_nee_ggx = Lsum;
     const float3 Li = light_L(lc, wi);
     const float n_dot_wi = dot3(n, wi);
     if (n_dot_wi > 0.f) {
@@ -155,6 +159,7 @@ __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf
             const double spec_w = lc.is_dir ? 1.0 : power_heuristic(lpdf, spec_pdf);
             float3 f = spec_f(mat, n, wi, wo) * n_dot_wi;
             if (f != make_float3(0.f, 0.f, 0.f)) Lsum = Lsum + ((f * (float)spec_w) * Li) / (float)lpdf;
+            o.c_nee_ggx = Lsum;
             f = diff_f(mat, n, wi, wo) * n_dot_wi;
             if (f != make_float3(0.f, 0.f, 0.f)) Lsum = Lsum + ((f * (float)diff_w) * Li) / (float)lpdf;
         }
@@ -203,6 +208,7 @@ __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf
     const float3 dir = ff_rand(key, dim_of(L, DIM_LOBE)) < 0.5f ? wi_diff : wi_spec;
     o.ext_d = dir;
     o.ext_f = brdf_f(mat, n, dir, wo);
+    o.ext_f_ggx = spec_f(mat, n, dir, wo);
     o.ext_pdf = brdf_pdf(mat, n, dir, wo);
     o.ext_cos = hmax(0.f, dot3(n, dir));
 }
@@ -222,6 +228,7 @@ __device__ inline void shade_diffuse(uint32_t mode, const LightCtx& lc, const FF
     const float3 dir = diff_sample(n, ff_rand(key, dim_of(L, DIM_DIFF)), ff_rand(key, dim_of(L, DIM_DIFF + 1)));
     o.ext_d = dir;
     o.ext_f = diff_f(mat, n, dir, wo);
+    o.c_nee_ggx = o.ext_f_ggx = make_float3(0.f, 0.f, 0.f);
     o.ext_pdf = (float)diff_get_pdf();
     o.ext_cos = hmax(0.f, dot3(n, dir));
 }
@@ -242,6 +249,8 @@ __device__ inline void shade_conductor(uint32_t mode, const LightCtx& lc, const 
     const float3 dir = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
     o.ext_d = dir;
     o.ext_f = spec_f(mat, n, dir, wo);
+    o.c_nee_ggx = o.c_nee;
+    o.ext_f_ggx = o.ext_f;
     o.ext_pdf = spec_get_pdf(n, dir, wo, r);
     o.ext_cos = hmax(0.f, dot3(n, dir));
 }
@@ -269,17 +278,20 @@ __device__ inline void shade_dielectric(uint32_t mode, const LightCtx& lc, const
     const float nd = dot3(n, wi);
     const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
     if (nd > 0.f && lpdf > 0.f) o.c_nee = ((spec_f(m, n, wi, wo) * nd) * light_L(lc, wi)) / lpdf;
+    o.c_nee_ggx = o.c_nee;
     if (ff_rand(key, dim_of(L, DIM_EXTRA)) < Fr) {
         const float3 dir = spec_sample(n, wo, m.roughness, ff_rand(key, dim_of(L, DIM_SPEC)),
                                        ff_rand(key, dim_of(L, DIM_SPEC + 1)));
         o.ext_d = dir;
         o.ext_f = spec_f(m, n, dir, wo) / Fr;
+        o.ext_f_ggx = o.ext_f;
         o.ext_pdf = spec_get_pdf(n, dir, wo, m.roughness);
         o.ext_cos = hmax(0.f, dot3(n, dir));
     } else {
         const float3 tint = mat.albedo;
         o.ext_d = -wo;
         o.ext_f = tint;
+        o.ext_f_ggx = make_float3(0.f, 0.f, 0.f);
         o.ext_pdf = 1.f;
         o.ext_cos = 1.f;
     }
@@ -289,13 +301,17 @@ __device__ inline void shade_dielectric(uint32_t mode, const LightCtx& lc, const
 // reflects with Schlick Fresnel at the coat IOR, the base is Lambertian
 // weighted by (1 - F).  Continuation picks the coat lobe or the base with
 // equal probability; the pdf is the 50/50 mixture, as BRDF_pdf's.
-__device__ inline float3 coat_f(const FFSurf& mat, float3 n, float3 wi, float3 wo, float r0)
+__device__ inline float3 coat_spec_f(const FFSurf& mat, float3 n, float3 wi, float3 wo, float r0)
 {
     FFSurf c = mat;
     c.fresnel = make_float3(r0, r0, r0);
     c.albedo = make_float3(1.f, 1.f, 1.f);
     c.metallic = 0.f;
-    const float3 spec = spec_f(c, n, wi, wo);
+    return spec_f(c, n, wi, wo);
+}
+__device__ inline float3 coat_f(const FFSurf& mat, float3 n, float3 wi, float3 wo, float r0)
+{
+    const float3 spec = coat_spec_f(mat, n, wi, wo, r0);
     const float3 h = normalize3(wo + wi);
     const float x = 1.f - hmax(0.f, dot3(h, wi));
     const float F = r0 + (1.f - r0) * x * x * x * x * x;
@@ -312,7 +328,12 @@ __device__ inline void shade_coat(uint32_t mode, const LightCtx& lc, const FFSur
     o.c_nee = make_float3(0.f, 0.f, 0.f);
     const float nd = dot3(n, wi);
     const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
-    if (nd > 0.f && lpdf > 0.f) o.c_nee = ((coat_f(mat, n, wi, wo, r0) * nd) * light_L(lc, wi)) / lpdf;
+    o.c_nee_ggx = o.c_nee;
+    if (nd > 0.f && lpdf > 0.f) {
+        const float3 s = (nd * light_L(lc, wi)) / lpdf;
+        o.c_nee = coat_f(mat, n, wi, wo, r0) * s;
+        o.c_nee_ggx = coat_spec_f(mat, n, wi, wo, r0) * s;
+    }
     const float r = mat.roughness;
     float3 dir;
     if (ff_rand(key, dim_of(L, DIM_LOBE)) < 0.5f) {
@@ -329,6 +350,7 @@ __device__ inline void shade_coat(uint32_t mode, const LightCtx& lc, const FFSur
     const float c = hmax(0.f, dot3(n, dir));
     o.ext_d = dir;
     o.ext_f = coat_f(mat, n, dir, wo, r0);
+    o.ext_f_ggx = coat_spec_f(mat, n, dir, wo, r0);
     o.ext_pdf = 0.5f * spec_get_pdf(n, dir, wo, r) + 0.5f * c * FF_1_PI;
     o.ext_cos = c;
 }

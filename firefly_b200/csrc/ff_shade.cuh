@@ -179,6 +179,27 @@ FF_D double geo_atten(float3 wi, float3 wo, float3 n, float r)
     return g1 * g2;
 }
 
+// d/dr of log(D * G) for the GGX lobe of spec_f at roughness r (the Fresnel
+// factor and the 4 NoV NoL denominator do not depend on r):
+//   D = a2 / (pi (nh2 (a2 - 1) + 1)^2), a2 = r^4:
+//       dlogD/dr = 4/r - 8 r^3 nh2 / (nh2 (a2 - 1) + 1)
+//   G = g(nl) g(nv), g(x) = x / (x (1 - k) + k), k = (r + 1)^2 / 8:
+//       dlogG/dr = -(r + 1)/4 * sum over x in {nl, nv} of (1 - x) / (x (1 - k) + k)
+// so that d spec_f / dr = spec_f * ggx_dlog_dr.  Used by the adjoint only.
+FF_D double ggx_dlog_dr(float3 n, float3 wi, float3 wo, float r)
+{
+    const float3 h = normalize3(wo + wi);
+    const double rd = (double)r;
+    const double a2 = rd * rd * rd * rd;
+    const double nh2 = sq_d((double)hmax(0.f, dot3(n, h)));
+    const double dlogD = 4.0 / rd - 8.0 * rd * rd * rd * nh2 / (nh2 * (a2 - 1.0) + 1.0);
+    const double k = (rd + 1.0) * (rd + 1.0) / 8.0;
+    const double nl = hmax(dot3(n, wi), 0.f);
+    const double nv = hmax(dot3(n, wo), 0.f);
+    const double dlogG = -(rd + 1.0) / 4.0 * ((1.0 - nl) / (nl * (1.0 - k) + k) + (1.0 - nv) / (nv * (1.0 - k) + k));
+    return dlogD + dlogG;
+}
+
 // power_heuristic(1, f, 1, g) (dMaterial.cu:114-119)
 FF_D double power_heuristic(double f, double g) { return (f * f) / (f * f + g * g); }
 

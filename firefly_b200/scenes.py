@@ -526,13 +526,27 @@ def albedo_texture(res: int = 512, seed: int = 0) -> np.ndarray:
     return np.stack(ch, -1).astype(np.float32)
 
 
+def roughness_texture(res: int = 512, seed: int = 0, lo: float = 0.1, hi: float = 0.6) -> np.ndarray:
+    """Seeded Perlin roughness in [lo, hi], (res, res, 3) float32; a
+    material's roughness_tex reads channel 0 (the three channels are equal)."""
+    r = np.clip(0.5 * (lo + hi) + 0.5 * (hi - lo) * perlin2(res, seed * 3 + 101), lo, hi)
+    return np.repeat(r[..., None], 3, -1).astype(np.float32)
+
+
 def textured_room(seed: int = 0, width: int = 512, height: int = 512, albedo=None, env=None, tex_res: int = 512,
-                  env_w: int = 256, env_h: int = 128, kind=A.FF_MAT_DIFFUSE) -> Scene:
+                  env_w: int = 256, env_h: int = 128, kind=A.FF_MAT_DIFFUSE, sphere_kind=None,
+                  roughness=None, sphere_metallic: float = 1.0) -> Scene:
     """The small room opened to the sky (no ceiling) for inverse rendering:
     floor, walls and sphere carry one albedo texture (texture 0); the
     environment map lights the room.  `albedo` (res, res, 3) and `env`
     (env_h, env_w, 3) default to the hidden parameters: a seeded Perlin
-    albedo in [0.1, 0.9] and a synthetic sky."""
+    albedo in [0.1, 0.9] and a synthetic sky.
+
+    With `sphere_kind` (a GGX kind: FF_MAT_MIX, CONDUCTOR, DIELECTRIC, COAT)
+    the sphere gets its own material of that kind, base colour 0.8 and
+    metallic `sphere_metallic`, whose roughness reads texture 1:
+    `roughness` (res, res, 3), by default a seeded Perlin roughness in
+    [0.1, 0.6]."""
     rng = np.random.default_rng(seed)
     lo, hi = np.array([-5, 0, -5], np.float32), np.array([5, 10, 5], np.float32)
     rP, rI = box_room(lo, hi)
@@ -566,8 +580,14 @@ def textured_room(seed: int = 0, width: int = 512, height: int = 512, albedo=Non
     mat_ids = np.zeros(len(I), np.uint32)
     mats = [material((0.5, 0.5, 0.5), kind=kind, roughness=1.0, base_color_tex=0)]
     tex = albedo_texture(tex_res, seed) if albedo is None else np.asarray(albedo, np.float32)
+    textures = [tex]
+    if sphere_kind is not None:
+        mat_ids[len(rI):] = 1
+        mats.append(material((0.8, 0.8, 0.8), kind=sphere_kind, roughness=0.5, metallic=sphere_metallic,
+                             roughness_tex=1))
+        textures.append(roughness_texture(tex_res, seed) if roughness is None else np.asarray(roughness, np.float32))
     sky = sky_env(env_w, env_h, seed=seed, sun_radiance=300.0, sun_diameter_deg=6.0) if env is None else env
     cam = make_camera(eye=(0.0, 8.0, 4.9), center=(center[0], center[1], center[2]), fovy=70.0, aspect=width / height,
                       near=0.05, far=60.0)
     return Scene(positions=P, indices=I, normals=N, texcoords=UV, material_ids=mat_ids, materials=mats,
-                 env_rgb=np.asarray(sky, np.float32), textures=[tex], camera=cam, width=width, height=height)
+                 env_rgb=np.asarray(sky, np.float32), textures=textures, camera=cam, width=width, height=height)

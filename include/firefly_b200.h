@@ -295,6 +295,8 @@ typedef struct ff_render_stats {
     /* ff_render_adjoint: texels touched by gradient atomics after the warp
      * pre-reduction (3 float atomics = 12 B each) */
     uint64_t grad_atomics;
+    /* ff_render_adjoint: roughness texels touched (1 float atomic = 4 B each) */
+    uint64_t grad_atomics_roughness;
 } ff_render_stats;
 
 /* Replaces PathTracer::draw + wavefront_pathtrace (PathTracer.cpp:59-79,
@@ -310,23 +312,29 @@ FF_API ff_status ff_render(ff_context* ctx, ff_scene* scene, const ff_render_set
 
 /* Gradient request of ff_render_adjoint.  d_image is dL/dI for the mean
  * radiance image I (width*height*3 floats).  Gradients are ADDED to
- * grad_texture (texels*3 floats of texture `texture`) and grad_env
- * (env texels*3 floats).  flags: FF_MEM_DEVICE when every pointer is device
- * memory, FF_ADJOINT_STORE_ALL for the store-all reference variant. */
+ * grad_texture (texels*3 floats of texture `texture`), grad_env
+ * (env texels*3 floats) and grad_roughness (texels*3 floats of texture
+ * `roughness_texture`; only channel 0, the one a material's roughness_tex
+ * reads, receives gradients).  flags: FF_MEM_DEVICE when every pointer is
+ * device memory, FF_ADJOINT_STORE_ALL for the store-all reference variant. */
 typedef struct ff_adjoint_desc {
     uint32_t width, height;
     const float* d_image;
-    int32_t texture;          /* texture receiving gradients, -1 = none */
+    int32_t texture;          /* albedo texture receiving gradients, -1 = none */
     float* grad_texture;
     float* grad_env;          /* NULL = no environment gradient */
     uint32_t flags;
+    int32_t roughness_texture; /* read only when grad_roughness != NULL */
+    float* grad_roughness;    /* NULL = no roughness gradient */
 } ff_adjoint_desc;
 
 /* Path-replay adjoint of ff_render (no counterpart in the reference, which
  * renders only): the same paths as ff_render in FF_MODE_CORRECTED for the same
  * settings (seed, spp, sample_offset, depths, light), replayed from their
- * seeds; gradients of the albedo texture of FF_MAT_DIFFUSE surfaces and of the
- * environment map (camera misses and NEE), with detached sampling.
+ * seeds; gradients of the albedo texture of FF_MAT_DIFFUSE surfaces, of the
+ * roughness texture of GGX surfaces (FF_MAT_MIX, CONDUCTOR, DIELECTRIC, COAT)
+ * and of the environment map (camera misses and NEE), with detached sampling
+ * (directions, pdfs, MIS weights and the roulette are not differentiated).
  * settings->mode must be FF_MODE_CORRECTED.  stats: rays traced, samples,
  * device time. */
 FF_API ff_status ff_render_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_settings* settings,

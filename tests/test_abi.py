@@ -47,3 +47,41 @@ def test_null_arguments_are_rejected(ff_lib):
     assert ff_lib.ff_scene_destroy(None) == 1
     assert ff_lib.ff_film_destroy(None) == 1
     assert ff_lib.ff_trace(None, None, None, 0, None, 0) == 1
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every struct the ctypes table mirrors has the header's size and field
+    offsets (a C program compiled from include/firefly_b200.h prints them)."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    from firefly_b200 import _abi
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not available")
+    structs = {n: getattr(_abi, n) for n in dir(_abi)
+               if n.startswith("ff_") and isinstance(getattr(_abi, n), type)
+               and issubclass(getattr(_abi, n), ctypes.Structure)}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "firefly_b200.h"', "int main(void) {"]
+    for n, cls in sorted(structs.items()):
+        lines.append(f'printf("{n} size %zu\\n", sizeof({n}));')
+        for f, *_ in cls._fields_:
+            lines.append(f'printf("{n} {f} %zu\\n", offsetof({n}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        a, b, c = ln.split()
+        got[(a, b)] = int(c)
+    bad = []
+    for n, cls in structs.items():
+        if got[(n, "size")] != ctypes.sizeof(cls):
+            bad.append(f"{n}: size {got[(n, 'size')]} vs ctypes {ctypes.sizeof(cls)}")
+        for f, *_ in cls._fields_:
+            if got[(n, f)] != getattr(cls, f).offset:
+                bad.append(f"{n}.{f}: offset {got[(n, f)]} vs ctypes {getattr(cls, f).offset}")
+    assert not bad, bad
