@@ -30,6 +30,7 @@ FF_TRACE_ANY = 2
 FF_RENDER_PROFILE = 1
 FF_LIGHT_ALL = -2
 FF_ADJOINT_STORE_ALL = 4
+FF_ADJOINT_MEGAKERNEL = 16
 FF_ENV_KEEP_TABLES = 8
 FF_CACHE_GRADIENTS_ONLY = 16
 FF_CACHE_LEVELS = 16

@@ -14,8 +14,13 @@
 //           before vertex k); at every NEE and camera-miss lookup of the
 //           environment, add dL/dI * (contribution / radiance looked up) to
 //           the env texels of the lookup's footprint.
-// The store-all variant keeps the vertices of pass 1 in local memory and
-// needs no replay; it is the reference the replay is checked against.
+// ff_render_adjoint runs the replay on the wavefront stages by default
+// (ff_wavefront_adjoint, ff_wavefront.cu: the same k_logic / k_shade /
+// k_trace stages as ff_render, one slot per path, primal pass then replay of
+// the same sample).  This file holds the one-thread-per-sample megakernel
+// variants: the replay (FF_ADJOINT_MEGAKERNEL, kept as a cross-check) and the
+// store-all variant, which keeps the vertices of pass 1 in local memory and
+// needs no replay; it is the reference both replays are checked against.
 // Sampling is detached: the importance tables and the Russian-roulette
 // probability are not differentiated.  Gradients reach albedo textures of
 // FF_MAT_DIFFUSE surfaces (their BRDF is linear in the albedo), roughness
@@ -27,12 +32,14 @@
 // Scatter: texel gradients go to global memory with atomicAdd after a
 // warp-level pre-reduction of lanes that hit the same texel (__match_any_sync).
 #include "ff_internal.h"
+#include "ff_adjoint.cuh"
 #include "ff_paths.cuh"
 #include "ff_trace.cuh"
 
 namespace {
 
 using namespace ffp;
+using namespace ffadj;
 
 constexpr int kAdjBlock = 128;
 constexpr int kMaxVerts = 16;
@@ -59,133 +66,20 @@ struct ADJ {
     unsigned int* err;
 };
 
-// Warp-cooperative scatter of a float3 into grad[3*idx .. 3*idx+2]: lanes
-// holding the same index are summed first, one lane per distinct index issues
-// the atomics.
-__device__ uint32_t scatter_add(float* grad, uint32_t idx, float3 v)
-{
-    const uint32_t active = __activemask();
-    const uint32_t peers = __match_any_sync(active, idx);
-    float3 sum = make_float3(0.f, 0.f, 0.f);
-    for (uint32_t m = peers; m; m &= m - 1) {
-        const int src = __ffs(m) - 1;
-        sum.x += __shfl_sync(peers, v.x, src);
-        sum.y += __shfl_sync(peers, v.y, src);
-        sum.z += __shfl_sync(peers, v.z, src);
-    }
-    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) {
-        atomicAdd(grad + 3 * (size_t)idx + 0, sum.x);
-        atomicAdd(grad + 3 * (size_t)idx + 1, sum.y);
-        atomicAdd(grad + 3 * (size_t)idx + 2, sum.z);
-        return 1u;   // one texel touched (12 B of atomics)
-    }
-    return 0u;
-}
-
-// Bilinear footprint of tex_bilinear: texel indices and weights.
-struct Footprint {
-    uint32_t idx[4];
-    float w[4];
-};
-__device__ Footprint footprint(int w, int h, float u, float v)
-{
-    float xb = u * (float)w - 0.5f;
-    float yb = v * (float)h - 0.5f;
-    float fx = floorf(xb), fy = floorf(yb);
-    float ax = xb - fx, ay = yb - fy;
-    ax = floorf(ax * 256.f + 0.5f) / 256.f;
-    ay = floorf(ay * 256.f + 0.5f) / 256.f;
-    int ix = (int)fx, iy = (int)fy;
-    int x0 = ix % w;
-    x0 = x0 < 0 ? x0 + w : x0;
-    int x1 = (x0 + 1 == w) ? 0 : x0 + 1;
-    int y0 = iy % h;
-    y0 = y0 < 0 ? y0 + h : y0;
-    int y1 = (y0 + 1 == h) ? 0 : y0 + 1;
-    Footprint f;
-    f.idx[0] = y0 * w + x0;
-    f.idx[1] = y0 * w + x1;
-    f.idx[2] = y1 * w + x0;
-    f.idx[3] = y1 * w + x1;
-    f.w[0] = (1.f - ax) * (1.f - ay);
-    f.w[1] = ax * (1.f - ay);
-    f.w[2] = (1.f - ax) * ay;
-    f.w[3] = ax * ay;
-    return f;
-}
-
-__device__ uint32_t scatter_footprint(float* grad, const Footprint& f, float3 g)
-{
-    uint32_t n = 0;
-    for (int i = 0; i < 4; ++i) n += scatter_add(grad, f.idx[i], g * f.w[i]);
-    return n;
-}
-
-// Scalar variant for the roughness channel: adds to grad[3*idx] only.
-__device__ uint32_t scatter_add1(float* grad, uint32_t idx, float v)
-{
-    const uint32_t active = __activemask();
-    const uint32_t peers = __match_any_sync(active, idx);
-    float sum = 0.f;
-    for (uint32_t m = peers; m; m &= m - 1) sum += __shfl_sync(peers, v, __ffs(m) - 1);
-    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) {
-        atomicAdd(grad + 3 * (size_t)idx, sum);
-        return 1u;
-    }
-    return 0u;
-}
-__device__ uint32_t scatter_footprint1(float* grad, const Footprint& f, float g)
-{
-    uint32_t n = 0;
-    for (int i = 0; i < 4; ++i) n += scatter_add1(grad, f.idx[i], g * f.w[i]);
-    return n;
-}
-
-// Roughness derivative of one vertex's terms (detached sampling: directions,
-// pdfs, MIS weights and the roulette stay fixed; only the GGX values D and G
-// move with r).  `imm` is d/dr of the radiance the vertex adds itself
-// (NEE, and for the mixed material the BSDF-sampled light hit; both are
-// beta-weighted), `dext` is d/dr log(ext_f) per channel: everything the path
-// gathers after the vertex carries one factor ext_f.
-struct RoughDeriv {
-    float3 imm, dext;
-};
-__device__ RoughDeriv rough_deriv(const ShadeOut& sh, float3 n, float3 wo, float3 wi, float r, bool vis, bool vis_s,
-                                  float3 beta)
-{
-    // each derivative is evaluated only where its GGX value is non-zero: the
-    // thin dielectric's transmission continues along -wo, where the half
-    // vector of ggx_dlog_dr is undefined (0 * NaN would poison the sum)
-    const float3 zero = make_float3(0.f, 0.f, 0.f);
-    RoughDeriv d;
-    float3 imm = zero;
-    if (vis && sh.c_nee_ggx != zero) imm = imm + sh.c_nee_ggx * (float)ggx_dlog_dr(n, wi, wo, r);
-    if (vis_s && sh.c_spec != zero) {
-        const float3 ws = make_float3(sh.r_spec.dx, sh.r_spec.dy, sh.r_spec.dz);
-        imm = imm + sh.c_spec * (float)ggx_dlog_dr(n, ws, wo, r);
-    }
-    d.imm = imm * beta;
-    d.dext = zero;
-    if (sh.ext_pdf != 0.f && sh.ext_f_ggx != zero) {
-        const float s = (float)ggx_dlog_dr(n, sh.ext_d, wo, r);
-        const float3 df = sh.ext_f_ggx * s;
-        d.dext = make_float3(sh.ext_f.x != 0.f ? df.x / sh.ext_f.x : 0.f, sh.ext_f.y != 0.f ? df.y / sh.ext_f.y : 0.f,
-                             sh.ext_f.z != 0.f ? df.z / sh.ext_f.z : 0.f);
-    }
-    return d;
-}
-
-__device__ bool closest_hit(const ADJ& a, float3 o, float3 d, FFStack& st, ff_hit& h)
+// The traversals and the shading switch are called, not inlined: each is one
+// copy of its code however many sites use it.
+__device__ __noinline__ bool closest_hit(const FFBvhView bvh, unsigned int* err, float3 o, float3 d, FFStack& st,
+                                         ff_hit& h)
 {
     FFRayState r;
     ff_ray_setup(r, o, d, 0.f, __int_as_float(0x7f800000), false);
-    if (a.bvh.num_nodes) {
+    if (bvh.num_nodes) {
         uint2 cur = ff_root_group(r);
         st.reset();
         uint32_t steps = 0;
-        while (!ff_traverse_step<false>(a.bvh, r, cur, st)) {
-            if (++steps > a.bvh.num_nodes + 2 || st.overflow) {
-                atomicAdd(a.err, 1u);
+        while (!ff_traverse_step<false>(bvh, r, cur, st)) {
+            if (++steps > bvh.num_nodes + 2 || st.overflow) {
+                atomicAdd(err, 1u);
                 break;
             }
         }
@@ -194,21 +88,34 @@ __device__ bool closest_hit(const ADJ& a, float3 o, float3 d, FFStack& st, ff_hi
     return h.prim >= 0;
 }
 
-__device__ bool occluded(const ADJ& a, const ff_ray& ray, FFStack& st)
+__device__ __noinline__ bool occluded(const FFBvhView bvh, unsigned int* err, const ff_ray ray, FFStack& st)
 {
-    if (!a.bvh.num_nodes) return false;
+    if (!bvh.num_nodes) return false;
     FFRayState r;
     ff_ray_setup(r, make_float3(ray.ox, ray.oy, ray.oz), make_float3(ray.dx, ray.dy, ray.dz), ray.tmin, ray.tmax, true);
     uint2 cur = ff_root_group(r);
     st.reset();
     uint32_t steps = 0;
-    while (!ff_traverse_step<true>(a.bvh, r, cur, st)) {
-        if (++steps > a.bvh.num_nodes + 2 || st.overflow) {
-            atomicAdd(a.err, 1u);
+    while (!ff_traverse_step<true>(bvh, r, cur, st)) {
+        if (++steps > bvh.num_nodes + 2 || st.overflow) {
+            atomicAdd(err, 1u);
             break;
         }
     }
     return r.prim != 0xffffffffu;
+}
+
+__device__ __noinline__ void shade_vertex(const LightCtx& lc, const FFSurf& surf, float3 pos, float3 n, float3 wo,
+                                          float3 wi, float3 sp, uint32_t key, uint32_t L, ShadeOut& sh)
+{
+    sh.c_spec = sh.c_diff = make_float3(0.f, 0.f, 0.f);
+    switch (surf.kind) {
+        case FF_MAT_MIX: shade_mix(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, sp, key, L, sh); break;
+        case FF_MAT_DIFFUSE: shade_diffuse(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+        case FF_MAT_CONDUCTOR: shade_conductor(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+        case FF_MAT_DIELECTRIC: shade_dielectric(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+        default: shade_coat(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+    }
 }
 
 struct VertexRec {
@@ -222,14 +129,23 @@ struct VertexRec {
     float3 L_after;     // radiance added up to and including the vertex's own terms
 };
 
-// One path sample.  MODE 0: primal (returns L_s).  MODE 1: replay with
-// gradients (L_total = L_s of pass 1).  MODE 2: primal that records the
-// vertices into rec (store-all).  ROUGH: roughness gradients requested (a
+// One path sample.  mode 0: primal (returns L_s).  mode 1: replay with
+// gradients (L_total = L_s of pass 1).  mode 2 (STORE_ALL only): primal that
+// records the vertices into rec.  ROUGH: roughness gradients requested (a
 // separate instantiation keeps the albedo/environment kernel's registers).
-template <int MODE, bool ROUGH>
-__device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack& st, float3 L_total, float3 dI,
-                           VertexRec* rec, int* n_rec, uint64_t& rays, uint64_t& atom, uint64_t& atom_r)
+// The mode is a run-time value and the kernel calls this function from one
+// site (a loop over the passes), and the shadow rays are traced from one
+// site (a loop over the three rays), so the kernel holds one copy of the
+// shading code and two of the traversal: with a copy per pass and per ray
+// the code outgrew the instruction cache (instruction-fetch stalls were the
+// largest stall reason).
+template <bool STORE_ALL, bool ROUGH>
+__device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_t pix, uint32_t sample, FFStack& st,
+                                           float3 L_total, float3 dI, VertexRec* rec, int* n_rec, uint64_t& rays,
+                                           uint64_t& atom, uint64_t& atom_r)
 {
+    const bool grad = mode != 0;
+    const bool record = STORE_ALL && mode == 2;
     const uint32_t key = ff_path_key(a.seed, pix, sample);
     float3 o, d;
     gen_camera_ray(a.cam, (int)a.W, (int)a.H, (int)(pix % a.W), (int)(pix / a.W), rand2(key, 0, DIM_CAM_JITTER),
@@ -243,14 +159,14 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
     uint32_t L = 0;
     for (;;) {
         ff_hit hit;
-        const bool found = closest_hit(a, o, d, st, hit);
+        const bool found = closest_hit(a.bvh, a.err, o, d, st, hit);
         ++rays;
         L += 1;
         bool terminate = (L > a.max_depth) || !found;
         if (!found && L == 1) {
             const float3 Le = env_L(a.env, d, true);
             const float3 c = beta * Le;
-            if (MODE != 0 && a.grad_env && a.env.rgb) {
+            if (grad && a.grad_env && a.env.rgb) {
                 float3 dd = d;
                 dd.y = clampf(dd.y, -1.f, 1.f);
                 const float2 uv = spherical_map(dd);
@@ -264,7 +180,7 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
             if (vis_s) lb = lb + sh.c_spec;
             if (vis_d) lb = lb + sh.c_diff;
             if (vis || vis_s || vis_d) {
-                if (MODE != 0 && vis && a.grad_env && lc.is_env && a.env.rgb) {
+                if (grad && vis && a.grad_env && lc.is_env && a.env.rgb) {
                     // NEE term c_nee = coef * Le(wl): d/dLe = beta * coef
                     const float2 uv = spherical_map(nee_dir);
                     atom += scatter_footprint(a.grad_env, footprint(a.env.width, a.env.height, uv.x, uv.y),
@@ -297,20 +213,21 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
         const ff_material& mm = a.mats[t.material];
         const FFSurf surf = resolve_surface(mm, a.tex, tuv);
         const float3 wo = -d;
-        sh.c_spec = sh.c_diff = make_float3(0.f, 0.f, 0.f);
-        switch (surf.kind) {
-            case FF_MAT_MIX: shade_mix(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, sp, key, L, sh); break;
-            case FF_MAT_DIFFUSE: shade_diffuse(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
-            case FF_MAT_CONDUCTOR: shade_conductor(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
-            case FF_MAT_DIELECTRIC: shade_dielectric(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
-            default: shade_coat(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
-        }
+        shade_vertex(lc, surf, pos, n, wo, wi, sp, key, L, sh);
         const float3 lo = pos + n * a.shadow_offset;
         sh.ray_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, sh.r_nee);
-        vis = sh.ray_nee && !occluded(a, sh.r_nee, st);
-        vis_s = sh.ray_spec && !occluded(a, sh.r_spec, st);
-        vis_d = sh.ray_diff && !occluded(a, sh.r_diff, st);
-        rays += (sh.ray_nee ? 1 : 0) + (sh.ray_spec ? 1 : 0) + (sh.ray_diff ? 1 : 0);
+        uint32_t visible = 0;
+#pragma unroll 1
+        for (int k = 0; k < 3; ++k) {
+            const bool want = k == 0 ? sh.ray_nee : (k == 1 ? sh.ray_spec : sh.ray_diff);
+            if (!want) continue;
+            const ff_ray r = k == 0 ? sh.r_nee : (k == 1 ? sh.r_spec : sh.r_diff);
+            if (!occluded(a.bvh, a.err, r, st)) visible |= 1u << k;
+            ++rays;
+        }
+        vis = (visible & 1u) != 0;
+        vis_s = (visible & 2u) != 0;
+        vis_d = (visible & 4u) != 0;
         // d(c_nee)/d(Le) for the environment gradient: c_nee is linear in Le(wi)
         nee_dir = wi;
         nee_dir.y = clampf(nee_dir.y, -1.f, 1.f);
@@ -322,34 +239,32 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
         const bool tex_grad = surf.kind == FF_MAT_DIFFUSE && mm.base_color_tex >= 0 && mm.base_color_tex == a.texture;
         // roughness gradient: GGX surfaces whose roughness comes from the
         // texture (above the 0.01 floor of resolve_surface, where it is flat)
-        const bool rough_grad = ROUGH && MODE != 0 && surf.kind != FF_MAT_DIFFUSE && mm.roughness_tex >= 0 &&
+        const bool rough_grad = ROUGH && grad && surf.kind != FF_MAT_DIFFUSE && mm.roughness_tex >= 0 &&
                                 mm.roughness_tex == a.rough_texture && surf.roughness > 0.01f;
-        RoughDeriv rd;
+        RoughTerms rt;
+        float3 rimm = make_float3(0.f, 0.f, 0.f);
         float3 L_after = Lacc;
         if (rough_grad) {
-            rd = rough_deriv(sh, n, wo, wi, surf.roughness, vis, vis_s, beta);
+            rt = rough_terms(sh, n, wo, wi, surf.roughness);
+            rimm = rough_own(rt, vis, vis_s, beta);
             float3 own = make_float3(0.f, 0.f, 0.f);
             if (vis) own = own + sh.c_nee;
             if (vis_s) own = own + sh.c_spec;
             if (vis_d) own = own + sh.c_diff;
             L_after = Lacc + own * beta;
         }
-        if (MODE == 1 && rough_grad) {
+        if (mode == 1 && rough_grad) {
             const float3 Lgt = L_total - L_after;
-            const float g = dot3(dI, rd.imm + Lgt * rd.dext);
+            const float g = dot3(dI, rimm + Lgt * rt.dext);
             const FFTexView tv = a.tex[a.rough_texture];
             atom_r += scatter_footprint1(a.grad_rough, footprint(tv.width, tv.height, tuv.x, tuv.y), g);
         }
-        if (MODE == 1 && tex_grad) {
-            // L_{>=k} / a_k: everything from this vertex on carries one factor a_k
-            const float3 Lge = L_total - Lacc;
-            const float3 g = make_float3(surf.albedo.x > 0.f ? Lge.x / surf.albedo.x : 0.f,
-                                         surf.albedo.y > 0.f ? Lge.y / surf.albedo.y : 0.f,
-                                         surf.albedo.z > 0.f ? Lge.z / surf.albedo.z : 0.f);
+        if (mode == 1 && tex_grad) {
             const FFTexView tv = a.tex[a.texture];
-            atom += scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, tuv.x, tuv.y), dI * g);
+            atom += scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, tuv.x, tuv.y),
+                                      albedo_grad(L_total - Lacc, surf.albedo, dI));
         }
-        if (MODE == 2 && (tex_grad || rough_grad) && *n_rec < kMaxVerts) {
+        if (record && (tex_grad || rough_grad) && *n_rec < kMaxVerts) {
             VertexRec& r = rec[(*n_rec)++];
             r.a = surf.albedo;
             r.L_before = Lacc;
@@ -358,8 +273,8 @@ __device__ float3 run_path(const ADJ& a, uint32_t pix, uint32_t sample, FFStack&
             r.albedo = tex_grad;
             r.rough = rough_grad;
             if (rough_grad) {
-                r.g_imm = dot3(dI, rd.imm);
-                r.dext = rd.dext;
+                r.g_imm = dot3(dI, rimm);
+                r.dext = rt.dext;
                 r.L_after = L_after;
             }
         }
@@ -389,14 +304,19 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(ADJ a)
         const float3 dI = make_float3(a.d_image[3 * (size_t)pix] * inv_spp, a.d_image[3 * (size_t)pix + 1] * inv_spp,
                                       a.d_image[3 * (size_t)pix + 2] * inv_spp);
         if (!STORE_ALL) {
-            const float3 Ls =
-                run_path<0, ROUGH>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, nullptr, nullptr, rays, atom, atom_r);
-            run_path<1, ROUGH>(a, pix, sample, st, Ls, dI, nullptr, nullptr, rays, atom, atom_r);
+            float3 Ls = make_float3(0.f, 0.f, 0.f);
+#pragma unroll 1
+            for (int pass = 0; pass < 2; ++pass) {
+                const float3 Lp = run_path<false, ROUGH>(a, pass, pix, sample, st, Ls, dI, nullptr, nullptr, rays, atom,
+                                                         atom_r);
+                if (pass == 0) Ls = Lp;
+            }
         } else {
             VertexRec rec[kMaxVerts];
             int n_rec = 0;
             const float3 Ls =
-                run_path<2, ROUGH>(a, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, rec, &n_rec, rays, atom, atom_r);
+                run_path<true, ROUGH>(a, 2, pix, sample, st, make_float3(0.f, 0.f, 0.f), dI, rec, &n_rec, rays, atom,
+                                      atom_r);
             for (int k = 0; k < n_rec; ++k) {
                 const VertexRec& r = rec[k];
                 if (ROUGH && r.rough) {
@@ -405,11 +325,9 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(ADJ a)
                     atom_r += scatter_footprint1(a.grad_rough, footprint(tv.width, tv.height, r.u, r.v), g);
                 }
                 if (!r.albedo) continue;
-                const float3 Lge = Ls - r.L_before;
-                const float3 g = make_float3(r.a.x > 0.f ? Lge.x / r.a.x : 0.f, r.a.y > 0.f ? Lge.y / r.a.y : 0.f,
-                                             r.a.z > 0.f ? Lge.z / r.a.z : 0.f);
                 const FFTexView tv = a.tex[a.texture];
-                atom += scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, r.u, r.v), dI * g);
+                atom += scatter_footprint(a.grad_tex, footprint(tv.width, tv.height, r.u, r.v),
+                                          albedo_grad(Ls - r.L_before, r.a, dI));
             }
         }
     }
@@ -432,7 +350,10 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
                        ff_render_stats* stats)
 {
     FF_REQUIRE(ad->width > 0 && ad->height > 0 && ad->d_image, "adjoint image required");
-    FF_REQUIRE(st->spp > 0 && st->max_depth >= 1 && st->max_depth < (uint32_t)kMaxVerts, "spp > 0, 1 <= max_depth < 16");
+    const bool store_all = (ad->flags & FF_ADJOINT_STORE_ALL) != 0;
+    const bool mega = store_all || (ad->flags & FF_ADJOINT_MEGAKERNEL) != 0;
+    FF_REQUIRE(st->spp > 0 && st->max_depth >= 1, "spp > 0 and max_depth >= 1 required");
+    FF_REQUIRE(!mega || st->max_depth < (uint32_t)kMaxVerts, "the megakernel variants take max_depth < 16");
     FF_REQUIRE(ad->texture < (int32_t)scene->textures.size(), "texture index out of range");
     FF_REQUIRE(ad->texture < 0 || ad->grad_texture, "grad_texture required for a texture gradient");
     FF_REQUIRE(st->light != FF_LIGHT_ALL, "the adjoint needs one light (FF_LIGHT_ALL is not supported)");
@@ -507,13 +428,22 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
     a.err = reinterpret_cast<unsigned int*>(ctr.as<char>() + 8);
     const uint64_t n = (uint64_t)npix * st->spp;
     const uint64_t blocks = (n + kAdjBlock - 1) / kAdjBlock;
-    FF_REQUIRE(blocks < (1ull << 31), "adjoint launch too large");
+    FF_REQUIRE(!mega || blocks < (1ull << 31), "adjoint launch too large");
     FF_CUDA_CHECK(cudaEventRecord(ctx->ev0, stream));
-    const bool store_all = (ad->flags & FF_ADJOINT_STORE_ALL) != 0;
-    if (store_all && rough) k_adjoint<true, true><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
-    else if (store_all) k_adjoint<true, false><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
-    else if (rough) k_adjoint<false, true><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
-    else k_adjoint<false, false><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    if (!mega) {
+        // the default: path replay on the wavefront stages
+        FFAdjointTarget t{ad->width, ad->height, d_image, ad->texture, ntex ? g_tex : nullptr, a.grad_env,
+                          a.rough_texture, a.grad_rough, ctr.as<unsigned long long>() + 2};
+        ff_wavefront_adjoint(ctx, scene, st, t, stats);
+    } else if (store_all && rough) {
+        k_adjoint<true, true><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    } else if (store_all) {
+        k_adjoint<true, false><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    } else if (rough) {
+        k_adjoint<false, true><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    } else {
+        k_adjoint<false, false><<<(unsigned)blocks, kAdjBlock, 0, stream>>>(a);
+    }
     FF_CUDA_CHECK(cudaGetLastError());
     FF_CUDA_CHECK(cudaEventRecord(ctx->ev1, stream));
     if (!dev) {
@@ -532,12 +462,16 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
     if (stats) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-        stats->extension_rays = h_ctr[0];
+        // the megakernel counts every traced ray (both passes) in h_ctr[0];
+        // the wavefront fills extension_rays / shadow_rays itself
+        if (mega) {
+            stats->extension_rays = h_ctr[0];
+            stats->kernel_launches = 1;
+        }
         stats->grad_atomics = h_ctr[2];
         stats->grad_atomics_roughness = h_ctr[3];
         stats->samples = n;
         stats->ms_total = ms;
-        stats->kernel_launches = 1;
     }
 }
 

@@ -116,6 +116,8 @@ ff_status ff_context_destroy(ff_context* ctx)
         ctx->io_hits.release();
         if (ctx->ev0) cudaEventDestroy(ctx->ev0);
         if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+        ff_wavefront_ws_free(ctx->adj_ws);
+        ctx->adj_ws = nullptr;
         if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
         if (prev >= 0) cudaSetDevice(prev);
     }

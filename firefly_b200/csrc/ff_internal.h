@@ -60,6 +60,9 @@ struct DevBuf {
     T* as() const { return reinterpret_cast<T*>(ptr); }
 };
 
+struct FFWavefrontWS;
+void ff_wavefront_ws_free(FFWavefrontWS* ws);
+
 struct ff_context {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -69,6 +72,7 @@ struct ff_context {
     DevBuf counters;      // small scratch of uint32 counters for persistent kernels
     DevBuf io_rays, io_hits;  // staging for host-pointer ff_trace calls
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    FFWavefrontWS* adj_ws = nullptr;   // path pool of ff_render_adjoint, kept between calls
 };
 
 // Per-original-triangle shading attributes (read once per hit).
@@ -120,9 +124,6 @@ struct ff_scene {
     size_t device_bytes() const;
 };
 
-struct FFWavefrontWS;
-void ff_wavefront_ws_free(FFWavefrontWS* ws);
-
 struct ff_film {
     ff_context* ctx = nullptr;
     uint32_t width = 0, height = 0;
@@ -168,6 +169,22 @@ void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d
 void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
                            uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter,
                            unsigned int* err);
+
+// ff_wavefront.cu: the path-replay adjoint on the wavefront stages.  Every
+// pointer is device memory; gradients are added to grad_* (null = not
+// requested); touched[0..1] count the texels the atomics touched.
+struct FFAdjointTarget {
+    uint32_t width, height;
+    const float* d_image;
+    int32_t texture;
+    float* grad_tex;
+    float* grad_env;
+    int32_t rough_texture;
+    float* grad_rough;
+    unsigned long long* touched;
+};
+void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, const FFAdjointTarget& t,
+                          ff_render_stats* stats);
 
 // ff_adjoint.cu
 void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, const ff_adjoint_desc* ad,

@@ -26,15 +26,26 @@
 // and samples j / (w*h) + k*m, and keeps a compensated (Kahan) FP32 sum of its
 // radiance.  The film adds the m slot sums per pixel in a fixed order, so
 // results do not depend on scheduling.  Frames repeat until no slot has work.
+//
+// The same stages run the path-replay adjoint (ff_render_adjoint): in the
+// adjoint instantiations (k_logic<true>, k_shade<K, false, true>) each slot
+// traces a sample once as the primal pass, keeps the sample's radiance L_s,
+// then replays the same sample from its seed.  During the replay k_shade
+// leaves each vertex's derivative terms in the slot, and k_logic, once the
+// vertex's shadow rays are answered, scatters dL/d(texel) of the albedo
+// texture, the roughness texture and the environment map.  The primal
+// instantiations compile none of that code.
 #include <algorithm>
 #include <vector>
 
+#include "ff_adjoint.cuh"
 #include "ff_internal.h"
 #include "ff_paths.cuh"
 
 namespace {
 
 using namespace ffp;
+using namespace ffadj;
 constexpr int kKinds = 5;
 constexpr uint32_t PH_START = 0, PH_FLIGHT = 1, PH_DONE = 2;
 constexpr int32_t SQ_NONE = -1, SQ_BLOCKED = -2;
@@ -95,7 +106,25 @@ struct WF {
     float rough_threshold;
     ffc::Record* queries;
     uint32_t* n_queries;
+    // path-replay adjoint (null / -1 in ff_render)
+    const float* d_image;        // W*H*3: dL/dI of the mean-radiance image
+    float inv_spp;
+    int32_t adj_texture;         // albedo texture receiving gradients, -1 none
+    float* grad_tex;
+    float* grad_env;             // null: no environment gradient
+    int32_t adj_rough;           // roughness texture receiving gradients, -1 none
+    float* grad_rough;           // null: no roughness gradient
+    unsigned long long* touched; // [0] albedo/env texel touches, [1] roughness texel touches
+    uint32_t* pass;              // per slot: 0 primal pass, 1 replay
+    float4* l_total;             // per slot: L_s of the sample being replayed
+    float4* v_albedo;            // per slot, last vertex: albedo, w = V_* flag bits
+    float4* v_nee;               // d c_nee / dr
+    float4* v_spec;              // d c_spec / dr
+    float4* v_dext;              // d log(ext_f) / dr
+    float4* v_coef;              // c_nee / Le(wi): d c_nee / d Le
 };
+// flags of WF::v_albedo.w: which gradients the vertex takes
+constexpr uint32_t V_ALBEDO = 1u, V_ROUGH = 2u, V_ENV = 4u;
 
 __device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
 __device__ __forceinline__ float4 f4(float3 v, float w = 0.f) { return make_float4(v.x, v.y, v.z, w); }
@@ -144,6 +173,10 @@ __device__ void start_sample(const WF& w, uint32_t s, uint32_t sample, bool& pus
     push = true;
 }
 
+// ADJ: the path-replay adjoint's instantiation (the slot's sum holds the
+// current sample's radiance only, in plain FP32 adds as the megakernel
+// adjoint sums it; no film).
+template <bool ADJ>
 __global__ void __launch_bounds__(256) k_logic(WF w)
 {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -151,6 +184,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
     ff_ray ray{};
     int kind = -1;
     bool active = false;
+    uint32_t touched = 0, touched_r = 0;
     if (s < w.P) {
         uint32_t ph = w.phase[s];
         if (ph == PH_START) {
@@ -158,6 +192,10 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             w.next_sample[s] = smp + w.m;
             start_sample(w, s, smp, push_ext, ray);
             w.phase[s] = PH_FLIGHT;
+            if (ADJ) {
+                w.pass[s] = 0;
+                w.acc[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
             active = true;
         } else if (ph == PH_FLIGHT) {
             active = true;
@@ -169,8 +207,31 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             float3 beta = xyz(w.beta[s]);
             float4 acc = w.acc[s], accc = w.acc_c[s];
             bool terminate = (L > w.max_depth) || !found;
+            // adjoint replay: dL/dI of this sample's pixel and the primal pass's L_s
+            const bool replay = ADJ && w.pass[s] != 0u;
+            float3 dI = make_float3(0.f, 0.f, 0.f), Ltot = make_float3(0.f, 0.f, 0.f);
+            if (replay) {
+                const uint32_t pix = slot_pixel(w, s);
+                dI = make_float3(w.d_image[3 * (size_t)pix] * w.inv_spp, w.d_image[3 * (size_t)pix + 1] * w.inv_spp,
+                                 w.d_image[3 * (size_t)pix + 2] * w.inv_spp);
+                Ltot = xyz(w.l_total[s]);
+            }
             // kernel.cu:332-338: environment radiance on a camera-ray miss
-            if (!found && L == 1) kahan_add(acc, accc, beta * env_L(w.env, rd, w.mode == FF_MODE_CORRECTED));
+            if (!found && L == 1) {
+                if (ADJ) {
+                    const float3 c = beta * env_L(w.env, rd, true);
+                    if (replay && w.grad_env && w.env.rgb) {
+                        float3 dd = rd;
+                        dd.y = clampf(dd.y, -1.f, 1.f);
+                        const float2 euv = spherical_map(dd);
+                        touched += scatter_footprint(w.grad_env, footprint(w.env.width, w.env.height, euv.x, euv.y),
+                                                     dI * beta);
+                    }
+                    acc = f4(xyz(acc) + c);
+                } else {
+                    kahan_add(acc, accc, beta * env_L(w.env, rd, w.mode == FF_MODE_CORRECTED));
+                }
+            }
             if (L > 1) {
                 // kernel.cu:357-359: light_brdf * beta when the NEE ray was unoccluded
                 const int4 q = w.sh_q[s];
@@ -183,7 +244,41 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                     if (vis) lb = lb + xyz(w.c_nee[s]);
                     if (vis_s) lb = lb + xyz(w.c_spec[s]);
                     if (vis_d) lb = lb + xyz(w.c_diff[s]);
-                    if (vis || vis_s || vis_d) kahan_add(acc, accc, lb * beta);
+                    if (ADJ) {
+                        if (replay) {
+                            // the previous vertex's gradients, now that its shadow rays are answered
+                            const float4 va = w.v_albedo[s];
+                            const uint32_t flags = __float_as_uint(va.w);
+                            const float2 uv = w.hit_uv[s];
+                            if (flags & V_ALBEDO) {
+                                const FFTexView tv = w.tex[w.adj_texture];
+                                touched += scatter_footprint(w.grad_tex, footprint(tv.width, tv.height, uv.x, uv.y),
+                                                             albedo_grad(Ltot - xyz(acc), xyz(va), dI));
+                            }
+                            if (flags & V_ROUGH) {
+                                RoughTerms rt;
+                                rt.nee = xyz(w.v_nee[s]);
+                                rt.spec = xyz(w.v_spec[s]);
+                                rt.dext = xyz(w.v_dext[s]);
+                                const float3 rimm = rough_own(rt, vis, vis_s, beta);
+                                const float3 L_after = xyz(acc) + lb * beta;
+                                const float g = dot3(dI, rimm + (Ltot - L_after) * rt.dext);
+                                const FFTexView tv = w.tex[w.adj_rough];
+                                touched_r += scatter_footprint1(w.grad_rough, footprint(tv.width, tv.height, uv.x, uv.y), g);
+                            }
+                            if ((flags & V_ENV) && vis) {
+                                // NEE term c_nee = coef * Le(wi): d/dLe = beta * coef
+                                float3 wl = xyz(w.light_wi[s]);
+                                wl.y = clampf(wl.y, -1.f, 1.f);
+                                const float2 euv = spherical_map(wl);
+                                touched += scatter_footprint(w.grad_env, footprint(w.env.width, w.env.height, euv.x, euv.y),
+                                                             dI * beta * xyz(w.v_coef[s]));
+                            }
+                        }
+                        if (vis || vis_s || vis_d) acc = f4(xyz(acc) + lb * beta);
+                    } else if (vis || vis_s || vis_d) {
+                        kahan_add(acc, accc, lb * beta);
+                    }
                 } else if (vis) {
                     // parity: the whole light_brdf, MIS terms included, rides on the NEE ray
                     float3 lb = xyz(w.c_nee[s]);
@@ -211,7 +306,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 }
             }
             w.acc[s] = acc;
-            w.acc_c[s] = accc;
+            if (!ADJ) w.acc_c[s] = accc;
             bool query = false;
             ffc::Record rec;
             if (!terminate) {
@@ -224,7 +319,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 const float wuv = (1.f - u) - v;
                 const float2 uv = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x,
                                               u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
-                if (w.cache_mode && L >= 2) {
+                if (!ADJ && w.cache_mode && L >= 2) {
                     const FFSurf surf = resolve_surface(w.mats[t.material], w.tex, uv);
                     if (is_rough(surf, w.rough_threshold)) {
                         // the cache answers for everything from this vertex on
@@ -248,19 +343,31 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 }
             }
             if (terminate) {
-                w.cnt[s] += 1u;
-                const uint32_t left = w.samples_left[s] - 1u;
-                w.samples_left[s] = left;
-                if (left > 0) {
-                    const uint32_t smp = w.next_sample[s];
-                    w.next_sample[s] = smp + w.m;
-                    start_sample(w, s, smp, push_ext, ray);
+                if (ADJ && !replay) {
+                    // primal pass done: keep L_s and replay the same sample from its seed
+                    w.l_total[s] = acc;
+                    w.pass[s] = 1u;
+                    w.acc[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    start_sample(w, s, w.next_sample[s] - w.m, push_ext, ray);
                 } else {
-                    w.phase[s] = PH_DONE;
-                    active = false;
+                    w.cnt[s] += 1u;
+                    const uint32_t left = w.samples_left[s] - 1u;
+                    w.samples_left[s] = left;
+                    if (ADJ) {
+                        w.pass[s] = 0u;
+                        w.acc[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                    if (left > 0) {
+                        const uint32_t smp = w.next_sample[s];
+                        w.next_sample[s] = smp + w.m;
+                        start_sample(w, s, smp, push_ext, ray);
+                    } else {
+                        w.phase[s] = PH_DONE;
+                        active = false;
+                    }
                 }
             }
-            if (w.cache_mode) {
+            if (!ADJ && w.cache_mode) {
                 const uint32_t qi = warp_append(w.n_queries, query, nullptr);
                 if (query) w.queries[qi] = rec;
             }
@@ -279,11 +386,21 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
     }
     const uint32_t am = __ballot_sync(0xffffffffu, active);
     if ((threadIdx.x & 31u) == 0 && am) atomicAdd(&w.ctr[C_ACTIVE], (uint32_t)__popc(am));
+    if (ADJ) {
+        touched = __reduce_add_sync(0xffffffffu, touched);
+        touched_r = __reduce_add_sync(0xffffffffu, touched_r);
+        if ((threadIdx.x & 31u) == 0) {
+            if (touched) atomicAdd(&w.touched[0], (unsigned long long)touched);
+            if (touched_r) atomicAdd(&w.touched[1], (unsigned long long)touched_r);
+        }
+    }
 }
 
 // SEL: the light is chosen per vertex (FF_LIGHT_ALL); otherwise one light
-// context serves the whole launch (fewer live registers).
-template <int KIND, bool SEL>
+// context serves the whole launch (fewer live registers).  ADJ: the adjoint's
+// instantiation, which also leaves the vertex's derivative terms in the slot
+// during a replay.
+template <int KIND, bool SEL, bool ADJ>
 __global__ void __launch_bounds__(128) k_shade(WF w)
 {
     const uint32_t n = w.ctr[C_MAT + KIND];
@@ -333,6 +450,29 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
             w.ext_cos[s] = o.ext_cos;
             w.ray_o[s] = f4(o.ext_o);
             w.ray_d[s] = f4(o.ext_d);
+            if (ADJ && w.pass[s] != 0u) {
+                const ff_material& mm = w.mats[__float_as_uint(hp.w)];
+                uint32_t flags = 0;
+                if (KIND == FF_MAT_DIFFUSE && w.grad_tex && mm.base_color_tex >= 0 && mm.base_color_tex == w.adj_texture)
+                    flags |= V_ALBEDO;
+                // roughness from the texture, above the 0.01 floor of resolve_surface (flat there)
+                if (KIND != FF_MAT_DIFFUSE && w.grad_rough && mm.roughness_tex >= 0 && mm.roughness_tex == w.adj_rough &&
+                    mat.roughness > 0.01f) {
+                    flags |= V_ROUGH;
+                    const RoughTerms rt = rough_terms(o, n, wo, wi, mat.roughness);
+                    w.v_nee[s] = f4(rt.nee);
+                    w.v_spec[s] = f4(rt.spec);
+                    w.v_dext[s] = f4(rt.dext);
+                }
+                if (w.grad_env && lc.is_env && w.env.rgb) {
+                    // c_nee is linear in Le(wi)
+                    const float3 Li = light_L(lc, wi);
+                    w.v_coef[s] = make_float4(Li.x != 0.f ? o.c_nee.x / Li.x : 0.f, Li.y != 0.f ? o.c_nee.y / Li.y : 0.f,
+                                              Li.z != 0.f ? o.c_nee.z / Li.z : 0.f, 0.f);
+                    flags |= V_ENV;
+                }
+                w.v_albedo[s] = f4(mat.albedo, __uint_as_float(flags));
+            }
         }
         const uint32_t qe = warp_append(&w.ctr[C_EXT], valid, &w.totals[0]);
         if (valid) {
@@ -355,6 +495,7 @@ __global__ void k_init(WF w, uint32_t spp, uint32_t sample_offset)
 {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= w.P) return;
+    if (w.pass) w.pass[s] = 0u;
     const uint32_t lane = s / w.WH;  // which of the m slots of its pixel
     const uint32_t left = lane < spp ? (spp - lane + w.m - 1) / w.m : 0u;
     w.samples_left[s] = left;
@@ -396,6 +537,8 @@ __global__ void k_reset_counters(uint32_t* ctr, unsigned long long* trace_counte
 struct FFWavefrontWS {
     uint32_t P = 0;
     DevBuf buf;
+    DevBuf adj_buf;   // the adjoint's per-slot arrays (allocated by ff_wavefront_adjoint only)
+    uint32_t adj_P = 0;
     WF w{};
     unsigned int* err = nullptr;
     unsigned long long* trace_ctr = nullptr;  // [0] closest, [1] any
@@ -558,20 +701,20 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
         for (int b = 0; b < 4; ++b) {
             k_reset_counters<<<1, 32, 0, stream>>>(w.ctr, ws->trace_ctr);
             mark();
-            k_logic<<<(P + 255) / 256, 256, 0, stream>>>(w);
+            k_logic<false><<<(P + 255) / 256, 256, 0, stream>>>(w);
             mark();
             if (w.lights.light == FF_LIGHT_ALL) {
-                if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX, true><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE, true><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR, true><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC, true><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT, true><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX, true, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE, true, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR, true, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC, true, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT, true, false><<<shade_blocks, 128, 0, stream>>>(w);
             } else {
-                if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX, false, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE, false, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR, false, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC, false, false><<<shade_blocks, 128, 0, stream>>>(w);
+                if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT, false, false><<<shade_blocks, 128, 0, stream>>>(w);
             }
             FF_CUDA_CHECK(cudaGetLastError());
             mark();
@@ -629,5 +772,146 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
         stats->samples = (uint64_t)st->spp * WH;
         stats->frames = frames;
         stats->ms_total = ms;
+    }
+}
+
+namespace {
+
+void adj_setup(FFWavefrontWS* ws, uint32_t P)
+{
+    WF& w = ws->w;
+    if (ws->adj_P != P || !ws->adj_buf.ptr) {
+        ws->adj_buf.release();
+        size_t b = 0;
+        auto add = [&](size_t sz) { b += (sz * P + 255) & ~size_t(255); };
+        add(4);
+        for (int k = 0; k < 6; ++k) add(16);
+        add(8);
+        ws->adj_buf.alloc(b);
+        ws->adj_P = P;
+    }
+    char* p = ws->adj_buf.as<char>();
+    w.pass = carve<uint32_t>(p, P);
+    w.l_total = carve<float4>(p, P);
+    w.v_albedo = carve<float4>(p, P);
+    w.v_nee = carve<float4>(p, P);
+    w.v_spec = carve<float4>(p, P);
+    w.v_dext = carve<float4>(p, P);
+    w.v_coef = carve<float4>(p, P);
+}
+
+template <bool SEL, bool ADJ>
+void launch_shade(const WF& w, const bool* kind_used, int blocks, cudaStream_t stream)
+{
+    if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
+    if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
+    if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
+    if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
+    if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
+}
+
+}  // namespace
+
+// The path-replay adjoint on the wavefront stages: every slot traces a
+// sample as the primal pass, then replays it from its seed; gradients are
+// scattered during the replay (k_logic<true>, k_shade<K, false, true>).
+// The caller records the timing events, stages host buffers and reads the
+// counters; this function leaves the stream unsynchronised except for the
+// frame-loop checks.
+void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_settings* st, const FFAdjointTarget& t,
+                          ff_render_stats* stats)
+{
+    FF_REQUIRE(st->max_depth >= 1 && st->max_depth <= 64, "max_depth must be in [1, 64]");
+    FF_REQUIRE(st->light != FF_LIGHT_ALL, "the adjoint needs one light (FF_LIGHT_ALL is not supported)");
+    cudaStream_t stream = ctx->stream;
+    const uint32_t WH = t.width * t.height;
+    const uint64_t target = st->max_paths ? st->max_paths : (1u << 21);
+    uint32_t m = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(st->spp, target / WH));
+    while ((uint64_t)m * WH > (1ull << 31)) --m;
+    const uint32_t P = m * WH;
+    if (!ctx->adj_ws) ctx->adj_ws = new FFWavefrontWS();
+    FFWavefrontWS* ws = ctx->adj_ws;
+    ws_setup(ws, P);
+    adj_setup(ws, P);
+    WF& w = ws->w;
+    w.WH = WH;
+    w.W = t.width;
+    w.H = t.height;
+    w.m = m;
+    w.seed = st->seed;
+    w.max_depth = st->max_depth;
+    w.rr_depth = st->rr_depth;
+    w.mode = FF_MODE_CORRECTED;
+    w.light = st->light;
+    w.shadow_offset = st->shadow_offset > 0.f ? st->shadow_offset : 0.001f;
+    w.shade = scene->shade.as<FFShadeTri>();
+    w.mats = scene->materials.as<ff_material>();
+    w.area = scene->area_lights.as<ff_area_light>();
+    w.n_area = scene->num_area_lights;
+    w.tex = scene->tex_table.as<FFTexView>();
+    w.env = ff_env_view(scene);
+    w.lights = ff_light_set(scene, st->light, FF_MODE_CORRECTED);
+    w.cam = scene->camera;
+    w.cache_mode = 0u;
+    w.rough_threshold = 0.f;
+    w.queries = nullptr;
+    w.n_queries = nullptr;
+    w.d_image = t.d_image;
+    w.inv_spp = 1.f / (float)st->spp;
+    w.adj_texture = t.texture;
+    w.grad_tex = t.grad_tex;
+    w.grad_env = t.grad_env;
+    w.adj_rough = t.rough_texture;
+    w.grad_rough = t.grad_rough;
+    w.touched = t.touched;
+    const FFBvhView bvh = scene->view();
+
+    std::vector<ff_material> mats(scene->num_materials);
+    FF_CUDA_CHECK(cudaMemcpyAsync(mats.data(), scene->materials.ptr, sizeof(ff_material) * mats.size(),
+                                  cudaMemcpyDeviceToHost, stream));
+    FF_CUDA_CHECK(cudaMemsetAsync(w.totals, 0, 8 * sizeof(unsigned long long), stream));
+    FF_CUDA_CHECK(cudaMemsetAsync(ws->err, 0, sizeof(unsigned int), stream));
+    FF_CUDA_CHECK(cudaStreamSynchronize(stream));
+    bool kind_used[kKinds] = {false, false, false, false, false};
+    for (auto& mt : mats) kind_used[mt.kind] = true;
+    int n_kinds = 0;
+    for (int k = 0; k < kKinds; ++k) n_kinds += kind_used[k] ? 1 : 0;
+
+    k_init<<<(P + 255) / 256, 256, 0, stream>>>(w, st->spp, st->sample_offset);
+    FF_CUDA_CHECK(cudaGetLastError());
+    const int shade_blocks = ctx->num_sms * 8;
+    uint32_t frames = 0;
+    uint32_t active = 1;
+    if (!ws->h_active) FF_CUDA_CHECK(cudaMallocHost(&ws->h_active, sizeof(uint32_t)));
+    uint32_t* h_active = ws->h_active;
+    // two passes per sample
+    const uint32_t max_frames = 2 * (st->spp + 1) * (st->max_depth + 2) + 8;
+    while (active && frames < max_frames) {
+        for (int b = 0; b < 4; ++b) {
+            k_reset_counters<<<1, 32, 0, stream>>>(w.ctr, ws->trace_ctr);
+            k_logic<true><<<(P + 255) / 256, 256, 0, stream>>>(w);
+            launch_shade<false, true>(w, kind_used, shade_blocks, stream);
+            FF_CUDA_CHECK(cudaGetLastError());
+            ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err);
+            ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, w.sh_hits, true, ws->trace_ctr + 1,
+                                  ws->err);
+            ++frames;
+        }
+        FF_CUDA_CHECK(cudaMemcpyAsync(h_active, w.ctr + C_ACTIVE, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        FF_CUDA_CHECK(cudaStreamSynchronize(stream));
+        active = *h_active;
+    }
+    if (active) throw FFError{FF_ERR_INTERNAL, "wavefront adjoint did not finish within its frame bound"};
+    unsigned long long totals[2] = {0, 0};
+    unsigned int err = 0;
+    FF_CUDA_CHECK(cudaMemcpyAsync(totals, w.totals, sizeof(totals), cudaMemcpyDeviceToHost, stream));
+    FF_CUDA_CHECK(cudaMemcpyAsync(&err, ws->err, sizeof(err), cudaMemcpyDeviceToHost, stream));
+    FF_CUDA_CHECK(cudaStreamSynchronize(stream));
+    if (err) throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
+    if (stats) {
+        stats->kernel_launches = frames * (3u + (uint32_t)n_kinds) + 1u;
+        stats->extension_rays = totals[0];
+        stats->shadow_rays = totals[1];
+        stats->frames = frames;
     }
 }

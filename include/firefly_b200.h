@@ -308,6 +308,8 @@ FF_API ff_status ff_render(ff_context* ctx, ff_scene* scene, const ff_render_set
 /* -------------------------------------------------------------- adjoint */
 
 #define FF_ADJOINT_STORE_ALL 4u   /* ff_adjoint_desc.flags: store-all-vertices reference variant */
+#define FF_ADJOINT_MEGAKERNEL 16u /* ff_adjoint_desc.flags: one-thread-per-sample replay (cross-check) instead of
+                                     the wavefront replay */
 #define FF_ENV_KEEP_TABLES   8u   /* ff_scene_set_environment: keep the importance tables */
 
 /* Gradient request of ff_render_adjoint.  d_image is dL/dI for the mean
