@@ -160,7 +160,7 @@ class dScene:
                        grad_env=None, spp: int = 1, max_depth: int = 3, rr_depth: int = 3, seed: int = 0,
                        light: int = -1, sample_offset: int = 0, shadow_offset: float = 0.001,
                        store_all: bool = False, roughness_texture: int = -1, grad_roughness=None,
-                       megakernel: bool = False) -> dict:
+                       megakernel: bool = False, profile: bool = False) -> dict:
         """Path-replay adjoint of PathTracer.draw(mode=FF_MODE_CORRECTED) with
         the same settings: adds dL/d(texture texels) to grad_texture,
         dL/d(env texels) to grad_env and dL/d(roughness texels, channel 0) to
@@ -168,11 +168,12 @@ class dScene:
         d_image = dL/dI of the mean-radiance image (height, width, 3).
         The replay runs on the wavefront stages; megakernel=True runs the
         one-thread-per-sample replay instead, store_all=True the store-all
-        reference variant."""
+        reference variant.  profile=True times the wavefront stages
+        (ms_logic, ms_shade, ms_trace_extension, ms_trace_shadow)."""
         dimg = np.ascontiguousarray(d_image, np.float32)
         s = A.ff_render_settings(spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed,
                                  mode=A.FF_MODE_CORRECTED, light=light, max_paths=0, sample_offset=sample_offset,
-                                 flags=0, shadow_offset=shadow_offset)
+                                 flags=A.FF_RENDER_PROFILE if profile else 0, shadow_offset=shadow_offset)
         d = A.ff_adjoint_desc(width=width, height=height, d_image=dimg.ctypes.data, texture=texture,
                               grad_texture=None if grad_texture is None else grad_texture.ctypes.data,
                               grad_env=None if grad_env is None else grad_env.ctypes.data,

@@ -205,7 +205,8 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             const bool found = hit.prim >= 0;
             const float3 ro = xyz(w.ray_o[s]), rd = xyz(w.ray_d[s]);
             float3 beta = xyz(w.beta[s]);
-            float4 acc = w.acc[s], accc = w.acc_c[s];
+            float4 acc = w.acc[s];
+            float4 accc = ADJ ? make_float4(0.f, 0.f, 0.f, 0.f) : w.acc_c[s];   // no compensation in the adjoint
             bool terminate = (L > w.max_depth) || !found;
             // adjoint replay: dL/dI of this sample's pixel and the primal pass's L_s
             const bool replay = ADJ && w.pass[s] != 0u;
@@ -279,7 +280,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                     } else if (vis || vis_s || vis_d) {
                         kahan_add(acc, accc, lb * beta);
                     }
-                } else if (vis) {
+                } else if (!ADJ && vis) {
                     // parity: the whole light_brdf, MIS terms included, rides on the NEE ray
                     float3 lb = xyz(w.c_nee[s]);
                     if (vis_s) lb = lb + xyz(w.c_spec[s]);
@@ -880,6 +881,16 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
     k_init<<<(P + 255) / 256, 256, 0, stream>>>(w, st->spp, st->sample_offset);
     FF_CUDA_CHECK(cudaGetLastError());
     const int shade_blocks = ctx->num_sms * 8;
+    // optional per-stage timing, as in ff_wavefront_render
+    const bool profile = stats && (st->flags & FF_RENDER_PROFILE);
+    std::vector<cudaEvent_t> evs;
+    auto mark = [&](void) {
+        if (!profile) return;
+        cudaEvent_t e;
+        FF_CUDA_CHECK(cudaEventCreate(&e));
+        FF_CUDA_CHECK(cudaEventRecord(e, stream));
+        evs.push_back(e);
+    };
     uint32_t frames = 0;
     uint32_t active = 1;
     if (!ws->h_active) FF_CUDA_CHECK(cudaMallocHost(&ws->h_active, sizeof(uint32_t)));
@@ -889,12 +900,17 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
     while (active && frames < max_frames) {
         for (int b = 0; b < 4; ++b) {
             k_reset_counters<<<1, 32, 0, stream>>>(w.ctr, ws->trace_ctr);
+            mark();
             k_logic<true><<<(P + 255) / 256, 256, 0, stream>>>(w);
+            mark();
             launch_shade<false, true>(w, kind_used, shade_blocks, stream);
             FF_CUDA_CHECK(cudaGetLastError());
+            mark();
             ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err);
+            mark();
             ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, w.sh_hits, true, ws->trace_ctr + 1,
                                   ws->err);
+            mark();
             ++frames;
         }
         FF_CUDA_CHECK(cudaMemcpyAsync(h_active, w.ctr + C_ACTIVE, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
@@ -908,6 +924,22 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
     FF_CUDA_CHECK(cudaMemcpyAsync(&err, ws->err, sizeof(err), cudaMemcpyDeviceToHost, stream));
     FF_CUDA_CHECK(cudaStreamSynchronize(stream));
     if (err) throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
+    if (profile) {
+        // 5 marks per frame: logic | shade | trace extension | trace shadow
+        float t[4] = {0.f, 0.f, 0.f, 0.f};
+        for (size_t f = 0; f + 5 <= evs.size(); f += 5) {
+            for (int k = 0; k < 4; ++k) {
+                float x = 0.f;
+                cudaEventElapsedTime(&x, evs[f + k], evs[f + k + 1]);
+                t[k] += x;
+            }
+        }
+        stats->ms_logic = t[0];
+        stats->ms_shade = t[1];
+        stats->ms_trace_extension = t[2];
+        stats->ms_trace_shadow = t[3];
+    }
+    for (auto e : evs) cudaEventDestroy(e);
     if (stats) {
         stats->kernel_launches = frames * (3u + (uint32_t)n_kinds) + 1u;
         stats->extension_rays = totals[0];
