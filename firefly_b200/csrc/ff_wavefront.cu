@@ -50,6 +50,13 @@ constexpr int kKinds = 5;
 constexpr uint32_t PH_START = 0, PH_FLIGHT = 1, PH_DONE = 2;
 constexpr int32_t SQ_NONE = -1, SQ_BLOCKED = -2;
 
+// Path-pool size when ff_render_settings.max_paths is 0: m slots per pixel,
+// m = min(spp, this / (w*h)), at least 1.  Measured on the 1.3M-triangle
+// 1080p scene at 64 spp: 2M slots 419 ms, 4M 360 ms, 8M 347 ms, 16M 342 ms
+// per step (bigger queues hide the traversal's latency better and need
+// fewer frames); 8M slots hold about 3.6 GB of path state.
+constexpr uint64_t kDefaultPoolTarget = 1ull << 23;
+
 // Counter words of one frame (zeroed at the start of each frame).
 enum { C_EXT = 0, C_SH = 1, C_MAT = 2, C_ACTIVE = 2 + kKinds, C_WORDS = 8 + kKinds };
 
@@ -630,7 +637,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     ff_check_light(scene, st->light, st->mode);
     cudaStream_t stream = ctx->stream;
     const uint32_t WH = film->width * film->height;
-    const uint64_t target = st->max_paths ? st->max_paths : (1u << 21);
+    const uint64_t target = st->max_paths ? st->max_paths : kDefaultPoolTarget;
     uint32_t m = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(st->spp, target / WH));
     while ((uint64_t)m * WH > (1ull << 31)) --m;
     const uint32_t P = m * WH;
@@ -826,7 +833,7 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
     FF_REQUIRE(st->light != FF_LIGHT_ALL, "the adjoint needs one light (FF_LIGHT_ALL is not supported)");
     cudaStream_t stream = ctx->stream;
     const uint32_t WH = t.width * t.height;
-    const uint64_t target = st->max_paths ? st->max_paths : (1u << 21);
+    const uint64_t target = st->max_paths ? st->max_paths : kDefaultPoolTarget;
     uint32_t m = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(st->spp, target / WH));
     while ((uint64_t)m * WH > (1ull << 31)) --m;
     const uint32_t P = m * WH;
