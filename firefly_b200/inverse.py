@@ -18,6 +18,7 @@ import time
 
 from . import _abi as A
 from . import lib
+from . import multigpu
 
 
 def _p(t):
@@ -26,7 +27,8 @@ def _p(t):
 
 def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, lr: float = 1e-2,
              max_depth: int = 3, rr_depth: int = 3, seed: int = 0, light: int = -1, texture: int = 0,
-             lr_env: float | None = None, lr_decay: float = 1.0, callback=None) -> dict:
+             lr_env: float | None = None, lr_decay: float = 1.0, callback=None, rank: int = 0, world: int = 1,
+             group=None) -> dict:
     """target: device float32 [h, w, 3]; albedo [th, tw, 3] and env [eh, ew, 3]:
     device float32 tensors updated in place (env only when its learning rate,
     lr_env, defaulting to lr, is non-zero).  Both rates fall geometrically by
@@ -34,6 +36,10 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
     size of the rate whatever the gradient's signal-to-noise ratio, so with a
     constant rate the texels that few samples see keep drifting by about the
     rate per step once their mean gradient is lost in the Monte Carlo noise.
+    With world > 1 (torch.distributed initialised, one process per GPU), rank
+    `rank` renders and replays samples [rank * spp, (rank + 1) * spp) of every
+    step; the films are summed and the gradients averaged across the ranks
+    (firefly_b200.multigpu), so every rank takes the same optimiser step.
     Returns timings and the loss history."""
     lr_env = lr if lr_env is None else lr_env
     import torch
@@ -56,14 +62,17 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
         if rc:
             raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
         tracer.clear_buffer()
+        off = multigpu.inverse_sample_offset(rank, spp)
         st = tracer.draw(ds, spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed + it, light=light,
-                         mode=A.FF_MODE_CORRECTED)
+                         mode=A.FF_MODE_CORRECTED, sample_offset=off)
         t_primal += st["ms_total"]
         launches += st["kernel_launches"]
         rc = L.ff_film_read(tracer.film, _p(rgba), _p(cnt), A.FF_MEM_DEVICE)
         if rc:
             raise RuntimeError(L.ff_last_error_message(ctx.handle).decode())
         ctx.sync()
+        if world > 1:
+            multigpu.allreduce_film(rgba, cnt, group=group)
         img = rgba[..., :3] / cnt.clamp(min=1)[..., None].float()
         diff = img - target
         losses.append(float(0.5 * (diff * diff).mean()))
@@ -72,7 +81,7 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
         g_env.zero_()
         torch.cuda.synchronize(dev)
         s = A.ff_render_settings(spp=spp, max_depth=max_depth, rr_depth=rr_depth, seed=seed + it + 0x40000000,
-                                 mode=A.FF_MODE_CORRECTED, light=light, max_paths=0, sample_offset=0, flags=0,
+                                 mode=A.FF_MODE_CORRECTED, light=light, max_paths=0, sample_offset=off, flags=0,
                                  shadow_offset=0.001)
         d = A.ff_adjoint_desc(width=w, height=h, d_image=d_image.data_ptr(), texture=texture,
                               grad_texture=g_tex.data_ptr(), grad_env=g_env.data_ptr(), flags=A.FF_MEM_DEVICE)
@@ -84,6 +93,10 @@ def optimize(ds, tracer, target, albedo, env, steps: int = 200, spp: int = 16, l
         adj_samples += ast.samples
         atomics += ast.grad_atomics
         launches += ast.kernel_launches + 2
+        if world > 1:
+            ctx.sync()
+            multigpu.allreduce_mean([g_tex, g_env], group=group)
+            torch.cuda.synchronize(dev)
         fall = lr_decay ** (it / max(1, steps - 1))
         for prm, g, m, v, hi, rate in ((albedo, g_tex, m_tex, v_tex, 1.0, lr), (env, g_env, m_env, v_env, 1e6, lr_env)):
             if rate == 0:
