@@ -55,6 +55,19 @@ RAY_BYTES, HIT_BYTES = 32, 16
 # vertex record (albedo + flags, uv, env coefficient, light direction: 56).
 # Primal ~410 B, replay ~490 B: 450 B on average.
 ADJ_LOGIC_BYTES_PER_HIT = 450
+# k_logic in ff_render, per consumed extension hit of a continuing path:
+# reads 296 B (slot words 16, hit 16, ray 32, throughput 16, sum and
+# compensation 32, shadow-queue indices 16 and ~1.5 shadow hits 24, light
+# terms 48, ext_f / pdf / cos 20, shading record 76), writes 144 B (sum and
+# compensation 32, next vertex 112).
+RENDER_LOGIC_BYTES_PER_HIT = 440
+# k_shade, per shaded vertex: reads the vertex (position, uv, normal,
+# direction, light sample, key, depth, queue entry: 100 B), writes the light
+# terms (48), ext_f / pdf / cos (20), the continuation ray into the slot (32)
+# and the extension queue (36), ~2.5 shadow rays (80) and their queue
+# indices (16): 332 B.  Environment and material lookups are L2 gathers and
+# not counted.
+RENDER_SHADE_BYTES_PER_VERTEX = 332
 RENDER = dict(width=1920, height=1080, spp=64, max_depth=8, rr_depth=3)
 
 
@@ -214,7 +227,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    rates = []
+    rates, secs = [], []
     kind = desc = None
     if args.workload == "render":
         scn = render_scene()
@@ -223,20 +236,24 @@ def run_reference(args):
             if r is None:
                 print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libffref.so was not built"}))
                 return 0
-            rate, kind, desc, _ = r
+            rate, kind, desc, sec = r
             if i >= args.warmup:
                 rates.append(rate)
+                secs.append(sec)
         workload, cfg = RENDER_WORKLOAD, dict(RENDER)
     else:
         _, batches = trace_batches(RAYS_PER_SET, 0)
         for i in range(args.warmup + args.steps):
-            rate, kind, desc, _ = cpu_trace_rate(batches, target_s=args.ref_step_s, threads=threads)
+            rate, kind, desc, sec = cpu_trace_rate(batches, target_s=args.ref_step_s, threads=threads)
             if i >= args.warmup:
                 rates.append(rate)
+                secs.append(sec)
         workload, cfg = TRACE_WORKLOAD, {"rays_per_step": 4 * RAYS_PER_SET}
     value = statistics.median(rates)
     line = {"metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup,
+            # one step = one bounded sample of the workload (see cpu_baseline.sample)
+            "ms_per_step": round(1e3 * statistics.median(secs), 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": workload, **cfg},
             "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": kind,
@@ -523,12 +540,23 @@ def run_render(args, ws, rank, local, dist):
         tds.close()
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        # dominant kernel: the shadow-ray trace (k_trace<any>) or the extension trace
-        stage = {"k_trace<any> (shadow queue)": (prof["ms_trace_shadow"], prof["shadow_rays"]),
-                 "k_trace<closest> (extension queue)": (prof["ms_trace_extension"], prof["extension_rays"])}
+        # dominant stage by device time (events of the profiled step), with the
+        # algorithmic bytes of one launch sequence: 48 B per traced ray (ray in,
+        # hit out), or the slot-state bytes above per consumed hit / shaded vertex
+        vertices = max(0, prof["extension_rays"] - prof["samples"])
+        stage = {"k_trace<any> (shadow queue)": (prof["ms_trace_shadow"], prof["shadow_rays"] * (RAY_BYTES + HIT_BYTES),
+                                                 "48 B per shadow ray"),
+                 "k_trace<closest> (extension queue)": (prof["ms_trace_extension"],
+                                                        prof["extension_rays"] * (RAY_BYTES + HIT_BYTES),
+                                                        "48 B per extension ray"),
+                 "k_logic": (prof["ms_logic"], prof["extension_rays"] * RENDER_LOGIC_BYTES_PER_HIT,
+                             f"{RENDER_LOGIC_BYTES_PER_HIT} B of slot state per consumed extension hit"),
+                 "k_shade (all kinds)": (prof["ms_shade"], vertices * RENDER_SHADE_BYTES_PER_VERTEX,
+                                         f"{RENDER_SHADE_BYTES_PER_VERTEX} B of slot state and queue entries per "
+                                         "shaded vertex")}
         dom = max(stage, key=lambda k: stage[k][0])
-        dms, drays = stage[dom]
-        achieved = drays * (RAY_BYTES + HIT_BYTES) / (dms / 1e3) / 1e9
+        dms, dbytes, dnote = stage[dom]
+        achieved = dbytes / (dms / 1e3) / 1e9
         cpu = None
         if not args.no_cpu:
             r = cpu_render_rate(scn, target_s=args.cpu_s, threads=os.cpu_count() or 1)
@@ -551,7 +579,9 @@ def run_render(args, ws, rank, local, dist):
                        "image_finite": finite, "relmse_vs_16k_spp": conv, "trace_micro": trace},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 5), "traffic": None, "peak_source": peak_kind,
-                         "bytes_per_ray": RAY_BYTES + HIT_BYTES},
+                         "algorithmic_bytes": dnote,
+                         "stages": {k: {"ms": round(v[0], 2), "achieved_gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1)
+                                        if v[0] > 0 else None} for k, v in stage.items()}},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 80,
                     "d2h_bytes_per_step": int(W * H * (16 + 4))},
