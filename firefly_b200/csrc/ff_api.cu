@@ -57,13 +57,14 @@ void upload(DevBuf& b, const void* host, size_t bytes, cudaStream_t st)
 size_t ff_scene::device_bytes() const
 {
     size_t total = nodes.bytes + tris.bytes + shade.bytes + materials.bytes + tex_table.bytes + area_lights.bytes + dir_lights.bytes +
-                   env.rgb.bytes + env.marginal.bytes + env.conditional.bytes + env.pdf.bytes + env.denom.bytes;
+                   env.rgb.bytes + env.marginal.bytes + env.conditional.bytes + env.pdf.bytes + env.denom.bytes + env.texel4.bytes;
     for (auto* t : textures) total += t->bytes;
     return total;
 }
 
 // Defined in ff_envmap.cu and ff_scene.cu.
 void ff_build_env_tables(ff_context* ctx, ff_scene* s);
+void ff_env_pack(ff_context* ctx, ff_scene* s);
 void ff_build_shading(ff_context* ctx, ff_scene* s, const ff_scene_desc* d, const float3* d_pos,
                       const uint3* d_idx);
 
@@ -322,6 +323,7 @@ extern "C" ff_status ff_scene_set_environment(ff_scene* s, const float* rgb, uin
                                       (flags & FF_MEM_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                       ctx->stream));
         if (!(flags & FF_ENV_KEEP_TABLES)) ff_build_env_tables(ctx, s);
+        else ff_env_pack(ctx, s);
         FF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
     });
 }

@@ -119,7 +119,30 @@ __global__ void __launch_bounds__(kEnvBlock) k_env_cond(const float* __restrict_
     }
 }
 
+// (r, g, b, pdf) per texel for the path kernels (FFEnvView::texel4).
+__global__ void k_env_pack(const float3* __restrict__ rgb, const float* __restrict__ pdf, size_t n,
+                           float4* __restrict__ out)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float3 c = rgb[i];
+    out[i] = make_float4(c.x, c.y, c.z, pdf[i]);
+}
+
 }  // namespace
+
+// Repack after the texels or the pdf changed (ff_scene_set_environment keeps
+// the tables when asked to: the new texels with the old pdf).
+void ff_env_pack(ff_context* ctx, ff_scene* s)
+{
+    FFEnvLight& e = s->env;
+    const size_t n = (size_t)e.width * e.height;
+    if (!n || !e.pdf.ptr) return;
+    e.texel4.alloc(sizeof(float4) * n);
+    k_env_pack<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(e.rgb.as<float3>(), e.pdf.as<float>(), n,
+                                                                     e.texel4.as<float4>());
+    FF_CUDA_CHECK(cudaGetLastError());
+}
 
 void ff_build_env_tables(ff_context* ctx, ff_scene* s)
 {
@@ -140,6 +163,7 @@ void ff_build_env_tables(ff_context* ctx, ff_scene* s)
     k_env_cond<<<h, kEnvBlock, 0, st>>>(lum.as<float>(), w, h, mp.as<double>(), e.denom.as<double>(),
                                         e.conditional.as<double>(), e.pdf.as<float>());
     FF_CUDA_CHECK(cudaGetLastError());
+    ff_env_pack(ctx, s);
     FF_CUDA_CHECK(cudaStreamSynchronize(st));
 }
 

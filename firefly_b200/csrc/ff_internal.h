@@ -91,6 +91,7 @@ struct FFEnvLight {
     DevBuf conditional;   // double[height*width]
     DevBuf pdf;           // float[height*width]
     DevBuf denom;         // double
+    DevBuf texel4;        // float4[height*width]: rgb and pdf packed for the path kernels
 };
 
 struct ff_scene {

@@ -152,6 +152,7 @@ FFEnvView ff_env_view(const ff_scene* s)
     e.height = s->env.height;
     e.color = s->env.color;
     e.radius = 10000.f;   // dEnvironmentLight.cu:14
+    e.texel4 = s->env.texel4.as<float4>();
     return e;
 }
 

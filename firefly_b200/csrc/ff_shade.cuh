@@ -290,7 +290,8 @@ FF_D float brdf_pdf(const FFSurf& m, float3 n, float3 wi, float3 wo)
 
 // ----------------------------------------------------------------- lights
 // Environment light with importance tables (dEnvironmentLight.cu).
-FF_D float3 tex_bilinear(const float3* texels, int w, int h, float u, float v);
+template <class T>
+FF_D float3 tex_bilinear(const T* texels, int w, int h, float u, float v);
 
 FF_D FFSurf resolve_surface(const ff_material& m, const FFTexView* tex, float2 uv)
 {
@@ -319,12 +320,24 @@ struct FFEnvView {
     int width, height;
     float3 color;            // constant colour when rgb == nullptr
     float radius;            // 10000 (dEnvironmentLight.cu:14)
+    // the same texels and pdf packed as (r, g, b, pdf), or nullptr: one
+    // aligned 16-B load per texel, a bilinear pair in one 32-B sector, and
+    // the pdf texel of a direction among the four texels of its bilinear
+    // lookup (shared cache lines for light_L + light_pdf of one direction)
+    const float4* texel4;
 };
 
 // tex2DLod<float4> with normalised coordinates, wrap addressing and linear
 // filtering: x_B = x*W - 0.5, i = floor(x_B), alpha = frac(x_B) with 8
 // fractional bits, as the CUDA Programming Guide specifies texture filtering.
-FF_D float3 tex_bilinear(const float3* texels, int w, int h, float u, float v)
+FF_D float3 texel3(const float3* t, int i) { return t[i]; }
+FF_D float3 texel3(const float4* t, int i)
+{
+    const float4 v = t[i];
+    return make_float3(v.x, v.y, v.z);
+}
+template <class T>
+FF_D float3 tex_bilinear(const T* texels, int w, int h, float u, float v)
 {
     float xb = u * (float)w - 0.5f;
     float yb = v * (float)h - 0.5f;
@@ -339,8 +352,8 @@ FF_D float3 tex_bilinear(const float3* texels, int w, int h, float u, float v)
     int y0 = iy % h;
     y0 = y0 < 0 ? y0 + h : y0;
     int y1 = (y0 + 1 == h) ? 0 : y0 + 1;
-    float3 t00 = texels[y0 * w + x0], t10 = texels[y0 * w + x1];
-    float3 t01 = texels[y1 * w + x0], t11 = texels[y1 * w + x1];
+    float3 t00 = texel3(texels, y0 * w + x0), t10 = texel3(texels, y0 * w + x1);
+    float3 t01 = texel3(texels, y1 * w + x0), t11 = texel3(texels, y1 * w + x1);
     float w00 = (1.f - ax) * (1.f - ay), w10 = ax * (1.f - ay), w01 = (1.f - ax) * ay, w11 = ax * ay;
     return make_float3(w00 * t00.x + w10 * t10.x + w01 * t01.x + w11 * t11.x,
                        w00 * t00.y + w10 * t10.y + w01 * t01.y + w11 * t11.y,
@@ -368,6 +381,7 @@ FF_D float3 env_L(const FFEnvView& e, float3 wi, bool corrected = false)
     if (!e.rgb) return e.color;
     if (corrected) wi.y = clampf(wi.y, -1.f, 1.f);
     float2 uv = spherical_map(wi);
+    if (e.texel4) return tex_bilinear(e.texel4, e.width, e.height, uv.x, uv.y);
     return tex_bilinear(e.rgb, e.width, e.height, uv.x, uv.y);
 }
 
@@ -414,7 +428,8 @@ FF_D float env_pdf_corrected(const FFEnvView& e, float3 wi)
     x = x < 0 ? 0 : (x >= e.width ? e.width - 1 : x);
     y = y < 0 ? 0 : (y >= e.height ? e.height - 1 : y);
     const float cl = sqrtf(hmax(0.f, 1.f - wi.y * wi.y));
-    return cl > 0.f ? e.pdf[(size_t)y * e.width + x] / cl : 0.f;
+    const size_t i = (size_t)y * e.width + x;
+    return cl > 0.f ? (e.texel4 ? e.texel4[i].w : e.pdf[i]) / cl : 0.f;
 }
 
 // get_pdf(isect, wi) (dEnvironmentLight.cu:83-103): pdf texel over sin(acos(wi.z))
@@ -423,7 +438,11 @@ FF_D float env_pdf(const FFEnvView& e, float3 wi)
     float2 uv = spherical_map(wi);
     int x = (int)(uv.x * (float)(e.width - 1));
     int y = (int)(uv.y * (float)(e.height - 1));
-    float p = (x >= 0 && y >= 0 && x < e.width && y < e.height) ? e.pdf[(size_t)y * e.width + x] : 0.f;
+    float p = 0.f;
+    if (x >= 0 && y >= 0 && x < e.width && y < e.height) {
+        const size_t i = (size_t)y * e.width + x;
+        p = e.texel4 ? e.texel4[i].w : e.pdf[i];
+    }
     return p / sinf(acosf(clampf(wi.z, -1.f, 1.f)));
 }
 
