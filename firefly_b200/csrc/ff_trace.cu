@@ -17,11 +17,16 @@ constexpr int kTraceBlock = 128;
 // Refill when at least this many lanes of the warp are idle.
 constexpr int kRefillIdle = 8;
 
-template <bool ANY>
+// Output: hits[ray] for every ray, or, with tags (the wavefront's queues),
+// per the ray's tag: a closest hit goes to hits[tag] (tag = the path slot, so
+// the next stage reads its hit in slot order without the queue index), an
+// any-hit answer to occ[tag] (1 occluded, 0 clear; tag = 4 * slot + shadow
+// ray index, so the next stage reads one 4-byte word of answers per slot).
+template <bool ANY, bool TAGGED>
 __global__ void __launch_bounds__(kTraceBlock, 8)
     k_trace(FFBvhView bvh, const ff_ray* __restrict__ rays, ff_hit* __restrict__ hits, uint64_t n,
             unsigned long long* __restrict__ counter, unsigned int* __restrict__ err,
-            const uint32_t* __restrict__ n_dev)
+            const uint32_t* __restrict__ n_dev, const uint32_t* __restrict__ tags, uint8_t* __restrict__ occ)
 {
     // Queue-driven launches (the wavefront) read the ray count written by the
     // producing stage; n is then the queue capacity.
@@ -41,6 +46,7 @@ __global__ void __launch_bounds__(kTraceBlock, 8)
     FFRayState r;
     uint2 cur = make_uint2(0u, 0u);
     uint64_t ray_id = 0;
+    uint32_t tag = 0;
     uint32_t steps = 0;
     bool active = false;
     bool exhausted = false;
@@ -58,13 +64,16 @@ __global__ void __launch_bounds__(kTraceBlock, 8)
                 if (ray_id < n) {
                     const float4 r0 = __ldg(reinterpret_cast<const float4*>(rays + ray_id));
                     const float4 r1 = __ldg(reinterpret_cast<const float4*>(rays + ray_id) + 1);
+                    if (TAGGED) tag = __ldg(tags + ray_id);
                     ff_ray_setup(r, make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), r0.w, r1.w, ANY);
                     cur = ff_root_group(r);
                     st.reset();
                     steps = 0;
                     active = bvh.num_nodes > 0;
                     if (!active) {
-                        hits[ray_id] = ff_hit{r.tmax, 0.f, 0.f, -1};
+                        if (!TAGGED) hits[ray_id] = ff_hit{r.tmax, 0.f, 0.f, -1};
+                        else if (ANY) occ[tag] = 0;
+                        else hits[tag] = ff_hit{r.tmax, 0.f, 0.f, -1};
                     }
                 } else {
                     exhausted = true;
@@ -83,7 +92,9 @@ __global__ void __launch_bounds__(kTraceBlock, 8)
                 if (done || steps > max_steps) {
                     const int32_t prim = r.prim == 0xffffffffu ? -1 : (int32_t)r.prim;
                     const float4 out = make_float4(r.tmax, r.u, r.v, __int_as_float(prim));
-                    *reinterpret_cast<float4*>(hits + ray_id) = out;
+                    if (!TAGGED) *reinterpret_cast<float4*>(hits + ray_id) = out;
+                    else if (ANY) occ[tag] = prim >= 0 ? 1 : 0;
+                    else *reinterpret_cast<float4*>(hits + tag) = out;
                     active = false;
                 }
             }
@@ -107,17 +118,19 @@ void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, u
     FF_CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), ctx->stream));
     int blocks_per_sm = 0;
     if (any_hit)
-        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true>, kTraceBlock, 0));
+        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true, false>, kTraceBlock, 0));
     else
-        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false>, kTraceBlock, 0));
+        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false, false>, kTraceBlock, 0));
     blocks_per_sm = blocks_per_sm < 1 ? 1 : blocks_per_sm;
     uint64_t grid = (uint64_t)ctx->num_sms * blocks_per_sm;
     const uint64_t need = (n + kTraceBlock - 1) / kTraceBlock;
     if (grid > need) grid = need;
     if (any_hit)
-        k_trace<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err, nullptr);
+        k_trace<true, false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter,
+                                                                              err, nullptr, nullptr, nullptr);
     else
-        k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err, nullptr);
+        k_trace<false, false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter,
+                                                                              err, nullptr, nullptr, nullptr);
     FF_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -129,17 +142,19 @@ void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d
     if (n == 0) return;
     int blocks_per_sm = 0;
     if (any_hit)
-        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true>, kTraceBlock, 0));
+        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true, false>, kTraceBlock, 0));
     else
-        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false>, kTraceBlock, 0));
+        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false, false>, kTraceBlock, 0));
     blocks_per_sm = blocks_per_sm < 1 ? 1 : blocks_per_sm;
     uint64_t grid = (uint64_t)ctx->num_sms * blocks_per_sm;
     const uint64_t need = (n + kTraceBlock - 1) / kTraceBlock;
     if (grid > need) grid = need;
     if (any_hit)
-        k_trace<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err, nullptr);
+        k_trace<true, false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter,
+                                                                              err, nullptr, nullptr, nullptr);
     else
-        k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter, err, nullptr);
+        k_trace<false, false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter,
+                                                                              err, nullptr, nullptr, nullptr);
     FF_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -147,24 +162,31 @@ void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d
 // n_dev (at most cap rays), on the context's stream.  counter must be zeroed
 // by the caller before the launch.
 void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
-                           uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter, unsigned int* err)
+                           uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter, unsigned int* err,
+                           const uint32_t* tags, uint8_t* occ)
 {
     if (cap == 0) return;
     static int bps[2] = {0, 0};
     int& blocks_per_sm = bps[any_hit ? 1 : 0];
     if (blocks_per_sm == 0) {
         if (any_hit)
-            FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true>, kTraceBlock, 0));
+            FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true, false>, kTraceBlock, 0));
         else
-            FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false>, kTraceBlock, 0));
+            FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false, false>, kTraceBlock, 0));
         blocks_per_sm = blocks_per_sm < 1 ? 1 : blocks_per_sm;
     }
     uint64_t grid = (uint64_t)ctx->num_sms * blocks_per_sm;
     const uint64_t need = (cap + kTraceBlock - 1) / kTraceBlock;
     if (grid > need) grid = need;
-    if (any_hit)
-        k_trace<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev);
+    const dim3 g((unsigned)grid), b(kTraceBlock);
+    cudaStream_t st = ctx->stream;
+    if (any_hit && tags)
+        k_trace<true, true><<<g, b, 0, st>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev, tags, occ);
+    else if (any_hit)
+        k_trace<true, false><<<g, b, 0, st>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev, tags, occ);
+    else if (tags)
+        k_trace<false, true><<<g, b, 0, st>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev, tags, occ);
     else
-        k_trace<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev);
+        k_trace<false, false><<<g, b, 0, st>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev, tags, occ);
     FF_CUDA_CHECK(cudaGetLastError());
 }

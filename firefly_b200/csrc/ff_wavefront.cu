@@ -48,7 +48,6 @@ using namespace ffp;
 using namespace ffadj;
 constexpr int kKinds = 5;
 constexpr uint32_t PH_START = 0, PH_FLIGHT = 1, PH_DONE = 2;
-constexpr int32_t SQ_NONE = -1, SQ_BLOCKED = -2;
 
 // Path-pool size when ff_render_settings.max_paths is 0: m slots per pixel,
 // m = min(spp, this / (w*h)), at least 1.  Measured on the 1.3M-triangle
@@ -75,8 +74,9 @@ struct WF {
     float4* beta;
     float4* ray_o;
     float4* ray_d;
-    int32_t* ext_q;
-    int4* sh_q;
+    // visibility word per slot: byte k = the trace's answer for shadow ray k
+    // (1 occluded), byte 3 = which shadow rays k_shade queued (bit k)
+    uint32_t* vis;
     float4* c_nee;
     float4* c_spec;
     float4* c_diff;
@@ -91,9 +91,10 @@ struct WF {
     uint32_t* cnt;
     // queues
     ff_ray* ext_rays;
-    ff_hit* ext_hits;
+    uint32_t* ext_tag;   // per queued extension ray: its slot
+    ff_hit* ext_hits;    // per slot: the closest hit of its extension ray (written by k_trace)
     ff_ray* sh_rays;
-    ff_hit* sh_hits;
+    uint32_t* sh_tag;    // per queued shadow ray: 4 * slot + k (k = 0 NEE, 1 spec, 2 diff)
     uint32_t* mat_queue;   // kKinds * P
     uint32_t* ctr;         // C_WORDS
     unsigned long long* totals;  // [0] extension rays, [1] shadow rays, [2] samples
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
         } else if (ph == PH_FLIGHT) {
             active = true;
             const uint32_t key = w.key[s];
-            const ff_hit hit = w.ext_hits[w.ext_q[s]];
+            const ff_hit hit = w.ext_hits[s];
             const uint32_t L = w.length[s] + 1;  // wf_extend's length++
             const bool found = hit.prim >= 0;
             const float3 ro = xyz(w.ray_o[s]), rd = xyz(w.ray_d[s]);
@@ -242,10 +243,10 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             }
             if (L > 1) {
                 // kernel.cu:357-359: light_brdf * beta when the NEE ray was unoccluded
-                const int4 q = w.sh_q[s];
-                const bool vis = q.x >= 0 && w.sh_hits[q.x].prim < 0;
-                const bool vis_s = q.y >= 0 && w.sh_hits[q.y].prim < 0;
-                const bool vis_d = q.z >= 0 && w.sh_hits[q.z].prim < 0;
+                const uint32_t vw = w.vis[s];
+                const bool vis = (vw & (1u << 24)) && !(vw & 0xffu);
+                const bool vis_s = (vw & (2u << 24)) && !(vw & 0xff00u);
+                const bool vis_d = (vw & (4u << 24)) && !(vw & 0xff0000u);
                 if (w.mode == FF_MODE_CORRECTED) {
                     // every term gated by its own visibility ray
                     float3 lb = make_float3(0.f, 0.f, 0.f);
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
     const uint32_t qe = warp_append(&w.ctr[C_EXT], push_ext, &w.totals[0]);
     if (push_ext) {
         w.ext_rays[qe] = ray;
-        w.ext_q[s] = (int32_t)qe;
+        w.ext_tag[qe] = s;
     }
 #pragma unroll
     for (int k = 0; k < kKinds; ++k) {
@@ -485,17 +486,25 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
         const uint32_t qe = warp_append(&w.ctr[C_EXT], valid, &w.totals[0]);
         if (valid) {
             w.ext_rays[qe] = make_ray(o.ext_o, o.ext_d, __int_as_float(0x7f800000));
-            w.ext_q[s] = (int32_t)qe;
+            w.ext_tag[qe] = s;
         }
         const uint32_t q0 = warp_append(&w.ctr[C_SH], o.ray_nee, &w.totals[1]);
         const uint32_t q1 = warp_append(&w.ctr[C_SH], o.ray_spec, &w.totals[1]);
         const uint32_t q2 = warp_append(&w.ctr[C_SH], o.ray_diff, &w.totals[1]);
-        if (o.ray_nee) w.sh_rays[q0] = o.r_nee;
-        if (o.ray_spec) w.sh_rays[q1] = o.r_spec;
-        if (o.ray_diff) w.sh_rays[q2] = o.r_diff;
+        if (o.ray_nee) {
+            w.sh_rays[q0] = o.r_nee;
+            w.sh_tag[q0] = 4u * s;
+        }
+        if (o.ray_spec) {
+            w.sh_rays[q1] = o.r_spec;
+            w.sh_tag[q1] = 4u * s + 1u;
+        }
+        if (o.ray_diff) {
+            w.sh_rays[q2] = o.r_diff;
+            w.sh_tag[q2] = 4u * s + 2u;
+        }
         if (valid)
-            w.sh_q[s] = make_int4(o.ray_nee ? (int)q0 : SQ_BLOCKED, o.ray_spec ? (int)q1 : SQ_NONE,
-                                  o.ray_diff ? (int)q2 : SQ_NONE, 0);
+            w.vis[s] = ((o.ray_nee ? 1u : 0u) | (o.ray_spec ? 2u : 0u) | (o.ray_diff ? 4u : 0u)) << 24;
     }
 }
 
@@ -512,7 +521,7 @@ __global__ void k_init(WF w, uint32_t spp, uint32_t sample_offset)
     w.acc[s] = make_float4(0.f, 0.f, 0.f, 0.f);
     w.acc_c[s] = make_float4(0.f, 0.f, 0.f, 0.f);
     w.cnt[s] = 0;
-    w.sh_q[s] = make_int4(SQ_NONE, SQ_NONE, SQ_NONE, 0);
+    w.vis[s] = 0u;
 }
 
 // Film += the m slot sums of each pixel, in slot order (compensated).
@@ -575,10 +584,10 @@ size_t ws_bytes(uint32_t P)
     size_t b = 0;
     auto add = [&](size_t s, size_t n) { b += (s * n + 255) & ~size_t(255); };
     add(4, P) /*samples_left*/; add(4, P); add(4, P); add(4, P); add(4, P);
-    add(16, P) /*beta*/; add(16, P); add(16, P); add(4, P); add(16, P);
+    add(16, P) /*beta*/; add(16, P); add(16, P); add(4, P) /*vis*/;
     add(16, P); add(16, P); add(16, P); add(16, P); add(4, P);
     add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(4, P); add(8, P);
-    add(sizeof(ff_ray), P); add(sizeof(ff_hit), P); add(sizeof(ff_ray), 3ull * P); add(sizeof(ff_hit), 3ull * P);
+    add(sizeof(ff_ray), P); add(4, P); add(sizeof(ff_hit), P); add(sizeof(ff_ray), 3ull * P); add(4, 3ull * P);
     add(4, (size_t)kKinds * P); add(4, 64); add(8, 8); add(4, 4); add(8, 4);
     return b;
 }
@@ -599,8 +608,7 @@ void ws_setup(FFWavefrontWS* ws, uint32_t P)
     w.beta = carve<float4>(p, P);
     w.ray_o = carve<float4>(p, P);
     w.ray_d = carve<float4>(p, P);
-    w.ext_q = carve<int32_t>(p, P);
-    w.sh_q = carve<int4>(p, P);
+    w.vis = carve<uint32_t>(p, P);
     w.c_nee = carve<float4>(p, P);
     w.c_spec = carve<float4>(p, P);
     w.c_diff = carve<float4>(p, P);
@@ -615,9 +623,10 @@ void ws_setup(FFWavefrontWS* ws, uint32_t P)
     w.cnt = carve<uint32_t>(p, P);
     w.hit_uv = carve<float2>(p, P);
     w.ext_rays = carve<ff_ray>(p, P);
+    w.ext_tag = carve<uint32_t>(p, P);
     w.ext_hits = carve<ff_hit>(p, P);
     w.sh_rays = carve<ff_ray>(p, 3ull * P);
-    w.sh_hits = carve<ff_hit>(p, 3ull * P);
+    w.sh_tag = carve<uint32_t>(p, 3ull * P);
     w.mat_queue = carve<uint32_t>(p, (size_t)kKinds * P);
     w.ctr = carve<uint32_t>(p, 64);
     w.totals = carve<unsigned long long>(p, 8);
@@ -639,7 +648,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     const uint32_t WH = film->width * film->height;
     const uint64_t target = st->max_paths ? st->max_paths : kDefaultPoolTarget;
     uint32_t m = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(st->spp, target / WH));
-    while ((uint64_t)m * WH > (1ull << 31)) --m;
+    while ((uint64_t)m * WH > (1ull << 30)) --m;   // shadow-ray tags are 4 * slot + k (uint32)
     const uint32_t P = m * WH;
     if (!film->ws) film->ws = new FFWavefrontWS();
     FFWavefrontWS* ws = film->ws;
@@ -726,10 +735,11 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
             }
             FF_CUDA_CHECK(cudaGetLastError());
             mark();
-            ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err);
+            ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err,
+                                  w.ext_tag, nullptr);
             mark();
-            ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, w.sh_hits, true, ws->trace_ctr + 1,
-                                  ws->err);
+            ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true, ws->trace_ctr + 1,
+                                  ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis));
             mark();
             ++frames;
         }
@@ -835,7 +845,7 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
     const uint32_t WH = t.width * t.height;
     const uint64_t target = st->max_paths ? st->max_paths : kDefaultPoolTarget;
     uint32_t m = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(st->spp, target / WH));
-    while ((uint64_t)m * WH > (1ull << 31)) --m;
+    while ((uint64_t)m * WH > (1ull << 30)) --m;   // shadow-ray tags are 4 * slot + k (uint32)
     const uint32_t P = m * WH;
     if (!ctx->adj_ws) ctx->adj_ws = new FFWavefrontWS();
     FFWavefrontWS* ws = ctx->adj_ws;
@@ -913,10 +923,11 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
             launch_shade<false, true>(w, kind_used, shade_blocks, stream);
             FF_CUDA_CHECK(cudaGetLastError());
             mark();
-            ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err);
+            ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err,
+                                  w.ext_tag, nullptr);
             mark();
-            ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, w.sh_hits, true, ws->trace_ctr + 1,
-                                  ws->err);
+            ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true, ws->trace_ctr + 1,
+                                  ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis));
             mark();
             ++frames;
         }
