@@ -132,6 +132,16 @@ class dScene:
         dirs = (A.ff_directional_light * max(1, len(dls)))(*dls)
         d.directional_lights = C.cast(dirs, C.c_void_p)
         d.num_directional_lights = len(dls)
+        tg, btg = getattr(s, "tangents", None), getattr(s, "bitangents", None)
+        if (tg is None) != (btg is None):
+            raise ValueError("tangents and bitangents come together")
+        if tg is not None:
+            tg = np.ascontiguousarray(tg, np.float32)
+            btg = np.ascontiguousarray(btg, np.float32)
+            if tg.shape != P.shape or btg.shape != P.shape:
+                raise ValueError("tangents / bitangents: one float3 per vertex")
+            self._keep += [tg, btg]
+        d.tangents, d.bitangents = _ptr(tg), _ptr(btg)
         if s.camera is not None:
             d.camera = s.camera
         h = C.c_void_p()

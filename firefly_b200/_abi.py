@@ -53,7 +53,7 @@ class ff_material(C.Structure):
     _fields_ = [("base_color", C.c_float * 3), ("emissive", C.c_float * 3), ("fresnel", C.c_float * 3),
                 ("roughness", C.c_float), ("metallic", C.c_float), ("radiance", C.c_float), ("ior", C.c_float),
                 ("kind", C.c_int32), ("base_color_tex", C.c_int32), ("roughness_tex", C.c_int32),
-                ("pad", C.c_int32)]
+                ("metallic_tex", C.c_int32), ("metallic_roughness_tex", C.c_int32), ("normal_tex", C.c_int32)]
 
 
 class ff_texture_desc(C.Structure):
@@ -85,7 +85,8 @@ class ff_scene_desc(C.Structure):
                 ("env_color", C.c_float * 3),
                 ("area_lights", C.c_void_p), ("num_area_lights", C.c_uint32),
                 ("camera", ff_camera), ("flags", C.c_uint32),
-                ("directional_lights", C.c_void_p), ("num_directional_lights", C.c_uint32)]
+                ("directional_lights", C.c_void_p), ("num_directional_lights", C.c_uint32),
+                ("tangents", C.c_void_p), ("bitangents", C.c_void_p)]
 
 
 class ff_scene_stats(C.Structure):

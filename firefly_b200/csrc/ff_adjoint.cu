@@ -47,6 +47,7 @@ constexpr int kMaxVerts = 16;
 struct ADJ {
     FFBvhView bvh;
     const FFShadeTri* shade;
+    const FFTangentTri* tan;
     const ff_material* mats;
     const FFTexView* tex;
     const ff_area_light* area;
@@ -204,17 +205,20 @@ __device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_
         // hit attributes
         const FFShadeTri& t = a.shade[hit.prim];
         const float u = hit.u, v = hit.v;
-        const float3 n = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
+        // ng: the interpolated normal the ray offsets follow (kernel.cu:437);
+        // n: the shading normal (get_normal: a normal texture's frame, else ng)
+        const float3 ng = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
         const float3 pos = o + hit.t * d;
         const float wuv = (1.f - u) - v;
         const float2 tuv = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x, u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
+        const ff_material& mm = a.mats[t.material];
+        const float3 n = shading_normal(mm, a.tex, a.tan, (uint32_t)hit.prim, u, v, tuv, ng);
         float3 wi, sp;
         sample_light(lc, pos, key, L, wi, sp);
-        const ff_material& mm = a.mats[t.material];
         const FFSurf surf = resolve_surface(mm, a.tex, tuv);
         const float3 wo = -d;
         shade_vertex(lc, surf, pos, n, wo, wi, sp, key, L, sh);
-        const float3 lo = pos + n * a.shadow_offset;
+        const float3 lo = pos + ng * a.shadow_offset;
         sh.ray_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, sh.r_nee);
         uint32_t visible = 0;
 #pragma unroll 1
@@ -239,8 +243,9 @@ __device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_
         const bool tex_grad = surf.kind == FF_MAT_DIFFUSE && mm.base_color_tex >= 0 && mm.base_color_tex == a.texture;
         // roughness gradient: GGX surfaces whose roughness comes from the
         // texture (above the 0.01 floor of resolve_surface, where it is flat)
-        const bool rough_grad = ROUGH && grad && surf.kind != FF_MAT_DIFFUSE && mm.roughness_tex >= 0 &&
-                                mm.roughness_tex == a.rough_texture && surf.roughness > 0.01f;
+        const bool rough_grad = ROUGH && grad && surf.kind != FF_MAT_DIFFUSE && mm.metallic_roughness_tex < 0 &&
+                                mm.roughness_tex >= 0 && mm.roughness_tex == a.rough_texture &&
+                                surf.roughness > 0.01f;
         RoughTerms rt;
         float3 rimm = make_float3(0.f, 0.f, 0.f);
         float3 L_after = Lacc;
@@ -278,8 +283,8 @@ __device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_
                 r.L_after = L_after;
             }
         }
-        const float side = dot3(sh.ext_d, n) >= 0.f ? 1.f : -1.f;
-        o = pos + n * (side * a.shadow_offset);
+        const float side = dot3(sh.ext_d, ng) >= 0.f ? 1.f : -1.f;
+        o = pos + ng * (side * a.shadow_offset);
         d = sh.ext_d;
     }
     return Lacc;
@@ -403,6 +408,7 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
     ADJ a;
     a.bvh = scene->view();
     a.shade = scene->shade.as<FFShadeTri>();
+    a.tan = scene->tangent.as<FFTangentTri>();
     a.mats = scene->materials.as<ff_material>();
     a.tex = scene->tex_table.as<FFTexView>();
     a.area = scene->area_lights.as<ff_area_light>();

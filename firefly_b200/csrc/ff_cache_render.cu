@@ -33,6 +33,7 @@ constexpr int kBlock = 128;
 struct CR {
     FFBvhView bvh;
     const FFShadeTri* shade;
+    const FFTangentTri* tan;
     const ff_material* mats;
     const FFTexView* tex;
     const ff_area_light* area;
@@ -127,12 +128,15 @@ __global__ void __launch_bounds__(kBlock) k_training_paths(CR a)
             if (terminate) break;
             const FFShadeTri& t = a.shade[hit.prim];
             const float u = hit.u, v = hit.v;
-            const float3 n = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
+            // ng: the interpolated normal the ray offsets follow (kernel.cu:437);
+            // n: the shading normal (get_normal: a normal texture's frame, else ng)
+            const float3 ng = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
             const float3 pos = o + hit.t * d;
             const float wuv = (1.f - u) - v;
             const float2 tuv = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x,
                                            u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
             const ff_material& mm = a.mats[t.material];
+            const float3 n = shading_normal(mm, a.tex, a.tan, (uint32_t)hit.prim, u, v, tuv, ng);
             const FFSurf surf = resolve_surface(mm, a.tex, tuv);
             const float3 wo = -d;
             if (L >= 2 && !tail && is_rough(surf, a.rough_threshold)) {
@@ -152,14 +156,14 @@ __global__ void __launch_bounds__(kBlock) k_training_paths(CR a)
                 case FF_MAT_DIELECTRIC: shade_dielectric(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
                 default: shade_coat(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
             }
-            const float3 lo = pos + n * a.shadow_offset;
+            const float3 lo = pos + ng * a.shadow_offset;
             sh.ray_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, sh.r_nee);
             vis = sh.ray_nee && !ff_occluded(a.bvh, sh.r_nee, st, a.err);
             vis_s = sh.ray_spec && !ff_occluded(a.bvh, sh.r_spec, st, a.err);
             vis_d = sh.ray_diff && !ff_occluded(a.bvh, sh.r_diff, st, a.err);
             n_shadow += (sh.ray_nee ? 1 : 0) + (sh.ray_spec ? 1 : 0) + (sh.ray_diff ? 1 : 0);
-            const float side = dot3(sh.ext_d, n) >= 0.f ? 1.f : -1.f;
-            o = pos + n * (side * a.shadow_offset);
+            const float side = dot3(sh.ext_d, ng) >= 0.f ? 1.f : -1.f;
+            o = pos + ng * (side * a.shadow_offset);
             d = sh.ext_d;
         }
         if (want_train) {
@@ -215,6 +219,7 @@ void ff_cached_render(ff_context* ctx, ff_scene* scene, ff_cache* c, const ff_re
     CR a;
     a.bvh = scene->view();
     a.shade = scene->shade.as<FFShadeTri>();
+    a.tan = scene->tangent.as<FFTangentTri>();
     a.mats = scene->materials.as<ff_material>();
     a.tex = scene->tex_table.as<FFTexView>();
     a.area = scene->area_lights.as<ff_area_light>();

@@ -104,6 +104,7 @@ struct ff_scene {
     DevBuf nodes;         // FFNode8[num_nodes]
     DevBuf tris;          // FFTri[num_tris] in leaf order
     DevBuf shade;         // FFShadeTri[num_tris] by original index
+    DevBuf tangent;       // FFTangentTri[num_tris] when a material has a normal texture, else empty
     DevBuf materials;     // ff_material[num_materials]
     uint32_t num_materials = 0;
     std::vector<DevBuf*> textures;

@@ -46,6 +46,52 @@ __global__ void k_build_shading(const float3* __restrict__ pos, const uint3* __r
     out[i] = s;
 }
 
+// Tangent frames for normal textures.  With per-vertex tangents and
+// bitangents (dVertex.cuh:8-9) each triangle takes its three vertices'.
+// Without them the frame is derived per triangle from the texture
+// coordinates: the edges e1 = v1 - v0 and e2 = v2 - v0 against their uv
+// differences give T = (e1 dv2 - e2 dv1) / det and B = (e2 du1 - e1 du2) / det
+// (det = du1 dv2 - du2 dv1; a degenerate uv mapping falls back to a frame
+// around the face normal).  No reference counterpart for the derivation: the
+// reference takes assimp's aiProcess_CalcTangentSpace frame.
+__global__ void k_build_tangents(const float3* __restrict__ pos, const uint3* __restrict__ idx,
+                                 const float2* __restrict__ uv, const float3* __restrict__ tan,
+                                 const float3* __restrict__ bitan, uint32_t n, FFTangentTri* __restrict__ out)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint3 t = idx[i];
+    FFTangentTri f;
+    if (tan && bitan) {
+        f.t0 = tan[t.x];
+        f.t1 = tan[t.y];
+        f.t2 = tan[t.z];
+        f.b0 = bitan[t.x];
+        f.b1 = bitan[t.y];
+        f.b2 = bitan[t.z];
+    } else {
+        const float3 v0 = pos[t.x], v1 = pos[t.y], v2 = pos[t.z];
+        const float3 e1 = rn_sub(v1, v0), e2 = rn_sub(v2, v0);
+        const float2 a = uv ? uv[t.x] : make_float2(0.f, 0.f), b = uv ? uv[t.y] : make_float2(0.f, 0.f),
+                     c = uv ? uv[t.z] : make_float2(0.f, 0.f);
+        const float du1 = b.x - a.x, dv1 = b.y - a.y, du2 = c.x - a.x, dv2 = c.y - a.y;
+        const float det = du1 * dv2 - du2 * dv1;
+        float3 T, B;
+        if (fabsf(det) > 1e-20f) {
+            const float r = 1.f / det;
+            T = make_float3((e1.x * dv2 - e2.x * dv1) * r, (e1.y * dv2 - e2.y * dv1) * r, (e1.z * dv2 - e2.z * dv1) * r);
+            B = make_float3((e2.x * du1 - e1.x * du2) * r, (e2.y * du1 - e1.y * du2) * r, (e2.z * du1 - e1.z * du2) * r);
+        } else {
+            const float3 nf = normalize3(rn_cross(e1, e2));
+            T = normalize3(rn_cross(nf, fabsf(nf.x) > 0.5f ? make_float3(0.f, 1.f, 0.f) : make_float3(1.f, 0.f, 0.f)));
+            B = rn_cross(nf, T);
+        }
+        f.t0 = f.t1 = f.t2 = T;
+        f.b0 = f.b1 = f.b2 = B;
+    }
+    out[i] = f;
+}
+
 }  // namespace
 
 void ff_build_env_tables(ff_context* ctx, ff_scene* s);
@@ -82,8 +128,37 @@ void ff_build_shading(ff_context* ctx, ff_scene* s, const ff_scene_desc* d, cons
         m.roughness = 1.f;
         m.ior = 1.5f;
         m.kind = FF_MAT_MIX;
-        m.base_color_tex = m.roughness_tex = -1;
+        m.base_color_tex = m.roughness_tex = m.metallic_tex = m.metallic_roughness_tex = m.normal_tex = -1;
         mats.push_back(m);
+    }
+    // texture indices in range (the kernels index the texture table with them)
+    for (const ff_material& mt : mats) {
+        for (int32_t ti : {mt.base_color_tex, mt.roughness_tex, mt.metallic_tex, mt.metallic_roughness_tex,
+                           mt.normal_tex})
+            FF_REQUIRE(ti < (int32_t)d->num_textures, "material texture index out of range");
+    }
+    // tangent frames, only when some material has a normal texture
+    bool normal_maps = false;
+    for (const ff_material& mt : mats) normal_maps |= mt.normal_tex >= 0;
+    FF_REQUIRE(!(d->tangents && !d->bitangents) && !(d->bitangents && !d->tangents),
+               "tangents and bitangents come together");
+    if (normal_maps && n) {
+        DevBuf tg, btg;
+        if (d->tangents && d->num_vertices) {
+            tg.alloc(sizeof(float3) * d->num_vertices);
+            btg.alloc(sizeof(float3) * d->num_vertices);
+            FF_CUDA_CHECK(cudaMemcpyAsync(tg.ptr, d->tangents, sizeof(float3) * d->num_vertices,
+                                          cudaMemcpyHostToDevice, st));
+            FF_CUDA_CHECK(cudaMemcpyAsync(btg.ptr, d->bitangents, sizeof(float3) * d->num_vertices,
+                                          cudaMemcpyHostToDevice, st));
+        }
+        s->tangent.alloc(sizeof(FFTangentTri) * n);
+        k_build_tangents<<<(n + 255) / 256, 256, 0, st>>>(d_pos, d_idx, uv.as<float2>(), tg.as<float3>(),
+                                                          btg.as<float3>(), n, s->tangent.as<FFTangentTri>());
+        FF_CUDA_CHECK(cudaGetLastError());
+        FF_CUDA_CHECK(cudaStreamSynchronize(st));   // tg / btg are freed on return
+    } else {
+        s->tangent.release();
     }
     s->num_materials = (uint32_t)mats.size();
     s->materials.alloc(sizeof(ff_material) * mats.size());

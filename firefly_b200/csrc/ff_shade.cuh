@@ -148,6 +148,13 @@ struct FFTexView {
     int width, height;
 };
 
+// Per-original-triangle tangent frame (the dVertex tangent and bitangent of
+// its three vertices), read only at hits on materials with a normal texture.
+struct FFTangentTri {
+    float3 t0, t1, t2;
+    float3 b0, b1, b2;
+};
+
 // diff_get_pdf = 1.f / (2.f * M_PI) in float, returned as double (dMaterial.cu:160-163)
 FF_D double diff_get_pdf() { return (double)(1.f / (2.f * FF_PI)); }
 
@@ -301,17 +308,53 @@ FF_D FFSurf resolve_surface(const ff_material& m, const FFTexView* tex, float2 u
         const FFTexView t = tex[m.base_color_tex];
         s.albedo = tex_bilinear(t.rgb, t.width, t.height, uv.x, uv.y);
     }
+    // get_roughness / get_metallic (dMaterial.cu:25-60): the packed glTF
+    // metallic-roughness texture first (roughness in y, metallic in z), then
+    // the single-channel textures (x), then the factors
     s.roughness = m.roughness;
-    if (m.roughness_tex >= 0) {
-        const FFTexView t = tex[m.roughness_tex];
-        s.roughness = hmax(tex_bilinear(t.rgb, t.width, t.height, uv.x, uv.y).x, 0.01f);
+    s.metallic = m.metallic;
+    if (m.metallic_roughness_tex >= 0) {
+        const FFTexView t = tex[m.metallic_roughness_tex];
+        const float3 c = tex_bilinear(t.rgb, t.width, t.height, uv.x, uv.y);
+        s.roughness = hmax(c.y, 0.01f);
+        s.metallic = c.z;
+    } else {
+        if (m.roughness_tex >= 0) {
+            const FFTexView t = tex[m.roughness_tex];
+            s.roughness = hmax(tex_bilinear(t.rgb, t.width, t.height, uv.x, uv.y).x, 0.01f);
+        }
+        if (m.metallic_tex >= 0) {
+            const FFTexView t = tex[m.metallic_tex];
+            s.metallic = tex_bilinear(t.rgb, t.width, t.height, uv.x, uv.y).x;
+        }
     }
     s.fresnel = make_float3(m.fresnel[0], m.fresnel[1], m.fresnel[2]);
-    s.metallic = m.metallic;
     s.ior = m.ior;
     s.kind = m.kind;
     return s;
 }
+// get_normal (dMaterial.cu:61-88): without a normal texture the interpolated
+// normal n; with one, the tangent and bitangent interpolated as the normal is
+// (dTriangle::hit, dTriangle.cu:94-96) and n form the frame TBN, the texel c
+// becomes q = c * 2 - 1, and the normal is normalize(TBN * q) with the
+// reference's Matrix4x4 * float3 (dMatrix.cuh:70-78): q.x T + q.y B + q.z N
+// summed in that order, plus the zero translation, over w = 1.
+FF_D float3 shading_normal(const ff_material& m, const FFTexView* tex, const FFTangentTri* tan, uint32_t prim,
+                           float u, float v, float2 uv, float3 n)
+{
+    if (m.normal_tex < 0 || !tan) return n;
+    const FFTangentTri& f = tan[prim];
+    const float3 T = normalize3(u * f.t1 + v * f.t2 + ((1.f - u) - v) * f.t0);
+    const float3 B = normalize3(u * f.b1 + v * f.b2 + ((1.f - u) - v) * f.b0);
+    const FFTexView t = tex[m.normal_tex];
+    const float3 c = tex_bilinear(t.rgb, t.width, t.height, uv.x, uv.y);
+    const float3 q = make_float3(c.x * 2.f - 1.f, c.y * 2.f - 1.f, c.z * 2.f - 1.f);
+    const float3 o = make_float3(((T.x * q.x + B.x * q.y) + n.x * q.z) + 0.f, ((T.y * q.x + B.y * q.y) + n.y * q.z) + 0.f,
+                                 ((T.z * q.x + B.z * q.y) + n.z * q.z) + 0.f);
+    const float w = ((0.f * q.x + 0.f * q.y) + 0.f * q.z) + 1.f;
+    return normalize3(make_float3(o.x / w, o.y / w, o.z / w));
+}
+
 struct FFEnvView {
     const float3* rgb;       // width*height texels, row y = v * height
     const double* marginal;  // marginal_y[height]

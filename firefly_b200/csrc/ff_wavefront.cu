@@ -83,7 +83,8 @@ struct WF {
     float4* ext_fp;   // f.xyz, pdf
     float* ext_cos;
     float4* hit_pos;  // xyz, w = material index bits
-    float4* hit_nrm;
+    float4* hit_nrm;      // shading normal
+    float4* hit_ngeo;     // interpolated normal, written only under a normal texture
     float4* light_wi;
     float4* light_sp;
     float4* acc;
@@ -100,6 +101,7 @@ struct WF {
     unsigned long long* totals;  // [0] extension rays, [1] shadow rays, [2] samples
     // scene
     const FFShadeTri* shade;
+    const FFTangentTri* tan;   // tangent frames, or null when no material has a normal texture
     const ff_material* mats;
     const ff_area_light* area;
     uint32_t n_area;
@@ -328,11 +330,15 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 const float wuv = (1.f - u) - v;
                 const float2 uv = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x,
                                               u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
+                const ff_material& mm = w.mats[t.material];
+                // get_normal: the shading normal (a normal texture's frame, else
+                // n); n stays the normal the ray offsets follow (kernel.cu:437)
+                const float3 ns = shading_normal(mm, w.tex, w.tan, (uint32_t)hit.prim, u, v, uv, n);
                 if (!ADJ && w.cache_mode && L >= 2) {
-                    const FFSurf surf = resolve_surface(w.mats[t.material], w.tex, uv);
+                    const FFSurf surf = resolve_surface(mm, w.tex, uv);
                     if (is_rough(surf, w.rough_threshold)) {
                         // the cache answers for everything from this vertex on
-                        rec = ffc::make_record(pos, surf.roughness, -rd, n, beta, s);
+                        rec = ffc::make_record(pos, surf.roughness, -rd, ns, beta, s);
                         query = true;
                         terminate = true;
                     }
@@ -345,10 +351,11 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                     w.length[s] = L;
                     w.beta[s] = f4(beta);
                     w.hit_pos[s] = f4(pos, __uint_as_float(t.material));
-                    w.hit_nrm[s] = f4(n);
+                    w.hit_nrm[s] = f4(ns);
+                    if (mm.normal_tex >= 0) w.hit_ngeo[s] = f4(n);
                     w.light_wi[s] = f4(wi);
                     w.light_sp[s] = f4(sp);
-                    kind = w.mats[t.material].kind;
+                    kind = mm.kind;
                 }
             }
             if (terminate) {
@@ -429,8 +436,12 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
             s = w.mat_queue[(size_t)KIND * w.P + qi];
             const float4 hp = w.hit_pos[s];
             const float3 pos = xyz(hp);
-            const FFSurf mat = resolve_surface(w.mats[__float_as_uint(hp.w)], w.tex, w.hit_uv[s]);
-            const float3 n = xyz(w.hit_nrm[s]);
+            const ff_material& mm = w.mats[__float_as_uint(hp.w)];
+            const FFSurf mat = resolve_surface(mm, w.tex, w.hit_uv[s]);
+            const float3 n = xyz(w.hit_nrm[s]);   // shading normal
+            // the normal the ray offsets follow (kernel.cu:437): differs from n
+            // only under a normal texture
+            const float3 ng = mm.normal_tex >= 0 ? xyz(w.hit_ngeo[s]) : n;
             const float3 wo = -xyz(w.ray_d[s]);
             const float3 wi = xyz(w.light_wi[s]);
             const float3 sp = xyz(w.light_sp[s]);
@@ -444,13 +455,13 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
             else if (KIND == FF_MAT_DIELECTRIC) shade_dielectric(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
             else shade_coat(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
             // NEE shadow ray of wf_shadow: light_ray = position + normal * SHADOW_OFFSET (kernel.cu:437)
-            const float3 lo = pos + n * w.shadow_offset;
+            const float3 lo = pos + ng * w.shadow_offset;
             o.ray_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, o.r_nee);
             // continuation ray: the reference starts it at the hit point (kernel.cu:643)
             o.ext_o = pos;
             if (w.mode == FF_MODE_CORRECTED) {
-                const float side = dot3(o.ext_d, n) >= 0.f ? 1.f : -1.f;
-                o.ext_o = pos + n * (side * w.shadow_offset);
+                const float side = dot3(o.ext_d, ng) >= 0.f ? 1.f : -1.f;
+                o.ext_o = pos + ng * (side * w.shadow_offset);
             }
             w.c_nee[s] = f4(o.c_nee);
             w.c_spec[s] = f4(o.c_spec);
@@ -460,13 +471,12 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
             w.ray_o[s] = f4(o.ext_o);
             w.ray_d[s] = f4(o.ext_d);
             if (ADJ && w.pass[s] != 0u) {
-                const ff_material& mm = w.mats[__float_as_uint(hp.w)];
                 uint32_t flags = 0;
                 if (KIND == FF_MAT_DIFFUSE && w.grad_tex && mm.base_color_tex >= 0 && mm.base_color_tex == w.adj_texture)
                     flags |= V_ALBEDO;
                 // roughness from the texture, above the 0.01 floor of resolve_surface (flat there)
-                if (KIND != FF_MAT_DIFFUSE && w.grad_rough && mm.roughness_tex >= 0 && mm.roughness_tex == w.adj_rough &&
-                    mat.roughness > 0.01f) {
+                if (KIND != FF_MAT_DIFFUSE && w.grad_rough && mm.metallic_roughness_tex < 0 && mm.roughness_tex >= 0 &&
+                    mm.roughness_tex == w.adj_rough && mat.roughness > 0.01f) {
                     flags |= V_ROUGH;
                     const RoughTerms rt = rough_terms(o, n, wo, wi, mat.roughness);
                     w.v_nee[s] = f4(rt.nee);
@@ -586,7 +596,7 @@ size_t ws_bytes(uint32_t P)
     add(4, P) /*samples_left*/; add(4, P); add(4, P); add(4, P); add(4, P);
     add(16, P) /*beta*/; add(16, P); add(16, P); add(4, P) /*vis*/;
     add(16, P); add(16, P); add(16, P); add(16, P); add(4, P);
-    add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(4, P); add(8, P);
+    add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(4, P); add(8, P);
     add(sizeof(ff_ray), P); add(4, P); add(sizeof(ff_hit), P); add(sizeof(ff_ray), 3ull * P); add(4, 3ull * P);
     add(4, (size_t)kKinds * P); add(4, 64); add(8, 8); add(4, 4); add(8, 4);
     return b;
@@ -616,6 +626,7 @@ void ws_setup(FFWavefrontWS* ws, uint32_t P)
     w.ext_cos = carve<float>(p, P);
     w.hit_pos = carve<float4>(p, P);
     w.hit_nrm = carve<float4>(p, P);
+    w.hit_ngeo = carve<float4>(p, P);
     w.light_wi = carve<float4>(p, P);
     w.light_sp = carve<float4>(p, P);
     w.acc = carve<float4>(p, P);
@@ -665,6 +676,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     w.light = st->light;
     w.shadow_offset = st->shadow_offset > 0.f ? st->shadow_offset : 0.001f;
     w.shade = scene->shade.as<FFShadeTri>();
+    w.tan = scene->tangent.as<FFTangentTri>();
     w.mats = scene->materials.as<ff_material>();
     w.area = scene->area_lights.as<ff_area_light>();
     w.n_area = scene->num_area_lights;
@@ -863,6 +875,7 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
     w.light = st->light;
     w.shadow_offset = st->shadow_offset > 0.f ? st->shadow_offset : 0.001f;
     w.shade = scene->shade.as<FFShadeTri>();
+    w.tan = scene->tangent.as<FFTangentTri>();
     w.mats = scene->materials.as<ff_material>();
     w.area = scene->area_lights.as<ff_area_light>();
     w.n_area = scene->num_area_lights;

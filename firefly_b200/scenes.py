@@ -162,6 +162,8 @@ class Scene:
     env_rgb: np.ndarray | None = None
     env_color: tuple = (0.0, 0.0, 0.0)
     textures: list = field(default_factory=list)   # (h, w, 3) float32 arrays, indexed by ff_material.*_tex
+    tangents: np.ndarray | None = None     # (V, 3) per-vertex tangent frame for normal textures, or None
+    bitangents: np.ndarray | None = None
     camera: A.ff_camera | None = None
     width: int = 256
     height: int = 256
@@ -189,7 +191,8 @@ def directional_light(direction, emissive=(1.0, 1.0, 1.0), radiance=1.0) -> A.ff
 
 
 def material(base_color, kind=A.FF_MAT_MIX, roughness=1.0, metallic=0.0, ior=1.5, fresnel=0.04,
-             emissive=(0, 0, 0), radiance=0.0, base_color_tex=-1, roughness_tex=-1) -> A.ff_material:
+             emissive=(0, 0, 0), radiance=0.0, base_color_tex=-1, roughness_tex=-1, metallic_tex=-1,
+             metallic_roughness_tex=-1, normal_tex=-1) -> A.ff_material:
     m = A.ff_material()
     for k in range(3):
         m.base_color[k] = float(base_color[k])
@@ -202,6 +205,9 @@ def material(base_color, kind=A.FF_MAT_MIX, roughness=1.0, metallic=0.0, ior=1.5
     m.kind = kind
     m.base_color_tex = base_color_tex
     m.roughness_tex = roughness_tex
+    m.metallic_tex = metallic_tex
+    m.metallic_roughness_tex = metallic_roughness_tex
+    m.normal_tex = normal_tex
     return m
 
 
@@ -591,3 +597,76 @@ def textured_room(seed: int = 0, width: int = 512, height: int = 512, albedo=Non
                       near=0.05, far=60.0)
     return Scene(positions=P, indices=I, normals=N, texcoords=UV, material_ids=mat_ids, materials=mats,
                  env_rgb=np.asarray(sky, np.float32), textures=textures, camera=cam, width=width, height=height)
+
+
+def vertex_tangents(positions, indices, texcoords, normals):
+    """Per-vertex tangent frame for normal textures: per triangle, dP/du and
+    dP/dv from the uv differences of its edges, summed at its vertices, then
+    made orthogonal to the vertex normal (Gram-Schmidt) and normalised; the
+    bitangent keeps the sign of dP/dv.  Returns (tangents, bitangents), both
+    (V, 3) float32."""
+    P = np.asarray(positions, np.float64)
+    I = np.asarray(indices, np.int64)
+    UV = np.asarray(texcoords, np.float64)
+    N = np.asarray(normals, np.float64).copy()
+    # vertices no triangle uses may carry a zero normal: any unit normal does
+    N[np.linalg.norm(N, axis=1) < 1e-12] = (0.0, 0.0, 1.0)
+    e1, e2 = P[I[:, 1]] - P[I[:, 0]], P[I[:, 2]] - P[I[:, 0]]
+    d1, d2 = UV[I[:, 1]] - UV[I[:, 0]], UV[I[:, 2]] - UV[I[:, 0]]
+    det = d1[:, 0] * d2[:, 1] - d2[:, 0] * d1[:, 1]
+    r = np.where(np.abs(det) > 1e-20, 1.0 / np.where(det == 0, 1.0, det), 0.0)[:, None]
+    T = (e1 * d2[:, 1:2] - e2 * d1[:, 1:2]) * r
+    B = (e2 * d1[:, 0:1] - e1 * d2[:, 0:1]) * r
+    Tv, Bv = np.zeros_like(P), np.zeros_like(P)
+    for k in range(3):
+        np.add.at(Tv, I[:, k], T)
+        np.add.at(Bv, I[:, k], B)
+    Tv -= N * (Tv * N).sum(1, keepdims=True)
+    # vertices without a uv gradient (poles, degenerate mappings): any tangent
+    bad = np.linalg.norm(Tv, axis=1) < 1e-12
+    alt = np.where(np.abs(N[:, :1]) > 0.5, np.array([[0.0, 1.0, 0.0]]), np.array([[1.0, 0.0, 0.0]]))
+    Tv[bad] = np.cross(N[bad], alt[bad])
+    Tv /= np.linalg.norm(Tv, axis=1, keepdims=True)
+    Bn = np.cross(N, Tv)
+    sign = np.where((Bn * Bv).sum(1, keepdims=True) < 0.0, -1.0, 1.0)
+    return Tv.astype(np.float32), (Bn * sign).astype(np.float32)
+
+
+def normal_texture(res: int = 64, seed: int = 0, strength: float = 0.6) -> np.ndarray:
+    """Tangent-space normal texture of a seeded bump field, stored as
+    0.5 + 0.5 * n (the usual 8-bit-style encoding), (res, res, 3) float32."""
+    h = perlin2(res, seed * 7 + 3)
+    gy, gx = np.gradient(h * res * strength / 8.0)
+    n = np.stack([-gx, -gy, np.ones_like(h)], -1)
+    n /= np.linalg.norm(n, axis=-1, keepdims=True)
+    return (0.5 + 0.5 * n).astype(np.float32)
+
+
+def pbr_textured_room(seed: int = 0, width: int = 64, height: int = 64, tex_res: int = 64, env=None,
+                      derive_tangents: bool = False) -> Scene:
+    """The room open to the sky with every material texture kind:
+    walls and floor FF_MAT_MIX with a base-colour texture (0), a packed
+    metallic-roughness texture (1: roughness in y, metallic in z) and a normal
+    texture (2); the sphere a GGX conductor with a roughness texture (3), a
+    metallic texture (4) and the normal texture.  Per-vertex tangents come with
+    the scene unless derive_tangents (the library then derives them)."""
+    base = textured_room(seed=seed, width=width, height=height, tex_res=tex_res, env=env, env_w=64, env_h=32,
+                         sphere_kind=A.FF_MAT_CONDUCTOR)
+    rng = np.random.default_rng(seed + 17)
+    rough = np.clip(0.35 + 0.25 * perlin2(tex_res, seed * 5 + 11), 0.05, 0.9)
+    metal = np.clip(0.5 + 0.5 * perlin2(tex_res, seed * 5 + 12), 0.0, 1.0)
+    mr = np.stack([np.zeros_like(rough), rough, metal], -1).astype(np.float32)
+    nt = normal_texture(tex_res, seed)
+    r1 = np.repeat(np.clip(0.2 + 0.3 * perlin2(tex_res, seed * 5 + 13), 0.05, 0.9)[..., None], 3, -1)
+    m1 = np.repeat(np.clip(0.7 + 0.3 * perlin2(tex_res, seed * 5 + 14), 0.0, 1.0)[..., None], 3, -1)
+    mats = [material((0.5, 0.5, 0.5), kind=A.FF_MAT_MIX, roughness=1.0, base_color_tex=0,
+                     metallic_roughness_tex=1, normal_tex=2),
+            material(tuple(rng.uniform(0.5, 0.9, 3)), kind=A.FF_MAT_CONDUCTOR, roughness=0.5, metallic=1.0,
+                     roughness_tex=3, metallic_tex=4, normal_tex=2)]
+    scn = Scene(positions=base.positions, indices=base.indices, normals=base.normals, texcoords=base.texcoords,
+                material_ids=base.material_ids, materials=mats, env_rgb=base.env_rgb,
+                textures=[base.textures[0], mr, nt, r1.astype(np.float32), m1.astype(np.float32)],
+                camera=base.camera, width=width, height=height)
+    if not derive_tangents:
+        scn.tangents, scn.bitangents = vertex_tangents(scn.positions, scn.indices, scn.texcoords, scn.normals)
+    return scn

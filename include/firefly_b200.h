@@ -91,7 +91,13 @@ typedef enum ff_material_kind {
 } ff_material_kind;
 
 /* Flattened dMaterial (dMaterial.cuh:9-31): glTF metallic-roughness factors.
- * Textures are referenced by index into ff_scene_desc.textures, -1 = none. */
+ * Textures are referenced by index into ff_scene_desc.textures, -1 = none,
+ * and read as the reference's get_albedo / get_roughness / get_metallic /
+ * get_normal read them (dMaterial.cu:10-88): the roughness from
+ * metallic_roughness_tex channel 1 if set, else roughness_tex channel 0 (both
+ * at least 0.01), else the factor; the metallic from metallic_roughness_tex
+ * channel 2, else metallic_tex channel 0, else the factor; the shading normal
+ * from normal_tex through the interpolated tangent frame (TBN * (2 t - 1)). */
 typedef struct ff_material {
     float base_color[3];      /* baseColorFactor */
     float emissive[3];        /* emissiveColorFactor */
@@ -101,9 +107,11 @@ typedef struct ff_material {
     float radiance;           /* emission scale, emissive_L = radiance * emissive */
     float ior;                /* FF_MAT_DIELECTRIC / FF_MAT_COAT only */
     int32_t kind;             /* ff_material_kind */
-    int32_t base_color_tex;   /* -1 = none */
-    int32_t roughness_tex;    /* -1 = none */
-    int32_t pad;
+    int32_t base_color_tex;   /* baseColorTexture, -1 = none */
+    int32_t roughness_tex;    /* roughnessTexture, -1 = none */
+    int32_t metallic_tex;     /* metallicTexture, -1 = none */
+    int32_t metallic_roughness_tex; /* metallicRoughnessTexture (glTF packing), -1 = none */
+    int32_t normal_tex;       /* normalTexture (tangent space), -1 = none */
 } ff_material;
 
 /* RGB float texture, row-major, texel (x, y) at data[3*(y*width + x)]. */
@@ -167,6 +175,11 @@ typedef struct ff_scene_desc {
     uint32_t flags;               /* reserved, 0 */
     const ff_directional_light* directional_lights;
     uint32_t num_directional_lights;
+    /* Per-vertex tangent frame for normal textures (dVertex.cuh:4-10), float3
+     * each; NULL = derived per triangle from positions and texcoords (the
+     * reference takes assimp's aiProcess_CalcTangentSpace frame). */
+    const float* tangents;
+    const float* bitangents;
 } ff_scene_desc;
 
 typedef struct ff_scene_stats {

@@ -57,6 +57,9 @@ typedef struct {
     int32_t kind;          /* 0 mix (wf_mat_mix), 1 diffuse (wf_mat_diffuse), 2 conductor (wf_mat_cook) */
     int32_t base_color_tex;  /* -1 = none */
     int32_t roughness_tex;   /* -1 = none */
+    int32_t metallic_tex;    /* -1 = none */
+    int32_t metallic_roughness_tex; /* -1 = none (glTF packing: roughness y, metallic z) */
+    int32_t normal_tex;      /* -1 = none (tangent space) */
 } ffo_material;
 
 typedef struct {
@@ -106,6 +109,10 @@ typedef struct {
      * vertex chosen uniformly among all (corrected mode) */
     const ffo_dir_light* dir_lights;
     int32_t num_dir_lights;
+    /* per-triangle vertex tangents and bitangents (num_tris x 9 each) for
+     * normal textures, or NULL */
+    const float* tangents;
+    const float* bitangents;
 } ffo_render_desc;
 
 /* Renders every pixel's spp samples; out_rgb (width*height*3 doubles) gets

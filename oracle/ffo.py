@@ -87,7 +87,8 @@ def shadow_hit(v0, v1, v2, o, d):
 class ffo_material(C.Structure):
     _fields_ = [("base_color", C.c_float * 3), ("fresnel", C.c_float * 3), ("roughness", C.c_float),
                 ("metallic", C.c_float), ("kind", C.c_int32), ("base_color_tex", C.c_int32),
-                ("roughness_tex", C.c_int32)]
+                ("roughness_tex", C.c_int32), ("metallic_tex", C.c_int32), ("metallic_roughness_tex", C.c_int32),
+                ("normal_tex", C.c_int32)]
 
 
 class ffo_texture(C.Structure):
@@ -109,7 +110,8 @@ class ffo_render_desc(C.Structure):
                 ("cam_jitter", C.c_float), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
                 ("sample_offset", C.c_int32), ("max_depth", C.c_int32), ("rr_depth", C.c_int32),
                 ("seed", C.c_uint32), ("mode", C.c_int32), ("light", C.c_int32), ("shadow_offset", C.c_float),
-                ("threads", C.c_int32), ("dir_lights", C.c_void_p), ("num_dir_lights", C.c_int32)]
+                ("threads", C.c_int32), ("dir_lights", C.c_void_p), ("num_dir_lights", C.c_int32),
+                ("tangents", C.c_void_p), ("bitangents", C.c_void_p)]
 
 
 class ffo_dir_light(C.Structure):
@@ -136,6 +138,8 @@ def render(scene, width, height, spp, max_depth=3, rr_depth=3, seed=0, mode=0, l
             mats[i].fresnel[k] = m.fresnel[k]
         mats[i].roughness, mats[i].metallic, mats[i].kind = m.roughness, m.metallic, m.kind
         mats[i].base_color_tex, mats[i].roughness_tex = m.base_color_tex, m.roughness_tex
+        mats[i].metallic_tex, mats[i].metallic_roughness_tex = m.metallic_tex, m.metallic_roughness_tex
+        mats[i].normal_tex = m.normal_tex
     texs = [np.ascontiguousarray(t, np.float32) for t in getattr(scene, "textures", [])]
     tdesc = (ffo_texture * max(1, len(texs)))()
     for i, t in enumerate(texs):
@@ -166,6 +170,12 @@ def render(scene, width, height, spp, max_depth=3, rr_depth=3, seed=0, mode=0, l
             dirs[i].emissive[k] = L.emissive[k]
         dirs[i].radiance = L.radiance
     d.dir_lights, d.num_dir_lights = C.cast(dirs, C.c_void_p), len(dls)
+    tg = btg = None
+    if getattr(scene, "tangents", None) is not None:
+        tg = np.ascontiguousarray(np.asarray(scene.tangents, np.float32)[scene.indices].reshape(-1, 9))
+        btg = np.ascontiguousarray(np.asarray(scene.bitangents, np.float32)[scene.indices].reshape(-1, 9))
+    d.tangents = None if tg is None else tg.ctypes.data
+    d.bitangents = None if btg is None else btg.ctypes.data
     d.env_rgb = None if env is None else env.ctypes.data
     d.env_w = 0 if env is None else env.shape[1]
     d.env_h = 0 if env is None else env.shape[0]

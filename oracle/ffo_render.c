@@ -689,7 +689,11 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int 
         sf.roughness = mm->roughness;
         sf.metallic = mm->metallic;
         sf.kind = mm->kind;
-        if (d->texcoords && (mm->base_color_tex >= 0 || mm->roughness_tex >= 0)) {
+        /* ng: the interpolated normal the ray offsets follow (kernel.cu:437);
+         * n becomes get_normal's shading normal below */
+        const v3 ng = n;
+        if (d->texcoords && (mm->base_color_tex >= 0 || mm->roughness_tex >= 0 || mm->metallic_tex >= 0 ||
+                             mm->metallic_roughness_tex >= 0 || mm->normal_tex >= 0)) {
             /* texcoord = u * uv1 + v * uv2 + (1 - u - v) * uv0 (dTriangle.cu:97) */
             const float* tc = d->texcoords + 6 * (size_t)prim;
             float wuv = (1.f - u) - v;
@@ -699,9 +703,40 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int 
                 const ffo_texture* tx = &d->textures[mm->base_color_tex];
                 sf.albedo = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv);
             }
-            if (mm->roughness_tex >= 0) {
-                const ffo_texture* tx = &d->textures[mm->roughness_tex];
-                sf.roughness = hmax(tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv).x, 0.01f);
+            /* get_roughness / get_metallic (dMaterial.cu:25-60): the packed
+             * metallic-roughness texture first (y, z), then roughness / metallic
+             * textures (x), then the factors */
+            if (mm->metallic_roughness_tex >= 0) {
+                const ffo_texture* tx = &d->textures[mm->metallic_roughness_tex];
+                v3 c = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv);
+                sf.roughness = hmax(c.y, 0.01f);
+                sf.metallic = c.z;
+            } else {
+                if (mm->roughness_tex >= 0) {
+                    const ffo_texture* tx = &d->textures[mm->roughness_tex];
+                    sf.roughness = hmax(tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv).x, 0.01f);
+                }
+                if (mm->metallic_tex >= 0) {
+                    const ffo_texture* tx = &d->textures[mm->metallic_tex];
+                    sf.metallic = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv).x;
+                }
+            }
+            /* get_normal (dMaterial.cu:61-88): TBN from the tangent and bitangent
+             * interpolated as the normal (dTriangle.cu:94-96), texel c mapped to
+             * q = c * 2 - 1, then Matrix4x4 * float3 (dMatrix.cuh:70-78):
+             * ((T q.x + B q.y) + N q.z) + 0 over w = ((0 + 0) + 0) + 1 */
+            if (mm->normal_tex >= 0 && d->tangents && d->bitangents) {
+                const float* tg = d->tangents + 9 * (size_t)prim;
+                const float* bt = d->bitangents + 9 * (size_t)prim;
+                v3 T = normalize(add(add(smul(u, ld3(tg + 3)), smul(v, ld3(tg + 6))), smul((1.f - u) - v, ld3(tg))));
+                v3 B = normalize(add(add(smul(u, ld3(bt + 3)), smul(v, ld3(bt + 6))), smul((1.f - u) - v, ld3(bt))));
+                const ffo_texture* tx = &d->textures[mm->normal_tex];
+                v3 c = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv);
+                v3 q = {c.x * 2.f - 1.f, c.y * 2.f - 1.f, c.z * 2.f - 1.f};
+                v3 o3 = {((T.x * q.x + B.x * q.y) + ng.x * q.z) + 0.f, ((T.y * q.x + B.y * q.y) + ng.y * q.z) + 0.f,
+                         ((T.z * q.x + B.z * q.y) + ng.z * q.z) + 0.f};
+                float w3 = ((0.f * q.x + 0.f * q.y) + 0.f * q.z) + 1.f;
+                n = normalize((v3){o3.x / w3, o3.y / w3, o3.z / w3});
             }
         }
         const surf_t* mat = &sf;
@@ -710,7 +745,7 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int 
         if (mat->kind == 0) shade_mix(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
         else if (mat->kind == 1) shade_diffuse(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
         else shade_conductor(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
-        v3 lo = add(pos, muls(n, d->shadow_offset));
+        v3 lo = add(pos, muls(ng, d->shadow_offset));
         sh.has_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, &sh.r_nee);
         vis_nee = sh.has_nee && !occluded(d, &sh.r_nee);
         vis_spec = sh.has_spec && !occluded(d, &sh.r_spec);
@@ -718,8 +753,8 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int 
         *n_sh += (uint64_t)(sh.has_nee + sh.has_spec + sh.has_diff);
         o = pos;
         if (corrected) {
-            float side = dot(sh.ext_d, n) >= 0.f ? 1.f : -1.f;
-            o = add(pos, muls(n, side * d->shadow_offset));
+            float side = dot(sh.ext_d, ng) >= 0.f ? 1.f : -1.f;
+            o = add(pos, muls(ng, side * d->shadow_offset));
         }
         dir = sh.ext_d;
     }

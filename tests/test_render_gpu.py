@@ -144,6 +144,51 @@ def test_textured_env_scene_parity(ctx, oracle):
         assert mre <= MRE_TOL
 
 
+def test_material_textures_and_normal_map_parity(ctx, oracle):
+    """Every material texture kind against the oracle, in both modes: a
+    base-colour texture, a packed metallic-roughness texture (roughness y,
+    metallic z) and a normal texture on the walls (mixed material); roughness
+    and metallic textures and the normal texture on a conductor sphere.  The
+    tangent frame comes per vertex with the scene (dMaterial.cu:10-88)."""
+    import firefly_b200 as ff
+    scn = scenes.pbr_textured_room(seed=3, width=48, height=48, tex_res=64)
+    for mode in (ff.FF_MODE_PARITY, ff.FF_MODE_CORRECTED):
+        got, n, stats = _gpu_render(ctx, scn, 48, 48, 4, light=-1, max_depth=4, rr_depth=3, seed=5, mode=mode)
+        ref, (ref_ext, ref_sh) = oracle.render(scn, 48, 48, 4, max_depth=4, rr_depth=3, seed=5, mode=mode, light=-1,
+                                               threads=cpu_threads())
+        fin = np.isfinite(got) & np.isfinite(ref)
+        assert np.array_equal(np.isfinite(got), np.isfinite(ref))
+        mre = _mre(got[fin], ref[fin])
+        print(f"[parity] material textures + normal map mode={mode}: mre={mre:.3e} "
+              f"ext={stats['extension_rays']}/{ref_ext} shadow={stats['shadow_rays']}/{ref_sh}")
+        assert mre <= MRE_TOL
+        assert abs(stats["extension_rays"] - ref_ext) <= max(2, 1e-3 * ref_ext)
+
+
+def test_normal_map_and_packed_textures_change_the_image(ctx):
+    """The normal texture, the packed metallic-roughness texture and derived
+    tangents (no per-vertex frame given) all reach the image."""
+    import firefly_b200 as ff
+    scn = scenes.pbr_textured_room(seed=3, width=48, height=48, tex_res=64)
+    kw = dict(light=-1, max_depth=4, rr_depth=3, seed=5, mode=ff.FF_MODE_CORRECTED)
+    img, _, _ = _gpu_render(ctx, scn, 48, 48, 16, **kw)
+    flat = scenes.pbr_textured_room(seed=3, width=48, height=48, tex_res=64)
+    for m in flat.materials:
+        m.normal_tex = -1
+    img_flat, _, _ = _gpu_render(ctx, flat, 48, 48, 16, **kw)
+    packed = scenes.pbr_textured_room(seed=3, width=48, height=48, tex_res=64)
+    packed.materials[0].metallic_roughness_tex = -1
+    img_factors, _, _ = _gpu_render(ctx, packed, 48, 48, 16, **kw)
+    derived = scenes.pbr_textured_room(seed=3, width=48, height=48, tex_res=64, derive_tangents=True)
+    img_derived, _, _ = _gpu_render(ctx, derived, 48, 48, 16, **kw)
+    for a in (img, img_flat, img_factors, img_derived):
+        assert np.isfinite(a).all() and a.mean() > 0
+    assert _mre(img, img_flat) > 1e-2, "the normal texture changes the shading"
+    assert _mre(img, img_factors) > 1e-2, "the packed texture replaces the factors"
+    # derived frames differ from the given ones only by the orientation within the tangent plane
+    assert _mre(img_derived, img) < 0.5
+
+
 def test_directional_light_and_light_selection_parity(ctx, oracle):
     """dDirectionalLight (delta: MIS weights 1, no BSDF-sampled visibility
     rays) as light 0 of the room open to the sky, in both modes; and
