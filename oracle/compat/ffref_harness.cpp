@@ -398,6 +398,34 @@ void ffref_spec_sample(const float* mat8, const float* isect6, const float* wo3,
 
 double ffref_power_heuristic(int nf, double f, int ng, double g) { return power_heuristic(nf, f, ng, g); }
 
+// get_albedo / get_roughness / get_metallic / get_normal (dMaterial.cu:10-88)
+// with material textures.  mat8: base colour[3], fresnel[3], roughness and
+// metallic factors; tex5: texture objects (ffref_tex_create) for the base
+// colour, roughness, metallic, metallic-roughness and normal slots, -1 none;
+// isect11: texcoord[2], normal[3], tangent[3], bitangent[3] (as dTriangle::hit
+// leaves them).  out8: albedo[3], roughness, metallic, normal[3].
+void ffref_surface(const float* mat8, const int* tex5, const float* isect11, float* out8)
+{
+    dMaterial m;
+    Isect is;
+    fill(m, is, mat8, isect11);   // position / normal slots overwritten below
+    m.baseColorTexture = tex5[0];
+    m.roughnessTexture = tex5[1];
+    m.metallicTexture = tex5[2];
+    m.metallicRoughnessTexture = tex5[3];
+    m.normalTexture = tex5[4];
+    is.texcoord = make_float2(isect11[0], isect11[1]);
+    is.normal = make_float3(isect11[2], isect11[3], isect11[4]);
+    is.tangent = make_float3(isect11[5], isect11[6], isect11[7]);
+    is.bitangent = make_float3(isect11[8], isect11[9], isect11[10]);
+    const float3 a = get_albedo(is);
+    const float r = get_roughness(is);
+    const float mt = get_metallic(is);
+    const float3 n = get_normal(is);
+    const float vals[8] = {a.x, a.y, a.z, r, mt, n.x, n.y, n.z};
+    std::memcpy(out8, vals, sizeof(vals));
+}
+
 // ------------------------------------------------------------------ camera
 // gen_ray (dCamera.cu:10-36) for pixel (px, py): cam = inv_view_proj[16]
 // (Matrix4x4 m[i][j] at 4*i+j), lens_radius, f.  out = o[3], d[3].

@@ -120,6 +120,12 @@ typedef struct {
  * Returns 0, or 1 for an invalid light selection. */
 int ffo_render(const ffo_render_desc* d, double* out_rgb, uint64_t* stats);
 
+/* Material texture reads (get_albedo / get_roughness / get_metallic /
+ * get_normal, dMaterial.cu:10-88) at one intersection: isect11 = texcoord[2],
+ * normal[3], tangent[3], bitangent[3]; out8 = albedo[3], roughness, metallic,
+ * normal[3]. */
+void ffo_probe_surface(const ffo_material* mm, const ffo_texture* textures, const float* isect11, float* out8);
+
 /* Environment tables of kernel.cu:65-149 (marginal[h], cond[h*w], pdf[h*w]). */
 void ffo_env_build(const float* rgb, int w, int h, double* marginal, double* cond, float* pdf, double* denom);
 

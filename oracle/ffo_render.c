@@ -604,6 +604,47 @@ static light_ctx select_light(const light_ctx* base, uint32_t key, uint32_t L)
 }
 
 /* One path sample; returns its radiance (sum of the contributions). */
+/* get_albedo / get_roughness / get_metallic (dMaterial.cu:10-60) at texcoord
+ * (tu, tv): the base-colour texture; the packed metallic-roughness texture
+ * first (roughness y, metallic z), then the roughness / metallic textures
+ * (x), then the factors already in sf. */
+static void resolve_textures(const ffo_material* mm, const ffo_texture* textures, float tu, float tv, surf_t* sf)
+{
+    if (mm->base_color_tex >= 0) {
+        const ffo_texture* tx = &textures[mm->base_color_tex];
+        sf->albedo = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv);
+    }
+    if (mm->metallic_roughness_tex >= 0) {
+        const ffo_texture* tx = &textures[mm->metallic_roughness_tex];
+        v3 c = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv);
+        sf->roughness = hmax(c.y, 0.01f);
+        sf->metallic = c.z;
+    } else {
+        if (mm->roughness_tex >= 0) {
+            const ffo_texture* tx = &textures[mm->roughness_tex];
+            sf->roughness = hmax(tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv).x, 0.01f);
+        }
+        if (mm->metallic_tex >= 0) {
+            const ffo_texture* tx = &textures[mm->metallic_tex];
+            sf->metallic = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv).x;
+        }
+    }
+}
+
+/* get_normal (dMaterial.cu:61-88) under a normal texture: texel c mapped to
+ * q = c * 2 - 1, then the Matrix4x4(T, B, N) * float3 product of
+ * dMatrix.cuh:70-78: ((T q.x + B q.y) + N q.z) + 0 over w = ((0 + 0) + 0) + 1,
+ * normalised. */
+static v3 normal_from_map(v3 T, v3 B, v3 N, v3 c)
+{
+    v3 q = {c.x * 2.f - 1.f, c.y * 2.f - 1.f, c.z * 2.f - 1.f};
+    v3 o3 = {((T.x * q.x + B.x * q.y) + N.x * q.z) + 0.f, ((T.y * q.x + B.y * q.y) + N.y * q.z) + 0.f,
+             ((T.z * q.x + B.z * q.y) + N.z * q.z) + 0.f};
+    float w3 = ((0.f * q.x + 0.f * q.y) + 0.f * q.z) + 1.f;
+    v3 r = {o3.x / w3, o3.y / w3, o3.z / w3};
+    return normalize(r);
+}
+
 static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int px, int py, uint32_t sample,
                         double out[3], uint64_t* n_ext, uint64_t* n_sh)
 {
@@ -699,44 +740,15 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int 
             float wuv = (1.f - u) - v;
             float tu = u * tc[2] + v * tc[4] + wuv * tc[0];
             float tv = u * tc[3] + v * tc[5] + wuv * tc[1];
-            if (mm->base_color_tex >= 0) {
-                const ffo_texture* tx = &d->textures[mm->base_color_tex];
-                sf.albedo = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv);
-            }
-            /* get_roughness / get_metallic (dMaterial.cu:25-60): the packed
-             * metallic-roughness texture first (y, z), then roughness / metallic
-             * textures (x), then the factors */
-            if (mm->metallic_roughness_tex >= 0) {
-                const ffo_texture* tx = &d->textures[mm->metallic_roughness_tex];
-                v3 c = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv);
-                sf.roughness = hmax(c.y, 0.01f);
-                sf.metallic = c.z;
-            } else {
-                if (mm->roughness_tex >= 0) {
-                    const ffo_texture* tx = &d->textures[mm->roughness_tex];
-                    sf.roughness = hmax(tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv).x, 0.01f);
-                }
-                if (mm->metallic_tex >= 0) {
-                    const ffo_texture* tx = &d->textures[mm->metallic_tex];
-                    sf.metallic = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv).x;
-                }
-            }
-            /* get_normal (dMaterial.cu:61-88): TBN from the tangent and bitangent
-             * interpolated as the normal (dTriangle.cu:94-96), texel c mapped to
-             * q = c * 2 - 1, then Matrix4x4 * float3 (dMatrix.cuh:70-78):
-             * ((T q.x + B q.y) + N q.z) + 0 over w = ((0 + 0) + 0) + 1 */
+            resolve_textures(mm, d->textures, tu, tv, &sf);
             if (mm->normal_tex >= 0 && d->tangents && d->bitangents) {
+                /* the frame interpolated as the normal is (dTriangle.cu:94-96) */
                 const float* tg = d->tangents + 9 * (size_t)prim;
                 const float* bt = d->bitangents + 9 * (size_t)prim;
                 v3 T = normalize(add(add(smul(u, ld3(tg + 3)), smul(v, ld3(tg + 6))), smul((1.f - u) - v, ld3(tg))));
                 v3 B = normalize(add(add(smul(u, ld3(bt + 3)), smul(v, ld3(bt + 6))), smul((1.f - u) - v, ld3(bt))));
                 const ffo_texture* tx = &d->textures[mm->normal_tex];
-                v3 c = tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv);
-                v3 q = {c.x * 2.f - 1.f, c.y * 2.f - 1.f, c.z * 2.f - 1.f};
-                v3 o3 = {((T.x * q.x + B.x * q.y) + ng.x * q.z) + 0.f, ((T.y * q.x + B.y * q.y) + ng.y * q.z) + 0.f,
-                         ((T.z * q.x + B.z * q.y) + ng.z * q.z) + 0.f};
-                float w3 = ((0.f * q.x + 0.f * q.y) + 0.f * q.z) + 1.f;
-                n = normalize((v3){o3.x / w3, o3.y / w3, o3.z / w3});
+                n = normal_from_map(T, B, ng, tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv));
             }
         }
         const surf_t* mat = &sf;
@@ -939,4 +951,28 @@ void ffo_probe_area(const ffo_area_light* L, const float* pos3, const float* u2,
     out[9] = rect_pdf(&r, ld3(pos3), up);
     v3 o = V(ray8[0], ray8[1], ray8[2]), dd = V(ray8[4], ray8[5], ray8[6]);
     out[10] = (float)rect_hit(&r, o, dd);
+}
+
+/* Probe of the material texture reads: isect11 = texcoord[2], normal[3],
+ * tangent[3], bitangent[3] (as dTriangle::hit leaves them); out8 = albedo[3],
+ * roughness, metallic, normal[3]. */
+void ffo_probe_surface(const ffo_material* mm, const ffo_texture* textures, const float* isect11, float* out8)
+{
+    surf_t sf;
+    sf.albedo = ld3(mm->base_color);
+    sf.fresnel = ld3(mm->fresnel);
+    sf.roughness = mm->roughness;
+    sf.metallic = mm->metallic;
+    sf.kind = mm->kind;
+    resolve_textures(mm, textures, isect11[0], isect11[1], &sf);
+    v3 N = ld3(isect11 + 2);
+    if (mm->normal_tex >= 0) {
+        const ffo_texture* tx = &textures[mm->normal_tex];
+        N = normal_from_map(ld3(isect11 + 5), ld3(isect11 + 8), N,
+                            tex_bilinear(tx->rgb, tx->width, tx->height, isect11[0], isect11[1]));
+    }
+    st3(out8, sf.albedo);
+    out8[3] = sf.roughness;
+    out8[4] = sf.metallic;
+    st3(out8 + 5, N);
 }

@@ -54,6 +54,8 @@ def load_ref():
         "ffref_area_hit": (C.c_int, [P, P]),
         "ffref_bvh_build": (P, [P, C.c_int, C.POINTER(C.c_double)]),
         "ffref_bvh_trace": (None, [P, P, C.c_long, P, C.c_int, C.c_int]),
+        "ffref_tex_create": (C.c_ulonglong, [P, C.c_int, C.c_int, C.c_int]),
+        "ffref_surface": (None, [P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -289,6 +291,37 @@ def main():
     bh = np.zeros((len(br), 2), np.float32)
     lib.ffref_bvh_trace(hb, p(br), len(br), p(bh), 0, 8)
     out.update(bvh_rays=br, bvh_hits=bh)
+
+    # ---- material texture reads (get_albedo / get_roughness / get_metallic /
+    # get_normal): random textures, materials with random slots, intersections
+    # with random texcoords (wrapping) and orthonormal-ish frames
+    srng = np.random.default_rng(777)
+    ntex = 6
+    stex = [srng.uniform(0.0, 1.0, (int(srng.integers(2, 9)), int(srng.integers(2, 9)), 3)).astype(np.float32)
+            for _ in range(ntex - 1)]
+    stex.append(scenes.normal_texture(16, seed=5))
+    tex_ids = [lib.ffref_tex_create(p(np.ascontiguousarray(t)), t.shape[1], t.shape[0], 3) for t in stex]
+    ns = 400
+    smat = np.zeros((ns, 8), np.float32)
+    smat[:, 0:3] = srng.uniform(0.1, 0.9, (ns, 3))
+    smat[:, 3:6] = 0.04
+    smat[:, 6] = srng.uniform(0.05, 1.0, ns)
+    smat[:, 7] = srng.uniform(0.0, 1.0, ns)
+    sslots = np.where(srng.uniform(size=(ns, 5)) < 0.5, srng.integers(0, ntex - 1, (ns, 5)), -1).astype(np.int32)
+    sslots[:, 4] = np.where(srng.uniform(size=ns) < 0.6, ntex - 1, -1)   # normal slot: the normal texture
+    sisect = np.zeros((ns, 11), np.float32)
+    sisect[:, 0:2] = srng.uniform(-0.5, 1.5, (ns, 2))
+    nrm = unit(srng, ns)
+    tan = unit(srng, ns)
+    tan = tan - nrm * (tan * nrm).sum(1, keepdims=True)
+    tan /= np.linalg.norm(tan, axis=1, keepdims=True)
+    sisect[:, 2:5], sisect[:, 5:8], sisect[:, 8:11] = nrm, tan, np.cross(nrm, tan)
+    sout = np.zeros((ns, 8), np.float32)
+    for i in range(ns):
+        ids = np.array([tex_ids[k] if k >= 0 else -1 for k in sslots[i]], np.int32)
+        lib.ffref_surface(p(smat[i]), p(ids), p(sisect[i]), p(sout[i]))
+    out.update(surf_mat=smat, surf_slots=sslots, surf_isect=sisect, surf_out=sout,
+               **{f"surf_tex{k}": t for k, t in enumerate(stex)})
 
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT} ({OUT.stat().st_size / 1e6:.2f} MB)")

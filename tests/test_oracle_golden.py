@@ -37,6 +37,7 @@ def lib(oracle):
         "ffo_probe_camera": (None, [P, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, P, P, P]),
         "ffo_probe_env": (None, [P, C.c_int, C.c_int, P, P, P, P, C.c_float, C.c_float, P, P]),
         "ffo_probe_area": (None, [P, P, P, P, P, P, P]),
+        "ffo_probe_surface": (None, [P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -189,3 +190,27 @@ def test_reference_bvh_agrees_with_brute_force(g, oracle):
     assert same.mean() >= 0.9999, same.mean()
     hit = same & (brute["prim"] >= 0)
     assert np.array_equal(ref[hit, 0], brute["t"][hit])
+
+
+def test_material_textures_and_normal_map(g, lib, oracle):
+    """get_albedo / get_roughness / get_metallic / get_normal with every
+    texture slot (base colour, roughness, metallic, packed metallic-roughness,
+    tangent-space normal) at random texcoords (wrapping) and tangent frames,
+    bit for bit against the reference's own routines."""
+    texs = [np.ascontiguousarray(g[f"surf_tex{k}"]) for k in range(6)]
+    tdesc = (oracle.ffo_texture * len(texs))()
+    for i, t in enumerate(texs):
+        tdesc[i].rgb, tdesc[i].width, tdesc[i].height = t.ctypes.data, t.shape[1], t.shape[0]
+    mats, slots, isect, ref = g["surf_mat"], g["surf_slots"], g["surf_isect"], g["surf_out"]
+    got = np.zeros_like(ref)
+    for i in range(len(mats)):
+        m = oracle.ffo_material()
+        for k in range(3):
+            m.base_color[k] = mats[i, k]
+            m.fresnel[k] = mats[i, 3 + k]
+        m.roughness, m.metallic, m.kind = float(mats[i, 6]), float(mats[i, 7]), 0
+        (m.base_color_tex, m.roughness_tex, m.metallic_tex, m.metallic_roughness_tex,
+         m.normal_tex) = (int(x) for x in slots[i])
+        lib.ffo_probe_surface(C.byref(m), C.cast(tdesc, C.c_void_p), p(np.ascontiguousarray(isect[i])), p(got[i]))
+    assert (slots[:, 4] >= 0).sum() > 100 and (slots[:, 3] >= 0).sum() > 100
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), ulps(got, ref).max()
