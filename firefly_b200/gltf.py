@@ -11,9 +11,18 @@ scene's nodes, with node matrices or TRS composed root to leaf; positions
 transformed by the node matrix and normals by its inverse transpose;
 missing normals generated as area-weighted vertex normals; texture
 coordinates flipped in v (1 - v) as aiProcess_FlipUVs does; one material per
-glTF material (base colour, roughness and metallic factors; image textures
-are not decoded); the first perspective camera found becomes the scene
-camera.
+glTF material (base colour, roughness and metallic factors, and the base
+colour, metallic-roughness and normal textures, Scene.cpp:206-212); tangent
+frames from TANGENT attributes (bitangent = cross(N, T) * w); the first
+perspective camera found becomes the scene camera.
+
+Images (PNG, JPEG: whatever PIL decodes) become float RGB textures of
+byte / 255 (16-bit images / 65535), rows flipped as the reference's loader
+flips them (stbi_set_flip_vertically_on_load, dTexture.cu:115-117; with the
+uv flip the two cancel).  A texture replaces its factor, as the reference's
+get_* functions read it (dMaterial.cu:10-60); no sRGB decoding is applied
+(the reference's loader applies none).  The reference decodes with
+stb_image, which is not in its checkout: the decoded values are not pinned.
 """
 from __future__ import annotations
 
@@ -112,20 +121,63 @@ def _smooth_normals(P: np.ndarray, I: np.ndarray) -> np.ndarray:
     return (N / np.where(ln > 0, ln, 1.0)).astype(np.float32)
 
 
+def _image(doc, bufs, base: Path, idx: int) -> np.ndarray:
+    """Image idx decoded to float32 (h, w, 3), rows flipped as stb flips them."""
+    import io
+
+    from PIL import Image
+    img = doc["images"][idx]
+    if "bufferView" in img:
+        bv = doc["bufferViews"][img["bufferView"]]
+        raw = bufs[bv["buffer"]][bv.get("byteOffset", 0):bv.get("byteOffset", 0) + bv["byteLength"]]
+    elif img.get("uri", "").startswith("data:"):
+        raw = base64.b64decode(img["uri"].split(",", 1)[1])
+    else:
+        raw = (base / img["uri"]).read_bytes()
+    im = Image.open(io.BytesIO(raw))
+    a = np.asarray(im)
+    scale = 65535.0 if a.dtype == np.uint16 or im.mode.startswith("I;16") else 255.0
+    a = a.astype(np.float64) / scale
+    if a.ndim == 2:
+        a = np.repeat(a[..., None], 3, -1)
+    elif a.shape[2] == 2:            # luminance + alpha
+        a = np.repeat(a[..., :1], 3, -1)
+    a = a[..., :3]
+    return np.ascontiguousarray(a[::-1]).astype(np.float32)
+
+
 def load(path, width: int = 512, height: int = 512, kind=A.FF_MAT_MIX) -> scenes.Scene:
     """A scenes.Scene from a glTF 2.0 file (lights come from the caller)."""
     path = Path(path)
     doc, bin_chunk = _load(path)
     bufs = _buffers(doc, path.parent, bin_chunk)
+    textures, tex_slot = [], {}
+
+    def slot(info):
+        """Scene texture index of a glTF textureInfo, -1 when absent."""
+        if not info or "index" not in info:
+            return -1
+        src = doc["textures"][info["index"]].get("source")
+        if src is None:
+            return -1
+        if src not in tex_slot:
+            tex_slot[src] = len(textures)
+            textures.append(_image(doc, bufs, path.parent, src))
+        return tex_slot[src]
+
     mats = []
     for m in doc.get("materials", []):
         pbr = m.get("pbrMetallicRoughness", {})
         bc = pbr.get("baseColorFactor", [1, 1, 1, 1])
         mats.append(scenes.material(bc[:3], kind=kind, roughness=float(pbr.get("roughnessFactor", 1.0)),
-                                    metallic=float(pbr.get("metallicFactor", 1.0))))
+                                    metallic=float(pbr.get("metallicFactor", 1.0)),
+                                    base_color_tex=slot(pbr.get("baseColorTexture")),
+                                    metallic_roughness_tex=slot(pbr.get("metallicRoughnessTexture")),
+                                    normal_tex=slot(m.get("normalTexture"))))
     default_mat = len(mats)
     mats.append(scenes.material((0.8, 0.8, 0.8), kind=kind))
-    Ps, Ns, UVs, Is, Ms = [], [], [], [], []
+    Ps, Ns, UVs, Is, Ms, Ts, Bs, Ls = [], [], [], [], [], [], [], []
+    any_tangents = False
     base = 0
     camera = None
     scene_idx = doc.get("scene", 0)
@@ -170,23 +222,45 @@ def load(path, width: int = 512, height: int = 512, kind=A.FF_MAT_MIX) -> scenes
                 UV[:, 1] = 1.0 - UV[:, 1]                       # aiProcess_FlipUVs
             else:
                 UV = np.zeros((len(P), 2), np.float32)
+            if "TANGENT" in at:
+                T4 = _accessor(doc, bufs, at["TANGENT"]).astype(np.float64)
+                T = T4[:, :3] @ M[:3, :3].T
+                T /= np.maximum(np.linalg.norm(T, axis=1, keepdims=True), 1e-30)
+                B = np.cross(N.astype(np.float64), T) * np.where(T4[:, 3:4] < 0.0, -1.0, 1.0)
+                Ts.append(T.astype(np.float32))
+                Bs.append(B.astype(np.float32))
+                any_tangents = True
+            else:
+                Ts.append(None)
+                Bs.append(None)
             Ps.append(Pw)
             Ns.append(N)
             UVs.append(UV)
             Is.append(I + base)
+            Ls.append(I)
             Ms.append(np.full(len(I), prim.get("material", default_mat), np.uint32))
             base += len(P)
     if not Ps:
         raise ValueError("the glTF scene has no triangle primitives")
+    tangents = bitangents = None
+    if any_tangents:
+        # primitives without TANGENT get the uv-derived frame
+        for k in range(len(Ts)):
+            if Ts[k] is None:
+                Ts[k], Bs[k] = scenes.vertex_tangents(Ps[k], Ls[k], UVs[k], Ns[k])
+        tangents, bitangents = np.concatenate(Ts), np.concatenate(Bs)
     return scenes.Scene(positions=np.concatenate(Ps), indices=np.concatenate(Is).astype(np.uint32),
                         normals=np.concatenate(Ns), texcoords=np.concatenate(UVs),
-                        material_ids=np.concatenate(Ms), materials=mats, camera=camera, width=width, height=height)
+                        material_ids=np.concatenate(Ms), materials=mats, camera=camera, width=width, height=height,
+                        textures=textures, tangents=tangents, bitangents=bitangents)
 
 
 def save(path, scene: scenes.Scene):
-    """Write the scene's mesh and material factors as a .glb (one node, one
-    mesh, one primitive per material): the inverse of load() for tests and
-    for exporting procedural scenes."""
+    """Write the scene's mesh, tangent frame, material factors and its base
+    colour, metallic-roughness and normal textures (PNG, 8 bits per channel)
+    as a .glb (one node, one mesh, one primitive per material): the inverse of
+    load() for tests and for exporting procedural scenes.  Single-channel
+    roughness and metallic textures have no core glTF slot and are left out."""
     path = Path(path)
     blobs, views, accessors, prims = [], [], [], []
 
@@ -214,18 +288,56 @@ def save(path, scene: scenes.Scene):
         uv = scene.texcoords.astype(np.float32).copy()
         uv[:, 1] = 1.0 - uv[:, 1]
         attrs["TEXCOORD_0"] = add(uv, 5126, "VEC2", 34962)
+    if getattr(scene, "tangents", None) is not None and scene.normals is not None:
+        T = np.asarray(scene.tangents, np.float64)
+        w = np.where((np.cross(np.asarray(scene.normals, np.float64), T) * np.asarray(scene.bitangents, np.float64))
+                     .sum(1, keepdims=True) < 0.0, -1.0, 1.0)
+        attrs["TANGENT"] = add(np.concatenate([T, w], 1).astype(np.float32), 5126, "VEC4", 34962)
     mids = scene.material_ids if scene.material_ids is not None else np.zeros(scene.num_triangles, np.uint32)
     for m in np.unique(mids):
         idx = scene.indices[mids == m].reshape(-1).astype(np.uint32)
         prims.append({"attributes": attrs, "indices": add(idx, 5125, "SCALAR", 34963), "material": int(m), "mode": 4})
-    mats = [{"pbrMetallicRoughness": {"baseColorFactor": [float(m.base_color[0]), float(m.base_color[1]),
-                                                          float(m.base_color[2]), 1.0],
-                                      "roughnessFactor": float(m.roughness), "metallicFactor": float(m.metallic)}}
-            for m in scene.materials]
+    images, textures, img_of = [], [], {}
+
+    def tex_ref(k):
+        """glTF textureInfo for scene texture k (PNG of round(255 t), rows
+        flipped back), or None."""
+        if k < 0:
+            return None
+        if k not in img_of:
+            import io
+
+            from PIL import Image
+            t = np.clip(np.asarray(scene.textures[k], np.float64)[::-1], 0.0, 1.0)
+            buf = io.BytesIO()
+            Image.fromarray(np.round(t * 255.0).astype(np.uint8), "RGB").save(buf, format="PNG")
+            raw = buf.getvalue()
+            off = sum(len(b) for b in blobs)
+            blobs.append(raw + b"\0" * ((-len(raw)) % 4))
+            views.append({"buffer": 0, "byteOffset": off, "byteLength": len(raw)})
+            images.append({"bufferView": len(views) - 1, "mimeType": "image/png"})
+            textures.append({"source": len(images) - 1})
+            img_of[k] = len(textures) - 1
+        return {"index": img_of[k]}
+
+    mats = []
+    for m in scene.materials:
+        pbr = {"baseColorFactor": [float(m.base_color[0]), float(m.base_color[1]), float(m.base_color[2]), 1.0],
+               "roughnessFactor": float(m.roughness), "metallicFactor": float(m.metallic)}
+        if tex_ref(m.base_color_tex):
+            pbr["baseColorTexture"] = tex_ref(m.base_color_tex)
+        if tex_ref(m.metallic_roughness_tex):
+            pbr["metallicRoughnessTexture"] = tex_ref(m.metallic_roughness_tex)
+        mat = {"pbrMetallicRoughness": pbr}
+        if tex_ref(m.normal_tex):
+            mat["normalTexture"] = tex_ref(m.normal_tex)
+        mats.append(mat)
     binary = b"".join(blobs)
     doc = {"asset": {"version": "2.0", "generator": "firefly_b200.gltf"}, "scene": 0, "scenes": [{"nodes": [0]}],
            "nodes": [{"mesh": 0}], "meshes": [{"primitives": prims}], "materials": mats,
            "buffers": [{"byteLength": len(binary)}], "bufferViews": views, "accessors": accessors}
+    if images:
+        doc["images"], doc["textures"] = images, textures
     js = json.dumps(doc).encode("utf-8")
     js += b" " * ((-len(js)) % 4)
     out = struct.pack("<III", 0x46546C67, 2, 12 + 8 + len(js) + 8 + len(binary))

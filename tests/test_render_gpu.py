@@ -189,6 +189,29 @@ def test_normal_map_and_packed_textures_change_the_image(ctx):
     assert _mre(img_derived, img) < 0.5
 
 
+def test_gltf_textured_round_trip_renders_the_same(ctx, tmp_path):
+    """A scene with base-colour, metallic-roughness and normal textures and a
+    tangent frame, written to .glb and read back, renders the same image."""
+    import firefly_b200 as ff
+    from firefly_b200 import gltf
+    scn = scenes.pbr_textured_room(seed=3, width=48, height=48, tex_res=32)
+    scn.textures = [(np.round(np.clip(t, 0.0, 1.0) * 255.0) / 255.0).astype(np.float32) for t in scn.textures]
+    for m in scn.materials:
+        m.roughness_tex = -1
+        m.metallic_tex = -1
+    gltf.save(tmp_path / "pbr.glb", scn)
+    got = gltf.load(tmp_path / "pbr.glb", 48, 48)
+    for a, b in zip(scn.materials, got.materials):
+        b.kind = a.kind
+    got.env_rgb, got.camera = scn.env_rgb, scn.camera
+    kw = dict(light=-1, max_depth=4, rr_depth=3, seed=5, mode=ff.FF_MODE_CORRECTED)
+    a, _, _ = _gpu_render(ctx, scn, 48, 48, 8, **kw)
+    b, _, _ = _gpu_render(ctx, got, 48, 48, 8, **kw)
+    mre = _mre(b, a)
+    print(f"[gltf] textured round trip: mre={mre:.3e}")
+    assert mre < 1e-4
+
+
 def test_directional_light_and_light_selection_parity(ctx, oracle):
     """dDirectionalLight (delta: MIS weights 1, no BSDF-sampled visibility
     rays) as light 0 of the room open to the sky, in both modes; and
