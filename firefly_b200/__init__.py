@@ -173,8 +173,10 @@ class dScene:
                        megakernel: bool = False, profile: bool = False) -> dict:
         """Path-replay adjoint of PathTracer.draw(mode=FF_MODE_CORRECTED) with
         the same settings: adds dL/d(texture texels) to grad_texture,
-        dL/d(env texels) to grad_env and dL/d(roughness texels, channel 0) to
-        grad_roughness (float32 host arrays shaped like their textures), given
+        dL/d(env texels) to grad_env and dL/d(roughness texels) to
+        grad_roughness (float32 host arrays shaped like their textures;
+        channel 0 where a material reads the texture as its roughness_tex,
+        channel 1 where it is the packed metallic_roughness_tex), given
         d_image = dL/dI of the mean-radiance image (height, width, 3).
         The replay runs on the wavefront stages; megakernel=True runs the
         one-thread-per-sample replay instead, store_all=True the store-all

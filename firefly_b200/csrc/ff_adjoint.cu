@@ -125,6 +125,7 @@ struct VertexRec {
     float u, v;         // texcoords
     bool albedo;        // the vertex takes an albedo gradient
     bool rough;         // the vertex takes a roughness gradient
+    int8_t rough_ch;    // channel of the roughness texture it reads (0 or 1)
     float g_imm;        // dI . d(own terms)/dr
     float3 dext;        // d/dr log(ext_f)
     float3 L_after;     // radiance added up to and including the vertex's own terms
@@ -243,9 +244,8 @@ __device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_
         const bool tex_grad = surf.kind == FF_MAT_DIFFUSE && mm.base_color_tex >= 0 && mm.base_color_tex == a.texture;
         // roughness gradient: GGX surfaces whose roughness comes from the
         // texture (above the 0.01 floor of resolve_surface, where it is flat)
-        const bool rough_grad = ROUGH && grad && surf.kind != FF_MAT_DIFFUSE && mm.metallic_roughness_tex < 0 &&
-                                mm.roughness_tex >= 0 && mm.roughness_tex == a.rough_texture &&
-                                surf.roughness > 0.01f;
+        const int rch = ROUGH && grad && surf.kind != FF_MAT_DIFFUSE ? rough_channel(mm, a.rough_texture) : -1;
+        const bool rough_grad = rch >= 0 && surf.roughness > 0.01f;
         RoughTerms rt;
         float3 rimm = make_float3(0.f, 0.f, 0.f);
         float3 L_after = Lacc;
@@ -262,7 +262,7 @@ __device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_
             const float3 Lgt = L_total - L_after;
             const float g = dot3(dI, rimm + Lgt * rt.dext);
             const FFTexView tv = a.tex[a.rough_texture];
-            atom_r += scatter_footprint1(a.grad_rough, footprint(tv.width, tv.height, tuv.x, tuv.y), g);
+            atom_r += scatter_footprint1(a.grad_rough, footprint(tv.width, tv.height, tuv.x, tuv.y), g, rch);
         }
         if (mode == 1 && tex_grad) {
             const FFTexView tv = a.tex[a.texture];
@@ -277,6 +277,7 @@ __device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_
             r.v = tuv.y;
             r.albedo = tex_grad;
             r.rough = rough_grad;
+            r.rough_ch = (int8_t)rch;
             if (rough_grad) {
                 r.g_imm = dot3(dI, rimm);
                 r.dext = rt.dext;
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(ADJ a)
                 if (ROUGH && r.rough) {
                     const float g = r.g_imm + dot3(dI, (Ls - r.L_after) * r.dext);
                     const FFTexView tv = a.tex[a.rough_texture];
-                    atom_r += scatter_footprint1(a.grad_rough, footprint(tv.width, tv.height, r.u, r.v), g);
+                    atom_r += scatter_footprint1(a.grad_rough, footprint(tv.width, tv.height, r.u, r.v), g, r.rough_ch);
                 }
                 if (!r.albedo) continue;
                 const FFTexView tv = a.tex[a.texture];

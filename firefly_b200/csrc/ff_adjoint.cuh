@@ -74,25 +74,36 @@ __device__ __forceinline__ uint32_t scatter_footprint(float* grad, const Footpri
     return n;
 }
 
-// Scalar variant for the roughness channel: adds to grad[3*idx] only.
-__device__ __forceinline__ uint32_t scatter_add1(float* grad, uint32_t idx, float v)
+// Scalar variant for the roughness channel: adds to grad[3*idx + ch] only.
+__device__ __forceinline__ uint32_t scatter_add1(float* grad, uint32_t idx, float v, int ch)
 {
     const uint32_t active = __activemask();
     const uint32_t peers = __match_any_sync(active, idx);
     float sum = 0.f;
     for (uint32_t m = peers; m; m &= m - 1) sum += __shfl_sync(peers, v, __ffs(m) - 1);
     if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) {
-        atomicAdd(grad + 3 * (size_t)idx, sum);
+        atomicAdd(grad + 3 * (size_t)idx + ch, sum);
         return 1u;
     }
     return 0u;
 }
-__device__ __forceinline__ uint32_t scatter_footprint1(float* grad, const Footprint& f, float g)
+__device__ __forceinline__ uint32_t scatter_footprint1(float* grad, const Footprint& f, float g, int ch)
 {
     uint32_t n = 0;
 #pragma unroll 1
-    for (int i = 0; i < 4; ++i) n += scatter_add1(grad, f.idx[i], g * f.w[i]);
+    for (int i = 0; i < 4; ++i) n += scatter_add1(grad, f.idx[i], g * f.w[i], ch);
     return n;
+}
+
+// Which channel of texture `adj` feeds the material's roughness, as
+// resolve_surface reads it (get_roughness, dMaterial.cu:25-42): y of the
+// packed metallic-roughness texture when the material has one, else x of the
+// single-channel roughness texture; -1 when the roughness does not come
+// from `adj`.
+__device__ __forceinline__ int rough_channel(const ff_material& m, int adj)
+{
+    if (m.metallic_roughness_tex >= 0) return m.metallic_roughness_tex == adj ? 1 : -1;
+    return (m.roughness_tex >= 0 && m.roughness_tex == adj) ? 0 : -1;
 }
 
 // Roughness derivative of one vertex's terms (detached sampling: directions,

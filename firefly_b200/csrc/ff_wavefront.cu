@@ -134,7 +134,7 @@ struct WF {
     float4* v_coef;              // c_nee / Le(wi): d c_nee / d Le
 };
 // flags of WF::v_albedo.w: which gradients the vertex takes
-constexpr uint32_t V_ALBEDO = 1u, V_ROUGH = 2u, V_ENV = 4u;
+constexpr uint32_t V_ALBEDO = 1u, V_ROUGH = 2u, V_ENV = 4u, V_ROUGH_Y = 8u;   // V_ROUGH_Y: roughness in channel y
 
 __device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
 __device__ __forceinline__ float4 f4(float3 v, float w = 0.f) { return make_float4(v.x, v.y, v.z, w); }
@@ -275,7 +275,8 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                                 const float3 L_after = xyz(acc) + lb * beta;
                                 const float g = dot3(dI, rimm + (Ltot - L_after) * rt.dext);
                                 const FFTexView tv = w.tex[w.adj_rough];
-                                touched_r += scatter_footprint1(w.grad_rough, footprint(tv.width, tv.height, uv.x, uv.y), g);
+                                touched_r += scatter_footprint1(w.grad_rough, footprint(tv.width, tv.height, uv.x, uv.y), g,
+                                                                (flags & V_ROUGH_Y) ? 1 : 0);
                             }
                             if ((flags & V_ENV) && vis) {
                                 // NEE term c_nee = coef * Le(wi): d/dLe = beta * coef
@@ -475,9 +476,9 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
                 if (KIND == FF_MAT_DIFFUSE && w.grad_tex && mm.base_color_tex >= 0 && mm.base_color_tex == w.adj_texture)
                     flags |= V_ALBEDO;
                 // roughness from the texture, above the 0.01 floor of resolve_surface (flat there)
-                if (KIND != FF_MAT_DIFFUSE && w.grad_rough && mm.metallic_roughness_tex < 0 && mm.roughness_tex >= 0 &&
-                    mm.roughness_tex == w.adj_rough && mat.roughness > 0.01f) {
-                    flags |= V_ROUGH;
+                const int rch = KIND != FF_MAT_DIFFUSE && w.grad_rough ? rough_channel(mm, w.adj_rough) : -1;
+                if (rch >= 0 && mat.roughness > 0.01f) {
+                    flags |= V_ROUGH | (rch == 1 ? V_ROUGH_Y : 0u);
                     const RoughTerms rt = rough_terms(o, n, wo, wi, mat.roughness);
                     w.v_nee[s] = f4(rt.nee);
                     w.v_spec[s] = f4(rt.spec);

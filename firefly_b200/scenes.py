@@ -541,7 +541,7 @@ def roughness_texture(res: int = 512, seed: int = 0, lo: float = 0.1, hi: float 
 
 def textured_room(seed: int = 0, width: int = 512, height: int = 512, albedo=None, env=None, tex_res: int = 512,
                   env_w: int = 256, env_h: int = 128, kind=A.FF_MAT_DIFFUSE, sphere_kind=None,
-                  roughness=None, sphere_metallic: float = 1.0) -> Scene:
+                  roughness=None, sphere_metallic: float = 1.0, packed: bool = False) -> Scene:
     """The small room opened to the sky (no ceiling) for inverse rendering:
     floor, walls and sphere carry one albedo texture (texture 0); the
     environment map lights the room.  `albedo` (res, res, 3) and `env`
@@ -552,7 +552,9 @@ def textured_room(seed: int = 0, width: int = 512, height: int = 512, albedo=Non
     the sphere gets its own material of that kind, base colour 0.8 and
     metallic `sphere_metallic`, whose roughness reads texture 1:
     `roughness` (res, res, 3), by default a seeded Perlin roughness in
-    [0.1, 0.6]."""
+    [0.1, 0.6].  With `packed` texture 1 is instead the sphere's glTF
+    metallic-roughness texture: channel x zero, y the roughness, z
+    `sphere_metallic`."""
     rng = np.random.default_rng(seed)
     lo, hi = np.array([-5, 0, -5], np.float32), np.array([5, 10, 5], np.float32)
     rP, rI = box_room(lo, hi)
@@ -589,9 +591,13 @@ def textured_room(seed: int = 0, width: int = 512, height: int = 512, albedo=Non
     textures = [tex]
     if sphere_kind is not None:
         mat_ids[len(rI):] = 1
+        rough = roughness_texture(tex_res, seed) if roughness is None else np.asarray(roughness, np.float32)
+        if packed:
+            rough = np.stack([np.zeros_like(rough[..., 0]), rough[..., 0],
+                              np.full_like(rough[..., 0], sphere_metallic)], -1).astype(np.float32)
         mats.append(material((0.8, 0.8, 0.8), kind=sphere_kind, roughness=0.5, metallic=sphere_metallic,
-                             roughness_tex=1))
-        textures.append(roughness_texture(tex_res, seed) if roughness is None else np.asarray(roughness, np.float32))
+                             roughness_tex=-1 if packed else 1, metallic_roughness_tex=1 if packed else -1))
+        textures.append(rough)
     sky = sky_env(env_w, env_h, seed=seed, sun_radiance=300.0, sun_diameter_deg=6.0) if env is None else env
     cam = make_camera(eye=(0.0, 8.0, 4.9), center=(center[0], center[1], center[2]), fovy=70.0, aspect=width / height,
                       near=0.05, far=60.0)

@@ -329,8 +329,9 @@ FF_API ff_status ff_render(ff_context* ctx, ff_scene* scene, const ff_render_set
  * radiance image I (width*height*3 floats).  Gradients are ADDED to
  * grad_texture (texels*3 floats of texture `texture`), grad_env
  * (env texels*3 floats) and grad_roughness (texels*3 floats of texture
- * `roughness_texture`; only channel 0, the one a material's roughness_tex
- * reads, receives gradients).  flags: FF_MEM_DEVICE when every pointer is
+ * `roughness_texture`: channel x where a material reads it as its
+ * roughness_tex, channel y where it is the material's packed
+ * metallic_roughness_tex; channel z, metallic, receives none).  flags: FF_MEM_DEVICE when every pointer is
  * device memory, FF_ADJOINT_STORE_ALL for the store-all reference variant. */
 typedef struct ff_adjoint_desc {
     uint32_t width, height;
