@@ -68,6 +68,12 @@ RENDER_LOGIC_BYTES_PER_HIT = 440
 # indices (16): 332 B.  Environment and material lookups are L2 gathers and
 # not counted.
 RENDER_SHADE_BYTES_PER_VERTEX = 332
+# Measured DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per unit
+# of each render stage: ncu over every launch of one timed 16-spp C2 step
+# (the 8.3M-slot pool of the 64-spp step; 36 frames), divided by the step's
+# units (consumed hits, shaded vertices, extension rays, shadow rays).
+RENDER_DRAM_BYTES_PER_UNIT = {"k_logic": 448.4, "k_shade (all kinds)": 599.1,
+                              "k_trace<closest> (extension queue)": 106.0, "k_trace<any> (shadow queue)": 51.2}
 RENDER = dict(width=1920, height=1080, spp=64, max_depth=8, rr_depth=3)
 
 
@@ -471,10 +477,13 @@ def run_render(args, ws, rank, local, dist):
     clocks.start()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     stats = []
+    # the NVTX range lets ncu capture exactly the timed steps (--nvtx --nvtx-include "timed/")
+    torch.cuda.nvtx.range_push("timed")
     t0.record(stream)
     for _ in range(args.steps):
         stats.append(step())
     t1.record(stream)
+    torch.cuda.nvtx.range_pop()
     barrier()
     clk = clocks.stop()
     ms_max = max_over_ranks(dist, dev, t0.elapsed_time(t1))
@@ -557,6 +566,14 @@ def run_render(args, ws, rank, local, dist):
         dom = max(stage, key=lambda k: stage[k][0])
         dms, dbytes, dnote = stage[dom]
         achieved = dbytes / (dms / 1e3) / 1e9
+        # DRAM traffic of one launch sequence (one frame) of the dominant
+        # stage: the measured bytes per unit times the frame's average units
+        units = {"k_logic": prof["extension_rays"], "k_shade (all kinds)": vertices,
+                 "k_trace<closest> (extension queue)": prof["extension_rays"],
+                 "k_trace<any> (shadow queue)": prof["shadow_rays"]}
+        frames = max(1, prof["frames"])
+        traffic = int(RENDER_DRAM_BYTES_PER_UNIT[dom] * units[dom] / frames)
+        alg_launch = int(dbytes / frames)
         cpu = None
         if not args.no_cpu:
             r = cpu_render_rate(scn, target_s=args.cpu_s, threads=os.cpu_count() or 1)
@@ -571,17 +588,25 @@ def run_render(args, ws, rank, local, dist):
             "config": {"workload": RENDER_WORKLOAD, **RENDER, "triangles": scn.num_triangles,
                        "bvh_nodes": ds.stats()["num_nodes"], "bvh_build_ms": round(ds.stats()["build_ms"], 2),
                        "mode": "corrected", "light": "environment (importance-sampled sky + sun)",
-                       "rays_per_step": int(rays / args.steps), "msamples_per_s": round(ws * samples / (ms_max / 1e3) / 1e6, 2),
+                       "rays_per_step": int(rays / args.steps),
+                       "units_per_step": {k: int(sum(s[k] for s in stats) / args.steps)
+                                          for k in ("extension_rays", "shadow_rays", "samples", "frames")},
+                       "msamples_per_s": round(ws * samples / (ms_max / 1e3) / 1e6, 2),
                        "frames_per_step": stats[-1]["frames"], "stage_ms_profiled_step": pstat,
                        "l2": "each step traces ~1.3G rays over a 0.27 GB scene; per-step state and queues ~0.5 GB",
                        "parallelism": (f"sample-parallel x{ws}: disjoint sample ranges of one frame, one film "
                                        f"all-reduce (41 MB) per step" if ws > 1 else "1 GPU"),
                        "image_finite": finite, "relmse_vs_16k_spp": conv, "trace_micro": trace},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 5), "traffic": None, "peak_source": peak_kind,
-                         "algorithmic_bytes": dnote,
+                         "frac": round(achieved / peak, 5), "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes": dnote, "algorithmic_bytes_per_launch": alg_launch,
+                         "traffic_note": ("bytes per frame's launch sequence of the dominant stage: ncu DRAM bytes "
+                                          "per unit of a 16-spp step on the same pool x this step's units per frame"),
                          "stages": {k: {"ms": round(v[0], 2), "achieved_gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1)
-                                        if v[0] > 0 else None} for k, v in stage.items()}},
+                                        if v[0] > 0 else None,
+                                        "algorithmic_bytes_per_unit": round(v[1] / max(1, units[k]), 1),
+                                        "dram_bytes_per_unit": RENDER_DRAM_BYTES_PER_UNIT[k]}
+                                    for k, v in stage.items()}},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 80,
                     "d2h_bytes_per_step": int(W * H * (16 + 4))},
