@@ -323,6 +323,69 @@ def trace_micro(ctx, ds_dev, args, rank, dev, stream, barrier, steps):
     return n * len(batches), per, total, batches, scn, ds, d_rays, d_hits
 
 
+L2_PROBE_SRC = b"""
+extern "C" __global__ void l2_read(const float4* __restrict__ a, unsigned long long n4, int reps, float* out)
+{
+    float acc = 0.f;
+    for (int r = 0; r < reps; ++r)
+        for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n4;
+             i += (unsigned long long)gridDim.x * blockDim.x) {
+            const float4 v = __ldcg(a + i);
+            acc += v.x + v.y + v.z + v.w;
+        }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+"""
+
+
+def l2_read_gbs(dev, mib=32, reps=40):
+    """Reference bandwidth for L2-resident reads: one kernel (compiled here
+    with NVRTC for sm_100a) reads a 32 MiB buffer, far below the 126 MB L2,
+    `reps` times with L1-bypassing 16-byte loads; bytes read per second, best
+    of 5 launches timed with CUDA events on the current stream.  None when
+    cuda-python is unavailable."""
+    import ctypes
+    import torch
+    try:
+        from cuda.bindings import driver as cu, nvrtc
+    except ImportError:
+        return None
+    err, prog = nvrtc.nvrtcCreateProgram(L2_PROBE_SRC, b"l2_probe.cu", 0, [], [])
+    opts = [b"--gpu-architecture=sm_100a"]
+    if nvrtc.nvrtcCompileProgram(prog, len(opts), opts)[0] != nvrtc.nvrtcResult.NVRTC_SUCCESS:
+        return None
+    _, size = nvrtc.nvrtcGetCUBINSize(prog)
+    cubin = b" " * size
+    nvrtc.nvrtcGetCUBIN(prog, cubin)
+    a = torch.ones(mib * 2 ** 18, dtype=torch.float32, device=dev)
+    threads, blocks = 256, torch.cuda.get_device_properties(dev).multi_processor_count * 8
+    out = torch.empty(threads * blocks, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize(dev)   # torch's context is current on this thread
+    err, mod = cu.cuModuleLoadData(cubin)
+    if err != cu.CUresult.CUDA_SUCCESS:
+        return None
+    _, fn = cu.cuModuleGetFunction(mod, b"l2_read")
+    cur = torch.cuda.current_stream(dev)
+    params = ((a.data_ptr(), a.numel() // 4, reps, out.data_ptr()),
+              (ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_void_p))
+
+    def launch():
+        r = cu.cuLaunchKernel(fn, blocks, 1, 1, threads, 1, 1, 0, cu.CUstream(cur.cuda_stream), params, 0)
+        assert r[0] == cu.CUresult.CUDA_SUCCESS, r
+    for _ in range(3):
+        launch()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        launch()
+        e1.record(cur)
+        e1.synchronize()
+        best = max(best, a.numel() * 4 * reps / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    cu.cuModuleUnload(mod)
+    return best
+
+
 # DRAM bytes per ray of k_trace launches, from an ncu capture at 4,194,304
 # rays per launch (profiles/k_trace_trace_micro.md); traffic scales with rays.
 TRACE_DRAM_BYTES_PER_RAY = {"coherent_closest": (134.470144e6 + 42.339328e6) / 4194304,
@@ -408,6 +471,24 @@ def run_trace(args, ws, rank, local, dist):
             rate, kind, desc, _ = cpu_trace_rate(batches, target_s=args.cpu_s, threads=os.cpu_count() or 1)
             cpu = {"value": round(rate, 3), "unit": "Mrays/s", "cores": os.cpu_count() or 1, "kind": kind, "sample": desc}
         ref_cuda = reference_cuda_trace(scn, batches, d_hits) if not args.no_ref_cuda else None
+        # traversal fetch bytes: node records and triangles each ray's traversal
+        # reads (counted by the same traversal on the device, outside the timed
+        # region), against an L2-resident copy
+        l2_ref = l2_read_gbs(dev)
+        fetch = {}
+        for k, (name, _, any_hit) in enumerate(batches):
+            wk = ds.trace_count(d_rays[k].data_ptr(), n, any_hit=any_hit)
+            fetch[name] = {"nodes_per_ray": round(wk["nodes"] / n, 3), "tris_per_ray": round(wk["tris"] / n, 3),
+                           "fetch_bytes_per_ray": round(wk["fetch_bytes_per_ray"], 1),
+                           "achieved_fetch_gbs": round(wk["fetch_bytes_per_ray"] * n / (per[k] / 1e3) / 1e9, 1)}
+        l2_fetch = {"per_batch": fetch, "l2_read_gbs": None if l2_ref is None else round(l2_ref, 1),
+                    "frac_of_l2_read": (None if l2_ref is None else
+                                        round(fetch[batches[k_dom][0]]["achieved_fetch_gbs"] / l2_ref, 4)),
+                    "node_bytes": wk["node_bytes"], "tri_bytes": wk["tri_bytes"],
+                    "note": ("fetched bytes = node records x node bytes + triangles tested x triangle bytes per ray; "
+                             "l2_read_gbs = a probe kernel reading a 32 MiB L2-resident buffer 40 times (L1 bypassed); "
+                             "the traversal's fetches are partly served by L1, so the fraction is an upper bound "
+                             "on its L2 load")}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
@@ -421,7 +502,7 @@ def run_trace(args, ws, rank, local, dist):
                          "traffic": int(TRACE_DRAM_BYTES_PER_RAY[batches[k_dom][0]] * n),
                          "traffic_source": "ncu dram__bytes_read+write of a 4,194,304-ray launch, scaled to the "
                                            "launch's rays (profiles/k_trace_trace_micro.md)",
-                         "peak_source": peak_kind, "bytes_per_ray": RAY_BYTES + HIT_BYTES},
+                         "peak_source": peak_kind, "bytes_per_ray": RAY_BYTES + HIT_BYTES, "l2_fetch": l2_fetch},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": int(rays_per_step * RAY_BYTES),
                     "d2h_bytes_per_step": int(rays_per_step * HIT_BYTES)},

@@ -229,6 +229,24 @@ class dScene:
         _check(lib().ff_trace(self.ctx.handle, self.handle, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr), flags),
                self.ctx.handle)
 
+    def trace_count(self, rays, n: int | None = None, any_hit: bool = False) -> dict:
+        """Traversal work of the rays (host array, or a device pointer with
+        n): node records fetched, triangles tested, and the fetched bytes per
+        ray (records times their sizes), for the same traversal ff_trace runs."""
+        flags = A.FF_TRACE_ANY if any_hit else A.FF_TRACE_CLOSEST
+        if isinstance(rays, int):
+            ptr, count = C.c_void_p(rays), int(n)
+            flags |= A.FF_MEM_DEVICE
+        else:
+            r = np.ascontiguousarray(rays.view(np.float32) if rays.dtype == RAY_DTYPE else rays,
+                                     np.float32).reshape(-1, 8)
+            ptr, count = _ptr(r), r.shape[0]
+        out = (C.c_uint64 * 4)()
+        _check(lib().ff_trace_count(self.ctx.handle, self.handle, ptr, count, flags, out), self.ctx.handle)
+        nodes, tris, node_b, tri_b = (int(v) for v in out)
+        return {"rays": count, "nodes": nodes, "tris": tris, "node_bytes": node_b, "tri_bytes": tri_b,
+                "fetch_bytes_per_ray": (nodes * node_b + tris * tri_b) / max(1, count)}
+
     def close(self):
         if getattr(self, "handle", None):
             if getattr(self.ctx, "handle", None):

@@ -151,6 +151,7 @@ SIGNATURES = {
     "ff_scene_get_stats": (C.c_int, [P, C.POINTER(ff_scene_stats)]),
     "ff_trace": (C.c_int, [P, P, P, C.c_uint64, P, C.c_uint32]),
     "ff_trace_host_noalloc": (C.c_int, [P, P, P, C.c_uint64, P, C.c_uint32]),
+    "ff_trace_count": (C.c_int, [P, P, P, C.c_uint64, C.c_uint32, P]),
     "ff_film_create": (C.c_int, [P, C.c_uint32, C.c_uint32, PP]),
     "ff_film_destroy": (C.c_int, [P]),
     "ff_film_clear": (C.c_int, [P]),

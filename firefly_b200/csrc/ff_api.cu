@@ -264,6 +264,48 @@ ff_status ff_trace(ff_context* ctx, const ff_scene* s, const ff_ray* rays, uint6
     });
 }
 
+ff_status ff_trace_count(ff_context* ctx, const ff_scene* s, const ff_ray* rays, uint64_t n, uint32_t flags,
+                         uint64_t* out)
+{
+    if (!ctx || !s || !out) return FF_ERR_INVALID_ARG;
+    if (n && !rays) return FF_ERR_INVALID_ARG;
+    if (s->ctx != ctx) {
+        ctx->last_error = "scene belongs to another context";
+        return FF_ERR_INVALID_ARG;
+    }
+    return guarded(ctx, [&] {
+        DeviceGuard g(ctx->device);
+        const bool any = (flags & FF_TRACE_ANY) != 0;
+        const ff_ray* d_rays = rays;
+        if (flags & FF_MEM_DEVICE) {
+            FF_REQUIRE((reinterpret_cast<uintptr_t>(rays) & 15) == 0, "device rays must be 16-byte aligned");
+        } else if (n) {
+            ctx->io_rays.alloc(sizeof(ff_ray) * n);
+            FF_CUDA_CHECK(cudaMemcpyAsync(ctx->io_rays.ptr, rays, sizeof(ff_ray) * n, cudaMemcpyHostToDevice,
+                                          ctx->stream));
+            d_rays = ctx->io_rays.as<ff_ray>();
+        }
+        // counters: [16..31] the two work totals, [8..11] the traversal error count
+        unsigned long long* d_out = reinterpret_cast<unsigned long long*>(ctx->counters.as<char>() + 16);
+        unsigned int* err = reinterpret_cast<unsigned int*>(ctx->counters.as<char>() + 8);
+        FF_CUDA_CHECK(cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), ctx->stream));
+        ff_launch_trace_count(ctx, s, d_rays, n, any, d_out, err);
+        unsigned long long h[2] = {0, 0};
+        unsigned int e = 0;
+        FF_CUDA_CHECK(cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        FF_CUDA_CHECK(cudaMemcpyAsync(&e, err, sizeof(e), cudaMemcpyDeviceToHost, ctx->stream));
+        FF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+        if (e) {
+            FF_CUDA_CHECK(cudaMemsetAsync(err, 0, sizeof(e), ctx->stream));
+            throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
+        }
+        out[0] = h[0];
+        out[1] = h[1];
+        out[2] = sizeof(FFNode8);
+        out[3] = sizeof(FFTri);
+    });
+}
+
 }  // extern "C"
 
 extern "C" ff_status ff_render(ff_context* ctx, ff_scene* scene, const ff_render_settings* settings, ff_film* film,

@@ -161,6 +161,10 @@ void ff_build_bvh(ff_context* ctx, ff_scene* s, const float3* d_pos, const uint3
 // ff_trace.cu
 void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n,
                      ff_hit* d_hits, bool any_hit);
+// ff_trace.cu: traversal work counts of n device rays (ff_trace_count):
+// d_out[0] += node records fetched, d_out[1] += triangles tested.
+void ff_launch_trace_count(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n, bool any_hit,
+                           unsigned long long* d_out, unsigned int* err);
 
 // ff_trace.cu: the trace launch with caller-supplied counters (used by the
 // no-allocation entry point).

@@ -105,7 +105,64 @@ __global__ void __launch_bounds__(kTraceBlock, 8)
     }
 }
 
+// Traversal work of n rays (ff_trace_count): one thread per ray over the same
+// traversal step as k_trace, so each ray visits the same nodes and tests the
+// same triangles; out[0] += node records fetched, out[1] += triangles tested.
+template <bool ANY>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_count(FFBvhView bvh, const ff_ray* __restrict__ rays,
+                                                             uint64_t n, unsigned long long* __restrict__ out,
+                                                             unsigned int* __restrict__ err)
+{
+    __shared__ uint2 s_stack[kShortStack * kTraceBlock];
+    FFStack st;
+    st.sm = s_stack + threadIdx.x;
+    st.stride = kTraceBlock;
+    st.sp = 0;
+    FFCount count;
+    const uint32_t max_steps = bvh.num_nodes + 2u;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (!bvh.num_nodes) break;
+        const float4 r0 = __ldg(reinterpret_cast<const float4*>(rays + i));
+        const float4 r1 = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
+        FFRayState r;
+        ff_ray_setup(r, make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), r0.w, r1.w, ANY);
+        uint2 cur = ff_root_group(r);
+        st.reset();
+        uint32_t steps = 0;
+        while (!ff_traverse_step<ANY>(bvh, r, cur, st, count)) {
+            if (st.overflow || ++steps > max_steps) {
+                atomicAdd(err, 1u);
+                break;
+            }
+        }
+    }
+    unsigned long long a = count.nodes, b = count.tris;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        atomicAdd(out, a);
+        atomicAdd(out + 1, b);
+    }
+}
+
 }  // namespace
+
+void ff_launch_trace_count(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n, bool any_hit,
+                           unsigned long long* d_out, unsigned int* err)
+{
+    if (n == 0) return;
+    uint64_t grid = (uint64_t)ctx->num_sms * 8;
+    const uint64_t need = (n + kTraceBlock - 1) / kTraceBlock;
+    if (grid > need) grid = need;
+    if (any_hit)
+        k_trace_count<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, n, d_out, err);
+    else
+        k_trace_count<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, n, d_out, err);
+    FF_CUDA_CHECK(cudaGetLastError());
+}
 
 void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n, ff_hit* d_hits,
                      bool any_hit)

@@ -223,11 +223,24 @@ struct FFStack {
     }
 };
 
+// Work counters for ff_traverse_step: FFNoCount compiles to nothing (the
+// product kernels); FFCount tallies the node records fetched and the
+// triangles tested (ff_trace_count).
+struct FFNoCount {
+    FF_D void node() {}
+    FF_D void tri() {}
+};
+struct FFCount {
+    unsigned long long nodes = 0, tris = 0;
+    FF_D void node() { ++nodes; }
+    FF_D void tri() { ++tris; }
+};
+
 // One traversal step: take the next child node of the current group, test
 // its children, then test the triangles it exposed.  Returns true when the
 // ray is finished.
-template <bool ANY>
-FF_D bool ff_traverse_step(const FFBvhView& bvh, FFRayState& r, uint2& cur, FFStack& st)
+template <bool ANY, class C>
+FF_D bool ff_traverse_step(const FFBvhView& bvh, FFRayState& r, uint2& cur, FFStack& st, C& count)
 {
     uint2 tri_group = make_uint2(0u, 0u);
     if (cur.y & 0xff000000u) {
@@ -240,6 +253,7 @@ FF_D bool ff_traverse_step(const FFBvhView& bvh, FFRayState& r, uint2& cur, FFSt
             st.overflow = true;
             return true;
         }
+        count.node();
         ff_intersect_node(bvh.nodes, child, r, cur, tri_group);
     }
     while (tri_group.y) {
@@ -249,6 +263,7 @@ FF_D bool ff_traverse_step(const FFBvhView& bvh, FFRayState& r, uint2& cur, FFSt
             st.overflow = true;
             return true;
         }
+        count.tri();
         if (ANY) {
             if (ff_test_tri_any(bvh.tris, tri_group.x + i, r)) return true;
         } else {
@@ -260,6 +275,12 @@ FF_D bool ff_traverse_step(const FFBvhView& bvh, FFRayState& r, uint2& cur, FFSt
         cur = st.pop();
     }
     return st.overflow;
+}
+template <bool ANY>
+FF_D bool ff_traverse_step(const FFBvhView& bvh, FFRayState& r, uint2& cur, FFStack& st)
+{
+    FFNoCount none;
+    return ff_traverse_step<ANY>(bvh, r, cur, st, none);
 }
 
 // Root group: a fake parent whose only internal child (node 0) sits in the

@@ -254,6 +254,16 @@ FF_API ff_status ff_trace(ff_context* ctx, const ff_scene* scene, const ff_ray* 
 FF_API ff_status ff_trace_host_noalloc(ff_context* ctx, const ff_scene* scene, const ff_ray* rays,
                                        uint64_t n, ff_hit* hits, uint32_t flags);
 
+/* Traversal work of n rays, for measurement; no counterpart in the
+ * reference.  Runs the same traversal as ff_trace (same rays and flags,
+ * FF_MEM_DEVICE when rays is a device pointer) without writing hits, and
+ * returns out[0] = 8-wide node records fetched, out[1] = triangles tested,
+ * out[2] = bytes per node record, out[3] = bytes per triangle record, so
+ * that (out[0]*out[2] + out[1]*out[3]) / n is the traversal's fetched bytes
+ * per ray.  Synchronous. */
+FF_API ff_status ff_trace_count(ff_context* ctx, const ff_scene* scene, const ff_ray* rays,
+                                uint64_t n, uint32_t flags, uint64_t* out);
+
 /* ------------------------------------------------------------------- film */
 
 /* Headless film replacing the GL surface of Interop (Interop.cpp:78-86) and

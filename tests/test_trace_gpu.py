@@ -182,3 +182,45 @@ def test_device_pointer_path_matches_host_path(room):
     ds.ctx.sync()
     dev = d_hits.cpu().numpy().view(np.uint8).view(host.dtype).reshape(-1)
     assert np.array_equal(dev.view(np.uint32), host.view(np.uint32))
+
+
+def test_trace_count(ctx, room):
+    """ff_trace_count: deterministic, the same from host and device rays,
+    at least the root node per ray and a tested triangle per hit, and on a
+    one-triangle scene at most one test per ray and node."""
+    import firefly_b200 as ff
+    import torch
+    scn, ds = room
+    rays = scenes.incoherent_rays(scn, 100_000, seed=23)
+    n = len(rays)
+    c1, c2 = ds.trace_count(rays), ds.trace_count(rays)
+    assert c1 == c2
+    d_rays = torch.from_numpy(rays).cuda()
+    torch.cuda.synchronize()
+    assert ds.trace_count(d_rays.data_ptr(), n) == c1
+    assert c1["node_bytes"] == 80 and c1["tri_bytes"] == 48
+    hits = ds.trace(rays)
+    assert c1["nodes"] >= n and c1["tris"] >= int((hits["prim"] >= 0).sum())
+    ca = ds.trace_count(rays, any_hit=True)
+    assert ca["nodes"] >= n and ca["tris"] >= int((ds.trace(rays, any_hit=True)["prim"] >= 0).sum())
+    print(f"[trace] room, incoherent: {c1['nodes'] / n:.2f} nodes, {c1['tris'] / n:.2f} tris per ray "
+          f"({c1['fetch_bytes_per_ray']:.0f} B); any-hit {ca['fetch_bytes_per_ray']:.0f} B")
+
+    one = scenes.Scene(positions=np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32),
+                       indices=np.array([[0, 1, 2]], np.uint32))
+    ds1 = ff.dScene(ctx, one)
+    nn = ds1.stats()["num_nodes"]
+    rng = np.random.default_rng(5)
+    r1 = np.zeros((4096, 8), np.float32)
+    r1[:, 0:2] = rng.uniform(-0.5, 1.5, (4096, 2))
+    r1[:, 2] = 1.0
+    r1[:, 6] = -1.0
+    r1[:, 7] = np.inf
+    c = ds1.trace_count(r1)
+    h = ds1.trace(r1)
+    assert len(r1) <= c["nodes"] <= nn * len(r1)
+    assert int((h["prim"] >= 0).sum()) <= c["tris"] <= len(r1)
+    empty = scenes.Scene(positions=np.zeros((0, 3), np.float32), indices=np.zeros((0, 3), np.uint32))
+    ds0 = ff.dScene(ctx, empty)
+    assert ds0.trace_count(r1[:10])["nodes"] == 0
+    assert ds.trace_count(rays[:0])["rays"] == 0
