@@ -45,6 +45,9 @@ RENDER_WORKLOAD = ("wavefront path tracer at scale: displaced icosphere 1,310,72
 TRACE_WORKLOAD = "trace micro: small room 4120 tris, 16M coherent + 16M incoherent rays, closest + any-hit"
 RAYS_PER_SET = 4096 * 4096
 RAY_BYTES, HIT_BYTES = 32, 16
+# The wavefront's traces read a tagged queue (32 B ray + 4 B tag): the
+# closest-hit trace writes a 16 B hit, the any-hit trace a 1 B answer.
+WF_CLOSEST_BYTES, WF_ANY_BYTES = 32 + 4 + 16, 32 + 4 + 1
 # k_logic in the adjoint, per slot in flight and frame (continuing path):
 # reads phase, key, ext_q, length, pass (20 B), the extension hit (16), ray
 # origin and direction (32), throughput (16), radiance sum (16), shadow-queue
@@ -75,6 +78,15 @@ RENDER_SHADE_BYTES_PER_VERTEX = 332
 RENDER_DRAM_BYTES_PER_UNIT = {"k_logic": 448.4, "k_shade (all kinds)": 599.1,
                               "k_trace<closest> (extension queue)": 106.0, "k_trace<any> (shadow queue)": 51.2}
 RENDER = dict(width=1920, height=1080, spp=64, max_depth=8, rr_depth=3)
+# Measured DRAM bytes per unit of the adjoint's stages (ncu over the profiled
+# 512x512, 16-spp adjoint call of --workload inverse, 12 frames): per
+# consumed extension hit for k_logic and k_shade, per traced ray for the traces.
+ADJ_DRAM_BYTES_PER_UNIT = {"k_logic (adjoint)": 334.1, "k_shade (adjoint)": 259.2,
+                           "k_trace closest (extension)": 52.0, "k_trace any (shadow)": 39.9}
+# k_cache_infer: measured DRAM bytes per query (ncu over 6 cached 1080p
+# frames, 9,513,224 queries): the 64 B record in and the film update; the
+# hash grid's FP16 copy stays in L2.
+CACHE_INFER_DRAM_BYTES_PER_QUERY = 110.8
 
 
 def dist_env():
@@ -474,7 +486,11 @@ def run_trace(args, ws, rank, local, dist):
         # traversal fetch bytes: node records and triangles each ray's traversal
         # reads (counted by the same traversal on the device, outside the timed
         # region), against an L2-resident copy
-        l2_ref = l2_read_gbs(dev)
+        try:
+            l2_ref = l2_read_gbs(dev)
+        except Exception as e:   # the reference bandwidth is optional
+            print(f"l2 read probe unavailable: {e}", file=sys.stderr)
+            l2_ref = None
         fetch = {}
         for k, (name, _, any_hit) in enumerate(batches):
             wk = ds.trace_count(d_rays[k].data_ptr(), n, any_hit=any_hit)
@@ -631,14 +647,15 @@ def run_render(args, ws, rank, local, dist):
     if rank == 0:
         peak, peak_kind = measured_peaks()
         # dominant stage by device time (events of the profiled step), with the
-        # algorithmic bytes of one launch sequence: 48 B per traced ray (ray in,
-        # hit out), or the slot-state bytes above per consumed hit / shaded vertex
+        # algorithmic bytes of one launch sequence: the traced rays' queue I/O,
+        # or the slot-state bytes above per consumed hit / shaded vertex
         vertices = max(0, prof["extension_rays"] - prof["samples"])
-        stage = {"k_trace<any> (shadow queue)": (prof["ms_trace_shadow"], prof["shadow_rays"] * (RAY_BYTES + HIT_BYTES),
-                                                 "48 B per shadow ray"),
+        stage = {"k_trace<any> (shadow queue)": (prof["ms_trace_shadow"], prof["shadow_rays"] * WF_ANY_BYTES,
+                                                 f"{WF_ANY_BYTES} B per shadow ray (ray + tag in, 1 B answer out)"),
                  "k_trace<closest> (extension queue)": (prof["ms_trace_extension"],
-                                                        prof["extension_rays"] * (RAY_BYTES + HIT_BYTES),
-                                                        "48 B per extension ray"),
+                                                        prof["extension_rays"] * WF_CLOSEST_BYTES,
+                                                        f"{WF_CLOSEST_BYTES} B per extension ray (ray + tag in, "
+                                                        "hit out)"),
                  "k_logic": (prof["ms_logic"], prof["extension_rays"] * RENDER_LOGIC_BYTES_PER_HIT,
                              f"{RENDER_LOGIC_BYTES_PER_HIT} B of slot state per consumed extension hit"),
                  "k_shade (all kinds)": (prof["ms_shade"], vertices * RENDER_SHADE_BYTES_PER_VERTEX,
@@ -798,22 +815,31 @@ def run_inverse(args, ws, rank, local, dist):
                     "extension hit (primal and replay passes averaged) over the stage's event-timed duration")
         elif "trace" in dom:
             rays = prof["extension_rays"] if "closest" in dom else prof["shadow_rays"]
-            achieved = rays * (RAY_BYTES + HIT_BYTES) / (stages[dom] / 1e3) / 1e9
-            note = ("algorithmic bytes = 48 B per ray (32 B ray in, 16 B hit out) x the stage's rays over its "
-                    "event-timed duration; BVH and triangles are L2-resident")
+            per = WF_CLOSEST_BYTES if "closest" in dom else WF_ANY_BYTES
+            achieved = rays * per / (stages[dom] / 1e3) / 1e9
+            note = (f"algorithmic bytes = {per} B per ray (32 B ray + 4 B tag in, the hit or answer out) x the "
+                    "stage's rays over its event-timed duration; BVH and triangles are L2-resident")
         else:
             adj_ms = r["adjoint_ms_per_step"]
             achieved = r["grad_atomics_per_step"] * 12 / (adj_ms / 1e3) / 1e9
             note = ("algorithmic bytes = 12 B of float atomics per texel touch after the warp pre-reduction "
                     "(counted by the kernels) over the whole adjoint")
+        # DRAM traffic of the dominant stage per frame: measured bytes per
+        # unit (ncu over the profiled call) x this call's units per frame
+        units = {"k_logic (adjoint)": prof["extension_rays"], "k_shade (adjoint)": prof["extension_rays"],
+                 "k_trace closest (extension)": prof["extension_rays"], "k_trace any (shadow)": prof["shadow_rays"]}
+        traffic = int(ADJ_DRAM_BYTES_PER_UNIT[dom] * units[dom] / max(1, prof["frames"]))
         cpu = None if args.no_cpu else inverse_cpu_baseline(target_s=args.cpu_s)
         line = {"metric": "adjoint spp/s", "value": round(value, 1), "unit": "samples/s", "n_gpus": ws,
                 "steps": r["steps"], "warmup": 0, "ms_per_step": r["adjoint_ms_per_step"] + r["primal_ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": r,
                 "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2),
-                             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": None,
-                             "peak_source": peak_kind, "note": note},
+                             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": traffic,
+                             "peak_source": peak_kind, "note": note,
+                             "traffic_note": ("DRAM bytes per frame of the dominant stage: ncu dram bytes per unit of "
+                                              "the profiled 512x512x16-spp adjoint call x its units per frame"),
+                             "dram_bytes_per_unit": ADJ_DRAM_BYTES_PER_UNIT},
                 "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(round(r["kernel_launches_per_step"] * r["steps"])), "clocks": clk}
         print(json.dumps(line), flush=True)
@@ -847,7 +873,10 @@ def inverse_e2e(ctx, dev, stream, iters=5, res=512):
     ms = e0.elapsed_time(e1)
     # one more call with per-stage events: the split between the wavefront
     # stages of the adjoint (outside the timed region)
+    # (the NVTX range lets ncu capture exactly this call: --nvtx --nvtx-include "profiled/")
+    torch.cuda.nvtx.range_push("profiled")
     prof = ds.render_adjoint(res, res, d_image, grad_texture=g_tex, grad_env=g_env, spp=16, seed=99, profile=True)
+    torch.cuda.nvtx.range_pop()
     ds.close()
     e2e = {"value": round(samples / (ms / 1e3), 1), "unit": "samples/s",
            "h2d_bytes_per_step": int(d_image.nbytes + g_tex.nbytes + g_env.nbytes),
@@ -1013,7 +1042,11 @@ def run_cache(args, ws, rank, local, dist):
                 "roofline": {"bound": "tensor", "kernel": "k_cache_infer (+ k_frame_to_film)",
                              "achieved": None if q_tflops is None else round(q_tflops, 3), "peak": peak,
                              "unit": "TFLOP/s", "frac": None if q_tflops is None else round(q_tflops / peak, 5),
-                             "traffic": None, "peak_source": peak_kind,
+                             "traffic": int(CACHE_INFER_DRAM_BYTES_PER_QUERY * prof["cache_queries"]
+                                            / max(1, prof["frames"])),
+                             "traffic_note": ("DRAM bytes of one k_cache_infer launch (one per frame): ncu dram bytes "
+                                              "per query over 6 frames x this run's queries per frame"),
+                             "peak_source": peak_kind,
                              "flops_per_query": 2 * (4 * 64 * 64 + 16 * 64)},
                 "cpu_baseline": None,
                 "cpu_baseline_note": "not timed for the cache: the plain tracer on the same GPU is the comparator",
