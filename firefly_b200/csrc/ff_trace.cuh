@@ -46,6 +46,13 @@ FF_D float byte_as_float(uint32_t lo4, uint32_t hi4, int s)
     return __uint_as_float(bits) - 8388608.0f;
 }
 
+// Byte s of (lo4, hi4) as the float 2^23 + byte (one byte permute); the
+// node test subtracts 2^23 from two such values with one packed add.
+FF_D float byte_plus_2p23(uint32_t lo4, uint32_t hi4, int s)
+{
+    return __uint_as_float(__byte_perm(s < 4 ? lo4 : hi4, 0x4B000000u, 0x7440u | (uint32_t)(s & 3)));
+}
+
 // Three-input min / max of sm_100 (one instruction instead of two; exact,
 // and NaN-ignoring like fminf / fmaxf).
 FF_D float fmin3f(float a, float b, float c)
@@ -87,18 +94,24 @@ FF_D void ff_intersect_node(const FFNode8* __restrict__ nodes, uint32_t idx, con
     const uint32_t nz0 = r.inv.z >= 0.f ? n3.x : n4.z, nz1 = r.inv.z >= 0.f ? n3.y : n4.w;
     const uint32_t fz0 = r.inv.z >= 0.f ? n4.z : n3.x, fz1 = r.inv.z >= 0.f ? n4.w : n3.y;
     const float tb = r.tmax + fabsf(r.tmax) * FF_BOX_WIDEN;
+    // x and y in packed FP32: one add removes 2^23 from two plane bytes and
+    // one fma gives two slab distances (the same IEEE operations per lane as
+    // fmaf, so the same values); z in scalar fmaf
+    const float2 axy = make_float2(ax, ay), bxy = make_float2(bx, by);
+    const float2 m23 = make_float2(-8388608.0f, -8388608.0f);
     uint32_t hits = 0, tmask = 0;
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
         const uint32_t meta = byte_of(n1.z, n1.w, s);
-        const float tnx = fmaf(byte_as_float(nx0, nx1, s), ax, bx);
-        const float tny = fmaf(byte_as_float(ny0, ny1, s), ay, by);
-        const float tnz = fmaf(byte_as_float(nz0, nz1, s), az, bz);
-        const float tfx = fmaf(byte_as_float(fx0, fx1, s), ax, bx);
-        const float tfy = fmaf(byte_as_float(fy0, fy1, s), ay, by);
-        const float tfz = fmaf(byte_as_float(fz0, fz1, s), az, bz);
-        float tn = fmax3f(tnx, tny, tnz);
-        float tf = fmin3f(tfx, tfy, tfz);
+        const float2 qn = __fadd2_rn(make_float2(byte_plus_2p23(nx0, nx1, s), byte_plus_2p23(ny0, ny1, s)), m23);
+        const float2 qf = __fadd2_rn(make_float2(byte_plus_2p23(fx0, fx1, s), byte_plus_2p23(fy0, fy1, s)), m23);
+        const float2 qz = __fadd2_rn(make_float2(byte_plus_2p23(nz0, nz1, s), byte_plus_2p23(fz0, fz1, s)), m23);
+        const float2 tnxy = __ffma2_rn(qn, axy, bxy);
+        const float2 tfxy = __ffma2_rn(qf, axy, bxy);
+        const float tnz = fmaf(qz.x, az, bz);
+        const float tfz = fmaf(qz.y, az, bz);
+        float tn = fmax3f(tnxy.x, tnxy.y, tnz);
+        float tf = fmin3f(tfxy.x, tfxy.y, tfz);
         tn = tn - fabsf(tn) * FF_BOX_WIDEN;
         tf = tf + fabsf(tf) * FF_BOX_WIDEN;
         const bool hit = meta != 0u && fmaxf(tn, r.tmin) <= fminf(tf, tb);
