@@ -175,7 +175,8 @@ void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d
 // tags, closest hits go to d_hits[tag] and any-hit answers to occ[tag].
 void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
                            uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter,
-                           unsigned int* err, const uint32_t* tags = nullptr, uint8_t* occ = nullptr);
+                           unsigned int* err, const uint32_t* tags = nullptr, uint8_t* occ = nullptr,
+                           cudaStream_t stream = nullptr);   // null: the context's stream
 
 // ff_wavefront.cu: the path-replay adjoint on the wavefront stages.  Every
 // pointer is device memory; gradients are added to grad_* (null = not

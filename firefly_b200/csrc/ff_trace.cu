@@ -220,7 +220,7 @@ void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d
 // by the caller before the launch.
 void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
                            uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter, unsigned int* err,
-                           const uint32_t* tags, uint8_t* occ)
+                           const uint32_t* tags, uint8_t* occ, cudaStream_t stream)
 {
     if (cap == 0) return;
     static int bps[2] = {0, 0};
@@ -236,7 +236,7 @@ void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* 
     const uint64_t need = (cap + kTraceBlock - 1) / kTraceBlock;
     if (grid > need) grid = need;
     const dim3 g((unsigned)grid), b(kTraceBlock);
-    cudaStream_t st = ctx->stream;
+    cudaStream_t st = stream ? stream : ctx->stream;
     if (any_hit && tags)
         k_trace<true, true><<<g, b, 0, st>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev, tags, occ);
     else if (any_hit)

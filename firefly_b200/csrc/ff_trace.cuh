@@ -102,7 +102,6 @@ FF_D void ff_intersect_node(const FFNode8* __restrict__ nodes, uint32_t idx, con
     uint32_t hits = 0, tmask = 0;
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
-        const uint32_t meta = byte_of(n1.z, n1.w, s);
         const float2 qn = __fadd2_rn(make_float2(byte_plus_2p23(nx0, nx1, s), byte_plus_2p23(ny0, ny1, s)), m23);
         const float2 qf = __fadd2_rn(make_float2(byte_plus_2p23(fx0, fx1, s), byte_plus_2p23(fy0, fy1, s)), m23);
         const float2 qz = __fadd2_rn(make_float2(byte_plus_2p23(nz0, nz1, s), byte_plus_2p23(fz0, fz1, s)), m23);
@@ -114,8 +113,10 @@ FF_D void ff_intersect_node(const FFNode8* __restrict__ nodes, uint32_t idx, con
         float tf = fmin3f(tfxy.x, tfxy.y, tfz);
         tn = tn - fabsf(tn) * FF_BOX_WIDEN;
         tf = tf + fabsf(tf) * FF_BOX_WIDEN;
-        const bool hit = meta != 0u && fmaxf(tn, r.tmin) <= fminf(tf, tb);
-        if (hit) {
+        // an empty slot (meta 0, not internal) adds nothing even where its
+        // degenerate box is hit, so no occupancy test is needed
+        if (fmaxf(tn, r.tmin) <= fminf(tf, tb)) {
+            const uint32_t meta = byte_of(n1.z, n1.w, s);
             if ((imask >> s) & 1u) hits |= 1u << (24 + (s ^ r.oct_inv));
             else tmask |= (meta >> 5) << (meta & 31u);
         }

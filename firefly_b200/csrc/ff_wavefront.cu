@@ -571,9 +571,16 @@ struct FFWavefrontWS {
     unsigned int* err = nullptr;
     unsigned long long* trace_ctr = nullptr;  // [0] closest, [1] any
     uint32_t* h_active = nullptr;             // pinned host word for the frame-loop check
+    // the any-hit trace runs on `side` beside the closest-hit trace: its
+    // blocks take the SMs the closest-hit trace's finished blocks leave
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     ~FFWavefrontWS()
     {
         if (h_active) cudaFreeHost(h_active);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
     }
 };
 
@@ -724,6 +731,11 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     uint32_t frames = 0;
     uint32_t active = 1;
     if (!ws->h_active) FF_CUDA_CHECK(cudaMallocHost(&ws->h_active, sizeof(uint32_t)));
+    if (!ws->side) {
+        FF_CUDA_CHECK(cudaStreamCreateWithFlags(&ws->side, cudaStreamNonBlocking));
+        FF_CUDA_CHECK(cudaEventCreateWithFlags(&ws->fork, cudaEventDisableTiming));
+        FF_CUDA_CHECK(cudaEventCreateWithFlags(&ws->join, cudaEventDisableTiming));
+    }
     uint32_t* h_active = ws->h_active;
     const uint32_t max_frames = (st->spp + 1) * (st->max_depth + 2) + 8;
     while (active && frames < max_frames) {
@@ -748,12 +760,26 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
             }
             FF_CUDA_CHECK(cudaGetLastError());
             mark();
-            ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err,
-                                  w.ext_tag, nullptr);
-            mark();
-            ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true, ws->trace_ctr + 1,
-                                  ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis));
-            mark();
+            if (profile) {
+                // stage timing: the two traces one after the other
+                ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
+                                      ws->err, w.ext_tag, nullptr);
+                mark();
+                ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
+                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis));
+                mark();
+            } else {
+                // the traces are independent (hits by slot, answers by shadow-ray tag)
+                FF_CUDA_CHECK(cudaEventRecord(ws->fork, stream));
+                FF_CUDA_CHECK(cudaStreamWaitEvent(ws->side, ws->fork, 0));
+                ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
+                                      ws->err, w.ext_tag, nullptr);
+                ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
+                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis),
+                                      ws->side);
+                FF_CUDA_CHECK(cudaEventRecord(ws->join, ws->side));
+                FF_CUDA_CHECK(cudaStreamWaitEvent(stream, ws->join, 0));
+            }
             ++frames;
         }
         FF_CUDA_CHECK(cudaMemcpyAsync(h_active, w.ctr + C_ACTIVE, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
