@@ -575,12 +575,30 @@ struct FFWavefrontWS {
     // blocks take the SMs the closest-hit trace's finished blocks leave
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
+    // k_shade of the second to fifth material kind in use, beside the first
+    cudaStream_t kind_side[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t kind_join[4] = {nullptr, nullptr, nullptr, nullptr};
+    void ensure_streams()
+    {
+        if (side) return;
+        FF_CUDA_CHECK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        FF_CUDA_CHECK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+        FF_CUDA_CHECK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+        for (int i = 0; i < 4; ++i) {
+            FF_CUDA_CHECK(cudaStreamCreateWithFlags(&kind_side[i], cudaStreamNonBlocking));
+            FF_CUDA_CHECK(cudaEventCreateWithFlags(&kind_join[i], cudaEventDisableTiming));
+        }
+    }
     ~FFWavefrontWS()
     {
         if (h_active) cudaFreeHost(h_active);
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
         if (side) cudaStreamDestroy(side);
+        for (int i = 0; i < 4; ++i) {
+            if (kind_join[i]) cudaEventDestroy(kind_join[i]);
+            if (kind_side[i]) cudaStreamDestroy(kind_side[i]);
+        }
     }
 };
 
@@ -595,6 +613,46 @@ T* carve(char*& p, size_t n)
     size_t bytes = (sizeof(T) * n + 255) & ~size_t(255);
     p += bytes;
     return r;
+}
+
+template <int K, bool SEL, bool ADJ>
+void shade_kind(const WF& w, int blocks, cudaStream_t stream)
+{
+    k_shade<K, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
+}
+
+// k_shade for every material kind in use.  With ws, the first kind runs on
+// `stream` and each further kind on a side stream of its own, all after the
+// work already on `stream` (k_logic); `stream` then waits for all of them.
+// The kinds shade disjoint slots and append to the queues with atomics, so
+// the order of their launches does not change any result.
+template <bool SEL, bool ADJ>
+void launch_shade(const WF& w, const bool* kind_used, int blocks, cudaStream_t stream, FFWavefrontWS* ws)
+{
+    using Fn = void (*)(const WF&, int, cudaStream_t);
+    Fn fns[kKinds];
+    fns[FF_MAT_MIX] = shade_kind<FF_MAT_MIX, SEL, ADJ>;
+    fns[FF_MAT_DIFFUSE] = shade_kind<FF_MAT_DIFFUSE, SEL, ADJ>;
+    fns[FF_MAT_CONDUCTOR] = shade_kind<FF_MAT_CONDUCTOR, SEL, ADJ>;
+    fns[FF_MAT_DIELECTRIC] = shade_kind<FF_MAT_DIELECTRIC, SEL, ADJ>;
+    fns[FF_MAT_COAT] = shade_kind<FF_MAT_COAT, SEL, ADJ>;
+    int n_side = 0;
+    bool first = true;
+    if (ws) FF_CUDA_CHECK(cudaEventRecord(ws->fork, stream));
+    for (int k = 0; k < kKinds; ++k) {
+        if (!kind_used[k]) continue;
+        if (!ws || first) {
+            fns[k](w, blocks, stream);
+            first = false;
+            continue;
+        }
+        cudaStream_t s = ws->kind_side[n_side];
+        FF_CUDA_CHECK(cudaStreamWaitEvent(s, ws->fork, 0));
+        fns[k](w, blocks, s);
+        FF_CUDA_CHECK(cudaEventRecord(ws->kind_join[n_side], s));
+        ++n_side;
+    }
+    for (int i = 0; i < n_side; ++i) FF_CUDA_CHECK(cudaStreamWaitEvent(stream, ws->kind_join[i], 0));
 }
 
 size_t ws_bytes(uint32_t P)
@@ -731,11 +789,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     uint32_t frames = 0;
     uint32_t active = 1;
     if (!ws->h_active) FF_CUDA_CHECK(cudaMallocHost(&ws->h_active, sizeof(uint32_t)));
-    if (!ws->side) {
-        FF_CUDA_CHECK(cudaStreamCreateWithFlags(&ws->side, cudaStreamNonBlocking));
-        FF_CUDA_CHECK(cudaEventCreateWithFlags(&ws->fork, cudaEventDisableTiming));
-        FF_CUDA_CHECK(cudaEventCreateWithFlags(&ws->join, cudaEventDisableTiming));
-    }
+    ws->ensure_streams();
     uint32_t* h_active = ws->h_active;
     const uint32_t max_frames = (st->spp + 1) * (st->max_depth + 2) + 8;
     while (active && frames < max_frames) {
@@ -745,19 +799,11 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
             mark();
             k_logic<false><<<(P + 255) / 256, 256, 0, stream>>>(w);
             mark();
-            if (w.lights.light == FF_LIGHT_ALL) {
-                if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX, true, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE, true, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR, true, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC, true, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT, true, false><<<shade_blocks, 128, 0, stream>>>(w);
-            } else {
-                if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX, false, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE, false, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR, false, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC, false, false><<<shade_blocks, 128, 0, stream>>>(w);
-                if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT, false, false><<<shade_blocks, 128, 0, stream>>>(w);
-            }
+            // with stage timing (profile) every launch stays on the one stream
+            if (w.lights.light == FF_LIGHT_ALL)
+                launch_shade<true, false>(w, kind_used, shade_blocks, stream, profile ? nullptr : ws);
+            else
+                launch_shade<false, false>(w, kind_used, shade_blocks, stream, profile ? nullptr : ws);
             FF_CUDA_CHECK(cudaGetLastError());
             mark();
             if (profile) {
@@ -857,15 +903,6 @@ void adj_setup(FFWavefrontWS* ws, uint32_t P)
     w.v_coef = carve<float4>(p, P);
 }
 
-template <bool SEL, bool ADJ>
-void launch_shade(const WF& w, const bool* kind_used, int blocks, cudaStream_t stream)
-{
-    if (kind_used[FF_MAT_MIX]) k_shade<FF_MAT_MIX, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
-    if (kind_used[FF_MAT_DIFFUSE]) k_shade<FF_MAT_DIFFUSE, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
-    if (kind_used[FF_MAT_CONDUCTOR]) k_shade<FF_MAT_CONDUCTOR, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
-    if (kind_used[FF_MAT_DIELECTRIC]) k_shade<FF_MAT_DIELECTRIC, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
-    if (kind_used[FF_MAT_COAT]) k_shade<FF_MAT_COAT, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
-}
 
 }  // namespace
 
@@ -951,6 +988,7 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
     uint32_t frames = 0;
     uint32_t active = 1;
     if (!ws->h_active) FF_CUDA_CHECK(cudaMallocHost(&ws->h_active, sizeof(uint32_t)));
+    ws->ensure_streams();
     uint32_t* h_active = ws->h_active;
     // two passes per sample
     const uint32_t max_frames = 2 * (st->spp + 1) * (st->max_depth + 2) + 8;
@@ -960,15 +998,28 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
             mark();
             k_logic<true><<<(P + 255) / 256, 256, 0, stream>>>(w);
             mark();
-            launch_shade<false, true>(w, kind_used, shade_blocks, stream);
+            // side streams as in ff_wavefront_render (one stream under stage timing)
+            launch_shade<false, true>(w, kind_used, shade_blocks, stream, profile ? nullptr : ws);
             FF_CUDA_CHECK(cudaGetLastError());
             mark();
-            ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr, ws->err,
-                                  w.ext_tag, nullptr);
-            mark();
-            ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true, ws->trace_ctr + 1,
-                                  ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis));
-            mark();
+            if (profile) {
+                ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
+                                      ws->err, w.ext_tag, nullptr);
+                mark();
+                ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
+                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis));
+                mark();
+            } else {
+                FF_CUDA_CHECK(cudaEventRecord(ws->fork, stream));
+                FF_CUDA_CHECK(cudaStreamWaitEvent(ws->side, ws->fork, 0));
+                ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
+                                      ws->err, w.ext_tag, nullptr);
+                ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
+                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis),
+                                      ws->side);
+                FF_CUDA_CHECK(cudaEventRecord(ws->join, ws->side));
+                FF_CUDA_CHECK(cudaStreamWaitEvent(stream, ws->join, 0));
+            }
             ++frames;
         }
         FF_CUDA_CHECK(cudaMemcpyAsync(h_active, w.ctr + C_ACTIVE, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
