@@ -113,6 +113,31 @@ def test_progressive_and_pool_size_invariance(ctx):
     ds.close()
 
 
+def test_stream_concurrency_is_invisible(ctx):
+    """ff_render runs the any-hit trace beside the closest-hit trace and the
+    material kinds' shade launches side by side; under stage timing
+    (profile) everything runs on one stream.  Both schedules give the same
+    image bit for bit (hits by slot, shadow answers by tag, disjoint slots)."""
+    import firefly_b200 as ff
+    sky = scenes.sky_env(64, 32, seed=0, sun_radiance=50.0, sun_diameter_deg=4.0)
+    scn = scenes.textured_room(seed=1, width=96, height=72, tex_res=32, env=sky, sphere_kind=ff.FF_MAT_CONDUCTOR)
+    ds = ff.dScene(ctx, scn)
+    pt = ff.PathTracer(ctx, 96, 72)
+    out = []
+    for profile in (False, True, False):
+        pt.clear_buffer()
+        st = pt.draw(ds, spp=8, max_depth=6, rr_depth=3, seed=7, light=-1, mode=ff.FF_MODE_CORRECTED,
+                     profile=profile)
+        out.append((pt.read(), st["extension_rays"], st["shadow_rays"]))
+    (a, na), ea, sa = out[0]
+    for (b, nb), eb, sb in out[1:]:
+        assert np.array_equal(na, nb) and ea == eb and sa == sb
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert a[..., :3].sum() > 0
+    pt.close()
+    ds.close()
+
+
 def test_render_argument_errors(ctx):
     import firefly_b200 as ff
     scn = scenes.small_room(seed=0, width=16, height=16)
