@@ -919,7 +919,7 @@ CACHE_TARGET = 0.01
 
 
 def checkpoints(limit):
-    """Sample counts at which the accumulated image is judged (about +25% each)."""
+    """Sample counts at which the accumulated image's error is measured (about +25% each)."""
     out, k = [], 1
     while k <= limit:
         out.append(k)
@@ -962,7 +962,7 @@ def run_cache(args, ws, rank, local, dist):
     pt = ff.PathTracer(ctx, W, H)
     cps = checkpoints(args.cache_max_frames)
 
-    def judge():
+    def error_now():
         img = pt.image()
         return convergence.relmse(img[y0:y0 + th, x0:x0 + tw], ref)
 
@@ -973,7 +973,7 @@ def run_cache(args, ws, rank, local, dist):
         for c in cps:
             ms += render_more(c - done, done)
             done = c
-            e = judge()
+            e = error_now()
             traj.append((c, round(ms, 2), round(e, 5)))
             if e <= CACHE_TARGET:
                 hit = ms
