@@ -14,12 +14,22 @@ scaling: every rank renders its own frame).  `e2e` times the same render
 through the public entry points with the camera uploaded from and the image
 read back to pinned host memory every step.
 
-`--workload trace`: the trace micro-benchmark (4,120-triangle room, 16M
-coherent + 16M incoherent rays, closest-hit and any-hit through ff_trace).
-The render line reports it in config.trace_micro when --with-trace is given.
+At 1 GPU the render line also carries, under "metrics", the lines of the
+other workloads, measured after the render's timed region (each in the same
+format as its own --workload line):
+  trace_micro     the trace micro-benchmark (4,120-triangle room, 16M coherent
+                  + 16M incoherent rays, closest-hit and any-hit through
+                  ff_trace), with the reference's own GPU traversal on the same
+                  rays and every ray checked against the oracle;
+  small_room      the plain tracer on the small room, 256 x 256 x 16 spp;
+  adjoint         path-replay adjoint samples per second (inverse rendering);
+  radiance_cache  time to relMSE 0.01 with the learned radiance cache against
+                  the plain tracer.
+--render-only skips them.
 
 Usage:
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload render|trace]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload render|trace|inverse|cache] [--render-only]
 Under torchrun every rank runs one GPU; rank 0 prints one JSON line.
 """
 from __future__ import annotations
@@ -399,7 +409,7 @@ def l2_read_gbs(dev, mib=32, reps=40):
 
 
 # DRAM bytes per ray of k_trace launches, from an ncu capture at 4,194,304
-# rays per launch (profiles/k_trace_trace_micro.md); traffic scales with rays.
+# rays per launch (the trace micro-benchmark's profile); traffic scales with rays.
 TRACE_DRAM_BYTES_PER_RAY = {"coherent_closest": (134.470144e6 + 42.339328e6) / 4194304,
                             "incoherent_closest": (135.088384e6 + 40.223232e6) / 4194304,
                             "coherent_any": (134.470144e6 + 42.339328e6) / 4194304,
@@ -435,6 +445,32 @@ def reference_cuda_trace(scn, batches, d_hits):
                      "reference's host SAH build, 200-byte dTriangle records, 80-byte Isect written per ray"}
 
 
+def oracle_trace_check(scn, batches, d_hits):
+    """Every ray of every batch against the oracle (its CPU hierarchy over
+    the same triangles, deciding each triangle with the restated
+    dTriangle::intersect / shadow_hit): closest hits must agree bit for bit
+    (prim, t, u, v; ties to the lowest index), any-hit answers as occluded or
+    not.  Outside the timed region, on all host threads."""
+    from oracle import ffo
+    t0 = time.perf_counter()
+    bvh = ffo.BVH(scn.triangle_soup())
+    out = {}
+    for k, (name, rays, any_hit) in enumerate(batches):
+        ours = d_hits[k].cpu().numpy().view(np.uint32)
+        ref = bvh.trace(rays, any_hit=any_hit).view(np.uint32).reshape(-1, 4)
+        if any_hit:
+            bad = (ours[:, 3].view(np.int32) >= 0) != (ref[:, 3].view(np.int32) >= 0)
+        else:
+            hit = ref[:, 3].view(np.int32) != -1
+            bad = (ours[:, 3] != ref[:, 3]) | (hit & np.any(ours[:, :3] != ref[:, :3], axis=1))
+        out[name] = {"rays": int(len(rays)), "mismatches": int(bad.sum())}
+    bvh.close()
+    return {"per_batch": out, "rays": int(sum(v["rays"] for v in out.values())),
+            "mismatches": int(sum(v["mismatches"] for v in out.values())),
+            "seconds": round(time.perf_counter() - t0, 1), "threads": os.cpu_count() or 1,
+            "compared": "closest: prim, t, u, v bit for bit; any-hit: occluded or not"}
+
+
 def run_trace(args, ws, rank, local, dist):
     import torch
     import firefly_b200 as ff
@@ -442,6 +478,16 @@ def run_trace(args, ws, rank, local, dist):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     ctx = ff.Context(local, stream=stream.cuda_stream)
+    line = trace_line(args, ws, rank, local, dist, ctx, dev, stream, args.steps)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def trace_line(args, ws, rank, local, dist, ctx, dev, stream, steps):
+    """The trace micro-benchmark (C3) on this rank; rank 0 gets its JSON line."""
+    import torch
+    import firefly_b200 as ff
 
     def barrier():
         if dist is not None:
@@ -450,10 +496,10 @@ def run_trace(args, ws, rank, local, dist):
     clocks = ClockSampler(local)
     clocks.start()
     rays_per_step, per, total_ms, batches, scn, ds, d_rays, d_hits = trace_micro(ctx, None, args, rank, dev, stream,
-                                                                                barrier, args.steps)
+                                                                                barrier, steps)
     clk = clocks.stop()
     ms_max = max_over_ranks(dist, dev, total_ms)
-    value = ws * rays_per_step * args.steps / (ms_max / 1e3) / 1e6
+    value = ws * rays_per_step * steps / (ms_max / 1e3) / 1e6
     n = batches[0][1].shape[0]
     # end to end through ff_trace with pinned host buffers
     h_rays = [torch.from_numpy(r).pin_memory() for _, r, _ in batches]
@@ -465,7 +511,7 @@ def run_trace(args, ws, rank, local, dist):
             ds.trace(views[k][0], any_hit=any_hit, out=views[k][1])
     e2e_step()
     barrier()
-    e2e_steps = max(1, min(args.steps, 5))
+    e2e_steps = max(1, min(steps, 5))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(e2e_steps):
@@ -483,6 +529,7 @@ def run_trace(args, ws, rank, local, dist):
             rate, kind, desc, _ = cpu_trace_rate(batches, target_s=args.cpu_s, threads=os.cpu_count() or 1)
             cpu = {"value": round(rate, 3), "unit": "Mrays/s", "cores": os.cpu_count() or 1, "kind": kind, "sample": desc}
         ref_cuda = reference_cuda_trace(scn, batches, d_hits) if not args.no_ref_cuda else None
+        check = None if args.no_oracle_check else oracle_trace_check(scn, batches, d_hits)
         # traversal fetch bytes: node records and triangles each ray's traversal
         # reads (counted by the same traversal on the device, outside the timed
         # region), against an L2-resident copy
@@ -506,28 +553,27 @@ def run_trace(args, ws, rank, local, dist):
                              "the traversal's fetches are partly served by L1, so the fraction is an upper bound "
                              "on its L2 load")}
         line = {
-            "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+            "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": ws, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": TRACE_WORKLOAD, "rays_per_step": rays_per_step, "triangles": scn.num_triangles,
                        "l2": "inputs larger than L2 (512 MiB of rays per batch)", "parallelism": f"replicas{ws}",
                        "per_batch_mrays": {b[0]: round(n / (t / 1e3) / 1e6, 1) for b, t in zip(batches, per)},
-                       "reference_cuda": ref_cuda},
+                       "reference_cuda": ref_cuda, "oracle_check": check},
             "roofline": {"bound": "hbm", "kernel": f"k_trace ({batches[k_dom][0]})", "achieved": round(achieved, 2),
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5),
                          "traffic": int(TRACE_DRAM_BYTES_PER_RAY[batches[k_dom][0]] * n),
                          "traffic_source": "ncu dram__bytes_read+write of a 4,194,304-ray launch, scaled to the "
-                                           "launch's rays (profiles/k_trace_trace_micro.md)",
+                                           "launch's rays",
                          "peak_source": peak_kind, "bytes_per_ray": RAY_BYTES + HIT_BYTES, "l2_fetch": l2_fetch},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": int(rays_per_step * RAY_BYTES),
                     "d2h_bytes_per_step": int(rays_per_step * HIT_BYTES)},
-            "gpu_launches": len(batches) * args.steps,
+            "gpu_launches": len(batches) * steps,
             "clocks": clk,
         }
-        print(json.dumps(line), flush=True)
     ds.close()
-    ctx.close()
+    return line if rank == 0 else None
 
 
 def run_render(args, ws, rank, local, dist):
@@ -638,12 +684,16 @@ def run_render(args, ws, rank, local, dist):
                 "spp": int(cnt.numpy()[y0, x0]), "reference_spp": info["spp"], "tile": info["tile"],
                 "reference_s": round(info["seconds"], 1), "accumulation": "float64"}
 
-    trace = None
-    if args.with_trace:
-        rps, per, total, batches, tscn, tds, _, _ = trace_micro(ctx, None, args, rank, dev, stream, barrier, 3)
-        trace = {"workload": TRACE_WORKLOAD, "mrays": round(rps * 3 / (total / 1e3) / 1e6, 1),
-                 "per_batch_mrays": {b[0]: round(len(b[1]) / (t / 1e3) / 1e6, 1) for b, t in zip(batches, per)}}
-        tds.close()
+    metrics = None
+    if ws == 1 and not args.render_only:
+        # the other three metrics and the small-room workload, measured after
+        # the render's timed region on the same GPU (one GPU only)
+        metrics = {"trace_micro": trace_line(args, ws, rank, local, dist, ctx, dev, stream, 3),
+                   "small_room": small_room_line(args, ws, rank, local, dist, ctx, dev, stream),
+                   "adjoint": inverse_line(args, ws, rank, local, dist, ctx, dev, stream, known_lighting_run=False),
+                   "radiance_cache": cache_line(args, ws, rank, local, dist, ctx, dev, stream)}
+    elif ws > 1:
+        metrics = {"note": "the trace micro-benchmark, small room, adjoint and cache lines are measured at 1 GPU"}
     if rank == 0:
         peak, peak_kind = measured_peaks()
         # dominant stage by device time (events of the profiled step), with the
@@ -694,7 +744,7 @@ def run_render(args, ws, rank, local, dist):
                        "l2": "each step traces ~1.3G rays over a 0.27 GB scene; per-step state and queues ~0.5 GB",
                        "parallelism": (f"sample-parallel x{ws}: disjoint sample ranges of one frame, one film "
                                        f"all-reduce (41 MB) per step" if ws > 1 else "1 GPU"),
-                       "image_finite": finite, "relmse_vs_16k_spp": conv, "trace_micro": trace},
+                       "image_finite": finite, "relmse_vs_16k_spp": conv},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 5), "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes": dnote, "algorithmic_bytes_per_launch": alg_launch,
@@ -710,11 +760,129 @@ def run_render(args, ws, rank, local, dist):
                     "d2h_bytes_per_step": int(W * H * (16 + 4))},
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
             "clocks": clk,
+            "metrics": metrics,
         }
         print(json.dumps(line), flush=True)
     pt.close()
     ds.close()
     ctx.close()
+
+
+SMALL_ROOM_WORKLOAD = ("plain tracer, small room: 24-tri box + 64x32 UV sphere (4,120 tris) at a seeded position, "
+                       "mix-material albedos U[0.2, 0.8], one area light of radiance 15; 256x256, 16 spp, depth 5, "
+                       "RR from depth 3, parity mode (the reference's behaviours), seed 0")
+SMALL_ROOM = dict(width=256, height=256, spp=16, max_depth=5, rr_depth=3)
+
+
+def small_room_line(args, ws, rank, local, dist, ctx, dev, stream, steps=20, warmup=3):
+    """The small-room workload (C1): extension + shadow rays per second of
+    whole 256 x 256 x 16-spp frames (every step renders 16 new samples per
+    pixel), with the reference's host-compiled path tracer on the same scene
+    beside it; rank 0 gets its JSON line."""
+    import ctypes as C
+    import torch
+    import firefly_b200 as ff
+    from firefly_b200 import scenes
+    W, H = SMALL_ROOM["width"], SMALL_ROOM["height"]
+    scn = scenes.small_room(seed=0, width=W, height=H)
+    ds = ff.dScene(ctx, scn)
+    pt = ff.PathTracer(ctx, W, H)
+    kw = dict(spp=SMALL_ROOM["spp"], max_depth=SMALL_ROOM["max_depth"], rr_depth=SMALL_ROOM["rr_depth"], light=0,
+              mode=ff.FF_MODE_PARITY, seed=0)
+    k = [0]
+
+    def step(profile=False):
+        pt.clear_buffer()
+        st = pt.draw(ds, sample_offset=SMALL_ROOM["spp"] * k[0], profile=profile, **kw)
+        k[0] += 1
+        return st
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    t0.record(stream)
+    for _ in range(steps):
+        stats.append(step())
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    ms = max_over_ranks(dist, dev, t0.elapsed_time(t1))
+    rays = sum(s["extension_rays"] + s["shadow_rays"] for s in stats)
+    samples = sum(s["samples"] for s in stats)
+    prof = step(profile=True)
+    # end to end: camera in, image and counts out to pinned host memory
+    img = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    cnt = torch.empty((H, W), dtype=torch.int32).pin_memory()
+    lib = ff.lib()
+
+    def e2e_step():
+        ds.update(scn.camera)
+        st = step()
+        assert lib.ff_film_read(pt.film, C.c_void_p(img.data_ptr()), C.c_void_p(cnt.data_ptr()), 0) == 0
+        return st
+    e2e_step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    est = []
+    e0.record(stream)
+    for _ in range(5):
+        est.append(e2e_step())
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e_ms = e0.elapsed_time(e1)
+    e_rays = sum(s["extension_rays"] + s["shadow_rays"] for s in est)
+    line = None
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        stages = {"k_trace<any> (shadow queue)": (prof["ms_trace_shadow"], prof["shadow_rays"] * WF_ANY_BYTES),
+                  "k_trace<closest> (extension queue)": (prof["ms_trace_extension"],
+                                                         prof["extension_rays"] * WF_CLOSEST_BYTES),
+                  "k_logic": (prof["ms_logic"], prof["extension_rays"] * RENDER_LOGIC_BYTES_PER_HIT),
+                  "k_shade (all kinds)": (prof["ms_shade"], max(0, prof["extension_rays"] - prof["samples"])
+                                          * RENDER_SHADE_BYTES_PER_VERTEX)}
+        dom = max(stages, key=lambda n: stages[n][0])
+        achieved = stages[dom][1] / (stages[dom][0] / 1e3) / 1e9
+        cpu = None
+        if not args.no_cpu:
+            from oracle import ffref
+            if ffref.available():
+                threads = os.cpu_count() or 1
+                _, st0, ms0 = ffref.render(scn, W, H, SMALL_ROOM["spp"], SMALL_ROOM["max_depth"],
+                                           SMALL_ROOM["rr_depth"], light=0, threads=threads, pixel_stride=64)
+                per_px = ms0[0] / 1e3 / max(1, st0[2] // SMALL_ROOM["spp"])
+                stride = max(1, int(W * H * per_px / max(args.cpu_s / 2, 1.0)))
+                _, st1, ms1 = ffref.render(scn, W, H, SMALL_ROOM["spp"], SMALL_ROOM["max_depth"],
+                                           SMALL_ROOM["rr_depth"], light=0, threads=threads, pixel_stride=stride)
+                cpu = {"value": round((st1[0] + st1[1]) / (ms1[0] / 1e3) / 1e6, 3), "unit": "Mrays/s",
+                       "cores": threads, "kind": "reference",
+                       "sample": (f"every {stride}th pixel of the 256x256 frame ({st1[2] // SMALL_ROOM['spp']} pixels "
+                                  f"x 16 spp, {st1[0] + st1[1]} rays, {ms1[0] / 1e3:.1f} s) with the reference's "
+                                  f"host-compiled path tracer (area light, its SAH BVH) on {threads} threads")}
+        line = {"metric": METRIC, "value": round(ws * rays / (ms / 1e3) / 1e6, 2), "unit": "Mrays/s", "n_gpus": ws,
+                "steps": steps, "warmup": warmup, "ms_per_step": round(ms / steps, 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": SMALL_ROOM_WORKLOAD, **SMALL_ROOM, "triangles": scn.num_triangles,
+                           "msamples_per_s": round(ws * samples / (ms / 1e3) / 1e6, 2),
+                           "rays_per_step": int(rays / steps), "frames_per_step": stats[-1]["frames"],
+                           "stage_ms_profiled_step": {n: round(prof[n], 3) for n in
+                                                      ("ms_total", "ms_logic", "ms_shade", "ms_trace_extension",
+                                                       "ms_trace_shadow")},
+                           "l2": "scene (0.5 MB) and the 1M-slot path state (0.45 GB) stay resident; each step "
+                                 "re-renders every pixel"},
+                "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak,
+                             "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": None,
+                             "peak_source": peak_kind,
+                             "note": "algorithmic bytes per unit as in the at-scale render line (slot state per hit "
+                                     "or vertex, queue I/O per ray) over the stage's event-timed duration"},
+                "cpu_baseline": cpu,
+                "e2e": {"value": round(e_rays / (e_ms / 1e3) / 1e6, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 80,
+                        "d2h_bytes_per_step": W * H * 20},
+                "gpu_launches": int(sum(s["kernel_launches"] for s in stats)), "clocks": clk}
+    pt.close()
+    ds.close()
+    return line
 
 
 INVERSE_WORKLOAD = ("inverse rendering on the room opened to the sky at 512x512: hidden 512x512 Perlin albedo in "
@@ -785,11 +953,21 @@ def run_inverse(args, ws, rank, local, dist):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     ctx = ff.Context(local, stream=stream.cuda_stream)
+    line = inverse_line(args, ws, rank, local, dist, ctx, dev, stream)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def inverse_line(args, ws, rank, local, dist, ctx, dev, stream, known_lighting_run=True):
+    """The inverse-rendering workload (C4): adjoint samples per second over
+    200 Adam steps; rank 0 gets its JSON line."""
     clocks = ClockSampler(local)
     clocks.start()
     r = inverse_experiment(ctx, steps=args.steps if args.steps > 5 else 200, dev=dev, rank=rank, world=ws)
-    r["known_lighting_run"] = inverse_experiment(ctx, steps=args.steps if args.steps > 5 else 200, dev=dev,
-                                                 known_lighting=True, rank=rank, world=ws)
+    if known_lighting_run:
+        r["known_lighting_run"] = inverse_experiment(ctx, steps=args.steps if args.steps > 5 else 200, dev=dev,
+                                                     known_lighting=True, rank=rank, world=ws)
     # every rank adjoints its own samples of each step (gradients averaged
     # across ranks): whole-job samples over the slowest rank's adjoint time
     adj_ms_max = max_over_ranks(dist, dev, r["adjoint_ms_per_step"])
@@ -842,8 +1020,7 @@ def run_inverse(args, ws, rank, local, dist):
                              "dram_bytes_per_unit": ADJ_DRAM_BYTES_PER_UNIT},
                 "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(round(r["kernel_launches_per_step"] * r["steps"])), "clocks": clk}
-        print(json.dumps(line), flush=True)
-    ctx.close()
+    return line if rank == 0 else None
 
 
 def inverse_e2e(ctx, dev, stream, iters=5, res=512):
@@ -928,16 +1105,27 @@ def checkpoints(limit):
 
 
 def run_cache(args, ws, rank, local, dist):
+    import torch
+    import firefly_b200 as ff
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx = ff.Context(local, stream=stream.cuda_stream)
+    line = cache_line(args, ws, rank, local, dist, ctx, dev, stream)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def cache_line(args, ws, rank, local, dist, ctx, dev, stream):
+    """The radiance-cache workload (C5): time to relMSE 0.01 against the
+    plain tracer; rank 0 gets its JSON line."""
     import ctypes as C
     import torch
     import firefly_b200 as ff
     from firefly_b200 import _abi as A
     from firefly_b200 import convergence, scenes
     from firefly_b200.cache import RadianceCache
-    dev = torch.device("cuda", local)
-    stream = torch.cuda.Stream(dev)
-    torch.cuda.set_stream(stream)
-    ctx = ff.Context(local, stream=stream.cuda_stream)
     W, H = 1920, 1080
     scn = scenes.small_room(seed=0, width=W, height=H)
     ds = ff.dScene(ctx, scn)
@@ -947,15 +1135,12 @@ def run_cache(args, ws, rank, local, dist):
         cache = RadianceCache(ds)
         pt = ff.PathTracer(ctx, W, H)
         st = cache.render(ds, pt, frames=args.cache_frames_only, seed=12, **kw)
-        if rank == 0:
-            print(json.dumps({"workload": "cached frames only (profiling)", "frames": args.cache_frames_only,
-                              "ms_total": st["ms_total"], "queries": st["cache_queries"],
-                              "records": st["cache_records"]}), flush=True)
         cache.close()
         pt.close()
         ds.close()
-        ctx.close()
-        return
+        return ({"workload": "cached frames only (profiling)", "frames": args.cache_frames_only,
+                 "ms_total": st["ms_total"], "queries": st["cache_queries"], "records": st["cache_records"]}
+                if rank == 0 else None)
     tile = convergence.centre_tile(W, H)
     ref, info = convergence.reference_image(ctx, ds, scn.camera, W, H, tile=tile, mode=ff.FF_MODE_CORRECTED, **kw)
     x0, y0, tw, th = tile
@@ -1054,11 +1239,10 @@ def run_cache(args, ws, rank, local, dist):
                         "d2h_bytes_per_step": W * H * 20},
                 "gpu_launches": int(warm["kernel_launches"]) + sum(1 for _ in cache_traj),
                 "clocks": clk}
-        print(json.dumps(line), flush=True)
     cache.close()
     pt.close()
     ds.close()
-    ctx.close()
+    return line if rank == 0 else None
 
 
 def main(argv=None):
@@ -1078,7 +1262,10 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-relmse", action="store_true", help="skip the 16k-spp reference tile and its relMSE")
     ap.add_argument("--no-ref-cuda", action="store_true", help="trace workload: skip the reference's GPU traversal")
-    ap.add_argument("--with-trace", action="store_true", help="also run the trace micro-benchmark (render line)")
+    ap.add_argument("--render-only", action="store_true",
+                    help="render workload: skip the trace, small-room, adjoint and cache lines")
+    ap.add_argument("--no-oracle-check", action="store_true",
+                    help="trace workload: skip the check of every ray against the oracle")
     ap.add_argument("--spp", type=int, default=RENDER["spp"], help="render workload: samples per pixel per step")
     args = ap.parse_args(argv)
     RENDER["spp"] = args.spp

@@ -206,11 +206,14 @@ class dScene:
         _check(lib().ff_scene_get_stats(self.handle, C.byref(st)), self.ctx.handle)
         return {k: (list(getattr(st, k)) if k.startswith("scene_") else getattr(st, k)) for k, _ in st._fields_}
 
-    def trace(self, rays: np.ndarray, any_hit: bool = False, out: np.ndarray | None = None) -> np.ndarray:
+    def trace(self, rays: np.ndarray, any_hit: bool = False, out: np.ndarray | None = None,
+              two_sided: bool = False) -> np.ndarray:
         """Host rays (n x 8 float32 or RAY_DTYPE) -> host hits (HIT_DTYPE).
 
         Synchronous: copies the rays in, traces, copies the hits out.  Pass
-        pinned buffers (rays and ``out``) for full copy bandwidth."""
+        pinned buffers (rays and ``out``) for full copy bandwidth.
+        two_sided: closest hits that also take back faces (FF_TRACE_TWO_SIDED;
+        a back face reports prim = -2 - index)."""
         if rays.dtype == RAY_DTYPE:
             rays = rays.view(np.float32)
         r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
@@ -218,22 +221,23 @@ class dScene:
             out = np.empty(r.shape[0], HIT_DTYPE)
         elif out.dtype != HIT_DTYPE or out.shape != (r.shape[0],) or not out.flags.c_contiguous:
             raise ValueError("out must be a contiguous HIT_DTYPE array with one entry per ray")
-        flags = A.FF_TRACE_ANY if any_hit else A.FF_TRACE_CLOSEST
+        flags = (A.FF_TRACE_ANY if any_hit else A.FF_TRACE_CLOSEST) | (A.FF_TRACE_TWO_SIDED if two_sided else 0)
         _check(lib().ff_trace(self.ctx.handle, self.handle, _ptr(r), r.shape[0], _ptr(out), flags),
                self.ctx.handle)
         return out
 
-    def trace_device(self, rays_ptr: int, n: int, hits_ptr: int, any_hit: bool = False):
+    def trace_device(self, rays_ptr: int, n: int, hits_ptr: int, any_hit: bool = False, two_sided: bool = False):
         """Device pointers (e.g. torch tensors' data_ptr()), asynchronous on the context stream."""
         flags = (A.FF_TRACE_ANY if any_hit else A.FF_TRACE_CLOSEST) | A.FF_MEM_DEVICE
+        flags |= A.FF_TRACE_TWO_SIDED if two_sided else 0
         _check(lib().ff_trace(self.ctx.handle, self.handle, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr), flags),
                self.ctx.handle)
 
-    def trace_count(self, rays, n: int | None = None, any_hit: bool = False) -> dict:
+    def trace_count(self, rays, n: int | None = None, any_hit: bool = False, two_sided: bool = False) -> dict:
         """Traversal work of the rays (host array, or a device pointer with
         n): node records fetched, triangles tested, and the fetched bytes per
         ray (records times their sizes), for the same traversal ff_trace runs."""
-        flags = A.FF_TRACE_ANY if any_hit else A.FF_TRACE_CLOSEST
+        flags = (A.FF_TRACE_ANY if any_hit else A.FF_TRACE_CLOSEST) | (A.FF_TRACE_TWO_SIDED if two_sided else 0)
         if isinstance(rays, int):
             ptr, count = C.c_void_p(rays), int(n)
             flags |= A.FF_MEM_DEVICE

@@ -27,6 +27,7 @@ FF_MEM_HOST = 0
 FF_MEM_DEVICE = 1
 FF_TRACE_CLOSEST = 0
 FF_TRACE_ANY = 2
+FF_TRACE_TWO_SIDED = 4
 FF_RENDER_PROFILE = 1
 FF_LIGHT_ALL = -2
 FF_ADJOINT_STORE_ALL = 4
@@ -37,6 +38,7 @@ FF_CACHE_LEVELS = 16
 FF_CACHE_MLP_PARAMS = 5 * 64 * 64
 FF_MODE_PARITY = 0
 FF_MODE_CORRECTED = 1
+FF_DEBUG_WAIT_DEFAULT = 0xFFFFFFFF
 
 FF_MAT_MIX = 0
 FF_MAT_DIFFUSE = 1
@@ -172,6 +174,9 @@ SIGNATURES = {
     "ff_cache_read_params": (C.c_int, [P, P, P, P, P]),
     "ff_cache_write_params": (C.c_int, [P, P, P]),
     "ff_render_cached": (C.c_int, [P, P, P, C.POINTER(ff_render_settings), P, C.POINTER(ff_render_stats)]),
+    "ff_debug_alloc_stats": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_int64)]),
+    "ff_debug_fail_alloc_after": (C.c_int, [C.c_int64]),
+    "ff_debug_cache_wait_limit": (C.c_int, [P, C.c_uint32]),
 }
 
 _lib = None

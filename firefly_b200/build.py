@@ -13,6 +13,7 @@ import argparse
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -58,18 +59,27 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
         return LIB
     OBJDIR.mkdir(parents=True, exist_ok=True)
     LIBDIR.mkdir(parents=True, exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for src in _sources():
         obj = OBJDIR / (src.stem + ".o")
         flags = list(COMMON)
         flags += ["-fmad=false"] if src.name in NO_FMAD else ["-fmad=true"]
         if ptxas_info:
             flags += ["-Xptxas", "-v"]
-        cmd = [NVCC, *ARCH, *flags, "-c", str(src), "-o", str(obj)]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append([NVCC, *ARCH, *flags, "-c", str(src), "-o", str(obj)])
         objs.append(str(obj))
+    # translation units compile independently: one nvcc per core
+    jobs = max(1, min(len(cmds), os.cpu_count() or 1))
+    with ThreadPoolExecutor(jobs) as pool:
+        results = list(pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+    for cmd, res in zip(cmds, results):
+        if verbose or res.returncode != 0 or ptxas_info:
+            print(" ".join(cmd), flush=True)
+            sys.stdout.write(res.stdout)
+            sys.stderr.write(res.stderr)
+    failed = [c for c, r in zip(cmds, results) if r.returncode != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(tmp), *objs, "-lpthread"]
     if verbose:

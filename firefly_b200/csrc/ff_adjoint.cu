@@ -24,7 +24,7 @@
 // Sampling is detached: the importance tables and the Russian-roulette
 // probability are not differentiated.  Gradients reach albedo textures of
 // FF_MAT_DIFFUSE surfaces (their BRDF is linear in the albedo), roughness
-// textures of the GGX surfaces (mixed, conductor, thin dielectric, coat:
+// textures of the GGX surfaces (mixed, conductor, rough dielectric, coat:
 // at vertex k, dI . [d(own terms)/dr + L_{>k} * dlog(ext_f)/dr] with
 // L_{>k} = L_s - (radiance up to and including vertex k's own terms), the
 // directions, pdfs and MIS weights held at their sampled values) and the
@@ -69,24 +69,24 @@ struct ADJ {
 
 // The traversals and the shading switch are called, not inlined: each is one
 // copy of its code however many sites use it.
-__device__ __noinline__ bool closest_hit(const FFBvhView bvh, unsigned int* err, float3 o, float3 d, FFStack& st,
-                                         ff_hit& h)
+__device__ __noinline__ bool closest_hit(const FFBvhView bvh, unsigned int* err, float3 o, float3 d, bool two,
+                                         FFStack& st, ff_hit& h)
 {
     FFRayState r;
-    ff_ray_setup(r, o, d, 0.f, __int_as_float(0x7f800000), false);
+    ff_ray_setup(r, o, d, two ? -0.f : 0.f, __int_as_float(0x7f800000), false);
     if (bvh.num_nodes) {
         uint2 cur = ff_root_group(r);
         st.reset();
         uint32_t steps = 0;
-        while (!ff_traverse_step<false>(bvh, r, cur, st)) {
+        while (!ff_traverse_step<false, true>(bvh, r, cur, st)) {
             if (++steps > bvh.num_nodes + 2 || st.overflow) {
                 atomicAdd(err, 1u);
                 break;
             }
         }
     }
-    h = ff_hit{r.tmax, r.u, r.v, r.prim == 0xffffffffu ? -1 : (int32_t)r.prim};
-    return h.prim >= 0;
+    h = ff_hit_of(r);
+    return h.prim != -1;
 }
 
 __device__ __noinline__ bool occluded(const FFBvhView bvh, unsigned int* err, const ff_ray ray, FFStack& st)
@@ -107,14 +107,14 @@ __device__ __noinline__ bool occluded(const FFBvhView bvh, unsigned int* err, co
 }
 
 __device__ __noinline__ void shade_vertex(const LightCtx& lc, const FFSurf& surf, float3 pos, float3 n, float3 wo,
-                                          float3 wi, float3 sp, uint32_t key, uint32_t L, ShadeOut& sh)
+                                          float3 wi, float3 sp, uint32_t key, uint32_t L, bool back, ShadeOut& sh)
 {
     sh.c_spec = sh.c_diff = make_float3(0.f, 0.f, 0.f);
     switch (surf.kind) {
         case FF_MAT_MIX: shade_mix(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, sp, key, L, sh); break;
         case FF_MAT_DIFFUSE: shade_diffuse(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
         case FF_MAT_CONDUCTOR: shade_conductor(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
-        case FF_MAT_DIELECTRIC: shade_dielectric(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+        case FF_MAT_DIELECTRIC: shade_dielectric(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, back, sh); break;
         default: shade_coat(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
     }
 }
@@ -159,9 +159,10 @@ __device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_
     bool vis = false, vis_s = false, vis_d = false;
     float3 nee_env_coef = make_float3(0.f, 0.f, 0.f), nee_dir = make_float3(0.f, 0.f, 0.f);
     uint32_t L = 0;
+    bool inside = false;   // the ray runs inside an object: traced two-sided
     for (;;) {
         ff_hit hit;
-        const bool found = closest_hit(a.bvh, a.err, o, d, st, hit);
+        const bool found = closest_hit(a.bvh, a.err, o, d, inside, st, hit);
         ++rays;
         L += 1;
         bool terminate = (L > a.max_depth) || !found;
@@ -204,22 +205,30 @@ __device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_
         }
         if (terminate) break;
         // hit attributes
-        const FFShadeTri& t = a.shade[hit.prim];
+        const bool back = hit_back(hit.prim);   // hit from inside an object
+        const uint32_t prim = hit_index(hit.prim);
+        const FFShadeTri& t = a.shade[prim];
         const float u = hit.u, v = hit.v;
         // ng: the interpolated normal the ray offsets follow (kernel.cu:437);
-        // n: the shading normal (get_normal: a normal texture's frame, else ng)
-        const float3 ng = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
+        // n: the shading normal (get_normal: a normal texture's frame, else ng);
+        // both face the ray
+        float3 ng = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
         const float3 pos = o + hit.t * d;
         const float wuv = (1.f - u) - v;
         const float2 tuv = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x, u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
         const ff_material& mm = a.mats[t.material];
-        const float3 n = shading_normal(mm, a.tex, a.tan, (uint32_t)hit.prim, u, v, tuv, ng);
+        float3 n = shading_normal(mm, a.tex, a.tan, prim, u, v, tuv, ng);
+        if (back) {
+            ng = -ng;
+            n = -n;
+        }
         float3 wi, sp;
         sample_light(lc, pos, key, L, wi, sp);
         const FFSurf surf = resolve_surface(mm, a.tex, tuv);
         const float3 wo = -d;
-        shade_vertex(lc, surf, pos, n, wo, wi, sp, key, L, sh);
-        const float3 lo = pos + ng * a.shadow_offset;
+        shade_vertex(lc, surf, pos, n, wo, wi, sp, key, L, back, sh);
+        const bool diel = surf.kind == FF_MAT_DIELECTRIC;
+        const float3 lo = pos + ng * (((diel && dot3(wi, ng) < 0.f) ? -1.f : 1.f) * a.shadow_offset);
         sh.ray_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, sh.r_nee);
         uint32_t visible = 0;
 #pragma unroll 1
@@ -250,7 +259,7 @@ __device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_
         float3 rimm = make_float3(0.f, 0.f, 0.f);
         float3 L_after = Lacc;
         if (rough_grad) {
-            rt = rough_terms(sh, n, wo, wi, surf.roughness);
+            rt = rough_terms(sh, n, wo, wi, surf.roughness, diel);
             rimm = rough_own(rt, vis, vis_s, beta);
             float3 own = make_float3(0.f, 0.f, 0.f);
             if (vis) own = own + sh.c_nee;
@@ -287,6 +296,7 @@ __device__ __forceinline__ float3 run_path(const ADJ& a, const int mode, uint32_
         const float side = dot3(sh.ext_d, ng) >= 0.f ? 1.f : -1.f;
         o = pos + ng * (side * a.shadow_offset);
         d = sh.ext_d;
+        inside = runs_inside(back, diel, side);
     }
     return Lacc;
 }

@@ -112,19 +112,27 @@ __device__ __forceinline__ int rough_channel(const ff_material& m, int adj)
 // mixed material's BSDF-sampled light term c_spec (before the throughput and
 // the visibility gate), `dext` is d/dr log(ext_f) per channel: everything the
 // path gathers after the vertex carries one factor ext_f.  Each derivative
-// is evaluated only where its GGX value is non-zero: the thin dielectric's
-// transmission continues along -wo, where the half vector of ggx_dlog_dr is
-// undefined (0 * NaN would poison the sum).
+// is evaluated only where its GGX value is non-zero (0 * NaN would poison the
+// sum).  The dielectric's terms are proportional to its D G as well; its
+// shading leaves d log(D G)/dr at the NEE and at the sampled direction in
+// dlog_nee / dlog_spec (its half vectors differ from ggx_dlog_dr's).
 struct RoughTerms {
     float3 nee, spec, dext;
 };
-__device__ __forceinline__ RoughTerms rough_terms(const ShadeOut& sh, float3 n, float3 wo, float3 wi, float r)
+__device__ __forceinline__ RoughTerms rough_terms(const ShadeOut& sh, float3 n, float3 wo, float3 wi, float r,
+                                                  bool dielectric)
 {
     const float3 zero = make_float3(0.f, 0.f, 0.f);
     RoughTerms t;
     t.nee = zero;
     t.spec = zero;
     t.dext = zero;
+    if (dielectric) {
+        t.nee = sh.c_nee * sh.dlog_nee;
+        t.spec = sh.c_spec * sh.dlog_spec;
+        if (sh.ext_pdf != 0.f && sh.ext_f != zero) t.dext = make_float3(sh.dlog_spec, sh.dlog_spec, sh.dlog_spec);
+        return t;
+    }
     if (sh.c_nee_ggx != zero) t.nee = sh.c_nee_ggx * (float)ggx_dlog_dr(n, wi, wo, r);
     if (sh.c_spec != zero) {
         const float3 ws = make_float3(sh.r_spec.dx, sh.r_spec.dy, sh.r_spec.dz);

@@ -97,7 +97,7 @@ ff_status ff_context_create(const ff_device_opts* opts, ff_context** out)
         FF_CUDA_CHECK(cudaEventCreate(&ctx->ev1));
     });
     if (st != FF_OK) {
-        delete ctx;
+        ff_context_destroy(ctx);   // the stream, events and buffers created before the failure
         return st;
     }
     *out = ctx;
@@ -165,6 +165,7 @@ ff_status ff_scene_create(ff_context* ctx, const ff_scene_desc* d, ff_scene** ou
         for (uint32_t m = 0; m < d->num_materials; ++m) {
             const ff_material& mt = d->materials[m];
             FF_REQUIRE(mt.kind >= FF_MAT_MIX && mt.kind <= FF_MAT_COAT, "unknown material kind");
+            if (mt.kind == FF_MAT_DIELECTRIC) s->refracts = true;
             FF_REQUIRE(mt.base_color_tex < (int32_t)d->num_textures, "texture index out of range");
             FF_REQUIRE(mt.roughness_tex < (int32_t)d->num_textures, "texture index out of range");
         }
@@ -240,16 +241,18 @@ ff_status ff_trace(ff_context* ctx, const ff_scene* s, const ff_ray* rays, uint6
     return guarded(ctx, [&] {
         DeviceGuard g(ctx->device);
         const bool any = (flags & FF_TRACE_ANY) != 0;
+        const bool two = (flags & FF_TRACE_TWO_SIDED) != 0;
+        FF_REQUIRE(!(any && two), "FF_TRACE_TWO_SIDED applies to closest hits (any-hit rays are two-sided already)");
         if (flags & FF_MEM_DEVICE) {
             FF_REQUIRE((reinterpret_cast<uintptr_t>(rays) & 15) == 0 && (reinterpret_cast<uintptr_t>(hits) & 15) == 0,
                        "device rays and hits must be 16-byte aligned");
-            ff_launch_trace(ctx, s, rays, n, hits, any);
+            ff_launch_trace(ctx, s, rays, n, hits, any, two);
         } else {
             ctx->io_rays.alloc(sizeof(ff_ray) * n);
             ctx->io_hits.alloc(sizeof(ff_hit) * n);
             FF_CUDA_CHECK(cudaMemcpyAsync(ctx->io_rays.ptr, rays, sizeof(ff_ray) * n, cudaMemcpyHostToDevice,
                                           ctx->stream));
-            ff_launch_trace(ctx, s, ctx->io_rays.as<ff_ray>(), n, ctx->io_hits.as<ff_hit>(), any);
+            ff_launch_trace(ctx, s, ctx->io_rays.as<ff_ray>(), n, ctx->io_hits.as<ff_hit>(), any, two);
             FF_CUDA_CHECK(cudaMemcpyAsync(hits, ctx->io_hits.ptr, sizeof(ff_hit) * n, cudaMemcpyDeviceToHost,
                                           ctx->stream));
             unsigned int err = 0;
@@ -276,6 +279,8 @@ ff_status ff_trace_count(ff_context* ctx, const ff_scene* s, const ff_ray* rays,
     return guarded(ctx, [&] {
         DeviceGuard g(ctx->device);
         const bool any = (flags & FF_TRACE_ANY) != 0;
+        const bool two = (flags & FF_TRACE_TWO_SIDED) != 0;
+        FF_REQUIRE(!(any && two), "FF_TRACE_TWO_SIDED applies to closest hits");
         const ff_ray* d_rays = rays;
         if (flags & FF_MEM_DEVICE) {
             FF_REQUIRE((reinterpret_cast<uintptr_t>(rays) & 15) == 0, "device rays must be 16-byte aligned");
@@ -289,7 +294,7 @@ ff_status ff_trace_count(ff_context* ctx, const ff_scene* s, const ff_ray* rays,
         unsigned long long* d_out = reinterpret_cast<unsigned long long*>(ctx->counters.as<char>() + 16);
         unsigned int* err = reinterpret_cast<unsigned int*>(ctx->counters.as<char>() + 8);
         FF_CUDA_CHECK(cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), ctx->stream));
-        ff_launch_trace_count(ctx, s, d_rays, n, any, d_out, err);
+        ff_launch_trace_count(ctx, s, d_rays, n, any, d_out, err, two);
         unsigned long long h[2] = {0, 0};
         unsigned int e = 0;
         FF_CUDA_CHECK(cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
@@ -368,4 +373,21 @@ extern "C" ff_status ff_scene_set_environment(ff_scene* s, const float* rgb, uin
         else ff_env_pack(ctx, s);
         FF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
     });
+}
+
+// ------------------------------------------------------------- test hooks
+
+FFAllocStats g_ff_alloc;
+
+extern "C" ff_status ff_debug_alloc_stats(uint64_t* total, int64_t* live)
+{
+    if (total) *total = g_ff_alloc.total.load();
+    if (live) *live = g_ff_alloc.live.load();
+    return FF_OK;
+}
+
+extern "C" ff_status ff_debug_fail_alloc_after(int64_t n)
+{
+    g_ff_alloc.fail_after.store(n < 0 ? -1 : n);
+    return FF_OK;
 }

@@ -144,6 +144,7 @@ struct CacheArgs {
     float* loss;                // train: sum of the per-record losses
     float inv_n;                // train: 1 / records in the batch
     unsigned int* err;
+    uint32_t wait_polls;        // bound of each MMA wait (the drain after a failure keeps kWaitPolls)
 };
 
 __device__ __forceinline__ uint32_t count_of(const CacheArgs& a)
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_cache_infer(CacheArgs a)
                 issue_forward(tmem, x0, w0 + (uint32_t)l * kWBytes, l + 1 < kLayers ? ID_FWD : ID_OUT);
                 mma_commit(mbar);
             }
-            const bool ok = mbar_wait(mbar, phase, kWaitPolls);
+            const bool ok = mbar_wait(mbar, phase, a.wait_polls);
             phase ^= 1u;
             if (__syncthreads_or(!ok)) {
                 failed = true;
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_cache_train(CacheArgs a)
 
     auto step = [&]() -> bool {         // commit, wait, agree
         if (tid == 0) mma_commit(mbar);
-        const bool ok = mbar_wait(mbar, phase, kWaitPolls);
+        const bool ok = mbar_wait(mbar, phase, a.wait_polls);
         phase ^= 1u;
         const bool bad = __syncthreads_or(!ok);
         fence_after_sync();
@@ -577,6 +578,7 @@ static CacheArgs make_args(ff_cache* c, const Record* recs, uint32_t n, const ui
     a.grad_w = c->mlp_grad.as<float>();
     a.loss = c->loss.as<float>();
     a.err = c->err.as<unsigned int>();
+    a.wait_polls = c->wait_polls == FF_DEBUG_WAIT_DEFAULT ? kWaitPolls : c->wait_polls;
     return a;
 }
 

@@ -125,6 +125,13 @@ ff_status ff_cache_destroy(ff_cache* c)
     return FF_OK;
 }
 
+ff_status ff_debug_cache_wait_limit(ff_cache* c, uint32_t polls)
+{
+    if (!c) return FF_ERR_INVALID_ARG;
+    c->wait_polls = polls;
+    return FF_OK;
+}
+
 ff_status ff_cache_reset(ff_cache* c)
 {
     if (!c) return FF_ERR_INVALID_ARG;

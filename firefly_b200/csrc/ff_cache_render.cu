@@ -93,10 +93,11 @@ __global__ void __launch_bounds__(kBlock) k_training_paths(CR a)
         bool tail = false;
         ShadeOut sh;
         bool vis = false, vis_s = false, vis_d = false;
+        bool inside = false;   // the ray runs inside an object: traced two-sided
         uint32_t L = 0;
         for (;;) {
             ff_hit hit;
-            const bool found = ff_closest_hit(a.bvh, o, d, st, a.err, hit);
+            const bool found = ff_closest_hit(a.bvh, o, d, st, a.err, hit, inside);
             ++n_ext;
             L += 1;
             bool terminate = (L > a.max_depth) || !found;
@@ -126,17 +127,24 @@ __global__ void __launch_bounds__(kBlock) k_training_paths(CR a)
                 }
             }
             if (terminate) break;
-            const FFShadeTri& t = a.shade[hit.prim];
+            const bool back = hit_back(hit.prim);   // hit from inside an object
+            const uint32_t prim = hit_index(hit.prim);
+            const FFShadeTri& t = a.shade[prim];
             const float u = hit.u, v = hit.v;
             // ng: the interpolated normal the ray offsets follow (kernel.cu:437);
-            // n: the shading normal (get_normal: a normal texture's frame, else ng)
-            const float3 ng = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
+            // n: the shading normal (get_normal: a normal texture's frame, else ng);
+            // both face the ray
+            float3 ng = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
             const float3 pos = o + hit.t * d;
             const float wuv = (1.f - u) - v;
             const float2 tuv = make_float2(u * t.uv1.x + v * t.uv2.x + wuv * t.uv0.x,
                                            u * t.uv1.y + v * t.uv2.y + wuv * t.uv0.y);
             const ff_material& mm = a.mats[t.material];
-            const float3 n = shading_normal(mm, a.tex, a.tan, (uint32_t)hit.prim, u, v, tuv, ng);
+            float3 n = shading_normal(mm, a.tex, a.tan, prim, u, v, tuv, ng);
+            if (back) {
+                ng = -ng;
+                n = -n;
+            }
             const FFSurf surf = resolve_surface(mm, a.tex, tuv);
             const float3 wo = -d;
             if (L >= 2 && !tail && is_rough(surf, a.rough_threshold)) {
@@ -153,10 +161,13 @@ __global__ void __launch_bounds__(kBlock) k_training_paths(CR a)
                 case FF_MAT_MIX: shade_mix(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, sp, key, L, sh); break;
                 case FF_MAT_DIFFUSE: shade_diffuse(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
                 case FF_MAT_CONDUCTOR: shade_conductor(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
-                case FF_MAT_DIELECTRIC: shade_dielectric(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+                case FF_MAT_DIELECTRIC:
+                    shade_dielectric(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, back, sh);
+                    break;
                 default: shade_coat(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
             }
-            const float3 lo = pos + ng * a.shadow_offset;
+            const bool diel = surf.kind == FF_MAT_DIELECTRIC;
+            const float3 lo = pos + ng * (((diel && dot3(wi, ng) < 0.f) ? -1.f : 1.f) * a.shadow_offset);
             sh.ray_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, sh.r_nee);
             vis = sh.ray_nee && !ff_occluded(a.bvh, sh.r_nee, st, a.err);
             vis_s = sh.ray_spec && !ff_occluded(a.bvh, sh.r_spec, st, a.err);
@@ -165,6 +176,7 @@ __global__ void __launch_bounds__(kBlock) k_training_paths(CR a)
             const float side = dot3(sh.ext_d, ng) >= 0.f ? 1.f : -1.f;
             o = pos + ng * (side * a.shadow_offset);
             d = sh.ext_d;
+            inside = runs_inside(back, diel, side);
         }
         if (want_train) {
             rec.v0 = Ltail.x;

@@ -129,6 +129,10 @@ struct __align__(16) FFTri {
 // routine reports as the closest (or any) hit.
 #define FF_BOX_WIDEN 2.44140625e-4f  // 2^-12
 
+// Bit 31 of a triangle index marks a back-face hit of a two-sided ray
+// (FFRayState::prim, and the material word of a path vertex).
+constexpr uint32_t kBackFace = 0x80000000u;
+
 struct FFBvhView {
     const FFNode8* nodes;
     const FFTri* tris;

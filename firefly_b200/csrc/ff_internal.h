@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -34,6 +35,27 @@ struct FFError {
         if (!(cond)) throw FFError{FF_ERR_INVALID_ARG, (msg)}; \
     } while (0)
 
+// Device allocations made through DevBuf, process-wide (ff_debug_alloc_stats),
+// and the test hook that refuses them (ff_debug_fail_alloc_after): while
+// fail_after >= 0, that many more allocations succeed and every later one
+// fails with FF_ERR_OOM without reaching cudaMalloc.
+struct FFAllocStats {
+    std::atomic<uint64_t> total{0};
+    std::atomic<int64_t> live{0};
+    std::atomic<int64_t> fail_after{-1};
+};
+extern FFAllocStats g_ff_alloc;
+
+inline bool ff_alloc_refused()
+{
+    int64_t left = g_ff_alloc.fail_after.load();
+    while (left >= 0) {
+        if (left == 0) return true;
+        if (g_ff_alloc.fail_after.compare_exchange_weak(left, left - 1)) return false;
+    }
+    return false;
+}
+
 // Owning device allocation.
 struct DevBuf {
     void* ptr = nullptr;
@@ -44,7 +66,10 @@ struct DevBuf {
     ~DevBuf() { release(); }
     void release()
     {
-        if (ptr) cudaFree(ptr);
+        if (ptr) {
+            cudaFree(ptr);
+            g_ff_alloc.live.fetch_sub(1);
+        }
         ptr = nullptr;
         bytes = 0;
     }
@@ -53,7 +78,10 @@ struct DevBuf {
         if (n <= bytes && ptr) return;
         release();
         if (n == 0) return;
+        if (ff_alloc_refused()) throw FFError{FF_ERR_OOM, "device allocation refused (ff_debug_fail_alloc_after)"};
         FF_CUDA_CHECK(cudaMalloc(&ptr, n));
+        g_ff_alloc.total.fetch_add(1);
+        g_ff_alloc.live.fetch_add(1);
         bytes = n;
     }
     template <class T>
@@ -73,6 +101,9 @@ struct ff_context {
     DevBuf io_rays, io_hits;  // staging for host-pointer ff_trace calls
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     FFWavefrontWS* adj_ws = nullptr;   // path pool of ff_render_adjoint, kept between calls
+    // resident blocks per SM of each queue-driven k_trace variant on this
+    // context's device (0 = not yet queried), indexed by any-hit | tagged << 1 | two-sided << 2
+    int trace_bps[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 // Per-original-triangle shading attributes (read once per hit).
@@ -115,6 +146,9 @@ struct ff_scene {
     uint32_t num_dir_lights = 0;
     FFEnvLight env;
     ff_camera camera{};
+    // some material refracts (FF_MAT_DIELECTRIC): paths can run inside
+    // objects, and the path tracer traces closest hits two-sided there
+    bool refracts = false;
     ~ff_scene()
     {
         for (auto* t : textures) delete t;
@@ -160,11 +194,11 @@ void ff_build_bvh(ff_context* ctx, ff_scene* s, const float3* d_pos, const uint3
 
 // ff_trace.cu
 void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n,
-                     ff_hit* d_hits, bool any_hit);
+                     ff_hit* d_hits, bool any_hit, bool two_sided = false);
 // ff_trace.cu: traversal work counts of n device rays (ff_trace_count):
 // d_out[0] += node records fetched, d_out[1] += triangles tested.
 void ff_launch_trace_count(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n, bool any_hit,
-                           unsigned long long* d_out, unsigned int* err);
+                           unsigned long long* d_out, unsigned int* err, bool two_sided = false);
 
 // ff_trace.cu: the trace launch with caller-supplied counters (used by the
 // no-allocation entry point).
@@ -176,7 +210,8 @@ void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d
 void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
                            uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter,
                            unsigned int* err, const uint32_t* tags = nullptr, uint8_t* occ = nullptr,
-                           cudaStream_t stream = nullptr);   // null: the context's stream
+                           cudaStream_t stream = nullptr,   // null: the context's stream
+                           bool two_sided = false);          // honour the per-ray two-sided mark
 
 // ff_wavefront.cu: the path-replay adjoint on the wavefront stages.  Every
 // pointer is device memory; gradients are added to grad_* (null = not
@@ -218,6 +253,7 @@ struct ff_cache {
     DevBuf mlp, mlp_img, mlp_grad, mlp_m, mlp_v;        // FP32 weights, their bf16 images, Adam state
     DevBuf loss;          // float: sum of training losses since the last reset of the counter
     DevBuf err;           // uint32: tensor-core waits that gave up
+    uint32_t wait_polls = FF_DEBUG_WAIT_DEFAULT;   // ff_debug_cache_wait_limit
     uint32_t step = 0;    // Adam steps taken
     // ff_render_cached workspace: training runs on `aux`, beside the pixel
     // paths on the context's stream

@@ -4,7 +4,8 @@
 // mix material (wf_mat_mix + BRDF_L / BRDF_f / BRDF_pdf,
 // CUDA-RayTracer/kernel.cu:617-651, dMaterial.cu:363-469), its single-lobe
 // stages (wf_mat_diffuse / wf_mat_cook, kernel.cu:546-614) and the two kinds
-// without a reference counterpart (thin dielectric, coated diffuse).
+// without a reference counterpart (rough dielectric, coated diffuse), and the
+// rules for paths that run inside refracting objects.
 #pragma once
 
 #include "ff_shade.cuh"
@@ -20,6 +21,9 @@ struct ShadeOut {
     ff_ray r_nee, r_spec, r_diff;
     float3 ext_o, ext_d, ext_f;
     float ext_pdf, ext_cos;
+    // d/dr log f of the dielectric at the NEE direction and at the sampled
+    // direction (the adjoint only; the GGX kinds use ggx_dlog_dr instead)
+    float dlog_nee, dlog_spec;
 };
 
 __device__ __forceinline__ ff_ray make_ray(float3 o, float3 d, float tmax)
@@ -130,12 +134,34 @@ __device__ __forceinline__ bool light_vis_ray(const LightCtx& lc, float3 o, floa
 }
 
 // A vertex where the radiance cache may answer: diffuse, or glossy enough
-// (roughness at or above the threshold); a thin dielectric never.
+// (roughness at or above the threshold); a dielectric never.
 __device__ __forceinline__ bool is_rough(const FFSurf& s, float threshold)
 {
     if (s.kind == FF_MAT_DIFFUSE) return true;
     if (s.kind == FF_MAT_DIELECTRIC) return false;
     return s.roughness >= threshold;
+}
+
+// Paths inside refracting objects (no reference counterpart: the reference
+// culls back faces, dTriangle.cu:5,41).  A closest hit of a two-sided trace
+// reports a back face as prim = -2 - index (ff_hit_of); such a vertex is
+// shaded from the inside, with every normal flipped to face the ray.
+__device__ __forceinline__ bool hit_back(int32_t prim) { return prim < -1; }
+__device__ __forceinline__ uint32_t hit_index(int32_t prim) { return (uint32_t)(prim < -1 ? -2 - prim : prim); }
+
+// The continuation ray of a vertex runs inside an object, and is traced
+// two-sided, when the vertex was hit from the inside and the ray stays on
+// that side, or when the ray refracts into the object.  side: the sign of
+// dot(ext_d, ng), ng facing the incoming ray.
+__device__ __forceinline__ bool runs_inside(bool back, bool dielectric, float side)
+{
+    return back != (dielectric && side < 0.f);
+}
+
+// An extension ray; a two-sided one carries the sign bit on tmin (ff_trace.cuh).
+__device__ __forceinline__ ff_ray make_ext_ray(float3 o, float3 d, bool two)
+{
+    return ff_ray{o.x, o.y, o.z, two ? -0.f : 0.f, d.x, d.y, d.z, __int_as_float(0x7f800000)};
 }
 
 // wf_mat_mix + BRDF_L / BRDF_f / BRDF_pdf (kernel.cu:617-651, dMaterial.cu:363-469)
@@ -255,46 +281,256 @@ __device__ inline void shade_conductor(uint32_t mode, const LightCtx& lc, const 
     o.ext_cos = hmax(0.f, dot3(n, dir));
 }
 
-// Thin GGX dielectric (no reference counterpart): with probability equal to
-// the Schlick reflectance at the surface's IOR the path reflects off a GGX
-// lobe, otherwise it is transmitted through the sheet unchanged.  The
-// transmission is a delta lobe (no NEE through it); the GGX reflection gets
-// light-sampled NEE.
+// ------------------------------------------------------------ dielectric
+// Rough dielectric interface (no reference counterpart; the reference defines
+// refract() at dMaterial.cu:97-113 but never calls it).  The BSDF of Walter,
+// Marschner, Li and Torrance 2007, "Microfacet models for refraction through
+// rough surfaces":
+//   D     GGX (their eq. 33) with alpha = r^2, the reference's GGX width
+//         (dMaterial.cu:120-125), alpha at least 1e-4;
+//   G     Smith shadowing for GGX, G1(wo, h) G1(wi, h) (eq. 34);
+//   F     the exact unpolarised Fresnel reflectance of the interface (eq. 22);
+//   f_r = F D G / (4 |n.wi| |n.wo|)                                  (eq. 20)
+//   f_t = (1 - F) D G |wi.h| |wo.h| eta_o^2
+//         / (|n.wi| |n.wo| (eta_o wo.h + eta_t wi.h)^2) * tint       (eq. 21)
+// with the radiance scaling (eta_o / eta_t)^2 of a camera path folded into
+// f_t, and the transmission tinted by the base colour.  h is the half vector
+// of reflection (wi + wo) or refraction (eta_o wo + eta_t wi, eq. 16),
+// oriented to the side of n.  Sampling draws a microfacet normal m from
+// D(m) |m.n| (eqs. 35-36), then reflects off m with probability F(wo.m) and
+// refracts through it otherwise (section 5.3); the pdf of a direction is
+// D(h) |h.n| |dh/dwi| times the probability of its branch (eqs. 14, 17).
+// wo lies on the side of n, in the medium of index eta_o; eta_t is the
+// other side's.  Everything here is FP32.
+struct Diel {
+    float alpha, eta_o, eta_t;
+    float3 tint;
+};
+
+// A hit from outside enters the object (eta_o = 1, eta_t = ior); a hit on a
+// back face (the ray runs inside) leaves it.
+__device__ __forceinline__ Diel diel_of(const FFSurf& m, bool back)
+{
+    const float ior = m.ior > 0.f ? m.ior : 1.5f;
+    Diel d;
+    d.alpha = hmax(m.roughness * m.roughness, 1e-4f);
+    d.eta_o = back ? ior : 1.f;
+    d.eta_t = back ? 1.f : ior;
+    d.tint = m.albedo;
+    return d;
+}
+
+// GGX D(m) for c = n.m (0 for c <= 0).
+__device__ __forceinline__ float ggx_d(float alpha, float c)
+{
+    if (!(c > 0.f)) return 0.f;
+    const float a2 = alpha * alpha;
+    const float c2 = c * c;
+    const float k = c2 * (a2 - 1.f) + 1.f;
+    return a2 / ((FF_PI * k) * k);
+}
+
+// tan^2 of the angle between v and n, from c = n.v.
+__device__ __forceinline__ float tan2_of(float c)
+{
+    const float c2 = c * c;
+    return hmax(0.f, 1.f - c2) / c2;
+}
+
+// Smith G1 for GGX: 2 / (1 + sqrt(1 + alpha^2 tan^2)), zero where v sees the
+// microfacet from the other side than the macro surface.
+__device__ __forceinline__ float smith_g1(float alpha, float vn, float vh)
+{
+    if (!(vh * vn > 0.f)) return 0.f;
+    return 2.f / (1.f + sqrtf(1.f + (alpha * alpha) * tan2_of(vn)));
+}
+
+// Fresnel reflectance of a dielectric interface for cos c = wo.m on the
+// incident side and relative index n = eta_t / eta_o; 1 under total
+// internal reflection.
+__device__ __forceinline__ float fresnel_dielectric(float c, float n)
+{
+    const float g2 = n * n - 1.f + c * c;
+    if (g2 < 0.f) return 1.f;
+    const float g = sqrtf(g2);
+    const float a = (g - c) / (g + c);
+    const float b = (c * (g + c) - 1.f) / (c * (g - c) + 1.f);
+    return (0.5f * (a * a)) * (1.f + b * b);
+}
+
+// Half vector of (wo, wi); false when the pair has none (grazing, or wi on
+// the wrong side of the microfacet).
+__device__ __forceinline__ bool diel_half(const Diel& d, float3 n, float3 wo, float3 wi, bool& refl, float3& h)
+{
+    const float cos_o = dot3(n, wo), cos_i = dot3(n, wi);
+    if (!(cos_o > 0.f) || cos_i == 0.f) return false;
+    refl = cos_i > 0.f;
+    if (refl) {
+        h = wo + wi;
+    } else {
+        h = wo * d.eta_o + wi * d.eta_t;
+    }
+    const float l2 = dot3(h, h);
+    if (!(l2 > 0.f)) return false;
+    h = normalize3(h);
+    if (dot3(h, n) < 0.f) h = -h;
+    const float woh = dot3(wo, h), wih = dot3(wi, h);
+    if (!(woh > 0.f)) return false;
+    return refl ? wih > 0.f : wih < 0.f;
+}
+
+// f(wi, wo) and the pdf of sampling wi given wo.
+__device__ __forceinline__ void diel_eval(const Diel& d, float3 n, float3 wo, float3 wi, float3& f, float& pdf)
+{
+    f = make_float3(0.f, 0.f, 0.f);
+    pdf = 0.f;
+    bool refl;
+    float3 h;
+    if (!diel_half(d, n, wo, wi, refl, h)) return;
+    const float cos_o = dot3(n, wo), cos_i = fabsf(dot3(n, wi));
+    const float ch = dot3(n, h), woh = dot3(wo, h), wih = dot3(wi, h);
+    const float D = ggx_d(d.alpha, ch);
+    const float G = smith_g1(d.alpha, cos_o, woh) * smith_g1(d.alpha, dot3(n, wi), wih);
+    const float F = fresnel_dielectric(woh, d.eta_t / d.eta_o);
+    if (refl) {
+        const float v = ((F * D) * G) / ((4.f * cos_i) * cos_o);
+        f = make_float3(v, v, v);
+        pdf = ((F * D) * ch) / (4.f * woh);
+    } else {
+        const float den = d.eta_o * woh + d.eta_t * wih;
+        const float den2 = den * den;
+        const float v = (((((1.f - F) * D) * G) * (-wih)) * woh * (d.eta_o * d.eta_o)) / ((cos_i * cos_o) * den2);
+        f = d.tint * v;
+        pdf = ((((1.f - F) * D) * ch) * (d.eta_t * d.eta_t) * (-wih)) / den2;
+    }
+}
+
+// A microfacet normal drawn from D(m) |m.n| (Walter et al. eqs. 35-36):
+// tan^2 theta = alpha^2 e0 / (1 - e0), phi = 2 pi e1, in the frame of n.
+__device__ __forceinline__ float3 ggx_sample_normal(float3 n, float alpha, float e0, float e1)
+{
+    const float t2 = (alpha * alpha) * (e0 / (1.f - e0));
+    const float ct = 1.f / sqrtf(1.f + t2);
+    const float st = sqrtf(t2) * ct;
+    const float phi = FF_2PI * e1;
+    float3 T, B;
+    frame(n, T, B);
+    return normalize3(T * (st * cosf(phi)) + B * (st * sinf(phi)) + n * ct);
+}
+
+// The sampled direction (reflection with probability F, else refraction);
+// false when the drawn microfacet faces away from wo, or when the reflected
+// (refracted) direction ends below (above) the macro surface: diel_eval
+// classifies a direction by its side of n, so such a sample has no density
+// under the branch that drew it and is dropped (weight 0), as in Walter et
+// al.'s sampling.
+__device__ __forceinline__ bool diel_sample(const Diel& d, float3 n, float3 wo, float e0, float e1, float e2,
+                                            float3& wi)
+{
+    const float3 m = ggx_sample_normal(n, d.alpha, e0, e1);
+    const float woh = dot3(wo, m);
+    if (!(woh > 0.f)) return false;
+    const float F = fresnel_dielectric(woh, d.eta_t / d.eta_o);
+    const bool refl = e2 < F;
+    float3 w;
+    if (refl) {
+        w = m * (2.f * woh) - wo;
+    } else {
+        const float eta = d.eta_o / d.eta_t;
+        const float k = 1.f - (eta * eta) * (1.f - woh * woh);
+        w = m * (eta * woh - sqrtf(hmax(k, 0.f))) - wo * eta;
+    }
+    w = normalize3(w);
+    const float c = dot3(n, w);
+    if (refl ? !(c > 0.f) : !(c < 0.f)) return false;
+    wi = w;
+    return true;
+}
+
+// d/dr of log(D G) at the pair (wo, wi) (the Fresnel term and the Jacobian
+// do not depend on the roughness): with alpha = r^2,
+//   dlogD/dalpha = 2 / alpha - 4 alpha c^2 / (c^2 (alpha^2 - 1) + 1)
+//   dlogG1/dalpha = -(alpha tan^2 / s) / (1 + s),  s = sqrt(1 + alpha^2 tan^2)
+// times dalpha/dr = 2 r (0 where alpha sits at its floor).  The adjoint only.
+__device__ __forceinline__ float diel_dlog_dr(const Diel& d, float3 n, float3 wo, float3 wi, float r)
+{
+    bool refl;
+    float3 h;
+    if (!diel_half(d, n, wo, wi, refl, h) || !(r * r > 1e-4f)) return 0.f;
+    const float a = d.alpha;
+    const float c = dot3(n, h), c2 = c * c;
+    const float dD = 2.f / a - 4.f * a * c2 / (c2 * (a * a - 1.f) + 1.f);
+    float dG = 0.f;
+    const float cs[2] = {dot3(n, wo), dot3(n, wi)};
+    for (int k = 0; k < 2; ++k) {
+        const float t2 = tan2_of(cs[k]);
+        const float sq = sqrtf(1.f + a * a * t2);
+        dG -= (a * t2 / sq) / (1.f + sq);
+    }
+    return 2.f * r * (dD + dG);
+}
+
+__device__ __forceinline__ float power_heuristic_f(float f, float g)
+{
+    const float f2 = f * f;
+    return f2 / (f2 + g * g);
+}
+
+// The dielectric vertex: light-sampled NEE weighted against the BSDF's pdf
+// (power heuristic; weight 1 for a delta light), the continuation sampled
+// from the BSDF, and, unless the light is a delta light, the light reached
+// along the continuation direction weighted against the light's pdf, traced
+// as a shadow ray (c_spec / r_spec, as BRDF_L's BSDF-sampled terms).  back:
+// the vertex was hit from inside the object.  The NEE shadow ray and the
+// continuation leave on the side of their direction (k_shade).
 __device__ inline void shade_dielectric(uint32_t mode, const LightCtx& lc, const FFSurf& mat, float3 pos, float3 n,
-                                 float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
+                                        float3 wo, float3 wi, uint32_t key, uint32_t L, bool back, ShadeOut& o)
 {
     (void)mode;
-    const float eta = mat.ior > 0.f ? mat.ior : 1.5f;
-    const float r0 = ((eta - 1.f) / (eta + 1.f)) * ((eta - 1.f) / (eta + 1.f));
-    const float cos_o = fabsf(dot3(n, wo));
-    const float x = 1.f - cos_o;
-    const float Fr = r0 + (1.f - r0) * x * x * x * x * x;
-    FFSurf m = mat;
-    m.fresnel = make_float3(r0, r0, r0);
-    m.albedo = make_float3(1.f, 1.f, 1.f);
-    m.metallic = 0.f;
+    const Diel d = diel_of(mat, back);
+    const float3 zero = make_float3(0.f, 0.f, 0.f);
     o.ray_spec = o.ray_diff = false;
-    o.c_nee = make_float3(0.f, 0.f, 0.f);
-    const float nd = dot3(n, wi);
-    const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
-    if (nd > 0.f && lpdf > 0.f) o.c_nee = ((spec_f(m, n, wi, wo) * nd) * light_L(lc, wi)) / lpdf;
-    o.c_nee_ggx = o.c_nee;
-    if (ff_rand(key, dim_of(L, DIM_EXTRA)) < Fr) {
-        const float3 dir = spec_sample(n, wo, m.roughness, ff_rand(key, dim_of(L, DIM_SPEC)),
-                                       ff_rand(key, dim_of(L, DIM_SPEC + 1)));
-        o.ext_d = dir;
-        o.ext_f = spec_f(m, n, dir, wo) / Fr;
-        o.ext_f_ggx = o.ext_f;
-        o.ext_pdf = spec_get_pdf(n, dir, wo, m.roughness);
-        o.ext_cos = hmax(0.f, dot3(n, dir));
-    } else {
-        const float3 tint = mat.albedo;
-        o.ext_d = -wo;
-        o.ext_f = tint;
-        o.ext_f_ggx = make_float3(0.f, 0.f, 0.f);
-        o.ext_pdf = 1.f;
-        o.ext_cos = 1.f;
+    o.c_nee = o.c_spec = o.c_diff = zero;
+    o.dlog_nee = o.dlog_spec = 0.f;
+    {
+        float3 f;
+        float bpdf;
+        diel_eval(d, n, wo, wi, f, bpdf);
+        const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+        if (f != zero && lpdf > 0.f) {
+            const float w = lc.is_dir ? 1.f : power_heuristic_f(lpdf, bpdf);
+            o.c_nee = ((f * (fabsf(dot3(n, wi)) * w)) * light_L(lc, wi)) / lpdf;
+            o.dlog_nee = diel_dlog_dr(d, n, wo, wi, mat.roughness);
+        }
     }
+    o.c_nee_ggx = o.c_nee;
+    float3 dir = n;
+    float3 f = zero;
+    float pdf = 0.f;
+    if (diel_sample(d, n, wo, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)),
+                    ff_rand(key, dim_of(L, DIM_EXTRA)), dir))
+        diel_eval(d, n, wo, dir, f, pdf);
+    else
+        dir = n;
+    const float c = fabsf(dot3(n, dir));
+    if (pdf > 0.f && f != zero) {
+        o.dlog_spec = diel_dlog_dr(d, n, wo, dir, mat.roughness);
+        ff_ray vr;
+        if (!lc.is_dir && light_vis_ray(lc, pos + dir * 0.001f, dir, key, L, DIM_SPEC_VIS, vr)) {
+            const float3 Li = light_L(lc, dir);
+            if (Li != zero) {
+                const float w = power_heuristic_f(pdf, light_pdf(lc, pos, dir, key, L, DIM_SPEC_PDF));
+                o.c_spec = ((f * (c * w)) * Li) / pdf;
+                o.ray_spec = true;
+                o.r_spec = vr;
+            }
+        }
+    }
+    o.ext_d = dir;
+    o.ext_f = f;
+    o.ext_f_ggx = f;
+    o.ext_pdf = pdf;
+    o.ext_cos = c;
 }
 
 // Diffuse base under a GGX clear coat (no reference counterpart): the coat

@@ -22,7 +22,10 @@ constexpr int kRefillIdle = 8;
 // the next stage reads its hit in slot order without the queue index), an
 // any-hit answer to occ[tag] (1 occluded, 0 clear; tag = 4 * slot + shadow
 // ray index, so the next stage reads one 4-byte word of answers per slot).
-template <bool ANY, bool TAGGED>
+//
+// TWO (closest hit only): rays whose tmin carries the sign bit are traced
+// two-sided (ff_test_tri_closest); a back-face hit reports prim = -2 - index.
+template <bool ANY, bool TAGGED, bool TWO = false>
 __global__ void __launch_bounds__(kTraceBlock, 8)
     k_trace(FFBvhView bvh, const ff_ray* __restrict__ rays, ff_hit* __restrict__ hits, uint64_t n,
             unsigned long long* __restrict__ counter, unsigned int* __restrict__ err,
@@ -65,7 +68,10 @@ __global__ void __launch_bounds__(kTraceBlock, 8)
                     const float4 r0 = __ldg(reinterpret_cast<const float4*>(rays + ray_id));
                     const float4 r1 = __ldg(reinterpret_cast<const float4*>(rays + ray_id) + 1);
                     if (TAGGED) tag = __ldg(tags + ray_id);
-                    ff_ray_setup(r, make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), r0.w, r1.w, ANY);
+                    // untagged two-sided launches (ff_trace with FF_TRACE_TWO_SIDED) mark every ray;
+                    // tagged ones (the wavefront) carry the mark in each ray's tmin
+                    const float tmin = (TWO && !TAGGED) ? -(r0.w > 0.f ? r0.w : 0.f) : r0.w;
+                    ff_ray_setup(r, make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), tmin, r1.w, ANY);
                     cur = ff_root_group(r);
                     st.reset();
                     steps = 0;
@@ -87,10 +93,10 @@ __global__ void __launch_bounds__(kTraceBlock, 8)
         // Traverse until enough lanes are idle to make a refill worthwhile.
         while (true) {
             if (active) {
-                const bool done = ff_traverse_step<ANY>(bvh, r, cur, st);
+                const bool done = ff_traverse_step<ANY, TWO>(bvh, r, cur, st);
                 if (st.overflow || ++steps > max_steps) atomicAdd(err, 1u);
                 if (done || steps > max_steps) {
-                    const int32_t prim = r.prim == 0xffffffffu ? -1 : (int32_t)r.prim;
+                    const int32_t prim = TWO ? ff_hit_of(r).prim : (r.prim == 0xffffffffu ? -1 : (int32_t)r.prim);
                     const float4 out = make_float4(r.tmax, r.u, r.v, __int_as_float(prim));
                     if (!TAGGED) *reinterpret_cast<float4*>(hits + ray_id) = out;
                     else if (ANY) occ[tag] = prim >= 0 ? 1 : 0;
@@ -108,7 +114,7 @@ __global__ void __launch_bounds__(kTraceBlock, 8)
 // Traversal work of n rays (ff_trace_count): one thread per ray over the same
 // traversal step as k_trace, so each ray visits the same nodes and tests the
 // same triangles; out[0] += node records fetched, out[1] += triangles tested.
-template <bool ANY>
+template <bool ANY, bool TWO = false>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_count(FFBvhView bvh, const ff_ray* __restrict__ rays,
                                                              uint64_t n, unsigned long long* __restrict__ out,
                                                              unsigned int* __restrict__ err)
@@ -125,11 +131,12 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_count(FFBvhView bvh, cons
         const float4 r0 = __ldg(reinterpret_cast<const float4*>(rays + i));
         const float4 r1 = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
         FFRayState r;
-        ff_ray_setup(r, make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), r0.w, r1.w, ANY);
+        const float tmin = TWO ? -(r0.w > 0.f ? r0.w : 0.f) : r0.w;
+        ff_ray_setup(r, make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), tmin, r1.w, ANY);
         uint2 cur = ff_root_group(r);
         st.reset();
         uint32_t steps = 0;
-        while (!ff_traverse_step<ANY>(bvh, r, cur, st, count)) {
+        while (!ff_traverse_step<ANY, FFCount, TWO>(bvh, r, cur, st, count)) {
             if (st.overflow || ++steps > max_steps) {
                 atomicAdd(err, 1u);
                 break;
@@ -151,7 +158,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_count(FFBvhView bvh, cons
 }  // namespace
 
 void ff_launch_trace_count(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n, bool any_hit,
-                           unsigned long long* d_out, unsigned int* err)
+                           unsigned long long* d_out, unsigned int* err, bool two_sided)
 {
     if (n == 0) return;
     uint64_t grid = (uint64_t)ctx->num_sms * 8;
@@ -159,13 +166,15 @@ void ff_launch_trace_count(ff_context* ctx, const ff_scene* s, const ff_ray* d_r
     if (grid > need) grid = need;
     if (any_hit)
         k_trace_count<true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, n, d_out, err);
+    else if (two_sided)
+        k_trace_count<false, true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, n, d_out, err);
     else
         k_trace_count<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, n, d_out, err);
     FF_CUDA_CHECK(cudaGetLastError());
 }
 
 void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, uint64_t n, ff_hit* d_hits,
-                     bool any_hit)
+                     bool any_hit, bool two_sided)
 {
     if (n == 0) return;
     unsigned long long* counter = ctx->counters.as<unsigned long long>();
@@ -173,11 +182,10 @@ void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, u
     // until read by ff_trace_errors / the host-pointer path)
     unsigned int* err = reinterpret_cast<unsigned int*>(ctx->counters.as<char>() + 8);
     FF_CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), ctx->stream));
+    const void* fn = any_hit ? (const void*)k_trace<true, false>
+                             : (two_sided ? (const void*)k_trace<false, false, true> : (const void*)k_trace<false, false>);
     int blocks_per_sm = 0;
-    if (any_hit)
-        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true, false>, kTraceBlock, 0));
-    else
-        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false, false>, kTraceBlock, 0));
+    FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, fn, kTraceBlock, 0));
     blocks_per_sm = blocks_per_sm < 1 ? 1 : blocks_per_sm;
     uint64_t grid = (uint64_t)ctx->num_sms * blocks_per_sm;
     const uint64_t need = (n + kTraceBlock - 1) / kTraceBlock;
@@ -185,6 +193,9 @@ void ff_launch_trace(ff_context* ctx, const ff_scene* s, const ff_ray* d_rays, u
     if (any_hit)
         k_trace<true, false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter,
                                                                               err, nullptr, nullptr, nullptr);
+    else if (two_sided)
+        k_trace<false, false, true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(
+            s->view(), d_rays, d_hits, n, counter, err, nullptr, nullptr, nullptr);
     else
         k_trace<false, false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, d_hits, n, counter,
                                                                               err, nullptr, nullptr, nullptr);
@@ -217,33 +228,32 @@ void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d
 
 // Trace a device-resident queue whose length the previous stage wrote to
 // n_dev (at most cap rays), on the context's stream.  counter must be zeroed
-// by the caller before the launch.
+// by the caller before the launch.  two_sided (closest hit only): the
+// kernel honours the per-ray two-sided mark (the sign bit of tmin).
 void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
                            uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter, unsigned int* err,
-                           const uint32_t* tags, uint8_t* occ, cudaStream_t stream)
+                           const uint32_t* tags, uint8_t* occ, cudaStream_t stream, bool two_sided)
 {
     if (cap == 0) return;
-    static int bps[2] = {0, 0};
-    int& blocks_per_sm = bps[any_hit ? 1 : 0];
+    const bool two = two_sided && !any_hit;
+    using Kernel = void (*)(FFBvhView, const ff_ray*, ff_hit*, uint64_t, unsigned long long*, unsigned int*,
+                            const uint32_t*, const uint32_t*, uint8_t*);
+    const Kernel fn = any_hit ? (tags ? k_trace<true, true> : k_trace<true, false>)
+                              : (tags ? (two ? k_trace<false, true, true> : k_trace<false, true>)
+                                      : (two ? k_trace<false, false, true> : k_trace<false, false>));
+    // occupancy of the variant launched, on the context's device; calls on
+    // one context are externally synchronised, so the per-context cache
+    // needs no lock
+    int& blocks_per_sm = ctx->trace_bps[(any_hit ? 1 : 0) | (tags ? 2 : 0) | (two ? 4 : 0)];
     if (blocks_per_sm == 0) {
-        if (any_hit)
-            FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<true, false>, kTraceBlock, 0));
-        else
-            FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<false, false>, kTraceBlock, 0));
-        blocks_per_sm = blocks_per_sm < 1 ? 1 : blocks_per_sm;
+        int b = 0;
+        FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kTraceBlock, 0));
+        blocks_per_sm = b < 1 ? 1 : b;
     }
     uint64_t grid = (uint64_t)ctx->num_sms * blocks_per_sm;
     const uint64_t need = (cap + kTraceBlock - 1) / kTraceBlock;
     if (grid > need) grid = need;
-    const dim3 g((unsigned)grid), b(kTraceBlock);
     cudaStream_t st = stream ? stream : ctx->stream;
-    if (any_hit && tags)
-        k_trace<true, true><<<g, b, 0, st>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev, tags, occ);
-    else if (any_hit)
-        k_trace<true, false><<<g, b, 0, st>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev, tags, occ);
-    else if (tags)
-        k_trace<false, true><<<g, b, 0, st>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev, tags, occ);
-    else
-        k_trace<false, false><<<g, b, 0, st>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev, tags, occ);
+    fn<<<dim3((unsigned)grid), dim3(kTraceBlock), 0, st>>>(bvh, d_rays, d_hits, cap, counter, err, n_dev, tags, occ);
     FF_CUDA_CHECK(cudaGetLastError());
 }

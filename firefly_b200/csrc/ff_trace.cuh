@@ -6,13 +6,32 @@
 #include "ff_common.cuh"
 
 // Per-ray traversal state kept in registers.
+//
+// Two-sided closest hits (rays inside a refracting object, and ff_trace with
+// FF_TRACE_TWO_SIDED) ride on the sign bit of tmin in the traversal kernels
+// instantiated with TWO = true: a ray whose tmin has its sign bit set (-0.0
+// for tmin 0) also accepts back faces, and such a ray's interval starts at
+// |tmin|.  A back-face hit keeps bit 31 of prim set.  Kernels with TWO =
+// false never look at the sign and cull back faces as the reference does.
 struct FFRayState {
     float3 o, d, inv;
     float tmin, tmax;   // closest-hit: tmax is the current best t (starts at min(tmax, K_HUGE))
     float u, v;
-    uint32_t prim;      // original triangle index, 0xffffffff = none
+    uint32_t prim;      // original triangle index, 0xffffffff = none; bit 31: back face (TWO kernels)
     uint32_t oct_inv;   // 7 ^ octant of d (bit a set = d_a < 0)
 };
+
+// A closest hit as the C ABI reports it: prim = the original index for a
+// front face, -2 - index for a back face of a two-sided ray, -1 for none.
+FF_D ff_hit ff_hit_of(const FFRayState& r)
+{
+    int32_t prim = -1;
+    if (r.prim != 0xffffffffu) {
+        const int32_t id = (int32_t)(r.prim & ~kBackFace);
+        prim = (r.prim & kBackFace) ? -2 - id : id;
+    }
+    return ff_hit{r.tmax, r.u, r.v, prim};
+}
 
 FF_D float safe_inv(float x)
 {
@@ -131,6 +150,14 @@ FF_D void ff_intersect_node(const FFNode8* __restrict__ nodes, uint32_t idx, con
 // edge tests compare float values, so they run in FP32 exactly as the
 // reference's float-vs-double comparisons; the FP64 reciprocal and products
 // run only for candidates that pass them.
+//
+// TWO: a ray with the sign bit of tmin set also takes back faces (no
+// reference counterpart: the reference only culls).  A back face is a
+// determinant at or below -K_EPSILON; the test then runs on the negated
+// determinant and numerators (negation is exact), i.e. the mirror image of
+// the front-face test, and the hit keeps kBackFace in prim.  Front faces go
+// through exactly the arithmetic above.
+template <bool TWO = false>
 FF_D void ff_test_tri_closest(const FFTri* __restrict__ tris, uint32_t k, FFRayState& r)
 {
     const float4 a = __ldg(&tris[k].a);
@@ -140,22 +167,28 @@ FF_D void ff_test_tri_closest(const FFTri* __restrict__ tris, uint32_t k, FFRayS
     const float3 e1 = make_float3(b.x, b.y, b.z);
     const float3 e2 = make_float3(c.x, c.y, c.z);
     const float3 pvec = rn_cross(r.d, e2);
-    const float det = rn_dot(e1, pvec);
-    if (det < FF_K_EPSILON) return;
+    float det = rn_dot(e1, pvec);
+    float sg = 1.f;
+    if (det < FF_K_EPSILON) {
+        if (!TWO || !signbit(r.tmin) || !(det <= -FF_K_EPSILON)) return;
+        sg = -1.f;
+        det = -det;
+    }
     const float3 tvec = rn_sub(r.o, v0);
-    const float uf = rn_dot(tvec, pvec);
+    const float uf = TWO ? sg * rn_dot(tvec, pvec) : rn_dot(tvec, pvec);
     if (uf < 0.f || uf > det) return;
     const float3 qvec = rn_cross(tvec, e1);
-    const float vf = rn_dot(r.d, qvec);
+    const float vf = TWO ? sg * rn_dot(r.d, qvec) : rn_dot(r.d, qvec);
     if (vf < 0.f || __fadd_rn(uf, vf) > det) return;
-    const float tf = rn_dot(e2, qvec);
+    const float tf = TWO ? sg * rn_dot(e2, qvec) : rn_dot(e2, qvec);
     const double inv_det = __drcp_rn((double)det);
     const float t = __double2float_rn(__dmul_rn((double)tf, inv_det));
-    if (t < 0.f || !(t >= r.tmin)) return;
+    if (t < 0.f || !(t >= (TWO ? fabsf(r.tmin) : r.tmin))) return;
     const uint32_t id = (uint32_t)__float_as_int(a.w);
-    if (t < r.tmax || (t == r.tmax && r.prim != 0xffffffffu && id < r.prim)) {
+    const uint32_t best = TWO ? (r.prim & ~kBackFace) : r.prim;
+    if (t < r.tmax || (t == r.tmax && r.prim != 0xffffffffu && id < best)) {
         r.tmax = t;
-        r.prim = id;
+        r.prim = (TWO && sg < 0.f) ? (id | kBackFace) : id;
         r.u = __double2float_rn(__dmul_rn((double)uf, inv_det));
         r.v = __double2float_rn(__dmul_rn((double)vf, inv_det));
     }
@@ -253,7 +286,7 @@ struct FFCount {
 // One traversal step: take the next child node of the current group, test
 // its children, then test the triangles it exposed.  Returns true when the
 // ray is finished.
-template <bool ANY, class C>
+template <bool ANY, class C, bool TWO = false>
 FF_D bool ff_traverse_step(const FFBvhView& bvh, FFRayState& r, uint2& cur, FFStack& st, C& count)
 {
     uint2 tri_group = make_uint2(0u, 0u);
@@ -281,7 +314,7 @@ FF_D bool ff_traverse_step(const FFBvhView& bvh, FFRayState& r, uint2& cur, FFSt
         if (ANY) {
             if (ff_test_tri_any(bvh.tris, tri_group.x + i, r)) return true;
         } else {
-            ff_test_tri_closest(bvh.tris, tri_group.x + i, r);
+            ff_test_tri_closest<TWO>(bvh.tris, tri_group.x + i, r);
         }
     }
     if (!(cur.y & 0xff000000u)) {
@@ -290,11 +323,11 @@ FF_D bool ff_traverse_step(const FFBvhView& bvh, FFRayState& r, uint2& cur, FFSt
     }
     return st.overflow;
 }
-template <bool ANY>
+template <bool ANY, bool TWO = false>
 FF_D bool ff_traverse_step(const FFBvhView& bvh, FFRayState& r, uint2& cur, FFStack& st)
 {
     FFNoCount none;
-    return ff_traverse_step<ANY>(bvh, r, cur, st, none);
+    return ff_traverse_step<ANY, FFNoCount, TWO>(bvh, r, cur, st, none);
 }
 
 // Root group: a fake parent whose only internal child (node 0) sits in the
@@ -305,25 +338,28 @@ FF_D uint2 ff_root_group(const FFRayState& r)
 }
 
 // One whole traversal per thread (megakernel paths): closest hit of the ray
-// (o, d, [0, inf)) or any hit of `ray`; a traversal that exceeds its step
-// bound or overflows the stack counts in *err and reports what it found.
-FF_D bool ff_closest_hit(const FFBvhView& bvh, float3 o, float3 d, FFStack& st, unsigned int* err, ff_hit& h)
+// (o, d, [0, inf)), two-sided when `two` (h.prim = -2 - index for a back
+// face), or any hit of `ray`; a traversal that exceeds its step bound or
+// overflows the stack counts in *err and reports what it found.  Returns
+// whether anything was hit.
+FF_D bool ff_closest_hit(const FFBvhView& bvh, float3 o, float3 d, FFStack& st, unsigned int* err, ff_hit& h,
+                         bool two = false)
 {
     FFRayState r;
-    ff_ray_setup(r, o, d, 0.f, __int_as_float(0x7f800000), false);
+    ff_ray_setup(r, o, d, two ? -0.f : 0.f, __int_as_float(0x7f800000), false);
     if (bvh.num_nodes) {
         uint2 cur = ff_root_group(r);
         st.reset();
         uint32_t steps = 0;
-        while (!ff_traverse_step<false>(bvh, r, cur, st)) {
+        while (!ff_traverse_step<false, true>(bvh, r, cur, st)) {
             if (++steps > bvh.num_nodes + 2 || st.overflow) {
                 atomicAdd(err, 1u);
                 break;
             }
         }
     }
-    h = ff_hit{r.tmax, r.u, r.v, r.prim == 0xffffffffu ? -1 : (int32_t)r.prim};
-    return h.prim >= 0;
+    h = ff_hit_of(r);
+    return h.prim != -1;
 }
 
 FF_D bool ff_occluded(const FFBvhView& bvh, const ff_ray& ray, FFStack& st, unsigned int* err)

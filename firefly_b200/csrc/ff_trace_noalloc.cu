@@ -39,7 +39,10 @@ void* g_scratch_addr[kMaxDevices] = {};
 // is only a host-side stand-in; the device address comes from
 // cudaGetSymbolAddress, taken once per device with that device current (the
 // first call on each device does this, so it must not be the first call
-// inside a stream capture).
+// inside a stream capture).  The address stays cached for the life of the
+// process: a cudaDeviceReset frees the array's device copy together with
+// every context and scene of this library on that device, after which this
+// entry point must not be called there.
 unsigned char* scratch_on(int dev)
 {
     std::lock_guard<std::mutex> lk(g_scratch_mu);
@@ -71,6 +74,10 @@ extern "C" ff_status ff_trace_host_noalloc(ff_context* ctx, const ff_scene* s, c
     }
     if (flags & FF_MEM_DEVICE) {
         ctx->last_error = "ff_trace_host_noalloc takes host pointers; use ff_trace for device pointers";
+        return FF_ERR_INVALID_ARG;
+    }
+    if (flags & FF_TRACE_TWO_SIDED) {
+        ctx->last_error = "ff_trace_host_noalloc traces one-sided closest hits or any hits; use ff_trace for FF_TRACE_TWO_SIDED";
         return FF_ERR_INVALID_ARG;
     }
     if (n == 0) return FF_OK;

@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             const uint32_t key = w.key[s];
             const ff_hit hit = w.ext_hits[s];
             const uint32_t L = w.length[s] + 1;  // wf_extend's length++
-            const bool found = hit.prim >= 0;
+            const bool found = hit.prim != -1;
             const float3 ro = xyz(w.ray_o[s]), rd = xyz(w.ray_d[s]);
             float3 beta = xyz(w.beta[s]);
             float4 acc = w.acc[s];
@@ -323,9 +323,11 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             ffc::Record rec;
             if (!terminate) {
                 // Continue: hit attributes (dTriangle::hit, dTriangle.cu:94-105).
-                const FFShadeTri& t = w.shade[hit.prim];
+                const bool back = hit_back(hit.prim);
+                const uint32_t prim = hit_index(hit.prim);
+                const FFShadeTri& t = w.shade[prim];
                 const float u = hit.u, v = hit.v;
-                const float3 n = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
+                float3 n = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
                 const float3 pos = ro + hit.t * rd;
                 // texcoord = u * uv1 + v * uv2 + (1 - u - v) * uv0 (dTriangle.cu:97)
                 const float wuv = (1.f - u) - v;
@@ -334,7 +336,11 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 const ff_material& mm = w.mats[t.material];
                 // get_normal: the shading normal (a normal texture's frame, else
                 // n); n stays the normal the ray offsets follow (kernel.cu:437)
-                const float3 ns = shading_normal(mm, w.tex, w.tan, (uint32_t)hit.prim, u, v, uv, n);
+                float3 ns = shading_normal(mm, w.tex, w.tan, prim, u, v, uv, n);
+                if (back) {   // a back face of a two-sided ray: shaded from the inside
+                    n = -n;
+                    ns = -ns;
+                }
                 if (!ADJ && w.cache_mode && L >= 2) {
                     const FFSurf surf = resolve_surface(mm, w.tex, uv);
                     if (is_rough(surf, w.rough_threshold)) {
@@ -351,7 +357,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                     sample_light(select_light(w.lights, key, L), pos, key, L, wi, sp);
                     w.length[s] = L;
                     w.beta[s] = f4(beta);
-                    w.hit_pos[s] = f4(pos, __uint_as_float(t.material));
+                    w.hit_pos[s] = f4(pos, __uint_as_float(t.material | (back ? kBackFace : 0u)));
                     w.hit_nrm[s] = f4(ns);
                     if (mm.normal_tex >= 0) w.hit_ngeo[s] = f4(n);
                     w.light_wi[s] = f4(wi);
@@ -432,12 +438,14 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
         const bool valid = qi < n;
         ShadeOut o;
         o.ray_nee = o.ray_spec = o.ray_diff = false;
+        bool ext_two = false;   // the continuation runs inside an object: traced two-sided
         uint32_t s = 0;
         if (valid) {
             s = w.mat_queue[(size_t)KIND * w.P + qi];
             const float4 hp = w.hit_pos[s];
             const float3 pos = xyz(hp);
-            const ff_material& mm = w.mats[__float_as_uint(hp.w)];
+            const bool back = (__float_as_uint(hp.w) & kBackFace) != 0;   // hit from inside an object
+            const ff_material& mm = w.mats[__float_as_uint(hp.w) & ~kBackFace];
             const FFSurf mat = resolve_surface(mm, w.tex, w.hit_uv[s]);
             const float3 n = xyz(w.hit_nrm[s]);   // shading normal
             // the normal the ray offsets follow (kernel.cu:437): differs from n
@@ -453,17 +461,21 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
             if (KIND == FF_MAT_MIX) shade_mix(w.mode, lc, mat, pos, n, wo, wi, sp, key, L, o);
             else if (KIND == FF_MAT_DIFFUSE) shade_diffuse(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
             else if (KIND == FF_MAT_CONDUCTOR) shade_conductor(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
-            else if (KIND == FF_MAT_DIELECTRIC) shade_dielectric(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
+            else if (KIND == FF_MAT_DIELECTRIC) shade_dielectric(w.mode, lc, mat, pos, n, wo, wi, key, L, back, o);
             else shade_coat(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
-            // NEE shadow ray of wf_shadow: light_ray = position + normal * SHADOW_OFFSET (kernel.cu:437)
-            const float3 lo = pos + ng * w.shadow_offset;
+            // NEE shadow ray of wf_shadow: light_ray = position + normal * SHADOW_OFFSET (kernel.cu:437);
+            // a dielectric's light may lie on the far side
+            const float nee_side = (KIND == FF_MAT_DIELECTRIC && dot3(wi, ng) < 0.f) ? -1.f : 1.f;
+            const float3 lo = pos + ng * (nee_side * w.shadow_offset);
             o.ray_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, o.r_nee);
-            // continuation ray: the reference starts it at the hit point (kernel.cu:643)
+            // continuation ray: the reference starts it at the hit point (kernel.cu:643);
+            // corrected mode, and every ray that leaves a dielectric or an
+            // inside vertex, starts off the surface on the side it leaves
+            const float side = dot3(o.ext_d, ng) >= 0.f ? 1.f : -1.f;
             o.ext_o = pos;
-            if (w.mode == FF_MODE_CORRECTED) {
-                const float side = dot3(o.ext_d, ng) >= 0.f ? 1.f : -1.f;
+            if (w.mode == FF_MODE_CORRECTED || KIND == FF_MAT_DIELECTRIC || back)
                 o.ext_o = pos + ng * (side * w.shadow_offset);
-            }
+            ext_two = runs_inside(back, KIND == FF_MAT_DIELECTRIC, side);
             w.c_nee[s] = f4(o.c_nee);
             w.c_spec[s] = f4(o.c_spec);
             w.c_diff[s] = f4(o.c_diff);
@@ -479,7 +491,7 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
                 const int rch = KIND != FF_MAT_DIFFUSE && w.grad_rough ? rough_channel(mm, w.adj_rough) : -1;
                 if (rch >= 0 && mat.roughness > 0.01f) {
                     flags |= V_ROUGH | (rch == 1 ? V_ROUGH_Y : 0u);
-                    const RoughTerms rt = rough_terms(o, n, wo, wi, mat.roughness);
+                    const RoughTerms rt = rough_terms(o, n, wo, wi, mat.roughness, KIND == FF_MAT_DIELECTRIC);
                     w.v_nee[s] = f4(rt.nee);
                     w.v_spec[s] = f4(rt.spec);
                     w.v_dext[s] = f4(rt.dext);
@@ -496,7 +508,7 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
         }
         const uint32_t qe = warp_append(&w.ctr[C_EXT], valid, &w.totals[0]);
         if (valid) {
-            w.ext_rays[qe] = make_ray(o.ext_o, o.ext_d, __int_as_float(0x7f800000));
+            w.ext_rays[qe] = make_ext_ray(o.ext_o, o.ext_d, ext_two);
             w.ext_tag[qe] = s;
         }
         const uint32_t q0 = warp_append(&w.ctr[C_SH], o.ray_nee, &w.totals[1]);
@@ -809,7 +821,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
             if (profile) {
                 // stage timing: the two traces one after the other
                 ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
-                                      ws->err, w.ext_tag, nullptr);
+                                      ws->err, w.ext_tag, nullptr, nullptr, scene->refracts);
                 mark();
                 ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
                                       ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis));
@@ -819,7 +831,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
                 FF_CUDA_CHECK(cudaEventRecord(ws->fork, stream));
                 FF_CUDA_CHECK(cudaStreamWaitEvent(ws->side, ws->fork, 0));
                 ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
-                                      ws->err, w.ext_tag, nullptr);
+                                      ws->err, w.ext_tag, nullptr, nullptr, scene->refracts);
                 ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
                                       ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis),
                                       ws->side);
@@ -1004,7 +1016,7 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
             mark();
             if (profile) {
                 ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
-                                      ws->err, w.ext_tag, nullptr);
+                                      ws->err, w.ext_tag, nullptr, nullptr, scene->refracts);
                 mark();
                 ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
                                       ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis));
@@ -1013,7 +1025,7 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
                 FF_CUDA_CHECK(cudaEventRecord(ws->fork, stream));
                 FF_CUDA_CHECK(cudaStreamWaitEvent(ws->side, ws->fork, 0));
                 ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
-                                      ws->err, w.ext_tag, nullptr);
+                                      ws->err, w.ext_tag, nullptr, nullptr, scene->refracts);
                 ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
                                       ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis),
                                       ws->side);

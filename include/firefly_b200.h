@@ -223,6 +223,13 @@ typedef struct ff_hit {
 
 #define FF_TRACE_CLOSEST 0u   /* intersect(), dTriangle.cu:140-213 */
 #define FF_TRACE_ANY     2u   /* intersect_shadows(), dTriangle.cu:215-259 */
+/* Closest hits that also take back faces (no counterpart in the reference,
+ * which culls them, dTriangle.cu:5,41): a back face passes the mirror image
+ * of the culling test (determinant <= -1e-6, the same FP32 edge tests and FP64
+ * epilogue on the negated determinant and numerators) and is reported as
+ * prim = -2 - index; front faces give exactly the culling test's answers.
+ * The path tracer traces rays inside refracting objects this way. */
+#define FF_TRACE_TWO_SIDED 4u
 /* Location of rays/hits: FF_MEM_DEVICE (bit 0) or host. */
 
 /* Replaces wf_extend / wf_shadow (kernel.cu:488-543): trace n rays against
@@ -247,9 +254,12 @@ FF_API ff_status ff_trace(ff_context* ctx, const ff_scene* scene, const ff_ray* 
  * FF_ERR_INVALID_ARG.  Its scratch is one fixed array of about 3 MiB in the
  * library's device image, held by every GPU that loads the library until the
  * process exits.  The first call on a device looks up that array's device
- * address; make that first call before any stream capture.  All calls on a
- * device share the array: calls whose GPU work overlaps race and must be
- * serialised by the caller. */
+ * address and keeps it for the life of the process; make that first call
+ * before any stream capture.  cudaDeviceReset invalidates that address
+ * together with every context and scene of this library on the device, so
+ * this entry point must not be called on a device after a reset.  All calls
+ * on a device share the array: calls whose GPU work overlaps race and must
+ * be serialised by the caller. */
 #define FF_NOALLOC_MAX_RAYS 65536u
 FF_API ff_status ff_trace_host_noalloc(ff_context* ctx, const ff_scene* scene, const ff_ray* rays,
                                        uint64_t n, ff_hit* hits, uint32_t flags);
@@ -284,7 +294,7 @@ FF_API ff_status ff_film_tonemap(ff_film* film, float exposure, uint8_t* rgba8, 
 #define FF_LIGHT_ALL (-2)      /* ff_render_settings.light: uniform light selection per vertex */
 #define FF_RENDER_PROFILE 1u  /* ff_render_settings.flags: time every stage with CUDA events */
 
-#define FF_MODE_PARITY    0u  /* reproduce the reference's behaviours, see DESIGN */
+#define FF_MODE_PARITY    0u  /* reproduce the reference's behaviours (RR, MIS gating, offsets, env pdf) */
 #define FF_MODE_CORRECTED 1u  /* unbiased RR, offset extension rays, fixed MIS gating */
 
 typedef struct ff_render_settings {
@@ -469,6 +479,27 @@ FF_API ff_status ff_cache_write_params(ff_cache* cache, const float* mlp, const 
  * optimiser steps of train_batch records) after the frame's queries. */
 FF_API ff_status ff_render_cached(ff_context* ctx, ff_scene* scene, ff_cache* cache,
                                   const ff_render_settings* settings, ff_film* film, ff_render_stats* stats);
+
+/* ------------------------------------------------------------------------
+ * Test hooks (no counterpart in the reference, whose checkCudaErrors exits
+ * the process, CudaHelpers.cpp:3-11): they drive the error paths that
+ * replace exit(99) without faulting or hanging a GPU.
+ * ------------------------------------------------------------------------ */
+#define FF_DEBUG_WAIT_DEFAULT 0xffffffffu
+
+/* Device allocations this library made since it was loaded (total) and the
+ * ones it still holds (live), over all contexts.  Either pointer may be NULL. */
+FF_API ff_status ff_debug_alloc_stats(uint64_t* total, int64_t* live);
+/* From now on the next n device allocations of this library succeed and
+ * every later one fails with FF_ERR_OOM, without calling cudaMalloc; n < 0
+ * turns the refusal off.  Process-wide. */
+FF_API ff_status ff_debug_fail_alloc_after(int64_t n);
+/* Bound of the radiance cache's tensor-core waits, in polls of the
+ * mbarrier (0: every wait gives up at once; FF_DEBUG_WAIT_DEFAULT: the
+ * built-in bound).  A wait that gives up makes the call return
+ * FF_ERR_TIMEOUT; the kernel first waits, with the built-in bound, for the
+ * tensor-core work it issued, then frees its tensor memory. */
+FF_API ff_status ff_debug_cache_wait_limit(ff_cache* cache, uint32_t polls);
 
 #ifdef __cplusplus
 }

@@ -28,6 +28,11 @@ extern "C" {
  * front-face hit and writes t, u, v; leaves them untouched on early exits. */
 int ffo_intersect_cull(const float* v0, const float* v1, const float* v2,
                        const float* o, const float* d, float* t, float* u, float* v);
+/* Two-sided closest-hit test (no reference counterpart): a front face is
+ * ffo_intersect_cull; a back face passes the mirror image of it (negated
+ * determinant and numerators) and sets *back. */
+int ffo_intersect_two_sided(const float* v0, const float* v1, const float* v2,
+                            const float* o, const float* d, float* t, float* u, float* v, int* back);
 /* dTriangle::shadow_hit (dTriangle.cu:110-138): two-sided, u/v in double. */
 int ffo_shadow_hit(const float* v0, const float* v1, const float* v2,
                    const float* o, const float* d, float* t);
@@ -38,6 +43,19 @@ int ffo_shadow_hit(const float* v0, const float* v1, const float* v2,
  * query.  Work is split over nthreads POSIX threads. */
 void ffo_trace_brute(const float* tris, int64_t n_tris, const float* rays, int64_t n,
                      void* hits, int any, int nthreads);
+/* The same with two_sided != 0 for two-sided closest hits (prim = -2 - id on
+ * a back face). */
+void ffo_trace_brute2(const float* tris, int64_t n_tris, const float* rays, int64_t n,
+                      void* hits, int any, int two_sided, int nthreads);
+
+/* The same queries over a CPU hierarchy (ffo_bvh.c), for large ray sets and
+ * meshes: identical closest-hit answers (t, u, v, prim); any-hit reports
+ * some occluder (prim >= 0) or -1, as ff_trace does. */
+typedef struct ffo_bvh ffo_bvh;
+ffo_bvh* ffo_bvh_build(const float* tris, int64_t n_tris);   /* keeps a pointer to tris */
+void ffo_bvh_free(ffo_bvh* b);
+void ffo_bvh_trace(const ffo_bvh* b, const float* rays, int64_t n, void* hits, int any, int two_sided,
+                   int nthreads);
 
 /* ---- sampler (dRandom.cu:10-27) ---- */
 uint32_t ffo_wang_hash(uint32_t s);
@@ -54,12 +72,14 @@ typedef struct {
     float fresnel[3];
     float roughness;
     float metallic;
-    int32_t kind;          /* 0 mix (wf_mat_mix), 1 diffuse (wf_mat_diffuse), 2 conductor (wf_mat_cook) */
+    int32_t kind;          /* 0 mix (wf_mat_mix), 1 diffuse (wf_mat_diffuse), 2 conductor (wf_mat_cook),
+                              3 rough dielectric, 4 diffuse under a GGX coat (no reference counterparts) */
     int32_t base_color_tex;  /* -1 = none */
     int32_t roughness_tex;   /* -1 = none */
     int32_t metallic_tex;    /* -1 = none */
     int32_t metallic_roughness_tex; /* -1 = none (glTF packing: roughness y, metallic z) */
     int32_t normal_tex;      /* -1 = none (tangent space) */
+    float ior;               /* kinds 3 (dielectric) and 4 (coat); <= 0 means 1.5 */
 } ffo_material;
 
 typedef struct {

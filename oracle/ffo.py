@@ -39,6 +39,24 @@ def load() -> C.CDLL:
         lib.ffo_shadow_hit.argtypes = [P] * 6
         lib.ffo_trace_brute.restype = None
         lib.ffo_trace_brute.argtypes = [P, C.c_int64, P, C.c_int64, P, C.c_int, C.c_int]
+        lib.ffo_trace_brute2.restype = None
+        lib.ffo_trace_brute2.argtypes = [P, C.c_int64, P, C.c_int64, P, C.c_int, C.c_int, C.c_int]
+        lib.ffo_bvh_build.restype = P
+        lib.ffo_bvh_build.argtypes = [P, C.c_int64]
+        lib.ffo_bvh_free.restype = None
+        lib.ffo_bvh_free.argtypes = [P]
+        lib.ffo_bvh_trace.restype = None
+        lib.ffo_bvh_trace.argtypes = [P, P, C.c_int64, P, C.c_int, C.c_int, C.c_int]
+        lib.ffo_intersect_two_sided.restype = C.c_int
+        lib.ffo_intersect_two_sided.argtypes = [P] * 9
+        lib.ffo_probe_dielectric.restype = None
+        lib.ffo_probe_dielectric.argtypes = [P, C.c_int, P, P, P, P]
+        lib.ffo_probe_dielectric_sample.restype = C.c_int
+        lib.ffo_probe_dielectric_sample.argtypes = [P, C.c_int, P, P, C.c_float, C.c_float, C.c_float, P]
+        lib.ffo_probe_fresnel_dielectric.restype = C.c_float
+        lib.ffo_probe_fresnel_dielectric.argtypes = [C.c_float, C.c_float]
+        lib.ffo_probe_coat.restype = None
+        lib.ffo_probe_coat.argtypes = [P, P, P, P, P]
         lib.ffo_wang_hash.restype = C.c_uint32
         lib.ffo_wang_hash.argtypes = [C.c_uint32]
         lib.ffo_rand.restype = C.c_float
@@ -56,15 +74,94 @@ def _p(a: np.ndarray):
 HIT_DTYPE = np.dtype([("t", np.float32), ("u", np.float32), ("v", np.float32), ("prim", np.int32)])
 
 
-def trace_brute(tris: np.ndarray, rays: np.ndarray, any_hit: bool = False, threads: int | None = None) -> np.ndarray:
-    """Brute-force reference query over a triangle soup (T x 9) for rays (n x 8)."""
+def trace_brute(tris: np.ndarray, rays: np.ndarray, any_hit: bool = False, threads: int | None = None,
+                two_sided: bool = False) -> np.ndarray:
+    """Brute-force reference query over a triangle soup (T x 9) for rays (n x 8).
+    two_sided: closest hits that also take back faces (prim = -2 - id there)."""
     lib = load()
     tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
     rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
     out = np.empty(rays.shape[0], HIT_DTYPE)
-    lib.ffo_trace_brute(_p(tris), tris.shape[0], _p(rays), rays.shape[0], _p(out), int(any_hit),
-                        threads or os.cpu_count() or 1)
+    lib.ffo_trace_brute2(_p(tris), tris.shape[0], _p(rays), rays.shape[0], _p(out), int(any_hit), int(two_sided),
+                         threads or os.cpu_count() or 1)
     return out
+
+
+class BVH:
+    """The oracle's ray queries over a CPU hierarchy (ffo_bvh.c): the same
+    closest hits as trace_brute (ties to the lowest index), for ray sets and
+    meshes too large for brute force.  Any-hit reports some occluder."""
+
+    def __init__(self, tris: np.ndarray):
+        self._tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+        self._h = load().ffo_bvh_build(_p(self._tris), self._tris.shape[0])
+        if not self._h:
+            raise MemoryError("ffo_bvh_build failed")
+
+    def trace(self, rays: np.ndarray, any_hit: bool = False, two_sided: bool = False,
+              threads: int | None = None) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        out = np.empty(rays.shape[0], HIT_DTYPE)
+        load().ffo_bvh_trace(self._h, _p(rays), rays.shape[0], _p(out), int(any_hit), int(two_sided),
+                             threads or os.cpu_count() or 1)
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().ffo_bvh_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def intersect_two_sided(v0, v1, v2, o, d):
+    lib = load()
+    arrs = [np.ascontiguousarray(x, np.float32) for x in (v0, v1, v2, o, d)]
+    t, u, v, back = C.c_float(0), C.c_float(0), C.c_float(0), C.c_int(0)
+    ok = lib.ffo_intersect_two_sided(*[_p(a) for a in arrs], C.byref(t), C.byref(u), C.byref(v), C.byref(back))
+    return ok, t.value, u.value, v.value, back.value
+
+
+def _mat5(tint, roughness, ior):
+    return np.array([tint[0], tint[1], tint[2], roughness, ior], np.float32)
+
+
+def dielectric_eval(tint, roughness, ior, back, n, wo, wi):
+    """The restated rough dielectric: (f rgb, pdf) of wi given wo."""
+    lib = load()
+    out = np.zeros(4, np.float32)
+    m = _mat5(tint, roughness, ior)
+    arrs = [np.ascontiguousarray(x, np.float32) for x in (n, wo, wi)]
+    lib.ffo_probe_dielectric(_p(m), int(back), *[_p(a) for a in arrs], _p(out))
+    return out[:3].copy(), float(out[3])
+
+
+def dielectric_sample(tint, roughness, ior, back, n, wo, e0, e1, e2):
+    """The restated sampling step: (ok, wi)."""
+    lib = load()
+    out = np.zeros(3, np.float32)
+    m = _mat5(tint, roughness, ior)
+    nn, ww = np.ascontiguousarray(n, np.float32), np.ascontiguousarray(wo, np.float32)
+    ok = lib.ffo_probe_dielectric_sample(_p(m), int(back), _p(nn), _p(ww), e0, e1, e2, _p(out))
+    return bool(ok), out
+
+
+def fresnel_dielectric(c, n):
+    return float(load().ffo_probe_fresnel_dielectric(c, n))
+
+
+def coat_eval(albedo, roughness, ior, n, wi, wo):
+    """The restated coat: (f rgb, pdf of the 50/50 continuation) of wi given wo."""
+    lib = load()
+    out = np.zeros(4, np.float32)
+    m = _mat5(albedo, roughness, ior)
+    arrs = [np.ascontiguousarray(x, np.float32) for x in (n, wi, wo)]
+    lib.ffo_probe_coat(_p(m), *[_p(a) for a in arrs], _p(out))
+    return out[:3].copy(), float(out[3])
 
 
 def intersect_cull(v0, v1, v2, o, d):
@@ -88,7 +185,7 @@ class ffo_material(C.Structure):
     _fields_ = [("base_color", C.c_float * 3), ("fresnel", C.c_float * 3), ("roughness", C.c_float),
                 ("metallic", C.c_float), ("kind", C.c_int32), ("base_color_tex", C.c_int32),
                 ("roughness_tex", C.c_int32), ("metallic_tex", C.c_int32), ("metallic_roughness_tex", C.c_int32),
-                ("normal_tex", C.c_int32)]
+                ("normal_tex", C.c_int32), ("ior", C.c_float)]
 
 
 class ffo_texture(C.Structure):
@@ -140,6 +237,7 @@ def render(scene, width, height, spp, max_depth=3, rr_depth=3, seed=0, mode=0, l
         mats[i].base_color_tex, mats[i].roughness_tex = m.base_color_tex, m.roughness_tex
         mats[i].metallic_tex, mats[i].metallic_roughness_tex = m.metallic_tex, m.metallic_roughness_tex
         mats[i].normal_tex = m.normal_tex
+        mats[i].ior = m.ior
     texs = [np.ascontiguousarray(t, np.float32) for t in getattr(scene, "textures", [])]
     tdesc = (ffo_texture * max(1, len(texs)))()
     for i, t in enumerate(texs):
@@ -192,6 +290,8 @@ def render(scene, width, height, spp, max_depth=3, rr_depth=3, seed=0, mode=0, l
     out = np.zeros((height, width, 3), np.float64)
     stats = np.zeros(2, np.uint64)
     rc = lib.ffo_render(C.byref(d), out.ctypes.data, stats.ctypes.data)
+    if rc == 2:
+        raise ValueError("oracle render: a material kind the oracle does not restate")
     if rc != 0:
         raise ValueError("oracle render: invalid light selection")
     return out, (int(stats[0]), int(stats[1]))

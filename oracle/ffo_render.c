@@ -139,7 +139,7 @@ static double geo_atten(v3 wi, v3 wo, v3 n, float r)
 }
 static double power_heuristic(double f, double g) { return (f * f) / (f * f + g * g); }
 /* a material resolved at a hit point (get_albedo / get_roughness, dMaterial.cu:10-43) */
-typedef struct { v3 albedo; v3 fresnel; float roughness, metallic; int kind; } surf_t;
+typedef struct { v3 albedo; v3 fresnel; float roughness, metallic, ior; int kind; } surf_t;
 static v3 f0_of(const surf_t* m, v3 a) { return lerp3(m->fresnel, a, m->metallic); }
 static v3 diff_f(const surf_t* mat, v3 wi, v3 wo)
 {
@@ -409,7 +409,9 @@ static int light_vis_ray(const light_ctx* lc, v3 o, v3 d, uint32_t key, uint32_t
 }
 
 /* ------------------------------------------------------------- tracing */
-static int closest(const ffo_render_desc* d, v3 o, v3 dir, float* t_out, float* u_out, float* v_out)
+/* Closest hit over all triangles, ties to the lowest index.  two_sided: a
+ * ray inside an object also takes back faces, returned as -2 - index. */
+static int closest(const ffo_render_desc* d, v3 o, v3 dir, int two_sided, float* t_out, float* u_out, float* v_out)
 {
     float best = K_HUGE, bu = 0, bv = 0;
     int prim = -1;
@@ -417,8 +419,11 @@ static int closest(const ffo_render_desc* d, v3 o, v3 dir, float* t_out, float* 
     for (int i = 0; i < d->num_tris; ++i) {
         const float* tri = d->tris + 9 * (size_t)i;
         float t, u, v;
-        if (ffo_intersect_cull(tri, tri + 3, tri + 6, oo, dd, &t, &u, &v) && !(t < 0) && t < best) {
-            best = t; bu = u; bv = v; prim = i;
+        int back = 0;
+        int ok = two_sided ? ffo_intersect_two_sided(tri, tri + 3, tri + 6, oo, dd, &t, &u, &v, &back)
+                           : ffo_intersect_cull(tri, tri + 3, tri + 6, oo, dd, &t, &u, &v);
+        if (ok && !(t < 0) && t < best) {
+            best = t; bu = u; bv = v; prim = back ? -2 - i : i;
         }
     }
     *t_out = best; *u_out = bu; *v_out = bv;
@@ -546,6 +551,234 @@ static void shade_conductor(const light_ctx* lc, int corrected, const surf_t* ma
     o->ext_cos = hmax(0.f, dot(n, dir));
 }
 
+/* ---------------------------------------------------------- dielectric
+ * Rough dielectric interface (no reference counterpart; the reference's
+ * refract(), dMaterial.cu:97-113, is never called), restated from Walter,
+ * Marschner, Li and Torrance 2007, "Microfacet models for refraction through
+ * rough surfaces", as the product computes it (shade_dielectric,
+ * firefly_b200/csrc/ff_paths.cuh), operation for operation in FP32:
+ *   D GGX (their eq. 33), alpha = max(r^2, 1e-4); G = G1(wo) G1(wi), Smith
+ *   for GGX (eq. 34); F exact unpolarised Fresnel (eq. 22);
+ *   f_r = F D G / (4 |n.wi| |n.wo|) (eq. 20);
+ *   f_t = (1 - F) D G |wi.h| |wo.h| eta_o^2 / (|n.wi| |n.wo| (eta_o wo.h + eta_t wi.h)^2) * tint (eq. 21,
+ *         radiance scaling folded in);
+ *   sampling: m from D(m)|m.n| (eqs. 35-36), reflect with probability F,
+ *   else refract (section 5.3); pdf = D(h) |h.n| |dh/dwi| x the branch's
+ *   probability (eqs. 14, 17). */
+typedef struct { float alpha, eta_o, eta_t; v3 tint; } diel_t;
+
+static diel_t diel_of(const surf_t* m, int back)
+{
+    float ior = m->ior > 0.f ? m->ior : 1.5f;
+    diel_t d;
+    d.alpha = hmax(m->roughness * m->roughness, 1e-4f);
+    d.eta_o = back ? ior : 1.f;
+    d.eta_t = back ? 1.f : ior;
+    d.tint = m->albedo;
+    return d;
+}
+static float ggx_d(float alpha, float c)
+{
+    if (!(c > 0.f)) return 0.f;
+    float a2 = alpha * alpha;
+    float c2 = c * c;
+    float k = c2 * (a2 - 1.f) + 1.f;
+    return a2 / ((PI_F * k) * k);
+}
+static float tan2_of(float c)
+{
+    float c2 = c * c;
+    return hmax(0.f, 1.f - c2) / c2;
+}
+static float smith_g1(float alpha, float vn, float vh)
+{
+    if (!(vh * vn > 0.f)) return 0.f;
+    return 2.f / (1.f + sqrtf(1.f + (alpha * alpha) * tan2_of(vn)));
+}
+static float fresnel_dielectric(float c, float n)
+{
+    float g2 = n * n - 1.f + c * c;
+    if (g2 < 0.f) return 1.f;
+    float g = sqrtf(g2);
+    float a = (g - c) / (g + c);
+    float b = (c * (g + c) - 1.f) / (c * (g - c) + 1.f);
+    return (0.5f * (a * a)) * (1.f + b * b);
+}
+static int diel_half(const diel_t* d, v3 n, v3 wo, v3 wi, int* refl, v3* h)
+{
+    float cos_o = dot(n, wo), cos_i = dot(n, wi);
+    if (!(cos_o > 0.f) || cos_i == 0.f) return 0;
+    *refl = cos_i > 0.f;
+    v3 hh = *refl ? add(wo, wi) : add(muls(wo, d->eta_o), muls(wi, d->eta_t));
+    float l2 = dot(hh, hh);
+    if (!(l2 > 0.f)) return 0;
+    hh = normalize(hh);
+    if (dot(hh, n) < 0.f) hh = neg(hh);
+    *h = hh;
+    float woh = dot(wo, hh), wih = dot(wi, hh);
+    if (!(woh > 0.f)) return 0;
+    return *refl ? wih > 0.f : wih < 0.f;
+}
+static void diel_eval(const diel_t* d, v3 n, v3 wo, v3 wi, v3* f, float* pdf)
+{
+    *f = V(0, 0, 0);
+    *pdf = 0.f;
+    int refl;
+    v3 h;
+    if (!diel_half(d, n, wo, wi, &refl, &h)) return;
+    float cos_o = dot(n, wo), cos_i = fabsf(dot(n, wi));
+    float ch = dot(n, h), woh = dot(wo, h), wih = dot(wi, h);
+    float D = ggx_d(d->alpha, ch);
+    float G = smith_g1(d->alpha, cos_o, woh) * smith_g1(d->alpha, dot(n, wi), wih);
+    float F = fresnel_dielectric(woh, d->eta_t / d->eta_o);
+    if (refl) {
+        float v = ((F * D) * G) / ((4.f * cos_i) * cos_o);
+        *f = V(v, v, v);
+        *pdf = ((F * D) * ch) / (4.f * woh);
+    } else {
+        float den = d->eta_o * woh + d->eta_t * wih;
+        float den2 = den * den;
+        float v = (((((1.f - F) * D) * G) * (-wih)) * woh * (d->eta_o * d->eta_o)) / ((cos_i * cos_o) * den2);
+        *f = muls(d->tint, v);
+        *pdf = ((((1.f - F) * D) * ch) * (d->eta_t * d->eta_t) * (-wih)) / den2;
+    }
+}
+static v3 ggx_sample_normal(v3 n, float alpha, float e0, float e1)
+{
+    float t2 = (alpha * alpha) * (e0 / (1.f - e0));
+    float ct = 1.f / sqrtf(1.f + t2);
+    float st = sqrtf(t2) * ct;
+    float phi = TWO_PI_F * e1;
+    v3 T, B;
+    frame(n, &T, &B);
+    return normalize(add(add(muls(T, st * cosf(phi)), muls(B, st * sinf(phi))), muls(n, ct)));
+}
+static int diel_sample(const diel_t* d, v3 n, v3 wo, float e0, float e1, float e2, v3* wi)
+{
+    v3 m = ggx_sample_normal(n, d->alpha, e0, e1);
+    float woh = dot(wo, m);
+    if (!(woh > 0.f)) return 0;
+    float F = fresnel_dielectric(woh, d->eta_t / d->eta_o);
+    int refl = e2 < F;
+    v3 w;
+    if (refl) {
+        w = sub(muls(m, 2.f * woh), wo);
+    } else {
+        float eta = d->eta_o / d->eta_t;
+        float k = 1.f - (eta * eta) * (1.f - woh * woh);
+        w = sub(muls(m, eta * woh - sqrtf(hmax(k, 0.f))), muls(wo, eta));
+    }
+    w = normalize(w);
+    /* a reflection below / refraction above the macro surface has no
+     * density under its branch (diel_eval classifies by side): dropped */
+    float c = dot(n, w);
+    if (refl ? !(c > 0.f) : !(c < 0.f)) return 0;
+    *wi = w;
+    return 1;
+}
+static float power_heuristic_f(float f, float g)
+{
+    float f2 = f * f;
+    return f2 / (f2 + g * g);
+}
+static void shade_dielectric(const light_ctx* lc, const surf_t* mat, v3 pos, v3 n, v3 wo, v3 wi, uint32_t key,
+                             uint32_t L, int back, shade_t* o)
+{
+    const diel_t d = diel_of(mat, back);
+    o->has_spec = o->has_diff = 0;
+    o->c_nee = o->c_spec = o->c_diff = V(0, 0, 0);
+    {
+        v3 f;
+        float bpdf;
+        diel_eval(&d, n, wo, wi, &f, &bpdf);
+        float lp = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+        if (!iszero(f) && lp > 0.f) {
+            float w = lc->is_dir ? 1.f : power_heuristic_f(lp, bpdf);
+            o->c_nee = divs(mul(muls(f, fabsf(dot(n, wi)) * w), light_L(lc, wi)), lp);
+        }
+    }
+    v3 dir = n, f = V(0, 0, 0);
+    float pdf = 0.f;
+    if (diel_sample(&d, n, wo, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1), R(key, L, DIM_EXTRA), &dir))
+        diel_eval(&d, n, wo, dir, &f, &pdf);
+    else
+        dir = n;
+    float c = fabsf(dot(n, dir));
+    if (pdf > 0.f && !iszero(f)) {
+        ray_t vr;
+        if (!lc->is_dir && light_vis_ray(lc, add(pos, muls(dir, 0.001f)), dir, key, L, DIM_SPEC_VIS, &vr)) {
+            v3 Li = light_L(lc, dir);
+            if (!iszero(Li)) {
+                float w = power_heuristic_f(pdf, light_pdf(lc, pos, dir, key, L, DIM_SPEC_PDF));
+                o->c_spec = divs(mul(muls(f, c * w), Li), pdf);
+                o->has_spec = 1;
+                o->r_spec = vr;
+            }
+        }
+    }
+    o->ext_d = dir;
+    o->ext_f = f;
+    o->ext_pdf = pdf;
+    o->ext_cos = c;
+}
+
+/* ----------------------------------------------------------------- coat
+ * Diffuse base under a GGX clear coat (no reference counterpart), as the
+ * product computes it (shade_coat, firefly_b200/csrc/ff_paths.cuh): the coat
+ * is the reference's spec_f (dMaterial.cu:266-288) with f0 = ((ior - 1) /
+ * (ior + 1))^2, white albedo and no metal; the base is albedo (1 - F) / pi
+ * with Schlick's F at the half vector; light-sampled NEE without MIS; the
+ * continuation picks the coat's GGX sample (spec_sample) or a cosine-weighted
+ * direction (concentric disk lifted to the hemisphere) with probability 1/2
+ * each, pdf the 50/50 mixture. */
+static v3 coat_spec_f(const surf_t* mat, v3 n, v3 wi, v3 wo, float r0)
+{
+    surf_t c = *mat;
+    c.fresnel = V(r0, r0, r0);
+    c.albedo = V(1.f, 1.f, 1.f);
+    c.metallic = 0.f;
+    return spec_f(&c, n, wi, wo);
+}
+static v3 coat_f(const surf_t* mat, v3 n, v3 wi, v3 wo, float r0)
+{
+    v3 spec = coat_spec_f(mat, n, wi, wo, r0);
+    v3 h = normalize(add(wo, wi));
+    float x = 1.f - hmax(0.f, dot(h, wi));
+    float F = r0 + (1.f - r0) * x * x * x * x * x;
+    return add(spec, muls(mat->albedo, (1.f - F) * INV_PI_F));
+}
+static void shade_coat(const light_ctx* lc, const surf_t* mat, v3 pos, v3 n, v3 wo, v3 wi, uint32_t key,
+                       uint32_t L, shade_t* o)
+{
+    float eta = mat->ior > 0.f ? mat->ior : 1.5f;
+    float r0 = ((eta - 1.f) / (eta + 1.f)) * ((eta - 1.f) / (eta + 1.f));
+    o->has_spec = o->has_diff = 0;
+    o->c_nee = V(0, 0, 0);
+    float nd = dot(n, wi);
+    float lp = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+    if (nd > 0.f && lp > 0.f) {
+        v3 sc = divs(smul(nd, light_L(lc, wi)), lp);
+        o->c_nee = mul(coat_f(mat, n, wi, wo, r0), sc);
+    }
+    float r = mat->roughness;
+    v3 dir;
+    if (R(key, L, DIM_LOBE) < 0.5f) {
+        dir = spec_sample(n, wo, r, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1));
+    } else {
+        v2 u = {R(key, L, DIM_DIFF), R(key, L, DIM_DIFF + 1)};
+        v2 dsk = concentric_disk(u);
+        float z = sqrtf(hmax(0.f, 1.f - dsk.x * dsk.x - dsk.y * dsk.y));
+        v3 T, B;
+        frame(n, &T, &B);
+        dir = normalize(add(add(muls(T, dsk.x), muls(B, dsk.y)), muls(n, z)));
+    }
+    float c = hmax(0.f, dot(n, dir));
+    o->ext_d = dir;
+    o->ext_f = coat_f(mat, n, dir, wo, r0);
+    o->ext_pdf = 0.5f * spec_get_pdf(n, dir, wo, r) + 0.5f * c * INV_PI_F;
+    o->ext_cos = c;
+}
+
 /* gen_ray (dCamera.cu:10-36); NDC in double because of the 0.5 double literal */
 static void camera_ray(const ffo_render_desc* d, int px, int py, v2 jit, v2 lens, v3* o, v3* dir)
 {
@@ -658,13 +891,16 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int 
     shade_t sh;
     memset(&sh, 0, sizeof(sh));
     int vis_nee = 0, vis_spec = 0, vis_diff = 0;
+    int inside = 0;   /* the ray runs inside an object: two-sided closest hit */
     out[0] = out[1] = out[2] = 0.0;
     for (;;) {
         float t, u, v;
-        int prim = closest(d, o, dir, &t, &u, &v);
+        int hit = closest(d, o, dir, inside, &t, &u, &v);
         (*n_ext)++;
         L += 1;
-        int found = prim >= 0;
+        int found = hit != -1;
+        int back = hit < -1;   /* a back face: the vertex is shaded from the inside */
+        int prim = back ? -2 - hit : hit;
         int terminate = (L > (uint32_t)d->max_depth) || !found;
         if (!found && L == 1) {
             v3 c = mul(beta, env_L(d, dir));
@@ -729,10 +965,11 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int 
         sf.fresnel = ld3(mm->fresnel);
         sf.roughness = mm->roughness;
         sf.metallic = mm->metallic;
+        sf.ior = mm->ior;
         sf.kind = mm->kind;
         /* ng: the interpolated normal the ray offsets follow (kernel.cu:437);
          * n becomes get_normal's shading normal below */
-        const v3 ng = n;
+        v3 ng = n;
         if (d->texcoords && (mm->base_color_tex >= 0 || mm->roughness_tex >= 0 || mm->metallic_tex >= 0 ||
                              mm->metallic_roughness_tex >= 0 || mm->normal_tex >= 0)) {
             /* texcoord = u * uv1 + v * uv2 + (1 - u - v) * uv0 (dTriangle.cu:97) */
@@ -751,23 +988,34 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int 
                 n = normal_from_map(T, B, ng, tex_bilinear(tx->rgb, tx->width, tx->height, tu, tv));
             }
         }
+        if (back) {   /* both normals face the ray */
+            ng = neg(ng);
+            n = neg(n);
+        }
         const surf_t* mat = &sf;
         v3 wo = neg(dir);
         memset(&sh, 0, sizeof(sh));
+        const int diel = mat->kind == 3;
         if (mat->kind == 0) shade_mix(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
         else if (mat->kind == 1) shade_diffuse(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
-        else shade_conductor(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
-        v3 lo = add(pos, muls(ng, d->shadow_offset));
+        else if (mat->kind == 2) shade_conductor(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
+        else if (diel) shade_dielectric(lc, mat, pos, n, wo, wi, key, L, back, &sh);
+        else shade_coat(lc, mat, pos, n, wo, wi, key, L, &sh);   /* kind 4; ffo_render rejects others */
+        /* a dielectric's light may lie on the far side */
+        float nee_side = (diel && dot(wi, ng) < 0.f) ? -1.f : 1.f;
+        v3 lo = add(pos, muls(ng, nee_side * d->shadow_offset));
         sh.has_nee = light_vis_ray(lc, lo, wi, key, L, DIM_NEE_VIS, &sh.r_nee);
         vis_nee = sh.has_nee && !occluded(d, &sh.r_nee);
         vis_spec = sh.has_spec && !occluded(d, &sh.r_spec);
         vis_diff = sh.has_diff && !occluded(d, &sh.r_diff);
         *n_sh += (uint64_t)(sh.has_nee + sh.has_spec + sh.has_diff);
+        /* the reference starts the continuation at the hit point (kernel.cu:643);
+         * corrected mode, and every ray leaving a dielectric or an inside
+         * vertex, starts off the surface on the side it leaves */
+        float side = dot(sh.ext_d, ng) >= 0.f ? 1.f : -1.f;
         o = pos;
-        if (corrected) {
-            float side = dot(sh.ext_d, ng) >= 0.f ? 1.f : -1.f;
-            o = add(pos, muls(ng, side * d->shadow_offset));
-        }
+        if (corrected || diel || back) o = add(pos, muls(ng, side * d->shadow_offset));
+        inside = back != (diel && side < 0.f);
         dir = sh.ext_d;
     }
 }
@@ -810,6 +1058,8 @@ int ffo_render(const ffo_render_desc* d, double* out_rgb, uint64_t* stats)
     if (d->light == -2 && (!lc.corrected || n_lights == 0)) return 1;
     if (d->light < -2 || (d->light == -1 && !d->env_rgb)) return 1;
     if (d->light >= d->num_area_lights + d->num_dir_lights) return 1;
+    for (int m = 0; m < d->num_materials; ++m)
+        if (d->materials[m].kind < 0 || d->materials[m].kind > 4) return 2;   /* a kind this oracle does not restate */
     if (d->env_rgb && (lc.is_env || d->light == -2)) {
         marginal = (double*)malloc(sizeof(double) * d->env_h);
         cond = (double*)malloc(sizeof(double) * (size_t)d->env_w * d->env_h);
@@ -975,4 +1225,49 @@ void ffo_probe_surface(const ffo_material* mm, const ffo_texture* textures, cons
     out8[3] = sf.roughness;
     out8[4] = sf.metallic;
     st3(out8 + 5, N);
+}
+
+/* Dielectric and coat probes (the restated lobes one call at a time, for
+ * the known-answer tests of tests/test_oracle_materials_cpu.py).
+ * mat5 = base colour (tint / albedo) [3], roughness, ior. */
+static surf_t mat5_of(const float* m5)
+{
+    surf_t m;
+    memset(&m, 0, sizeof(m));
+    m.albedo = ld3(m5);
+    m.fresnel = V(0.04f, 0.04f, 0.04f);
+    m.roughness = m5[3];
+    m.ior = m5[4];
+    return m;
+}
+void ffo_probe_dielectric(const float* mat5, int back, const float* n3, const float* wo3, const float* wi3, float* out4)
+{
+    surf_t m = mat5_of(mat5);
+    diel_t d = diel_of(&m, back);
+    v3 f;
+    float pdf;
+    diel_eval(&d, ld3(n3), ld3(wo3), ld3(wi3), &f, &pdf);
+    st3(out4, f);
+    out4[3] = pdf;
+}
+int ffo_probe_dielectric_sample(const float* mat5, int back, const float* n3, const float* wo3, float e0, float e1,
+                                float e2, float* wi3)
+{
+    surf_t m = mat5_of(mat5);
+    diel_t d = diel_of(&m, back);
+    v3 wi = V(0, 0, 0);
+    int ok = diel_sample(&d, ld3(n3), ld3(wo3), e0, e1, e2, &wi);
+    st3(wi3, wi);
+    return ok;
+}
+float ffo_probe_fresnel_dielectric(float c, float n) { return fresnel_dielectric(c, n); }
+void ffo_probe_coat(const float* mat5, const float* n3, const float* wi3, const float* wo3, float* out4)
+{
+    surf_t m = mat5_of(mat5);
+    float eta = m.ior > 0.f ? m.ior : 1.5f;
+    float r0 = ((eta - 1.f) / (eta + 1.f)) * ((eta - 1.f) / (eta + 1.f));
+    v3 n = ld3(n3), wi = ld3(wi3), wo = ld3(wo3);
+    st3(out4, coat_f(&m, n, wi, wo, r0));
+    float c = hmax(0.f, dot(n, wi));
+    out4[3] = 0.5f * spec_get_pdf(n, wi, wo, m.roughness) + 0.5f * c * INV_PI_F;
 }

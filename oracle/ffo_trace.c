@@ -60,6 +60,42 @@ int ffo_intersect_cull(const float* p0, const float* p1, const float* p2,
     return 1;
 }
 
+/* Two-sided closest-hit test (no reference counterpart: the reference only
+ * culls, dTriangle.cu:5,41).  A front face (det >= K_EPSILON) is exactly
+ * ffo_intersect_cull; a back face (det <= -K_EPSILON) runs the same test on
+ * the negated determinant and numerators (negation is exact), the mirror
+ * image of the culling test.  *back reports which.  The product restates it
+ * in ff_test_tri_closest<TWO> (firefly_b200/csrc/ff_trace.cuh). */
+int ffo_intersect_two_sided(const float* p0, const float* p1, const float* p2,
+                            const float* po, const float* pd, float* t, float* u, float* v, int* back)
+{
+    v3 v0 = mk(p0), v1 = mk(p1), v2 = mk(p2), o = mk(po), d = mk(pd);
+    v3 e1 = sub(v1, v0);
+    v3 e2 = sub(v2, v0);
+    v3 pvec = cross(d, e2);
+    float detf = dot(e1, pvec);
+    float sg = 1.f;
+    *back = 0;
+    if (detf < FFO_K_EPSILON) {
+        if (!(detf <= -FFO_K_EPSILON)) return 0;
+        sg = -1.f;
+        *back = 1;
+    }
+    double det = (double)(sg * detf);
+    v3 tvec = sub(o, v0);
+    float uu = sg * dot(tvec, pvec);
+    if (uu < 0.0 || uu > det) return 0;
+    v3 qvec = cross(tvec, e1);
+    float vv = sg * dot(d, qvec);
+    if (vv < 0.0 || uu + vv > det) return 0;
+    float tt = sg * dot(e2, qvec);
+    double inv_det = 1.0 / det;
+    *t = (float)(tt * inv_det);
+    *u = (float)(uu * inv_det);
+    *v = (float)(vv * inv_det);
+    return 1;
+}
+
 int ffo_shadow_hit(const float* p0, const float* p1, const float* p2,
                    const float* po, const float* pd, float* t)
 {
@@ -89,6 +125,7 @@ typedef struct {
     int64_t begin, end;
     uint32_t* hits;
     int any;
+    int two_sided;
 } job_t;
 
 static void* run_job(void* arg)
@@ -112,6 +149,17 @@ static void* run_job(void* arg)
                     best_t = t;
                     break;
                 }
+            } else if (j->two_sided) {
+                /* strict < over increasing ids: ties go to the lowest id; a
+                 * back face is reported as -2 - id */
+                int back = 0;
+                if (ffo_intersect_two_sided(tri, tri + 3, tri + 6, o, d, &t, &u, &v, &back) &&
+                    !(t < 0) && t >= tmin && t < best_t) {
+                    best = back ? -2 - (int32_t)i : (int32_t)i;
+                    best_t = t;
+                    best_u = u;
+                    best_v = v;
+                }
             } else {
                 /* strict < over increasing ids: ties go to the lowest id */
                 if (ffo_intersect_cull(tri, tri + 3, tri + 6, o, d, &t, &u, &v) &&
@@ -125,7 +173,7 @@ static void* run_job(void* arg)
         }
         uint32_t* h = j->hits + 4 * r;
         float out[3];
-        if (best < 0) {
+        if (best == -1) {
             out[0] = j->any ? tmax : (tmax < FFO_K_HUGE ? tmax : FFO_K_HUGE);
             out[1] = 0.f;
             out[2] = 0.f;
@@ -143,6 +191,12 @@ static void* run_job(void* arg)
 void ffo_trace_brute(const float* tris, int64_t n_tris, const float* rays, int64_t n,
                      void* hits, int any, int nthreads)
 {
+    ffo_trace_brute2(tris, n_tris, rays, n, hits, any, 0, nthreads);
+}
+
+void ffo_trace_brute2(const float* tris, int64_t n_tris, const float* rays, int64_t n,
+                      void* hits, int any, int two_sided, int nthreads)
+{
     if (nthreads < 1) nthreads = 1;
     if (nthreads > 256) nthreads = 256;
     pthread_t th[256];
@@ -157,6 +211,7 @@ void ffo_trace_brute(const float* tris, int64_t n_tris, const float* rays, int64
         jobs[k].end = (k + 1) * chunk < n ? (k + 1) * chunk : n;
         jobs[k].hits = (uint32_t*)hits;
         jobs[k].any = any;
+        jobs[k].two_sided = two_sided;
         if (pthread_create(&th[k], NULL, run_job, &jobs[k]) == 0) {
             started |= 0;
         } else {

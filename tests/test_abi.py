@@ -85,3 +85,14 @@ def test_struct_layouts_match_the_header(tmp_path):
             if got[(n, f)] != getattr(cls, f).offset:
                 bad.append(f"{n}.{f}: offset {got[(n, f)]} vs ctypes {getattr(cls, f).offset}")
     assert not bad, bad
+
+
+def test_debug_hooks_need_no_device(ff_lib):
+    """The allocation counters and the refusal switch work without a GPU."""
+    total, live = ctypes.c_uint64(7), ctypes.c_int64(7)
+    assert ff_lib.ff_debug_alloc_stats(ctypes.byref(total), ctypes.byref(live)) == 0
+    assert total.value >= 0
+    assert ff_lib.ff_debug_alloc_stats(None, None) == 0
+    assert ff_lib.ff_debug_fail_alloc_after(3) == 0
+    assert ff_lib.ff_debug_fail_alloc_after(-1) == 0
+    assert ff_lib.ff_debug_cache_wait_limit(None, 0) == 1

@@ -129,7 +129,11 @@ def test_env_gradient_vs_central_differences(setup):
     e = np.zeros_like(start.env_rgb)
     ds.render_adjoint(W, H, dimg, grad_env=e, texture=-1, **SET)
     flat = np.abs(e).reshape(-1)
-    picks = np.argsort(-flat)[:24]
+    # 64 random texel channels among those the paths reach (the importance
+    # tables are kept, so the image is linear in every texel)
+    cand = np.nonzero(flat > 1e-3 * flat.max())[0]
+    picks = np.random.default_rng(3).choice(cand, size=min(64, len(cand)), replace=False)
+    assert len(picks) == 64
     env = start.env_rgb.copy()
     fd = []
     for k in picks:
@@ -148,6 +152,7 @@ def test_env_gradient_vs_central_differences(setup):
     rel = np.abs(ad - fd) / np.maximum(np.abs(fd), 1e-12)
     print(f"[adjoint] env FD: median rel err {np.median(rel):.2e}, max {rel.max():.2e}, n={len(picks)}")
     assert np.median(rel) < 1e-2
+    assert np.mean(rel < 5e-2) > 0.9
     assert np.corrcoef(ad, fd)[0, 1] > 0.999
 
 
@@ -273,11 +278,12 @@ def test_roughness_gradient_nee_vs_central_differences(rough_setup, light):
     """Depth 1 (camera vertex + NEE): the light-sampled directions do not
     depend on the roughness, so common random numbers make the central
     difference of one seed's render the derivative the adjoint computes.
-    The mixed material under the environment also adds a BSDF-sampled light
-    term whose direction moves with r; under the directional light (a delta
-    light: no BSDF-sampled term) it is checked like the others."""
+    The mixed material and the dielectric under the environment also add a
+    BSDF-sampled light term whose direction moves with r (and MIS weights
+    that depend on r); under the directional light (a delta light: no
+    BSDF-sampled term, weight 1) they are checked like the others."""
     kind, ds, pt, scn = rough_setup
-    if kind == "MIX" and light == -1:
+    if kind in ("MIX", "DIELECTRIC") and light == -1:
         pytest.skip("the BSDF-sampled light term's direction moves with r (checked in expectation below)")
     st = dict(SET, max_depth=1, spp=4, light=light)
     w = _linear_weights()

@@ -10,6 +10,8 @@ import numpy as np
 
 from firefly_b200 import gltf, scenes
 
+ROOT = __import__("pathlib").Path(__file__).resolve().parent.parent
+
 
 def _tri_set(P, I):
     return sorted(tuple(np.round(P[t].ravel(), 5)) for t in I)
@@ -129,3 +131,22 @@ def test_gltf_external_png_rows_and_scaling(tmp_path):
     assert np.array_equal(tex, (img[::-1] / 255.0).astype(np.float32))
     # the flipped v of the first vertex (glTF v = 0) is 1: the top image row sits at texture row h - 1
     assert got.texcoords[0, 1] == 1.0
+
+
+def test_committed_fixture_decodes_to_known_texels():
+    """tests/golden/room_pbr.glb (made by tests/golden/make_gltf_fixture.py)
+    holds textures whose texels are integer formulas of (x, y): the import
+    must give exactly formula / 255 with the rows flipped as the reference's
+    loader flips them (stbi_set_flip_vertically_on_load, dTexture.cu:115-117),
+    the material slots of the file, and its geometry."""
+    from firefly_b200 import gltf
+    from tests.golden.make_gltf_fixture import formula_bytes
+    scn = gltf.load(ROOT / "tests" / "golden" / "room_pbr.glb", 48, 48)
+    assert len(scn.textures) == 3
+    for k in range(3):
+        want = formula_bytes(k)[::-1].astype(np.float32) / 255.0
+        assert np.array_equal(scn.textures[k], want), k
+    m0 = scn.materials[0]
+    assert (m0.base_color_tex, m0.metallic_roughness_tex, m0.normal_tex) == (0, 1, 2)
+    assert scn.num_triangles == 4116
+    assert scn.tangents is not None and np.isfinite(scn.tangents).all()

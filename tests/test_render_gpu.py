@@ -304,3 +304,77 @@ def test_render_edge_cases(ctx, oracle):
     ref, _ = oracle.render(scn, 16, 16, 3, max_depth=5, rr_depth=3, seed=4, mode=1, light=0, threads=cpu_threads())
     assert np.all(n2 == 3)
     assert _mre(got_small_pool / 3, ref / 3) <= MRE_TOL
+
+
+def tonemap_restated(rgba: np.ndarray, n: np.ndarray, exposure: float) -> np.ndarray:
+    """wf_logic's display write (CUDA-RayTracer/kernel.cu:446-454) in float32:
+    final_col = accum / (float)n, *= exposure, /= (final_col + 1), then
+    (int)255 * c per channel and alpha 255; pixels without samples stay
+    black.  The reference stores into a signed char4 (values above 127
+    wrap); the headless film saturates to 0..255 instead."""
+    f32 = np.float32
+    acc = rgba[..., :3].astype(f32)
+    nn = n.astype(f32)[..., None]
+    col = (acc / np.where(nn >= 1, nn, f32(1))).astype(f32)
+    col = (col * f32(exposure)).astype(f32)
+    col = (col / (col + f32(1))).astype(f32)
+    byte = np.clip(np.trunc((f32(255) * col).astype(f32)), 0, 255).astype(np.uint8)
+    out = np.zeros(rgba.shape[:2] + (4,), np.uint8)
+    out[..., :3] = np.where(n[..., None] >= 1, byte, 0)
+    out[..., 3] = 255
+    return out
+
+
+def test_tonemap_matches_the_reference_display_formula(ctx):
+    """ff_film_tonemap byte for byte against the restated kernel.cu:446-454,
+    on dark and bright pixels (exposure 16 pushes many channels past the 0.5
+    point of x / (1 + x), where the reference's signed char4 would wrap) and
+    on an empty film."""
+    import firefly_b200 as ff
+    w, h = 64, 48
+    scn = scenes.small_room(seed=1, width=w, height=h)
+    ds = ff.dScene(ctx, scn)
+    pt = ff.PathTracer(ctx, w, h)
+    try:
+        pt.draw(ds, spp=6, max_depth=5, seed=11, light=0)
+        for exposure in (1.0, 16.0, 0.25):
+            rgba, n = pt.read()
+            got = pt.tonemap(exposure)
+            want = tonemap_restated(rgba, n, exposure)
+            assert np.array_equal(got, want), (exposure, int((got != want).sum()))
+            if exposure > 8.0:
+                assert (got[..., :3] > 128).mean() > 0.1
+        # an empty film maps to opaque black
+        pt.clear_buffer()
+        got = pt.tonemap(1.0)
+        assert np.all(got[..., :3] == 0) and np.all(got[..., 3] == 255)
+    finally:
+        pt.close()
+        ds.close()
+
+
+def test_committed_gltf_renders_like_the_oracle(ctx, oracle):
+    """The committed .glb fixture (tests/golden/room_pbr.glb: base-colour,
+    metallic-roughness and normal textures with known texels, a tangent
+    frame) imported through firefly_b200.gltf and rendered on the GPU agrees
+    with the oracle rendering the same imported scene: MRE <= 1e-4 and the
+    same ray counts, in both modes."""
+    import firefly_b200 as ff
+    from firefly_b200 import gltf
+    from tests.conftest import ROOT
+    scn = gltf.load(ROOT / "tests" / "golden" / "room_pbr.glb", 48, 48)
+    scn.env_rgb = scenes.sky_env(64, 32, seed=2, sun_radiance=20.0, sun_diameter_deg=8.0)
+    # the camera of the scene the fixture was made from
+    scn.camera = scenes.pbr_textured_room(seed=3, width=48, height=48, tex_res=16).camera
+    for mode in (ff.FF_MODE_PARITY, ff.FF_MODE_CORRECTED):
+        got, n, stats = _gpu_render(ctx, scn, 48, 48, 4, light=-1, max_depth=4, rr_depth=3, seed=21, mode=mode)
+        ref, (re, rs) = oracle.render(scn, 48, 48, 4, max_depth=4, rr_depth=3, seed=21, mode=mode, light=-1,
+                                      threads=cpu_threads())
+        fin = np.isfinite(got) & np.isfinite(ref)
+        assert np.array_equal(np.isfinite(got), np.isfinite(ref))
+        mre = _mre(got[fin], ref[fin])
+        print(f"[gltf] fixture mode={mode}: mre={mre:.3e} ext={stats['extension_rays']}/{re} "
+              f"shadow={stats['shadow_rays']}/{rs}")
+        assert ref[fin].mean() > 0 and mre <= MRE_TOL
+        assert abs(stats["extension_rays"] - re) <= max(2, 1e-3 * re)
+        assert abs(stats["shadow_rays"] - rs) <= max(2, 1e-3 * rs)

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 def _same_closest(got, ref):
     gp, rp = got["prim"], ref["prim"]
     bad = gp != rp
-    hit = rp >= 0
+    hit = rp != -1          # two-sided traces report back faces as -2 - index
     for f in ("t", "u", "v"):
         g = got[f].view(np.uint32)
         r = ref[f].view(np.uint32)
@@ -224,3 +224,117 @@ def test_trace_count(ctx, room):
     ds0 = ff.dScene(ctx, empty)
     assert ds0.trace_count(r1[:10])["nodes"] == 0
     assert ds.trace_count(rays[:0])["rays"] == 0
+
+
+def _check_two_sided(scn, dscene, oracle, rays):
+    got = dscene.trace(rays, two_sided=True)
+    ref = oracle.trace_brute(scn.triangle_soup(), rays, two_sided=True, threads=cpu_threads())
+    bad = _same_closest(got, ref)
+    n_bad = int(bad.sum())
+    assert n_bad == 0, (f"{n_bad} of {len(rays)} two-sided hits differ; first: ray {np.argmax(bad)} "
+                        f"got {got[np.argmax(bad)]} ref {ref[np.argmax(bad)]}")
+    return got
+
+
+def test_two_sided_closest(room, oracle):
+    """FF_TRACE_TWO_SIDED (the traversal of rays inside refracting objects):
+    bit-exact against the oracle's mirrored culling test, back faces as
+    prim = -2 - index, ties to the lowest index; a front-face answer equals
+    the culling trace's answer for the same ray."""
+    scn, ds = room
+    P = np.asarray(scn.positions, np.float64)
+    sphere = P[24:]
+    c = sphere.mean(0)
+    rad = float(np.linalg.norm(sphere - c, axis=1).max())
+    rng = np.random.default_rng(41)
+    rays = scenes.incoherent_rays(scn, 150_000, seed=42)
+    # half the origins inside the sphere: their rays leave through back faces
+    k = len(rays) // 2
+    u = rng.normal(size=(k, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    rays[:k, 0:3] = (c + u * (0.95 * rad * rng.random((k, 1)) ** (1 / 3))).astype(np.float32)
+    got = _check_two_sided(scn, ds, oracle, rays)
+    back = got["prim"] < -1
+    assert back[:k].mean() > 0.9 and back[k:].mean() > 0.01
+    cull = ds.trace(rays)
+    front = got["prim"] >= 0
+    assert np.array_equal(got[front].view(np.uint32), cull[front].view(np.uint32))
+    # edge cases of the mirrored test: the coincident-triangle tie, rays along
+    # the axes from inside the sphere, and a tmin interval
+    r2 = rays[:20_000].copy()
+    axes = np.eye(3, dtype=np.float32)
+    r2[:3000, 4:7] = axes[np.arange(3000) % 3] * np.where(np.arange(3000) % 2 == 0, 1, -1)[:, None]
+    r2[3000:6000, 3] = rng.uniform(0.0, 1.0, 3000).astype(np.float32)
+    _check_two_sided(scn, ds, oracle, r2)
+
+
+def test_two_sided_ties_and_device_path(ctx, oracle):
+    import firefly_b200 as ff
+    import torch
+    # 40 coincident copies of one triangle, half of them wound the other way:
+    # every ray hits at the same t from either side; the lowest index wins
+    P = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    I = np.arange(120, dtype=np.uint32).reshape(40, 3)
+    I[1::2] = I[1::2][:, [0, 2, 1]]
+    scn = scenes.Scene(positions=np.tile(P, (40, 1)), indices=I)
+    ds = ff.dScene(ctx, scn)
+    rng = np.random.default_rng(43)
+    rays = np.zeros((8000, 8), np.float32)
+    rays[:, 0:2] = rng.uniform(-0.5, 1.5, (8000, 2))
+    rays[:, 2] = rng.choice([-1.0, 1.0], 8000)
+    rays[:, 6] = -np.sign(rays[:, 2])
+    rays[:, 7] = np.inf
+    got = _check_two_sided(scn, ds, oracle, rays)
+    hit = got["prim"] != -1
+    # index 0 faces +z: rays from above see its front, rays from below its back
+    assert set(np.unique(got["prim"][hit])) <= {0, -2}
+    d_rays = torch.from_numpy(rays).cuda()
+    d_hits = torch.empty((len(rays), 4), dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    ds.trace_device(d_rays.data_ptr(), len(rays), d_hits.data_ptr(), two_sided=True)
+    ds.ctx.sync()
+    dev = d_hits.cpu().numpy().view(np.uint8).view(got.dtype).reshape(-1)
+    assert np.array_equal(dev.view(np.uint32), got.view(np.uint32))
+    # any-hit rays are two-sided already: the flag is refused for them
+    with pytest.raises(ff.FireflyError):
+        ds.trace(rays, any_hit=True, two_sided=True)
+
+
+def test_at_scale_mesh_bit_exact(ctx, oracle):
+    """The at-scale mesh itself (icosphere subdivided 8x and displaced, in the
+    room: 1,310,732 triangles; its 8-wide BVH quantises boxes on a far finer
+    grid than the small room's): 1M incoherent rays and the 1920 x 1080
+    camera frame's primary rays, closest hits bit for bit (ids, t, u, v;
+    ties to the lowest index) against the oracle's CPU hierarchy, which
+    decides every triangle with the same restated test as the brute force;
+    any-hit answers for 500k rays with random tmax; two-sided closest hits
+    for 500k rays from inside the sphere."""
+    import firefly_b200 as ff
+    scn = scenes.displaced_icosphere(subdiv=8, width=1920, height=1080, env_w=64, env_h=32)
+    assert scn.num_triangles == 1_310_732
+    ds = ff.dScene(ctx, scn)
+    bvh = oracle.BVH(scn.triangle_soup())
+    try:
+        sets = {"incoherent": scenes.incoherent_rays(scn, 1_000_000, seed=51),
+                "camera": scenes.camera_rays(scn, 1920, 1080)}
+        for name, rays in sets.items():
+            got = ds.trace(rays)
+            ref = bvh.trace(rays, threads=cpu_threads())
+            bad = _same_closest(got, ref)
+            assert int(bad.sum()) == 0, (name, int(bad.sum()), got[np.argmax(bad)], ref[np.argmax(bad)])
+            assert (got["prim"] >= 0).mean() > 0.5
+        anyr = scenes.with_random_tmax(scenes.incoherent_rays(scn, 500_000, seed=52), scn, seed=53)
+        ga, ra = ds.trace(anyr, any_hit=True), bvh.trace(anyr, any_hit=True, threads=cpu_threads())
+        assert np.array_equal(ga["prim"] >= 0, ra["prim"] >= 0)
+        P = np.asarray(scn.positions, np.float64)[24:]   # the sphere (after the room's 24 vertices)
+        c = P.mean(0)
+        rng = np.random.default_rng(54)
+        inside = scenes.incoherent_rays(scn, 500_000, seed=55)
+        inside[:, 0:3] = (c + rng.normal(size=(len(inside), 3)) * 0.3).astype(np.float32)
+        g2, r2 = ds.trace(inside, two_sided=True), bvh.trace(inside, two_sided=True, threads=cpu_threads())
+        bad = _same_closest(g2, r2)
+        assert int(bad.sum()) == 0, int(bad.sum())
+        assert (g2["prim"] < -1).mean() > 0.9
+    finally:
+        bvh.close()
+        ds.close()

@@ -7,7 +7,10 @@ The entry point is called through the C ABI and its hits must equal those of
 ff_trace (the existing entry point) bit for bit, the tolerance of every trace
 test here, on two calls in a row: the scratch array it stages through keeps
 the previous call's contents, so the second call checks that nothing stale
-leaks into it.  The file is named to be collected last.
+leaks into it.  Across both calls the library's own count of device
+allocations (ff_debug_alloc_stats, every cudaMalloc it makes goes through
+one wrapper) must not move: the point of the entry point is that it
+allocates nothing.  The file is named to be collected last.
 """
 from __future__ import annotations
 
@@ -30,6 +33,12 @@ def _noalloc(lib, ctx, ds, rays, any_hit):
     return st, out
 
 
+def _alloc_stats(lib):
+    total, live = C.c_uint64(), C.c_int64()
+    assert lib.ff_debug_alloc_stats(C.byref(total), C.byref(live)) == 0
+    return total.value, live.value
+
+
 def test_noalloc_matches_ff_trace_on_two_calls():
     import firefly_b200 as ff
     from firefly_b200 import _abi as A
@@ -42,14 +51,18 @@ def test_noalloc_matches_ff_trace_on_two_calls():
         ds = ff.dScene(ctx, scn)
         # call 1: the maximum size, closest-hit
         rays1 = scenes.incoherent_rays(scn, A.FF_NOALLOC_MAX_RAYS, seed=101)
+        before = _alloc_stats(lib)
         st, got1 = _noalloc(lib, ctx, ds, rays1, any_hit=False)
         assert st == A.FF_OK, lib.ff_last_error_message(ctx.handle)
+        assert _alloc_stats(lib) == before, "the first call allocated device memory"
         ref1 = ds.trace(rays1)
         assert np.array_equal(got1.view(np.uint32), ref1.view(np.uint32))
         # call 2: fewer rays, any-hit, into the same scratch
         rays2 = scenes.with_random_tmax(scenes.incoherent_rays(scn, 40_000, seed=102), scn, seed=103)
+        before = _alloc_stats(lib)
         st, got2 = _noalloc(lib, ctx, ds, rays2, any_hit=True)
         assert st == A.FF_OK, lib.ff_last_error_message(ctx.handle)
+        assert _alloc_stats(lib) == before, "the second call allocated device memory"
         ref2 = ds.trace(rays2, any_hit=True)
         assert np.array_equal(got2.view(np.uint32), ref2.view(np.uint32))
         assert 0 < (got2["prim"] >= 0).sum() < len(rays2)
