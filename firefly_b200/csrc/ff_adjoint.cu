@@ -111,9 +111,9 @@ __device__ __noinline__ void shade_vertex(const LightCtx& lc, const FFSurf& surf
 {
     sh.c_spec = sh.c_diff = make_float3(0.f, 0.f, 0.f);
     switch (surf.kind) {
-        case FF_MAT_MIX: shade_mix(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, sp, key, L, sh); break;
-        case FF_MAT_DIFFUSE: shade_diffuse(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
-        case FF_MAT_CONDUCTOR: shade_conductor(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+        case FF_MAT_MIX: shade_mix<true>(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, sp, key, L, sh); break;
+        case FF_MAT_DIFFUSE: shade_diffuse<true>(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+        case FF_MAT_CONDUCTOR: shade_conductor<true>(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
         case FF_MAT_DIELECTRIC: shade_dielectric(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, back, sh); break;
         default: shade_coat(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
     }

@@ -133,13 +133,14 @@ __device__ __forceinline__ RoughTerms rough_terms(const ShadeOut& sh, float3 n, 
         if (sh.ext_pdf != 0.f && sh.ext_f != zero) t.dext = make_float3(sh.dlog_spec, sh.dlog_spec, sh.dlog_spec);
         return t;
     }
-    if (sh.c_nee_ggx != zero) t.nee = sh.c_nee_ggx * (float)ggx_dlog_dr(n, wi, wo, r);
+    // the adjoint runs in corrected mode: the FP32 GGX lobes
+    if (sh.c_nee_ggx != zero) t.nee = sh.c_nee_ggx * ggx_dlog_dr32(n, wi, wo, r);
     if (sh.c_spec != zero) {
         const float3 ws = make_float3(sh.r_spec.dx, sh.r_spec.dy, sh.r_spec.dz);
-        t.spec = sh.c_spec * (float)ggx_dlog_dr(n, ws, wo, r);
+        t.spec = sh.c_spec * ggx_dlog_dr32(n, ws, wo, r);
     }
     if (sh.ext_pdf != 0.f && sh.ext_f_ggx != zero) {
-        const float s = (float)ggx_dlog_dr(n, sh.ext_d, wo, r);
+        const float s = ggx_dlog_dr32(n, sh.ext_d, wo, r);
         const float3 df = sh.ext_f_ggx * s;
         t.dext = make_float3(sh.ext_f.x != 0.f ? df.x / sh.ext_f.x : 0.f, sh.ext_f.y != 0.f ? df.y / sh.ext_f.y : 0.f,
                              sh.ext_f.z != 0.f ? df.z / sh.ext_f.z : 0.f);

@@ -162,6 +162,7 @@ ff_status ff_scene_create(ff_context* ctx, const ff_scene_desc* d, ff_scene** ou
                 FF_REQUIRE(d->material_ids[i] < (d->num_materials ? d->num_materials : 1u),
                            "material id out of range");
         }
+        FF_REQUIRE(d->num_materials < (1u << 24), "at most 2^24 - 1 materials");
         for (uint32_t m = 0; m < d->num_materials; ++m) {
             const ff_material& mt = d->materials[m];
             FF_REQUIRE(mt.kind >= FF_MAT_MIX && mt.kind <= FF_MAT_COAT, "unknown material kind");

@@ -158,9 +158,9 @@ __global__ void __launch_bounds__(kBlock) k_training_paths(CR a)
             sample_light(lc, pos, key, L, wi, sp);
             sh.c_spec = sh.c_diff = make_float3(0.f, 0.f, 0.f);
             switch (surf.kind) {
-                case FF_MAT_MIX: shade_mix(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, sp, key, L, sh); break;
-                case FF_MAT_DIFFUSE: shade_diffuse(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
-                case FF_MAT_CONDUCTOR: shade_conductor(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+                case FF_MAT_MIX: shade_mix<true>(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, sp, key, L, sh); break;
+                case FF_MAT_DIFFUSE: shade_diffuse<true>(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
+                case FF_MAT_CONDUCTOR: shade_conductor<true>(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, sh); break;
                 case FF_MAT_DIELECTRIC:
                     shade_dielectric(FF_MODE_CORRECTED, lc, surf, pos, n, wo, wi, key, L, back, sh);
                     break;

@@ -164,10 +164,15 @@ __device__ __forceinline__ ff_ray make_ext_ray(float3 o, float3 d, bool two)
     return ff_ray{o.x, o.y, o.z, two ? -0.f : 0.f, d.x, d.y, d.z, __int_as_float(0x7f800000)};
 }
 
-// wf_mat_mix + BRDF_L / BRDF_f / BRDF_pdf (kernel.cu:617-651, dMaterial.cu:363-469)
+// wf_mat_mix + BRDF_L / BRDF_f / BRDF_pdf (kernel.cu:617-651, dMaterial.cu:363-469).
+// F32 selects the lobe set: the reference's FP64 arithmetic (parity mode) or
+// the FP32 restatement (corrected mode), Lobes in ff_shade.cuh.
+template <bool F32>
 __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf& mat, float3 pos, float3 n, float3 wo,
-                          float3 wi, float3 sp, uint32_t key, uint32_t L, ShadeOut& o)
+                                 float3 wi, float3 sp, uint32_t key, uint32_t L, ShadeOut& o)
 {
+    using LB = Lobes<F32>;
+    using real = typename LB::real;
     (void)sp;
     const bool corrected = mode == FF_MODE_CORRECTED;
     const float r = mat.roughness;
@@ -176,22 +181,23 @@ __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf
     const float3 Li = light_L(lc, wi);
     const float n_dot_wi = dot3(n, wi);
     if (n_dot_wi > 0.f) {
-        const double diff_pdf = diff_get_pdf();
-        const double spec_pdf = spec_get_pdf(n, wi, wo, r);
-        const double lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+        const real diff_pdf = LB::diff_pdf();
+        const real spec_pdf = LB::spec_pdf(n, wi, wo, r);
+        const real lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
         if (lpdf > 0.f && Li != make_float3(0.f, 0.f, 0.f)) {
             // dMaterial.cu:386-393: weights 1 for a delta light
-            const double diff_w = lc.is_dir ? 1.0 : power_heuristic(lpdf, diff_pdf);
-            const double spec_w = lc.is_dir ? 1.0 : power_heuristic(lpdf, spec_pdf);
-            float3 f = spec_f(mat, n, wi, wo) * n_dot_wi;
+            const real diff_w = lc.is_dir ? (real)1 : LB::power(lpdf, diff_pdf);
+            const real spec_w = lc.is_dir ? (real)1 : LB::power(lpdf, spec_pdf);
+            float3 f = LB::spec(mat, n, wi, wo) * n_dot_wi;
             if (f != make_float3(0.f, 0.f, 0.f)) Lsum = Lsum + ((f * (float)spec_w) * Li) / (float)lpdf;
             o.c_nee_ggx = Lsum;
-            f = diff_f(mat, n, wi, wo) * n_dot_wi;
+            f = LB::diff(mat, n, wi, wo) * n_dot_wi;
             if (f != make_float3(0.f, 0.f, 0.f)) Lsum = Lsum + ((f * (float)diff_w) * Li) / (float)lpdf;
         }
     }
     o.c_nee = Lsum;
-    const float3 wi_spec = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
+    const float3 wi_spec =
+        LB::sample_spec(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
     const float3 wi_diff = diff_sample(n, ff_rand(key, dim_of(L, DIM_DIFF)), ff_rand(key, dim_of(L, DIM_DIFF + 1)));
     // BSDF-sampled MIS terms (none for a delta light, dMaterial.cu:410);
     // their visibility is traced as shadow rays
@@ -201,10 +207,10 @@ __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf
         const float nd = dot3(n, wi_spec);
         ff_ray vr;
         if (nd > 0.f && light_vis_ray(lc, org, wi_spec, key, L, DIM_SPEC_VIS, vr)) {
-            const double spdf = spec_get_pdf(n, wi_spec, wo, r);
-            const double lpdf = light_pdf(lc, pos, wi_spec, key, L, DIM_SPEC_PDF);
-            const double wgt = power_heuristic(spdf, lpdf);
-            const float3 f = spec_f(mat, n, wi_spec, wo) * nd;
+            const real spdf = LB::spec_pdf(n, wi_spec, wo, r);
+            const real lpdf = light_pdf(lc, pos, wi_spec, key, L, DIM_SPEC_PDF);
+            const real wgt = LB::power(spdf, lpdf);
+            const float3 f = LB::spec(mat, n, wi_spec, wo) * nd;
             const float3 Li2 = light_L(lc, wi_spec);
             if (f != make_float3(0.f, 0.f, 0.f) && spdf > 0.f && Li2 != make_float3(0.f, 0.f, 0.f)) {
                 o.c_spec = ((f * Li2) * (float)wgt) / (float)spdf;
@@ -219,10 +225,10 @@ __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf
         const float nd = dot3(n, wi_diff);
         ff_ray vr;
         if (nd > 0.f && light_vis_ray(lc, org, wi_diff, key, L, DIM_DIFF_VIS, vr)) {
-            const double dpdf = diff_get_pdf();
-            const double lpdf = light_pdf(lc, pos, wi_diff, key, L, DIM_DIFF_PDF);
-            const double wgt = power_heuristic(dpdf, lpdf);
-            const float3 f = diff_f(mat, n, wi_diff, wo) * nd;
+            const real dpdf = LB::diff_pdf();
+            const real lpdf = light_pdf(lc, pos, wi_diff, key, L, DIM_DIFF_PDF);
+            const real wgt = LB::power(dpdf, lpdf);
+            const float3 f = LB::diff(mat, n, wi_diff, wo) * nd;
             const float3 Li2 = light_L(lc, wi_diff);
             if (f != make_float3(0.f, 0.f, 0.f) && dpdf > 0.f && Li2 != make_float3(0.f, 0.f, 0.f)) {
                 o.c_diff = ((f * Li2) * (float)wgt) / (float)dpdf;
@@ -233,51 +239,58 @@ __device__ inline void shade_mix(uint32_t mode, const LightCtx& lc, const FFSurf
     }
     const float3 dir = ff_rand(key, dim_of(L, DIM_LOBE)) < 0.5f ? wi_diff : wi_spec;
     o.ext_d = dir;
-    o.ext_f = brdf_f(mat, n, dir, wo);
-    o.ext_f_ggx = spec_f(mat, n, dir, wo);
-    o.ext_pdf = brdf_pdf(mat, n, dir, wo);
+    // BRDF_f = spec_f + diff_f, BRDF_pdf = 0.5 (spec_pdf + diff_pdf) (dMaterial.cu:459-469)
+    o.ext_f_ggx = LB::spec(mat, n, dir, wo);
+    o.ext_f = o.ext_f_ggx + LB::diff(mat, n, dir, wo);
+    if constexpr (F32) o.ext_pdf = 0.5f * (LB::spec_pdf(n, dir, wo, r) + LB::diff_pdf());
+    else o.ext_pdf = (float)(0.5 * (double)(LB::spec_pdf(n, dir, wo, r) + (float)LB::diff_pdf()));
     o.ext_cos = hmax(0.f, dot3(n, dir));
 }
 
 // wf_mat_diffuse (kernel.cu:546-577): diff_L returns 0 in the reference (dMaterial.cu:179-227).
+template <bool F32>
 __device__ inline void shade_diffuse(uint32_t mode, const LightCtx& lc, const FFSurf& mat, float3 pos, float3 n,
-                              float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
+                                     float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
 {
+    using LB = Lobes<F32>;
     o.c_nee = make_float3(0.f, 0.f, 0.f);
     if (mode == FF_MODE_CORRECTED) {
         const float nd = dot3(n, wi);
         const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
         const float3 Li = light_L(lc, wi);
-        if (nd > 0.f && lpdf > 0.f) o.c_nee = ((diff_f(mat, n, wi, wo) * nd) * Li) / lpdf;
+        if (nd > 0.f && lpdf > 0.f) o.c_nee = ((LB::diff(mat, n, wi, wo) * nd) * Li) / lpdf;
     }
     o.ray_spec = o.ray_diff = false;
     const float3 dir = diff_sample(n, ff_rand(key, dim_of(L, DIM_DIFF)), ff_rand(key, dim_of(L, DIM_DIFF + 1)));
     o.ext_d = dir;
-    o.ext_f = diff_f(mat, n, dir, wo);
+    o.ext_f = LB::diff(mat, n, dir, wo);
     o.c_nee_ggx = o.ext_f_ggx = make_float3(0.f, 0.f, 0.f);
-    o.ext_pdf = (float)diff_get_pdf();
+    o.ext_pdf = (float)LB::diff_pdf();
     o.ext_cos = hmax(0.f, dot3(n, dir));
 }
 
 // wf_mat_cook (kernel.cu:580-614): spec_L returns 0 in the reference (dMaterial.cu:314-361).
+template <bool F32>
 __device__ inline void shade_conductor(uint32_t mode, const LightCtx& lc, const FFSurf& mat, float3 pos, float3 n,
-                                float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
+                                       float3 wo, float3 wi, uint32_t key, uint32_t L, ShadeOut& o)
 {
+    using LB = Lobes<F32>;
     o.c_nee = make_float3(0.f, 0.f, 0.f);
     if (mode == FF_MODE_CORRECTED) {
         const float nd = dot3(n, wi);
         const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
         const float3 Li = light_L(lc, wi);
-        if (nd > 0.f && lpdf > 0.f) o.c_nee = ((spec_f(mat, n, wi, wo) * nd) * Li) / lpdf;
+        if (nd > 0.f && lpdf > 0.f) o.c_nee = ((LB::spec(mat, n, wi, wo) * nd) * Li) / lpdf;
     }
     o.ray_spec = o.ray_diff = false;
     const float r = mat.roughness;
-    const float3 dir = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
+    const float3 dir =
+        LB::sample_spec(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
     o.ext_d = dir;
-    o.ext_f = spec_f(mat, n, dir, wo);
+    o.ext_f = LB::spec(mat, n, dir, wo);
     o.c_nee_ggx = o.c_nee;
     o.ext_f_ggx = o.ext_f;
-    o.ext_pdf = spec_get_pdf(n, dir, wo, r);
+    o.ext_pdf = LB::spec_pdf(n, dir, wo, r);
     o.ext_cos = hmax(0.f, dot3(n, dir));
 }
 
@@ -409,9 +422,10 @@ __device__ __forceinline__ void diel_eval(const Diel& d, float3 n, float3 wo, fl
 // tan^2 theta = alpha^2 e0 / (1 - e0), phi = 2 pi e1, in the frame of n.
 __device__ __forceinline__ float3 ggx_sample_normal(float3 n, float alpha, float e0, float e1)
 {
+    // e0 = 1 (the sampler can return 1.0f) gives t2 = inf: theta = pi / 2
     const float t2 = (alpha * alpha) * (e0 / (1.f - e0));
     const float ct = 1.f / sqrtf(1.f + t2);
-    const float st = sqrtf(t2) * ct;
+    const float st = isinf(t2) ? 1.f : sqrtf(t2) * ct;
     const float phi = FF_2PI * e1;
     float3 T, B;
     frame(n, T, B);
@@ -470,12 +484,6 @@ __device__ __forceinline__ float diel_dlog_dr(const Diel& d, float3 n, float3 wo
     return 2.f * r * (dD + dG);
 }
 
-__device__ __forceinline__ float power_heuristic_f(float f, float g)
-{
-    const float f2 = f * f;
-    return f2 / (f2 + g * g);
-}
-
 // The dielectric vertex: light-sampled NEE weighted against the BSDF's pdf
 // (power heuristic; weight 1 for a delta light), the continuation sampled
 // from the BSDF, and, unless the light is a delta light, the light reached
@@ -498,7 +506,7 @@ __device__ inline void shade_dielectric(uint32_t mode, const LightCtx& lc, const
         diel_eval(d, n, wo, wi, f, bpdf);
         const float lpdf = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
         if (f != zero && lpdf > 0.f) {
-            const float w = lc.is_dir ? 1.f : power_heuristic_f(lpdf, bpdf);
+            const float w = lc.is_dir ? 1.f : power_heuristic32(lpdf, bpdf);
             o.c_nee = ((f * (fabsf(dot3(n, wi)) * w)) * light_L(lc, wi)) / lpdf;
             o.dlog_nee = diel_dlog_dr(d, n, wo, wi, mat.roughness);
         }
@@ -519,7 +527,7 @@ __device__ inline void shade_dielectric(uint32_t mode, const LightCtx& lc, const
         if (!lc.is_dir && light_vis_ray(lc, pos + dir * 0.001f, dir, key, L, DIM_SPEC_VIS, vr)) {
             const float3 Li = light_L(lc, dir);
             if (Li != zero) {
-                const float w = power_heuristic_f(pdf, light_pdf(lc, pos, dir, key, L, DIM_SPEC_PDF));
+                const float w = power_heuristic32(pdf, light_pdf(lc, pos, dir, key, L, DIM_SPEC_PDF));
                 o.c_spec = ((f * (c * w)) * Li) / pdf;
                 o.ray_spec = true;
                 o.r_spec = vr;
@@ -536,14 +544,16 @@ __device__ inline void shade_dielectric(uint32_t mode, const LightCtx& lc, const
 // Diffuse base under a GGX clear coat (no reference counterpart): the coat
 // reflects with Schlick Fresnel at the coat IOR, the base is Lambertian
 // weighted by (1 - F).  Continuation picks the coat lobe or the base with
-// equal probability; the pdf is the 50/50 mixture, as BRDF_pdf's.
+// equal probability; the pdf is the 50/50 mixture, as BRDF_pdf's.  The GGX
+// lobe is the reference's spec_f in FP32 (spec_f32): there is no reference
+// image of this material to match.
 __device__ inline float3 coat_spec_f(const FFSurf& mat, float3 n, float3 wi, float3 wo, float r0)
 {
     FFSurf c = mat;
     c.fresnel = make_float3(r0, r0, r0);
     c.albedo = make_float3(1.f, 1.f, 1.f);
     c.metallic = 0.f;
-    return spec_f(c, n, wi, wo);
+    return spec_f32(c, n, wi, wo);
 }
 __device__ inline float3 coat_f(const FFSurf& mat, float3 n, float3 wi, float3 wo, float r0)
 {
@@ -573,7 +583,7 @@ __device__ inline void shade_coat(uint32_t mode, const LightCtx& lc, const FFSur
     const float r = mat.roughness;
     float3 dir;
     if (ff_rand(key, dim_of(L, DIM_LOBE)) < 0.5f) {
-        dir = spec_sample(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
+        dir = spec_sample32(n, wo, r, ff_rand(key, dim_of(L, DIM_SPEC)), ff_rand(key, dim_of(L, DIM_SPEC + 1)));
     } else {
         // cosine-weighted hemisphere (concentric disk lifted to the hemisphere)
         const float2 dsk = concentric_disk(make_float2(ff_rand(key, dim_of(L, DIM_DIFF)),
@@ -587,7 +597,7 @@ __device__ inline void shade_coat(uint32_t mode, const LightCtx& lc, const FFSur
     o.ext_d = dir;
     o.ext_f = coat_f(mat, n, dir, wo, r0);
     o.ext_f_ggx = coat_spec_f(mat, n, dir, wo, r0);
-    o.ext_pdf = 0.5f * spec_get_pdf(n, dir, wo, r) + 0.5f * c * FF_1_PI;
+    o.ext_pdf = 0.5f * spec_get_pdf32(n, dir, wo, r) + 0.5f * c * FF_1_PI;
     o.ext_cos = c;
 }
 

@@ -295,6 +295,128 @@ FF_D float brdf_pdf(const FFSurf& m, float3 n, float3 wi, float3 wo)
     return (float)(0.5 * (double)(sp + dp));
 }
 
+// ------------------------------------------------ FP32 lobes (corrected mode)
+// The same lobes with every intermediate in FP32.  The reference widens the
+// GGX D and G terms, the Fresnel power, the sampling angles and the MIS
+// weights to double (dMaterial.cu:114-313); parity mode keeps that, so that
+// images match the reference's, while corrected mode, which has no reference
+// counterpart to match, computes them in FP32 (the FP64 units of the SM are
+// a fraction of its FP32 units, and doubles take two registers each).  Same
+// formulas and operand order; the GGX sample takes cos and sin of theta from
+// tan(theta) = r^2 sqrt(e0 / (1 - e0)) instead of going through atan.
+FF_D float ggx_ndf32(float3 n, float3 h, float r)
+{
+    const float a2 = r * r * r * r;
+    const float nh = hmax(0.f, dot3(n, h));
+    const float k = (nh * nh) * (a2 - 1.f) + 1.f;
+    return a2 / (FF_PI * (k * k));
+}
+FF_D float geo_atten32(float3 wi, float3 wo, float3 n, float r)
+{
+    const float rp = r + 1.f;
+    const float k = (rp * rp) / 8.f;
+    const float nl = hmax(dot3(n, wi), 0.f);
+    const float nv = hmax(dot3(n, wo), 0.f);
+    return (nl / (nl * (1.f - k) + k)) * (nv / (nv * (1.f - k) + k));
+}
+FF_D float3 fresnel32(float3 f0, float3 h, float3 wo)
+{
+    const float x = 1.f - hmax(0.f, dot3(h, wo));
+    const float x2 = x * x;
+    const float p = (x2 * x2) * x;
+    return f0 + (1.f - f0) * p;
+}
+FF_D float spec_get_pdf32(float3 n, float3 wi, float3 wo, float r)
+{
+    const float3 wh = normalize3(wo + wi);
+    const float whn = hmax(dot3(wh, n), 0.f);
+    const float wowh = hmax(dot3(wo, wh), 0.f);
+    return (ggx_ndf32(n, wh, r) * whn) / hmax(4.f * wowh, 0.001f);
+}
+FF_D float3 spec_f32(const FFSurf& mat, float3 n, float3 wi, float3 wo)
+{
+    const float r = mat.roughness;
+    const float3 f0 = f0_of(mat, mat.albedo);
+    const float3 wh = normalize3(wo + wi);
+    const float ndwi = hmax(dot3(n, wi), 0.f);
+    const float ndwo = hmax(dot3(n, wo), 0.f);
+    const float3 F = fresnel32(f0, wh, wi);
+    const float3 num = (ggx_ndf32(n, wh, r) * geo_atten32(wi, wo, n, r)) * F;
+    return num / hmax((4.f * ndwo) * ndwi, 0.001f);
+}
+FF_D float3 diff_f32(const FFSurf& mat, float3 n, float3 wi, float3 wo)
+{
+    (void)n;
+    const float3 a = mat.albedo;
+    const float3 wh = normalize3(wo + wi);
+    float3 kd = make_float3(1.f, 1.f, 1.f) - fresnel32(f0_of(mat, a), wh, wi);
+    kd = kd * (1.f - mat.metallic);
+    return (kd * a) * FF_1_PI;
+}
+FF_D float3 spec_sample32(float3 N, float3 wo, float r, float e0, float e1)
+{
+    // e0 = 1 (the sampler can return 1.0f) gives t = inf: theta = pi / 2
+    const float t = (r * r) * sqrtf(e0 / (1.f - e0));
+    const float ct = 1.f / sqrtf(1.f + t * t);
+    const float st = isinf(t) ? 1.f : t * ct;
+    const float phi = FF_2PI * e1;
+    float3 T, B;
+    frame(N, T, B);
+    const float3 s = T * (st * cosf(phi)) + N * ct + B * (st * sinf(phi));
+    return -reflect3(wo, normalize3(s));
+}
+FF_D float power_heuristic32(float f, float g)
+{
+    const float f2 = f * f;
+    return f2 / (f2 + g * g);
+}
+// d/dr log(D G) of the FP32 GGX lobe (ggx_dlog_dr's derivation).
+FF_D float ggx_dlog_dr32(float3 n, float3 wi, float3 wo, float r)
+{
+    const float3 h = normalize3(wo + wi);
+    const float a2 = r * r * r * r;
+    const float nh = hmax(0.f, dot3(n, h));
+    const float nh2 = nh * nh;
+    const float dlogD = 4.f / r - 8.f * r * r * r * nh2 / (nh2 * (a2 - 1.f) + 1.f);
+    const float k = (r + 1.f) * (r + 1.f) / 8.f;
+    const float nl = hmax(dot3(n, wi), 0.f);
+    const float nv = hmax(dot3(n, wo), 0.f);
+    return dlogD - (r + 1.f) / 4.f * ((1.f - nl) / (nl * (1.f - k) + k) + (1.f - nv) / (nv * (1.f - k) + k));
+}
+
+// The lobe set of a mode: Lobes<false> the reference's (FP64 where it is
+// FP64: parity mode), Lobes<true> the FP32 restatement (corrected mode).
+template <bool F32>
+struct Lobes;
+template <>
+struct Lobes<false> {
+    using real = double;
+    static FF_D double diff_pdf() { return diff_get_pdf(); }
+    static FF_D float spec_pdf(float3 n, float3 wi, float3 wo, float r) { return spec_get_pdf(n, wi, wo, r); }
+    static FF_D float3 spec(const FFSurf& m, float3 n, float3 wi, float3 wo) { return spec_f(m, n, wi, wo); }
+    static FF_D float3 diff(const FFSurf& m, float3 n, float3 wi, float3 wo) { return diff_f(m, n, wi, wo); }
+    static FF_D float3 sample_spec(float3 n, float3 wo, float r, float e0, float e1)
+    {
+        return spec_sample(n, wo, r, e0, e1);
+    }
+    static FF_D double power(double f, double g) { return power_heuristic(f, g); }
+    static FF_D float dlog_dr(float3 n, float3 wi, float3 wo, float r) { return (float)ggx_dlog_dr(n, wi, wo, r); }
+};
+template <>
+struct Lobes<true> {
+    using real = float;
+    static FF_D float diff_pdf() { return 1.f / (2.f * FF_PI); }
+    static FF_D float spec_pdf(float3 n, float3 wi, float3 wo, float r) { return spec_get_pdf32(n, wi, wo, r); }
+    static FF_D float3 spec(const FFSurf& m, float3 n, float3 wi, float3 wo) { return spec_f32(m, n, wi, wo); }
+    static FF_D float3 diff(const FFSurf& m, float3 n, float3 wi, float3 wo) { return diff_f32(m, n, wi, wo); }
+    static FF_D float3 sample_spec(float3 n, float3 wo, float r, float e0, float e1)
+    {
+        return spec_sample32(n, wo, r, e0, e1);
+    }
+    static FF_D float power(float f, float g) { return power_heuristic32(f, g); }
+    static FF_D float dlog_dr(float3 n, float3 wi, float3 wo, float r) { return ggx_dlog_dr32(n, wi, wo, r); }
+};
+
 // ----------------------------------------------------------------- lights
 // Environment light with importance tables (dEnvironmentLight.cu).
 template <class T>

@@ -36,6 +36,7 @@
 // texture, the roughness texture and the environment map.  The primal
 // instantiations compile none of that code.
 #include <algorithm>
+#include <cstddef>
 #include <vector>
 
 #include "ff_adjoint.cuh"
@@ -59,6 +60,45 @@ constexpr uint64_t kDefaultPoolTarget = 1ull << 23;
 // Counter words of one frame (zeroed at the start of each frame).
 enum { C_EXT = 0, C_SH = 1, C_MAT = 2, C_ACTIVE = 2 + kKinds, C_WORDS = 8 + kKinds };
 
+// The slot's ray (origin, direction) and its visibility word: byte k = the
+// any-hit trace's answer for shadow ray k (1 occluded), byte 3 = which shadow
+// rays k_shade queued (bit k).
+struct __align__(32) SlotRay {
+    float ox, oy, oz;
+    uint32_t vis;
+    float dx, dy, dz, pad;
+};
+// What a vertex's shading leaves for k_logic.
+struct __align__(32) SlotShade {
+    float nee_x, nee_y, nee_z, pdf;   // c_nee, ext_pdf
+    float f_x, f_y, f_z, cosine;      // ext_f, ext_cos
+};
+struct __align__(32) SlotMis {
+    float spec_x, spec_y, spec_z, pad0;   // c_spec
+    float diff_x, diff_y, diff_z, pad1;   // c_diff
+};
+// The vertex k_logic hands to k_shade.  word = material index (bits 0-23) |
+// path length (bits 24-30) | hit from inside an object (bit 31).
+struct __align__(32) SlotVtx {
+    float px, py, pz;
+    uint32_t word;
+    float nx, ny, nz;   // shading normal
+    uint32_t key;
+    float wix, wiy, wiz;   // NEE direction
+    float u;
+    float wox, woy, woz;   // toward the previous vertex
+    float v;
+};
+static_assert(sizeof(SlotRay) == 32 && sizeof(SlotShade) == 32 && sizeof(SlotMis) == 32 && sizeof(SlotVtx) == 64,
+              "slot records are whole 32-byte sectors");
+constexpr uint32_t kVtxMatBits = 24, kVtxLenShift = 24, kVtxLenMask = 0x7f;
+// Byte of shadow ray k's answer for slot s in the SlotRay array (the tag the
+// any-hit trace writes to): the low three bytes of the vis word.
+__device__ __forceinline__ uint32_t vis_byte(uint32_t s, uint32_t k)
+{
+    return (uint32_t)sizeof(SlotRay) * s + (uint32_t)offsetof(SlotRay, vis) + k;
+}
+
 struct WF {
     // launch constants
     uint32_t P, WH, W, H, m;
@@ -72,21 +112,15 @@ struct WF {
     uint32_t* length;
     uint32_t* phase;
     float4* beta;
-    float4* ray_o;
-    float4* ray_d;
-    // visibility word per slot: byte k = the trace's answer for shadow ray k
-    // (1 occluded), byte 3 = which shadow rays k_shade queued (bit k)
-    uint32_t* vis;
-    float4* c_nee;
-    float4* c_spec;
-    float4* c_diff;
-    float4* ext_fp;   // f.xyz, pdf
-    float* ext_cos;
-    float4* hit_pos;  // xyz, w = material index bits
-    float4* hit_nrm;      // shading normal
+    // Per-slot records that k_shade reaches through its material queue, i.e.
+    // scattered over the slots: each is whole 32-byte sectors, so a scattered
+    // access moves no bytes it does not use (a lone 16-byte field fetches or
+    // fills a half-used sector).
+    SlotRay* ray;     // the slot's current ray and its visibility word
+    SlotShade* shd;   // k_shade -> k_logic: NEE term, continuation f / pdf / cos
+    SlotMis* mis;     // k_shade -> k_logic: BSDF-sampled light terms (mix, dielectric)
+    SlotVtx* vtx;     // k_logic -> k_shade: the vertex to shade
     float4* hit_ngeo;     // interpolated normal, written only under a normal texture
-    float4* light_wi;
-    float4* light_sp;
     float4* acc;
     float4* acc_c;
     uint32_t* cnt;
@@ -95,7 +129,7 @@ struct WF {
     uint32_t* ext_tag;   // per queued extension ray: its slot
     ff_hit* ext_hits;    // per slot: the closest hit of its extension ray (written by k_trace)
     ff_ray* sh_rays;
-    uint32_t* sh_tag;    // per queued shadow ray: 4 * slot + k (k = 0 NEE, 1 spec, 2 diff)
+    uint32_t* sh_tag;    // per queued shadow ray: the byte of its answer in the SlotRay array (vis_byte)
     uint32_t* mat_queue;   // kKinds * P
     uint32_t* ctr;         // C_WORDS
     unsigned long long* totals;  // [0] extension rays, [1] shadow rays, [2] samples
@@ -106,7 +140,6 @@ struct WF {
     const ff_area_light* area;
     uint32_t n_area;
     const FFTexView* tex;
-    float2* hit_uv;
     FFEnvView env;
     FFLightSet lights;
     ff_camera cam;
@@ -177,8 +210,7 @@ __device__ void start_sample(const WF& w, uint32_t s, uint32_t sample, bool& pus
     const int x = (int)(pix % w.W), y = (int)(pix / w.W);
     float3 o, d;
     gen_camera_ray(w.cam, (int)w.W, (int)w.H, x, y, rand2(key, 0, DIM_CAM_JITTER), rand2(key, 0, DIM_CAM_LENS), o, d);
-    w.ray_o[s] = f4(o);
-    w.ray_d[s] = f4(d);
+    w.ray[s] = SlotRay{o.x, o.y, o.z, 0u, d.x, d.y, d.z, 0.f};
     ray = ff_ray{o.x, o.y, o.z, 0.f, d.x, d.y, d.z, __int_as_float(0x7f800000)};
     push = true;
 }
@@ -213,7 +245,8 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             const ff_hit hit = w.ext_hits[s];
             const uint32_t L = w.length[s] + 1;  // wf_extend's length++
             const bool found = hit.prim != -1;
-            const float3 ro = xyz(w.ray_o[s]), rd = xyz(w.ray_d[s]);
+            const SlotRay sr = w.ray[s];
+            const float3 ro = make_float3(sr.ox, sr.oy, sr.oz), rd = make_float3(sr.dx, sr.dy, sr.dz);
             float3 beta = xyz(w.beta[s]);
             float4 acc = w.acc[s];
             float4 accc = ADJ ? make_float4(0.f, 0.f, 0.f, 0.f) : w.acc_c[s];   // no compensation in the adjoint
@@ -245,22 +278,27 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             }
             if (L > 1) {
                 // kernel.cu:357-359: light_brdf * beta when the NEE ray was unoccluded
-                const uint32_t vw = w.vis[s];
+                const uint32_t vw = sr.vis;
+                const SlotShade sd = w.shd[s];
                 const bool vis = (vw & (1u << 24)) && !(vw & 0xffu);
                 const bool vis_s = (vw & (2u << 24)) && !(vw & 0xff00u);
                 const bool vis_d = (vw & (4u << 24)) && !(vw & 0xff0000u);
                 if (w.mode == FF_MODE_CORRECTED) {
                     // every term gated by its own visibility ray
                     float3 lb = make_float3(0.f, 0.f, 0.f);
-                    if (vis) lb = lb + xyz(w.c_nee[s]);
-                    if (vis_s) lb = lb + xyz(w.c_spec[s]);
-                    if (vis_d) lb = lb + xyz(w.c_diff[s]);
+                    if (vis) lb = lb + make_float3(sd.nee_x, sd.nee_y, sd.nee_z);
+                    if (vis_s || vis_d) {
+                        const SlotMis sm = w.mis[s];
+                        if (vis_s) lb = lb + make_float3(sm.spec_x, sm.spec_y, sm.spec_z);
+                        if (vis_d) lb = lb + make_float3(sm.diff_x, sm.diff_y, sm.diff_z);
+                    }
                     if (ADJ) {
                         if (replay) {
                             // the previous vertex's gradients, now that its shadow rays are answered
                             const float4 va = w.v_albedo[s];
                             const uint32_t flags = __float_as_uint(va.w);
-                            const float2 uv = w.hit_uv[s];
+                            const SlotVtx& pv = w.vtx[s];   // the previous vertex
+                            const float2 uv = make_float2(pv.u, pv.v);
                             if (flags & V_ALBEDO) {
                                 const FFTexView tv = w.tex[w.adj_texture];
                                 touched += scatter_footprint(w.grad_tex, footprint(tv.width, tv.height, uv.x, uv.y),
@@ -280,7 +318,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                             }
                             if ((flags & V_ENV) && vis) {
                                 // NEE term c_nee = coef * Le(wi): d/dLe = beta * coef
-                                float3 wl = xyz(w.light_wi[s]);
+                                float3 wl = make_float3(pv.wix, pv.wiy, pv.wiz);
                                 wl.y = clampf(wl.y, -1.f, 1.f);
                                 const float2 euv = spherical_map(wl);
                                 touched += scatter_footprint(w.grad_env, footprint(w.env.width, w.env.height, euv.x, euv.y),
@@ -293,15 +331,17 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                     }
                 } else if (!ADJ && vis) {
                     // parity: the whole light_brdf, MIS terms included, rides on the NEE ray
-                    float3 lb = xyz(w.c_nee[s]);
-                    if (vis_s) lb = lb + xyz(w.c_spec[s]);
-                    if (vis_d) lb = lb + xyz(w.c_diff[s]);
+                    float3 lb = make_float3(sd.nee_x, sd.nee_y, sd.nee_z);
+                    if (vis_s || vis_d) {
+                        const SlotMis sm = w.mis[s];
+                        if (vis_s) lb = lb + make_float3(sm.spec_x, sm.spec_y, sm.spec_z);
+                        if (vis_d) lb = lb + make_float3(sm.diff_x, sm.diff_y, sm.diff_z);
+                    }
                     kahan_add(acc, accc, lb * beta);
                 }
-                const float4 fp = w.ext_fp[s];
-                const float3 f = xyz(fp);
-                const float pdf = fp.w;
-                const float cosine = w.ext_cos[s];
+                const float3 f = make_float3(sd.f_x, sd.f_y, sd.f_z);
+                const float pdf = sd.pdf;
+                const float cosine = sd.cosine;
                 if (f == make_float3(0.f, 0.f, 0.f) || pdf == 0.f) {
                     terminate = true;
                 } else {
@@ -351,17 +391,22 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                     }
                 }
                 if (!query) {
-                    w.hit_uv[s] = uv;
                     // Light sample (kernel.cu:435, light get_direction).
                     float3 wi, sp;
                     sample_light(select_light(w.lights, key, L), pos, key, L, wi, sp);
                     w.length[s] = L;
                     w.beta[s] = f4(beta);
-                    w.hit_pos[s] = f4(pos, __uint_as_float(t.material | (back ? kBackFace : 0u)));
-                    w.hit_nrm[s] = f4(ns);
+                    SlotVtx vx;
+                    vx.px = pos.x, vx.py = pos.y, vx.pz = pos.z;
+                    vx.word = t.material | (L << kVtxLenShift) | (back ? kBackFace : 0u);
+                    vx.nx = ns.x, vx.ny = ns.y, vx.nz = ns.z;
+                    vx.key = key;
+                    vx.wix = wi.x, vx.wiy = wi.y, vx.wiz = wi.z;   // (the sample point is not needed downstream)
+                    vx.u = uv.x;
+                    vx.wox = -rd.x, vx.woy = -rd.y, vx.woz = -rd.z;
+                    vx.v = uv.y;
+                    w.vtx[s] = vx;
                     if (mm.normal_tex >= 0) w.hit_ngeo[s] = f4(n);
-                    w.light_wi[s] = f4(wi);
-                    w.light_sp[s] = f4(sp);
                     kind = mm.kind;
                 }
             }
@@ -422,8 +467,9 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
 // SEL: the light is chosen per vertex (FF_LIGHT_ALL); otherwise one light
 // context serves the whole launch (fewer live registers).  ADJ: the adjoint's
 // instantiation, which also leaves the vertex's derivative terms in the slot
-// during a replay.
-template <int KIND, bool SEL, bool ADJ>
+// during a replay.  CORR: corrected mode, whose reference lobes run in FP32
+// (parity mode keeps the reference's FP64 arithmetic; Lobes, ff_shade.cuh).
+template <int KIND, bool SEL, bool ADJ, bool CORR>
 __global__ void __launch_bounds__(128) k_shade(WF w)
 {
     const uint32_t n = w.ctr[C_MAT + KIND];
@@ -442,25 +488,25 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
         uint32_t s = 0;
         if (valid) {
             s = w.mat_queue[(size_t)KIND * w.P + qi];
-            const float4 hp = w.hit_pos[s];
-            const float3 pos = xyz(hp);
-            const bool back = (__float_as_uint(hp.w) & kBackFace) != 0;   // hit from inside an object
-            const ff_material& mm = w.mats[__float_as_uint(hp.w) & ~kBackFace];
-            const FFSurf mat = resolve_surface(mm, w.tex, w.hit_uv[s]);
-            const float3 n = xyz(w.hit_nrm[s]);   // shading normal
+            const SlotVtx vx = w.vtx[s];
+            const float3 pos = make_float3(vx.px, vx.py, vx.pz);
+            const bool back = (vx.word & kBackFace) != 0;   // hit from inside an object
+            const ff_material& mm = w.mats[vx.word & ((1u << kVtxMatBits) - 1u)];
+            const FFSurf mat = resolve_surface(mm, w.tex, make_float2(vx.u, vx.v));
+            const float3 n = make_float3(vx.nx, vx.ny, vx.nz);   // shading normal
             // the normal the ray offsets follow (kernel.cu:437): differs from n
             // only under a normal texture
             const float3 ng = mm.normal_tex >= 0 ? xyz(w.hit_ngeo[s]) : n;
-            const float3 wo = -xyz(w.ray_d[s]);
-            const float3 wi = xyz(w.light_wi[s]);
-            const float3 sp = xyz(w.light_sp[s]);
-            const uint32_t key = w.key[s];
-            const uint32_t L = w.length[s];
+            const float3 wo = make_float3(vx.wox, vx.woy, vx.woz);
+            const float3 wi = make_float3(vx.wix, vx.wiy, vx.wiz);
+            const float3 sp = make_float3(0.f, 0.f, 0.f);   // BRDF_L does not use the NEE sample point
+            const uint32_t key = vx.key;
+            const uint32_t L = (vx.word >> kVtxLenShift) & kVtxLenMask;
             if (SEL) lc = select_light(w.lights, key, L);
             o.c_spec = o.c_diff = make_float3(0.f, 0.f, 0.f);
-            if (KIND == FF_MAT_MIX) shade_mix(w.mode, lc, mat, pos, n, wo, wi, sp, key, L, o);
-            else if (KIND == FF_MAT_DIFFUSE) shade_diffuse(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
-            else if (KIND == FF_MAT_CONDUCTOR) shade_conductor(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
+            if (KIND == FF_MAT_MIX) shade_mix<CORR>(w.mode, lc, mat, pos, n, wo, wi, sp, key, L, o);
+            else if (KIND == FF_MAT_DIFFUSE) shade_diffuse<CORR>(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
+            else if (KIND == FF_MAT_CONDUCTOR) shade_conductor<CORR>(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
             else if (KIND == FF_MAT_DIELECTRIC) shade_dielectric(w.mode, lc, mat, pos, n, wo, wi, key, L, back, o);
             else shade_coat(w.mode, lc, mat, pos, n, wo, wi, key, L, o);
             // NEE shadow ray of wf_shadow: light_ray = position + normal * SHADOW_OFFSET (kernel.cu:437);
@@ -476,13 +522,9 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
             if (w.mode == FF_MODE_CORRECTED || KIND == FF_MAT_DIELECTRIC || back)
                 o.ext_o = pos + ng * (side * w.shadow_offset);
             ext_two = runs_inside(back, KIND == FF_MAT_DIELECTRIC, side);
-            w.c_nee[s] = f4(o.c_nee);
-            w.c_spec[s] = f4(o.c_spec);
-            w.c_diff[s] = f4(o.c_diff);
-            w.ext_fp[s] = f4(o.ext_f, o.ext_pdf);
-            w.ext_cos[s] = o.ext_cos;
-            w.ray_o[s] = f4(o.ext_o);
-            w.ray_d[s] = f4(o.ext_d);
+            w.shd[s] = SlotShade{o.c_nee.x, o.c_nee.y, o.c_nee.z, o.ext_pdf, o.ext_f.x, o.ext_f.y, o.ext_f.z, o.ext_cos};
+            if (KIND == FF_MAT_MIX || KIND == FF_MAT_DIELECTRIC)   // the kinds with BSDF-sampled light terms
+                w.mis[s] = SlotMis{o.c_spec.x, o.c_spec.y, o.c_spec.z, 0.f, o.c_diff.x, o.c_diff.y, o.c_diff.z, 0.f};
             if (ADJ && w.pass[s] != 0u) {
                 uint32_t flags = 0;
                 if (KIND == FF_MAT_DIFFUSE && w.grad_tex && mm.base_color_tex >= 0 && mm.base_color_tex == w.adj_texture)
@@ -516,18 +558,21 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
         const uint32_t q2 = warp_append(&w.ctr[C_SH], o.ray_diff, &w.totals[1]);
         if (o.ray_nee) {
             w.sh_rays[q0] = o.r_nee;
-            w.sh_tag[q0] = 4u * s;
+            w.sh_tag[q0] = vis_byte(s, 0);
         }
         if (o.ray_spec) {
             w.sh_rays[q1] = o.r_spec;
-            w.sh_tag[q1] = 4u * s + 1u;
+            w.sh_tag[q1] = vis_byte(s, 1);
         }
         if (o.ray_diff) {
             w.sh_rays[q2] = o.r_diff;
-            w.sh_tag[q2] = 4u * s + 2u;
+            w.sh_tag[q2] = vis_byte(s, 2);
         }
-        if (valid)
-            w.vis[s] = ((o.ray_nee ? 1u : 0u) | (o.ray_spec ? 2u : 0u) | (o.ray_diff ? 4u : 0u)) << 24;
+        if (valid) {
+            // the continuation ray and the queued-rays byte, one whole record
+            const uint32_t queued = ((o.ray_nee ? 1u : 0u) | (o.ray_spec ? 2u : 0u) | (o.ray_diff ? 4u : 0u)) << 24;
+            w.ray[s] = SlotRay{o.ext_o.x, o.ext_o.y, o.ext_o.z, queued, o.ext_d.x, o.ext_d.y, o.ext_d.z, 0.f};
+        }
     }
 }
 
@@ -544,7 +589,7 @@ __global__ void k_init(WF w, uint32_t spp, uint32_t sample_offset)
     w.acc[s] = make_float4(0.f, 0.f, 0.f, 0.f);
     w.acc_c[s] = make_float4(0.f, 0.f, 0.f, 0.f);
     w.cnt[s] = 0;
-    w.vis[s] = 0u;
+    w.ray[s].vis = 0u;
 }
 
 // Film += the m slot sums of each pixel, in slot order (compensated).
@@ -627,10 +672,10 @@ T* carve(char*& p, size_t n)
     return r;
 }
 
-template <int K, bool SEL, bool ADJ>
+template <int K, bool SEL, bool ADJ, bool CORR>
 void shade_kind(const WF& w, int blocks, cudaStream_t stream)
 {
-    k_shade<K, SEL, ADJ><<<blocks, 128, 0, stream>>>(w);
+    k_shade<K, SEL, ADJ, CORR><<<blocks, 128, 0, stream>>>(w);
 }
 
 // k_shade for every material kind in use.  With ws, the first kind runs on
@@ -638,16 +683,16 @@ void shade_kind(const WF& w, int blocks, cudaStream_t stream)
 // work already on `stream` (k_logic); `stream` then waits for all of them.
 // The kinds shade disjoint slots and append to the queues with atomics, so
 // the order of their launches does not change any result.
-template <bool SEL, bool ADJ>
+template <bool SEL, bool ADJ, bool CORR>
 void launch_shade(const WF& w, const bool* kind_used, int blocks, cudaStream_t stream, FFWavefrontWS* ws)
 {
     using Fn = void (*)(const WF&, int, cudaStream_t);
     Fn fns[kKinds];
-    fns[FF_MAT_MIX] = shade_kind<FF_MAT_MIX, SEL, ADJ>;
-    fns[FF_MAT_DIFFUSE] = shade_kind<FF_MAT_DIFFUSE, SEL, ADJ>;
-    fns[FF_MAT_CONDUCTOR] = shade_kind<FF_MAT_CONDUCTOR, SEL, ADJ>;
-    fns[FF_MAT_DIELECTRIC] = shade_kind<FF_MAT_DIELECTRIC, SEL, ADJ>;
-    fns[FF_MAT_COAT] = shade_kind<FF_MAT_COAT, SEL, ADJ>;
+    fns[FF_MAT_MIX] = shade_kind<FF_MAT_MIX, SEL, ADJ, CORR>;
+    fns[FF_MAT_DIFFUSE] = shade_kind<FF_MAT_DIFFUSE, SEL, ADJ, CORR>;
+    fns[FF_MAT_CONDUCTOR] = shade_kind<FF_MAT_CONDUCTOR, SEL, ADJ, CORR>;
+    fns[FF_MAT_DIELECTRIC] = shade_kind<FF_MAT_DIELECTRIC, SEL, ADJ, CORR>;
+    fns[FF_MAT_COAT] = shade_kind<FF_MAT_COAT, SEL, ADJ, CORR>;
     int n_side = 0;
     bool first = true;
     if (ws) FF_CUDA_CHECK(cudaEventRecord(ws->fork, stream));
@@ -672,9 +717,8 @@ size_t ws_bytes(uint32_t P)
     size_t b = 0;
     auto add = [&](size_t s, size_t n) { b += (s * n + 255) & ~size_t(255); };
     add(4, P) /*samples_left*/; add(4, P); add(4, P); add(4, P); add(4, P);
-    add(16, P) /*beta*/; add(16, P); add(16, P); add(4, P) /*vis*/;
-    add(16, P); add(16, P); add(16, P); add(16, P); add(4, P);
-    add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(16, P); add(4, P); add(8, P);
+    add(16, P) /*beta*/; add(sizeof(SlotRay), P); add(sizeof(SlotShade), P); add(sizeof(SlotMis), P);
+    add(sizeof(SlotVtx), P); add(16, P) /*hit_ngeo*/; add(16, P); add(16, P) /*acc, acc_c*/; add(4, P) /*cnt*/;
     add(sizeof(ff_ray), P); add(4, P); add(sizeof(ff_hit), P); add(sizeof(ff_ray), 3ull * P); add(4, 3ull * P);
     add(4, (size_t)kKinds * P); add(4, 64); add(8, 8); add(4, 4); add(8, 4);
     return b;
@@ -694,23 +738,14 @@ void ws_setup(FFWavefrontWS* ws, uint32_t P)
     w.length = carve<uint32_t>(p, P);
     w.phase = carve<uint32_t>(p, P);
     w.beta = carve<float4>(p, P);
-    w.ray_o = carve<float4>(p, P);
-    w.ray_d = carve<float4>(p, P);
-    w.vis = carve<uint32_t>(p, P);
-    w.c_nee = carve<float4>(p, P);
-    w.c_spec = carve<float4>(p, P);
-    w.c_diff = carve<float4>(p, P);
-    w.ext_fp = carve<float4>(p, P);
-    w.ext_cos = carve<float>(p, P);
-    w.hit_pos = carve<float4>(p, P);
-    w.hit_nrm = carve<float4>(p, P);
+    w.ray = carve<SlotRay>(p, P);
+    w.shd = carve<SlotShade>(p, P);
+    w.mis = carve<SlotMis>(p, P);
+    w.vtx = carve<SlotVtx>(p, P);
     w.hit_ngeo = carve<float4>(p, P);
-    w.light_wi = carve<float4>(p, P);
-    w.light_sp = carve<float4>(p, P);
     w.acc = carve<float4>(p, P);
     w.acc_c = carve<float4>(p, P);
     w.cnt = carve<uint32_t>(p, P);
-    w.hit_uv = carve<float2>(p, P);
     w.ext_rays = carve<ff_ray>(p, P);
     w.ext_tag = carve<uint32_t>(p, P);
     w.ext_hits = carve<ff_hit>(p, P);
@@ -737,7 +772,9 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     const uint32_t WH = film->width * film->height;
     const uint64_t target = st->max_paths ? st->max_paths : kDefaultPoolTarget;
     uint32_t m = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(st->spp, target / WH));
-    while ((uint64_t)m * WH > (1ull << 30)) --m;   // shadow-ray tags are 4 * slot + k (uint32)
+    // shadow-ray tags are byte offsets into the SlotRay array (uint32): 32 * slot + 15 at most
+    FF_REQUIRE((uint64_t)WH < (1ull << 27), "film too large for the path pool (at most 2^27 - 1 pixels)");
+    while (m > 1 && (uint64_t)m * WH >= (1ull << 27)) --m;
     const uint32_t P = m * WH;
     if (!film->ws) film->ws = new FFWavefrontWS();
     FFWavefrontWS* ws = film->ws;
@@ -812,10 +849,12 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
             k_logic<false><<<(P + 255) / 256, 256, 0, stream>>>(w);
             mark();
             // with stage timing (profile) every launch stays on the one stream
-            if (w.lights.light == FF_LIGHT_ALL)
-                launch_shade<true, false>(w, kind_used, shade_blocks, stream, profile ? nullptr : ws);
-            else
-                launch_shade<false, false>(w, kind_used, shade_blocks, stream, profile ? nullptr : ws);
+            FFWavefrontWS* side = profile ? nullptr : ws;
+            const bool sel = w.lights.light == FF_LIGHT_ALL, corr = w.mode == FF_MODE_CORRECTED;
+            // light selection needs the corrected mode (checked above)
+            if (sel) launch_shade<true, false, true>(w, kind_used, shade_blocks, stream, side);
+            else if (corr) launch_shade<false, false, true>(w, kind_used, shade_blocks, stream, side);
+            else launch_shade<false, false, false>(w, kind_used, shade_blocks, stream, side);
             FF_CUDA_CHECK(cudaGetLastError());
             mark();
             if (profile) {
@@ -824,7 +863,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
                                       ws->err, w.ext_tag, nullptr, nullptr, scene->refracts);
                 mark();
                 ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
-                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis));
+                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.ray));
                 mark();
             } else {
                 // the traces are independent (hits by slot, answers by shadow-ray tag)
@@ -833,7 +872,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
                 ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
                                       ws->err, w.ext_tag, nullptr, nullptr, scene->refracts);
                 ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
-                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis),
+                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.ray),
                                       ws->side);
                 FF_CUDA_CHECK(cudaEventRecord(ws->join, ws->side));
                 FF_CUDA_CHECK(cudaStreamWaitEvent(stream, ws->join, 0));
@@ -933,7 +972,9 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
     const uint32_t WH = t.width * t.height;
     const uint64_t target = st->max_paths ? st->max_paths : kDefaultPoolTarget;
     uint32_t m = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(st->spp, target / WH));
-    while ((uint64_t)m * WH > (1ull << 30)) --m;   // shadow-ray tags are 4 * slot + k (uint32)
+    // shadow-ray tags are byte offsets into the SlotRay array (uint32): 32 * slot + 15 at most
+    FF_REQUIRE((uint64_t)WH < (1ull << 27), "film too large for the path pool (at most 2^27 - 1 pixels)");
+    while (m > 1 && (uint64_t)m * WH >= (1ull << 27)) --m;
     const uint32_t P = m * WH;
     if (!ctx->adj_ws) ctx->adj_ws = new FFWavefrontWS();
     FFWavefrontWS* ws = ctx->adj_ws;
@@ -1011,7 +1052,7 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
             k_logic<true><<<(P + 255) / 256, 256, 0, stream>>>(w);
             mark();
             // side streams as in ff_wavefront_render (one stream under stage timing)
-            launch_shade<false, true>(w, kind_used, shade_blocks, stream, profile ? nullptr : ws);
+            launch_shade<false, true, true>(w, kind_used, shade_blocks, stream, profile ? nullptr : ws);
             FF_CUDA_CHECK(cudaGetLastError());
             mark();
             if (profile) {
@@ -1019,7 +1060,7 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
                                       ws->err, w.ext_tag, nullptr, nullptr, scene->refracts);
                 mark();
                 ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
-                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis));
+                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.ray));
                 mark();
             } else {
                 FF_CUDA_CHECK(cudaEventRecord(ws->fork, stream));
@@ -1027,7 +1068,7 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
                 ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
                                       ws->err, w.ext_tag, nullptr, nullptr, scene->refracts);
                 ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
-                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.vis),
+                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.ray),
                                       ws->side);
                 FF_CUDA_CHECK(cudaEventRecord(ws->join, ws->side));
                 FF_CUDA_CHECK(cudaStreamWaitEvent(stream, ws->join, 0));

@@ -197,6 +197,69 @@ static float brdf_pdf(const surf_t* m, v3 n, v3 wi, v3 wo)
     return (float)(0.5 * (double)(sp + dp));
 }
 
+/* FP32 lobes of the corrected mode (the product's Lobes<true>,
+ * firefly_b200/csrc/ff_shade.cuh): the same formulas and operand order with
+ * every intermediate in float; the GGX sample takes cos and sin of theta
+ * from tan(theta) = r^2 sqrt(e0 / (1 - e0)).  Parity mode keeps the
+ * reference's FP64 (the functions above). */
+static float ggx_ndf32(v3 n, v3 h, float r)
+{
+    float a2 = r * r * r * r;
+    float nh = hmax(0.f, dot(n, h));
+    float k = (nh * nh) * (a2 - 1.f) + 1.f;
+    return a2 / (PI_F * (k * k));
+}
+static float geo_atten32(v3 wi, v3 wo, v3 n, float r)
+{
+    float rp = r + 1.f;
+    float k = (rp * rp) / 8.f;
+    float nl = hmax(dot(n, wi), 0.f), nv = hmax(dot(n, wo), 0.f);
+    return (nl / (nl * (1.f - k) + k)) * (nv / (nv * (1.f - k) + k));
+}
+static v3 fresnel32(v3 f0, v3 h, v3 wo)
+{
+    float x = 1.f - hmax(0.f, dot(h, wo));
+    float x2 = x * x;
+    float p = (x2 * x2) * x;
+    return add(f0, muls(ssub(1.f, f0), p));
+}
+static float spec_get_pdf32(v3 n, v3 wi, v3 wo, float r)
+{
+    v3 wh = normalize(add(wo, wi));
+    float whn = hmax(dot(wh, n), 0.f), wowh = hmax(dot(wo, wh), 0.f);
+    return (ggx_ndf32(n, wh, r) * whn) / hmax(4.f * wowh, 0.001f);
+}
+static v3 spec_f32(const surf_t* mat, v3 n, v3 wi, v3 wo)
+{
+    float r = mat->roughness;
+    v3 f0 = f0_of(mat, mat->albedo);
+    v3 wh = normalize(add(wo, wi));
+    float ndwi = hmax(dot(n, wi), 0.f), ndwo = hmax(dot(n, wo), 0.f);
+    v3 F = fresnel32(f0, wh, wi);
+    v3 num = smul(ggx_ndf32(n, wh, r) * geo_atten32(wi, wo, n, r), F);
+    return divs(num, hmax((4.f * ndwo) * ndwi, 0.001f));
+}
+static v3 diff_f32(const surf_t* mat, v3 wi, v3 wo)
+{
+    v3 a = mat->albedo;
+    v3 wh = normalize(add(wo, wi));
+    v3 kd = sub(V(1.f, 1.f, 1.f), fresnel32(f0_of(mat, a), wh, wi));
+    kd = muls(kd, 1.f - mat->metallic);
+    return muls(mul(kd, a), INV_PI_F);
+}
+static v3 spec_sample32(v3 N, v3 wo, float r, float e0, float e1)
+{
+    float t = (r * r) * sqrtf(e0 / (1.f - e0));   /* e0 = 1: t = inf, theta = pi / 2 */
+    float ct = 1.f / sqrtf(1.f + t * t);
+    float st = isinf(t) ? 1.f : t * ct;
+    float phi = TWO_PI_F * e1;
+    v3 T, B;
+    frame(N, &T, &B);
+    v3 s = add(add(muls(T, st * cosf(phi)), muls(N, ct)), muls(B, st * sinf(phi)));
+    return neg(reflect(wo, normalize(s)));
+}
+static float diff_pdf32(void) { return 1.f / (2.f * PI_F); }
+
 /* ------------------------------------------------------------- lights */
 /* luminance (dMath.cuh:1503-1507): double arithmetic, float result */
 static float luminance(v3 c) { return (float)(0.299 * (double)c.x + 0.587 * (double)c.y + 0.114 * (double)c.z); }
@@ -514,6 +577,77 @@ static void shade_mix(const light_ctx* lc, int corrected, const surf_t* mat, v3 
     o->ext_cos = hmax(0.f, dot(n, dir));
 }
 
+/* shade_mix in corrected mode: the FP32 lobes (the product's shade_mix<true>). */
+static float power_heuristic32(float f, float g)
+{
+    float f2 = f * f;
+    return f2 / (f2 + g * g);
+}
+static void shade_mix32(const light_ctx* lc, const surf_t* mat, v3 pos, v3 n, v3 wo, v3 wi, uint32_t key,
+                        uint32_t L, shade_t* o)
+{
+    float r = mat->roughness;
+    v3 Lsum = V(0, 0, 0);
+    v3 Li = light_L(lc, wi);
+    float ndwi = dot(n, wi);
+    if (ndwi > 0.f) {
+        float dp = diff_pdf32();
+        float sp = spec_get_pdf32(n, wi, wo, r);
+        float lp = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
+        if (lp > 0.f && !iszero(Li)) {
+            float dw = lc->is_dir ? 1.f : power_heuristic32(lp, dp), sw = lc->is_dir ? 1.f : power_heuristic32(lp, sp);
+            v3 f = muls(spec_f32(mat, n, wi, wo), ndwi);
+            if (!iszero(f)) Lsum = add(Lsum, divs(mul(muls(f, sw), Li), lp));
+            f = muls(diff_f32(mat, wi, wo), ndwi);
+            if (!iszero(f)) Lsum = add(Lsum, divs(mul(muls(f, dw), Li), lp));
+        }
+    }
+    o->c_nee = Lsum;
+    v3 wi_spec = spec_sample32(n, wo, r, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1));
+    v3 wi_diff = diff_sample(n, R(key, L, DIM_DIFF), R(key, L, DIM_DIFF + 1));
+    o->has_spec = o->has_diff = 0;
+    if (!lc->is_dir) {
+        v3 org = add(pos, muls(wi_spec, 0.001f));
+        float nd = dot(n, wi_spec);
+        ray_t vr;
+        if (nd > 0.f && light_vis_ray(lc, org, wi_spec, key, L, DIM_SPEC_VIS, &vr)) {
+            float sp = spec_get_pdf32(n, wi_spec, wo, r);
+            float lp = light_pdf(lc, pos, wi_spec, key, L, DIM_SPEC_PDF);
+            float w = power_heuristic32(sp, lp);
+            v3 f = muls(spec_f32(mat, n, wi_spec, wo), nd);
+            v3 Li2 = light_L(lc, wi_spec);
+            if (!iszero(f) && sp > 0.f && !iszero(Li2)) {
+                o->c_spec = divs(muls(mul(f, Li2), w), sp);
+                o->has_spec = 1;
+                o->r_spec = vr;
+            }
+        }
+    }
+    if (!lc->is_dir) {
+        v3 org = add(pos, muls(wi_diff, 0.001f));
+        float nd = dot(n, wi_diff);
+        ray_t vr;
+        if (nd > 0.f && light_vis_ray(lc, org, wi_diff, key, L, DIM_DIFF_VIS, &vr)) {
+            float dp = diff_pdf32();
+            float lp = light_pdf(lc, pos, wi_diff, key, L, DIM_DIFF_PDF);
+            float w = power_heuristic32(dp, lp);
+            v3 f = muls(diff_f32(mat, wi_diff, wo), nd);
+            v3 Li2 = light_L(lc, wi_diff);
+            if (!iszero(f) && dp > 0.f && !iszero(Li2)) {
+                o->c_diff = divs(muls(mul(f, Li2), w), dp);
+                o->has_diff = 1;
+                o->r_diff = vr;
+            }
+        }
+    }
+    v3 dir = R(key, L, DIM_LOBE) < 0.5f ? wi_diff : wi_spec;
+    o->ext_d = dir;
+    v3 fs = spec_f32(mat, n, dir, wo);
+    o->ext_f = add(fs, diff_f32(mat, dir, wo));
+    o->ext_pdf = 0.5f * (spec_get_pdf32(n, dir, wo, r) + diff_pdf32());
+    o->ext_cos = hmax(0.f, dot(n, dir));
+}
+
 static void shade_diffuse(const light_ctx* lc, int corrected, const surf_t* mat, v3 pos, v3 n, v3 wo, v3 wi,
                           uint32_t key, uint32_t L, shade_t* o)
 {
@@ -522,13 +656,13 @@ static void shade_diffuse(const light_ctx* lc, int corrected, const surf_t* mat,
         float nd = dot(n, wi);
         float lp = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
         v3 Li = light_L(lc, wi);
-        if (nd > 0.f && lp > 0.f) o->c_nee = divs(mul(muls(diff_f(mat, wi, wo), nd), Li), lp);
+        if (nd > 0.f && lp > 0.f) o->c_nee = divs(mul(muls(diff_f32(mat, wi, wo), nd), Li), lp);
     }
     o->has_spec = o->has_diff = 0;
     v3 dir = diff_sample(n, R(key, L, DIM_DIFF), R(key, L, DIM_DIFF + 1));
     o->ext_d = dir;
-    o->ext_f = diff_f(mat, dir, wo);
-    o->ext_pdf = (float)diff_get_pdf();
+    o->ext_f = corrected ? diff_f32(mat, dir, wo) : diff_f(mat, dir, wo);
+    o->ext_pdf = corrected ? diff_pdf32() : (float)diff_get_pdf();
     o->ext_cos = hmax(0.f, dot(n, dir));
 }
 
@@ -540,14 +674,15 @@ static void shade_conductor(const light_ctx* lc, int corrected, const surf_t* ma
         float nd = dot(n, wi);
         float lp = light_pdf(lc, pos, wi, key, L, DIM_NEE_PDF);
         v3 Li = light_L(lc, wi);
-        if (nd > 0.f && lp > 0.f) o->c_nee = divs(mul(muls(spec_f(mat, n, wi, wo), nd), Li), lp);
+        if (nd > 0.f && lp > 0.f) o->c_nee = divs(mul(muls(spec_f32(mat, n, wi, wo), nd), Li), lp);
     }
     o->has_spec = o->has_diff = 0;
     float r = mat->roughness;
-    v3 dir = spec_sample(n, wo, r, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1));
+    v3 dir = corrected ? spec_sample32(n, wo, r, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1))
+                       : spec_sample(n, wo, r, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1));
     o->ext_d = dir;
-    o->ext_f = spec_f(mat, n, dir, wo);
-    o->ext_pdf = spec_get_pdf(n, dir, wo, r);
+    o->ext_f = corrected ? spec_f32(mat, n, dir, wo) : spec_f(mat, n, dir, wo);
+    o->ext_pdf = corrected ? spec_get_pdf32(n, dir, wo, r) : spec_get_pdf(n, dir, wo, r);
     o->ext_cos = hmax(0.f, dot(n, dir));
 }
 
@@ -645,9 +780,9 @@ static void diel_eval(const diel_t* d, v3 n, v3 wo, v3 wi, v3* f, float* pdf)
 }
 static v3 ggx_sample_normal(v3 n, float alpha, float e0, float e1)
 {
-    float t2 = (alpha * alpha) * (e0 / (1.f - e0));
+    float t2 = (alpha * alpha) * (e0 / (1.f - e0));   /* e0 = 1: t2 = inf, theta = pi / 2 */
     float ct = 1.f / sqrtf(1.f + t2);
-    float st = sqrtf(t2) * ct;
+    float st = isinf(t2) ? 1.f : sqrtf(t2) * ct;
     float phi = TWO_PI_F * e1;
     v3 T, B;
     frame(n, &T, &B);
@@ -737,7 +872,7 @@ static v3 coat_spec_f(const surf_t* mat, v3 n, v3 wi, v3 wo, float r0)
     c.fresnel = V(r0, r0, r0);
     c.albedo = V(1.f, 1.f, 1.f);
     c.metallic = 0.f;
-    return spec_f(&c, n, wi, wo);
+    return spec_f32(&c, n, wi, wo);
 }
 static v3 coat_f(const surf_t* mat, v3 n, v3 wi, v3 wo, float r0)
 {
@@ -763,7 +898,7 @@ static void shade_coat(const light_ctx* lc, const surf_t* mat, v3 pos, v3 n, v3 
     float r = mat->roughness;
     v3 dir;
     if (R(key, L, DIM_LOBE) < 0.5f) {
-        dir = spec_sample(n, wo, r, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1));
+        dir = spec_sample32(n, wo, r, R(key, L, DIM_SPEC), R(key, L, DIM_SPEC + 1));
     } else {
         v2 u = {R(key, L, DIM_DIFF), R(key, L, DIM_DIFF + 1)};
         v2 dsk = concentric_disk(u);
@@ -775,7 +910,7 @@ static void shade_coat(const light_ctx* lc, const surf_t* mat, v3 pos, v3 n, v3 
     float c = hmax(0.f, dot(n, dir));
     o->ext_d = dir;
     o->ext_f = coat_f(mat, n, dir, wo, r0);
-    o->ext_pdf = 0.5f * spec_get_pdf(n, dir, wo, r) + 0.5f * c * INV_PI_F;
+    o->ext_pdf = 0.5f * spec_get_pdf32(n, dir, wo, r) + 0.5f * c * INV_PI_F;
     o->ext_cos = c;
 }
 
@@ -996,7 +1131,10 @@ static void path_sample(const ffo_render_desc* d, const light_ctx* lc_base, int 
         v3 wo = neg(dir);
         memset(&sh, 0, sizeof(sh));
         const int diel = mat->kind == 3;
-        if (mat->kind == 0) shade_mix(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
+        if (mat->kind == 0) {
+            if (corrected) shade_mix32(lc, mat, pos, n, wo, wi, key, L, &sh);
+            else shade_mix(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
+        }
         else if (mat->kind == 1) shade_diffuse(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
         else if (mat->kind == 2) shade_conductor(lc, corrected, mat, pos, n, wo, wi, key, L, &sh);
         else if (diel) shade_dielectric(lc, mat, pos, n, wo, wi, key, L, back, &sh);
@@ -1269,5 +1407,5 @@ void ffo_probe_coat(const float* mat5, const float* n3, const float* wi3, const 
     v3 n = ld3(n3), wi = ld3(wi3), wo = ld3(wo3);
     st3(out4, coat_f(&m, n, wi, wo, r0));
     float c = hmax(0.f, dot(n, wi));
-    out4[3] = 0.5f * spec_get_pdf(n, wi, wo, m.roughness) + 0.5f * c * INV_PI_F;
+    out4[3] = 0.5f * spec_get_pdf32(n, wi, wo, m.roughness) + 0.5f * c * INV_PI_F;
 }

@@ -243,7 +243,7 @@ def test_two_sided_closest(room, oracle):
     the culling trace's answer for the same ray."""
     scn, ds = room
     P = np.asarray(scn.positions, np.float64)
-    sphere = P[24:]
+    sphere = P[np.unique(np.asarray(scn.indices)[np.asarray(scn.material_ids) == 1])]
     c = sphere.mean(0)
     rad = float(np.linalg.norm(sphere - c, axis=1).max())
     rng = np.random.default_rng(41)
