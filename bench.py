@@ -55,6 +55,8 @@ RENDER_WORKLOAD = ("wavefront path tracer at scale: displaced icosphere 1,310,72
 TRACE_WORKLOAD = "trace micro: small room 4120 tris, 16M coherent + 16M incoherent rays, closest + any-hit"
 RAYS_PER_SET = 4096 * 4096
 RAY_BYTES, HIT_BYTES = 32, 16
+# The traversal's records: an 8-wide quantized node (80 B), a triangle (48 B).
+NODE_BYTES, TRI_BYTES = 80, 48
 # The wavefront's traces read a tagged queue (32 B ray + 4 B tag): the
 # closest-hit trace writes a 16 B hit, the any-hit trace a 1 B answer.
 WF_CLOSEST_BYTES, WF_ANY_BYTES = 32 + 4 + 16, 32 + 4 + 1
@@ -62,31 +64,31 @@ WF_CLOSEST_BYTES, WF_ANY_BYTES = 32 + 4 + 16, 32 + 4 + 1
 # reads phase, key, ext_q, length, pass (20 B), the extension hit (16), ray
 # origin and direction (32), throughput (16), radiance sum (16), shadow-queue
 # indices (16) and ~1.5 shadow hits (24), the three light terms (48), ext_f /
-# pdf / cos (20), the triangle's shading record (76); writes the sum (16) and
+# pdf / cos (20), the triangle's shading record (64); writes the sum (16) and
 # the next vertex (uv, length, throughput, position, normal, light sample,
 # queue entry: 112).  The replay pass adds dL/dI (12), L_s (16) and the
 # vertex record (albedo + flags, uv, env coefficient, light direction: 56).
-# Primal ~410 B, replay ~490 B: 450 B on average.
-ADJ_LOGIC_BYTES_PER_HIT = 450
+# Primal ~398 B, replay ~478 B: 438 B on average.
+ADJ_LOGIC_BYTES_PER_HIT = 438
 # k_logic in ff_render, per consumed extension hit of a continuing path:
-# reads 296 B (slot words 16, hit 16, ray 32, throughput 16, sum and
-# compensation 32, shadow-queue indices 16 and ~1.5 shadow hits 24, light
-# terms 48, ext_f / pdf / cos 20, shading record 76), writes 144 B (sum and
-# compensation 32, next vertex 112).
-RENDER_LOGIC_BYTES_PER_HIT = 440
-# k_shade, per shaded vertex: reads the vertex (position, uv, normal,
-# direction, light sample, key, depth, queue entry: 100 B), writes the light
-# terms (48), ext_f / pdf / cos (20), the continuation ray into the slot (32)
-# and the extension queue (36), ~2.5 shadow rays (80) and their queue
-# indices (16): 332 B.  Environment and material lookups are L2 gathers and
-# not counted.
-RENDER_SHADE_BYTES_PER_VERTEX = 332
+# reads the slot words (12 B), the hit (16), the ray record (32), throughput,
+# sum and compensation (48), the shading record (32) and the triangle's
+# shading attributes (64); writes sum, compensation, length and throughput
+# (52) and the vertex record (64): 320 B.
+RENDER_LOGIC_BYTES_PER_HIT = 320
+# k_shade, per shaded vertex: reads the vertex record (64 B) and its queue
+# entry (4), writes the shading record (32), the ray record (32) and the
+# extension-queue entry (36): 168 B; plus 36 B per shadow-queue entry (32 B
+# ray, 4 B tag).  Environment and material lookups are L2 gathers and not
+# counted; the mix and dielectric kinds add a 32-B record not counted either.
+RENDER_SHADE_BYTES_PER_VERTEX = 168
+SHADOW_QUEUE_BYTES = 36
 # Measured DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per unit
-# of each render stage: ncu over every launch of one timed 16-spp C2 step
-# (the 8.3M-slot pool of the 64-spp step; 36 frames), divided by the step's
-# units (consumed hits, shaded vertices, extension rays, shadow rays).
-RENDER_DRAM_BYTES_PER_UNIT = {"k_logic": 448.4, "k_shade (all kinds)": 599.1,
-                              "k_trace<closest> (extension queue)": 106.0, "k_trace<any> (shadow queue)": 51.2}
+# of each render stage: ncu over every launch of one timed 16-spp C2 step on
+# a 2,097,152-slot pool (104 frames), divided by the step's units (consumed
+# hits, shaded vertices, extension rays, shadow rays).
+RENDER_DRAM_BYTES_PER_UNIT = {"k_logic": 339.0, "k_shade (all kinds)": 351.7,
+                              "k_trace<closest> (extension queue)": 117.2, "k_trace<any> (shadow queue)": 75.9}
 RENDER = dict(width=1920, height=1080, spp=64, max_depth=8, rr_depth=3)
 # Measured DRAM bytes per unit of the adjoint's stages (ncu over the profiled
 # 512x512, 16-spp adjoint call of --workload inverse, 12 frames): per
@@ -708,9 +710,10 @@ def run_render(args, ws, rank, local, dist):
                                                         "hit out)"),
                  "k_logic": (prof["ms_logic"], prof["extension_rays"] * RENDER_LOGIC_BYTES_PER_HIT,
                              f"{RENDER_LOGIC_BYTES_PER_HIT} B of slot state per consumed extension hit"),
-                 "k_shade (all kinds)": (prof["ms_shade"], vertices * RENDER_SHADE_BYTES_PER_VERTEX,
-                                         f"{RENDER_SHADE_BYTES_PER_VERTEX} B of slot state and queue entries per "
-                                         "shaded vertex")}
+                 "k_shade (all kinds)": (prof["ms_shade"], vertices * RENDER_SHADE_BYTES_PER_VERTEX
+                                         + prof["shadow_rays"] * SHADOW_QUEUE_BYTES,
+                                         f"{RENDER_SHADE_BYTES_PER_VERTEX} B of slot records and queue entries per "
+                                         f"shaded vertex + {SHADOW_QUEUE_BYTES} B per shadow-queue entry")}
         dom = max(stage, key=lambda k: stage[k][0])
         dms, dbytes, dnote = stage[dom]
         achieved = dbytes / (dms / 1e3) / 1e9
@@ -729,6 +732,34 @@ def run_render(args, ws, rank, local, dist):
                 cpu = {"value": round(r[0], 3), "unit": "Mrays/s", "cores": os.cpu_count() or 1, "kind": r[1],
                        "sample": r[2]}
         pstat = {k: round(prof[k], 2) for k in ("ms_total", "ms_logic", "ms_shade", "ms_trace_extension", "ms_trace_shadow")}
+        # the traces' node and triangle fetches (counted by a second pass of the
+        # same traversal over each frame's queues in the profiled step) against
+        # an L2-resident read: the traversal reads a 0.27 GB scene mostly from
+        # L2, so this and the issue rate bound it rather than DRAM
+        try:
+            l2_ref = l2_read_gbs(dev)
+        except Exception as e:   # the reference bandwidth is optional
+            print(f"l2 read probe unavailable: {e}", file=sys.stderr)
+            l2_ref = None
+        l2_fetch = {}
+        for name, ms_k, rays_k, nodes_k, tris_k in (
+                ("k_trace<closest> (extension queue)", prof["ms_trace_extension"], prof["extension_rays"],
+                 prof["ext_nodes"], prof["ext_tris"]),
+                ("k_trace<any> (shadow queue)", prof["ms_trace_shadow"], prof["shadow_rays"],
+                 prof["shadow_nodes"], prof["shadow_tris"])):
+            fb = nodes_k * NODE_BYTES + tris_k * TRI_BYTES
+            gbs = fb / (ms_k / 1e3) / 1e9 if ms_k > 0 else None
+            l2_fetch[name] = {"nodes_per_ray": round(nodes_k / max(1, rays_k), 3),
+                              "tris_per_ray": round(tris_k / max(1, rays_k), 3),
+                              "fetch_bytes_per_ray": round(fb / max(1, rays_k), 1),
+                              "achieved_fetch_gbs": None if gbs is None else round(gbs, 1),
+                              "frac_of_l2_read": None if (gbs is None or l2_ref is None) else round(gbs / l2_ref, 4)}
+        l2_fetch = {"stages": l2_fetch, "l2_read_gbs": None if l2_ref is None else round(l2_ref, 1),
+                    "node_bytes": NODE_BYTES, "tri_bytes": TRI_BYTES,
+                    "note": ("fetched bytes = 8-wide node records x node bytes + triangles tested x triangle bytes, "
+                             "counted over the profiled step's queues; l2_read_gbs = a probe kernel reading a 32 MiB "
+                             "L2-resident buffer 40 times (L1 bypassed); part of the fetches hit L1, so the fraction "
+                             "is an upper bound on the L2 load")}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
@@ -749,12 +780,13 @@ def run_render(args, ws, rank, local, dist):
                          "frac": round(achieved / peak, 5), "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes": dnote, "algorithmic_bytes_per_launch": alg_launch,
                          "traffic_note": ("bytes per frame's launch sequence of the dominant stage: ncu DRAM bytes "
-                                          "per unit of a 16-spp step on the same pool x this step's units per frame"),
+                                          "per unit of a 16-spp step on a 2M-slot pool x this step's units per frame"),
                          "stages": {k: {"ms": round(v[0], 2), "achieved_gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1)
                                         if v[0] > 0 else None,
                                         "algorithmic_bytes_per_unit": round(v[1] / max(1, units[k]), 1),
                                         "dram_bytes_per_unit": RENDER_DRAM_BYTES_PER_UNIT[k]}
-                                    for k, v in stage.items()}},
+                                    for k, v in stage.items()},
+                         "l2_fetch": l2_fetch},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 80,
                     "d2h_bytes_per_step": int(W * H * (16 + 4))},
@@ -841,7 +873,7 @@ def small_room_line(args, ws, rank, local, dist, ctx, dev, stream, steps=20, war
                                                          prof["extension_rays"] * WF_CLOSEST_BYTES),
                   "k_logic": (prof["ms_logic"], prof["extension_rays"] * RENDER_LOGIC_BYTES_PER_HIT),
                   "k_shade (all kinds)": (prof["ms_shade"], max(0, prof["extension_rays"] - prof["samples"])
-                                          * RENDER_SHADE_BYTES_PER_VERTEX)}
+                                          * RENDER_SHADE_BYTES_PER_VERTEX + prof["shadow_rays"] * SHADOW_QUEUE_BYTES)}
         dom = max(stages, key=lambda n: stages[n][0])
         achieved = stages[dom][1] / (stages[dom][0] / 1e3) / 1e9
         cpu = None

@@ -109,7 +109,8 @@ class ff_render_stats(C.Structure):
                 ("ms_trace_shadow", C.c_float), ("ms_logic", C.c_float), ("ms_shade", C.c_float),
                 ("kernel_launches", C.c_uint32), ("ms_cache_paths", C.c_float), ("ms_cache_train", C.c_float),
                 ("ms_cache_query", C.c_float), ("cache_queries", C.c_uint64), ("cache_records", C.c_uint64),
-                ("grad_atomics", C.c_uint64), ("grad_atomics_roughness", C.c_uint64)]
+                ("grad_atomics", C.c_uint64), ("grad_atomics_roughness", C.c_uint64), ("ext_nodes", C.c_uint64),
+                ("ext_tris", C.c_uint64), ("shadow_nodes", C.c_uint64), ("shadow_tris", C.c_uint64)]
 
 
 class ff_adjoint_desc(C.Structure):

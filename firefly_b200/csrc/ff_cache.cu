@@ -8,7 +8,12 @@
 // accumulator its warp may read (subpartition w % 4).
 //   k_cache_infer  encode -> X (smem) -> 5 MMAs chains (K = 64 in four K=16
 //                  steps) with a ReLU/bf16 epilogue TMEM -> smem between
-//                  layers; activations overwrite the input tile.
+//                  layers; activations overwrite the input tile.  Its CTA
+//                  runs kGroups independent tile pipelines of 4 warps (one
+//                  thread per row, all 64 columns) over one copy of the
+//                  weights: while one group waits on its MMAs the others
+//                  gather hash-grid features, so the encoder's L2 gathers
+//                  overlap the tensor-core chains of the other tiles.
 //   k_cache_train  the same forward keeping every layer's activations, the
 //                  relative-L2 loss gradient, then per layer (top down) the
 //                  weight gradient act^T * delta (M = 64, both operands
@@ -41,10 +46,12 @@ constexpr uint32_t kWBytes = 64u * 128u;                  // one 64 x 64 bf16 we
 constexpr uint32_t kImgBytes = kLayers * kWBytes;         // 40 KB
 constexpr uint32_t kParams = kLayers * kWidth * kWidth;   // FP32 master weights (W4 rows >= 3 stay zero)
 constexpr uint32_t kWaitPolls = 1u << 22;
-constexpr uint32_t kInferSmem = kImgBytes + kTileBytes + 1024 + 64;
+constexpr int kGroups = 3;                                // inference: tile pipelines per CTA
+constexpr int kInferThreads = 128 * kGroups;
+constexpr uint32_t kInferSmem = kImgBytes + kGroups * kTileBytes + 1024 + 64;
 constexpr uint32_t kTrainSmem = kImgBytes + 6 * kTileBytes + 1024 + 64;
 constexpr uint32_t kTrainTmemCols = 512;                  // D (64) + 5 weight-gradient accumulators (5 x 64)
-constexpr uint32_t kInferTmemCols = 64;
+constexpr uint32_t kInferTmemCols = 256;                 // 64 per group, allocated as a power of two
 
 constexpr uint32_t ID_FWD = idesc_bf16(128, 64, false, false);
 constexpr uint32_t ID_OUT = idesc_bf16(128, 16, false, false);
@@ -161,60 +168,85 @@ __device__ __forceinline__ uint8_t* aligned_smem(uint8_t* raw)
     return raw + (((s + 1023u) & ~1023u) - s);
 }
 
-__global__ void __launch_bounds__(kThreads, 3) k_cache_infer(CacheArgs a)
+// Barrier of one group's 128 threads (ids 1..kGroups; 0 is __syncthreads).
+__device__ __forceinline__ void group_sync(uint32_t id)
+{
+    asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory");
+}
+// The same barrier, returning whether any of the group's threads passed p.
+__device__ __forceinline__ bool group_sync_or(uint32_t id, bool p)
+{
+    uint32_t any;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(any)
+        : "r"((uint32_t)p), "r"(id)
+        : "memory");
+    return any != 0;
+}
+
+__global__ void __launch_bounds__(kInferThreads, 2) k_cache_infer(CacheArgs a)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = aligned_smem(smem_raw);
     uint8_t* w_s = base;
-    uint8_t* act = base + kImgBytes;
-    uint64_t* mbar_p = reinterpret_cast<uint64_t*>(act + kTileBytes);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(act + kTileBytes + 16);
+    uint64_t* mbars = reinterpret_cast<uint64_t*>(base + kImgBytes + kGroups * kTileBytes);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbars + kGroups);
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
-    const uint32_t q = warp & 3u, h = warp >> 2, r = 32u * q + lane;
-    const uint32_t mbar = smem_addr(mbar_p);
+    // group g = warps 4g..4g+3; warp 4g+q reads TMEM lanes 32q.. (its subpartition)
+    const uint32_t g = warp >> 2, q = warp & 3u, r = 32u * q + lane;
+    uint8_t* act = base + kImgBytes + g * kTileBytes;
+    const uint32_t mbar = smem_addr(mbars + g), bar = 1u + g;
+    const bool leader = (tid & 127u) == 0;
     const uint32_t n = count_of(a);
     const uint32_t tiles = (n + kTile - 1) / kTile;
-    if (blockIdx.x >= tiles) return;            // block-uniform, before any TMEM is held
+    if (blockIdx.x * kGroups >= tiles) return;  // block-uniform, before any TMEM is held
 
     load_weights(a.w_img, w_s);
-    if (tid == 0) mbar_init(mbar, 1);
+    if (tid < kGroups) mbar_init(smem_addr(mbars + tid), 1);
     __syncwarp();
     if (warp == 0) tmem_alloc(smem_addr(tslot), kInferTmemCols);
     fence_smem_async();
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
-    const uint32_t tmem = *tslot;
+    const uint32_t tmem_all = *tslot;
+    const uint32_t tmem = tmem_all + 64u * g;   // this group's accumulator columns
     const uint32_t trow = tmem_addr(tmem, 32u * q, 0);
     const uint32_t w0 = smem_addr(w_s), x0 = smem_addr(act);
     uint32_t phase = 0;
     bool failed = false;
 
-    for (uint32_t t = blockIdx.x; t < tiles && !failed; t += gridDim.x) {
+    for (uint32_t t = blockIdx.x * kGroups + g; t < tiles && !failed; t += gridDim.x * kGroups) {
         const uint32_t i = t * kTile + r;
         const bool valid = i < n;
         Record rec;
         if (valid) rec = a.recs[i];
-        encode_half(a.grid, rec, valid, h, r, act);
+        encode_half(a.grid, rec, valid, 0, r, act);
+        encode_half(a.grid, rec, valid, 1, r, act);
         fence_smem_async();
         fence_before_sync();
-        __syncthreads();
+        group_sync(bar);
         for (int l = 0; l < kLayers; ++l) {
-            if (tid == 0) {
+            if (leader) {
                 fence_after_sync();
                 issue_forward(tmem, x0, w0 + (uint32_t)l * kWBytes, l + 1 < kLayers ? ID_FWD : ID_OUT);
                 mma_commit(mbar);
             }
             const bool ok = mbar_wait(mbar, phase, a.wait_polls);
             phase ^= 1u;
-            if (__syncthreads_or(!ok)) {
+            if (group_sync_or(bar, !ok)) {
                 failed = true;
                 break;
             }
             fence_after_sync();
             if (l + 1 < kLayers) {
-                relu_epilogue(trow, h, r, act);
-            } else if (h == 0) {
+                relu_epilogue(trow, 0, r, act);
+                relu_epilogue(trow, 1, r, act);
+            } else {
                 float y[16];
                 tmem_ld16(trow, y);
                 if (valid) {
@@ -235,10 +267,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_cache_infer(CacheArgs a)
             }
             fence_smem_async();
             fence_before_sync();
-            __syncthreads();
+            group_sync(bar);
         }
     }
-    if (failed && tid == 0) {
+    if (failed && leader) {
         atomicAdd(a.err, 1u);
         mbar_wait(mbar, phase ^ 1u, kWaitPolls);   // the commit that did not arrive, once more
     }
@@ -246,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_cache_infer(CacheArgs a)
     __syncthreads();
     if (warp == 0) {
         fence_after_sync();
-        tmem_dealloc(tmem, kInferTmemCols);
+        tmem_dealloc(tmem_all, kInferTmemCols);
     }
 }
 
@@ -591,8 +623,8 @@ void ff_cache_launch_infer(ff_cache* c, const void* recs, uint32_t n_max, const 
     a.out_rgb = out_rgb;
     a.frame = frame;
     const uint32_t tiles = (n_max + kTile - 1) / kTile;
-    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)c->ctx->num_sms * 3u);
-    k_cache_infer<<<grid, kThreads, kInferSmem, c->ctx->stream>>>(a);
+    const uint32_t grid = std::min<uint32_t>((tiles + kGroups - 1) / kGroups, (uint32_t)c->ctx->num_sms * 2u);
+    k_cache_infer<<<grid, kInferThreads, kInferSmem, c->ctx->stream>>>(a);
     FF_CUDA_CHECK(cudaGetLastError());
 }
 

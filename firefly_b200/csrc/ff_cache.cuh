@@ -105,16 +105,40 @@ __device__ __forceinline__ void level_corners(const Grid& g, int l, float3 p, Co
     }
 }
 
+// Entry j (0..3) of four packed half2 entries.
+__device__ __forceinline__ uint32_t pick4(uint4 q, uint32_t j)
+{
+    return j == 0u ? q.x : (j == 1u ? q.y : (j == 2u ? q.z : q.w));
+}
+__device__ __forceinline__ float2 half2_bits(uint32_t u)
+{
+    __half2 h;
+    *reinterpret_cast<uint32_t*>(&h) = u;
+    return __half22float2(h);
+}
+
+// Trilinear feature of level l at p.  Corners k (x) and k + 1 (x + 1) share
+// y and z, so their entries usually sit in one aligned group of four: on a
+// dense level they are neighbours, and on a hashed level x enters the hash
+// by XOR, so the two indices differ in the bits of x ^ (x + 1), which stay
+// below 4 three times in four.  The group is one 16-byte load (one sector
+// per lane instead of two); an entry outside it is read alone.  The sum runs
+// over the corners in the same order, so the feature is unchanged.
 __device__ __forceinline__ float2 level_feature(const Grid& g, int l, float3 p)
 {
     Corners c;
     level_corners(g, l, p, c);
     float2 f = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const float2 e = __half22float2(g.table_h[c.idx[k]]);
-        f.x += c.w[k] * e.x;
-        f.y += c.w[k] * e.y;
+    for (int k = 0; k < 8; k += 2) {
+        const uint32_t i0 = c.idx[k], i1 = c.idx[k + 1];
+        const uint4 q = *reinterpret_cast<const uint4*>(g.table_h + (i0 & ~3u));
+        const uint32_t b1 = (i0 ^ i1) < 4u ? pick4(q, i1 & 3u) : *reinterpret_cast<const uint32_t*>(g.table_h + i1);
+        const float2 e0 = half2_bits(pick4(q, i0 & 3u)), e1 = half2_bits(b1);
+        f.x += c.w[k] * e0.x;
+        f.y += c.w[k] * e0.y;
+        f.x += c.w[k + 1] * e1.x;
+        f.y += c.w[k + 1] * e1.y;
     }
     return f;
 }

@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kBlock) k_training_paths(CR a)
             if (terminate) break;
             const bool back = hit_back(hit.prim);   // hit from inside an object
             const uint32_t prim = hit_index(hit.prim);
-            const FFShadeTri& t = a.shade[prim];
+            const FFShadeRec t = ff_load_shade(a.shade, prim);
             const float u = hit.u, v = hit.v;
             // ng: the interpolated normal the ray offsets follow (kernel.cu:437);
             // n: the shading normal (get_normal: a normal texture's frame, else ng);

@@ -26,23 +26,16 @@ __global__ void k_build_shading(const float3* __restrict__ pos, const uint3* __r
     float l2 = rn_dot(c, c);
     float inv = 1.0f / sqrtf(l2);
     float3 fn = make_float3(c.x * inv, c.y * inv, c.z * inv);
+    const float3 n0 = nrm ? nrm[t.x] : fn, n1 = nrm ? nrm[t.y] : fn, n2 = nrm ? nrm[t.z] : fn;
+    const float2 zero = make_float2(0.f, 0.f);
+    const float2 uv0 = uv ? uv[t.x] : zero, uv1 = uv ? uv[t.y] : zero, uv2 = uv ? uv[t.z] : zero;
     FFShadeTri s;
-    s.face_n = fn;
-    if (nrm) {
-        s.n0 = nrm[t.x];
-        s.n1 = nrm[t.y];
-        s.n2 = nrm[t.z];
-    } else {
-        s.n0 = s.n1 = s.n2 = fn;
-    }
-    if (uv) {
-        s.uv0 = uv[t.x];
-        s.uv1 = uv[t.y];
-        s.uv2 = uv[t.z];
-    } else {
-        s.uv0 = s.uv1 = s.uv2 = make_float2(0.f, 0.f);
-    }
+    s.n0x = n0.x, s.n0y = n0.y, s.n0z = n0.z;
+    s.n1x = n1.x, s.n1y = n1.y, s.n1z = n1.z;
+    s.n2x = n2.x, s.n2y = n2.y, s.n2z = n2.z;
     s.material = mat ? mat[i] : 0u;
+    s.u0 = uv0.x, s.v0 = uv0.y, s.u1 = uv1.x, s.v1 = uv1.y, s.u2 = uv2.x, s.v2 = uv2.y;
+    s.pad[0] = s.pad[1] = s.pad[2] = s.pad[3] = 0.f;
     out[i] = s;
 }
 

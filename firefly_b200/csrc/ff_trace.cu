@@ -114,11 +114,15 @@ __global__ void __launch_bounds__(kTraceBlock, 8)
 // Traversal work of n rays (ff_trace_count): one thread per ray over the same
 // traversal step as k_trace, so each ray visits the same nodes and tests the
 // same triangles; out[0] += node records fetched, out[1] += triangles tested.
-template <bool ANY, bool TWO = false>
+// QUEUE: a wavefront queue whose length is in n_dev (n its capacity), whose
+// rays carry their own two-sided mark (as k_trace<*, tagged> reads them).
+template <bool ANY, bool TWO = false, bool QUEUE = false>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_count(FFBvhView bvh, const ff_ray* __restrict__ rays,
                                                              uint64_t n, unsigned long long* __restrict__ out,
-                                                             unsigned int* __restrict__ err)
+                                                             unsigned int* __restrict__ err,
+                                                             const uint32_t* __restrict__ n_dev = nullptr)
 {
+    if (QUEUE) n = min(n, (uint64_t)*n_dev);
     __shared__ uint2 s_stack[kShortStack * kTraceBlock];
     FFStack st;
     st.sm = s_stack + threadIdx.x;
@@ -131,7 +135,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_count(FFBvhView bvh, cons
         const float4 r0 = __ldg(reinterpret_cast<const float4*>(rays + i));
         const float4 r1 = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
         FFRayState r;
-        const float tmin = TWO ? -(r0.w > 0.f ? r0.w : 0.f) : r0.w;
+        const float tmin = (TWO && !QUEUE) ? -(r0.w > 0.f ? r0.w : 0.f) : r0.w;
         ff_ray_setup(r, make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z), tmin, r1.w, ANY);
         uint2 cur = ff_root_group(r);
         st.reset();
@@ -170,6 +174,24 @@ void ff_launch_trace_count(ff_context* ctx, const ff_scene* s, const ff_ray* d_r
         k_trace_count<false, true><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, n, d_out, err);
     else
         k_trace_count<false><<<(unsigned)grid, kTraceBlock, 0, ctx->stream>>>(s->view(), d_rays, n, d_out, err);
+    FF_CUDA_CHECK(cudaGetLastError());
+}
+
+void ff_launch_trace_count_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
+                                 uint64_t cap, bool any_hit, bool two_sided, unsigned long long* d_out,
+                                 unsigned int* err, cudaStream_t stream)
+{
+    if (cap == 0) return;
+    uint64_t grid = (uint64_t)ctx->num_sms * 8;
+    const uint64_t need = (cap + kTraceBlock - 1) / kTraceBlock;
+    if (grid > need) grid = need;
+    const dim3 g((unsigned)grid), b(kTraceBlock);
+    if (any_hit)
+        k_trace_count<true, false, true><<<g, b, 0, stream>>>(bvh, d_rays, cap, d_out, err, n_dev);
+    else if (two_sided)
+        k_trace_count<false, true, true><<<g, b, 0, stream>>>(bvh, d_rays, cap, d_out, err, n_dev);
+    else
+        k_trace_count<false, false, true><<<g, b, 0, stream>>>(bvh, d_rays, cap, d_out, err, n_dev);
     FF_CUDA_CHECK(cudaGetLastError());
 }
 

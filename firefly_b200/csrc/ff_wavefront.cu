@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 // Continue: hit attributes (dTriangle::hit, dTriangle.cu:94-105).
                 const bool back = hit_back(hit.prim);
                 const uint32_t prim = hit_index(hit.prim);
-                const FFShadeTri& t = w.shade[prim];
+                const FFShadeRec t = ff_load_shade(w.shade, prim);
                 const float u = hit.u, v = hit.v;
                 float3 n = normalize3(u * t.n1 + v * t.n2 + ((1.f - u) - v) * t.n0);
                 const float3 pos = ro + hit.t * rd;
@@ -627,6 +627,7 @@ struct FFWavefrontWS {
     WF w{};
     unsigned int* err = nullptr;
     unsigned long long* trace_ctr = nullptr;  // [0] closest, [1] any
+    unsigned long long* fetch = nullptr;      // profiled renders: nodes / tris of the closest, then the any-hit traces
     uint32_t* h_active = nullptr;             // pinned host word for the frame-loop check
     // the any-hit trace runs on `side` beside the closest-hit trace: its
     // blocks take the SMs the closest-hit trace's finished blocks leave
@@ -720,7 +721,7 @@ size_t ws_bytes(uint32_t P)
     add(16, P) /*beta*/; add(sizeof(SlotRay), P); add(sizeof(SlotShade), P); add(sizeof(SlotMis), P);
     add(sizeof(SlotVtx), P); add(16, P) /*hit_ngeo*/; add(16, P); add(16, P) /*acc, acc_c*/; add(4, P) /*cnt*/;
     add(sizeof(ff_ray), P); add(4, P); add(sizeof(ff_hit), P); add(sizeof(ff_ray), 3ull * P); add(4, 3ull * P);
-    add(4, (size_t)kKinds * P); add(4, 64); add(8, 8); add(4, 4); add(8, 4);
+    add(4, (size_t)kKinds * P); add(4, 64); add(8, 8); add(4, 4); add(8, 4); add(8, 4);
     return b;
 }
 
@@ -756,6 +757,7 @@ void ws_setup(FFWavefrontWS* ws, uint32_t P)
     w.totals = carve<unsigned long long>(p, 8);
     ws->err = carve<unsigned int>(p, 4);
     ws->trace_ctr = carve<unsigned long long>(p, 4);
+    ws->fetch = carve<unsigned long long>(p, 4);
     ws->P = P;
 }
 
@@ -815,6 +817,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
                                   cudaMemcpyDeviceToHost, stream));
     FF_CUDA_CHECK(cudaMemsetAsync(w.totals, 0, 8 * sizeof(unsigned long long), stream));
     FF_CUDA_CHECK(cudaMemsetAsync(ws->err, 0, sizeof(unsigned int), stream));
+    FF_CUDA_CHECK(cudaMemsetAsync(ws->fetch, 0, 4 * sizeof(unsigned long long), stream));
     FF_CUDA_CHECK(cudaStreamSynchronize(stream));
     bool kind_used[kKinds] = {false, false, false, false, false};
     for (auto& mt : mats) kind_used[mt.kind] = true;
@@ -865,6 +868,12 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
                 ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
                                       ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.ray));
                 mark();
+                // the traversal work of this frame's queues, counted by a second pass of the same
+                // traversal (outside the stage marks)
+                ff_launch_trace_count_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, false, scene->refracts, ws->fetch,
+                                            ws->err, stream);
+                ff_launch_trace_count_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, true, false, ws->fetch + 2,
+                                            ws->err, stream);
             } else {
                 // the traces are independent (hits by slot, answers by shadow-ray tag)
                 FF_CUDA_CHECK(cudaEventRecord(ws->fork, stream));
@@ -895,15 +904,20 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
                                                    film->count.as<uint32_t>());
     FF_CUDA_CHECK(cudaGetLastError());
     FF_CUDA_CHECK(cudaEventRecord(ctx->ev1, stream));
-    unsigned long long totals[3] = {0, 0, 0};
+    unsigned long long totals[3] = {0, 0, 0}, fetch[4] = {0, 0, 0, 0};
     unsigned int err = 0;
     FF_CUDA_CHECK(cudaMemcpyAsync(totals, w.totals, sizeof(totals), cudaMemcpyDeviceToHost, stream));
     FF_CUDA_CHECK(cudaMemcpyAsync(&err, ws->err, sizeof(err), cudaMemcpyDeviceToHost, stream));
+    if (profile) FF_CUDA_CHECK(cudaMemcpyAsync(fetch, ws->fetch, sizeof(fetch), cudaMemcpyDeviceToHost, stream));
     FF_CUDA_CHECK(cudaStreamSynchronize(stream));
     if (err) throw FFError{FF_ERR_INTERNAL, "traversal exceeded its step bound (malformed BVH)"};
     if (stats) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        stats->ext_nodes = fetch[0];
+        stats->ext_tris = fetch[1];
+        stats->shadow_nodes = fetch[2];
+        stats->shadow_tris = fetch[3];
         if (profile) {
             // 5 marks per frame: logic | shade | trace ext | trace shadow
             float t[4] = {0.f, 0.f, 0.f, 0.f};
@@ -920,7 +934,8 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
             stats->ms_trace_shadow = t[3];
         }
         for (auto e : evs) cudaEventDestroy(e);
-        stats->kernel_launches = frames * (3u + (uint32_t)n_kinds) + 2u;
+        // profiled renders add the two counting passes per frame
+        stats->kernel_launches = frames * (3u + (uint32_t)n_kinds + (profile ? 2u : 0u)) + 2u;
         stats->extension_rays = totals[0];
         stats->shadow_rays = totals[1];
         stats->samples = (uint64_t)st->spp * WH;

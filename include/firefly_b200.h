@@ -214,8 +214,9 @@ typedef struct ff_ray {
 
 /* Closest-hit result (16 bytes).  prim is the caller's ORIGINAL triangle
  * index (the reference reports the post-reorder index, dTriangle.cu:172;
- * orderedPrims maps it back, BVH.cpp:95-96), -1 on a miss.  u weights the
- * second vertex and v the third, as in dTriangle::hit (dTriangle.cu:94-97). */
+ * orderedPrims maps it back, BVH.cpp:95-96), -1 on a miss, and -2 - index
+ * for a back face of an FF_TRACE_TWO_SIDED query.  u weights the second
+ * vertex and v the third, as in dTriangle::hit (dTriangle.cu:94-97). */
 typedef struct ff_hit {
     float t, u, v;
     int32_t prim;
@@ -330,6 +331,11 @@ typedef struct ff_render_stats {
     uint64_t grad_atomics;
     /* ff_render_adjoint: roughness texels touched (1 float atomic = 4 B each) */
     uint64_t grad_atomics_roughness;
+    /* ff_render with FF_RENDER_PROFILE: the traversal work of the traced
+     * rays, counted by a second pass of the same traversal over each frame's
+     * queues (8-wide node records fetched, triangles tested; a node record is
+     * 80 B, a triangle record 48 B) */
+    uint64_t ext_nodes, ext_tris, shadow_nodes, shadow_tris;
 } ff_render_stats;
 
 /* Replaces PathTracer::draw + wavefront_pathtrace (PathTracer.cpp:59-79,

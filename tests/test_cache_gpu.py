@@ -129,8 +129,10 @@ def test_query_matches_reference(setup):
     scale = np.abs(y_ref).max()
     print(f"[cache] query: max |err| {err.max():.3e}, mean {err.mean():.3e}, |y| max {scale:.3f}")
     assert np.all(np.isfinite(y))
-    assert err.max() <= 2e-2 * scale
-    assert err.mean() <= 2e-3 * scale
+    # float32 accumulation-order differences only (measured max 4.5e-8, mean
+    # 1.2e-9 at |y| max 0.21): operands round to bf16 identically on both sides
+    assert err.max() <= 2e-6 * scale
+    assert err.mean() <= 5e-8 * scale
     # edge cases: one record, an exact multiple of the tile
     assert np.allclose(cache.query(recs[:1]), y[:1], atol=1e-6)
     assert np.allclose(cache.query(recs[:256]), y[:256], atol=1e-6)
@@ -154,13 +156,14 @@ def test_gradients_match_reference(setup):
         a, b = gw[l, :rows], gw_ref[l, :rows]
         rel = np.abs(a - b).max() / np.abs(b).max()
         print(f"[cache] dW{l}: max rel err {rel:.3e} (|dW| max {np.abs(b).max():.3e})")
-        assert rel < 5e-2
+        # measured 2.2e-3 .. 3.4e-3: the backward rounds deltas to bf16 where torch keeps float32
+        assert rel < 2e-2
     assert np.all(gw[4, 3:] == 0)
     gg, gg_ref = p["grad_grid"].reshape(-1, 2), G.grad.numpy()
     touched = np.abs(gg_ref).sum(-1) > 0
     rel = np.abs(gg[touched] - gg_ref[touched]).max() / np.abs(gg_ref).max()
     print(f"[cache] grid grad: {touched.sum()} entries, max rel err {rel:.3e}")
-    assert rel < 5e-2
+    assert rel < 3e-2   # measured 6.0e-3
     assert np.all(gg[~touched] == 0)
 
 
