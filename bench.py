@@ -72,16 +72,17 @@ WF_CLOSEST_BYTES, WF_ANY_BYTES = 32 + 4 + 16, 32 + 4 + 1
 ADJ_LOGIC_BYTES_PER_HIT = 438
 # k_logic in ff_render, per consumed extension hit of a continuing path:
 # reads the slot words (12 B), the hit (16), the ray record (32), throughput,
-# sum and compensation (48), the shading record (32) and the triangle's
+# sum and compensation (48), the shading record (32), the pending light-term
+# record of two frames back and its answer word (68) and the triangle's
 # shading attributes (64); writes sum, compensation, length and throughput
-# (52) and the vertex record (64): 320 B.
-RENDER_LOGIC_BYTES_PER_HIT = 320
-# k_shade, per shaded vertex: reads the vertex record (64 B) and its queue
-# entry (4), writes the shading record (32), the ray record (32) and the
-# extension-queue entry (36): 168 B; plus 36 B per shadow-queue entry (32 B
-# ray, 4 B tag).  Environment and material lookups are L2 gathers and not
-# counted; the mix and dielectric kinds add a 32-B record not counted either.
-RENDER_SHADE_BYTES_PER_VERTEX = 168
+# (52) and the vertex record (64): 388 B.
+RENDER_LOGIC_BYTES_PER_HIT = 388
+# k_shade, per shaded vertex: reads the vertex record (64 B), its queue
+# entry (4) and the throughput (16), writes the shading record (32), the ray
+# record (32), the extension-queue entry (36) and the pending light-term
+# record (64): 248 B; plus 36 B per shadow-queue entry (32 B ray, 4 B tag).
+# Environment and material lookups are L2 gathers and not counted.
+RENDER_SHADE_BYTES_PER_VERTEX = 248
 SHADOW_QUEUE_BYTES = 36
 # Measured DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per unit
 # of each render stage: ncu over every launch of one timed 16-spp C2 step on
@@ -99,6 +100,8 @@ ADJ_DRAM_BYTES_PER_UNIT = {"k_logic (adjoint)": 334.1, "k_shade (adjoint)": 259.
 # frames, 9,513,224 queries): the 64 B record in and the film update; the
 # hash grid's FP16 copy stays in L2.
 CACHE_INFER_DRAM_BYTES_PER_QUERY = 110.8
+# k_cache_infer's encoder: 16 levels x 8 corners x one 4-B FP16 pair per query.
+CACHE_GATHER_BYTES_PER_QUERY = 16 * 8 * 4
 
 
 def dist_env():
@@ -1245,6 +1248,23 @@ def cache_line(args, ws, rank, local, dist, ctx, dev, stream):
         peak, peak_kind = measured_peaks("bf16_tflops")
         q_flops = prof["cache_queries"] * 2.0 * (4 * 64 * 64 + 16 * 64)
         q_tflops = q_flops / (prof["ms_cache_query"] / 1e3) / 1e12 if prof["ms_cache_query"] > 0 else None
+        # the encoder's hash-grid gathers (16 levels x 8 corners x 4 B per
+        # query, from the L2-resident FP16 table) against an L2-resident read
+        try:
+            l2_ref = l2_read_gbs(dev)
+        except Exception as e:   # the reference bandwidth is optional
+            print(f"l2 read probe unavailable: {e}", file=sys.stderr)
+            l2_ref = None
+        g_gbs = (prof["cache_queries"] * CACHE_GATHER_BYTES_PER_QUERY / (prof["ms_cache_query"] / 1e3) / 1e9
+                 if prof["ms_cache_query"] > 0 else None)
+        l2_gather = {"gather_bytes_per_query": CACHE_GATHER_BYTES_PER_QUERY,
+                     "achieved_gather_gbs": None if g_gbs is None else round(g_gbs, 1),
+                     "l2_read_gbs": None if l2_ref is None else round(l2_ref, 1),
+                     "frac_of_l2_read": None if (g_gbs is None or l2_ref is None) else round(g_gbs / l2_ref, 4),
+                     "note": ("the kernel is bound by these gathers (L1 and L2 throughput), not by the tensor pipe; "
+                              "l2_read_gbs = a probe kernel reading a 32 MiB L2-resident buffer 40 times (L1 "
+                              "bypassed); each 4-B entry moves a 32-B sector, two corners per sector where they "
+                              "share an aligned group of four")}
         line = {"metric": "time-to-relMSE 0.01 (learned radiance cache)", "value": None if ms != ms else round(ms, 2),
                 "unit": "ms", "n_gpus": ws, "steps": len(cache_traj), "warmup": args.cache_warmup,
                 "ms_per_step": None, "higher_is_better": False, "scaling": "replicas", "vs_baseline": None,
@@ -1267,7 +1287,7 @@ def cache_line(args, ws, rank, local, dist, ctx, dev, stream):
                              "traffic_note": ("DRAM bytes of one k_cache_infer launch (one per frame): ncu dram bytes "
                                               "per query over 6 frames x this run's queries per frame"),
                              "peak_source": peak_kind,
-                             "flops_per_query": 2 * (4 * 64 * 64 + 16 * 64)},
+                             "flops_per_query": 2 * (4 * 64 * 64 + 16 * 64), "l2_gather": l2_gather},
                 "cpu_baseline": None,
                 "cpu_baseline_note": "not timed for the cache: the plain tracer on the same GPU is the comparator",
                 "e2e": {"value": round(e2e_ms, 2), "unit": "ms", "h2d_bytes_per_step": 80,

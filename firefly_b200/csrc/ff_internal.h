@@ -248,7 +248,8 @@ void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* 
                            uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter,
                            unsigned int* err, const uint32_t* tags = nullptr, uint8_t* occ = nullptr,
                            cudaStream_t stream = nullptr,   // null: the context's stream
-                           bool two_sided = false);          // honour the per-ray two-sided mark
+                           bool two_sided = false,
+                           int max_blocks_per_sm = 0);      // 0: as many as fit (the grid fills the GPU)          // honour the per-ray two-sided mark
 
 // ff_wavefront.cu: the path-replay adjoint on the wavefront stages.  Every
 // pointer is device memory; gradients are added to grad_* (null = not

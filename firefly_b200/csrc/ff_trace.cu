@@ -254,7 +254,7 @@ void ff_launch_trace_scratch(ff_context* ctx, const ff_scene* s, const ff_ray* d
 // kernel honours the per-ray two-sided mark (the sign bit of tmin).
 void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* d_rays, const uint32_t* n_dev,
                            uint64_t cap, ff_hit* d_hits, bool any_hit, unsigned long long* counter, unsigned int* err,
-                           const uint32_t* tags, uint8_t* occ, cudaStream_t stream, bool two_sided)
+                           const uint32_t* tags, uint8_t* occ, cudaStream_t stream, bool two_sided, int max_blocks_per_sm)
 {
     if (cap == 0) return;
     const bool two = two_sided && !any_hit;
@@ -272,7 +272,8 @@ void ff_launch_trace_queue(ff_context* ctx, const FFBvhView& bvh, const ff_ray* 
         FF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kTraceBlock, 0));
         blocks_per_sm = b < 1 ? 1 : b;
     }
-    uint64_t grid = (uint64_t)ctx->num_sms * blocks_per_sm;
+    const int bps = max_blocks_per_sm > 0 && max_blocks_per_sm < blocks_per_sm ? max_blocks_per_sm : blocks_per_sm;
+    uint64_t grid = (uint64_t)ctx->num_sms * bps;
     const uint64_t need = (cap + kTraceBlock - 1) / kTraceBlock;
     if (grid > need) grid = need;
     cudaStream_t st = stream ? stream : ctx->stream;

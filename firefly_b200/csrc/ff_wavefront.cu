@@ -57,8 +57,10 @@ constexpr uint32_t PH_START = 0, PH_FLIGHT = 1, PH_DONE = 2;
 // fewer frames); 8M slots hold about 3.6 GB of path state.
 constexpr uint64_t kDefaultPoolTarget = 1ull << 23;
 
-// Counter words of one frame (zeroed at the start of each frame).
+// Counter words of one frame (zeroed at the start of each frame); one block
+// of kCtrStride words per frame parity.
 enum { C_EXT = 0, C_SH = 1, C_MAT = 2, C_ACTIVE = 2 + kKinds, C_WORDS = 8 + kKinds };
+constexpr uint32_t kCtrStride = 32;
 
 // The slot's ray (origin, direction) and its visibility word: byte k = the
 // any-hit trace's answer for shadow ray k (1 occluded), byte 3 = which shadow
@@ -89,8 +91,26 @@ struct __align__(32) SlotVtx {
     float wox, woy, woz;   // toward the previous vertex
     float v;
 };
-static_assert(sizeof(SlotRay) == 32 && sizeof(SlotShade) == 32 && sizeof(SlotMis) == 32 && sizeof(SlotVtx) == 64,
+// Deferred light terms (ff_render without the cache): what a vertex's
+// shading leaves for the k_logic two frames later, after the any-hit trace
+// that runs beside the next frame has answered its shadow rays: the
+// throughput at the vertex, the frame stamp, the three light terms and the
+// rays queued.  Indexed [frame parity][slot].
+struct __align__(32) SlotPend {
+    float bx, by, bz;
+    uint32_t stamp;   // frame + kStampBase of the shading; any other value: nothing pending
+    float nee_x, nee_y, nee_z;
+    uint32_t queued;  // bit k: shadow ray k was queued
+    float spec_x, spec_y, spec_z, pad0;
+    float diff_x, diff_y, diff_z, pad1;
+};
+static_assert(sizeof(SlotRay) == 32 && sizeof(SlotShade) == 32 && sizeof(SlotMis) == 32 && sizeof(SlotVtx) == 64 &&
+                  sizeof(SlotPend) == 64,
               "slot records are whole 32-byte sectors");
+constexpr uint32_t kStampBase = 16;
+// Deferred mode: blocks per SM of the any-hit trace (its persistent grid),
+// leaving the rest of each SM to k_logic and k_shade of the next frame.
+constexpr int kDeferShadowBlocks = 4;   // stamps of real frames are >= 16; 0 marks an empty record
 constexpr uint32_t kVtxMatBits = 24, kVtxLenShift = 24, kVtxLenMask = 0x7f;
 // Byte of shadow ray k's answer for slot s in the SlotRay array (the tag the
 // any-hit trace writes to): the low three bytes of the vis word.
@@ -124,12 +144,20 @@ struct WF {
     float4* acc;
     float4* acc_c;
     uint32_t* cnt;
+    // deferred light terms (defer = 1): the frame's parity and number, the
+    // pending records and the any-hit answers (byte k of a slot's word: shadow
+    // ray k occluded), both [2][P]; the shadow queue and the frame counters
+    // are per parity too, so that the any-hit trace of frame f runs beside
+    // k_logic and k_shade of frame f + 1
+    uint32_t defer, par, frame;
+    SlotPend* pend;
+    uint32_t* vis2;
     // queues
     ff_ray* ext_rays;
     uint32_t* ext_tag;   // per queued extension ray: its slot
     ff_hit* ext_hits;    // per slot: the closest hit of its extension ray (written by k_trace)
     ff_ray* sh_rays;
-    uint32_t* sh_tag;    // per queued shadow ray: the byte of its answer in the SlotRay array (vis_byte)
+    uint32_t* sh_tag;    // per queued shadow ray: the byte of its answer (vis_byte, or 4 * slot + k in vis2)
     uint32_t* mat_queue;   // kKinds * P
     uint32_t* ctr;         // C_WORDS
     unsigned long long* totals;  // [0] extension rays, [1] shadow rays, [2] samples
@@ -215,6 +243,40 @@ __device__ void start_sample(const WF& w, uint32_t s, uint32_t sample, bool& pus
     push = true;
 }
 
+// Deferred mode: the light terms of the vertex slot s shaded two frames ago
+// (its pending record of this frame's parity, stamp frame - 2), gated by
+// their shadow rays' answers exactly as k_logic gates them without
+// deferral, into the slot's compensated sum.  Returns whether anything was
+// pending.
+__device__ __forceinline__ bool consume_pending(const WF& w, uint32_t s, float4& acc, float4& accc)
+{
+    const size_t i = (size_t)w.par * w.P + s;
+    const float4* pq = reinterpret_cast<const float4*>(w.pend + i);
+    const float4 a = pq[0];
+    if (__float_as_uint(a.w) != w.frame + kStampBase - 2u) return false;
+    const float4 b = pq[1];
+    const uint32_t q = __float_as_uint(b.w);
+    const uint32_t vw = w.vis2[i];
+    const bool vis = (q & 1u) && !(vw & 0xffu);
+    const bool vis_s = (q & 2u) && !(vw & 0xff00u);
+    const bool vis_d = (q & 4u) && !(vw & 0xff0000u);
+    const float3 beta = xyz(a);
+    if (w.mode == FF_MODE_CORRECTED) {
+        float3 lb = make_float3(0.f, 0.f, 0.f);
+        if (vis) lb = lb + xyz(b);
+        if (vis_s) lb = lb + xyz(pq[2]);
+        if (vis_d) lb = lb + xyz(pq[3]);
+        if (vis || vis_s || vis_d) kahan_add(acc, accc, lb * beta);
+    } else if (vis) {
+        // parity: the whole light_brdf, MIS terms included, rides on the NEE ray
+        float3 lb = xyz(b);
+        if (vis_s) lb = lb + xyz(pq[2]);
+        if (vis_d) lb = lb + xyz(pq[3]);
+        kahan_add(acc, accc, lb * beta);
+    }
+    return true;
+}
+
 // ADJ: the path-replay adjoint's instantiation (the slot's sum holds the
 // current sample's radiance only, in plain FP32 adds as the megakernel
 // adjoint sums it; no film).
@@ -250,6 +312,7 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
             float3 beta = xyz(w.beta[s]);
             float4 acc = w.acc[s];
             float4 accc = ADJ ? make_float4(0.f, 0.f, 0.f, 0.f) : w.acc_c[s];   // no compensation in the adjoint
+            if (!ADJ && w.defer) consume_pending(w, s, acc, accc);
             bool terminate = (L > w.max_depth) || !found;
             // adjoint replay: dL/dI of this sample's pixel and the primal pass's L_s
             const bool replay = ADJ && w.pass[s] != 0u;
@@ -277,67 +340,69 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 }
             }
             if (L > 1) {
-                // kernel.cu:357-359: light_brdf * beta when the NEE ray was unoccluded
-                const uint32_t vw = sr.vis;
                 const SlotShade sd = w.shd[s];
-                const bool vis = (vw & (1u << 24)) && !(vw & 0xffu);
-                const bool vis_s = (vw & (2u << 24)) && !(vw & 0xff00u);
-                const bool vis_d = (vw & (4u << 24)) && !(vw & 0xff0000u);
-                if (w.mode == FF_MODE_CORRECTED) {
-                    // every term gated by its own visibility ray
-                    float3 lb = make_float3(0.f, 0.f, 0.f);
-                    if (vis) lb = lb + make_float3(sd.nee_x, sd.nee_y, sd.nee_z);
-                    if (vis_s || vis_d) {
-                        const SlotMis sm = w.mis[s];
-                        if (vis_s) lb = lb + make_float3(sm.spec_x, sm.spec_y, sm.spec_z);
-                        if (vis_d) lb = lb + make_float3(sm.diff_x, sm.diff_y, sm.diff_z);
-                    }
-                    if (ADJ) {
-                        if (replay) {
-                            // the previous vertex's gradients, now that its shadow rays are answered
-                            const float4 va = w.v_albedo[s];
-                            const uint32_t flags = __float_as_uint(va.w);
-                            const SlotVtx& pv = w.vtx[s];   // the previous vertex
-                            const float2 uv = make_float2(pv.u, pv.v);
-                            if (flags & V_ALBEDO) {
-                                const FFTexView tv = w.tex[w.adj_texture];
-                                touched += scatter_footprint(w.grad_tex, footprint(tv.width, tv.height, uv.x, uv.y),
-                                                             albedo_grad(Ltot - xyz(acc), xyz(va), dI));
-                            }
-                            if (flags & V_ROUGH) {
-                                RoughTerms rt;
-                                rt.nee = xyz(w.v_nee[s]);
-                                rt.spec = xyz(w.v_spec[s]);
-                                rt.dext = xyz(w.v_dext[s]);
-                                const float3 rimm = rough_own(rt, vis, vis_s, beta);
-                                const float3 L_after = xyz(acc) + lb * beta;
-                                const float g = dot3(dI, rimm + (Ltot - L_after) * rt.dext);
-                                const FFTexView tv = w.tex[w.adj_rough];
-                                touched_r += scatter_footprint1(w.grad_rough, footprint(tv.width, tv.height, uv.x, uv.y), g,
-                                                                (flags & V_ROUGH_Y) ? 1 : 0);
-                            }
-                            if ((flags & V_ENV) && vis) {
-                                // NEE term c_nee = coef * Le(wi): d/dLe = beta * coef
-                                float3 wl = make_float3(pv.wix, pv.wiy, pv.wiz);
-                                wl.y = clampf(wl.y, -1.f, 1.f);
-                                const float2 euv = spherical_map(wl);
-                                touched += scatter_footprint(w.grad_env, footprint(w.env.width, w.env.height, euv.x, euv.y),
-                                                             dI * beta * xyz(w.v_coef[s]));
-                            }
+                if (ADJ || !w.defer) {   // (deferred light terms were added above)
+                    // kernel.cu:357-359: light_brdf * beta when the NEE ray was unoccluded
+                    const uint32_t vw = sr.vis;
+                    const bool vis = (vw & (1u << 24)) && !(vw & 0xffu);
+                    const bool vis_s = (vw & (2u << 24)) && !(vw & 0xff00u);
+                    const bool vis_d = (vw & (4u << 24)) && !(vw & 0xff0000u);
+                    if (w.mode == FF_MODE_CORRECTED) {
+                        // every term gated by its own visibility ray
+                        float3 lb = make_float3(0.f, 0.f, 0.f);
+                        if (vis) lb = lb + make_float3(sd.nee_x, sd.nee_y, sd.nee_z);
+                        if (vis_s || vis_d) {
+                            const SlotMis sm = w.mis[s];
+                            if (vis_s) lb = lb + make_float3(sm.spec_x, sm.spec_y, sm.spec_z);
+                            if (vis_d) lb = lb + make_float3(sm.diff_x, sm.diff_y, sm.diff_z);
                         }
-                        if (vis || vis_s || vis_d) acc = f4(xyz(acc) + lb * beta);
-                    } else if (vis || vis_s || vis_d) {
+                        if (ADJ) {
+                            if (replay) {
+                                // the previous vertex's gradients, now that its shadow rays are answered
+                                const float4 va = w.v_albedo[s];
+                                const uint32_t flags = __float_as_uint(va.w);
+                                const SlotVtx& pv = w.vtx[s];   // the previous vertex
+                                const float2 uv = make_float2(pv.u, pv.v);
+                                if (flags & V_ALBEDO) {
+                                    const FFTexView tv = w.tex[w.adj_texture];
+                                    touched += scatter_footprint(w.grad_tex, footprint(tv.width, tv.height, uv.x, uv.y),
+                                                                 albedo_grad(Ltot - xyz(acc), xyz(va), dI));
+                                }
+                                if (flags & V_ROUGH) {
+                                    RoughTerms rt;
+                                    rt.nee = xyz(w.v_nee[s]);
+                                    rt.spec = xyz(w.v_spec[s]);
+                                    rt.dext = xyz(w.v_dext[s]);
+                                    const float3 rimm = rough_own(rt, vis, vis_s, beta);
+                                    const float3 L_after = xyz(acc) + lb * beta;
+                                    const float g = dot3(dI, rimm + (Ltot - L_after) * rt.dext);
+                                    const FFTexView tv = w.tex[w.adj_rough];
+                                    touched_r += scatter_footprint1(w.grad_rough, footprint(tv.width, tv.height, uv.x, uv.y), g,
+                                                                    (flags & V_ROUGH_Y) ? 1 : 0);
+                                }
+                                if ((flags & V_ENV) && vis) {
+                                    // NEE term c_nee = coef * Le(wi): d/dLe = beta * coef
+                                    float3 wl = make_float3(pv.wix, pv.wiy, pv.wiz);
+                                    wl.y = clampf(wl.y, -1.f, 1.f);
+                                    const float2 euv = spherical_map(wl);
+                                    touched += scatter_footprint(w.grad_env, footprint(w.env.width, w.env.height, euv.x, euv.y),
+                                                                 dI * beta * xyz(w.v_coef[s]));
+                                }
+                            }
+                            if (vis || vis_s || vis_d) acc = f4(xyz(acc) + lb * beta);
+                        } else if (vis || vis_s || vis_d) {
+                            kahan_add(acc, accc, lb * beta);
+                        }
+                    } else if (!ADJ && vis) {
+                        // parity: the whole light_brdf, MIS terms included, rides on the NEE ray
+                        float3 lb = make_float3(sd.nee_x, sd.nee_y, sd.nee_z);
+                        if (vis_s || vis_d) {
+                            const SlotMis sm = w.mis[s];
+                            if (vis_s) lb = lb + make_float3(sm.spec_x, sm.spec_y, sm.spec_z);
+                            if (vis_d) lb = lb + make_float3(sm.diff_x, sm.diff_y, sm.diff_z);
+                        }
                         kahan_add(acc, accc, lb * beta);
                     }
-                } else if (!ADJ && vis) {
-                    // parity: the whole light_brdf, MIS terms included, rides on the NEE ray
-                    float3 lb = make_float3(sd.nee_x, sd.nee_y, sd.nee_z);
-                    if (vis_s || vis_d) {
-                        const SlotMis sm = w.mis[s];
-                        if (vis_s) lb = lb + make_float3(sm.spec_x, sm.spec_y, sm.spec_z);
-                        if (vis_d) lb = lb + make_float3(sm.diff_x, sm.diff_y, sm.diff_z);
-                    }
-                    kahan_add(acc, accc, lb * beta);
                 }
                 const float3 f = make_float3(sd.f_x, sd.f_y, sd.f_z);
                 const float pdf = sd.pdf;
@@ -439,6 +504,13 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 const uint32_t qi = warp_append(w.n_queries, query, nullptr);
                 if (query) w.queries[qi] = rec;
             }
+        } else if (!ADJ && w.defer) {
+            // a finished slot: the light terms of its last vertex may still be pending
+            float4 acc = w.acc[s], accc = w.acc_c[s];
+            if (consume_pending(w, s, acc, accc)) {
+                w.acc[s] = acc;
+                w.acc_c[s] = accc;
+            }
         }
     }
     // compaction into the extension queue and the material queues
@@ -486,6 +558,7 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
         o.ray_nee = o.ray_spec = o.ray_diff = false;
         bool ext_two = false;   // the continuation runs inside an object: traced two-sided
         uint32_t s = 0;
+        float4 beta_v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (valid) {
             s = w.mat_queue[(size_t)KIND * w.P + qi];
             const SlotVtx vx = w.vtx[s];
@@ -523,7 +596,8 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
                 o.ext_o = pos + ng * (side * w.shadow_offset);
             ext_two = runs_inside(back, KIND == FF_MAT_DIELECTRIC, side);
             w.shd[s] = SlotShade{o.c_nee.x, o.c_nee.y, o.c_nee.z, o.ext_pdf, o.ext_f.x, o.ext_f.y, o.ext_f.z, o.ext_cos};
-            if (KIND == FF_MAT_MIX || KIND == FF_MAT_DIELECTRIC)   // the kinds with BSDF-sampled light terms
+            // the kinds with BSDF-sampled light terms (deferred mode: in the pending record)
+            if ((KIND == FF_MAT_MIX || KIND == FF_MAT_DIELECTRIC) && (ADJ || !w.defer))
                 w.mis[s] = SlotMis{o.c_spec.x, o.c_spec.y, o.c_spec.z, 0.f, o.c_diff.x, o.c_diff.y, o.c_diff.z, 0.f};
             if (ADJ && w.pass[s] != 0u) {
                 uint32_t flags = 0;
@@ -556,22 +630,33 @@ __global__ void __launch_bounds__(128) k_shade(WF w)
         const uint32_t q0 = warp_append(&w.ctr[C_SH], o.ray_nee, &w.totals[1]);
         const uint32_t q1 = warp_append(&w.ctr[C_SH], o.ray_spec, &w.totals[1]);
         const uint32_t q2 = warp_append(&w.ctr[C_SH], o.ray_diff, &w.totals[1]);
+        // answer tags: bytes of the slot's vis word in SlotRay, or of its word in vis2 (deferred mode)
+        const bool defer = !ADJ && w.defer;
         if (o.ray_nee) {
             w.sh_rays[q0] = o.r_nee;
-            w.sh_tag[q0] = vis_byte(s, 0);
+            w.sh_tag[q0] = defer ? 4u * s : vis_byte(s, 0);
         }
         if (o.ray_spec) {
             w.sh_rays[q1] = o.r_spec;
-            w.sh_tag[q1] = vis_byte(s, 1);
+            w.sh_tag[q1] = defer ? 4u * s + 1u : vis_byte(s, 1);
         }
         if (o.ray_diff) {
             w.sh_rays[q2] = o.r_diff;
-            w.sh_tag[q2] = vis_byte(s, 2);
+            w.sh_tag[q2] = defer ? 4u * s + 2u : vis_byte(s, 2);
         }
         if (valid) {
             // the continuation ray and the queued-rays byte, one whole record
             const uint32_t queued = ((o.ray_nee ? 1u : 0u) | (o.ray_spec ? 2u : 0u) | (o.ray_diff ? 4u : 0u)) << 24;
             w.ray[s] = SlotRay{o.ext_o.x, o.ext_o.y, o.ext_o.z, queued, o.ext_d.x, o.ext_d.y, o.ext_d.z, 0.f};
+            if (defer) {
+                // the light terms with the throughput they multiply, for k_logic two frames on
+                beta_v = w.beta[s];   // the throughput at this vertex
+                float4* pq = reinterpret_cast<float4*>(w.pend + (size_t)w.par * w.P + s);
+                pq[0] = make_float4(beta_v.x, beta_v.y, beta_v.z, __uint_as_float(w.frame + kStampBase));
+                pq[1] = make_float4(o.c_nee.x, o.c_nee.y, o.c_nee.z, __uint_as_float(queued >> 24));
+                pq[2] = f4(o.c_spec);
+                pq[3] = f4(o.c_diff);
+            }
         }
     }
 }
@@ -590,6 +675,23 @@ __global__ void k_init(WF w, uint32_t spp, uint32_t sample_offset)
     w.acc_c[s] = make_float4(0.f, 0.f, 0.f, 0.f);
     w.cnt[s] = 0;
     w.ray[s].vis = 0u;
+    if (w.defer) {
+        w.pend[s].stamp = 0u;
+        w.pend[(size_t)w.P + s].stamp = 0u;
+    }
+}
+
+// Deferred mode: the light terms still pending after the last frame (stamp
+// w.frame - 2 of the parity of w.frame).
+__global__ void k_flush_pending(WF w)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= w.P) return;
+    float4 acc = w.acc[s], accc = w.acc_c[s];
+    if (consume_pending(w, s, acc, accc)) {
+        w.acc[s] = acc;
+        w.acc_c[s] = accc;
+    }
 }
 
 // Film += the m slot sums of each pixel, in slot order (compensated).
@@ -623,16 +725,26 @@ struct FFWavefrontWS {
     uint32_t P = 0;
     DevBuf buf;
     DevBuf adj_buf;   // the adjoint's per-slot arrays (allocated by ff_wavefront_adjoint only)
+    DevBuf defer_buf; // the deferred light terms' arrays (allocated by ff_render only)
+    uint32_t defer_P = 0;
     uint32_t adj_P = 0;
     WF w{};
     unsigned int* err = nullptr;
-    unsigned long long* trace_ctr = nullptr;  // [0] closest, [1] any
+    unsigned long long* trace_ctr = nullptr;  // per frame parity p: [2p] closest, [2p + 1] any
+    // per frame parity p: the counter words (ctr_base + kCtrStride * p) and the
+    // shadow queue (sh_rays_base[p], sh_tag_base[p]); WF points at the current
+    // frame's
+    uint32_t* ctr_base = nullptr;
+    ff_ray* sh_rays_base[2] = {nullptr, nullptr};
+    uint32_t* sh_tag_base[2] = {nullptr, nullptr};
     unsigned long long* fetch = nullptr;      // profiled renders: nodes / tris of the closest, then the any-hit traces
     uint32_t* h_active = nullptr;             // pinned host word for the frame-loop check
     // the any-hit trace runs on `side` beside the closest-hit trace: its
     // blocks take the SMs the closest-hit trace's finished blocks leave
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
+    // deferred mode: the any-hit trace of the last frame of each parity done
+    cudaEvent_t sh_done[2] = {nullptr, nullptr};
     // k_shade of the second to fifth material kind in use, beside the first
     cudaStream_t kind_side[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t kind_join[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -642,6 +754,7 @@ struct FFWavefrontWS {
         FF_CUDA_CHECK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
         FF_CUDA_CHECK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
         FF_CUDA_CHECK(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+        for (int i = 0; i < 2; ++i) FF_CUDA_CHECK(cudaEventCreateWithFlags(&sh_done[i], cudaEventDisableTiming));
         for (int i = 0; i < 4; ++i) {
             FF_CUDA_CHECK(cudaStreamCreateWithFlags(&kind_side[i], cudaStreamNonBlocking));
             FF_CUDA_CHECK(cudaEventCreateWithFlags(&kind_join[i], cudaEventDisableTiming));
@@ -652,6 +765,8 @@ struct FFWavefrontWS {
         if (h_active) cudaFreeHost(h_active);
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
+        for (int i = 0; i < 2; ++i)
+            if (sh_done[i]) cudaEventDestroy(sh_done[i]);
         if (side) cudaStreamDestroy(side);
         for (int i = 0; i < 4; ++i) {
             if (kind_join[i]) cudaEventDestroy(kind_join[i]);
@@ -721,14 +836,15 @@ size_t ws_bytes(uint32_t P)
     add(16, P) /*beta*/; add(sizeof(SlotRay), P); add(sizeof(SlotShade), P); add(sizeof(SlotMis), P);
     add(sizeof(SlotVtx), P); add(16, P) /*hit_ngeo*/; add(16, P); add(16, P) /*acc, acc_c*/; add(4, P) /*cnt*/;
     add(sizeof(ff_ray), P); add(4, P); add(sizeof(ff_hit), P); add(sizeof(ff_ray), 3ull * P); add(4, 3ull * P);
-    add(4, (size_t)kKinds * P); add(4, 64); add(8, 8); add(4, 4); add(8, 4); add(8, 4);
+    add(4, (size_t)kKinds * P); add(4, 2 * kCtrStride); add(8, 8); add(4, 4); add(8, 4); add(8, 4);
     return b;
 }
 
 void ws_setup(FFWavefrontWS* ws, uint32_t P)
 {
     if (ws->P == P && ws->buf.ptr) return;
-    ws->buf.release();
+    // a pool of another size: the allocation is kept when it is large enough
+    // (freeing and allocating gigabytes costs milliseconds)
     ws->buf.alloc(ws_bytes(P));
     char* p = ws->buf.as<char>();
     WF& w = ws->w;
@@ -750,15 +866,42 @@ void ws_setup(FFWavefrontWS* ws, uint32_t P)
     w.ext_rays = carve<ff_ray>(p, P);
     w.ext_tag = carve<uint32_t>(p, P);
     w.ext_hits = carve<ff_hit>(p, P);
-    w.sh_rays = carve<ff_ray>(p, 3ull * P);
-    w.sh_tag = carve<uint32_t>(p, 3ull * P);
+    ws->sh_rays_base[0] = w.sh_rays = carve<ff_ray>(p, 3ull * P);
+    ws->sh_tag_base[0] = w.sh_tag = carve<uint32_t>(p, 3ull * P);
     w.mat_queue = carve<uint32_t>(p, (size_t)kKinds * P);
-    w.ctr = carve<uint32_t>(p, 64);
+    ws->ctr_base = w.ctr = carve<uint32_t>(p, 2 * kCtrStride);
+    w.defer = w.par = w.frame = 0u;
     w.totals = carve<unsigned long long>(p, 8);
     ws->err = carve<unsigned int>(p, 4);
     ws->trace_ctr = carve<unsigned long long>(p, 4);
     ws->fetch = carve<unsigned long long>(p, 4);
+    ws->sh_rays_base[1] = nullptr;
+    ws->sh_tag_base[1] = nullptr;
+    w.pend = nullptr;
+    w.vis2 = nullptr;
+    ws->defer_P = 0;   // carved again by defer_setup, in its allocation if large enough
     ws->P = P;
+}
+
+// The deferred light terms' arrays (ff_render only, allocated on its first
+// call for this pool size): the second frame parity's shadow queue, the
+// pending records and the answer words of both parities.
+void defer_setup(FFWavefrontWS* ws, uint32_t P)
+{
+    if (ws->defer_P == P && ws->defer_buf.ptr) return;
+    size_t b = 0;
+    auto add = [&](size_t sz, size_t n) { b += (sz * n + 255) & ~size_t(255); };
+    add(sizeof(ff_ray), 3ull * P);
+    add(4, 3ull * P);
+    add(sizeof(SlotPend), 2ull * P);
+    add(4, 2ull * P);
+    ws->defer_buf.alloc(b);
+    char* p = ws->defer_buf.as<char>();
+    ws->sh_rays_base[1] = carve<ff_ray>(p, 3ull * P);
+    ws->sh_tag_base[1] = carve<uint32_t>(p, 3ull * P);
+    ws->w.pend = carve<SlotPend>(p, 2ull * P);
+    ws->w.vis2 = carve<uint32_t>(p, 2ull * P);
+    ws->defer_P = P;
 }
 
 }  // namespace
@@ -822,6 +965,10 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     bool kind_used[kKinds] = {false, false, false, false, false};
     for (auto& mt : mats) kind_used[mt.kind] = true;
 
+    // deferred light terms: every render but the cached one (see the frame loop)
+    const bool defer = hook == nullptr;
+    if (defer) defer_setup(ws, P);
+    w.defer = defer ? 1u : 0u;
     FF_CUDA_CHECK(cudaEventRecord(ctx->ev0, stream));
     k_init<<<(P + 255) / 256, 256, 0, stream>>>(w, st->spp, st->sample_offset);
     FF_CUDA_CHECK(cudaGetLastError());
@@ -844,10 +991,30 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
     ws->ensure_streams();
     uint32_t* h_active = ws->h_active;
     const uint32_t max_frames = (st->spp + 1) * (st->max_depth + 2) + 8;
+    // Deferred light terms (every render but the cached one): the any-hit
+    // trace of frame f runs on the side stream beside k_logic, k_shade and
+    // the closest-hit trace of frame f + 1, and k_logic of frame f + 2 adds
+    // the light terms its answers let through.  Frames of one parity share
+    // counters, a shadow queue and pending records, so frame f + 2 waits for
+    // the any-hit trace of frame f.  Under stage timing everything stays on
+    // the one stream.
+    auto set_frame = [&](uint32_t f) -> uint32_t {
+        const uint32_t par = defer ? (f & 1u) : 0u;
+        w.par = par;
+        w.frame = f;
+        w.ctr = ws->ctr_base + kCtrStride * par;
+        w.sh_rays = ws->sh_rays_base[par];
+        w.sh_tag = ws->sh_tag_base[par];
+        return par;
+    };
     while (active && frames < max_frames) {
         // a batch of frames between host checks
         for (int b = 0; b < 4; ++b) {
-            k_reset_counters<<<1, 32, 0, stream>>>(w.ctr, ws->trace_ctr);
+            const uint32_t par = set_frame(frames);
+            unsigned long long* tctr = ws->trace_ctr + 2 * par;
+            uint8_t* occ = defer ? reinterpret_cast<uint8_t*>(w.vis2 + (size_t)par * P) : reinterpret_cast<uint8_t*>(w.ray);
+            if (defer && !profile && frames >= 2) FF_CUDA_CHECK(cudaStreamWaitEvent(stream, ws->sh_done[par], 0));
+            k_reset_counters<<<1, 32, 0, stream>>>(w.ctr, tctr);
             mark();
             k_logic<false><<<(P + 255) / 256, 256, 0, stream>>>(w);
             mark();
@@ -862,11 +1029,11 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
             mark();
             if (profile) {
                 // stage timing: the two traces one after the other
-                ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
-                                      ws->err, w.ext_tag, nullptr, nullptr, scene->refracts);
+                ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, tctr, ws->err,
+                                      w.ext_tag, nullptr, nullptr, scene->refracts);
                 mark();
-                ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
-                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.ray));
+                ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true, tctr + 1, ws->err,
+                                      w.sh_tag, occ);
                 mark();
                 // the traversal work of this frame's queues, counted by a second pass of the same
                 // traversal (outside the stage marks)
@@ -878,13 +1045,16 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
                 // the traces are independent (hits by slot, answers by shadow-ray tag)
                 FF_CUDA_CHECK(cudaEventRecord(ws->fork, stream));
                 FF_CUDA_CHECK(cudaStreamWaitEvent(ws->side, ws->fork, 0));
-                ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, ws->trace_ctr,
-                                      ws->err, w.ext_tag, nullptr, nullptr, scene->refracts);
-                ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true,
-                                      ws->trace_ctr + 1, ws->err, w.sh_tag, reinterpret_cast<uint8_t*>(w.ray),
-                                      ws->side);
-                FF_CUDA_CHECK(cudaEventRecord(ws->join, ws->side));
-                FF_CUDA_CHECK(cudaStreamWaitEvent(stream, ws->join, 0));
+                ff_launch_trace_queue(ctx, bvh, w.ext_rays, w.ctr + C_EXT, P, w.ext_hits, false, tctr, ws->err,
+                                      w.ext_tag, nullptr, nullptr, scene->refracts);
+                ff_launch_trace_queue(ctx, bvh, w.sh_rays, w.ctr + C_SH, 3ull * P, nullptr, true, tctr + 1, ws->err,
+                                      w.sh_tag, occ, ws->side, false, defer ? kDeferShadowBlocks : 0);
+                if (defer) {
+                    FF_CUDA_CHECK(cudaEventRecord(ws->sh_done[par], ws->side));
+                } else {
+                    FF_CUDA_CHECK(cudaEventRecord(ws->join, ws->side));
+                    FF_CUDA_CHECK(cudaStreamWaitEvent(stream, ws->join, 0));
+                }
             }
             ++frames;
         }
@@ -893,6 +1063,18 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
         active = *h_active;
     }
     if (active) throw FFError{FF_ERR_INTERNAL, "wavefront did not finish within its frame bound"};
+    if (defer) {
+        // the light terms of the last two frames, once their any-hit traces are done
+        if (!profile) {
+            FF_CUDA_CHECK(cudaStreamWaitEvent(stream, ws->sh_done[0], 0));
+            FF_CUDA_CHECK(cudaStreamWaitEvent(stream, ws->sh_done[1], 0));
+        }
+        for (uint32_t f = frames; f < frames + 2; ++f) {
+            set_frame(f);
+            k_flush_pending<<<(P + 255) / 256, 256, 0, stream>>>(w);
+        }
+        FF_CUDA_CHECK(cudaGetLastError());
+    }
     // cache answers join their slots' sums before the film update
     if (hook) {
         if (hook->wait_before_query) FF_CUDA_CHECK(cudaStreamWaitEvent(stream, hook->wait_before_query, 0));
@@ -919,10 +1101,11 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
         stats->shadow_nodes = fetch[2];
         stats->shadow_tris = fetch[3];
         if (profile) {
-            // 5 marks per frame: logic | shade | trace ext | trace shadow
+            // marks per frame: reset | logic | shade | trace ext | trace shadow
+            const size_t per = 5;
             float t[4] = {0.f, 0.f, 0.f, 0.f};
-            for (size_t f = 0; f + 4 < evs.size() + 1 && f + 4 <= evs.size(); f += 5) {
-                for (int k = 0; k < 4; ++k) {
+            for (size_t f = 0; f + per <= evs.size(); f += per) {
+                for (size_t k = 0; k + 1 < per; ++k) {
                     float x = 0.f;
                     cudaEventElapsedTime(&x, evs[f + k], evs[f + k + 1]);
                     t[k] += x;
@@ -935,7 +1118,7 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
         }
         for (auto e : evs) cudaEventDestroy(e);
         // profiled renders add the two counting passes per frame
-        stats->kernel_launches = frames * (3u + (uint32_t)n_kinds + (profile ? 2u : 0u)) + 2u;
+        stats->kernel_launches = frames * (3u + (uint32_t)n_kinds + (profile ? 2u : 0u)) + 2u + (defer ? 2u : 0u);
         stats->extension_rays = totals[0];
         stats->shadow_rays = totals[1];
         stats->samples = (uint64_t)st->spp * WH;
@@ -1019,6 +1202,11 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
     w.rough_threshold = 0.f;
     w.queries = nullptr;
     w.n_queries = nullptr;
+    // no deferred light terms: the replay needs each vertex's answers at the next frame
+    w.defer = w.par = w.frame = 0u;
+    w.ctr = ws->ctr_base;
+    w.sh_rays = ws->sh_rays_base[0];
+    w.sh_tag = ws->sh_tag_base[0];
     w.d_image = t.d_image;
     w.inv_spp = 1.f / (float)st->spp;
     w.adj_texture = t.texture;
