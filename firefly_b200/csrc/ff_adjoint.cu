@@ -388,7 +388,10 @@ void ff_adjoint_render(ff_context* ctx, ff_scene* scene, const ff_render_setting
     const size_t ntex = ad->texture >= 0 ? (size_t)3 * texels(ad->texture) : 0;
     const size_t nrough = rough ? (size_t)3 * texels(ad->roughness_texture) : 0;
     const size_t nenv = (size_t)3 * scene->env.width * scene->env.height;
-    DevBuf dimg, gtex, genv, grough, ctr;
+    // staging of host buffers and the counters, kept on the context between
+    // calls (calls on one context are externally synchronised)
+    DevBuf &dimg = ctx->adj_io[0], &gtex = ctx->adj_io[1], &genv = ctx->adj_io[2], &grough = ctx->adj_io[3],
+           &ctr = ctx->adj_io[4];
     const float* d_image = ad->d_image;
     float* g_tex = ad->grad_texture;
     float* g_env = ad->grad_env;

@@ -115,6 +115,7 @@ ff_status ff_context_destroy(ff_context* ctx)
         ctx->counters.release();
         ctx->io_rays.release();
         ctx->io_hits.release();
+        for (auto& b : ctx->adj_io) b.release();
         if (ctx->ev0) cudaEventDestroy(ctx->ev0);
         if (ctx->ev1) cudaEventDestroy(ctx->ev1);
         ff_wavefront_ws_free(ctx->adj_ws);

@@ -99,6 +99,7 @@ struct ff_context {
     std::string last_error;
     DevBuf counters;      // small scratch of uint32 counters for persistent kernels
     DevBuf io_rays, io_hits;  // staging for host-pointer ff_trace calls
+    DevBuf adj_io[5];         // ff_render_adjoint: staged image, texture / env / roughness gradients, counters
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     FFWavefrontWS* adj_ws = nullptr;   // path pool of ff_render_adjoint, kept between calls
     // resident blocks per SM of each queue-driven k_trace variant on this
