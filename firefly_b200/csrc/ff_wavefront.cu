@@ -108,9 +108,11 @@ static_assert(sizeof(SlotRay) == 32 && sizeof(SlotShade) == 32 && sizeof(SlotMis
                   sizeof(SlotPend) == 64,
               "slot records are whole 32-byte sectors");
 constexpr uint32_t kStampBase = 16;
-// Deferred mode: blocks per SM of the any-hit trace (its persistent grid),
-// leaving the rest of each SM to k_logic and k_shade of the next frame.
-constexpr int kDeferShadowBlocks = 4;   // stamps of real frames are >= 16; 0 marks an empty record
+// Deferred mode: blocks per SM of the any-hit trace (its persistent grid, of
+// 8 that fit), leaving the rest of each SM to k_logic and k_shade of the next
+// frame.  Measured on the 1.3M-triangle scene at 64 spp: 3 blocks 262.7 ms
+// per step, 4: 265.4-266.0, 5: 268.7, 6: 272.7.
+constexpr int kDeferShadowBlocks = 3;   // stamps of real frames are >= 16; 0 marks an empty record
 constexpr uint32_t kVtxMatBits = 24, kVtxLenShift = 24, kVtxLenMask = 0x7f;
 // Byte of shadow ray k's answer for slot s in the SlotRay array (the tag the
 // any-hit trace writes to): the low three bytes of the vis word.
