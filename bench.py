@@ -88,8 +88,8 @@ SHADOW_QUEUE_BYTES = 36
 # of each render stage: ncu over every launch of one timed 16-spp C2 step on
 # a 2,097,152-slot pool (104 frames), divided by the step's units (consumed
 # hits, shaded vertices, extension rays, shadow rays).
-RENDER_DRAM_BYTES_PER_UNIT = {"k_logic": 456.5, "k_shade (all kinds)": 418.5,
-                              "k_trace<closest> (extension queue)": 117.4, "k_trace<any> (shadow queue)": 54.8}
+RENDER_DRAM_BYTES_PER_UNIT = {"k_logic": 456.8, "k_shade (all kinds)": 418.7,
+                              "k_trace<closest> (extension queue)": 109.4, "k_trace<any> (shadow queue)": 48.5}
 RENDER = dict(width=1920, height=1080, spp=64, max_depth=8, rr_depth=3)
 # Measured DRAM bytes per unit of the adjoint's stages (ncu over the profiled
 # 512x512, 16-spp adjoint call of --workload inverse, 12 frames): per
