@@ -206,6 +206,19 @@ class dScene:
         _check(lib().ff_scene_get_stats(self.handle, C.byref(st)), self.ctx.handle)
         return {k: (list(getattr(st, k)) if k.startswith("scene_") else getattr(st, k)) for k, _ in st._fields_}
 
+    def read_bvh(self) -> tuple[np.ndarray, np.ndarray]:
+        """The 8-wide BVH as ff_trace walks it (ff_scene_read_bvh): node records
+        (num_nodes x 80 bytes, uint8) and triangle records in leaf order
+        (num_tris x 48 bytes, uint8)."""
+        nn, nt = C.c_uint32(), C.c_uint32()
+        _check(lib().ff_scene_read_bvh(self.handle, None, 0, None, 0, C.byref(nn), C.byref(nt)), self.ctx.handle)
+        nodes = np.empty((nn.value, 80), np.uint8)
+        tris = np.empty((nt.value, 48), np.uint8)
+        _check(lib().ff_scene_read_bvh(self.handle, C.c_void_p(nodes.ctypes.data), nodes.nbytes,
+                                       C.c_void_p(tris.ctypes.data), tris.nbytes, C.byref(nn), C.byref(nt)),
+               self.ctx.handle)
+        return nodes, tris
+
     def trace(self, rays: np.ndarray, any_hit: bool = False, out: np.ndarray | None = None,
               two_sided: bool = False) -> np.ndarray:
         """Host rays (n x 8 float32 or RAY_DTYPE) -> host hits (HIT_DTYPE).

@@ -162,6 +162,7 @@ SIGNATURES = {
     "ff_film_tonemap": (C.c_int, [P, C.c_float, P, C.c_uint32]),
     "ff_render": (C.c_int, [P, P, C.POINTER(ff_render_settings), P, C.POINTER(ff_render_stats)]),
     "ff_scene_read_env_tables": (C.c_int, [P, P, P, P, P]),
+    "ff_scene_read_bvh": (C.c_int, [P, P, C.c_uint64, P, C.c_uint64, P, P]),
     "ff_render_adjoint": (C.c_int, [P, P, C.POINTER(ff_render_settings), C.POINTER(ff_adjoint_desc),
                                     C.POINTER(ff_render_stats)]),
     "ff_scene_set_texture": (C.c_int, [P, C.c_uint32, P, C.c_uint32]),

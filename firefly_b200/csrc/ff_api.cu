@@ -230,6 +230,24 @@ ff_status ff_scene_get_stats(const ff_scene* s, ff_scene_stats* out)
     return FF_OK;
 }
 
+ff_status ff_scene_read_bvh(const ff_scene* s, void* nodes, uint64_t nodes_capacity, void* tris,
+                            uint64_t tris_capacity, uint32_t* num_nodes, uint32_t* num_tris)
+{
+    if (!s) return FF_ERR_INVALID_ARG;
+    ff_context* ctx = s->ctx;
+    return guarded(ctx, [&] {
+        DeviceGuard g(ctx->device);
+        if (num_nodes) *num_nodes = s->num_nodes;
+        if (num_tris) *num_tris = s->num_tris;
+        const uint64_t nb = (uint64_t)sizeof(FFNode8) * s->num_nodes, tb = (uint64_t)sizeof(FFTri) * s->num_tris;
+        FF_REQUIRE(!nodes || nodes_capacity >= nb, "node buffer smaller than num_nodes * 80 bytes");
+        FF_REQUIRE(!tris || tris_capacity >= tb, "triangle buffer smaller than num_tris * 48 bytes");
+        if (nodes && nb) FF_CUDA_CHECK(cudaMemcpyAsync(nodes, s->nodes.ptr, nb, cudaMemcpyDeviceToHost, ctx->stream));
+        if (tris && tb) FF_CUDA_CHECK(cudaMemcpyAsync(tris, s->tris.ptr, tb, cudaMemcpyDeviceToHost, ctx->stream));
+        FF_CUDA_CHECK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
 ff_status ff_trace(ff_context* ctx, const ff_scene* s, const ff_ray* rays, uint64_t n, ff_hit* hits,
                    uint32_t flags)
 {

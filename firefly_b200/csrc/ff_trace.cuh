@@ -112,7 +112,9 @@ FF_D void ff_intersect_node(const FFNode8* __restrict__ nodes, uint32_t idx, con
     const uint32_t fy0 = r.inv.y >= 0.f ? n4.x : n2.z, fy1 = r.inv.y >= 0.f ? n4.y : n2.w;
     const uint32_t nz0 = r.inv.z >= 0.f ? n3.x : n4.z, nz1 = r.inv.z >= 0.f ? n3.y : n4.w;
     const uint32_t fz0 = r.inv.z >= 0.f ? n4.z : n3.x, fz1 = r.inv.z >= 0.f ? n4.w : n3.y;
-    const float tb = r.tmax + fabsf(r.tmax) * FF_BOX_WIDEN;
+    // the widening as explicit fused multiply-adds: the same result in every
+    // translation unit, whatever its contraction setting (-fmad)
+    const float tb = __fmaf_rn(fabsf(r.tmax), FF_BOX_WIDEN, r.tmax);
     // x and y in packed FP32: one add removes 2^23 from two plane bytes and
     // one fma gives two slab distances (the same IEEE operations per lane as
     // fmaf, so the same values); z in scalar fmaf
@@ -130,8 +132,8 @@ FF_D void ff_intersect_node(const FFNode8* __restrict__ nodes, uint32_t idx, con
         const float tfz = fmaf(qz.y, az, bz);
         float tn = fmax3f(tnxy.x, tnxy.y, tnz);
         float tf = fmin3f(tfxy.x, tfxy.y, tfz);
-        tn = tn - fabsf(tn) * FF_BOX_WIDEN;
-        tf = tf + fabsf(tf) * FF_BOX_WIDEN;
+        tn = __fmaf_rn(-fabsf(tn), FF_BOX_WIDEN, tn);
+        tf = __fmaf_rn(fabsf(tf), FF_BOX_WIDEN, tf);
         // an empty slot (meta 0, not internal) adds nothing even where its
         // degenerate box is hit, so no occupancy test is needed
         if (fmaxf(tn, r.tmin) <= fminf(tf, tb)) {

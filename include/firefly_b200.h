@@ -413,6 +413,20 @@ FF_API ff_status ff_optimizer_adam_step(ff_context* ctx, float* param, const flo
 FF_API ff_status ff_scene_read_env_tables(const ff_scene* scene, double* marginal, double* conditional,
                                    float* pdf, double* pdf_denom);
 
+/* No counterpart in the reference: the scene's 8-wide BVH as ff_trace walks
+ * it, copied to host memory for inspection and tests.  nodes receives
+ * *num_nodes records of 80 bytes: origin (3 floats), three biased exponents
+ * and the internal-child mask (4 bytes), the first internal child and the
+ * first triangle (2 uint32), per slot a meta byte (0 empty; internal 0x20 |
+ * 24 + slot; leaf: unary triangle count << 5 | offset from the first
+ * triangle), then the quantised planes lo x, y, z and hi x, y, z (8 bytes
+ * each).  tris receives *num_tris records of 48 bytes in leaf order: v0 with
+ * the original index as the fourth word's bits, e1 = v1 - v0, e2 = v2 - v0
+ * (each padded to 4 floats).  With nodes or tris NULL only the counts are
+ * written; a capacity (bytes) below the size returns FF_ERR_INVALID_ARG. */
+FF_API ff_status ff_scene_read_bvh(const ff_scene* scene, void* nodes, uint64_t nodes_capacity, void* tris,
+                                   uint64_t tris_capacity, uint32_t* num_nodes, uint32_t* num_tris);
+
 /* ------------------------------------------------------------------------
  * Learned radiance cache (no counterpart in the reference).  A multiresolution
  * hash grid (FF_CACHE_LEVELS levels x 2 features, 2^log2_table_size entries per

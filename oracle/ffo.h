@@ -36,6 +36,14 @@ int ffo_intersect_two_sided(const float* v0, const float* v1, const float* v2,
 /* dTriangle::shadow_hit (dTriangle.cu:110-138): two-sided, u/v in double. */
 int ffo_shadow_hit(const float* v0, const float* v1, const float* v2,
                    const float* o, const float* d, float* t);
+/* The same three tests on v0 and the edges e1 = v1 - v0, e2 = v2 - v0 as the
+ * reference rounds them (the device BVH stores the edges). */
+int ffo_intersect_cull_e(const float* v0, const float* e1, const float* e2,
+                         const float* o, const float* d, float* t, float* u, float* v);
+int ffo_intersect_two_sided_e(const float* v0, const float* e1, const float* e2,
+                              const float* o, const float* d, float* t, float* u, float* v, int* back);
+int ffo_shadow_hit_e(const float* v0, const float* e1, const float* e2,
+                     const float* o, const float* d, float* t);
 
 /* Brute-force ray queries over a triangle soup (tris: n_tris x 9 floats,
  * v0 v1 v2).  rays: n x 8 floats (o, tmin, d, tmax) as ff_ray.  hits: n x 4
@@ -56,6 +64,18 @@ ffo_bvh* ffo_bvh_build(const float* tris, int64_t n_tris);   /* keeps a pointer 
 void ffo_bvh_free(ffo_bvh* b);
 void ffo_bvh_trace(const ffo_bvh* b, const float* rays, int64_t n, void* hits, int any, int two_sided,
                    int nthreads);
+
+/* The device's own traversal restated (ffo_bvh8.c): the 8-wide quantised BVH
+ * that ff_scene_read_bvh returns (nodes: num_nodes x 80-byte FFNode8, tris:
+ * num_tris x 48-byte FFTri in leaf order) walked exactly as ff_traverse_step
+ * walks it, with the same box arithmetic, child order, stack and triangle
+ * tests.  hits as ffo_trace_brute2 (two_sided: a ray with the sign bit of tmin
+ * set takes back faces, as the device's two-sided launches mark them);
+ * counts[0] += node records fetched, counts[1] += triangles tested (ff_trace_count).
+ * Returns the number of rays whose traversal overflowed its stack or step bound. */
+int64_t ffo_bvh8_trace(const void* nodes, uint32_t num_nodes, const void* tris, uint32_t num_tris,
+                       const float* rays, int64_t n, void* hits, int any, int two_sided,
+                       uint64_t* counts, int nthreads);
 
 /* ---- sampler (dRandom.cu:10-27) ---- */
 uint32_t ffo_wang_hash(uint32_t s);

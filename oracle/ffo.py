@@ -47,6 +47,8 @@ def load() -> C.CDLL:
         lib.ffo_bvh_free.argtypes = [P]
         lib.ffo_bvh_trace.restype = None
         lib.ffo_bvh_trace.argtypes = [P, P, C.c_int64, P, C.c_int, C.c_int, C.c_int]
+        lib.ffo_bvh8_trace.restype = C.c_int64
+        lib.ffo_bvh8_trace.argtypes = [P, C.c_uint32, P, C.c_uint32, P, C.c_int64, P, C.c_int, C.c_int, P, C.c_int]
         lib.ffo_intersect_two_sided.restype = C.c_int
         lib.ffo_intersect_two_sided.argtypes = [P] * 9
         lib.ffo_probe_dielectric.restype = None
@@ -116,6 +118,22 @@ class BVH:
             self.close()
         except Exception:
             pass
+
+
+def bvh8_trace(nodes: np.ndarray, tris: np.ndarray, rays: np.ndarray, any_hit: bool = False,
+               two_sided: bool = False, threads: int | None = None):
+    """The device traversal restated (ffo_bvh8.c) over a BVH read back with
+    ff_scene_read_bvh: (hits as HIT_DTYPE, node records fetched, triangles
+    tested, rays whose traversal overflowed)."""
+    nodes = np.ascontiguousarray(nodes, np.uint8)
+    tris = np.ascontiguousarray(tris, np.uint8)
+    assert nodes.size % 80 == 0 and tris.size % 48 == 0
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    out = np.empty(rays.shape[0], HIT_DTYPE)
+    counts = np.zeros(2, np.uint64)
+    errors = load().ffo_bvh8_trace(_p(nodes), nodes.size // 80, _p(tris), tris.size // 48, _p(rays), rays.shape[0],
+                                   _p(out), int(any_hit), int(two_sided), _p(counts), threads or os.cpu_count() or 1)
+    return out, int(counts[0]), int(counts[1]), int(errors)
 
 
 def intersect_two_sided(v0, v1, v2, o, d):

@@ -35,12 +35,13 @@ static inline v3 cross(v3 a, v3 b)
     return r;
 }
 
-int ffo_intersect_cull(const float* p0, const float* p1, const float* p2,
-                       const float* po, const float* pd, float* t, float* u, float* v)
+/* The tests below on the vertex v0 and the edges e1 = v1 - v0, e2 = v2 - v0
+ * as the reference rounds them (dTriangle.cu:35-36); the *_e forms take the
+ * edges directly (the device BVH stores them, ffo_bvh8.c). */
+int ffo_intersect_cull_e(const float* p0, const float* pe1, const float* pe2,
+                         const float* po, const float* pd, float* t, float* u, float* v)
 {
-    v3 v0 = mk(p0), v1 = mk(p1), v2 = mk(p2), o = mk(po), d = mk(pd);
-    v3 e1 = sub(v1, v0);
-    v3 e2 = sub(v2, v0);
+    v3 v0 = mk(p0), e1 = mk(pe1), e2 = mk(pe2), o = mk(po), d = mk(pd);
     v3 pvec = cross(d, e2);
     double det = dot(e1, pvec);             /* float dot widened to double */
     if (det < FFO_K_EPSILON) return 0;      /* K_EPSILON is a float constant */
@@ -60,18 +61,24 @@ int ffo_intersect_cull(const float* p0, const float* p1, const float* p2,
     return 1;
 }
 
+int ffo_intersect_cull(const float* p0, const float* p1, const float* p2,
+                       const float* po, const float* pd, float* t, float* u, float* v)
+{
+    v3 v0 = mk(p0), v1 = mk(p1), v2 = mk(p2);
+    v3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+    return ffo_intersect_cull_e(p0, &e1.x, &e2.x, po, pd, t, u, v);
+}
+
 /* Two-sided closest-hit test (no reference counterpart: the reference only
  * culls, dTriangle.cu:5,41).  A front face (det >= K_EPSILON) is exactly
  * ffo_intersect_cull; a back face (det <= -K_EPSILON) runs the same test on
  * the negated determinant and numerators (negation is exact), the mirror
  * image of the culling test.  *back reports which.  The product restates it
  * in ff_test_tri_closest<TWO> (firefly_b200/csrc/ff_trace.cuh). */
-int ffo_intersect_two_sided(const float* p0, const float* p1, const float* p2,
-                            const float* po, const float* pd, float* t, float* u, float* v, int* back)
+int ffo_intersect_two_sided_e(const float* p0, const float* pe1, const float* pe2,
+                              const float* po, const float* pd, float* t, float* u, float* v, int* back)
 {
-    v3 v0 = mk(p0), v1 = mk(p1), v2 = mk(p2), o = mk(po), d = mk(pd);
-    v3 e1 = sub(v1, v0);
-    v3 e2 = sub(v2, v0);
+    v3 v0 = mk(p0), e1 = mk(pe1), e2 = mk(pe2), o = mk(po), d = mk(pd);
     v3 pvec = cross(d, e2);
     float detf = dot(e1, pvec);
     float sg = 1.f;
@@ -96,12 +103,18 @@ int ffo_intersect_two_sided(const float* p0, const float* p1, const float* p2,
     return 1;
 }
 
-int ffo_shadow_hit(const float* p0, const float* p1, const float* p2,
-                   const float* po, const float* pd, float* t)
+int ffo_intersect_two_sided(const float* p0, const float* p1, const float* p2,
+                            const float* po, const float* pd, float* t, float* u, float* v, int* back)
 {
-    v3 v0 = mk(p0), v1 = mk(p1), v2 = mk(p2), o = mk(po), d = mk(pd);
-    v3 e1 = sub(v1, v0);
-    v3 e2 = sub(v2, v0);
+    v3 v0 = mk(p0), v1 = mk(p1), v2 = mk(p2);
+    v3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+    return ffo_intersect_two_sided_e(p0, &e1.x, &e2.x, po, pd, t, u, v, back);
+}
+
+int ffo_shadow_hit_e(const float* p0, const float* pe1, const float* pe2,
+                     const float* po, const float* pd, float* t)
+{
+    v3 v0 = mk(p0), e1 = mk(pe1), e2 = mk(pe2), o = mk(po), d = mk(pd);
     v3 pvec = cross(d, e2);
     double det = dot(e1, pvec);
     if (det > -FFO_K_EPSILON && det < FFO_K_EPSILON) return 0;
@@ -116,6 +129,14 @@ int ffo_shadow_hit(const float* p0, const float* p1, const float* p2,
     *t = tt;
     if (tt < 0) return 0;
     return 1;
+}
+
+int ffo_shadow_hit(const float* p0, const float* p1, const float* p2,
+                   const float* po, const float* pd, float* t)
+{
+    v3 v0 = mk(p0), v1 = mk(p1), v2 = mk(p2);
+    v3 e1 = sub(v1, v0), e2 = sub(v2, v0);
+    return ffo_shadow_hit_e(p0, &e1.x, &e2.x, po, pd, t);
 }
 
 typedef struct {

@@ -338,3 +338,45 @@ def test_at_scale_mesh_bit_exact(ctx, oracle):
     finally:
         bvh.close()
         ds.close()
+
+
+def test_traversal_pinned_by_oracle_restatement(ctx, oracle):
+    """ff_trace_count's node and triangle counts, and ff_trace's answers, against
+    the oracle's restatement of the device traversal (oracle/ffo_bvh8.c: the
+    same box arithmetic, child order, stack and triangle tests) over the BVH
+    read back from the device (ff_scene_read_bvh): the counts are equal ray
+    set by ray set, closest hits bit for bit, and any-hit answers report the
+    same occluder at the same t (the same traversal order finds it first)."""
+    import firefly_b200 as ff
+    for name, scn in (("room", scenes.small_room(seed=0)),
+                      ("sphere in room", scenes.displaced_icosphere(subdiv=6, width=320, height=180,
+                                                                    env_w=64, env_h=32))):
+        ds = ff.dScene(ctx, scn)
+        try:
+            nodes, tris = ds.read_bvh()
+            st = ds.stats()
+            assert nodes.shape == (st["num_nodes"], 80) and tris.shape == (st["num_triangles"], 48)
+            rng = np.random.default_rng(61)
+            sets = [("incoherent", scenes.incoherent_rays(scn, 200_000, seed=62), False, False),
+                    ("camera", scenes.camera_rays(scn, 320, 180), False, False),
+                    ("any", scenes.with_random_tmax(scenes.incoherent_rays(scn, 200_000, seed=63), scn, seed=64),
+                     True, False)]
+            inside = scenes.incoherent_rays(scn, 100_000, seed=65)
+            P = np.asarray(scn.positions, np.float64)[24:] if name != "room" else np.asarray(scn.positions)
+            inside[:, 0:3] = (P.mean(0) + rng.normal(size=(len(inside), 3)) * 0.2).astype(np.float32)
+            sets.append(("two-sided", inside, False, True))
+            for label, rays, any_hit, two in sets:
+                got = ds.trace(rays, any_hit=any_hit, two_sided=two)
+                cnt = ds.trace_count(rays, any_hit=any_hit, two_sided=two)
+                ref, n_nodes, n_tris, errors = oracle.bvh8_trace(nodes, tris, rays, any_hit=any_hit,
+                                                                 two_sided=two, threads=cpu_threads())
+                assert errors == 0
+                assert (cnt["nodes"], cnt["tris"]) == (n_nodes, n_tris), (name, label, cnt, n_nodes, n_tris)
+                bad = got["prim"] != ref["prim"]
+                for f in ("t", "u", "v"):
+                    bad |= got[f].view(np.uint32) != ref[f].view(np.uint32)
+                assert int(bad.sum()) == 0, (name, label, int(bad.sum()), got[np.argmax(bad)], ref[np.argmax(bad)])
+                print(f"[trace] {name}, {label}: {n_nodes / len(rays):.3f} nodes, {n_tris / len(rays):.3f} "
+                      f"triangles per ray, equal on the device and in the restatement")
+        finally:
+            ds.close()
