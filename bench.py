@@ -553,7 +553,9 @@ def trace_line(args, ws, rank, local, dist, ctx, dev, stream, steps):
                     "frac_of_l2_read": (None if l2_ref is None else
                                         round(fetch[batches[k_dom][0]]["achieved_fetch_gbs"] / l2_ref, 4)),
                     "node_bytes": wk["node_bytes"], "tri_bytes": wk["tri_bytes"],
-                    "note": ("fetched bytes = node records x node bytes + triangles tested x triangle bytes per ray; "
+                    "note": ("fetched bytes = node records x node bytes + triangles tested x triangle bytes per ray "
+                             "(the device traversal's counts, equal to the oracle's restatement of it: "
+                             "tests/test_trace_gpu.py); "
                              "l2_read_gbs = a probe kernel reading a 32 MiB L2-resident buffer 40 times (L1 bypassed); "
                              "the traversal's fetches are partly served by L1, so the fraction is an upper bound "
                              "on its L2 load")}
@@ -760,9 +762,10 @@ def run_render(args, ws, rank, local, dist):
         l2_fetch = {"stages": l2_fetch, "l2_read_gbs": None if l2_ref is None else round(l2_ref, 1),
                     "node_bytes": NODE_BYTES, "tri_bytes": TRI_BYTES,
                     "note": ("fetched bytes = 8-wide node records x node bytes + triangles tested x triangle bytes, "
-                             "counted over the profiled step's queues; l2_read_gbs = a probe kernel reading a 32 MiB "
-                             "L2-resident buffer 40 times (L1 bypassed); part of the fetches hit L1, so the fraction "
-                             "is an upper bound on the L2 load")}
+                             "counted over the profiled step's queues by the device traversal, whose counts equal "
+                             "the oracle's restatement of it (tests/test_trace_gpu.py); l2_read_gbs = a probe kernel "
+                             "reading a 32 MiB L2-resident buffer 40 times (L1 bypassed); part of the fetches hit "
+                             "L1, so the fraction is an upper bound on the L2 load")}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,

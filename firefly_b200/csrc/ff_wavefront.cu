@@ -1120,7 +1120,9 @@ void ff_wavefront_render(ff_context* ctx, ff_scene* scene, const ff_render_setti
         }
         for (auto e : evs) cudaEventDestroy(e);
         // profiled renders add the two counting passes per frame
-        stats->kernel_launches = frames * (3u + (uint32_t)n_kinds + (profile ? 2u : 0u)) + 2u + (defer ? 2u : 0u);
+        // per frame: counter reset, logic, one shade per kind, two traces
+        // (+ two counting passes when profiled); init and resolve; the flush
+        stats->kernel_launches = frames * (4u + (uint32_t)n_kinds + (profile ? 2u : 0u)) + 2u + (defer ? 2u : 0u);
         stats->extension_rays = totals[0];
         stats->shadow_rays = totals[1];
         stats->samples = (uint64_t)st->spp * WH;
@@ -1308,7 +1310,7 @@ void ff_wavefront_adjoint(ff_context* ctx, ff_scene* scene, const ff_render_sett
     }
     for (auto e : evs) cudaEventDestroy(e);
     if (stats) {
-        stats->kernel_launches = frames * (3u + (uint32_t)n_kinds) + 1u;
+        stats->kernel_launches = frames * (4u + (uint32_t)n_kinds) + 1u;   // counter reset, logic, shades, traces; init
         stats->extension_rays = totals[0];
         stats->shadow_rays = totals[1];
         stats->frames = frames;
