@@ -48,7 +48,9 @@ namespace {
 using namespace ffp;
 using namespace ffadj;
 constexpr int kKinds = 5;
-constexpr uint32_t PH_START = 0, PH_FLIGHT = 1, PH_DONE = 2;
+// PH_DRAINED (deferred mode): finished, and the last pending light terms
+// added, so later frames skip the slot without reading its records.
+constexpr uint32_t PH_START = 0, PH_FLIGHT = 1, PH_DONE = 2, PH_DRAINED = 3;
 
 // Path-pool size when ff_render_settings.max_paths is 0: m slots per pixel,
 // m = min(spp, this / (w*h)), at least 1.  Measured on the 1.3M-triangle
@@ -506,13 +508,15 @@ __global__ void __launch_bounds__(256) k_logic(WF w)
                 const uint32_t qi = warp_append(w.n_queries, query, nullptr);
                 if (query) w.queries[qi] = rec;
             }
-        } else if (!ADJ && w.defer) {
-            // a finished slot: the light terms of its last vertex may still be pending
+        } else if (!ADJ && w.defer && ph == PH_DONE) {
+            // a slot that finished in the previous frame: the light terms of its
+            // last vertex (shaded two frames ago) are the only ones still pending
             float4 acc = w.acc[s], accc = w.acc_c[s];
             if (consume_pending(w, s, acc, accc)) {
                 w.acc[s] = acc;
                 w.acc_c[s] = accc;
             }
+            w.phase[s] = PH_DRAINED;
         }
     }
     // compaction into the extension queue and the material queues
