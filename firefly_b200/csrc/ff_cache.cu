@@ -87,7 +87,7 @@ __device__ void encode_half(const Grid& g, const Record& rec, bool valid, uint32
     float f[32];
     if (valid) {
         const float3 p = normalised_pos(g, rec.px, rec.py, rec.pz);
-#pragma unroll 2
+#pragma unroll   // all 8 levels' loads in flight (78 registers, no spills; query stage 2.39 -> 2.30 ms / 4 frames)
         for (int j = 0; j < 8; ++j) {
             const float2 e = level_feature(g, 8 * (int)h + j, p);
             f[2 * j] = e.x;
