@@ -179,6 +179,7 @@ SIGNATURES = {
     "ff_debug_alloc_stats": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_int64)]),
     "ff_debug_fail_alloc_after": (C.c_int, [C.c_int64]),
     "ff_debug_cache_wait_limit": (C.c_int, [P, C.c_uint32]),
+    "ff_debug_env_pick": (C.c_int, [P, P, C.c_uint64, P]),
 }
 
 _lib = None

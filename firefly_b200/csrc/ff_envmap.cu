@@ -5,12 +5,18 @@
 // (CUDA-RayTracer/kernel.cu:65-149), which run as single-thread <<<1,1>>>
 // loops (and one thread per row) over every texel.  Same tables, same FP64
 // accumulation and the same luminance of the bilinear fetch at each texel's
-// corner (u = i/w, v = j/h); the sums are reassociated into per-row block
-// reductions and block scans:
+// corner (u = i/w, v = j/h); the sums over whole rows are reassociated into
+// block reductions, while the CDFs are the reference's running sums (one
+// thread along each row, and along the marginal), so that every CDF is sorted
+// by construction (a scan's tree of partial sums can leave two neighbours one
+// ulp out of order):
 //   k_env_rows      one block per row: luminance of every texel, row sum
-//   k_env_marginal  one block: pdf denominator, marginal pdf and CDF (scan)
-//   k_env_cond      one block per row: conditional CDF (block scan) and the
-//                   pdf texture lum * sin(pi v) / denom * w*h / (2 pi^2)
+//   k_env_marginal  one block: pdf denominator, marginal pdf and CDF
+//   k_env_cond      one block per row: the pdf texture lum * sin(pi v) /
+//                   denom * w*h / (2 pi^2) (all threads) and the conditional
+//                   CDF (one running sum)
+//   k_env_guide     one block per CDF: the guide table of its searches
+//                   (kGuideFull, ff_shade.cuh)
 // Traffic per texel: 12 B of RGB read (L2-resident neighbours for the
 // bilinear weights), 4 B luminance written and read back, 8 B CDF and 4 B pdf
 // written: HBM-bound at about 28 B per texel.
@@ -57,10 +63,8 @@ __global__ void __launch_bounds__(kEnvBlock) k_env_marginal(const double* __rest
                                                             double* __restrict__ marginal_y, double* __restrict__ denom)
 {
     using Reduce = cub::BlockReduce<double, kEnvBlock>;
-    using Scan = cub::BlockScan<double, kEnvBlock>;
     __shared__ union {
         typename Reduce::TempStorage r;
-        typename Scan::TempStorage s;
     } tmp;
     __shared__ double s_denom;
     // pdf denominator: sum_j sum_i lum_ij * sin(pi v_j)
@@ -70,23 +74,18 @@ __global__ void __launch_bounds__(kEnvBlock) k_env_marginal(const double* __rest
     if (threadIdx.x == 0) s_denom = d;
     __syncthreads();
     const double dn = s_denom;
-    // marginal pdf and its inclusive scan, in chunks of kEnvBlock rows
-    double carry = 0.0;
-    for (int base = 0; base < h; base += kEnvBlock) {
-        const int j = base + threadIdx.x;
-        double mp = 0.0;
-        if (j < h) {
-            mp = row_sum[j] * (row_sin(j, h) / dn);
-            marginal_p[j] = mp;
+    // marginal pdf, then its CDF as the reference sums it:
+    // marginal_y[j] = marginal_p[j] + marginal_y[j - 1]
+    for (int j = threadIdx.x; j < h; j += kEnvBlock) marginal_p[j] = row_sum[j] * (row_sin(j, h) / dn);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double run = 0.0;
+        for (int j = 0; j < h; ++j) {
+            run = j == 0 ? marginal_p[0] : marginal_p[j] + run;
+            marginal_y[j] = run;
         }
-        double incl;
-        double chunk_total;
-        Scan(tmp.s).InclusiveSum(mp, incl, chunk_total);
-        if (j < h) marginal_y[j] = carry + incl;
-        carry += chunk_total;
-        __syncthreads();
+        *denom = dn;
     }
-    if (threadIdx.x == 0) *denom = dn;
 }
 
 __global__ void __launch_bounds__(kEnvBlock) k_env_cond(const float* __restrict__ lum, int w, int h,
@@ -94,28 +93,59 @@ __global__ void __launch_bounds__(kEnvBlock) k_env_cond(const float* __restrict_
                                                         const double* __restrict__ denom, double* __restrict__ cond,
                                                         float* __restrict__ pdf)
 {
-    using Scan = cub::BlockScan<double, kEnvBlock>;
-    __shared__ typename Scan::TempStorage tmp;
     const int j = blockIdx.x;
     const double s = row_sin(j, h);
     const double dn = *denom;
     const double val = s / (dn * marginal_p[j]);
     const float scale = (float)(w * h) / (2.f * FF_PI * FF_PI);
-    // each thread owns one contiguous chunk of the row
-    const int chunk = (w + kEnvBlock - 1) / kEnvBlock;
-    const int i0 = min(w, (int)threadIdx.x * chunk), i1 = min(w, i0 + chunk);
     const float* row = lum + (size_t)j * w;
-    double local = 0.0;
-    for (int i = i0; i < i1; ++i) local += (double)row[i] * val;
-    double prefix;
-    Scan(tmp).ExclusiveSum(local, prefix);
-    double run = prefix;
-    for (int i = i0; i < i1; ++i) {
-        const double l = (double)row[i];
-        run += l * val;
-        cond[(size_t)j * w + i] = run;
-        float p = (float)((l * s) / dn);
+    for (int i = threadIdx.x; i < w; i += kEnvBlock) {
+        float p = (float)(((double)row[i] * s) / dn);
         pdf[(size_t)j * w + i] = p * scale;
+    }
+    // conds_y[y][x] = lum * val + conds_y[y][x - 1]: one dependent add per
+    // texel (about 2,000 per row), rows in parallel
+    if (threadIdx.x == 0) {
+        double run = 0.0;
+        double* c = cond + (size_t)j * w;
+        for (int i = 0; i < w; ++i) {
+            const double t = (double)row[i] * val;
+            run = i == 0 ? t : t + run;
+            c[i] = run;
+        }
+    }
+}
+
+// One block per CDF: blockIdx.x < h is conditional row blockIdx.x, h the
+// marginal.  Entry k of its guide = upper_bound of k / G, by the search loop
+// of upper_bound_ref; every entry kGuideFull when the list is not sorted.
+__global__ void __launch_bounds__(kEnvBlock) k_env_guide(const double* __restrict__ marginal,
+                                                         const double* __restrict__ cond, int w, int h,
+                                                         uint32_t* __restrict__ guide_m, uint32_t* __restrict__ guide_c)
+{
+    const int j = blockIdx.x;
+    const bool is_row = j < h;
+    const double* list = is_row ? cond + (size_t)j * w : marginal;
+    const int size = is_row ? w : h;
+    const int G = is_row ? kGuideCond : kGuideMarginal;
+    uint32_t* g = is_row ? guide_c + (size_t)j * (kGuideCond + 1) : guide_m;
+    int bad = 0;
+    for (int i = threadIdx.x; i < size; i += kEnvBlock)
+        bad |= (i + 1 < size) ? !(list[i] <= list[i + 1]) : !(list[i] == list[i]);
+    bad = __syncthreads_or(bad);
+    for (int k = threadIdx.x; k <= G; k += kEnvBlock) {
+        if (bad) {
+            g[k] = kGuideFull;
+            continue;
+        }
+        const float val = (float)k / (float)G;
+        int left = 0, right = size;
+        while (left < right) {
+            const int middle = (right - left) / 2 + left;
+            if ((double)val >= list[middle]) left = middle + 1;
+            else right = middle;
+        }
+        g[k] = (uint32_t)left;
     }
 }
 
@@ -162,9 +192,61 @@ void ff_build_env_tables(ff_context* ctx, ff_scene* s)
                                             e.denom.as<double>());
     k_env_cond<<<h, kEnvBlock, 0, st>>>(lum.as<float>(), w, h, mp.as<double>(), e.denom.as<double>(),
                                         e.conditional.as<double>(), e.pdf.as<float>());
+    e.guide.alloc(sizeof(uint32_t) * ((size_t)kGuideMarginal + 1 + (size_t)h * (kGuideCond + 1)));
+    k_env_guide<<<h + 1, kEnvBlock, 0, st>>>(e.marginal.as<double>(), e.conditional.as<double>(), w, h,
+                                             e.guide.as<uint32_t>(), e.guide.as<uint32_t>() + kGuideMarginal + 1);
     FF_CUDA_CHECK(cudaGetLastError());
     ff_env_pack(ctx, s);
     FF_CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
+namespace {
+
+__global__ void k_env_pick(FFEnvView e, const float2* __restrict__ exy, uint64_t n, int2* __restrict__ xy)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float ex = exy[i].x, ey = exy[i].y;
+    // the searches and clamps of env_sample / env_sample_corrected
+    int y = (int)((float)upper_bound_ref<kGuideMarginal>(e.marginal, e.height, ey, e.guide_m) - 1.f);
+    y = y < 0 ? 0 : (y >= e.height ? e.height - 1 : y);
+    int x = (int)((float)upper_bound_ref<kGuideCond>(e.cond + (size_t)y * e.width, e.width, ex, guide_row(e, y)) - 1.f);
+    x = x < 0 ? 0 : (x >= e.width ? e.width - 1 : x);
+    xy[i] = make_int2(x, y);
+}
+
+}  // namespace
+
+extern "C" ff_status ff_debug_env_pick(const ff_scene* scene, const float* exy, uint64_t n, int32_t* xy)
+{
+    if (!scene || (n && (!exy || !xy))) return FF_ERR_INVALID_ARG;
+    ff_context* ctx = scene->ctx;
+    if (scene->env.width == 0) {
+        ctx->last_error = "scene has no environment map";
+        return FF_ERR_INVALID_ARG;
+    }
+    if (n == 0) return FF_OK;
+    if (n > (1ull << 32)) {
+        ctx->last_error = "ff_debug_env_pick: more than 2^32 draws";
+        return FF_ERR_INVALID_ARG;
+    }
+    try {
+        FF_CUDA_CHECK(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        DevBuf d_in, d_out;
+        d_in.alloc(sizeof(float2) * n);
+        d_out.alloc(sizeof(int2) * n);
+        FF_CUDA_CHECK(cudaMemcpyAsync(d_in.ptr, exy, sizeof(float2) * n, cudaMemcpyHostToDevice, st));
+        k_env_pick<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ff_env_view(scene), d_in.as<float2>(), n,
+                                                                 d_out.as<int2>());
+        FF_CUDA_CHECK(cudaGetLastError());
+        FF_CUDA_CHECK(cudaMemcpyAsync(xy, d_out.ptr, sizeof(int2) * n, cudaMemcpyDeviceToHost, st));
+        FF_CUDA_CHECK(cudaStreamSynchronize(st));
+        return FF_OK;
+    } catch (const FFError& err) {
+        ctx->last_error = err.msg;
+        return err.status;
+    }
 }
 
 extern "C" ff_status ff_scene_read_env_tables(const ff_scene* scene, double* marginal, double* conditional, float* pdf,

@@ -155,6 +155,7 @@ struct FFEnvLight {
     DevBuf pdf;           // float[height*width]
     DevBuf denom;         // double
     DevBuf texel4;        // float4[height*width]: rgb and pdf packed for the path kernels
+    DevBuf guide;         // uint32: the marginal's search guide, then one per conditional row
 };
 
 struct ff_scene {

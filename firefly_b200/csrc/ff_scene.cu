@@ -215,6 +215,8 @@ FFEnvView ff_env_view(const ff_scene* s)
     e.rgb = s->env.rgb.as<float3>();
     e.marginal = s->env.marginal.as<double>();
     e.cond = s->env.conditional.as<double>();
+    e.guide_m = s->env.guide.as<uint32_t>();
+    e.guide_c = e.guide_m ? e.guide_m + kGuideMarginal + 1 : nullptr;
     e.pdf = s->env.pdf.as<float>();
     e.width = s->env.width;
     e.height = s->env.height;

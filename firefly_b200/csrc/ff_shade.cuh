@@ -477,10 +477,23 @@ FF_D float3 shading_normal(const ff_material& m, const FFTexView* tex, const FFT
     return normalize3(make_float3(o.x / w, o.y / w, o.z / w));
 }
 
+// Guide tables of the CDF searches (built with the tables, ff_envmap.cu):
+// for a list of n sorted entries and G buckets, entry k (0 <= k <= G) is
+// upper_bound of k / G, the first index whose entry exceeds k / G.  A value v
+// in [k / G, (k + 1) / G] has its upper_bound between entries k and k + 1,
+// so the search starts from that range instead of [0, n) and ends at the
+// same index (upper_bound is monotone in v).  A list that is not sorted
+// (or holds a NaN) has every entry kGuideFull: its searches run over [0, n).
+constexpr int kGuideMarginal = 1024;   // buckets of the marginal CDF
+constexpr int kGuideCond = 512;        // buckets of each conditional row
+constexpr uint32_t kGuideFull = 0x80000000u;
+
 struct FFEnvView {
     const float3* rgb;       // width*height texels, row y = v * height
     const double* marginal;  // marginal_y[height]
     const double* cond;      // conds_y[height][width] row-major
+    const uint32_t* guide_m;  // kGuideMarginal + 1 entries, or nullptr
+    const uint32_t* guide_c;  // height rows of kGuideCond + 1 entries, or nullptr
     const float* pdf;        // pdf texels, already scaled by w*h/(2 pi^2)
     int width, height;
     float3 color;            // constant colour when rgb == nullptr
@@ -526,9 +539,21 @@ FF_D float3 tex_bilinear(const T* texels, int w, int h, float u, float v)
 }
 
 // upper_bound (Helpers.cu:16-31), including its list[left <= val] index.
-FF_D int upper_bound_ref(const double* list, int size, float val)
+// With a guide table (see kGuideFull) the search starts from the bucket's
+// range; the index it ends at, and so the result, is the full search's.
+template <int G = 0>
+FF_D int upper_bound_ref(const double* list, int size, float val, const uint32_t* guide = nullptr)
 {
     int left = 0, right = size;
+    if (G > 0 && guide && val >= 0.f && val <= 1.f) {
+        // val * G is exact (G a power of two), so k / G <= val <= (k + 1) / G
+        const int k = min((int)(val * (float)G), G - 1);
+        const uint32_t a = guide[k], b = guide[k + 1];
+        if (!(a & kGuideFull)) {
+            left = (int)a;
+            right = (int)b;
+        }
+    }
     while (left < right) {
         int middle = (right - left) / 2 + left;
         if ((double)val >= list[middle]) left = middle + 1;
@@ -550,12 +575,17 @@ FF_D float3 env_L(const FFEnvView& e, float3 wi, bool corrected = false)
     return tex_bilinear(e.rgb, e.width, e.height, uv.x, uv.y);
 }
 
+FF_D const uint32_t* guide_row(const FFEnvView& e, int y)
+{
+    return e.guide_c ? e.guide_c + (size_t)y * (kGuideCond + 1) : nullptr;
+}
+
 // get_direction (dEnvironmentLight.cu:41-58); ex = first draw, ey = second.
 FF_D void env_sample(const FFEnvView& e, float3 pos, float ex, float ey, float3& wi, float3& sp)
 {
-    int y = (int)((float)upper_bound_ref(e.marginal, e.height, ey) - 1.f);
+    int y = (int)((float)upper_bound_ref<kGuideMarginal>(e.marginal, e.height, ey, e.guide_m) - 1.f);
     y = y < 0 ? 0 : (y >= e.height ? e.height - 1 : y);
-    int x = (int)((float)upper_bound_ref(e.cond + (size_t)y * e.width, e.width, ex) - 1.f);
+    int x = (int)((float)upper_bound_ref<kGuideCond>(e.cond + (size_t)y * e.width, e.width, ex, guide_row(e, y)) - 1.f);
     x = x < 0 ? 0 : (x >= e.width ? e.width - 1 : x);
     float u = (float)x / (float)e.width;
     float v = (float)y / (float)e.height;
@@ -573,9 +603,9 @@ FF_D void env_sample(const FFEnvView& e, float3 pos, float ex, float ey, float3&
 FF_D void env_sample_corrected(const FFEnvView& e, float3 pos, float ex, float ey, float jx, float jy, float3& wi,
                                float3& sp)
 {
-    int y = (int)((float)upper_bound_ref(e.marginal, e.height, ey) - 1.f);
+    int y = (int)((float)upper_bound_ref<kGuideMarginal>(e.marginal, e.height, ey, e.guide_m) - 1.f);
     y = y < 0 ? 0 : (y >= e.height ? e.height - 1 : y);
-    int x = (int)((float)upper_bound_ref(e.cond + (size_t)y * e.width, e.width, ex) - 1.f);
+    int x = (int)((float)upper_bound_ref<kGuideCond>(e.cond + (size_t)y * e.width, e.width, ex, guide_row(e, y)) - 1.f);
     x = x < 0 ? 0 : (x >= e.width ? e.width - 1 : x);
     const float u = ((float)x + jx) / (float)e.width;
     const float v = ((float)y + jy) / (float)e.height;

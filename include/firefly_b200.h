@@ -520,6 +520,13 @@ FF_API ff_status ff_debug_fail_alloc_after(int64_t n);
  * FF_ERR_TIMEOUT; the kernel first waits, with the built-in bound, for the
  * tensor-core work it issued, then frees its tensor memory. */
 FF_API ff_status ff_debug_cache_wait_limit(ff_cache* cache, uint32_t polls);
+/* The texel the environment light's importance sampling picks for each of
+ * n draw pairs (ex, ey) (host array of 2n floats): the two CDF searches of
+ * get_direction (CUDA-RayTracer/dEnvironmentLight.cu:41-58) as the path
+ * kernels run them, guide tables included, on the device.  xy (host, 2n
+ * int32) receives the column x and row y of each pick.  For tests of the
+ * searches against the tables of ff_scene_read_env_tables. */
+FF_API ff_status ff_debug_env_pick(const ff_scene* scene, const float* exy, uint64_t n, int32_t* xy);
 
 #ifdef __cplusplus
 }

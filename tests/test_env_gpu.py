@@ -51,6 +51,95 @@ def test_env_tables_match_oracle(ctx, oracle, w, h):
     ds.close()
 
 
+def _upper_bound(lst, vals):
+    """upper_bound of Helpers.cu:16-31 for float32 draws: the binary search's
+    end index (numpy's right-sided search where the list is sorted, the loop
+    itself where it is not), then the reference's list[left <= val] step."""
+    vals = np.asarray(vals, np.float32)
+    n = len(lst)
+    if np.all(lst[:-1] <= lst[1:]):
+        left = np.searchsorted(lst, vals.astype(np.float64), side="right")
+    else:
+        left = np.empty(len(vals), np.int64)
+        for i, v in enumerate(vals.astype(np.float64)):
+            lo, hi = 0, n
+            while lo < hi:
+                mid = (hi - lo) // 2 + lo
+                if v >= lst[mid]:
+                    lo = mid + 1
+                else:
+                    hi = mid
+            left[i] = lo
+    idx = np.where(left.astype(np.float32) <= vals, 1, 0)
+    return left + ((left < n) & (lst[idx] != 0.0))
+
+
+def _picks_expected(marginal, cond, exy):
+    h, w = cond.shape
+    y = np.clip(_upper_bound(marginal, exy[:, 1]) - 1, 0, h - 1)
+    x = np.empty(len(exy), np.int64)
+    for row in np.unique(y):
+        sel = y == row
+        x[sel] = np.clip(_upper_bound(cond[row], exy[sel, 0]) - 1, 0, w - 1)
+    return x, y
+
+
+def _edge_draws(values, rng, n_random):
+    """Uniform draws, the guide tables' bucket edges k / G, the table entries
+    themselves as floats, their float neighbours, and 0 and 1."""
+    edges = np.concatenate([np.arange(1025) / 1024.0, np.arange(513) / 512.0, values, [0.0, 1.0]]).astype(np.float32)
+    edges = edges[(edges >= 0) & (edges <= 1)]
+    near = np.concatenate([edges, np.nextafter(edges, np.float32(0)), np.nextafter(edges, np.float32(1))])
+    return np.concatenate([rng.random(n_random, dtype=np.float32), near]).astype(np.float32)
+
+
+@pytest.mark.parametrize("case", ["sky_sun_2048", "zero_rows_256"])
+def test_env_pick_matches_full_search(ctx, case):
+    """The light sample's texel (guided CDF searches, ff_debug_env_pick) is
+    the one the reference's full upper_bound searches pick, draw for draw,
+    on the device's own tables: at the C2 sky (2048 x 1024, 0.5 degree sun of
+    5e4) and at a sky with black rows and black runs of texels (CDF plateaus,
+    rows of zero probability whose conditional CDF is NaN)."""
+    import firefly_b200 as ff
+    rng = np.random.default_rng(7)
+    if case == "sky_sun_2048":
+        env = scenes.sky_env(2048, 1024, seed=0)
+    else:
+        env = scenes.sky_env(256, 128, seed=3, sun_radiance=500.0, sun_diameter_deg=3.0)
+        env[40:56] = 0.0
+        env[70:90, 10:120] = 0.0
+    scn = scenes.sphere_under_sky(seed=0)
+    scn.env_rgb = env
+    h, w = env.shape[:2]
+    ds = ff.dScene(ctx, scn)
+    marginal, cond, _, _ = _tables(ds, w, h)
+    ok = np.all(np.isfinite(cond), axis=1)
+    # the CDFs are running sums: every finite row is sorted (the guide tables then apply)
+    assert np.all(marginal[:-1] <= marginal[1:])
+    assert np.all(cond[ok, :-1] <= cond[ok, 1:])
+    # ey: draws and edges of the marginal; ex: draws and edges of the rows the
+    # draws land in (plus the sun's row)
+    ey = _edge_draws(marginal, rng, 200_000)
+    rows = np.unique(np.clip(_upper_bound(marginal, ey[:2000]) - 1, 0, h - 1))
+    ex_vals = _edge_draws(cond[rows[:16]].ravel(), rng, 200_000)
+    m = max(len(ex_vals), len(ey))
+    exy = np.stack([np.resize(ex_vals, m), np.resize(rng.permutation(ey), m)], axis=1).astype(np.float32)
+    # every ex edge also against the row the sun sits in
+    sun_row = int(np.argmax(np.diff(marginal, prepend=0.0)))
+    ey_sun = np.float32(marginal[sun_row - 1] if sun_row > 0 else 0.0)
+    exy = np.concatenate([exy, np.stack([ex_vals, np.full(len(ex_vals), ey_sun, np.float32)], axis=1)])
+    exy = np.ascontiguousarray(exy, np.float32)
+    xy = np.zeros((len(exy), 2), np.int32)
+    st = ff.lib().ff_debug_env_pick(ds.handle, exy.ctypes.data_as(C.c_void_p), len(exy),
+                                    xy.ctypes.data_as(C.c_void_p))
+    assert st == 0
+    x, y = _picks_expected(marginal, cond, exy)
+    print(f"[env pick] {case}: {len(exy)} draws, {len(np.unique(y))} rows, {int((~ok).sum())} NaN rows")
+    assert np.array_equal(xy[:, 1], y)
+    assert np.array_equal(xy[:, 0], x)
+    ds.close()
+
+
 def test_env_render_parity(ctx, oracle):
     import firefly_b200 as ff
     scn = scenes.sphere_under_sky(seed=0, width=64, height=64)
