@@ -3,6 +3,7 @@
 // Every entry point catches FFError and CUDA failures and returns an
 // ff_status; nothing here exits or aborts the process (the reference calls
 // exit(99) from checkCudaErrors, CUDA-RayTracer/CudaHelpers.cpp:3-11).
+#include <algorithm>
 #include <cstring>
 #include <new>
 
@@ -116,6 +117,12 @@ ff_status ff_context_destroy(ff_context* ctx)
         ctx->io_rays.release();
         ctx->io_hits.release();
         for (auto& b : ctx->adj_io) b.release();
+        if (ctx->io_in) cudaStreamSynchronize(ctx->io_in);
+        if (ctx->io_out) cudaStreamSynchronize(ctx->io_out);
+        for (cudaEvent_t e : {ctx->io_ev_start, ctx->io_ev_in, ctx->io_ev_traced})
+            if (e) cudaEventDestroy(e);
+        if (ctx->io_in) cudaStreamDestroy(ctx->io_in);
+        if (ctx->io_out) cudaStreamDestroy(ctx->io_out);
         if (ctx->ev0) cudaEventDestroy(ctx->ev0);
         if (ctx->ev1) cudaEventDestroy(ctx->ev1);
         ff_wavefront_ws_free(ctx->adj_ws);
@@ -248,6 +255,61 @@ ff_status ff_scene_read_bvh(const ff_scene* s, void* nodes, uint64_t nodes_capac
     });
 }
 
+namespace {
+
+// Rays per chunk of a host-pointer trace: 64 MB in, 32 MB out.
+constexpr uint64_t kIoChunk = 1ull << 21;
+
+// The host-pointer trace as a three-stage pipeline over chunks: the copy in
+// of chunk i + 1 (io_in) and the copy out of chunk i - 1 (io_out) run beside
+// the trace of chunk i (the context's stream), so both copy directions are
+// busy at once and the call takes about the longer of the two copies instead
+// of their sum.  Every chunk has its own range of the staging buffers; one
+// event per edge suffices because each wait is enqueued right after the
+// record it waits for.  Returns with all three streams' work enqueued; the
+// caller synchronises.
+void trace_host_chunks(ff_context* ctx, const ff_scene* s, const ff_ray* rays, uint64_t n, ff_hit* hits, bool any,
+                       bool two)
+{
+    if (!ctx->io_in) {
+        FF_CUDA_CHECK(cudaStreamCreateWithFlags(&ctx->io_in, cudaStreamNonBlocking));
+        FF_CUDA_CHECK(cudaStreamCreateWithFlags(&ctx->io_out, cudaStreamNonBlocking));
+        FF_CUDA_CHECK(cudaEventCreateWithFlags(&ctx->io_ev_start, cudaEventDisableTiming));
+        FF_CUDA_CHECK(cudaEventCreateWithFlags(&ctx->io_ev_in, cudaEventDisableTiming));
+        FF_CUDA_CHECK(cudaEventCreateWithFlags(&ctx->io_ev_traced, cudaEventDisableTiming));
+    }
+    ff_ray* d_rays = ctx->io_rays.as<ff_ray>();
+    ff_hit* d_hits = ctx->io_hits.as<ff_hit>();
+    try {
+        // the copies in start after the work already on the context's stream
+        FF_CUDA_CHECK(cudaEventRecord(ctx->io_ev_start, ctx->stream));
+        FF_CUDA_CHECK(cudaStreamWaitEvent(ctx->io_in, ctx->io_ev_start, 0));
+        for (uint64_t off = 0; off < n; off += kIoChunk) {
+            const uint64_t m = std::min(kIoChunk, n - off);
+            FF_CUDA_CHECK(cudaMemcpyAsync(d_rays + off, rays + off, sizeof(ff_ray) * m, cudaMemcpyHostToDevice,
+                                          ctx->io_in));
+            FF_CUDA_CHECK(cudaEventRecord(ctx->io_ev_in, ctx->io_in));
+            FF_CUDA_CHECK(cudaStreamWaitEvent(ctx->stream, ctx->io_ev_in, 0));
+            ff_launch_trace(ctx, s, d_rays + off, m, d_hits + off, any, two);
+            FF_CUDA_CHECK(cudaEventRecord(ctx->io_ev_traced, ctx->stream));
+            FF_CUDA_CHECK(cudaStreamWaitEvent(ctx->io_out, ctx->io_ev_traced, 0));
+            FF_CUDA_CHECK(cudaMemcpyAsync(hits + off, d_hits + off, sizeof(ff_hit) * m, cudaMemcpyDeviceToHost,
+                                          ctx->io_out));
+        }
+        // the context's stream ends after the last copy out
+        FF_CUDA_CHECK(cudaEventRecord(ctx->io_ev_traced, ctx->io_out));
+        FF_CUDA_CHECK(cudaStreamWaitEvent(ctx->stream, ctx->io_ev_traced, 0));
+    } catch (...) {
+        // no copy may still touch the caller's buffers after the call returns
+        cudaStreamSynchronize(ctx->io_in);
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamSynchronize(ctx->io_out);
+        throw;
+    }
+}
+
+}  // namespace
+
 ff_status ff_trace(ff_context* ctx, const ff_scene* s, const ff_ray* rays, uint64_t n, ff_hit* hits,
                    uint32_t flags)
 {
@@ -270,11 +332,7 @@ ff_status ff_trace(ff_context* ctx, const ff_scene* s, const ff_ray* rays, uint6
         } else {
             ctx->io_rays.alloc(sizeof(ff_ray) * n);
             ctx->io_hits.alloc(sizeof(ff_hit) * n);
-            FF_CUDA_CHECK(cudaMemcpyAsync(ctx->io_rays.ptr, rays, sizeof(ff_ray) * n, cudaMemcpyHostToDevice,
-                                          ctx->stream));
-            ff_launch_trace(ctx, s, ctx->io_rays.as<ff_ray>(), n, ctx->io_hits.as<ff_hit>(), any, two);
-            FF_CUDA_CHECK(cudaMemcpyAsync(hits, ctx->io_hits.ptr, sizeof(ff_hit) * n, cudaMemcpyDeviceToHost,
-                                          ctx->stream));
+            trace_host_chunks(ctx, s, rays, n, hits, any, two);
             unsigned int err = 0;
             FF_CUDA_CHECK(cudaMemcpyAsync(&err, ctx->counters.as<char>() + 8, sizeof(err), cudaMemcpyDeviceToHost,
                                           ctx->stream));

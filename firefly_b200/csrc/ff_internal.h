@@ -99,6 +99,10 @@ struct ff_context {
     std::string last_error;
     DevBuf counters;      // small scratch of uint32 counters for persistent kernels
     DevBuf io_rays, io_hits;  // staging for host-pointer ff_trace calls
+    // host-pointer ff_trace: rays copied in on io_in, hits copied out on
+    // io_out, each chunk's trace on `stream` between them (created on first use)
+    cudaStream_t io_in = nullptr, io_out = nullptr;
+    cudaEvent_t io_ev_start = nullptr, io_ev_in = nullptr, io_ev_traced = nullptr;
     DevBuf adj_io[5];         // ff_render_adjoint: staged image, texture / env / roughness gradients, counters
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     FFWavefrontWS* adj_ws = nullptr;   // path pool of ff_render_adjoint, kept between calls
