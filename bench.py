@@ -90,6 +90,15 @@ SHADOW_QUEUE_BYTES = 36
 # hits, shaded vertices, extension rays, shadow rays).
 RENDER_DRAM_BYTES_PER_UNIT = {"k_logic": 456.8, "k_shade (all kinds)": 418.7,
                               "k_trace<closest> (extension queue)": 109.4, "k_trace<any> (shadow queue)": 48.5}
+# Issue slots busy (smsp__issue_active) of the closest-hit traversal on C2:
+# ncu --set full of one steady-state launch of the same 16-spp, 2M-slot step
+# (a figure from that capture, not measured by this run).
+RENDER_ISSUE_SLOTS = {"k_trace<closest> (extension queue)": 0.696}
+# Issue slots busy of the trace micro-benchmark's four launches (ncu --set full
+# of one launch per batch kind, 4,194,304 rays each; figures from that
+# capture, not measured by this run): the traversal is issue-bound.
+TRACE_ISSUE_SLOTS = {"coherent_closest": 0.835, "incoherent_closest": 0.775, "coherent_any": 0.804,
+                     "incoherent_any": 0.749}
 RENDER = dict(width=1920, height=1080, spp=64, max_depth=8, rr_depth=3)
 # Measured DRAM bytes per unit of the adjoint's stages (ncu over the profiled
 # 512x512, 16-spp adjoint call of --workload inverse, 12 frames): per
@@ -572,7 +581,12 @@ def trace_line(args, ws, rank, local, dist, ctx, dev, stream, steps):
                          "traffic": int(TRACE_DRAM_BYTES_PER_RAY[batches[k_dom][0]] * n),
                          "traffic_source": "ncu dram__bytes_read+write of a 4,194,304-ray launch, scaled to the "
                                            "launch's rays",
-                         "peak_source": peak_kind, "bytes_per_ray": RAY_BYTES + HIT_BYTES, "l2_fetch": l2_fetch},
+                         "peak_source": peak_kind, "bytes_per_ray": RAY_BYTES + HIT_BYTES, "l2_fetch": l2_fetch,
+                         "issue_slots_busy": {"per_batch": TRACE_ISSUE_SLOTS,
+                                              "source": "ncu smsp__issue_active of one launch per batch kind "
+                                                        "(4,194,304 rays), not measured by this run",
+                                              "note": "the bound of this kernel: instruction issue under "
+                                                      "divergence, not HBM (frac) or L2 (l2_fetch)"}},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": int(rays_per_step * RAY_BYTES),
                     "d2h_bytes_per_step": int(rays_per_step * HIT_BYTES)},
@@ -719,14 +733,19 @@ def run_render(args, ws, rank, local, dist):
                                          + prof["shadow_rays"] * SHADOW_QUEUE_BYTES,
                                          f"{RENDER_SHADE_BYTES_PER_VERTEX} B of slot records and queue entries per "
                                          f"shaded vertex + {SHADOW_QUEUE_BYTES} B per shadow-queue entry")}
-        dom = max(stage, key=lambda k: stage[k][0])
+        units = {"k_logic": prof["extension_rays"], "k_shade (all kinds)": vertices,
+                 "k_trace<closest> (extension queue)": prof["extension_rays"],
+                 "k_trace<any> (shadow queue)": prof["shadow_rays"]}
+        # the HBM roofline's kernel: the stage that moves the most DRAM bytes
+        # in the step (measured bytes per unit x units).  The three stages on
+        # the frame's critical path take about the same device time each, and
+        # the two traversals are bound by instruction issue, not by HBM
+        dram_step = {k: RENDER_DRAM_BYTES_PER_UNIT[k] * units[k] for k in stage}
+        dom = max(stage, key=lambda k: dram_step[k])
         dms, dbytes, dnote = stage[dom]
         achieved = dbytes / (dms / 1e3) / 1e9
         # DRAM traffic of one launch sequence (one frame) of the dominant
         # stage: the measured bytes per unit times the frame's average units
-        units = {"k_logic": prof["extension_rays"], "k_shade (all kinds)": vertices,
-                 "k_trace<closest> (extension queue)": prof["extension_rays"],
-                 "k_trace<any> (shadow queue)": prof["shadow_rays"]}
         frames = max(1, prof["frames"])
         traffic = int(RENDER_DRAM_BYTES_PER_UNIT[dom] * units[dom] / frames)
         alg_launch = int(dbytes / frames)
@@ -787,10 +806,18 @@ def run_render(args, ws, rank, local, dist):
                          "algorithmic_bytes": dnote, "algorithmic_bytes_per_launch": alg_launch,
                          "traffic_note": ("bytes per frame's launch sequence of the dominant stage: ncu DRAM bytes "
                                           "per unit of a 16-spp step on a 2M-slot pool x this step's units per frame"),
+                         "selection": ("the stage with the most DRAM bytes in the step (dram_gb_per_step); the "
+                                       "stages' device times (ms) are within a few percent of each other, and the "
+                                       "traversals are bound by instruction issue (see issue_slots_busy and "
+                                       "l2_fetch), where an HBM fraction does not apply"),
                          "stages": {k: {"ms": round(v[0], 2), "achieved_gbs": round(v[1] / (v[0] / 1e3) / 1e9, 1)
                                         if v[0] > 0 else None,
+                                        "frac": round(v[1] / (v[0] / 1e3) / 1e9 / peak, 4) if v[0] > 0 else None,
                                         "algorithmic_bytes_per_unit": round(v[1] / max(1, units[k]), 1),
-                                        "dram_bytes_per_unit": RENDER_DRAM_BYTES_PER_UNIT[k]}
+                                        "dram_bytes_per_unit": RENDER_DRAM_BYTES_PER_UNIT[k],
+                                        "dram_gb_per_step": round(dram_step[k] / args.steps / 1e9, 1),
+                                        **({"issue_slots_busy": RENDER_ISSUE_SLOTS[k]} if k in RENDER_ISSUE_SLOTS
+                                           else {})}
                                     for k, v in stage.items()},
                          "l2_fetch": l2_fetch},
             "cpu_baseline": cpu,
