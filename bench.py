@@ -737,7 +737,7 @@ def run_render(args, ws, rank, local, dist):
                  "k_trace<closest> (extension queue)": prof["extension_rays"],
                  "k_trace<any> (shadow queue)": prof["shadow_rays"]}
         # the HBM roofline's kernel: the stage that moves the most DRAM bytes
-        # in the step (measured bytes per unit x units).  The three stages on
+        # in the step (measured bytes per unit x the profiled step's units).  The three stages on
         # the frame's critical path take about the same device time each, and
         # the two traversals are bound by instruction issue, not by HBM
         dram_step = {k: RENDER_DRAM_BYTES_PER_UNIT[k] * units[k] for k in stage}
@@ -815,7 +815,7 @@ def run_render(args, ws, rank, local, dist):
                                         "frac": round(v[1] / (v[0] / 1e3) / 1e9 / peak, 4) if v[0] > 0 else None,
                                         "algorithmic_bytes_per_unit": round(v[1] / max(1, units[k]), 1),
                                         "dram_bytes_per_unit": RENDER_DRAM_BYTES_PER_UNIT[k],
-                                        "dram_gb_per_step": round(dram_step[k] / args.steps / 1e9, 1),
+                                        "dram_gb_per_step": round(dram_step[k] / 1e9, 1),
                                         **({"issue_slots_busy": RENDER_ISSUE_SLOTS[k]} if k in RENDER_ISSUE_SLOTS
                                            else {})}
                                     for k, v in stage.items()},
