@@ -1,7 +1,7 @@
 """Image parity of ff_render against the oracle's restatement of the
 reference's wavefront stages, with the same per-pixel sampler seeds.
 
-Tolerance (north star): mean relative error <= 1e-4, measured as
+Tolerance: mean relative error <= 1e-4 (the bar for floating-point parity), measured as
     mre = sum |gpu - oracle| / sum |oracle|
 over all pixels and channels of the per-pixel mean radiance.  Both sides
 follow the reference's arithmetic operation by operation; what remains are
