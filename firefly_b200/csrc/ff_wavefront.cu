@@ -113,7 +113,9 @@ constexpr uint32_t kStampBase = 16;
 // Deferred mode: blocks per SM of the any-hit trace (its persistent grid, of
 // 8 that fit), leaving the rest of each SM to k_logic and k_shade of the next
 // frame.  Measured on the 1.3M-triangle scene at 64 spp: 3 blocks 262.7 ms
-// per step, 4: 265.4-266.0, 5: 268.7, 6: 272.7.
+// per step, 4: 265.4-266.0, 5: 268.7, 6: 272.7; later, against 256.3-256.4
+// with 3: 2 blocks 267.4-267.6, 1: 298.2 (the trace then outlasts the next
+// frame, whose successor waits for it).
 constexpr int kDeferShadowBlocks = 3;   // stamps of real frames are >= 16; 0 marks an empty record
 constexpr uint32_t kVtxMatBits = 24, kVtxLenShift = 24, kVtxLenMask = 0x7f;
 // Byte of shadow ray k's answer for slot s in the SlotRay array (the tag the
