@@ -34,7 +34,8 @@ def test_env_tables_match_oracle(ctx, oracle, w, h):
     ds = ff.dScene(ctx, scn)
     gm, gc, gp, gd = _tables(ds, w, h)
     rm, rc, rp, rd = oracle.env_build(scn.env_rgb)
-    # The FP64 sums are reassociated into block reductions and scans, and the
+    # The FP64 row sums and the denominator are reassociated into block
+    # reductions (the CDFs are running sums in the reference's order), and the
     # float sine of a row (sin(M_PI * v), a float in the reference) can land
     # one float ulp away from the host libm's sinf (row 6 of 64 does: glibc
     # returns 0.2902847, the device's correctly rounded double sine gives
