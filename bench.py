@@ -1093,7 +1093,7 @@ def inverse_line(args, ws, rank, local, dist, ctx, dev, stream, known_lighting_r
 def inverse_e2e(ctx, dev, stream, iters=5, res=512):
     """The adjoint through the public API with host buffers: d_image in,
     texture and env gradients out, every call (ff_render_adjoint with host
-    pointers)."""
+    pointers into pinned host memory, as the other lines' e2e)."""
     import torch
     import firefly_b200 as ff
     from firefly_b200 import scenes
@@ -1101,9 +1101,13 @@ def inverse_e2e(ctx, dev, stream, iters=5, res=512):
     scn = scenes.textured_room(seed=0, width=res, height=res, tex_res=512, env=sky)
     ds = ff.dScene(ctx, scn)
     rng = np.random.default_rng(0)
-    d_image = (rng.normal(size=(res, res, 3)) / (res * res * 3)).astype(np.float32)
-    g_tex = np.zeros((512, 512, 3), np.float32)
-    g_env = np.zeros_like(sky, dtype=np.float32)
+
+    def pinned(shape):
+        return torch.zeros(shape, dtype=torch.float32).pin_memory().numpy()
+    d_image = pinned((res, res, 3))
+    d_image[...] = (rng.normal(size=(res, res, 3)) / (res * res * 3)).astype(np.float32)
+    g_tex = pinned((512, 512, 3))
+    g_env = pinned(sky.shape)
     ds.render_adjoint(res, res, d_image, grad_texture=g_tex, grad_env=g_env, spp=16, seed=1)
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
